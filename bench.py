@@ -1,0 +1,383 @@
+"""Benchmark of the icFlow assembly path on B200.
+
+One step = one Newton assembly (zero + tetrahedra + cohesive zones with damage
+state and flags + contact response -> BCSR values and rhs) of a fixed
+structure, on the polycrystal-compression workload: 1 mm cube, 32^3
+hexahedra split into 196,608 tets, 128 Voronoi grains with cohesive zones on
+every grain boundary (per-boundary lognormal strengths, mean 1 MPa, cv 0.2),
+two rigid platens overlapping the cube by a quarter cell (penalty 1e8),
+dt = 1e-5 s, FP64.  Inputs are synthetic (seeded), as icFlow ships no setups.
+
+  value  assemblies/s with inputs resident in HBM (device events around each
+         step; L2 is flushed between steps by writing a 256 MiB buffer, outside
+         the timed region)
+  e2e    the same through the C ABI with host buffers: H2D of the tentative
+         node state (un, vn, an) from pinned memory, assembly, D2H of vals and
+         rhs into pinned memory, every step
+
+`--impl reference` times the reference's own kernels compiled for the host
+(oracle/_ref, all host threads) on the same workload.  Under torchrun each rank
+assembles its own specimen (seed = rank, weak scaling, no collective in the
+data path); timing is max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Newton assemblies/s (elem+CZ+contact->BCSR)"
+H = 1e-5
+FLUSH_BYTES = 256 << 20
+
+
+def build_workload(seed: int, n: int = 32, grains: int = 128):
+    from icflow_b200 import mesh as M
+
+    coll = M.polycrystal(n=n, grains=grains, seed=seed, platens=True, gap=-0.25)
+    rng = np.random.default_rng(seed + 101)
+    nn = len(coll.x0)
+    # a compressed state: uniform strain 1e-4 toward the mid-plane plus noise
+    zc = 0.5e-3
+    un = np.zeros((nn, 3))
+    un[:, 2] = -1e-4 * (coll.x0[:, 2] - zc)
+    un += (rng.random((nn, 3)) - 0.5) * 2e-9
+    un[coll.anchored] = 0.0
+    vn = (rng.random((nn, 3)) - 0.5) * 1e-3
+    an = (rng.random((nn, 3)) - 0.5) * 1e-1
+    sig = M.lognormal_strengths(len(coll.czs), seed=seed, granule_pairs=coll.meshes[0].cz_grains)
+    pairs = M.candidate_pairs(coll, coll.x0 + un)
+    return coll, (un, vn, an), sig, pairs
+
+
+def algorithmic_bytes(nnz, n_active, n_nodes, n_tet, n_cz, n_imp) -> int:
+    """Compulsory traffic of one assembly, FP64 layout, each item once:
+    72 B per 3x3 block written, 24 B per rhs row, 96 B per node (x0, u, v, a),
+    56 B per tet (4 ids + 10 upper-block slots), 240 B per CZ (6 ids, 21 slots,
+    6 state in, 6 tentative out, 4 averages, flags), 56 B per impact."""
+    return 72 * nnz + 24 * n_active + 96 * n_nodes + 56 * n_tet + 240 * n_cz + 56 * n_imp
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-assembly DRAM bytes from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "assembly_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("dram_bytes_per_assembly")
+        except (ValueError, OSError):
+            return None
+    return None
+
+
+def cpu_baseline(coll, state, sig, pairs, bound_s: float = 12.0, nthreads: int = 0):
+    """The reference's own kernels (oracle/_ref) on the host over the same
+    workload; returns (assemblies/s, threads, kind, sample)."""
+    from oracle.oracle import Oracle, RefKernels, ref_available
+
+    O = Oracle()
+    kind = "reference" if ref_available() else "port"
+    from icflow_b200.model_prms import config_prms
+
+    prms = config_prms(penaltyK=1e8)
+    from tests.harness import orc_prms_from
+
+    p = orc_prms_from(O, prms)
+    un, vn, an = state
+    xt = coll.x0 + un
+    masks = O.narrow_phase(pairs, coll.selem, xt)
+    imps = O.impacts(pairs, masks, coll.selem, coll.adj_off, coll.adj, coll.faces, xt)
+    N, rows, cols = O.build_structure(coll.alt, coll.elems, coll.czs, imps)
+    ep = O.pcsr(coll.elems, 4, coll.alt, rows, cols, N)
+    cp = O.pcsr(coll.czs, 6, coll.alt, rows, cols, N)
+    ipc = O.pcsr(imps, 4, coll.alt, rows, cols, N)
+    nc = len(coll.czs)
+    pmax = np.zeros((nc, 3))
+    tmax = np.zeros((nc, 3))
+    threads = nthreads or os.cpu_count()
+    if kind == "reference":
+        R = RefKernels(nthreads=threads)
+        R.set_constants(p)
+        qs = [O.ppr_for(p, s, s) for s in sig]
+        per_cz = (sig, sig, np.array([q.deln for q in qs]), np.array([q.delt for q in qs]))
+
+        def one():
+            st = R.pack_nodes(coll.x0, un, vn, an)
+            vals = np.zeros(9 * len(cols))
+            rhs = np.zeros(3 * N)
+            R.elem_kernel(st, H, coll.elems, ep, vals, rhs)
+            R.cz_kernel(st, H, coll.czs, cp, pmax, tmax, vals, rhs, per_cz=per_cz)
+            R.collision_kernel(st, H, imps, ipc, vals, rhs, prms.penaltyK, prms.DistanceEpsilon)
+    else:
+        threads = 1
+        qs = [O.ppr_for(p, s, s) for s in sig]
+
+        def one():
+            O.assemble(p, H, coll.x0, un, vn, an, coll.elems, ep, coll.czs, cp, pmax, tmax, imps, ipc,
+                       len(cols), N, cz_ppr=qs)
+    one()  # warm-up
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        one()
+        n += 1
+        if time.perf_counter() - t0 > bound_s:
+            break
+    dt = time.perf_counter() - t0
+    return n / dt, threads, kind, f"{n} full assemblies of the workload in {dt:.1f} s"
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    coll, state, sig, pairs = build_workload(0)
+    steps = max(args.steps, 1)
+    rate, threads, kind, sample = cpu_baseline(coll, state, sig, pairs,
+                                               bound_s=min(60.0, 2.0 * steps))
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "assemblies/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / rate, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "polycrystal compression, 1 mm cube, 196608 tets, 128 grains, "
+                                   "CZs on grain boundaries, rigid platens in contact",
+                       "tets": int(len(coll.elems)), "czs": int(len(coll.czs))},
+            "cpu_baseline": {"value": rate, "unit": "assemblies/s", "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "assemblies/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    from icflow_b200 import _lib
+    from icflow_b200.gpu_functionality import GPU_Functionality
+    from icflow_b200.model_prms import config_prms
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = local if ws > 1 else 0
+    torch.cuda.set_device(dev)
+
+    coll, state, sig, pairs = build_workload(rank)
+    prms = config_prms(penaltyK=1e8)
+    gf = GPU_Functionality(dev)
+    gf.prms = prms
+    gf.mc = coll
+    gf.SetConstants()
+    gf.TransferStaticDataToDevice()
+    gf.SetCZStrengths(sig, sig)
+    un, vn, an = state
+    gf.TransferNodesToGPU(un, vn, an)
+    nc = len(coll.czs)
+    gf.TransferPCSR(np.zeros((nc, 3)), np.zeros((nc, 3)), np.zeros(nc, np.int32))
+    imps = gf.NarrowPhaseCollisionDetection(pairs)
+    N, nnz = gf.CreateStructure(copy_back=False)
+    lib = gf.lib
+    bufs = gf.DeviceBuffers()
+    stream = torch.cuda.ExternalStream(bufs.stream, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+
+    def assemble_async():
+        rc = lib.icf_assemble_async(gf.ctx, H)
+        if rc:
+            _lib.check(gf.ctx, rc)
+
+    # warm-up
+    for _ in range(args.warmup):
+        assemble_async()
+    cnt = _lib.icf_counts()
+    _lib.check(gf.ctx, lib.icf_read_counts(gf.ctx, C.byref(cnt)))
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+
+    # device-resident timing, L2 flushed between steps outside the events
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(dev) as clk:
+        barrier()
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.zero_()
+                starts[i].record(stream)
+                assemble_async()
+                ends[i].record(stream)
+        barrier()
+        ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+        ms_dev = float(np.mean(ms))
+
+        # end to end through the C ABI with pinned host buffers
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+        hun, hvn, han = pin(un), pin(vn), pin(an)
+        hvals = torch.empty(9 * nnz, dtype=torch.float64).pin_memory().numpy()
+        hrhs = torch.empty(3 * N, dtype=torch.float64).pin_memory().numpy()
+        for _ in range(max(1, args.warmup // 2)):
+            gf.TransferNodesToGPU(hun, hvn, han)
+            gf.AssembleElemsAndCZs(H)
+            gf.TransferLinearSystemToHost(hvals, hrhs)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            gf.TransferNodesToGPU(hun, hvn, han)
+            gf.AssembleElemsAndCZs(H)
+            gf.TransferLinearSystemToHost(hvals, hrhs)
+        e1.record(stream)
+        barrier()
+        ms_e2e = e0.elapsed_time(e1) / args.steps
+    clocks = clk.summary()
+
+    if ws > 1:
+        t = torch.tensor([ms_dev, ms_e2e], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_dev, ms_e2e = float(t[0]), float(t[1])
+
+    B = algorithmic_bytes(nnz, N, len(coll.x0), len(coll.elems), nc, len(imps))
+    peak, peak_kind = measured_peak()
+    achieved = B / (ms_dev * 1e-3) / 1e9
+    launches_per_step = 4 + (1 if len(imps) else 0) + (1 if len(imps) else 0)
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ws * 1000.0 / ms_dev, "unit": "assemblies/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded polycrystal; no public dataset exists for this path)",
+            "config": {"workload": "polycrystal compression, 1 mm cube, 32^3 hex -> 6 tets, 128 grains, "
+                                   "CZs on grain boundaries, rigid platens in contact, dt 1e-5",
+                       "tets": int(len(coll.elems)), "czs": int(nc), "nodes": int(len(coll.x0)),
+                       "active_rows": int(N), "blocks": int(nnz), "impacts": int(len(imps)),
+                       "l2": "flushed between steps (256 MiB write), outside the timed region"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": ncu_traffic(),
+                         "algorithmic_bytes": B, "peak_source": peak_kind,
+                         "scope": "whole assembly (all kernels of one step)"},
+            "e2e": {"value": ws * 1000.0 / ms_e2e, "unit": "assemblies/s",
+                    "h2d_bytes_per_step": int(3 * un.nbytes), "d2h_bytes_per_step": int(8 * (9 * nnz + 3 * N))},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks,
+        }
+        if not args.no_cpu:
+            rate, threads, kind, sample = cpu_baseline(coll, state, sig, pairs, bound_s=args.cpu_seconds)
+            line["cpu_baseline"] = {"value": rate, "unit": "assemblies/s", "cores": threads, "kind": kind,
+                                    "sample": sample}
+    gf.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

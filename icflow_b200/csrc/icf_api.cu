@@ -1,0 +1,686 @@
+// icf_api.cu -- the extern "C" entry points of libicflow_b200.
+//
+// Each function mirrors one public member of icFlow's GPU_Functionality
+// (v3Library/Simulation/GPU/GPU_Functionality.cs) or of the classes it works
+// with; the header include/icflow_b200.h lists the correspondence.  Errors are
+// returned as negative codes with a message in icf_last_error(); nothing
+// throws across the ABI.
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "icf_internal.cuh"
+
+// ---- helpers -----------------------------------------------------------------
+int icf_fail(icf_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int icf_scratch(icf_ctx *ctx, size_t bytes) {
+  if (bytes <= ctx->tmp_bytes && ctx->d_tmp) return ICF_OK;
+  cudaFree(ctx->d_tmp);
+  ctx->d_tmp = nullptr;
+  const size_t b = bytes + bytes / 4 + 1024;
+  cudaError_t e = cudaMalloc(&ctx->d_tmp, b);
+  if (e != cudaSuccess) {
+    ctx->tmp_bytes = 0;
+    return icf_fail(ctx, ICF_ERR_CUDA, std::string("scratch allocation: ") + cudaGetErrorString(e));
+  }
+  ctx->tmp_bytes = b;
+  return ICF_OK;
+}
+
+template <typename T>
+static int dalloc(icf_ctx *ctx, T **p, size_t n) {
+  cudaFree(*p);
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(p, sizeof(T) * n);
+  if (e != cudaSuccess)
+    return icf_fail(ctx, ICF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return ICF_OK;
+}
+
+#define ICF_TRY(x)            \
+  do {                        \
+    int rc_ = (x);            \
+    if (rc_ != ICF_OK) return rc_; \
+  } while (0)
+
+#define ICF_CHECK_CTX(ctx)                        \
+  do {                                            \
+    if (!(ctx)) return ICF_ERR_ARG;               \
+    cudaError_t e_ = cudaSetDevice((ctx)->device); \
+    if (e_ != cudaSuccess)                        \
+      return icf_fail((ctx), ICF_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+static double macaulay(double a, double b) { return a > b ? a - b : 0.0; }
+
+// Normal and tangential characteristic lengths of the PPR potential
+// (ModelPrms.cs:284-285) for given strengths.
+static void ppr_lengths(const icf_params *p, double f_tn, double f_tt, double *deln, double *delt) {
+  const double a = p->alpha, b = p->beta, rn = p->lambda_n, rt = p->lambda_t;
+  *deln = (p->phi_n / f_tn) * a * rn * std::pow(1.0 - rn, a - 1.0) * ((a / p->p_m) + 1.0) *
+          std::pow((a / p->p_m) * rn + 1.0, p->p_m - 1.0);
+  *delt = (p->phi_t / f_tt) * b * rt * std::pow(1.0 - rt, b - 1.0) * ((b / p->p_n) + 1.0) *
+          std::pow((b / p->p_n) * rt + 1.0, p->p_n - 1.0);
+}
+
+icf_dprm icf_make_dprm(const icf_ctx *ctx) {
+  const icf_params &p = ctx->prm;
+  icf_dprm d;
+  d.lam = p.E[1];       // nu * Y / ((1+nu)(1-2nu))
+  d.mu = p.E[3 * 6 + 3]; // (1/2 - nu) * Y / ((1+nu)(1-2nu))
+  d.rho20 = p.rho / 20.0;
+  d.dm = p.dampingMass;
+  d.ds = p.dampingStiffness;
+  d.nbeta = p.NewmarkBeta;
+  d.ngamma = p.NewmarkGamma;
+  d.grav_rho = p.gravity * p.rho;
+  d.f_tn = p.f_tn;
+  d.f_tt = p.f_tt;
+  d.alpha = p.alpha;
+  d.beta = p.beta;
+  d.rn = p.rn;
+  d.rt = p.rt;
+  d.p_m = p.p_m;
+  d.p_n = p.p_n;
+  d.deln = p.deln;
+  d.delt = p.delt;
+  d.pMtn = p.pMtn;
+  d.pMnt = p.pMnt;
+  d.gam_n = p.gam_n;
+  d.gam_t = p.gam_t;
+  for (int i = 0; i < 9; i++) d.sf[i] = p.sf[i];
+  d.penaltyK = p.penaltyK;
+  d.eps2 = p.DistanceEpsilon * p.DistanceEpsilon;
+  return d;
+}
+
+extern "C" {
+
+const char *icf_version(void) { return "icflow_b200 1.0 sm_100a"; }
+
+const char *icf_last_error(const icf_ctx *ctx) {
+  if (!ctx) return "null context";
+  return ctx->err.c_str();
+}
+
+// ModelPrms.SetComputedVariables (ModelPrms.cs:237-349) and the thresholds
+// of Recompute (:112-113).
+int icf_params_derive(icf_params *p) {
+  if (!p) return ICF_ERR_ARG;
+  const double mc = p->rho / 20.0;
+  for (int r = 0; r < 12; r++)
+    for (int c = 0; c < 12; c++) p->M[r * 12 + c] = (r % 3 == c % 3) ? (r == c ? 2.0 * mc : mc) : 0.0;
+  const double k = p->Y / ((1.0 + p->nu) * (1.0 - 2.0 * p->nu));
+  for (int i = 0; i < 36; i++) p->E[i] = 0;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) p->E[i * 6 + j] = (i == j ? 1.0 - p->nu : p->nu) * k;
+  for (int i = 3; i < 6; i++) p->E[i * 6 + i] = (0.5 - p->nu) * k;
+
+  p->G_fn = p->phi_n;
+  p->G_ft = p->phi_t;
+  p->f_tn = p->sigma_max;
+  p->f_tt = p->tau_max;
+  p->rn = p->lambda_n;
+  p->rt = p->lambda_t;
+  p->pMnt = macaulay(p->G_fn, p->G_ft);
+  p->pMtn = macaulay(p->G_ft, p->G_fn);
+  const double rn2 = p->rn * p->rn, rt2 = p->rt * p->rt;
+  p->p_m = (p->alpha * (p->alpha - 1.0) * rn2) / (1.0 - p->alpha * rn2);
+  p->p_n = (p->beta * (p->beta - 1.0) * rt2) / (1.0 - p->beta * rt2);
+  if (p->G_fn < p->G_ft) {
+    p->gam_n = std::pow(p->alpha / p->p_m, p->p_m);
+    p->gam_t = -p->G_ft * std::pow(p->beta / p->p_n, p->p_n);
+  } else {
+    p->gam_n = -p->G_fn * std::pow(p->alpha / p->p_m, p->p_m);
+    p->gam_t = std::pow(p->beta / p->p_n, p->p_n);
+  }
+  ppr_lengths(p, p->f_tn, p->f_tt, &p->deln, &p->delt);
+  p->nThreshold = p->deln * p->lambda_n;
+  p->tThreshold = p->delt * p->lambda_t;
+
+  const double g1[3] = {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0};
+  const double g2[3] = {2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0};
+  for (int gp = 0; gp < 3; gp++) {
+    p->sf[0 * 3 + gp] = 1.0 - g1[gp] - g2[gp];
+    p->sf[1 * 3 + gp] = g1[gp];
+    p->sf[2 * 3 + gp] = g2[gp];
+  }
+  for (int i = 0; i < 162; i++) p->B[i] = 0;
+  for (int gp = 0; gp < 3; gp++)
+    for (int n = 0; n < 3; n++)
+      for (int c = 0; c < 3; c++) {
+        p->B[(gp * 3 + c) * 18 + 3 * n + c] = p->sf[n * 3 + gp];
+        p->B[(gp * 3 + c) * 18 + 9 + 3 * n + c] = -p->sf[n * 3 + gp];
+      }
+  return ICF_OK;
+}
+
+int icf_create(int device, icf_ctx **out) {
+  if (!out) return ICF_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return ICF_ERR_NODEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) return ICF_ERR_NODEVICE;
+  icf_ctx *ctx = new (std::nothrow) icf_ctx();
+  if (!ctx) return ICF_ERR_SIZE;
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&ctx->d_counts, 8 * sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_counts, 8 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_norm, 260 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_norm, 2 * sizeof(double)) != cudaSuccess) {
+    delete ctx;
+    return ICF_ERR_CUDA;
+  }
+  memset(ctx->h_counts, 0, 8 * sizeof(int));
+  *out = ctx;
+  return ICF_OK;
+}
+
+static void free_all(icf_ctx *c) {
+  void *ptrs[] = {c->d_elem, c->d_cz, c->d_alt, c->d_selem, c->d_adj_off, c->d_adj, c->d_faces,
+                  c->d_x0, c->d_xc, c->d_va, c->d_u, c->d_v, c->d_a, c->d_du, c->d_un, c->d_h3,
+                  c->d_czs, c->d_czfail, c->d_cztent, c->d_czflags, c->d_czavg, c->d_czprm,
+                  c->d_es, c->d_cs, c->d_ks, c->d_skeys, c->d_rc_off, c->d_rc, c->d_rows, c->d_cols,
+                  c->d_src, c->d_mkeys, c->d_imp, c->d_cr_slot, c->d_cr_off, c->d_cr, c->d_pairs,
+                  c->d_masks, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
+                  c->imp_inc.off, c->imp_inc.inc, c->d_tmp};
+  for (void *p : ptrs) cudaFree(p);
+}
+
+int icf_destroy(icf_ctx *ctx) {
+  if (!ctx) return ICF_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  cudaFree(ctx->d_counts);
+  cudaFree(ctx->d_norm);
+  cudaFreeHost(ctx->h_counts);
+  cudaFreeHost(ctx->h_norm);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return ICF_OK;
+}
+
+int icf_set_constants(icf_ctx *ctx, const icf_params *p) {
+  ICF_CHECK_CTX(ctx);
+  if (!p) return icf_fail(ctx, ICF_ERR_ARG, "null params");
+  icf_params q = *p;
+  icf_params_derive(&q);
+  if (!(q.NewmarkBeta > 0) || !(q.deln > 0) || !(q.delt > 0) || !std::isfinite(q.p_m) ||
+      !std::isfinite(q.p_n))
+    return icf_fail(ctx, ICF_ERR_ARG, "parameters give a degenerate PPR law or Newmark scheme");
+  ctx->prm = q;
+  ctx->have_prm = true;
+  if (ctx->per_cz_prm) ctx->per_cz_prm = false;  // strengths must be set again
+  return ICF_OK;
+}
+
+int icf_set_precision(icf_ctx *ctx, int precision) {
+  ICF_CHECK_CTX(ctx);
+  if (precision != ICF_FP64 && precision != ICF_FP32_MIXED)
+    return icf_fail(ctx, ICF_ERR_ARG, "unknown precision");
+  ctx->precision = precision;
+  return ICF_OK;
+}
+
+int icf_set_cz_strength(icf_ctx *ctx, int n_czs, const double *sigma_max, const double *tau_max) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_prm) return icf_fail(ctx, ICF_ERR_STATE, "icf_set_constants first");
+  if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  if (!sigma_max || !tau_max) {
+    ctx->per_cz_prm = false;
+    return ICF_OK;
+  }
+  if (n_czs != ctx->n_cz) return icf_fail(ctx, ICF_ERR_ARG, "n_czs does not match the mesh");
+  std::vector<double4> h((size_t)n_czs);
+  for (int c = 0; c < n_czs; c++) {
+    if (!(sigma_max[c] > 0) || !(tau_max[c] > 0))
+      return icf_fail(ctx, ICF_ERR_ARG, "CZ strengths must be positive");
+    double dn, dt;
+    ppr_lengths(&ctx->prm, sigma_max[c], tau_max[c], &dn, &dt);
+    h[c] = make_double4(sigma_max[c], tau_max[c], dn, dt);
+  }
+  ICF_TRY(dalloc(ctx, &ctx->d_czprm, (size_t)n_czs));
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_czprm, h.data(), sizeof(double4) * (size_t)n_czs, cudaMemcpyHostToDevice));
+  ctx->per_cz_prm = true;
+  return ICF_OK;
+}
+
+int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *alt_id, int n_elems,
+                        const int *elems, int n_czs, const int *czs, int n_surface,
+                        const int *surface_elems, const int *adj_offsets, const int *adj_faces,
+                        int n_faces, const int *faces) {
+  ICF_CHECK_CTX(ctx);
+  if (n_nodes <= 0 || !x0 || !alt_id || n_elems < 0 || n_czs < 0 || n_surface < 0 || n_faces < 0)
+    return icf_fail(ctx, ICF_ERR_ARG, "bad sizes or null arrays");
+  if ((n_elems && !elems) || (n_czs && !czs) ||
+      (n_surface && (!surface_elems || !adj_offsets || !adj_faces || !faces)))
+    return icf_fail(ctx, ICF_ERR_ARG, "null unit arrays");
+  if (n_elems >= ICF_MAX_TET_UNITS || n_czs >= ICF_MAX_CZ_UNITS)
+    return icf_fail(ctx, ICF_ERR_SIZE, "unit count beyond the contribution-code range");
+  // host-side validation of every index (the kernels trust them)
+  int n_active = 0;
+  for (int i = 0; i < n_nodes; i++) {
+    if (alt_id[i] >= n_nodes) return icf_fail(ctx, ICF_ERR_ARG, "alt_id out of range");
+    if (alt_id[i] >= 0) n_active++;
+    if (!std::isfinite(x0[3 * i]) || !std::isfinite(x0[3 * i + 1]) || !std::isfinite(x0[3 * i + 2]))
+      return icf_fail(ctx, ICF_ERR_ARG, "non-finite rest coordinate");
+  }
+  for (long long i = 0; i < 4LL * n_elems; i++)
+    if (elems[i] < 0 || elems[i] >= n_nodes) return icf_fail(ctx, ICF_ERR_ARG, "element node id out of range");
+  for (long long i = 0; i < 6LL * n_czs; i++)
+    if (czs[i] < 0 || czs[i] >= n_nodes) return icf_fail(ctx, ICF_ERR_ARG, "CZ node id out of range");
+  for (long long i = 0; i < 3LL * n_faces; i++)
+    if (faces[i] < 0 || faces[i] >= n_nodes) return icf_fail(ctx, ICF_ERR_ARG, "face node id out of range");
+  if (n_surface) {
+    if (adj_offsets[0] != 0) return icf_fail(ctx, ICF_ERR_ARG, "adj_offsets[0] must be 0");
+    for (int i = 0; i < n_surface; i++)
+      if (adj_offsets[i + 1] < adj_offsets[i]) return icf_fail(ctx, ICF_ERR_ARG, "adj_offsets not ascending");
+    for (long long i = 0; i < 4LL * n_surface; i++)
+      if (surface_elems[i] < 0 || surface_elems[i] >= n_nodes)
+        return icf_fail(ctx, ICF_ERR_ARG, "surface element node id out of range");
+    for (int i = 0; i < adj_offsets[n_surface]; i++)
+      if (adj_faces[i] < 0 || adj_faces[i] >= n_faces) return icf_fail(ctx, ICF_ERR_ARG, "adjacent face id out of range");
+  }
+  cudaStream_t s = ctx->stream;
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  free_all(ctx);
+  ctx->d_elem = nullptr; ctx->d_cz = nullptr; ctx->d_alt = nullptr; ctx->d_selem = nullptr;
+  ctx->d_adj_off = ctx->d_adj = ctx->d_faces = nullptr;
+  ctx->d_x0 = ctx->d_xc = nullptr; ctx->d_va = nullptr;
+  ctx->d_u = ctx->d_v = ctx->d_a = ctx->d_du = ctx->d_un = ctx->d_h3 = nullptr;
+  ctx->d_czs = nullptr; ctx->d_czfail = nullptr; ctx->d_cztent = nullptr; ctx->d_czflags = nullptr;
+  ctx->d_czavg = nullptr; ctx->d_czprm = nullptr; ctx->d_es = nullptr; ctx->d_cs = nullptr;
+  ctx->d_ks = nullptr; ctx->ks_cap = 0; ctx->d_skeys = nullptr; ctx->d_rc_off = nullptr; ctx->d_rc = nullptr;
+  ctx->d_rows = ctx->d_cols = ctx->d_src = nullptr; ctx->rows_cap = ctx->cols_cap = 0; ctx->d_mkeys = nullptr;
+  ctx->d_imp = nullptr; ctx->imp_cap = 0; ctx->n_imp = 0; ctx->d_cr_slot = ctx->d_cr_off = nullptr;
+  ctx->d_cr = nullptr; ctx->cr_cap = 0; ctx->n_crs = 0; ctx->d_pairs = ctx->d_masks = nullptr;
+  ctx->pairs_cap = 0; ctx->n_pairs = 0; ctx->d_vals = ctx->d_rhs = ctx->d_nodeF = nullptr; ctx->vals_cap = 0;
+  ctx->tet_inc = icf_node_inc(); ctx->imp_inc = icf_node_inc(); ctx->d_tmp = nullptr; ctx->tmp_bytes = 0;
+  ctx->per_cz_prm = false;
+  ctx->have_structure = false;
+  ctx->have_nodes = false;
+  ctx->nnz_s = 0;
+  ctx->nnz = 0;
+  ctx->N = 0;
+
+  ctx->n_nodes = n_nodes;
+  ctx->n_elem = n_elems;
+  ctx->n_cz = n_czs;
+  ctx->n_surf = n_surface;
+  ctx->n_faces = n_faces;
+  ctx->h_alt.assign(alt_id, alt_id + n_nodes);
+  const size_t n = (size_t)n_nodes;
+  ICF_TRY(dalloc(ctx, &ctx->d_alt, n));
+  ICF_TRY(dalloc(ctx, &ctx->d_x0, n));
+  ICF_TRY(dalloc(ctx, &ctx->d_xc, n));
+  ICF_TRY(dalloc(ctx, &ctx->d_va, 3 * n));
+  ICF_TRY(dalloc(ctx, &ctx->d_u, 3 * n));
+  ICF_TRY(dalloc(ctx, &ctx->d_v, 3 * n));
+  ICF_TRY(dalloc(ctx, &ctx->d_a, 3 * n));
+  ICF_TRY(dalloc(ctx, &ctx->d_du, 3 * n));
+  ICF_TRY(dalloc(ctx, &ctx->d_un, 3 * n));
+  ICF_TRY(dalloc(ctx, &ctx->d_h3, 9 * n));
+  ICF_TRY(dalloc(ctx, &ctx->d_nodeF, 3 * n));
+  ICF_TRY(dalloc(ctx, &ctx->d_elem, (size_t)n_elems));
+  ICF_TRY(dalloc(ctx, &ctx->d_es, 8 * (size_t)n_elems));
+  ICF_TRY(dalloc(ctx, &ctx->d_cz, 8 * (size_t)n_czs));
+  ICF_TRY(dalloc(ctx, &ctx->d_czs, 8 * (size_t)n_czs));
+  ICF_TRY(dalloc(ctx, &ctx->d_czfail, (size_t)n_czs));
+  ICF_TRY(dalloc(ctx, &ctx->d_cztent, 2 * (size_t)n_czs));
+  ICF_TRY(dalloc(ctx, &ctx->d_czflags, (size_t)n_czs));
+  ICF_TRY(dalloc(ctx, &ctx->d_czavg, 4 * (size_t)n_czs));
+  ICF_TRY(dalloc(ctx, &ctx->d_cs, ICF_CZ_STAGE * (size_t)n_czs));
+
+  std::vector<double4> hx(n);
+  for (size_t i = 0; i < n; i++) hx[i] = make_double4(x0[3 * i], x0[3 * i + 1], x0[3 * i + 2], 0.0);
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_alt, alt_id, sizeof(int) * n, cudaMemcpyHostToDevice));
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_x0, hx.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_xc, hx.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  ICF_CUDA(ctx, cudaMemset(ctx->d_va, 0, sizeof(double2) * 3 * n));
+  ICF_CUDA(ctx, cudaMemset(ctx->d_u, 0, sizeof(double) * 3 * n));
+  ICF_CUDA(ctx, cudaMemset(ctx->d_v, 0, sizeof(double) * 3 * n));
+  ICF_CUDA(ctx, cudaMemset(ctx->d_a, 0, sizeof(double) * 3 * n));
+  ICF_CUDA(ctx, cudaMemset(ctx->d_du, 0, sizeof(double) * 3 * n));
+  ICF_CUDA(ctx, cudaMemset(ctx->d_un, 0, sizeof(double) * 3 * n));
+  ICF_CUDA(ctx, cudaMemset(ctx->d_nodeF, 0, sizeof(double) * 3 * n));
+  if (n_elems)
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_elem, elems, sizeof(int4) * (size_t)n_elems, cudaMemcpyHostToDevice));
+  if (n_czs) {
+    std::vector<int> hc(8 * (size_t)n_czs, 0);
+    for (int c = 0; c < n_czs; c++)
+      for (int i = 0; i < 6; i++) hc[8 * (size_t)c + i] = czs[6 * (size_t)c + i];
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_cz, hc.data(), sizeof(int) * hc.size(), cudaMemcpyHostToDevice));
+    ICF_CUDA(ctx, cudaMemset(ctx->d_czs, 0, sizeof(double) * 8 * (size_t)n_czs));
+    ICF_CUDA(ctx, cudaMemset(ctx->d_czfail, 0, sizeof(int) * (size_t)n_czs));
+    ICF_CUDA(ctx, cudaMemset(ctx->d_cztent, 0, sizeof(double) * 2 * (size_t)n_czs));
+    ICF_CUDA(ctx, cudaMemset(ctx->d_czflags, 0, sizeof(int) * (size_t)n_czs));
+    ICF_CUDA(ctx, cudaMemset(ctx->d_czavg, 0, sizeof(double) * 4 * (size_t)n_czs));
+  }
+  if (n_surface) {
+    ICF_TRY(dalloc(ctx, &ctx->d_selem, (size_t)n_surface));
+    ICF_TRY(dalloc(ctx, &ctx->d_adj_off, (size_t)n_surface + 1));
+    ICF_TRY(dalloc(ctx, &ctx->d_adj, (size_t)adj_offsets[n_surface]));
+    ICF_TRY(dalloc(ctx, &ctx->d_faces, 3 * (size_t)n_faces));
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_selem, surface_elems, sizeof(int4) * (size_t)n_surface, cudaMemcpyHostToDevice));
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_adj_off, adj_offsets, sizeof(int) * ((size_t)n_surface + 1), cudaMemcpyHostToDevice));
+    if (adj_offsets[n_surface] > 0)
+      ICF_CUDA(ctx, cudaMemcpy(ctx->d_adj, adj_faces, sizeof(int) * (size_t)adj_offsets[n_surface], cudaMemcpyHostToDevice));
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_faces, faces, sizeof(int) * 3 * (size_t)n_faces, cudaMemcpyHostToDevice));
+  }
+  ctx->have_static = true;
+  return ICF_OK;
+}
+
+int icf_transfer_nodes(icf_ctx *ctx, int n_nodes, const double *un, const double *vn, const double *an) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  if (n_nodes != ctx->n_nodes || !un || !vn || !an) return icf_fail(ctx, ICF_ERR_ARG, "bad node arrays");
+  const size_t b = sizeof(double) * 3 * (size_t)n_nodes;
+  cudaStream_t s = ctx->stream;
+  double *dun = ctx->d_h3, *dvn = ctx->d_h3 + 3 * (size_t)n_nodes, *dan = ctx->d_h3 + 6 * (size_t)n_nodes;
+  ICF_CUDA(ctx, cudaMemcpyAsync(dun, un, b, cudaMemcpyHostToDevice, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(dvn, vn, b, cudaMemcpyHostToDevice, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(dan, an, b, cudaMemcpyHostToDevice, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(ctx->d_un, un, b, cudaMemcpyHostToDevice, s));
+  ICF_TRY(icf_launch_pack_nodes(ctx, dun, dvn, dan));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  ctx->have_nodes = true;
+  return ICF_OK;
+}
+
+int icf_transfer_cz_state(icf_ctx *ctx, int n_czs, const double *pmax, const double *tmax, const int *failed) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  if (n_czs != ctx->n_cz || !pmax || !tmax || !failed) return icf_fail(ctx, ICF_ERR_ARG, "bad CZ arrays");
+  std::vector<double> h(8 * (size_t)n_czs, 0.0);
+  for (int c = 0; c < n_czs; c++)
+    for (int i = 0; i < 3; i++) {
+      h[8 * (size_t)c + i] = pmax[3 * (size_t)c + i];
+      h[8 * (size_t)c + 3 + i] = tmax[3 * (size_t)c + i];
+    }
+  if (n_czs) {
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_czs, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_czfail, failed, sizeof(int) * (size_t)n_czs, cudaMemcpyHostToDevice));
+  }
+  return ICF_OK;
+}
+
+int icf_narrow_phase(icf_ctx *ctx, int n_pairs, const int *pairs, int *n_impacts) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  if (n_pairs < 0 || (n_pairs && !pairs) || !n_impacts) return icf_fail(ctx, ICF_ERR_ARG, "bad pair list");
+  if (ctx->prm.CollisionScheme == 0 || n_pairs == 0) {
+    ctx->n_imp = 0;
+    ctx->n_pairs = 0;
+    *n_impacts = 0;
+    return ICF_OK;
+  }
+  if (ctx->n_surf == 0) return icf_fail(ctx, ICF_ERR_STATE, "no surface elements were transferred");
+  for (long long i = 0; i < 2LL * n_pairs; i++)
+    if (pairs[i] < 0 || pairs[i] >= ctx->n_surf) return icf_fail(ctx, ICF_ERR_ARG, "pair element id out of range");
+  if (n_pairs > ctx->pairs_cap) {
+    ICF_TRY(dalloc(ctx, &ctx->d_pairs, 2 * (size_t)n_pairs));
+    ICF_TRY(dalloc(ctx, &ctx->d_masks, (size_t)n_pairs));
+    ctx->pairs_cap = n_pairs;
+  }
+  ICF_CUDA(ctx, cudaMemcpyAsync(ctx->d_pairs, pairs, sizeof(int) * 2 * (size_t)n_pairs, cudaMemcpyHostToDevice,
+                                ctx->stream));
+  ctx->n_pairs = n_pairs;
+  ICF_TRY(icf_run_narrow_phase(ctx, n_pairs, n_impacts));
+  ctx->have_structure = false;
+  return ICF_OK;
+}
+
+int icf_get_narrow_masks(icf_ctx *ctx, int capacity, int *masks) {
+  ICF_CHECK_CTX(ctx);
+  if (!masks || capacity < ctx->n_pairs) return icf_fail(ctx, ICF_ERR_SIZE, "mask buffer too small");
+  if (ctx->n_pairs)
+    ICF_CUDA(ctx, cudaMemcpy(masks, ctx->d_masks, sizeof(int) * (size_t)ctx->n_pairs, cudaMemcpyDeviceToHost));
+  return ICF_OK;
+}
+
+int icf_get_impacts(icf_ctx *ctx, int capacity, int *impacts) {
+  ICF_CHECK_CTX(ctx);
+  if (!impacts || capacity < ctx->n_imp) return icf_fail(ctx, ICF_ERR_SIZE, "impact buffer too small");
+  if (ctx->n_imp)
+    ICF_CUDA(ctx, cudaMemcpy(impacts, ctx->d_imp, sizeof(int4) * (size_t)ctx->n_imp, cudaMemcpyDeviceToHost));
+  return ICF_OK;
+}
+
+int icf_set_impacts(icf_ctx *ctx, int n_impacts, const int *impacts) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  if (n_impacts < 0 || (n_impacts && !impacts)) return icf_fail(ctx, ICF_ERR_ARG, "bad impact list");
+  if (n_impacts >= ICF_MAX_TET_UNITS) return icf_fail(ctx, ICF_ERR_SIZE, "too many impacts");
+  for (long long i = 0; i < 4LL * n_impacts; i++)
+    if (impacts[i] < 0 || impacts[i] >= ctx->n_nodes) return icf_fail(ctx, ICF_ERR_ARG, "impact node id out of range");
+  if (n_impacts > ctx->imp_cap) {
+    ICF_TRY(dalloc(ctx, &ctx->d_imp, 2 * (size_t)n_impacts));
+    ctx->imp_cap = 2 * n_impacts;
+  }
+  if (n_impacts)
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_imp, impacts, sizeof(int4) * (size_t)n_impacts, cudaMemcpyHostToDevice));
+  ctx->n_imp = n_impacts;
+  ctx->have_structure = false;
+  return ICF_OK;
+}
+
+int icf_create_structure(icf_ctx *ctx, int *N, int *nnz) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  if (!ctx->d_skeys) ICF_TRY(icf_build_static_pattern(ctx));
+  ICF_TRY(icf_build_merged_pattern(ctx));
+  ctx->have_structure = true;
+  if (N) *N = ctx->N;
+  if (nnz) *nnz = ctx->nnz;
+  return ICF_OK;
+}
+
+int icf_get_structure(icf_ctx *ctx, int *csr_rows, int *csr_cols) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  if (csr_rows)
+    ICF_CUDA(ctx, cudaMemcpy(csr_rows, ctx->d_rows, sizeof(int) * ((size_t)ctx->N + 1), cudaMemcpyDeviceToHost));
+  if (csr_cols && ctx->nnz)
+    ICF_CUDA(ctx, cudaMemcpy(csr_cols, ctx->d_cols, sizeof(int) * (size_t)ctx->nnz, cudaMemcpyDeviceToHost));
+  return ICF_OK;
+}
+
+int icf_get_pcsr(icf_ctx *ctx, int kind, long long capacity, int *out) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  long long need;
+  if (kind == 0) need = 20LL * ctx->n_elem;
+  else if (kind == 1) need = 42LL * ctx->n_cz;
+  else if (kind == 2) need = 20LL * ctx->n_imp;
+  else return icf_fail(ctx, ICF_ERR_ARG, "kind must be 0, 1 or 2");
+  if (!out || capacity < need) return icf_fail(ctx, ICF_ERR_SIZE, "pcsr buffer too small");
+  if (need == 0) return ICF_OK;
+  int *d = nullptr;
+  ICF_CUDA(ctx, cudaMalloc(&d, sizeof(int) * (size_t)need));
+  int rc = icf_launch_pcsr(ctx, kind, d);
+  if (rc == ICF_OK) {
+    cudaError_t e = cudaMemcpyAsync(out, d, sizeof(int) * (size_t)need, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = icf_fail(ctx, ICF_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaFree(d);
+  return rc;
+}
+
+int icf_assemble_async(icf_ctx *ctx, double h) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_prm) return icf_fail(ctx, ICF_ERR_STATE, "icf_set_constants first");
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  if (!(h > 0) || !std::isfinite(h)) return icf_fail(ctx, ICF_ERR_ARG, "time step must be positive");
+  return icf_launch_assembly(ctx, h);
+}
+
+int icf_read_counts(icf_ctx *ctx, icf_counts *c) {
+  ICF_CHECK_CTX(ctx);
+  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (c) {
+    c->nElems = ctx->n_elem;
+    c->nCZ = ctx->n_cz;
+    c->nCZDamaged = ctx->h_counts[0];
+    c->nCZFailedThisStep = ctx->h_counts[1];
+    c->nCZContact = ctx->h_counts[2];
+    c->nImpacts = ctx->n_imp;
+    c->nImpactsActive = ctx->h_counts[3];
+    c->nonFinite = ctx->h_counts[4];
+  }
+  if (ctx->h_counts[4]) return icf_fail(ctx, ICF_ERR_NUMERIC, "non-finite value in the assembled rhs");
+  return ICF_OK;
+}
+
+int icf_assemble(icf_ctx *ctx, double h, icf_counts *counts) {
+  ICF_TRY(icf_assemble_async(ctx, h));
+  return icf_read_counts(ctx, counts);
+}
+
+int icf_transfer_linear_system(icf_ctx *ctx, double *vals, double *rhs) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  cudaStream_t s = ctx->stream;
+  if (vals && ctx->nnz)
+    ICF_CUDA(ctx, cudaMemcpyAsync(vals, ctx->d_vals, sizeof(double) * 9 * (size_t)ctx->nnz, cudaMemcpyDeviceToHost, s));
+  if (rhs && ctx->N)
+    ICF_CUDA(ctx, cudaMemcpyAsync(rhs, ctx->d_rhs, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  return ICF_OK;
+}
+
+int icf_get_cz_tentative(icf_ctx *ctx, double *tent, int *flags, double *avg4) {
+  ICF_CHECK_CTX(ctx);
+  const size_t n = (size_t)ctx->n_cz;
+  if (!n) return ICF_OK;
+  cudaStream_t s = ctx->stream;
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  if (tent) ICF_CUDA(ctx, cudaMemcpy(tent, ctx->d_cztent, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
+  if (avg4) ICF_CUDA(ctx, cudaMemcpy(avg4, ctx->d_czavg, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
+  if (flags) {
+    std::vector<int> f(n);
+    ICF_CUDA(ctx, cudaMemcpy(f.data(), ctx->d_czflags, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    for (size_t c = 0; c < n; c++) {
+      flags[3 * c] = f[c] & 1;
+      flags[3 * c + 1] = (f[c] >> 1) & 1;
+      flags[3 * c + 2] = (f[c] >> 2) & 1;
+    }
+  }
+  return ICF_OK;
+}
+
+int icf_transfer_updated_state(icf_ctx *ctx, double *pmax, double *tmax, int *failed, double *avg4,
+                               double *node_F) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "assemble first");
+  cudaStream_t s = ctx->stream;
+  ICF_TRY(icf_launch_commit_cz(ctx));
+  if (node_F) ICF_TRY(icf_launch_node_force(ctx));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  const size_t n = (size_t)ctx->n_cz;
+  if (n && (pmax || tmax)) {
+    std::vector<double> h(8 * n);
+    ICF_CUDA(ctx, cudaMemcpy(h.data(), ctx->d_czs, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost));
+    for (size_t c = 0; c < n; c++)
+      for (int i = 0; i < 3; i++) {
+        if (pmax) pmax[3 * c + i] = h[8 * c + i];
+        if (tmax) tmax[3 * c + i] = h[8 * c + 3 + i];
+      }
+  }
+  if (n && failed) ICF_CUDA(ctx, cudaMemcpy(failed, ctx->d_czfail, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  if (n && avg4) ICF_CUDA(ctx, cudaMemcpy(avg4, ctx->d_czavg, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
+  if (node_F)
+    ICF_CUDA(ctx, cudaMemcpy(node_F, ctx->d_nodeF, sizeof(double) * 3 * (size_t)ctx->n_nodes, cudaMemcpyDeviceToHost));
+  return ICF_OK;
+}
+
+int icf_get_device_buffers(icf_ctx *ctx, icf_device_buffers *out) {
+  ICF_CHECK_CTX(ctx);
+  if (!out) return icf_fail(ctx, ICF_ERR_ARG, "null output");
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  out->vals = ctx->d_vals;
+  out->rhs = ctx->d_rhs;
+  out->csr_rows = ctx->d_rows;
+  out->csr_cols = ctx->d_cols;
+  out->stream = (void *)ctx->stream;
+  out->N = ctx->N;
+  out->nnz = ctx->nnz;
+  return ICF_OK;
+}
+
+// ---- Newmark kinematics --------------------------------------------------------
+int icf_set_node_state(icf_ctx *ctx, int n_nodes, const double *u, const double *v, const double *a) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  if (n_nodes != ctx->n_nodes || !u || !v || !a) return icf_fail(ctx, ICF_ERR_ARG, "bad node arrays");
+  const size_t b = sizeof(double) * 3 * (size_t)n_nodes;
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_u, u, b, cudaMemcpyHostToDevice));
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_v, v, b, cudaMemcpyHostToDevice));
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_a, a, b, cudaMemcpyHostToDevice));
+  return ICF_OK;
+}
+
+int icf_get_node_state(icf_ctx *ctx, double *u, double *v, double *a, double *du) {
+  ICF_CHECK_CTX(ctx);
+  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const size_t b = sizeof(double) * 3 * (size_t)ctx->n_nodes;
+  if (u) ICF_CUDA(ctx, cudaMemcpy(u, ctx->d_u, b, cudaMemcpyDeviceToHost));
+  if (v) ICF_CUDA(ctx, cudaMemcpy(v, ctx->d_v, b, cudaMemcpyDeviceToHost));
+  if (a) ICF_CUDA(ctx, cudaMemcpy(a, ctx->d_a, b, cudaMemcpyDeviceToHost));
+  if (du) ICF_CUDA(ctx, cudaMemcpy(du, ctx->d_du, b, cudaMemcpyDeviceToHost));
+  return ICF_OK;
+}
+
+int icf_set_du(icf_ctx *ctx, int n_nodes, const double *du) {
+  ICF_CHECK_CTX(ctx);
+  if (n_nodes != ctx->n_nodes || !du) return icf_fail(ctx, ICF_ERR_ARG, "bad du array");
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_du, du, sizeof(double) * 3 * (size_t)n_nodes, cudaMemcpyHostToDevice));
+  return ICF_OK;
+}
+
+int icf_infer_tentative(icf_ctx *ctx, double h) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static || !ctx->have_prm) return icf_fail(ctx, ICF_ERR_STATE, "static data and constants first");
+  if (!(h > 0)) return icf_fail(ctx, ICF_ERR_ARG, "time step must be positive");
+  ICF_TRY(icf_launch_infer(ctx, h));
+  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->have_nodes = true;
+  return ICF_OK;
+}
+
+int icf_add_dx(icf_ctx *ctx, const double *dx, double *norm) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  if (!dx) return icf_fail(ctx, ICF_ERR_ARG, "null dx");
+  cudaStream_t s = ctx->stream;
+  double *d = ctx->d_h3;  // 9 * n_nodes >= 3 * N
+  ICF_CUDA(ctx, cudaMemcpyAsync(d, dx, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyHostToDevice, s));
+  ICF_TRY(icf_launch_add_dx(ctx, d));
+  ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_norm, ctx->d_norm, sizeof(double), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  if (norm) *norm = ctx->h_norm[0];
+  return ICF_OK;
+}
+
+int icf_accept_tentative(icf_ctx *ctx, double h) {
+  ICF_CHECK_CTX(ctx);
+  if (!(h > 0)) return icf_fail(ctx, ICF_ERR_ARG, "time step must be positive");
+  ICF_TRY(icf_launch_accept(ctx, h));
+  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ICF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,760 @@
+// icf_assembly.cu -- per-unit kernels and the atomic-free BCSR gather.
+//
+// One assembly (icf_launch_assembly) is:
+//   k_tet_unit    one thread per tetrahedron: corotational force, rotated
+//                 shape-function gradients and the Newmark rhs of each vertex
+//                 (element_kernels2.h:19-159 and :195-263) -> tet staging
+//   k_cz_unit     one thread per cohesive zone: mid-plane frame, PPR law at
+//                 three Gauss points, tentative damage state and flags
+//                 (cz_kernels.h:210-434) -> CZ staging
+//   k_imp_unit    one thread per impact (icf_contact.cu)
+//   k_gather      one thread per BCSR block: sums the contributions listed
+//                 for that block in the pattern's slot-sorted code list, then
+//                 writes the block once (and the rhs row for diagonal blocks)
+//   k_imp_add     adds impact contributions to the blocks they touch
+// Each block is written by exactly one thread in a fixed order, so the result
+// is bit-reproducible; the reference's CAS-loop atomics (atomic_add.h:1-13)
+// have no counterpart.
+#include "icf_internal.cuh"
+#include "icf_ppr.cuh"
+
+namespace {
+
+// ---- small vector helpers ---------------------------------------------------
+__device__ __forceinline__ void ld_node(const double4 *__restrict__ p, int i,
+                                        double o[3]) {
+  const double4 v = p[i];
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+}
+
+// Orthonormal frame of three points as in fastRotationMatrix
+// (elem_kernels9/matrix_math1.h:32-71): columns unit(p1-p0),
+// unit((p1-p0) x (p2-p0)), unit(col1 x col0).
+__device__ __forceinline__ void frame3(const double p0[3], const double p1[3],
+                                       const double p2[3], double R[3][3]) {
+  double d[3], w[3];
+  for (int k = 0; k < 3; k++) {
+    d[k] = p1[k] - p0[k];
+    w[k] = p2[k] - p0[k];
+  }
+  double r = rsqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  for (int k = 0; k < 3; k++) R[k][0] = d[k] * r;
+  double c0 = -d[2] * w[1] + d[1] * w[2];
+  double c1 = d[2] * w[0] - d[0] * w[2];
+  double c2 = -d[1] * w[0] + d[0] * w[1];
+  r = rsqrt(c0 * c0 + c1 * c1 + c2 * c2);
+  R[0][1] = c0 * r;
+  R[1][1] = c1 * r;
+  R[2][1] = c2 * r;
+  c0 = R[1][1] * R[2][0] - R[1][0] * R[2][1];
+  c1 = -R[0][1] * R[2][0] + R[0][0] * R[2][1];
+  c2 = R[0][1] * R[1][0] - R[0][0] * R[1][1];
+  r = rsqrt(c0 * c0 + c1 * c1 + c2 * c2);
+  R[0][2] = c0 * r;
+  R[1][2] = c1 * r;
+  R[2][2] = c2 * r;
+}
+
+// ---- tetrahedra ---------------------------------------------------------------
+// Closed form of the reference's K = V B^T E B for isotropic E:
+//   K_ab = V (lam g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I)
+// so that, with h_b = R g_b (R = R1 R0^T, the corotational rotation),
+//   Df_ab = R K_ab R^T = V (lam h_a h_b^T + mu h_b h_a^T + mu (h_a.h_b) I)
+//   f_a   = R sum_b K_ab xr_b = V R sigma(F) g_a,  F = sum_b xr_b g_b^T,
+//           sigma(F) = lam tr(F) I + mu (F + F^T),  xr_b = R^T xc_b - x0_b
+//   sum_b Df_ab v_b = V (lam tr(L) I + mu (L + L^T)) h_a,  L = sum_b v_b h_b^T
+// and the consistent mass is M_ab = rho/20 (1 + delta_ab) I.  The staging
+// record of vertex a is {h_a, V} and {rhs_a, 0}; k_gather rebuilds
+// LHS_ab = stiffCoeff Df_ab + massCoeff M_ab from it.
+__global__ void __launch_bounds__(128)
+    k_tet_unit(int ne, const int4 *__restrict__ elem,
+               const double4 *__restrict__ x0, const double4 *__restrict__ xc,
+               const double2 *__restrict__ va, icf_dprm P,
+               double4 *__restrict__ es) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int4 id = __ldg(elem + e);
+  const int nid[4] = {id.x, id.y, id.z, id.w};
+  double X[4][3], C[4][3], Vn[4][3], An[4][3];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    ld_node(x0, nid[i], X[i]);
+    ld_node(xc, nid[i], C[i]);
+    const double2 q0 = __ldg(va + 3 * nid[i]), q1 = __ldg(va + 3 * nid[i] + 1),
+                  q2 = __ldg(va + 3 * nid[i] + 2);
+    Vn[i][0] = q0.x; Vn[i][1] = q0.y; Vn[i][2] = q1.x;
+    An[i][0] = q1.y; An[i][1] = q2.x; An[i][2] = q2.y;
+  }
+  // rest volume and shape-function gradients (element_kernels2.h:38-57)
+  const double x12 = X[0][0] - X[1][0], x13 = X[0][0] - X[2][0], x14 = X[0][0] - X[3][0];
+  const double x23 = X[1][0] - X[2][0], x24 = X[1][0] - X[3][0], x34 = X[2][0] - X[3][0];
+  const double y12 = X[0][1] - X[1][1], y13 = X[0][1] - X[2][1], y14 = X[0][1] - X[3][1];
+  const double y23 = X[1][1] - X[2][1], y24 = X[1][1] - X[3][1], y34 = X[2][1] - X[3][1];
+  const double z12 = X[0][2] - X[1][2], z13 = X[0][2] - X[2][2], z14 = X[0][2] - X[3][2];
+  const double z23 = X[1][2] - X[2][2], z24 = X[1][2] - X[3][2], z34 = X[2][2] - X[3][2];
+  const double Jdet = -x12 * (y23 * z34 - y34 * z23) - x23 * (y34 * z12 - y12 * z34) -
+                      x34 * (y12 * z23 - y23 * z12);
+  const double V = Jdet / 6.;
+  const double iJ = 1.0 / Jdet;
+  double g[4][3];
+  g[0][0] = (y24 * z23 - y23 * z24) * iJ;  // a1 = y42 z32 - y32 z42
+  g[0][1] = (x23 * z24 - x24 * z23) * iJ;  // b1 = x32 z42 - x42 z32
+  g[0][2] = (x24 * y23 - x23 * y24) * iJ;  // c1 = x42 y32 - x32 y42
+  g[1][0] = (y13 * z34 - y34 * z13) * iJ;  // a2 = y31 z43 - y34 z13
+  g[1][1] = (x34 * z13 - x13 * z34) * iJ;  // b2 = x43 z31 - x13 z34
+  g[1][2] = (x13 * y34 - x34 * y13) * iJ;  // c2 = x31 y43 - x34 y13
+  g[2][0] = (y24 * z14 - y14 * z24) * iJ;  // a3
+  g[2][1] = (x14 * z24 - x24 * z14) * iJ;  // b3
+  g[2][2] = (x24 * y14 - x14 * y24) * iJ;  // c3
+  g[3][0] = (y12 * z13 - y13 * z12) * iJ;  // a4 = y13 z21 - y12 z31
+  g[3][1] = (x13 * z12 - x12 * z13) * iJ;  // b4 = x21 z13 - x31 z12
+  g[3][2] = (x12 * y13 - x13 * y12) * iJ;  // c4 = x13 y21 - x12 y31
+
+  // corotational rotation R = R1 R0^T (:175-201)
+  double R0[3][3], R1[3][3], R[3][3];
+  frame3(X[0], X[1], X[2], R0);
+  frame3(C[0], C[1], C[2], R1);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      R[i][j] = R1[i][0] * R0[j][0] + R1[i][1] * R0[j][1] + R1[i][2] * R0[j][2];
+
+  // F = sum_b (R^T xc_b - x0_b) g_b^T and the stress sigma(F)
+  double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    double xr[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      xr[k] = (C[b][0] * R[0][k] + C[b][1] * R[1][k] + C[b][2] * R[2][k]) - X[b][k];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) F[k][l] += xr[k] * g[b][l];
+  }
+  const double trF = F[0][0] + F[1][1] + F[2][2];
+  double S[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int l = 0; l < 3; l++)
+      S[k][l] = P.mu * (F[k][l] + F[l][k]) + (k == l ? P.lam * trF : 0.0);
+
+  // rotated gradients h_b = R g_b and L = sum_b v_b h_b^T
+  double h[4][3];
+  double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  double sv[3] = {0, 0, 0}, sa[3] = {0, 0, 0};
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      h[b][k] = R[k][0] * g[b][0] + R[k][1] * g[b][1] + R[k][2] * g[b][2];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      sv[k] += Vn[b][k];
+      sa[k] += An[b][k];
+#pragma unroll
+      for (int l = 0; l < 3; l++) L[k][l] += Vn[b][k] * h[b][l];
+    }
+  }
+  const double trL = L[0][0] + L[1][1] + L[2][2];
+  const double mV = P.rho20 * V;
+  const double gz = P.grav_rho * V / 4;
+
+  double4 *out = es + 8 * (size_t)e;
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    double sg[3], f[3], dv[3], r[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) sg[k] = S[k][0] * g[a][0] + S[k][1] * g[a][1] + S[k][2] * g[a][2];
+#pragma unroll
+    for (int k = 0; k < 3; k++) f[k] = V * (R[k][0] * sg[0] + R[k][1] * sg[1] + R[k][2] * sg[2]);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double Lh = (L[k][0] + L[0][k]) * h[a][0] + (L[k][1] + L[1][k]) * h[a][1] +
+                        (L[k][2] + L[2][k]) * h[a][2];
+      dv[k] = V * (P.lam * trL * h[a][k] + P.mu * Lh);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double damp = mV * P.dm * (Vn[a][k] + sv[k]) + P.ds * dv[k];
+      const double inert = mV * (An[a][k] + sa[k]);
+      r[k] = (k == 2 ? gz : 0.0) - f[k] - damp - inert;
+    }
+    out[a] = make_double4(h[a][0], h[a][1], h[a][2], V);
+    out[4 + a] = make_double4(r[0], r[1], r[2], 0.0);
+  }
+}
+
+// ---- cohesive zones -------------------------------------------------------------
+// Geometry up to the Gauss-point openings is evaluated with separately
+// rounded products and sums (the __d*_rn intrinsics are never fused), so the
+// openings that drive the law's branch decisions are the same numbers the
+// checker computes.  Everything after the law may use fused multiply-adds.
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+// CZRotationMatrix (cz_kernels9/matrix_math.h:15-68).
+__device__ __forceinline__ void cz_frame(const double m0[3], const double m1[3],
+                                         const double m2[3], double R[3][3],
+                                         double &aJ) {
+  double p1[3], p2[3], n[3], r[3];
+  for (int k = 0; k < 3; k++) {
+    p1[k] = sub(m1[k], m0[k]);
+    p2[k] = sub(m0[k], m2[k]);
+  }
+  const double l1 = sqrt(add(add(mul(p1[0], p1[0]), mul(p1[1], p1[1])), mul(p1[2], p1[2])));
+  for (int k = 0; k < 3; k++) R[0][k] = p1[k] / l1;
+  n[0] = add(mul(-p1[2], p2[1]), mul(p1[1], p2[2]));
+  n[1] = sub(mul(p1[2], p2[0]), mul(p1[0], p2[2]));
+  n[2] = add(mul(-p1[1], p2[0]), mul(p1[0], p2[1]));
+  double ln = sqrt(add(add(mul(n[0], n[0]), mul(n[1], n[1])), mul(n[2], n[2])));
+  aJ = ln / 2;
+  for (int k = 0; k < 3; k++) {
+    n[k] = n[k] / ln;
+    R[2][k] = n[k];
+    p1[k] = p1[k] / l1;
+  }
+  r[0] = add(mul(-n[2], p1[1]), mul(n[1], p1[2]));
+  r[1] = sub(mul(n[2], p1[0]), mul(n[0], p1[2]));
+  r[2] = add(mul(-n[1], p1[0]), mul(n[0], p1[1]));
+  ln = sqrt(add(add(mul(r[0], r[0]), mul(r[1], r[1])), mul(r[2], r[2])));
+  for (int k = 0; k < 3; k++) R[1][k] = r[k] / ln;
+}
+
+// Staging of one CZ (ICF_CZ_STAGE doubles).  With s_a = +sf[a][gp] for the
+// first face's vertices (a < 3) and -sf[a-3][gp] for the second's, the
+// reference's B^T T_d B (cz_kernels.h:366-401) gives the block
+//   Keff_ab = sum_gp s_a s_b Q_gp,   Q_gp = (aJ/3) R^T T_d R
+// and the rhs rhs_a = -sum_gp s_a (aJ/3) R^T T (:343-364).  Both depend on a
+// and b only through a mod 3, b mod 3 and the face signs, so the record holds
+//   Kt[i][j] = sum_gp sf[i][gp] sf[j][gp] Q_gp   (i <= j, symmetric 3x3: 6)
+//   rt[i]    = sum_gp sf[i][gp] (aJ/3) R^T T_gp  (3)
+// i.e. 36 + 9 doubles.
+__global__ void __launch_bounds__(128)
+    k_cz_unit(int nc, const int *__restrict__ cz, const double4 *__restrict__ xc,
+              const double *__restrict__ czs, const int *__restrict__ czfail,
+              const double4 *__restrict__ czprm, icf_dprm P,
+              double *__restrict__ cs, double *__restrict__ cztent,
+              int *__restrict__ czflags, double *__restrict__ czavg,
+              int *__restrict__ counts) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double *st = cs + (size_t)c * ICF_CZ_STAGE;
+  int flag = 0;
+  if (__ldg(czfail + c)) {
+    for (int i = 0; i < ICF_CZ_STAGE; i++) st[i] = 0;
+    czflags[c] = 0;
+    return;
+  }
+  icf_ppr_c q;
+  q.alpha = P.alpha; q.beta = P.beta; q.p_m = P.p_m; q.p_n = P.p_n;
+  q.gam_n = P.gam_n; q.gam_t = P.gam_t; q.pMtn = P.pMtn; q.pMnt = P.pMnt;
+  q.rn = P.rn; q.rt = P.rt;
+  if (czprm) {
+    const double4 w = czprm[c];
+    q.f_tn = w.x; q.f_tt = w.y; q.deln = w.z; q.delt = w.w;
+  } else {
+    q.f_tn = P.f_tn; q.f_tt = P.f_tt; q.deln = P.deln; q.delt = P.delt;
+  }
+
+  const int4 i0 = __ldg(reinterpret_cast<const int4 *>(cz) + 2 * c);
+  const int2 i1 = __ldg(reinterpret_cast<const int2 *>(cz) + 4 * c + 2);
+  const int nid[6] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y};
+  double x[6][3];
+#pragma unroll
+  for (int i = 0; i < 6; i++) ld_node(xc, nid[i], x[i]);
+  double pmax[3], tmax[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    pmax[i] = __ldg(czs + 8 * (size_t)c + i);
+    tmax[i] = __ldg(czs + 8 * (size_t)c + 3 + i);
+  }
+
+  // mid-plane, its frame and local coordinates (:243-266)
+  double mp[3][3], R[3][3], aJ;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) mp[i][k] = mul(add(x[i][k], x[i + 3][k]), 0.5);
+  cz_frame(mp[0], mp[1], mp[2], R, aJ);
+  double xr[6][3];
+#pragma unroll
+  for (int n = 0; n < 6; n++)
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      xr[n][k] = add(add(mul(x[n][0], R[k][0]), mul(x[n][1], R[k][1])), mul(x[n][2], R[k][2]));
+
+  double Kt[6][6], rt[3][3];
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) Kt[i][j] = 0;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) rt[i][j] = 0;
+  bool anyc = false, anyf = false;
+  double aDn = 0, aDt = 0, aTn = 0, aTt = 0;
+  const double cw = (1.0 / 3.0) * aJ;
+
+#pragma unroll 1
+  for (int gp = 0; gp < 3; gp++) {
+    double o[3] = {0, 0, 0};
+#pragma unroll
+    for (int n = 0; n < 3; n++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) o[k] = add(o[k], mul(sub(xr[n][k], xr[n + 3][k]), P.sf[n * 3 + gp]));
+    const double opn = o[2];
+    const double opt = sqrt(add(mul(o[0], o[0]), mul(o[1], o[1])));
+    const icf_law Lw = icf_cz_law(q, pmax[gp], tmax[gp], opn, opt);
+    anyc |= Lw.contact;
+    anyf |= Lw.failed;
+    aDn += opn / 3;
+    aDt += opt / 3;
+    aTn += Lw.Tn / 3;
+    aTt += Lw.Tt / 3;
+
+    // local traction and tangent (:301-340); the tangent is symmetric
+    double T[3], Td[3][3];
+    if (opt < 1e-20) {
+      T[0] = 0; T[1] = 0; T[2] = Lw.Tn;
+      Td[0][0] = Lw.Dtt; Td[1][1] = Lw.Dtt; Td[2][2] = Lw.Dnn;
+      Td[0][1] = Td[1][0] = 0;
+      Td[0][2] = Td[2][0] = Lw.Dnt;
+      Td[1][2] = Td[2][1] = Lw.Dnt;
+    } else {
+      const double io = 1.0 / opt;
+      T[0] = Lw.Tt * o[0] * io;
+      T[1] = Lw.Tt * o[1] * io;
+      T[2] = Lw.Tn;
+      const double io2 = io * io, io3 = io2 * io;
+      const double u00 = o[0] * o[0], u10 = o[1] * o[0], u11 = o[1] * o[1];
+      Td[0][0] = Lw.Dtt * u00 * io2 + Lw.Tt * u11 * io3;
+      Td[1][1] = Lw.Dtt * u11 * io2 + Lw.Tt * u00 * io3;
+      Td[2][2] = Lw.Dnn;
+      Td[0][1] = Td[1][0] = Lw.Dtt * u10 * io2 - Lw.Tt * u10 * io3;
+      Td[0][2] = Td[2][0] = Lw.Dnt * o[0] * io;
+      Td[1][2] = Td[2][1] = Lw.Dnt * o[1] * io;
+    }
+    // world-frame traction and tangent, weighted by aJ/3
+    double tw[3], TR[3][3], Q[6];
+#pragma unroll
+    for (int k = 0; k < 3; k++) tw[k] = cw * (R[0][k] * T[0] + R[1][k] * T[1] + R[2][k] * T[2]);
+#pragma unroll
+    for (int m = 0; m < 3; m++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) TR[m][l] = Td[m][0] * R[0][l] + Td[m][1] * R[1][l] + Td[m][2] * R[2][l];
+    {
+      int p = 0;
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int l = k; l < 3; l++)
+          Q[p++] = cw * (R[0][k] * TR[0][l] + R[1][k] * TR[1][l] + R[2][k] * TR[2][l]);
+    }
+    int pr = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const double si = P.sf[i * 3 + gp];
+#pragma unroll
+      for (int k = 0; k < 3; k++) rt[i][k] += si * tw[k];
+#pragma unroll
+      for (int j = i; j < 3; j++, pr++) {
+        const double w = si * P.sf[j * 3 + gp];
+#pragma unroll
+        for (int t = 0; t < 6; t++) Kt[pr][t] += w * Q[t];
+      }
+    }
+  }
+
+  double pm = fmax(fmax(pmax[0], pmax[1]), pmax[2]);
+  double tm = fmax(fmax(tmax[0], tmax[1]), tmax[2]);
+  bool damaged = false;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+    if (pmax[i] >= q.deln * q.rn || tmax[i] >= q.delt * q.rt) damaged = true;
+  cztent[2 * (size_t)c] = pm;
+  cztent[2 * (size_t)c + 1] = tm;
+  flag = (anyc ? 1 : 0) | ((!anyf && damaged) ? 2 : 0) | (anyf ? 4 : 0);
+  czflags[c] = flag;
+  double4 *av = reinterpret_cast<double4 *>(czavg) + c;
+  if (anyf) {
+    *av = make_double4(0, 0, 0, 0);
+    for (int i = 0; i < ICF_CZ_STAGE; i++) st[i] = 0;
+  } else {
+    *av = make_double4(aDn, aDt, aTn, aTt);
+    double2 *s2 = reinterpret_cast<double2 *>(st);
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+      s2[3 * p + 0] = make_double2(Kt[p][0], Kt[p][1]);
+      s2[3 * p + 1] = make_double2(Kt[p][2], Kt[p][3]);
+      s2[3 * p + 2] = make_double2(Kt[p][4], Kt[p][5]);
+    }
+    s2[18] = make_double2(rt[0][0], rt[0][1]);
+    s2[19] = make_double2(rt[0][2], rt[1][0]);
+    s2[20] = make_double2(rt[1][1], rt[1][2]);
+    s2[21] = make_double2(rt[2][0], rt[2][1]);
+    s2[22] = make_double2(rt[2][2], 0.0);
+    s2[23] = make_double2(0.0, 0.0);
+  }
+  // counters (integer atomics: order-independent)
+  const unsigned full = __activemask();
+  const int dmg = __popc(__ballot_sync(full, (flag & 2) != 0));
+  const int fl = __popc(__ballot_sync(full, (flag & 4) != 0));
+  const int ct = __popc(__ballot_sync(full, (flag & 1) != 0));
+  if ((threadIdx.x & 31) == __ffs(full) - 1) {
+    if (dmg) atomicAdd(counts + 0, dmg);
+    if (fl) atomicAdd(counts + 1, fl);
+    if (ct) atomicAdd(counts + 2, ct);
+  }
+}
+
+// ---- the gather ----------------------------------------------------------------
+__device__ __forceinline__ int sym_pair(int i, int j) {
+  // (0,0)0 (0,1)1 (0,2)2 (1,1)3 (1,2)4 (2,2)5
+  const int lo = i < j ? i : j, hi = i < j ? j : i;
+  return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
+}
+
+__global__ void __launch_bounds__(256)
+    k_gather(int nnz, const int *__restrict__ src, int identity,
+             const int *__restrict__ cols, const int *__restrict__ rc_off,
+             const uint32_t *__restrict__ rc, const double4 *__restrict__ es,
+             const double *__restrict__ cs, double sc, double mc, double lam,
+             double mu, double *__restrict__ vals, double *__restrict__ rhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nnz) return;
+  const int st = identity ? s : __ldg(src + s);
+  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double r[3] = {0, 0, 0};
+  bool diag = false;
+  if (st >= 0) {
+    const int beg = __ldg(rc_off + st), end = __ldg(rc_off + st + 1);
+    for (int qi = beg; qi < end; qi++) {
+      const uint32_t code = __ldg(rc + qi);
+      if ((code >> 30) == ICF_KIND_TET) {
+        const uint32_t e = (code >> 4) & 0x3FFFFFFu, a = (code >> 2) & 3u, bb = code & 3u;
+        const double4 A = es[8 * (size_t)e + a];
+        const double4 Bv = es[8 * (size_t)e + bb];
+        const double V = A.w;
+        const double ha[3] = {A.x, A.y, A.z}, hb[3] = {Bv.x, Bv.y, Bv.z};
+        const double dot = ha[0] * hb[0] + ha[1] * hb[1] + ha[2] * hb[2];
+        const double c1 = sc * V * lam, c2 = sc * V * mu;
+        const double cd = c2 * dot + mc * V * (a == bb ? 2.0 : 1.0);
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+#pragma unroll
+          for (int l = 0; l < 3; l++)
+            b[3 * k + l] += c1 * ha[k] * hb[l] + c2 * hb[k] * ha[l] + (k == l ? cd : 0.0);
+        if (a == bb) {
+          const double4 Rr = es[8 * (size_t)e + 4 + a];
+          r[0] += Rr.x;
+          r[1] += Rr.y;
+          r[2] += Rr.z;
+          diag = true;
+        }
+      } else {
+        const uint32_t c = (code >> 6) & 0xFFFFFFu, a = (code >> 3) & 7u, bb = code & 7u;
+        const double *S = cs + (size_t)c * ICF_CZ_STAGE;
+        const int ia = a % 3, ib = bb % 3;
+        const double sg = ((a < 3) == (bb < 3)) ? 1.0 : -1.0;
+        const double2 *K2 = reinterpret_cast<const double2 *>(S + 6 * sym_pair(ia, ib));
+        const double2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
+        // symmetric 3x3: xx xy xz yy yz zz
+        b[0] += sg * k01.x; b[1] += sg * k01.y; b[2] += sg * k23.x;
+        b[3] += sg * k01.y; b[4] += sg * k23.y; b[5] += sg * k45.x;
+        b[6] += sg * k23.x; b[7] += sg * k45.x; b[8] += sg * k45.y;
+        if (a == bb) {
+          const double sa = (a < 3) ? -1.0 : 1.0;
+          r[0] += sa * __ldg(S + 36 + 3 * ia + 0);
+          r[1] += sa * __ldg(S + 36 + 3 * ia + 1);
+          r[2] += sa * __ldg(S + 36 + 3 * ia + 2);
+          diag = true;
+        }
+      }
+    }
+  }
+  double *o = vals + 9 * (size_t)s;
+#pragma unroll
+  for (int k = 0; k < 9; k++) o[k] = b[k];
+  if (diag) {
+    const int row = __ldg(cols + s);
+    rhs[3 * (size_t)row + 0] = r[0];
+    rhs[3 * (size_t)row + 1] = r[1];
+    rhs[3 * (size_t)row + 2] = r[2];
+  }
+}
+
+// Impact contributions, one thread per block they touch (sorted by slot).
+__global__ void k_imp_add(int n_slots, const int *__restrict__ slot,
+                          const int *__restrict__ off,
+                          const uint32_t *__restrict__ code,
+                          const int *__restrict__ cols,
+                          const double *__restrict__ ks,
+                          double *__restrict__ vals, double *__restrict__ rhs) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots) return;
+  const int s = slot[g];
+  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, r[3] = {0, 0, 0};
+  bool diag = false;
+  for (int q = off[g]; q < off[g + 1]; q++) {
+    const uint32_t cd = code[q];
+    const uint32_t u = (cd >> 4) & 0x3FFFFFFu, a = (cd >> 2) & 3u, bb = cd & 3u;
+    const double *K = ks + (size_t)u * ICF_IMP_STAGE;
+    for (int k = 0; k < 3; k++)
+      for (int l = 0; l < 3; l++) b[3 * k + l] += K[(3 * a + k) * 12 + 3 * bb + l];
+    if (a == bb) {
+      for (int k = 0; k < 3; k++) r[k] += K[144 + 3 * a + k];
+      diag = true;
+    }
+  }
+  double *o = vals + 9 * (size_t)s;
+  for (int k = 0; k < 9; k++) o[k] += b[k];
+  if (diag) {
+    const int row = cols[s];
+    for (int k = 0; k < 3; k++) rhs[3 * (size_t)row + k] += r[k];
+  }
+}
+
+// NaN/Inf scan of the rhs (cheap; the matrix inherits non-finite values from
+// the same units).
+__global__ void k_finite(int n, const double *__restrict__ x, int *flag) {
+  int bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (!isfinite(x[i])) bad = 1;
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// Node forces (the F field of the node array, GPU_Functionality.cs:519-527):
+// per node the sum of the rhs of every tet vertex on it plus impact forces.
+__global__ void k_node_force(int n, const int *__restrict__ off,
+                             const int *__restrict__ inc,
+                             const double4 *__restrict__ es,
+                             const int *__restrict__ ioff,
+                             const int *__restrict__ iinc,
+                             const double *__restrict__ ks,
+                             double *__restrict__ F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double f[3] = {0, 0, 0};
+  for (int q = off[i]; q < off[i + 1]; q++) {
+    const int code = inc[q];
+    const double4 r = es[8 * (size_t)(code >> 2) + 4 + (code & 3)];
+    f[0] += r.x;
+    f[1] += r.y;
+    f[2] += r.z;
+  }
+  if (ioff)
+    for (int q = ioff[i]; q < ioff[i + 1]; q++) {
+      const int code = iinc[q];
+      const double *K = ks + (size_t)(code >> 2) * ICF_IMP_STAGE + 144 + 3 * (code & 3);
+      f[0] += K[0];
+      f[1] += K[1];
+      f[2] += K[2];
+    }
+  F[3 * (size_t)i + 0] = f[0];
+  F[3 * (size_t)i + 1] = f[1];
+  F[3 * (size_t)i + 2] = f[2];
+}
+
+// ---- node packing and Newmark kinematics ------------------------------------------
+__global__ void k_pack_nodes(int n, const double4 *__restrict__ x0,
+                             const double *__restrict__ un,
+                             const double *__restrict__ vn,
+                             const double *__restrict__ an,
+                             double4 *__restrict__ xc, double2 *__restrict__ va) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 p = x0[i];
+  xc[i] = make_double4(p.x + un[3 * i], p.y + un[3 * i + 1], p.z + un[3 * i + 2], 0.0);
+  va[3 * i + 0] = make_double2(vn[3 * i], vn[3 * i + 1]);
+  va[3 * i + 1] = make_double2(vn[3 * i + 2], an[3 * i]);
+  va[3 * i + 2] = make_double2(an[3 * i + 1], an[3 * i + 2]);
+}
+
+// InferTentativeValues (Node.cs:79-97) fused with the node packing.
+__global__ void k_infer(int n, double h, double beta, double gamma,
+                        const double4 *__restrict__ x0,
+                        const double *__restrict__ u, const double *__restrict__ v,
+                        const double *__restrict__ a, const double *__restrict__ du,
+                        double *__restrict__ un, double4 *__restrict__ xc,
+                        double2 *__restrict__ va) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double unx[3], vnx[3], anx[3];
+  for (int k = 0; k < 3; k++) {
+    const size_t j = 3 * (size_t)i + k;
+    unx[k] = u[j] + du[j];
+    anx[k] = a[j] * (1.0 - 1.0 / (2 * beta)) + du[j] / (h * h * beta) + v[j] * (-1.0 / (h * beta));
+    vnx[k] = v[j] + h * ((1.0 - gamma) * a[j] + gamma * anx[k]);
+    un[j] = unx[k];
+  }
+  const double4 p = x0[i];
+  xc[i] = make_double4(p.x + unx[0], p.y + unx[1], p.z + unx[2], 0.0);
+  va[3 * i + 0] = make_double2(vnx[0], vnx[1]);
+  va[3 * i + 1] = make_double2(vnx[2], anx[0]);
+  va[3 * i + 2] = make_double2(anx[1], anx[2]);
+}
+
+__global__ void k_add_dx(int n, const int *__restrict__ alt,
+                         const double *__restrict__ dx, double *__restrict__ du) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int r = alt[i];
+  if (r < 0) return;
+  for (int k = 0; k < 3; k++) du[3 * (size_t)i + k] += dx[3 * (size_t)r + k];
+}
+
+// sum of squares with a fixed reduction tree (deterministic)
+__global__ void k_sumsq(int n, const double *__restrict__ x, double *__restrict__ part) {
+  __shared__ double sh[256];
+  double s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += x[i] * x[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+__global__ void k_sum_parts(int n, const double *__restrict__ part, double *out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0;
+    for (int i = 0; i < n; i++) s += part[i];
+    *out = s;
+  }
+}
+
+// AcceptTentativeValues (Node.cs:62-77).
+__global__ void k_accept(int n, double h, const double4 *__restrict__ x0,
+                         double *__restrict__ u, double *__restrict__ v,
+                         double *__restrict__ a, const double *__restrict__ un,
+                         double *__restrict__ du, double4 *__restrict__ xc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double c[3];
+  for (int k = 0; k < 3; k++) {
+    const size_t j = 3 * (size_t)i + k;
+    const double vnew = (un[j] - u[j]) / h;
+    a[j] = (vnew - v[j]) / h;
+    v[j] = vnew;
+    u[j] = un[j];
+    du[j] = 0;
+    c[k] = u[j];
+  }
+  const double4 p = x0[i];
+  xc[i] = make_double4(p.x + c[0], p.y + c[1], p.z + c[2], 0.0);
+}
+
+// Commit of the tentative CZ state (TransferUpdatedStateToHost, :496-516).
+__global__ void k_commit_cz(int nc, const double *__restrict__ tent,
+                            const int *__restrict__ flags, double *__restrict__ czs,
+                            int *__restrict__ fail) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc || fail[c]) return;
+  if (flags[c] & 4) fail[c] = 1;
+  for (int i = 0; i < 3; i++) {
+    czs[8 * (size_t)c + i] = tent[2 * (size_t)c];
+    czs[8 * (size_t)c + 3 + i] = tent[2 * (size_t)c + 1];
+  }
+}
+
+}  // namespace
+
+// ---- host launchers --------------------------------------------------------------
+int icf_launch_assembly(icf_ctx *ctx, double h) {
+  const icf_dprm P = icf_make_dprm(ctx);
+  cudaStream_t s = ctx->stream;
+  ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, 8 * sizeof(int), s));
+  ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
+  if (ctx->n_elem > 0)
+    k_tet_unit<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0,
+                                                          ctx->d_xc, ctx->d_va, P, ctx->d_es);
+  if (ctx->n_cz > 0)
+    k_cz_unit<<<icf_blocks(ctx->n_cz, 128), 128, 0, s>>>(
+        ctx->n_cz, ctx->d_cz, ctx->d_xc, ctx->d_czs, ctx->d_czfail,
+        ctx->per_cz_prm ? ctx->d_czprm : nullptr, P, ctx->d_cs, ctx->d_cztent, ctx->d_czflags,
+        ctx->d_czavg, ctx->d_counts);
+  if (ctx->n_imp > 0) {
+    const int rc = icf_launch_imp_unit(ctx);
+    if (rc) return rc;
+  }
+  const double nb = ctx->prm.NewmarkBeta, ng = ctx->prm.NewmarkGamma;
+  const double sc = 1.0 + ctx->prm.dampingStiffness * ng / (h * nb);
+  const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
+  if (ctx->nnz > 0)
+    k_gather<<<icf_blocks(ctx->nnz, 256), 256, 0, s>>>(
+        ctx->nnz, ctx->d_src, ctx->src_identity ? 1 : 0, ctx->d_cols, ctx->d_rc_off, ctx->d_rc,
+        ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals, ctx->d_rhs);
+  if (ctx->n_crs > 0)
+    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off,
+                                                        ctx->d_cr, ctx->d_cols, ctx->d_ks,
+                                                        ctx->d_vals, ctx->d_rhs);
+  if (ctx->N > 0)
+    k_finite<<<icf_blocks(3LL * ctx->N, 256) < 1184 ? icf_blocks(3LL * ctx->N, 256) : 1184, 256, 0,
+               s>>>(3 * ctx->N, ctx->d_rhs, ctx->d_counts + 4);
+  ICF_CUDA(ctx, cudaGetLastError());
+  ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int),
+                                cudaMemcpyDeviceToHost, s));
+  return ICF_OK;
+}
+
+int icf_launch_node_force(icf_ctx *ctx) {
+  icf_node_inc t, m;
+  int rc = icf_get_node_inc(ctx, &t, &m);
+  if (rc) return rc;
+  k_node_force<<<icf_blocks(ctx->n_nodes, 128), 128, 0, ctx->stream>>>(
+      ctx->n_nodes, t.off, t.inc, ctx->d_es, ctx->n_imp > 0 ? m.off : nullptr, m.inc, ctx->d_ks,
+      ctx->d_nodeF);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
+int icf_launch_pack_nodes(icf_ctx *ctx, const double *d_un, const double *d_vn,
+                          const double *d_an) {
+  k_pack_nodes<<<icf_blocks(ctx->n_nodes, 256), 256, 0, ctx->stream>>>(
+      ctx->n_nodes, ctx->d_x0, d_un, d_vn, d_an, ctx->d_xc, ctx->d_va);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
+int icf_launch_infer(icf_ctx *ctx, double h) {
+  k_infer<<<icf_blocks(ctx->n_nodes, 256), 256, 0, ctx->stream>>>(
+      ctx->n_nodes, h, ctx->prm.NewmarkBeta, ctx->prm.NewmarkGamma, ctx->d_x0, ctx->d_u, ctx->d_v,
+      ctx->d_a, ctx->d_du, ctx->d_un, ctx->d_xc, ctx->d_va);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
+int icf_launch_add_dx(icf_ctx *ctx, const double *d_dx) {
+  k_add_dx<<<icf_blocks(ctx->n_nodes, 256), 256, 0, ctx->stream>>>(ctx->n_nodes, ctx->d_alt, d_dx,
+                                                                  ctx->d_du);
+  const int n = 3 * ctx->N;
+  const int nb = 256;
+  k_sumsq<<<nb, 256, 0, ctx->stream>>>(n, d_dx, ctx->d_norm + 1);
+  k_sum_parts<<<1, 32, 0, ctx->stream>>>(nb, ctx->d_norm + 1, ctx->d_norm);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
+int icf_launch_accept(icf_ctx *ctx, double h) {
+  k_accept<<<icf_blocks(ctx->n_nodes, 256), 256, 0, ctx->stream>>>(
+      ctx->n_nodes, h, ctx->d_x0, ctx->d_u, ctx->d_v, ctx->d_a, ctx->d_un, ctx->d_du, ctx->d_xc);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
+int icf_launch_commit_cz(icf_ctx *ctx) {
+  if (ctx->n_cz == 0) return ICF_OK;
+  k_commit_cz<<<icf_blocks(ctx->n_cz, 256), 256, 0, ctx->stream>>>(
+      ctx->n_cz, ctx->d_cztent, ctx->d_czflags, ctx->d_czs, ctx->d_czfail);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}

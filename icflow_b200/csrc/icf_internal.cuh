@@ -1,0 +1,190 @@
+// icf_internal.cuh -- shared definitions of the icflow_b200 library (not part
+// of the public ABI).
+//
+// Device data layout (one context):
+//   nodes     x0[n]  double4 {x, y, z, 0}        rest coordinates (static)
+//             xc[n]  double4 {x, y, z, 0}        x0 + un of this iteration
+//             va[n]  double2[3] {vx vy | vz ax | ay az}
+//   tets      elem[ne] int4                       global node ids
+//   CZs       cz[nc*8] int                        6 node ids + 2 pad (32 B)
+//   CZ state  czs[nc*8] double                    pmax[3], tmax[3], pad
+//   staging   es[ne*8] double4                    per tet vertex a:
+//                                                 es[8e+a]   = {h_a, V}
+//                                                 es[8e+4+a] = {rhs_a, 0}
+//             cs[nc*48] double                    per CZ: 6 symmetric 3x3
+//                                                 blocks Kt[i][j] (i<=j, 6 each)
+//                                                 then rt[3][3], pad
+//             ks[ni*160] double                   per impact: 144 LHS + 12 rhs
+//   pattern   static keys (row<<32|col) sorted, rc_off[nnz_s+1], rc[] codes
+//             merged pattern rows/cols + src (static index of merged slot)
+//
+// Contribution codes (32 bit), one per (unit, row vertex a, column vertex b)
+// with alt(b) >= alt(a):
+//   bits 31..30 kind: 0 tet, 1 CZ, 2 impact
+//   tet/impact: bits 29..4 unit, 3..2 a, 1..0 b
+//   CZ:         bits 29..6 unit, 5..3 a, 2..0 b
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/icflow_b200.h"
+
+#define ICF_KIND_TET 0u
+#define ICF_KIND_CZ 1u
+#define ICF_KIND_IMP 2u
+#define ICF_MAX_TET_UNITS (1 << 26)
+#define ICF_MAX_CZ_UNITS (1 << 24)
+#define ICF_CZ_STAGE 48   // doubles per CZ in the staging buffer
+#define ICF_IMP_STAGE 160 // doubles per impact in the staging buffer
+
+// node -> (unit << 2 | vertex) incidence list in CSR form
+struct icf_node_inc {
+  int *off = nullptr, *inc = nullptr;
+};
+
+__host__ __device__ inline uint32_t icf_code_tet(uint32_t kind, uint32_t u,
+                                                 uint32_t a, uint32_t b) {
+  return (kind << 30) | (u << 4) | (a << 2) | b;
+}
+__host__ __device__ inline uint32_t icf_code_cz(uint32_t u, uint32_t a,
+                                                uint32_t b) {
+  return (ICF_KIND_CZ << 30) | (u << 6) | (a << 3) | b;
+}
+
+// Parameters the kernels read, passed by value (they live in the kernel
+// parameter bank, i.e. constant memory).
+struct icf_dprm {
+  double lam, mu;   // Lame constants of the isotropic E
+  double rho20;     // rho / 20 (consistent mass pattern)
+  double dm, ds;    // Rayleigh damping (mass, stiffness)
+  double nbeta, ngamma;
+  double grav_rho;  // gravity * rho
+  // PPR (global values; per-CZ f_tn, f_tt, deln, delt may override)
+  double f_tn, f_tt, alpha, beta, rn, rt, p_m, p_n, deln, delt, pMtn, pMnt,
+      gam_n, gam_t;
+  double sf[9];     // sf[node*3+gp]
+  double penaltyK, eps2;
+};
+
+struct icf_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  icf_params prm{};
+  bool have_prm = false;
+  int precision = ICF_FP64;
+
+  // sizes
+  int n_nodes = 0, n_elem = 0, n_cz = 0, n_surf = 0, n_faces = 0;
+  int N = 0;          // rows of the pattern
+  int nnz_s = 0;      // static blocks
+  long long n_rc = 0; // static contribution codes
+  int nnz = 0;        // merged blocks
+  bool have_static = false, have_nodes = false, have_structure = false;
+  bool src_identity = true;
+
+  // topology
+  int4 *d_elem = nullptr;
+  int *d_cz = nullptr;
+  int *d_alt = nullptr;
+  int4 *d_selem = nullptr;
+  int *d_adj_off = nullptr, *d_adj = nullptr, *d_faces = nullptr;
+  std::vector<int> h_alt;
+
+  // node state
+  double4 *d_x0 = nullptr, *d_xc = nullptr;
+  double2 *d_va = nullptr;
+  double *d_u = nullptr, *d_v = nullptr, *d_a = nullptr, *d_du = nullptr;
+  double *d_un = nullptr; // tentative displacement (for accept)
+  double *d_h3 = nullptr; // H2D staging for n_nodes*3 fields (3 arrays)
+
+  // CZ state
+  double *d_czs = nullptr;      // current pmax[3], tmax[3]
+  int *d_czfail = nullptr;      // committed failed flag
+  double *d_cztent = nullptr;   // pmax_, tmax_
+  int *d_czflags = nullptr;     // contact | damaged<<1 | failed<<2
+  double *d_czavg = nullptr;    // avgDn, avgDt, avgTn, avgTt
+  double4 *d_czprm = nullptr;   // per-CZ f_tn, f_tt, deln, delt
+  bool per_cz_prm = false;
+
+  // staging
+  double4 *d_es = nullptr;
+  double *d_cs = nullptr;
+  double *d_ks = nullptr;
+  int ks_cap = 0;
+
+  // static pattern
+  unsigned long long *d_skeys = nullptr;
+  int *d_rc_off = nullptr;
+  uint32_t *d_rc = nullptr;
+
+  // merged pattern
+  int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;
+  int rows_cap = 0, cols_cap = 0;
+  unsigned long long *d_mkeys = nullptr;
+
+  // impacts and their contributions
+  int n_imp = 0, imp_cap = 0;
+  int4 *d_imp = nullptr;
+  int n_crs = 0;                  // slots touched by impacts
+  int *d_cr_slot = nullptr, *d_cr_off = nullptr;
+  uint32_t *d_cr = nullptr;
+  int cr_cap = 0;
+
+  // narrow phase
+  int n_pairs = 0, pairs_cap = 0;
+  int *d_pairs = nullptr, *d_masks = nullptr;
+
+  // node incidence lists for the node forces
+  icf_node_inc tet_inc, imp_inc;
+
+  // outputs
+  double *d_vals = nullptr, *d_rhs = nullptr, *d_nodeF = nullptr;
+  int vals_cap = 0;
+
+  // counters: [0] damaged [1] failed [2] contact [3] active impacts [4] nonfinite
+  int *d_counts = nullptr;
+  int *h_counts = nullptr; // pinned
+  double *d_norm = nullptr;
+  double *h_norm = nullptr; // pinned
+
+  // scratch
+  void *d_tmp = nullptr;
+  size_t tmp_bytes = 0;
+};
+
+// ---- error plumbing ---------------------------------------------------------
+int icf_fail(icf_ctx *ctx, int code, const std::string &msg);
+#define ICF_CUDA(ctx, call)                                                    \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess)                                                     \
+      return icf_fail((ctx), ICF_ERR_CUDA,                                     \
+                      std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+int icf_scratch(icf_ctx *ctx, size_t bytes);
+
+inline unsigned icf_blocks(long long n, int bs) {
+  return (unsigned)((n + bs - 1) / bs);
+}
+
+icf_dprm icf_make_dprm(const icf_ctx *ctx);
+
+// ---- kernels and launchers implemented in the .cu files ---------------------
+int icf_build_static_pattern(icf_ctx *ctx);
+int icf_build_merged_pattern(icf_ctx *ctx);
+int icf_launch_assembly(icf_ctx *ctx, double h);
+int icf_launch_node_force(icf_ctx *ctx);
+int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts);
+int icf_launch_pcsr(icf_ctx *ctx, int kind, int *d_out);
+int icf_launch_pack_nodes(icf_ctx *ctx, const double *d_un, const double *d_vn,
+                          const double *d_an);
+int icf_launch_infer(icf_ctx *ctx, double h);
+int icf_launch_add_dx(icf_ctx *ctx, const double *d_dx);
+int icf_launch_accept(icf_ctx *ctx, double h);
+int icf_launch_commit_cz(icf_ctx *ctx);
+int icf_launch_imp_unit(icf_ctx *ctx);
+int icf_get_node_inc(icf_ctx *ctx, icf_node_inc *tets, icf_node_inc *imps);

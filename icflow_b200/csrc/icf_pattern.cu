@@ -1,0 +1,555 @@
+// icf_pattern.cu -- the upper-triangular 3x3-block sparsity pattern and the
+// slot-sorted contribution lists, built on the device.
+//
+// Static part (elements and every CZ that is not failed when the pattern is
+// first built; MeshCollection.cs:91-109, j >= i).  The reference never
+// clears its static neighbour sets (CSRDictionary.ClearStatic has no
+// caller), so the static pattern only grows: it is built once and kept.
+// Dynamic part (impacts, ImplicitModel3.cs:177-196, j > i) is merged into it
+// on every icf_create_structure call.  Columns ascend within a row
+// (CSRDictionary.cs:90) and slots number the blocks row by row.
+//
+// Each candidate block (unit, a, b) is a 64-bit key (alt_a << 32 | alt_b)
+// paired with a 32-bit contribution code.  A stable radix sort by key puts
+// the contributions of every block next to each other, in unit order; the
+// run heads are the slots.  That sorted code list is what k_gather walks.
+#include <cub/cub.cuh>
+
+#include "icf_internal.cuh"
+
+namespace {
+constexpr unsigned long long KMAX = ~0ull;
+
+__global__ void k_cand_tet(int ne, const int4 *__restrict__ elem, const int *__restrict__ alt,
+                           unsigned long long *__restrict__ key, uint32_t *__restrict__ code) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int4 id = elem[e];
+  const int nid[4] = {id.x, id.y, id.z, id.w};
+  int al[4];
+  for (int i = 0; i < 4; i++) al[i] = alt[nid[i]];
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) {
+      const size_t o = 16 * (size_t)e + 4 * a + b;
+      const bool ok = al[a] >= 0 && al[b] >= 0 && al[b] >= al[a];
+      key[o] = ok ? (((unsigned long long)al[a] << 32) | (unsigned)al[b]) : KMAX;
+      code[o] = icf_code_tet(ICF_KIND_TET, e, a, b);
+    }
+}
+
+__global__ void k_cand_cz(int nc, const int *__restrict__ cz, const int *__restrict__ fail,
+                          const int *__restrict__ alt, unsigned long long *__restrict__ key,
+                          uint32_t *__restrict__ code) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  int al[6];
+  for (int i = 0; i < 6; i++) al[i] = alt[cz[8 * c + i]];
+  const bool live = fail[c] == 0;
+  for (int a = 0; a < 6; a++)
+    for (int b = 0; b < 6; b++) {
+      const size_t o = 36 * (size_t)c + 6 * a + b;
+      const bool ok = live && al[a] >= 0 && al[b] >= 0 && al[b] >= al[a];
+      key[o] = ok ? (((unsigned long long)al[a] << 32) | (unsigned)al[b]) : KMAX;
+      code[o] = icf_code_cz(c, a, b);
+    }
+}
+
+// run heads of a sorted key array (KMAX excluded)
+__global__ void k_heads(long long n, const unsigned long long *__restrict__ key, int *__restrict__ flag) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long k = key[i];
+  flag[i] = (k != KMAX && (i == 0 || key[i - 1] != k)) ? 1 : 0;
+}
+
+__global__ void k_slots(long long n, const unsigned long long *__restrict__ key,
+                        const int *__restrict__ flag, const int *__restrict__ incl,
+                        unsigned long long *__restrict__ skey, int *__restrict__ off) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n || !flag[i]) return;
+  const int s = incl[i] - 1;
+  skey[s] = key[i];
+  off[s] = (int)i;
+}
+
+__device__ __forceinline__ long long lower_bound_u64(const unsigned long long *a, long long n,
+                                                     unsigned long long v) {
+  long long lo = 0, hi = n;
+  while (lo < hi) {
+    const long long m = (lo + hi) >> 1;
+    if (a[m] < v) lo = m + 1;
+    else hi = m;
+  }
+  return lo;
+}
+
+__global__ void k_count_valid(long long n, const unsigned long long *__restrict__ key, long long *out) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *out = lower_bound_u64(key, n, KMAX);
+}
+
+__global__ void k_rows(int N, int nnz, const unsigned long long *__restrict__ key, int *__restrict__ rows) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > N) return;
+  rows[r] = (int)lower_bound_u64(key, nnz, (unsigned long long)r << 32);
+}
+
+__global__ void k_cols(int nnz, const unsigned long long *__restrict__ key, int *__restrict__ cols) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nnz) return;
+  cols[s] = (int)(key[s] & 0xffffffffull);
+}
+
+__global__ void k_cand_dyn(int ni, const int4 *__restrict__ imp, const int *__restrict__ alt,
+                           unsigned long long *__restrict__ key) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= ni) return;
+  const int4 id = imp[u];
+  const int nid[4] = {id.x, id.y, id.z, id.w};
+  int al[4];
+  for (int i = 0; i < 4; i++) al[i] = nid[i] >= 0 ? alt[nid[i]] : -1;
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) {
+      const bool ok = al[a] >= 0 && al[b] >= 0 && al[b] > al[a];
+      key[16 * (size_t)u + 4 * a + b] = ok ? (((unsigned long long)al[a] << 32) | (unsigned)al[b]) : KMAX;
+    }
+}
+
+// keep dynamic keys that are new (not in the static pattern); flag rows that
+// fall outside the pattern (the reference would throw there)
+__global__ void k_dyn_new(int n, const unsigned long long *__restrict__ dkey,
+                          const unsigned long long *__restrict__ skey, int nnz_s, int N,
+                          int *__restrict__ keep, int *__restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long k = dkey[i];
+  int kp = 0;
+  if (k != KMAX) {
+    if ((int)(k >> 32) >= N) atomicOr(bad, 1);
+    const long long p = lower_bound_u64(skey, nnz_s, k);
+    kp = !(p < nnz_s && skey[p] == k);
+  }
+  keep[i] = kp;
+}
+
+__global__ void k_merge_static(int nnz_s, const unsigned long long *__restrict__ skey,
+                               const unsigned long long *__restrict__ dkey, int nd,
+                               unsigned long long *__restrict__ mkey, int *__restrict__ src) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz_s) return;
+  const long long p = i + lower_bound_u64(dkey, nd, skey[i]);
+  mkey[p] = skey[i];
+  src[p] = i;
+}
+
+__global__ void k_merge_dyn(int nd, const unsigned long long *__restrict__ dkey,
+                            const unsigned long long *__restrict__ skey, int nnz_s,
+                            unsigned long long *__restrict__ mkey, int *__restrict__ src) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nd) return;
+  const long long p = j + lower_bound_u64(skey, nnz_s, dkey[j]);
+  mkey[p] = dkey[j];
+  src[p] = -1;
+}
+
+// impact contributions keyed by their merged slot
+__global__ void k_cand_imp_rc(int ni, const int4 *__restrict__ imp, const int *__restrict__ alt,
+                              const unsigned long long *__restrict__ mkey, int nnz,
+                              int *__restrict__ slot, uint32_t *__restrict__ code) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= ni) return;
+  const int4 id = imp[u];
+  const int nid[4] = {id.x, id.y, id.z, id.w};
+  int al[4];
+  for (int i = 0; i < 4; i++) al[i] = nid[i] >= 0 ? alt[nid[i]] : -1;
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) {
+      const size_t o = 16 * (size_t)u + 4 * a + b;
+      int s = 0x7fffffff;
+      if (al[a] >= 0 && al[b] >= 0 && al[b] >= al[a]) {
+        const unsigned long long k = ((unsigned long long)al[a] << 32) | (unsigned)al[b];
+        const long long p = lower_bound_u64(mkey, nnz, k);
+        if (p < nnz && mkey[p] == k) s = (int)p;
+      }
+      slot[o] = s;
+      code[o] = icf_code_tet(ICF_KIND_IMP, u, a, b);
+    }
+}
+
+// node incidence lists: (node, unit << 2 | vertex)
+__global__ void k_node_inc_tet(int ne, const int4 *__restrict__ elem, int *__restrict__ node,
+                               int *__restrict__ code) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int4 id = elem[e];
+  const int nid[4] = {id.x, id.y, id.z, id.w};
+  for (int a = 0; a < 4; a++) {
+    node[4 * (size_t)e + a] = nid[a];
+    code[4 * (size_t)e + a] = (e << 2) | a;
+  }
+}
+__global__ void k_node_inc_imp(int ni, const int4 *__restrict__ imp, int *__restrict__ node,
+                               int *__restrict__ code) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= ni) return;
+  const int4 id = imp[u];
+  const int nid[4] = {id.x, id.y, id.z, id.w};
+  for (int a = 0; a < 4; a++) {
+    node[4 * (size_t)u + a] = nid[a] >= 0 ? nid[a] : 0x7fffffff;
+    code[4 * (size_t)u + a] = (u << 2) | a;
+  }
+}
+__global__ void k_offsets_from_sorted(int n_items, const int *__restrict__ node, int n_nodes,
+                                      int *__restrict__ off) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n_nodes) return;
+  int lo = 0, hi = n_items;
+  while (lo < hi) {
+    const int m = (lo + hi) >> 1;
+    if (node[m] < i) lo = m + 1;
+    else hi = m;
+  }
+  off[i] = lo;
+}
+
+// pcsr maps in the reference's logical layout
+__global__ void k_pcsr(int n, int k, const int *__restrict__ nodes, int stride,
+                       const int *__restrict__ alt, const unsigned long long *__restrict__ mkey,
+                       int nnz, int *__restrict__ out) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const int w = k * k + k;
+  int al[6];
+  for (int i = 0; i < k; i++) {
+    const int nd = nodes[(size_t)u * stride + i];
+    al[i] = nd >= 0 ? alt[nd] : -1;
+  }
+  for (int i = 0; i < k; i++) {
+    for (int j = 0; j < k; j++) {
+      int s = -1;
+      if (al[i] >= 0 && al[j] >= 0 && al[j] >= al[i]) {
+        const unsigned long long key = ((unsigned long long)al[i] << 32) | (unsigned)al[j];
+        const long long p = lower_bound_u64(mkey, nnz, key);
+        if (p < nnz && mkey[p] == key) s = (int)p;
+      }
+      out[(size_t)u * w + i * k + j] = s;
+    }
+    out[(size_t)u * w + k * k + i] = al[i];
+  }
+}
+
+}  // namespace
+
+template <typename T>
+static int sort_pairs(icf_ctx *ctx, T *k_in, T *k_out, int *v_in, int *v_out, int n) {
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, k_in, k_out, v_in, v_out, n, 0, (int)(8 * sizeof(T)),
+                                  ctx->stream);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k_in, k_out, v_in, v_out, n, 0,
+                                                (int)(8 * sizeof(T)), ctx->stream));
+  return ICF_OK;
+}
+
+// node -> (unit, vertex) lists for the node forces
+static int build_inc(icf_ctx *ctx, int n_items, void (*fill)(icf_ctx *, int *, int *),
+                     icf_node_inc *out) {
+  cudaStream_t s = ctx->stream;
+  cudaFree(out->off);
+  cudaFree(out->inc);
+  out->off = out->inc = nullptr;
+  ICF_CUDA(ctx, cudaMalloc(&out->off, sizeof(int) * (size_t)(ctx->n_nodes + 1)));
+  ICF_CUDA(ctx, cudaMalloc(&out->inc, sizeof(int) * (size_t)(n_items > 0 ? n_items : 1)));
+  if (n_items == 0) {
+    ICF_CUDA(ctx, cudaMemsetAsync(out->off, 0, sizeof(int) * (size_t)(ctx->n_nodes + 1), s));
+    return ICF_OK;
+  }
+  int *nd0, *nd1, *cd0;
+  ICF_CUDA(ctx, cudaMallocAsync(&nd0, sizeof(int) * n_items, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&nd1, sizeof(int) * n_items, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&cd0, sizeof(int) * n_items, s));
+  fill(ctx, nd0, cd0);
+  ICF_CUDA(ctx, cudaGetLastError());
+  int rc = sort_pairs<int>(ctx, nd0, nd1, cd0, out->inc, n_items);
+  if (rc) return rc;
+  k_offsets_from_sorted<<<icf_blocks(ctx->n_nodes + 1, 256), 256, 0, s>>>(n_items, nd1, ctx->n_nodes,
+                                                                         out->off);
+  ICF_CUDA(ctx, cudaGetLastError());
+  ICF_CUDA(ctx, cudaFreeAsync(nd0, s));
+  ICF_CUDA(ctx, cudaFreeAsync(nd1, s));
+  ICF_CUDA(ctx, cudaFreeAsync(cd0, s));
+  return ICF_OK;
+}
+
+static void fill_tet(icf_ctx *ctx, int *node, int *code) {
+  k_node_inc_tet<<<icf_blocks(ctx->n_elem, 256), 256, 0, ctx->stream>>>(ctx->n_elem, ctx->d_elem, node,
+                                                                       code);
+}
+static void fill_imp(icf_ctx *ctx, int *node, int *code) {
+  k_node_inc_imp<<<icf_blocks(ctx->n_imp, 256), 256, 0, ctx->stream>>>(ctx->n_imp, ctx->d_imp, node, code);
+}
+
+int icf_get_node_inc(icf_ctx *ctx, icf_node_inc *tets, icf_node_inc *imps) {
+  if (!ctx->tet_inc.off) {
+    int rc = build_inc(ctx, 4 * ctx->n_elem, fill_tet, &ctx->tet_inc);
+    if (rc) return rc;
+  }
+  // impact incidences are rebuilt whenever asked (impacts change per iteration)
+  int rc = build_inc(ctx, 4 * ctx->n_imp, fill_imp, &ctx->imp_inc);
+  if (rc) return rc;
+  *tets = ctx->tet_inc;
+  *imps = ctx->imp_inc;
+  return ICF_OK;
+}
+
+int icf_build_static_pattern(icf_ctx *ctx) {
+  cudaStream_t s = ctx->stream;
+  const long long nc = 16LL * ctx->n_elem + 36LL * ctx->n_cz;
+  if (nc >= (1LL << 31)) return icf_fail(ctx, ICF_ERR_SIZE, "pattern candidate count exceeds 2^31");
+  if (nc == 0) {
+    ctx->nnz_s = 0;
+    ctx->n_rc = 0;
+    ctx->N = 0;
+    ICF_CUDA(ctx, cudaMalloc(&ctx->d_skeys, sizeof(unsigned long long)));
+    ICF_CUDA(ctx, cudaMalloc(&ctx->d_rc_off, sizeof(int)));
+    ICF_CUDA(ctx, cudaMemset(ctx->d_rc_off, 0, sizeof(int)));
+    return ICF_OK;
+  }
+  unsigned long long *k0, *k1;
+  uint32_t *c0;
+  int *flag, *incl;
+  long long *d_nv;
+  ICF_CUDA(ctx, cudaMallocAsync(&k0, sizeof(unsigned long long) * (nc + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&k1, sizeof(unsigned long long) * (nc + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&c0, sizeof(uint32_t) * (nc + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&flag, sizeof(int) * (nc + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&incl, sizeof(int) * (nc + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&d_nv, sizeof(long long), s));
+  if (ctx->d_rc) cudaFree(ctx->d_rc);
+  ctx->d_rc = nullptr;
+  ICF_CUDA(ctx, cudaMalloc(&ctx->d_rc, sizeof(uint32_t) * (nc + 1)));
+  if (ctx->n_elem)
+    k_cand_tet<<<icf_blocks(ctx->n_elem, 256), 256, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_alt, k0, c0);
+  if (ctx->n_cz)
+    k_cand_cz<<<icf_blocks(ctx->n_cz, 256), 256, 0, s>>>(ctx->n_cz, ctx->d_cz, ctx->d_czfail, ctx->d_alt,
+                                                        k0 + 16LL * ctx->n_elem, c0 + 16LL * ctx->n_elem);
+  ICF_CUDA(ctx, cudaGetLastError());
+  {
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, c0, ctx->d_rc, (int)nc, 0, 64, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, c0, ctx->d_rc, (int)nc, 0, 64, s));
+  }
+  k_heads<<<icf_blocks(nc, 256), 256, 0, s>>>(nc, k1, flag);
+  {
+    size_t tb = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tb, flag, incl, (int)nc, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceScan::InclusiveSum(ctx->d_tmp, tb, flag, incl, (int)nc, s));
+  }
+  int nnz_s = 0;
+  long long nv = 0;
+  k_count_valid<<<1, 32, 0, s>>>(nc, k1, d_nv);
+  if (nc > 0) ICF_CUDA(ctx, cudaMemcpyAsync(&nnz_s, incl + nc - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(&nv, d_nv, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  cudaFree(ctx->d_skeys);
+  cudaFree(ctx->d_rc_off);
+  ctx->d_skeys = nullptr;
+  ctx->d_rc_off = nullptr;
+  ICF_CUDA(ctx, cudaMalloc(&ctx->d_skeys, sizeof(unsigned long long) * (size_t)(nnz_s + 1)));
+  ICF_CUDA(ctx, cudaMalloc(&ctx->d_rc_off, sizeof(int) * (size_t)(nnz_s + 1)));
+  k_slots<<<icf_blocks(nc, 256), 256, 0, s>>>(nc, k1, flag, incl, ctx->d_skeys, ctx->d_rc_off);
+  const int nvi = (int)nv;
+  ICF_CUDA(ctx, cudaMemcpyAsync(ctx->d_rc_off + nnz_s, &nvi, sizeof(int), cudaMemcpyHostToDevice, s));
+  unsigned long long last = 0;
+  if (nnz_s > 0)
+    ICF_CUDA(ctx, cudaMemcpyAsync(&last, ctx->d_skeys + nnz_s - 1, sizeof(last), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaFreeAsync(k0, s));
+  ICF_CUDA(ctx, cudaFreeAsync(k1, s));
+  ICF_CUDA(ctx, cudaFreeAsync(c0, s));
+  ICF_CUDA(ctx, cudaFreeAsync(flag, s));
+  ICF_CUDA(ctx, cudaFreeAsync(incl, s));
+  ICF_CUDA(ctx, cudaFreeAsync(d_nv, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  ctx->nnz_s = nnz_s;
+  ctx->n_rc = nv;
+  ctx->N = nnz_s > 0 ? (int)(last >> 32) + 1 : 0;
+  return ICF_OK;
+}
+
+template <typename T>
+static int grow(icf_ctx *ctx, T **p, int *cap, long long n) {
+  if (n <= *cap && *p) return ICF_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  const long long c = n + n / 4 + 16;
+  ICF_CUDA(ctx, cudaMalloc(p, sizeof(T) * (size_t)c));
+  *cap = (int)c;
+  return ICF_OK;
+}
+
+int icf_build_merged_pattern(icf_ctx *ctx) {
+  cudaStream_t s = ctx->stream;
+  const int nnz_s = ctx->nnz_s, N = ctx->N;
+  int nd = 0;
+  unsigned long long *dkeys = nullptr;
+  if (ctx->n_imp > 0) {
+    const int n = 16 * ctx->n_imp;
+    unsigned long long *a, *b;
+    int *keep, *d_nd, *d_bad;
+    ICF_CUDA(ctx, cudaMallocAsync(&a, sizeof(unsigned long long) * n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&b, sizeof(unsigned long long) * n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&keep, sizeof(int) * n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&d_nd, sizeof(int) * 2, s));
+    d_bad = d_nd + 1;
+    ICF_CUDA(ctx, cudaMemsetAsync(d_nd, 0, sizeof(int) * 2, s));
+    k_cand_dyn<<<icf_blocks(ctx->n_imp, 128), 128, 0, s>>>(ctx->n_imp, ctx->d_imp, ctx->d_alt, a);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, a, b, n, 0, 64, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, a, b, n, 0, 64, s));
+    tb = 0;
+    cub::DeviceSelect::Unique(nullptr, tb, b, a, d_nd, n, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, b, a, d_nd, n, s));
+    int nu = 0;
+    ICF_CUDA(ctx, cudaMemcpyAsync(&nu, d_nd, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    if (nu > 0) k_dyn_new<<<icf_blocks(nu, 128), 128, 0, s>>>(nu, a, ctx->d_skeys, nnz_s, N, keep, d_bad);
+    tb = 0;
+    cub::DeviceSelect::Flagged(nullptr, tb, a, keep, b, d_nd, nu, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceSelect::Flagged(ctx->d_tmp, tb, a, keep, b, d_nd, nu, s));
+    int hb[2] = {0, 0};
+    ICF_CUDA(ctx, cudaMemcpyAsync(hb, d_nd, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    nd = hb[0];
+    if (hb[1]) return icf_fail(ctx, ICF_ERR_STATE, "an impact references a row outside the pattern");
+    dkeys = b;
+    ICF_CUDA(ctx, cudaFreeAsync(a, s));
+    ICF_CUDA(ctx, cudaFreeAsync(keep, s));
+    ICF_CUDA(ctx, cudaFreeAsync(d_nd, s));
+  }
+  const int nnz = nnz_s + nd;
+  if (nnz + 1 > ctx->cols_cap || !ctx->d_cols) {
+    cudaFree(ctx->d_cols);
+    cudaFree(ctx->d_src);
+    cudaFree(ctx->d_mkeys);
+    ctx->d_cols = ctx->d_src = nullptr;
+    ctx->d_mkeys = nullptr;
+    const long long cap = nnz + 1 + nnz / 8 + 64;
+    ICF_CUDA(ctx, cudaMalloc(&ctx->d_cols, sizeof(int) * (size_t)cap));
+    ICF_CUDA(ctx, cudaMalloc(&ctx->d_src, sizeof(int) * (size_t)cap));
+    ICF_CUDA(ctx, cudaMalloc(&ctx->d_mkeys, sizeof(unsigned long long) * (size_t)cap));
+    ctx->cols_cap = (int)cap;
+  }
+  int rc = grow(ctx, &ctx->d_rows, &ctx->rows_cap, (long long)N + 1);
+  if (rc) return rc;
+  if (nd == 0) {
+    ICF_CUDA(ctx, cudaMemcpyAsync(ctx->d_mkeys, ctx->d_skeys, sizeof(unsigned long long) * (size_t)nnz_s,
+                                  cudaMemcpyDeviceToDevice, s));
+    ctx->src_identity = true;
+  } else {
+    if (nnz_s > 0)
+      k_merge_static<<<icf_blocks(nnz_s, 256), 256, 0, s>>>(nnz_s, ctx->d_skeys, dkeys, nd, ctx->d_mkeys,
+                                                           ctx->d_src);
+    k_merge_dyn<<<icf_blocks(nd, 256), 256, 0, s>>>(nd, dkeys, ctx->d_skeys, nnz_s, ctx->d_mkeys, ctx->d_src);
+    ctx->src_identity = false;
+  }
+  if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
+  if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
+  k_rows<<<icf_blocks((long long)N + 1, 256), 256, 0, s>>>(N, nnz, ctx->d_mkeys, ctx->d_rows);
+  ICF_CUDA(ctx, cudaGetLastError());
+  ctx->nnz = nnz;
+
+  // impact contributions grouped by slot
+  ctx->n_crs = 0;
+  if (ctx->n_imp > 0) {
+    const int n = 16 * ctx->n_imp;
+    int *sl0, *sl1, *d_nr, *cnt;
+    uint32_t *cd0;
+    ICF_CUDA(ctx, cudaMallocAsync(&sl0, sizeof(int) * n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&sl1, sizeof(int) * n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&cd0, sizeof(uint32_t) * n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&cnt, sizeof(int) * (n + 1), s));
+    ICF_CUDA(ctx, cudaMallocAsync(&d_nr, sizeof(int), s));
+    if (n + 2 > ctx->cr_cap || !ctx->d_cr) {
+      cudaFree(ctx->d_cr);
+      cudaFree(ctx->d_cr_slot);
+      cudaFree(ctx->d_cr_off);
+      ctx->d_cr = nullptr;
+      ctx->d_cr_slot = ctx->d_cr_off = nullptr;
+      const long long cap = 2LL * n + 2;
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr, sizeof(uint32_t) * (size_t)cap));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr_slot, sizeof(int) * (size_t)cap));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr_off, sizeof(int) * (size_t)cap));
+      ctx->cr_cap = (int)cap;
+    }
+    k_cand_imp_rc<<<icf_blocks(ctx->n_imp, 128), 128, 0, s>>>(ctx->n_imp, ctx->d_imp, ctx->d_alt,
+                                                             ctx->d_mkeys, nnz, sl0, cd0);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, sl0, sl1, cd0, ctx->d_cr, n, 0, 32, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, sl0, sl1, cd0, ctx->d_cr, n, 0, 32, s));
+    tb = 0;
+    cub::DeviceRunLengthEncode::Encode(nullptr, tb, sl1, ctx->d_cr_slot, cnt, d_nr, n, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRunLengthEncode::Encode(ctx->d_tmp, tb, sl1, ctx->d_cr_slot, cnt, d_nr, n, s));
+    int nr = 0;
+    ICF_CUDA(ctx, cudaMemcpyAsync(&nr, d_nr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    // the last run is the invalid slot marker when any candidate was skipped
+    int last = 0;
+    if (nr > 0) {
+      ICF_CUDA(ctx, cudaMemcpyAsync(&last, ctx->d_cr_slot + nr - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+      ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    }
+    const int nvalid = (nr > 0 && last == 0x7fffffff) ? nr - 1 : nr;
+    ICF_CUDA(ctx, cudaMemsetAsync(cnt + nr, 0, sizeof(int), s));
+    tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, ctx->d_cr_off, nr + 1, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, cnt, ctx->d_cr_off, nr + 1, s));
+    ICF_CUDA(ctx, cudaFreeAsync(sl0, s));
+    ICF_CUDA(ctx, cudaFreeAsync(sl1, s));
+    ICF_CUDA(ctx, cudaFreeAsync(cd0, s));
+    ICF_CUDA(ctx, cudaFreeAsync(cnt, s));
+    ICF_CUDA(ctx, cudaFreeAsync(d_nr, s));
+    ctx->n_crs = nvalid;
+    // impact staging
+    if (ctx->n_imp > ctx->ks_cap) {
+      cudaFree(ctx->d_ks);
+      ctx->d_ks = nullptr;
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_ks, sizeof(double) * ICF_IMP_STAGE * (size_t)(2 * ctx->n_imp)));
+      ctx->ks_cap = 2 * ctx->n_imp;
+    }
+  }
+  // outputs
+  if ((long long)nnz * 9 > ctx->vals_cap || !ctx->d_vals) {
+    cudaFree(ctx->d_vals);
+    ctx->d_vals = nullptr;
+    const long long c = 9LL * (nnz + nnz / 8 + 64);
+    ICF_CUDA(ctx, cudaMalloc(&ctx->d_vals, sizeof(double) * (size_t)c));
+    ctx->vals_cap = (int)(c > 0x7fffffff ? 0x7fffffff : c);
+  }
+  cudaFree(ctx->d_rhs);
+  ctx->d_rhs = nullptr;
+  ICF_CUDA(ctx, cudaMalloc(&ctx->d_rhs, sizeof(double) * (size_t)(3LL * N + 3)));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  return ICF_OK;
+}
+
+int icf_launch_pcsr(icf_ctx *ctx, int kind, int *d_out) {
+  cudaStream_t s = ctx->stream;
+  if (kind == 0 && ctx->n_elem)
+    k_pcsr<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, 4, reinterpret_cast<const int *>(ctx->d_elem),
+                                                       4, ctx->d_alt, ctx->d_mkeys, ctx->nnz, d_out);
+  else if (kind == 1 && ctx->n_cz)
+    k_pcsr<<<icf_blocks(ctx->n_cz, 128), 128, 0, s>>>(ctx->n_cz, 6, ctx->d_cz, 8, ctx->d_alt, ctx->d_mkeys,
+                                                     ctx->nnz, d_out);
+  else if (kind == 2 && ctx->n_imp)
+    k_pcsr<<<icf_blocks(ctx->n_imp, 128), 128, 0, s>>>(ctx->n_imp, 4, reinterpret_cast<const int *>(ctx->d_imp),
+                                                      4, ctx->d_alt, ctx->d_mkeys, ctx->nnz, d_out);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}

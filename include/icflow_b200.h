@@ -1,0 +1,221 @@
+/* icflow_b200.h -- C ABI of the B200 (sm_100a) assembly path for icFlow.
+ *
+ * This library replaces the ManagedCUDA/PTX layer of icFlow, i.e. the C#
+ * class GPU_Functionality (v3Library/Simulation/GPU/GPU_Functionality.cs:13)
+ * together with the sparsity-pattern builder CSRDictionary
+ * (v3Library/Simulation/LinearSystem/CSRDictionary.cs:17) and the Newmark
+ * node kinematics of Node (v3Library/Geometry/Node.cs:62-97).  It follows the
+ * in-repo precedent of a Cdecl C-ABI DLL called through P/Invoke
+ * (LinearSystem.cs:45-46 -> PardisoLoader2/dllmain.cpp:30).
+ *
+ * Conventions
+ *  - Every function returns int: ICF_OK (0) or a negative ICF_ERR_* code;
+ *    icf_last_error() gives a message.  Nothing aborts, nothing throws.
+ *  - Host buffers belong to the caller and are used only during the call.
+ *  - Node fields are arrays of n_nodes x 3 doubles (x, y, z per node), in
+ *    MeshCollection.allNodes order (globalNodeId).  Unit node lists are
+ *    n x 4 (tets, impacts) or n x 6 (cohesive zones) ints of global node ids.
+ *  - alt_id[node] is the row of the node in the linear system (Node.altId),
+ *    -1 for anchored nodes (ImplicitModel3.cs:62-73).
+ *  - Calls on one context must come from one thread at a time; distinct
+ *    contexts are independent.  Each call makes its device current.
+ *  - Results are deterministic: no floating-point atomics are used, so two
+ *    runs on the same input give bit-identical matrices.
+ */
+#ifndef ICFLOW_B200_H
+#define ICFLOW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ICF_OK 0
+#define ICF_ERR_ARG (-1)      /* null pointer, bad index, bad count */
+#define ICF_ERR_SIZE (-2)     /* buffer or capacity too small, unit limit */
+#define ICF_ERR_CUDA (-3)     /* CUDA runtime error */
+#define ICF_ERR_STATE (-4)    /* call order (e.g. assemble before structure) */
+#define ICF_ERR_NUMERIC (-5)  /* NaN/Inf produced on the device */
+#define ICF_ERR_NODEVICE (-6) /* no usable sm_100 device */
+
+typedef struct icf_ctx icf_ctx;
+
+/* Mirror of ModelPrms (v3Library/Simulation/DataSheets/ModelPrms.cs);
+ * field names kept.  The block after "derived" is filled by
+ * icf_params_derive (ModelPrms.SetComputedVariables, :237-322). */
+typedef struct icf_params {
+  double InitialTimeStep;
+  /* material, :133-156 */
+  double Y, nu, rho, dampingMass, dampingStiffness, gravity;
+  /* integration, :177-209 */
+  double NewmarkBeta, NewmarkGamma;
+  double ConvergenceEpsilon, ConvergenceCutoff;
+  double maxDamagePerStep, maxFailPerStep;
+  int maxIterations, minIterations;
+  /* cohesive zones, :37-65 */
+  double alpha, beta, lambda_n, lambda_t, phi_n, phi_t, sigma_max, tau_max;
+  /* collisions, :158-175 (CollisionScheme: 0 None, 1 Everything) */
+  int CollisionScheme;
+  double penaltyK, DistanceEpsilon;
+  /* derived */
+  double E[36];  /* E[i*6+j], isotropic elasticity, engineering shear */
+  double M[144]; /* M[i*12+j], consistent mass pattern (times volume) */
+  double sf[9];  /* sf[node*3+gp] */
+  double B[162]; /* B[(gp*3+coord)*18+dof] */
+  double G_fn, G_ft, f_tn, f_tt, rn, rt, p_m, p_n, deln, delt, pMtn, pMnt,
+      gam_n, gam_t;
+  double nThreshold, tThreshold;
+} icf_params;
+
+/* Arithmetic of the element and CZ Hessians.  FP64 everywhere (ICF_FP64) or
+ * FP32 Hessians with FP64 rotation, near-separation cohesive law and FP64
+ * accumulation (ICF_FP32_MIXED). */
+#define ICF_FP64 0
+#define ICF_FP32_MIXED 1
+
+/* Per-assembly counters (FrameInfo fields set by AssembleElemsAndCZs,
+ * GPU_Functionality.cs:444-475, and NarrowPhaseCollisionDetection). */
+typedef struct icf_counts {
+  int nElems;            /* elastic elements assembled */
+  int nCZ;               /* non-failed CZs assembled */
+  int nCZDamaged;        /* Sum(TENTATIVE_DAMAGED) */
+  int nCZFailedThisStep; /* Sum(TENTATIVE_FAILED) */
+  int nCZContact;        /* CZs with a Gauss point in contact */
+  int nImpacts;          /* impacts in the current structure */
+  int nImpactsActive;    /* impacts that produced a penalty response */
+  int nonFinite;         /* 1 if a NaN/Inf reached the matrix or rhs */
+} icf_counts;
+
+/* Device buffers, for callers that chain device work (graphs, solvers).
+ * Pointers stay valid until the next call that changes the pattern size. */
+typedef struct icf_device_buffers {
+  double *vals;    /* nnz*9: block s at vals[9s], row-major 3x3 */
+  double *rhs;     /* N*3 */
+  int *csr_rows;   /* N+1 */
+  int *csr_cols;   /* nnz */
+  void *stream;    /* cudaStream_t used by the context */
+  int N, nnz;
+} icf_device_buffers;
+
+/* ---- context, GPU_Functionality(int deviceID) :112-137 ----------------- */
+int icf_create(int device, icf_ctx **out);
+int icf_destroy(icf_ctx *ctx);
+const char *icf_last_error(const icf_ctx *ctx);
+/* Library version string, e.g. "icflow_b200 1.0 sm_100a". */
+const char *icf_version(void);
+
+/* ---- parameters, ModelPrms.SetComputedVariables :237-322 ---------------- */
+/* Host only; fills the derived block of *p. */
+int icf_params_derive(icf_params *p);
+/* SetConstants, GPU_Functionality.cs:151-194 (derives, then uploads). */
+int icf_set_constants(icf_ctx *ctx, const icf_params *p);
+int icf_set_precision(icf_ctx *ctx, int precision);
+/* Per-CZ strengths (extension of cz_constants.h:7, which is global in the
+ * reference): sigma_max[c], tau_max[c] for every CZ; NULL restores the
+ * global values.  deln/delt are derived per CZ. */
+int icf_set_cz_strength(icf_ctx *ctx, int n_czs, const double *sigma_max,
+                        const double *tau_max);
+
+/* ---- static data, TransferStaticDataToDevice :255-302 ------------------- */
+/* Mesh topology and the tables the narrow phase needs:
+ *   elems[n_elems*4]        elastic elements (MeshCollection.elasticElements)
+ *   czs[n_czs*6]            all CZs (vrts[0..5], CZ.cs:488)
+ *   alt_id[n_nodes]         row per node, -1 anchored
+ *   x0[n_nodes*3]           rest coordinates
+ *   surface_elems[n_surface*4]                 (MeshCollection.surfaceElements)
+ *   adj_offsets[n_surface+1], adj_faces[...]   Element.adjFaces in order
+ *   faces[n_faces*3]        MeshCollection.allFaces vertices
+ * The static sparsity pattern (elements + CZs, MeshCollection.cs:91-109) is
+ * built here on the device.  n_surface may be 0 (no contact). */
+int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0,
+                        const int *alt_id, int n_elems, const int *elems,
+                        int n_czs, const int *czs, int n_surface,
+                        const int *surface_elems, const int *adj_offsets,
+                        const int *adj_faces, int n_faces, const int *faces);
+
+/* ---- per-iteration node state, TransferNodesToGPU :307-343 -------------- */
+/* un, vn, an: tentative displacement, velocity, acceleration (Node.un*, vn*,
+ * an*).  The current position x0 + un is formed on the device. */
+int icf_transfer_nodes(icf_ctx *ctx, int n_nodes, const double *un,
+                       const double *vn, const double *an);
+
+/* ---- CZ damage state, TransferPCSR :374-413 ----------------------------- */
+/* Current pmax[n*3], tmax[n*3] and failed[n] of every CZ.  Failed CZs are
+ * skipped by the assembly (the reference drops them from nonFailedCZs). */
+int icf_transfer_cz_state(icf_ctx *ctx, int n_czs, const double *pmax,
+                          const double *tmax, const int *failed);
+
+/* ---- contact, NarrowPhaseCollisionDetection :539-616 -------------------- */
+/* pairs[n_pairs*2]: surface-element ids from the broad phase.  Runs the
+ * vertex-inclusion test, expands the masks into the set of (node, element)
+ * tuples (ascending by node, then element) and resolves each tuple to its
+ * closest adjacent face.  The impacts become part of the next structure. */
+int icf_narrow_phase(icf_ctx *ctx, int n_pairs, const int *pairs,
+                     int *n_impacts);
+/* impacts[n*4] = (node, face vertex 0, 1, 2), the c_itet rows of :611. */
+int icf_get_impacts(icf_ctx *ctx, int capacity, int *impacts);
+/* Supply an impact list directly (e.g. one read back with ReadImpacts). */
+int icf_set_impacts(icf_ctx *ctx, int n_impacts, const int *impacts);
+/* 8-bit inclusion masks of the last icf_narrow_phase call (kNarrowPhase_new
+ * output, narrowphase.h:91-154), one per pair. */
+int icf_get_narrow_masks(icf_ctx *ctx, int capacity, int *masks);
+
+/* ---- pattern, LinearSystem.CreateStructure :29-43 ------------------------ */
+/* Static pattern plus the contact pairs of the current impacts
+ * (ImplicitModel3.cs:177-196), columns ascending per row
+ * (CSRDictionary.cs:64-97).  Returns N (rows) and nnz (blocks). */
+int icf_create_structure(icf_ctx *ctx, int *N, int *nnz);
+/* csr_rows[N+1], csr_cols[nnz] (the ia/ja arrays handed to PARDISO). */
+int icf_get_structure(icf_ctx *ctx, int *csr_rows, int *csr_cols);
+/* Per-unit slot maps in the reference's logical layout (the pcsr part of
+ * g_ie_pcsr / g_icz / g_icr, GPU_Functionality.cs:355-368, 388-401,
+ * 645-662): kind 0 = elements (20 ints each: 16 slots i*4+j, 4 rows),
+ * kind 1 = CZs (42 ints: 36 slots i*6+j, 6 rows), kind 2 = impacts (20). */
+int icf_get_pcsr(icf_ctx *ctx, int kind, long long capacity, int *out);
+
+/* ---- assembly, AssembleElemsAndCZs :439-479 + collisionResponse :627-676 */
+/* Zero, element, CZ (with tentative damage state and flags) and contact
+ * contributions into the device BCSR values and rhs.  Synchronous. */
+int icf_assemble(icf_ctx *ctx, double h, icf_counts *counts);
+/* Same work, enqueued on the context stream without waiting; counters are
+ * read later with icf_read_counts.  Capturable in a CUDA graph once the
+ * pattern is built. */
+int icf_assemble_async(icf_ctx *ctx, double h);
+int icf_read_counts(icf_ctx *ctx, icf_counts *counts);
+
+/* ---- results ------------------------------------------------------------- */
+/* TransferLinearSystemToHost :481-485: vals[nnz*9], rhs[N*3] (either may be
+ * NULL). */
+int icf_transfer_linear_system(icf_ctx *ctx, double *vals, double *rhs);
+/* TransferUpdatedStateToHost :487-528: commits the tentative CZ state on the
+ * device (pmax, tmax <- tentative; failed |= tentatively failed) and copies
+ * it back; node_F[n_nodes*3] receives the elastic + contact forces of the
+ * last assembly.  Any output may be NULL. */
+int icf_transfer_updated_state(icf_ctx *ctx, double *pmax, double *tmax,
+                               int *failed, double *avg4, double *node_F);
+/* Tentative CZ results of the last assembly without committing:
+ * tent[n*2] = pmax_, tmax_; flags[n*3] = contact, damaged, failed;
+ * avg4[n*4] = avgDn, avgDt, avgTn, avgTt. */
+int icf_get_cz_tentative(icf_ctx *ctx, double *tent, int *flags, double *avg4);
+int icf_get_device_buffers(icf_ctx *ctx, icf_device_buffers *out);
+
+/* ---- Newmark kinematics on the device, Node.cs:62-97 --------------------- */
+/* Committed state u, v, a (n_nodes*3 each). */
+int icf_set_node_state(icf_ctx *ctx, int n_nodes, const double *u,
+                       const double *v, const double *a);
+int icf_get_node_state(icf_ctx *ctx, double *u, double *v, double *a,
+                       double *du);
+/* du for every node (the Newton increment accumulated so far). */
+int icf_set_du(icf_ctx *ctx, int n_nodes, const double *du);
+/* InferTentativeValues (Node.cs:89-97) for all nodes, then the device node
+ * state used by icf_assemble is updated, as icf_transfer_nodes would. */
+int icf_infer_tentative(icf_ctx *ctx, double h);
+/* _XtoDU (ImplicitModel3.cs:247-256): du += dx[altId] for active nodes;
+ * dx has N*3 entries.  Returns sum(dx^2) in *norm (NormOfDx). */
+int icf_add_dx(icf_ctx *ctx, const double *dx, double *norm);
+/* AcceptTentativeValues (Node.cs:62-77). */
+int icf_accept_tentative(icf_ctx *ctx, double h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,173 @@
+"""CUDA path vs the CPU oracle through the C ABI (needs a B200)."""
+import numpy as np
+import pytest
+
+from icflow_b200 import mesh as M
+from icflow_b200.gpu_functionality import GPU_Functionality
+from icflow_b200.model_prms import config_prms
+from tests.harness import (FP64_TOL, Oracle, compare, gpu_assemble, oracle_assemble,
+                           orc_prms_from, random_state, rowwise_rel, vec_rel)
+
+pytestmark = pytest.mark.gpu
+H = 1e-4
+
+
+@pytest.fixture(scope="module")
+def O():
+    return Oracle()
+
+
+def _gf(coll, prms):
+    gf = GPU_Functionality(0)
+    gf.prms = prms
+    gf.mc = coll
+    gf.SetConstants()
+    gf.TransferStaticDataToDevice()
+    return gf
+
+
+def _zeros_cz(coll):
+    nc = len(coll.czs)
+    return np.zeros((nc, 3)), np.zeros((nc, 3)), np.zeros(nc, np.int32)
+
+
+@pytest.mark.parametrize("seed,du", [(0, 1e-7), (1, 2e-6), (2, 8e-6), (3, 3e-5)])
+def test_cantilever_parity(O, seed, du):
+    coll = M.cantilever()
+    prms = config_prms()
+    gf = _gf(coll, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    state = random_state(coll, seed, du=du)
+    g = gpu_assemble(gf, coll, state, H, pmax, tmax, failed)
+    o = oracle_assemble(O, orc_prms_from(O, prms), coll, state, H, pmax, tmax, np.zeros((0, 4), np.int32))
+    compare(g, o)
+    assert g["counts"].nCZFailedThisStep == int(o["flags"][:, 2].sum())
+    assert g["counts"].nCZDamaged == int(o["flags"][:, 1].sum())
+    gf.close()
+
+
+def test_damaged_and_failed_state(O):
+    """Pre-damaged CZs (unload/reload branches), CZs committed as failed before
+    the pattern is built, and per-CZ strengths."""
+    coll = M.polycrystal(n=6, grains=6, seed=3, platens=False)
+    prms = config_prms()
+    p = orc_prms_from(O, prms)
+    rng = np.random.default_rng(5)
+    nc = len(coll.czs)
+    q = p.ppr
+    pmax = rng.random((nc, 3)) * q.deln * 0.3
+    tmax = rng.random((nc, 3)) * q.delt * 0.3
+    pmax[rng.random(nc) < 0.3] = 0
+    failed = (rng.random(nc) < 0.1).astype(np.int32)
+    sig = M.lognormal_strengths(nc, seed=2, granule_pairs=coll.meshes[0].cz_grains)
+    gf = _gf(coll, prms)
+    gf.SetCZStrengths(sig, sig)
+    state = random_state(coll, 9, du=2e-6)
+    g = gpu_assemble(gf, coll, state, H, pmax, tmax, failed)
+    live = failed == 0
+    o = oracle_assemble(O, p, coll, state, H, pmax, tmax, np.zeros((0, 4), np.int32),
+                        cz_sigma=(sig, sig), cz_live=live)
+    rep = compare(g, o)
+    assert rep["vals_rowwise"] <= FP64_TOL
+    gf.close()
+
+
+def test_contact_parity(O):
+    """Platens overlapping a small polycrystal: narrow-phase masks, the impact
+    set and the pattern with contact pairs are bit-exact; the assembled matrix
+    matches to 1e-12."""
+    coll = M.polycrystal(n=8, grains=8, seed=1, platens=True, gap=-0.3)
+    prms = config_prms(penaltyK=1e8)
+    p = orc_prms_from(O, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    state = random_state(coll, 4, du=1e-7)
+    xt = coll.x0 + state[0]
+    pairs = M.candidate_pairs(coll, xt)
+    assert len(pairs) > 0
+    gf = _gf(coll, prms)
+    g = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+    masks_g = gf.NarrowPhaseMasks(len(pairs))
+    masks_o = O.narrow_phase(pairs, coll.selem, xt)
+    assert np.array_equal(masks_g, masks_o)
+    imp_o = O.impacts(pairs, masks_o, coll.selem, coll.adj_off, coll.adj, coll.faces, xt)
+    assert len(imp_o) > 0
+    assert np.array_equal(gf.c_itet, imp_o)
+    o = oracle_assemble(O, p, coll, state, H, pmax, tmax, imp_o)
+    rep = compare(g, o)
+    assert g["counts"].nImpacts == len(imp_o)
+    gf.close()
+
+
+def test_deterministic(O):
+    coll = M.polycrystal(n=6, grains=5, seed=2, platens=True, gap=-0.3)
+    prms = config_prms(penaltyK=1e8)
+    gf = _gf(coll, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    state = random_state(coll, 1, du=1e-6)
+    pairs = M.candidate_pairs(coll, coll.x0 + state[0])
+    a = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+    b = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+    assert np.array_equal(a["vals"], b["vals"]) and np.array_equal(a["rhs"], b["rhs"])
+    gf.close()
+
+
+def test_node_forces_and_commit(O):
+    coll = M.cantilever()
+    prms = config_prms()
+    p = orc_prms_from(O, prms)
+    gf = _gf(coll, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    state = random_state(coll, 3, du=4e-6)
+    gpu_assemble(gf, coll, state, H, pmax, tmax, failed)
+    st = gf.TransferUpdatedStateToHost()
+    o = oracle_assemble(O, p, coll, state, H, pmax, tmax, np.zeros((0, 4), np.int32))
+    assert vec_rel(o["nodeF"], st["nodeF"]) <= FP64_TOL
+    assert np.array_equal(st["failed"], o["flags"][:, 2])
+    assert vec_rel(o["tent"][:, 0], st["pmax"][:, 0]) <= FP64_TOL
+    assert vec_rel(o["tent"][:, 1], st["tmax"][:, 2]) <= FP64_TOL
+    gf.close()
+
+
+def test_newmark_on_device(O):
+    coll = M.cantilever()
+    prms = config_prms()
+    gf = _gf(coll, prms)
+    rng = np.random.default_rng(0)
+    n = len(coll.x0)
+    u, v, a, du = (rng.random((n, 3)) - 0.5 for _ in range(4))
+    u *= 1e-4
+    du *= 1e-6
+    gf.SetNodeState(u, v, a)
+    gf.SetDU(du)
+    gf.InferTentativeValues(H)
+    un_o, vn_o, an_o, xt_o = O.newmark_infer(H, 0.25, 0.5, coll.x0, u, v, a, du)
+    gf.CreateStructure(copy_back=False)
+    dx = rng.random(3 * gf.linearSystem.N) - 0.5
+    nrm = gf.XtoDU(dx)
+    assert abs(nrm - float(dx @ dx)) <= 1e-13 * float(dx @ dx)
+    gf.AcceptTentativeValues(H)
+    u2, v2, a2, du2 = gf.GetNodeState()
+    uo, vo, ao, duo, _ = O.newmark_accept(H, coll.x0, u, v, a, un_o, du)
+    assert np.allclose(u2, uo, rtol=0, atol=1e-18) and np.array_equal(du2, np.zeros_like(du2))
+    assert vec_rel(vo, v2) <= 1e-12 and vec_rel(ao, a2) <= 1e-12
+    gf.close()
+
+
+def test_error_paths():
+    """Bad arguments are rejected on the host with an error code; nothing
+    reaches the GPU."""
+    from icflow_b200 import _lib
+
+    coll = M.cantilever()
+    gf = _gf(coll, config_prms())
+    lib = _lib.load()
+    assert lib.icf_assemble(gf.ctx, 1e-4, None) == _lib.ICF_ERR_STATE
+    bad = np.array([[0, 1, 2, 10 ** 7]], np.int32)
+    assert lib.icf_set_impacts(gf.ctx, 1, _lib.iptr(bad)) == _lib.ICF_ERR_ARG
+    assert b"out of range" in lib.icf_last_error(gf.ctx)
+    pairs = np.array([[0, 10 ** 7]], np.int32)
+    n = _lib.C.c_int()
+    assert lib.icf_narrow_phase(gf.ctx, 1, _lib.iptr(pairs), _lib.C.byref(n)) == _lib.ICF_ERR_ARG
+    gf.CreateStructure()
+    assert lib.icf_assemble(gf.ctx, -1.0, None) == _lib.ICF_ERR_ARG
+    gf.close()
