@@ -23,7 +23,8 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # Files whose integer outputs depend on floating-point comparisons are built
 # without fused multiply-add so that every operation rounds on its own.
 NO_FMA = {"icf_contact.cu"}
-SOURCES = ["icf_api.cu", "icf_assembly.cu", "icf_pattern.cu", "icf_contact.cu", "icf_mlp.cu"]
+SOURCES = ["icf_api.cu", "icf_assembly.cu", "icf_pattern.cu", "icf_contact.cu", "icf_contact_deriv.cu",
+           "icf_mlp.cu"]
 
 
 def nvcc() -> str:

@@ -193,7 +193,8 @@ static void free_all(icf_ctx *c) {
                   c->d_czs, c->d_czfail, c->d_cztent, c->d_czflags, c->d_czavg, c->d_czprm,
                   c->d_es, c->d_cs, c->d_ks, c->d_skeys, c->d_rc_off, c->d_rc, c->d_rows, c->d_cols,
                   c->d_src, c->d_mkeys, c->d_imp, c->d_cr_slot, c->d_cr_off, c->d_cr, c->d_pairs,
-                  c->d_masks, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
+                  c->d_masks, c->d_imp_ci, c->d_imp_cd, c->d_rc_mid, c->d_diag, c->d_offd,
+                  c->d_s2m, c->d_dynpos, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
                   c->imp_inc.off, c->imp_inc.inc, c->d_tmp};
   for (void *p : ptrs) cudaFree(p);
 }
@@ -222,6 +223,15 @@ int icf_set_constants(icf_ctx *ctx, const icf_params *p) {
     return icf_fail(ctx, ICF_ERR_ARG, "parameters give a degenerate PPR law or Newmark scheme");
   ctx->prm = q;
   ctx->have_prm = true;
+  // PPR axis factors at zero opening (the law's constant evaluations)
+  const double ax[2][4] = {{q.alpha, q.p_m, q.gam_n, q.pMnt}, {q.beta, q.p_n, q.gam_t, q.pMtn}};
+  for (int i = 0; i < 2; i++) {
+    const double a = ax[i][0], pp = ax[i][1], s = pp / a;
+    const double s0 = std::pow(s, pp), s1 = s0 / s, s2 = s1 / s;
+    ctx->axis0[3 * i + 0] = ax[i][2] * 1.0 * s0 + ax[i][3];
+    ctx->axis0[3 * i + 1] = (pp * 1.0 * s1) - (a * 1.0 * s0);
+    ctx->axis0[3 * i + 2] = (pp * pp - pp) * 1.0 * s2 + (a * a - a) * 1.0 * s0 - 2.0 * a * pp * 1.0 * s1;
+  }
   if (ctx->per_cz_prm) ctx->per_cz_prm = false;  // strengths must be set again
   return ICF_OK;
 }
@@ -302,7 +312,9 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->d_u = ctx->d_v = ctx->d_a = ctx->d_du = ctx->d_un = ctx->d_h3 = nullptr;
   ctx->d_czs = nullptr; ctx->d_czfail = nullptr; ctx->d_cztent = nullptr; ctx->d_czflags = nullptr;
   ctx->d_czavg = nullptr; ctx->d_czprm = nullptr; ctx->d_es = nullptr; ctx->d_cs = nullptr;
-  ctx->d_ks = nullptr; ctx->ks_cap = 0; ctx->d_skeys = nullptr; ctx->d_rc_off = nullptr; ctx->d_rc = nullptr;
+  ctx->d_ks = nullptr; ctx->ks_cap = 0; ctx->d_imp_ci = nullptr; ctx->d_imp_cd = nullptr;
+  ctx->d_rc_mid = ctx->d_diag = ctx->d_offd = nullptr; ctx->n_offd = 0;
+  ctx->d_s2m = ctx->d_dynpos = nullptr; ctx->s2m_cap = ctx->dynpos_cap = ctx->n_dyn = 0; ctx->d_skeys = nullptr; ctx->d_rc_off = nullptr; ctx->d_rc = nullptr;
   ctx->d_rows = ctx->d_cols = ctx->d_src = nullptr; ctx->rows_cap = ctx->cols_cap = 0; ctx->d_mkeys = nullptr;
   ctx->d_imp = nullptr; ctx->imp_cap = 0; ctx->n_imp = 0; ctx->d_cr_slot = ctx->d_cr_off = nullptr;
   ctx->d_cr = nullptr; ctx->cr_cap = 0; ctx->n_crs = 0; ctx->d_pairs = ctx->d_masks = nullptr;

@@ -4,17 +4,19 @@
 //   k_tet_unit    one thread per tetrahedron: corotational force, rotated
 //                 shape-function gradients and the Newmark rhs of each vertex
 //                 (element_kernels2.h:19-159 and :195-263) -> tet staging
-//   k_cz_unit     one thread per cohesive zone: mid-plane frame, PPR law at
-//                 three Gauss points, tentative damage state and flags
-//                 (cz_kernels.h:210-434) -> CZ staging
-//   k_imp_unit    one thread per impact (icf_contact.cu)
-//   k_gather      one thread per BCSR block: sums the contributions listed
-//                 for that block in the pattern's slot-sorted code list, then
-//                 writes the block once (and the rhs row for diagonal blocks)
+//   k_cz_gp       three threads per cohesive zone, one per Gauss point:
+//                 mid-plane frame, PPR law, then the Gauss points combine into
+//                 the CZ staging, tentative damage state and flags
+//                 (cz_kernels.h:210-434)
+//   k_imp_*       impacts (icf_contact.cu, icf_contact_deriv.cu)
+//   k_gather_*    one thread per BCSR block (diagonal blocks by row, then the
+//                 off-diagonal ones): sums the contributions listed for the
+//                 block in the pattern's slot-sorted code list and writes it
+//                 once (and the rhs row of a diagonal block)
 //   k_imp_add     adds impact contributions to the blocks they touch
-// Each block is written by exactly one thread in a fixed order, so the result
-// is bit-reproducible; the reference's CAS-loop atomics (atomic_add.h:1-13)
-// have no counterpart.
+// Each block is summed in a fixed order and written once, so the result is
+// bit-reproducible; the reference's CAS-loop atomics (atomic_add.h:1-13) have
+// no counterpart.
 #include "icf_internal.cuh"
 #include "icf_ppr.cuh"
 
@@ -68,7 +70,7 @@ __device__ __forceinline__ void frame3(const double p0[3], const double p1[3],
 // and the consistent mass is M_ab = rho/20 (1 + delta_ab) I.  The staging
 // record of vertex a is {h_a, V} and {rhs_a, 0}; k_gather rebuilds
 // LHS_ab = stiffCoeff Df_ab + massCoeff M_ab from it.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 3)
     k_tet_unit(int ne, const int4 *__restrict__ elem,
                const double4 *__restrict__ x0, const double4 *__restrict__ xc,
                const double2 *__restrict__ va, icf_dprm P,
@@ -235,91 +237,66 @@ __device__ __forceinline__ void cz_frame(const double m0[3], const double m1[3],
 //   Kt[i][j] = sum_gp sf[i][gp] sf[j][gp] Q_gp   (i <= j, symmetric 3x3: 6)
 //   rt[i]    = sum_gp sf[i][gp] (aJ/3) R^T T_gp  (3)
 // i.e. 36 + 9 doubles.
-__global__ void __launch_bounds__(128)
-    k_cz_unit(int nc, const int *__restrict__ cz, const double4 *__restrict__ xc,
-              const double *__restrict__ czs, const int *__restrict__ czfail,
-              const double4 *__restrict__ czprm, icf_dprm P,
-              double *__restrict__ cs, double *__restrict__ cztent,
-              int *__restrict__ czflags, double *__restrict__ czavg,
-              int *__restrict__ counts) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
-  double *st = cs + (size_t)c * ICF_CZ_STAGE;
-  int flag = 0;
-  if (__ldg(czfail + c)) {
-    for (int i = 0; i < ICF_CZ_STAGE; i++) st[i] = 0;
-    czflags[c] = 0;
-    return;
-  }
-  icf_ppr_c q;
-  q.alpha = P.alpha; q.beta = P.beta; q.p_m = P.p_m; q.p_n = P.p_n;
-  q.gam_n = P.gam_n; q.gam_t = P.gam_t; q.pMtn = P.pMtn; q.pMnt = P.pMnt;
-  q.rn = P.rn; q.rt = P.rt;
-  if (czprm) {
-    const double4 w = czprm[c];
-    q.f_tn = w.x; q.f_tt = w.y; q.deln = w.z; q.delt = w.w;
-  } else {
-    q.f_tn = P.f_tn; q.f_tt = P.f_tt; q.deln = P.deln; q.delt = P.delt;
-  }
+//
+// Three threads per CZ, one per Gauss point: each evaluates the frame, its
+// opening and the law; the three combine through shared memory in Gauss point
+// order 0, 1, 2 (the reference's accumulation order).
+constexpr int CZ_PER_BLOCK = 32;
+__global__ void __launch_bounds__(3 * CZ_PER_BLOCK)
+    k_cz_gp(int nc, const int *__restrict__ cz, const double4 *__restrict__ xc,
+            const double *__restrict__ czs, const int *__restrict__ czfail,
+            const double4 *__restrict__ czprm, icf_dprm P, icf_law_c LC,
+            double *__restrict__ cs, double *__restrict__ cztent, int *__restrict__ czflags,
+            double *__restrict__ czavg, int *__restrict__ counts) {
+  __shared__ double sQ[3 * CZ_PER_BLOCK][6];
+  __shared__ double sTw[3 * CZ_PER_BLOCK][3];
+  __shared__ double sAv[3 * CZ_PER_BLOCK][4];
+  __shared__ double sPT[3 * CZ_PER_BLOCK][2];
+  __shared__ int sFl[3 * CZ_PER_BLOCK];
+  __shared__ double sOut[CZ_PER_BLOCK * ICF_CZ_STAGE];
+  const int t = threadIdx.x;
+  const int j = t / 3, gp = t - 3 * j;
+  const int c = blockIdx.x * CZ_PER_BLOCK + j;
+  const bool live = c < nc && __ldg(czfail + c) == 0;
+  double deln = P.deln, delt = P.delt, f_tn = P.f_tn, f_tt = P.f_tt;
+  int fl = 0;
+  if (live) {
+    if (czprm) {
+      const double4 w = czprm[c];
+      f_tn = w.x; f_tt = w.y; deln = w.z; delt = w.w;
+    }
+    const int4 i0 = __ldg(reinterpret_cast<const int4 *>(cz) + 2 * c);
+    const int2 i1 = __ldg(reinterpret_cast<const int2 *>(cz) + 4 * c + 2);
+    const int nid[6] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y};
+    double x[6][3];
+#pragma unroll
+    for (int i = 0; i < 6; i++) ld_node(xc, nid[i], x[i]);
+    double pmax = __ldg(czs + 8 * (size_t)c + gp);
+    double tmax = __ldg(czs + 8 * (size_t)c + 3 + gp);
 
-  const int4 i0 = __ldg(reinterpret_cast<const int4 *>(cz) + 2 * c);
-  const int2 i1 = __ldg(reinterpret_cast<const int2 *>(cz) + 4 * c + 2);
-  const int nid[6] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y};
-  double x[6][3];
+    // mid-plane, its frame, local coordinates and the opening (:243-290)
+    double mp[3][3], R[3][3], aJ;
 #pragma unroll
-  for (int i = 0; i < 6; i++) ld_node(xc, nid[i], x[i]);
-  double pmax[3], tmax[3];
+    for (int i = 0; i < 3; i++)
 #pragma unroll
-  for (int i = 0; i < 3; i++) {
-    pmax[i] = __ldg(czs + 8 * (size_t)c + i);
-    tmax[i] = __ldg(czs + 8 * (size_t)c + 3 + i);
-  }
-
-  // mid-plane, its frame and local coordinates (:243-266)
-  double mp[3][3], R[3][3], aJ;
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int k = 0; k < 3; k++) mp[i][k] = mul(add(x[i][k], x[i + 3][k]), 0.5);
-  cz_frame(mp[0], mp[1], mp[2], R, aJ);
-  double xr[6][3];
-#pragma unroll
-  for (int n = 0; n < 6; n++)
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-      xr[n][k] = add(add(mul(x[n][0], R[k][0]), mul(x[n][1], R[k][1])), mul(x[n][2], R[k][2]));
-
-  double Kt[6][6], rt[3][3];
-#pragma unroll
-  for (int i = 0; i < 6; i++)
-#pragma unroll
-    for (int j = 0; j < 6; j++) Kt[i][j] = 0;
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) rt[i][j] = 0;
-  bool anyc = false, anyf = false;
-  double aDn = 0, aDt = 0, aTn = 0, aTt = 0;
-  const double cw = (1.0 / 3.0) * aJ;
-
-#pragma unroll 1
-  for (int gp = 0; gp < 3; gp++) {
+      for (int k = 0; k < 3; k++) mp[i][k] = mul(add(x[i][k], x[i + 3][k]), 0.5);
+    cz_frame(mp[0], mp[1], mp[2], R, aJ);
     double o[3] = {0, 0, 0};
 #pragma unroll
-    for (int n = 0; n < 3; n++)
+    for (int n = 0; n < 3; n++) {
+      const double sfn = P.sf[n * 3 + gp];
 #pragma unroll
-      for (int k = 0; k < 3; k++) o[k] = add(o[k], mul(sub(xr[n][k], xr[n + 3][k]), P.sf[n * 3 + gp]));
+      for (int k = 0; k < 3; k++) {
+        const double xa = add(add(mul(x[n][0], R[k][0]), mul(x[n][1], R[k][1])), mul(x[n][2], R[k][2]));
+        const double xb = add(add(mul(x[n + 3][0], R[k][0]), mul(x[n + 3][1], R[k][1])), mul(x[n + 3][2], R[k][2]));
+        o[k] = add(o[k], mul(sub(xa, xb), sfn));
+      }
+    }
     const double opn = o[2];
     const double opt = sqrt(add(mul(o[0], o[0]), mul(o[1], o[1])));
-    const icf_law Lw = icf_cz_law(q, pmax[gp], tmax[gp], opn, opt);
-    anyc |= Lw.contact;
-    anyf |= Lw.failed;
-    aDn += opn / 3;
-    aDt += opt / 3;
-    aTn += Lw.Tn / 3;
-    aTt += Lw.Tt / 3;
+    const icf_law Lw = icf_cz_law_axes(LC, f_tn, f_tt, deln, delt, pmax, tmax, opn, opt);
 
-    // local traction and tangent (:301-340); the tangent is symmetric
+    // local traction and its (symmetric) tangent (:301-340)
     double T[3], Td[3][3];
     if (opt < 1e-20) {
       T[0] = 0; T[1] = 0; T[2] = Lw.Tn;
@@ -341,77 +318,99 @@ __global__ void __launch_bounds__(128)
       Td[0][2] = Td[2][0] = Lw.Dnt * o[0] * io;
       Td[1][2] = Td[2][1] = Lw.Dnt * o[1] * io;
     }
-    // world-frame traction and tangent, weighted by aJ/3
-    double tw[3], TR[3][3], Q[6];
+    const double cw = (1.0 / 3.0) * aJ;
 #pragma unroll
-    for (int k = 0; k < 3; k++) tw[k] = cw * (R[0][k] * T[0] + R[1][k] * T[1] + R[2][k] * T[2]);
+    for (int k = 0; k < 3; k++) sTw[t][k] = cw * (R[0][k] * T[0] + R[1][k] * T[1] + R[2][k] * T[2]);
+    double TR[3][3];
 #pragma unroll
     for (int m = 0; m < 3; m++)
 #pragma unroll
       for (int l = 0; l < 3; l++) TR[m][l] = Td[m][0] * R[0][l] + Td[m][1] * R[1][l] + Td[m][2] * R[2][l];
-    {
-      int p = 0;
+    int p = 0;
 #pragma unroll
-      for (int k = 0; k < 3; k++)
+    for (int k = 0; k < 3; k++)
 #pragma unroll
-        for (int l = k; l < 3; l++)
-          Q[p++] = cw * (R[0][k] * TR[0][l] + R[1][k] * TR[1][l] + R[2][k] * TR[2][l]);
-    }
-    int pr = 0;
+      for (int l = k; l < 3; l++)
+        sQ[t][p++] = cw * (R[0][k] * TR[0][l] + R[1][k] * TR[1][l] + R[2][k] * TR[2][l]);
+    sAv[t][0] = opn;
+    sAv[t][1] = opt;
+    sAv[t][2] = Lw.Tn;
+    sAv[t][3] = Lw.Tt;
+    sPT[t][0] = pmax;
+    sPT[t][1] = tmax;
+    const bool dmg = pmax >= deln * LC.rn || tmax >= delt * LC.rt;
+    fl = (Lw.contact ? 1 : 0) | (Lw.failed ? 4 : 0) | (dmg ? 2 : 0);
+  }
+  sFl[t] = fl;
+  __syncthreads();
+
+  // combine the three Gauss points of CZ j; thread gp builds 16 of the 48 values
+  const int b3 = 3 * j;
+  const bool failed = live && (((sFl[b3] | sFl[b3 + 1] | sFl[b3 + 2]) & 4) != 0);
+  for (int v = 16 * gp; v < 16 * gp + 16; v++) {
+    double val = 0.0;
+    if (live && !failed) {
+      if (v < 36) {
+        const int pr = v / 6, comp = v - 6 * pr;
+        const int pi = pr < 3 ? 0 : (pr < 5 ? 1 : 2);
+        const int pj = pr < 3 ? pr : (pr < 5 ? pr - 2 : 2);
 #pragma unroll
-    for (int i = 0; i < 3; i++) {
-      const double si = P.sf[i * 3 + gp];
+        for (int g = 0; g < 3; g++) val += (P.sf[pi * 3 + g] * P.sf[pj * 3 + g]) * sQ[b3 + g][comp];
+      } else if (v < 45) {
+        const int i = (v - 36) / 3, k = (v - 36) - 3 * i;
 #pragma unroll
-      for (int k = 0; k < 3; k++) rt[i][k] += si * tw[k];
-#pragma unroll
-      for (int j = i; j < 3; j++, pr++) {
-        const double w = si * P.sf[j * 3 + gp];
-#pragma unroll
-        for (int t = 0; t < 6; t++) Kt[pr][t] += w * Q[t];
+        for (int g = 0; g < 3; g++) val += P.sf[i * 3 + g] * sTw[b3 + g][k];
       }
     }
+    sOut[j * ICF_CZ_STAGE + v] = val;
   }
-
-  double pm = fmax(fmax(pmax[0], pmax[1]), pmax[2]);
-  double tm = fmax(fmax(tmax[0], tmax[1]), tmax[2]);
-  bool damaged = false;
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-    if (pmax[i] >= q.deln * q.rn || tmax[i] >= q.delt * q.rt) damaged = true;
-  cztent[2 * (size_t)c] = pm;
-  cztent[2 * (size_t)c + 1] = tm;
-  flag = (anyc ? 1 : 0) | ((!anyf && damaged) ? 2 : 0) | (anyf ? 4 : 0);
-  czflags[c] = flag;
-  double4 *av = reinterpret_cast<double4 *>(czavg) + c;
-  if (anyf) {
-    *av = make_double4(0, 0, 0, 0);
-    for (int i = 0; i < ICF_CZ_STAGE; i++) st[i] = 0;
-  } else {
-    *av = make_double4(aDn, aDt, aTn, aTt);
-    double2 *s2 = reinterpret_cast<double2 *>(st);
-#pragma unroll
-    for (int p = 0; p < 6; p++) {
-      s2[3 * p + 0] = make_double2(Kt[p][0], Kt[p][1]);
-      s2[3 * p + 1] = make_double2(Kt[p][2], Kt[p][3]);
-      s2[3 * p + 2] = make_double2(Kt[p][4], Kt[p][5]);
-    }
-    s2[18] = make_double2(rt[0][0], rt[0][1]);
-    s2[19] = make_double2(rt[0][2], rt[1][0]);
-    s2[20] = make_double2(rt[1][1], rt[1][2]);
-    s2[21] = make_double2(rt[2][0], rt[2][1]);
-    s2[22] = make_double2(rt[2][2], 0.0);
-    s2[23] = make_double2(0.0, 0.0);
+  int flag = 0;
+  if (gp == 0 && live) {
+    const int f0 = sFl[b3], f1 = sFl[b3 + 1], f2 = sFl[b3 + 2];
+    const bool anyc = ((f0 | f1 | f2) & 1) != 0, damaged = ((f0 | f1 | f2) & 2) != 0;
+    flag = (anyc ? 1 : 0) | ((!failed && damaged) ? 2 : 0) | (failed ? 4 : 0);
+    czflags[c] = flag;
+    cztent[2 * (size_t)c] = fmax(fmax(sPT[b3][0], sPT[b3 + 1][0]), sPT[b3 + 2][0]);
+    cztent[2 * (size_t)c + 1] = fmax(fmax(sPT[b3][1], sPT[b3 + 1][1]), sPT[b3 + 2][1]);
+    double av[4] = {0, 0, 0, 0};
+    for (int g = 0; g < 3; g++)
+      for (int k = 0; k < 4; k++) av[k] += sAv[b3 + g][k] / 3;
+    reinterpret_cast<double4 *>(czavg)[c] =
+        failed ? make_double4(0, 0, 0, 0) : make_double4(av[0], av[1], av[2], av[3]);
+  } else if (gp == 0 && c < nc) {
+    czflags[c] = 0;
   }
+  __syncthreads();
+  // coalesced store of the block's staging records
+  const int c0 = blockIdx.x * CZ_PER_BLOCK;
+  const int nvals = min(CZ_PER_BLOCK, nc - c0) * ICF_CZ_STAGE;
+  double *dst = cs + (size_t)c0 * ICF_CZ_STAGE;
+  for (int i = t; i < nvals; i += 3 * CZ_PER_BLOCK) dst[i] = sOut[i];
   // counters (integer atomics: order-independent)
-  const unsigned full = __activemask();
-  const int dmg = __popc(__ballot_sync(full, (flag & 2) != 0));
-  const int fl = __popc(__ballot_sync(full, (flag & 4) != 0));
-  const int ct = __popc(__ballot_sync(full, (flag & 1) != 0));
-  if ((threadIdx.x & 31) == __ffs(full) - 1) {
-    if (dmg) atomicAdd(counts + 0, dmg);
-    if (fl) atomicAdd(counts + 1, fl);
-    if (ct) atomicAdd(counts + 2, ct);
+  if (t < 32) {
+    int dm = 0, fa = 0, ct = 0;
+    for (int jj = t; jj < CZ_PER_BLOCK; jj += 32) {
+      const int cc = c0 + jj;
+      if (cc >= nc) continue;
+      const int f0 = sFl[3 * jj], f1 = sFl[3 * jj + 1], f2 = sFl[3 * jj + 2];
+      const int o = f0 | f1 | f2;
+      const bool fl_ = (o & 4) != 0;
+      dm += (!fl_ && (o & 2)) ? 1 : 0;
+      fa += fl_ ? 1 : 0;
+      ct += (o & 1) ? 1 : 0;
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+      dm += __shfl_down_sync(0xffffffffu, dm, d);
+      fa += __shfl_down_sync(0xffffffffu, fa, d);
+      ct += __shfl_down_sync(0xffffffffu, ct, d);
+    }
+    if (t == 0) {
+      if (dm) atomicAdd(counts + 0, dm);
+      if (fa) atomicAdd(counts + 1, fa);
+      if (ct) atomicAdd(counts + 2, ct);
+    }
   }
+  (void)flag;
 }
 
 // ---- the gather ----------------------------------------------------------------
@@ -421,73 +420,105 @@ __device__ __forceinline__ int sym_pair(int i, int j) {
   return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
 }
 
-__global__ void __launch_bounds__(256)
-    k_gather(int nnz, const int *__restrict__ src, int identity,
-             const int *__restrict__ cols, const int *__restrict__ rc_off,
-             const uint32_t *__restrict__ rc, const double4 *__restrict__ es,
-             const double *__restrict__ cs, double sc, double mc, double lam,
-             double mu, double *__restrict__ vals, double *__restrict__ rhs) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nnz) return;
-  const int st = identity ? s : __ldg(src + s);
-  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  double r[3] = {0, 0, 0};
-  bool diag = false;
-  if (st >= 0) {
-    const int beg = __ldg(rc_off + st), end = __ldg(rc_off + st + 1);
-    for (int qi = beg; qi < end; qi++) {
-      const uint32_t code = __ldg(rc + qi);
-      if ((code >> 30) == ICF_KIND_TET) {
-        const uint32_t e = (code >> 4) & 0x3FFFFFFu, a = (code >> 2) & 3u, bb = code & 3u;
-        const double4 A = es[8 * (size_t)e + a];
-        const double4 Bv = es[8 * (size_t)e + bb];
-        const double V = A.w;
-        const double ha[3] = {A.x, A.y, A.z}, hb[3] = {Bv.x, Bv.y, Bv.z};
-        const double dot = ha[0] * hb[0] + ha[1] * hb[1] + ha[2] * hb[2];
-        const double c1 = sc * V * lam, c2 = sc * V * mu;
-        const double cd = c2 * dot + mc * V * (a == bb ? 2.0 : 1.0);
+// Contribution of one tet code to its block (and, for a diagonal block, to the
+// rhs row): LHS_ab = stiffCoeff Df_ab + massCoeff M_ab rebuilt from the
+// staging record (see k_tet_unit).
+__device__ __forceinline__ void add_tet(uint32_t code, const double4 *__restrict__ es, double sc,
+                                        double mc, double lam, double mu, double b[9], double r[3]) {
+  const uint32_t e = (code >> 4) & 0x3FFFFFFu, a = (code >> 2) & 3u, bb = code & 3u;
+  const double4 A = es[8 * (size_t)e + a];
+  const double4 Bv = es[8 * (size_t)e + bb];
+  const double V = A.w;
+  const double ha[3] = {A.x, A.y, A.z}, hb[3] = {Bv.x, Bv.y, Bv.z};
+  const double dot = ha[0] * hb[0] + ha[1] * hb[1] + ha[2] * hb[2];
+  const double c1 = sc * V * lam, c2 = sc * V * mu;
+  const double cd = c2 * dot + mc * V * (a == bb ? 2.0 : 1.0);
 #pragma unroll
-        for (int k = 0; k < 3; k++)
+  for (int k = 0; k < 3; k++)
 #pragma unroll
-          for (int l = 0; l < 3; l++)
-            b[3 * k + l] += c1 * ha[k] * hb[l] + c2 * hb[k] * ha[l] + (k == l ? cd : 0.0);
-        if (a == bb) {
-          const double4 Rr = es[8 * (size_t)e + 4 + a];
-          r[0] += Rr.x;
-          r[1] += Rr.y;
-          r[2] += Rr.z;
-          diag = true;
-        }
-      } else {
-        const uint32_t c = (code >> 6) & 0xFFFFFFu, a = (code >> 3) & 7u, bb = code & 7u;
-        const double *S = cs + (size_t)c * ICF_CZ_STAGE;
-        const int ia = a % 3, ib = bb % 3;
-        const double sg = ((a < 3) == (bb < 3)) ? 1.0 : -1.0;
-        const double2 *K2 = reinterpret_cast<const double2 *>(S + 6 * sym_pair(ia, ib));
-        const double2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
-        // symmetric 3x3: xx xy xz yy yz zz
-        b[0] += sg * k01.x; b[1] += sg * k01.y; b[2] += sg * k23.x;
-        b[3] += sg * k01.y; b[4] += sg * k23.y; b[5] += sg * k45.x;
-        b[6] += sg * k23.x; b[7] += sg * k45.x; b[8] += sg * k45.y;
-        if (a == bb) {
-          const double sa = (a < 3) ? -1.0 : 1.0;
-          r[0] += sa * __ldg(S + 36 + 3 * ia + 0);
-          r[1] += sa * __ldg(S + 36 + 3 * ia + 1);
-          r[2] += sa * __ldg(S + 36 + 3 * ia + 2);
-          diag = true;
-        }
-      }
-    }
+    for (int l = 0; l < 3; l++) b[3 * k + l] += c1 * ha[k] * hb[l] + c2 * hb[k] * ha[l] + (k == l ? cd : 0.0);
+  if (r != nullptr) {
+    const double4 Rr = es[8 * (size_t)e + 4 + a];
+    r[0] += Rr.x;
+    r[1] += Rr.y;
+    r[2] += Rr.z;
   }
-  double *o = vals + 9 * (size_t)s;
+}
+
+// Contribution of one CZ code: +-Kt[a mod 3][b mod 3] (symmetric 3x3) and,
+// for a diagonal block, -+rt[a mod 3].
+__device__ __forceinline__ void add_cz(uint32_t code, const double *__restrict__ cs, double b[9],
+                                       double r[3]) {
+  const uint32_t c = (code >> 6) & 0xFFFFFFu, a = (code >> 3) & 7u, bb = code & 7u;
+  const double *S = cs + (size_t)c * ICF_CZ_STAGE;
+  const int ia = a % 3, ib = bb % 3;
+  const double sg = ((a < 3) == (bb < 3)) ? 1.0 : -1.0;
+  const double2 *K2 = reinterpret_cast<const double2 *>(S + 6 * sym_pair(ia, ib));
+  const double2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
+  b[0] += sg * k01.x; b[1] += sg * k01.y; b[2] += sg * k23.x;
+  b[3] += sg * k01.y; b[4] += sg * k23.y; b[5] += sg * k45.x;
+  b[6] += sg * k23.x; b[7] += sg * k45.x; b[8] += sg * k45.y;
+  if (r != nullptr) {
+    const double sa = (a < 3) ? -1.0 : 1.0;
+    r[0] += sa * __ldg(S + 36 + 3 * ia + 0);
+    r[1] += sa * __ldg(S + 36 + 3 * ia + 1);
+    r[2] += sa * __ldg(S + 36 + 3 * ia + 2);
+  }
+}
+
+// Diagonal blocks: one thread per row.  Every code of a diagonal block has
+// a == b, so the rhs row is summed alongside.  Tet codes precede CZ codes in
+// each block's list; the two loops keep the kinds apart so lanes do not
+// diverge on the kind.
+__global__ void __launch_bounds__(128)
+    k_gather_diag(int N, const int *__restrict__ diag, const int *__restrict__ rc_off,
+                  const int *__restrict__ rc_mid, const uint32_t *__restrict__ rc,
+                  const int *__restrict__ s2m, int identity, const double4 *__restrict__ es,
+                  const double *__restrict__ cs, double sc, double mc, double lam, double mu,
+                  double *__restrict__ vals, double *__restrict__ rhs) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= N) return;
+  const int st = __ldg(diag + row);
+  if (st < 0) return;
+  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, r[3] = {0, 0, 0};
+  const int q0 = __ldg(rc_off + st), qm = __ldg(rc_mid + st), q1 = __ldg(rc_off + st + 1);
+  for (int q = q0; q < qm; q++) add_tet(__ldg(rc + q), es, sc, mc, lam, mu, b, r);
+  for (int q = qm; q < q1; q++) add_cz(__ldg(rc + q), cs, b, r);
+  const int pos = identity ? st : __ldg(s2m + st);
+  double *o = vals + 9 * (size_t)pos;
 #pragma unroll
   for (int k = 0; k < 9; k++) o[k] = b[k];
-  if (diag) {
-    const int row = __ldg(cols + s);
-    rhs[3 * (size_t)row + 0] = r[0];
-    rhs[3 * (size_t)row + 1] = r[1];
-    rhs[3 * (size_t)row + 2] = r[2];
-  }
+  rhs[3 * (size_t)row + 0] = r[0];
+  rhs[3 * (size_t)row + 1] = r[1];
+  rhs[3 * (size_t)row + 2] = r[2];
+}
+
+// Off-diagonal blocks: one thread per block of the compacted list, so the
+// lanes of a warp have lists of similar length (about three tets each).
+__global__ void __launch_bounds__(256)
+    k_gather_off(int n_off, const int *__restrict__ offd, const int *__restrict__ rc_off,
+                 const int *__restrict__ rc_mid, const uint32_t *__restrict__ rc,
+                 const int *__restrict__ s2m, int identity, const double4 *__restrict__ es,
+                 const double *__restrict__ cs, double sc, double mc, double lam, double mu,
+                 double *__restrict__ vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_off) return;
+  const int st = __ldg(offd + i);
+  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const int q0 = __ldg(rc_off + st), qm = __ldg(rc_mid + st), q1 = __ldg(rc_off + st + 1);
+  for (int q = q0; q < qm; q++) add_tet(__ldg(rc + q), es, sc, mc, lam, mu, b, nullptr);
+  for (int q = qm; q < q1; q++) add_cz(__ldg(rc + q), cs, b, nullptr);
+  const int pos = identity ? st : __ldg(s2m + st);
+  double *o = vals + 9 * (size_t)pos;
+#pragma unroll
+  for (int k = 0; k < 9; k++) o[k] = b[k];
+}
+
+// Blocks that only contact pairs create start at zero.
+__global__ void k_zero_dyn(int nd, const int *__restrict__ pos, double *__restrict__ vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 9 * nd) return;
+  vals[9 * (size_t)pos[i / 9] + (i % 9)] = 0.0;
 }
 
 // Impact contributions, one thread per block they touch (sorted by slot).
@@ -677,11 +708,18 @@ int icf_launch_assembly(icf_ctx *ctx, double h) {
   if (ctx->n_elem > 0)
     k_tet_unit<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0,
                                                           ctx->d_xc, ctx->d_va, P, ctx->d_es);
-  if (ctx->n_cz > 0)
-    k_cz_unit<<<icf_blocks(ctx->n_cz, 128), 128, 0, s>>>(
+  if (ctx->n_cz > 0) {
+    icf_law_c LC;
+    LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
+    LC.gam_n = P.gam_n; LC.gam_t = P.gam_t; LC.pMtn = P.pMtn; LC.pMnt = P.pMnt;
+    LC.rn = P.rn; LC.rt = P.rt;
+    LC.N0 = icf_axis{ctx->axis0[0], ctx->axis0[1], ctx->axis0[2]};
+    LC.T0 = icf_axis{ctx->axis0[3], ctx->axis0[4], ctx->axis0[5]};
+    k_cz_gp<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, s>>>(
         ctx->n_cz, ctx->d_cz, ctx->d_xc, ctx->d_czs, ctx->d_czfail,
-        ctx->per_cz_prm ? ctx->d_czprm : nullptr, P, ctx->d_cs, ctx->d_cztent, ctx->d_czflags,
+        ctx->per_cz_prm ? ctx->d_czprm : nullptr, P, LC, ctx->d_cs, ctx->d_cztent, ctx->d_czflags,
         ctx->d_czavg, ctx->d_counts);
+  }
   if (ctx->n_imp > 0) {
     const int rc = icf_launch_imp_unit(ctx);
     if (rc) return rc;
@@ -689,10 +727,17 @@ int icf_launch_assembly(icf_ctx *ctx, double h) {
   const double nb = ctx->prm.NewmarkBeta, ng = ctx->prm.NewmarkGamma;
   const double sc = 1.0 + ctx->prm.dampingStiffness * ng / (h * nb);
   const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
-  if (ctx->nnz > 0)
-    k_gather<<<icf_blocks(ctx->nnz, 256), 256, 0, s>>>(
-        ctx->nnz, ctx->d_src, ctx->src_identity ? 1 : 0, ctx->d_cols, ctx->d_rc_off, ctx->d_rc,
-        ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals, ctx->d_rhs);
+  const int ident = ctx->src_identity ? 1 : 0;
+  if (ctx->N > 0)
+    k_gather_diag<<<icf_blocks(ctx->N, 128), 128, 0, s>>>(
+        ctx->N, ctx->d_diag, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_rc, ctx->d_s2m, ident, ctx->d_es,
+        ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals, ctx->d_rhs);
+  if (ctx->n_offd > 0)
+    k_gather_off<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(
+        ctx->n_offd, ctx->d_offd, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_rc, ctx->d_s2m, ident, ctx->d_es,
+        ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals);
+  if (ctx->n_dyn > 0)
+    k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, s>>>(ctx->n_dyn, ctx->d_dynpos, ctx->d_vals);
   if (ctx->n_crs > 0)
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off,
                                                         ctx->d_cr, ctx->d_cols, ctx->d_ks,

@@ -11,9 +11,10 @@
 //                 done on the device as keys (node << 32 | element)
 //   k_closest     kFindClosestFace (narrowphase.h:159-201) with dtn
 //                 (dist_node2tri.h:14-129)
-//   k_imp_unit    kCollisionResponseForce (collision_response.h:38-127) with
-//                 the point-triangle distance derivatives pt()
-//                 (point_triange_v2.h:13-841)
+//   k_imp_classify  the decision part of kCollisionResponseForce
+//                 (collision_response.h:38-91): Voronoi region of pt()
+//                 (point_triange_v2.h:589-841), barycentrics and distance;
+//                 the derivatives follow in icf_contact_deriv.cu
 #include <cub/cub.cuh>
 
 #include "icf_internal.cuh"
@@ -181,28 +182,40 @@ __global__ void k_closest(int n, const unsigned long long *__restrict__ keys,
   imp[i] = make_int4(node, faces[3 * best], faces[3 * best + 1], faces[3 * best + 2]);
 }
 
-// ---- point-triangle distance with first and second derivatives ----------------------
-// x = (p, v0, v1, v2).  Vertex-vertex: |x_a - x_b|^2.
-__device__ double pt_vv(const double x[12], int ia, int ib, double fd[12], double sd[144]) {
+// ---- point-triangle classification -------------------------------------------------
+// The Voronoi region of pt (point_triange_v2.h:589-841), its barycentric
+// coordinates (s, t) and the squared distance, evaluated exactly as the CPU
+// checker does.  The derivatives are computed separately (icf_contact_deriv.cu)
+// once the region is known.  x = (p, v0, v1, v2); kind 0 = interior (plane),
+// 1 = vertex (block ib), 2 = edge (blocks ia, ib, nearer endpoint first).
+struct pt_cls {
+  int kind, ia, ib;
+  double s, t, dsq;
+};
+
+__device__ double vv_dsq(const double x[12], int ia, int ib) {
   double dsq = 0;
   for (int k = 0; k < 3; k++) {
     const double d = x[3 * ia + k] - x[3 * ib + k];
-    fd[3 * ia + k] = 2 * d;
-    fd[3 * ib + k] = -(2 * d);
-    sd[(3 * ia + k) * 12 + 3 * ia + k] = 2;
-    sd[(3 * ib + k) * 12 + 3 * ib + k] = 2;
-    sd[(3 * ia + k) * 12 + 3 * ib + k] = -2;
-    sd[(3 * ib + k) * 12 + 3 * ia + k] = -2;
     dsq += d * d;
   }
   return dsq;
 }
 
-// Point y[0..2] to the line (y[3..5], y[6..8]): dist^2 = f1 - g / f2 with
-// f1 = |q1-p|^2, g = ((q1-p).(q2-q1))^2, f2 = |q2-q1|^2
-// (vertex_edge_distance_and_derivs, point_triange_v2.h:152-232).
-__device__ double pt_line(const double y[9], double fd[9], double sd[81]) {
-  const double *P = y, *Q1 = y + 3, *Q2 = y + 6;
+// distance to the line through the edge, nearer endpoint first
+// (vertex_edge_distance_and_derivs_12, :237-294, and :152-177)
+__device__ double ve_dsq(const double x[12], int &ia, int &ib) {
+  double da = 0, db = 0;
+  for (int k = 0; k < 3; k++) {
+    da += (x[k] - x[3 * ia + k]) * (x[k] - x[3 * ia + k]);
+    db += (x[k] - x[3 * ib + k]) * (x[k] - x[3 * ib + k]);
+  }
+  if (da > db) {
+    const int s = ia;
+    ia = ib;
+    ib = s;
+  }
+  const double *P = x, *Q1 = x + 3 * ia, *Q2 = x + 3 * ib;
   double el2 = 0, rde = 0;
   for (int k = 0; k < 3; k++) {
     el2 += (Q2[k] - Q1[k]) * (Q2[k] - Q1[k]);
@@ -214,207 +227,12 @@ __device__ double pt_line(const double y[9], double fd[9], double sd[81]) {
     const double d = P[k] - u * Q1[k] - t * Q2[k];
     dist2 += d * d;
   }
-  double sp = 0, spd[9];
-  for (int k = 0; k < 3; k++) {
-    spd[k] = Q1[k] - Q2[k];
-    spd[3 + k] = P[k] - 2 * Q1[k] + Q2[k];
-    spd[6 + k] = Q1[k] - P[k];
-    sp += (Q1[k] - P[k]) * (Q2[k] - Q1[k]);
-  }
-  // second derivatives of sp: -2 on (q1,q1), -1 on (p,q2), +1 on (p,q1), (q2,q1)
-  auto spdd = [](int i, int j) -> double {
-    if (i % 3 != j % 3) return 0.0;
-    const int bi = i / 3, bj = j / 3;
-    if (bi == 1 && bj == 1) return -2.0;
-    if ((bi == 0 && bj == 2) || (bi == 2 && bj == 0)) return -1.0;
-    if ((bi == 0 && bj == 1) || (bi == 1 && bj == 0) || (bi == 2 && bj == 1) || (bi == 1 && bj == 2))
-      return 1.0;
-    return 0.0;
-  };
-  const double g = sp * sp;
-  double gd[9], f1d[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, f2d[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  double f2 = 0;
-  for (int i = 0; i < 9; i++) gd[i] = 2 * sp * spd[i];
-  for (int k = 0; k < 3; k++) {
-    const double a = Q1[k] - P[k], b = Q2[k] - Q1[k];
-    f2 += b * b;
-    f1d[3 + k] = 2 * a;
-    f1d[k] = -(2 * a);
-    f2d[6 + k] = 2 * b;
-    f2d[3 + k] = -(2 * b);
-  }
-  auto f1dd = [](int i, int j) -> double {
-    if (i % 3 != j % 3) return 0.0;
-    const int bi = i / 3, bj = j / 3;
-    if (bi == 2 || bj == 2) return 0.0;
-    return bi == bj ? 2.0 : -2.0;
-  };
-  auto f2dd = [](int i, int j) -> double {
-    if (i % 3 != j % 3) return 0.0;
-    const int bi = i / 3, bj = j / 3;
-    if (bi == 0 || bj == 0) return 0.0;
-    return bi == bj ? 2.0 : -2.0;
-  };
-  const double f2sq = f2 * f2, f2cu = f2sq * f2;
-  for (int i = 0; i < 9; i++) {
-    fd[i] = f1d[i] + (g * f2d[i] - f2 * gd[i]) / f2sq;
-    for (int j = 0; j < 9; j++) {
-      const double gdd = 2 * (spd[i] * spd[j] + sp * spdd(i, j));
-      const double t1 = -2 * g * f2d[i] * f2d[j] / f2cu;
-      const double t2 = (gd[i] * f2d[j] + gd[j] * f2d[i]) / f2sq;
-      const double t3 = f1dd(i, j);
-      const double t4 = g * f2dd(i, j) / f2sq;
-      const double t5 = -gdd / f2;
-      sd[i * 9 + j] = t1 + t2 + t3 + t4 + t5;
-    }
-  }
   return dist2;
 }
 
-// Point to the edge (ia, ib) of x[12]; the nearer endpoint is the origin.
-__device__ double pt_ve(const double x[12], int ia, int ib, double fd[12], double sd[144]) {
-  double da = 0, db = 0;
-  for (int k = 0; k < 3; k++) {
-    da += (x[k] - x[3 * ia + k]) * (x[k] - x[3 * ia + k]);
-    db += (x[k] - x[3 * ib + k]) * (x[k] - x[3 * ib + k]);
-  }
-  if (da > db) {
-    const int s = ia;
-    ia = ib;
-    ib = s;
-  }
-  double y[9], yd[9], ydd[81];
-  const int blk[3] = {0, ia, ib};
-  for (int b = 0; b < 3; b++)
-    for (int k = 0; k < 3; k++) y[3 * b + k] = x[3 * blk[b] + k];
-  const double r = pt_line(y, yd, ydd);
-  for (int bi = 0; bi < 3; bi++)
-    for (int k = 0; k < 3; k++) {
-      fd[3 * blk[bi] + k] = yd[3 * bi + k];
-      for (int bj = 0; bj < 3; bj++)
-        for (int l = 0; l < 3; l++)
-          sd[(3 * blk[bi] + k) * 12 + 3 * blk[bj] + l] = ydd[(3 * bi + k) * 9 + 3 * bj + l];
-    }
-  return r;
-}
-
-// Interior region: |q|^2 with q = s v1 + t v2 + (1-s-t) v0 - p and the
-// barycentric foot point s(x), t(x) of the plane (point_plane_distance,
-// point_triange_v2.h:449-582).  The gradients of a..e come from their
-// bilinear structure (a = e0.e0, b = e0.e1, c = e1.e1, d = e0.w, e = e1.w;
-// e0 = v1-v0, e1 = v2-v0, w = v0-p); their Hessians are multiples of the
-// identity per 3x3 block.
-struct sel {
-  int bp, bn;  // +x[block bp] - x[block bn]
-};
-__device__ void bil(sel A, sel C, const double ax[3], const double cx[3], double g[12],
-                    double H[4][4]) {
-  for (int i = 0; i < 12; i++) g[i] = 0;
-  for (int i = 0; i < 4; i++)
-    for (int j = 0; j < 4; j++) H[i][j] = 0;
-  for (int k = 0; k < 3; k++) {
-    g[3 * A.bp + k] += cx[k];
-    g[3 * A.bn + k] -= cx[k];
-    g[3 * C.bp + k] += ax[k];
-    g[3 * C.bn + k] -= ax[k];
-  }
-  const int ab[2] = {A.bp, A.bn}, cb[2] = {C.bp, C.bn};
-  const double sg[2] = {1.0, -1.0};
-  for (int i = 0; i < 2; i++)
-    for (int j = 0; j < 2; j++) {
-      H[ab[i]][cb[j]] += sg[i] * sg[j];
-      H[cb[j]][ab[i]] += sg[i] * sg[j];
-    }
-}
-
-__device__ double pt_plane(const double x[12], double fd[12], double sd[144]) {
-  const double *P = x, *V0 = x + 3, *V1 = x + 6, *V2 = x + 9;
-  double e0[3], e1[3], w[3];
-  for (int k = 0; k < 3; k++) {
-    e0[k] = -V0[k] + V1[k];
-    e1[k] = -V0[k] + V2[k];
-    w[k] = -P[k] + V0[k];
-  }
-  const double a = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
-  const double b = e1[1] * e0[1] + e1[2] * e0[2] + e0[0] * e1[0];
-  const double c = e1[1] * e1[1] + e1[2] * e1[2] + e1[0] * e1[0];
-  const double d = w[0] * e0[0] + w[1] * e0[1] + w[2] * e0[2];
-  const double e = e1[1] * w[1] + e1[2] * w[2] + w[0] * e1[0];
-  const double det = a * c - b * b, det2 = det * det, det3 = det2 * det;
-  const double inv = 1. / det;
-  const double s = (b * e - c * d) * inv, t = (b * d - a * e) * inv;
-  const double u = 1 - (s + t);
-  double q[3], dist2 = 0;
-  for (int k = 0; k < 3; k++) {
-    q[k] = -P[k] + V1[k] * s + V2[k] * t + V0[k] * u;
-    dist2 += q[k] * q[k];
-  }
-  const sel E0 = {2, 1}, E1 = {3, 1}, W = {1, 0};
-  double ag[12], bg[12], cg[12], dg[12], eg[12];
-  double aH[4][4], bH[4][4], cH[4][4], dH[4][4], eH[4][4];
-  bil(E0, E0, e0, e0, ag, aH);
-  bil(E0, E1, e0, e1, bg, bH);
-  bil(E1, E1, e1, e1, cg, cH);
-  bil(E0, W, e0, w, dg, dH);
-  bil(E1, W, e1, w, eg, eH);
-  double s1[12], t1[12], u1[12], det1[12], J[3][12];
-  for (int i = 0; i < 12; i++) {
-    det1[i] = c * ag[i] + a * cg[i] - 2 * b * bg[i];
-    s1[i] = ((c * d - b * e) * det1[i]) / det2 + ((e * bg[i] + b * eg[i]) - (d * cg[i] + c * dg[i])) / det;
-    t1[i] = ((a * e - b * d) * det1[i]) / det2 + ((d * bg[i] + b * dg[i]) - (a * eg[i] + e * ag[i])) / det;
-    u1[i] = -(s1[i] + t1[i]);
-  }
-  for (int k = 0; k < 3; k++)
-    for (int i = 0; i < 12; i++) {
-      double v = V1[k] * s1[i] + V2[k] * t1[i] + V0[k] * u1[i];
-      if (i == k) v -= 1;
-      if (i == 3 + k) v += u;
-      if (i == 6 + k) v += s;
-      if (i == 9 + k) v += t;
-      J[k][i] = v;
-    }
-  for (int i = 0; i < 12; i++) fd[i] = 2 * (q[0] * J[0][i] + q[1] * J[1][i] + q[2] * J[2][i]);
-  const double sN = -(c * d) + b * e, tN = b * d - a * e;
-  for (int i = 0; i < 12; i++)
-    for (int j = 0; j < 12; j++) {
-      const bool same = (i % 3) == (j % 3);
-      const int bi = i / 3, bj = j / 3;
-      const double a2 = same ? aH[bi][bj] : 0, b2 = same ? bH[bi][bj] : 0;
-      const double c2 = same ? cH[bi][bj] : 0, d2 = same ? dH[bi][bj] : 0;
-      const double e2 = same ? eH[bi][bj] : 0;
-      const double dt2 = -2 * bg[i] * bg[j] + ag[j] * cg[i] + ag[i] * cg[j] + c * a2 - 2 * b * b2 + a * c2;
-      const double s2 =
-          (-(cg[j] * dg[i]) - cg[i] * dg[j] + bg[j] * eg[i] + bg[i] * eg[j] + e * b2 - d * c2 - c * d2 + b * e2) / det -
-          ((det1[j] * (e * bg[i] - d * cg[i] - c * dg[i] + b * eg[i])) +
-           (det1[i] * (e * bg[j] - d * cg[j] - c * dg[j] + b * eg[j])) + (sN * dt2)) / det2 +
-          (2 * sN * det1[i] * det1[j]) / det3;
-      const double t2 =
-          (bg[j] * dg[i] + bg[i] * dg[j] - ag[j] * eg[i] - ag[i] * eg[j] - e * a2 + d * b2 + b * d2 - a * e2) / det -
-          ((det1[j] * (-(e * ag[i]) + d * bg[i] + b * dg[i] - a * eg[i])) +
-           (det1[i] * (-(e * ag[j]) + d * bg[j] + b * dg[j] - a * eg[j])) + (tN * dt2)) / det2 +
-          (2 * tN * det1[i] * det1[j]) / det3;
-      const double u2 = -(s2 + t2);
-      double acc = 0;
-      for (int k = 0; k < 3; k++) {
-        double q2 = V1[k] * s2 + V2[k] * t2 + V0[k] * u2;
-        if (i == 3 + k) q2 += u1[j];
-        if (j == 3 + k) q2 += u1[i];
-        if (i == 6 + k) q2 += s1[j];
-        if (j == 6 + k) q2 += s1[i];
-        if (i == 9 + k) q2 += t1[j];
-        if (j == 9 + k) q2 += t1[i];
-        acc += J[k][i] * J[k][j] + q[k] * q2;
-      }
-      sd[i * 12 + j] = 2 * acc;
-    }
-  return dist2;
-}
-
-// pt (point_triange_v2.h:589-841): Voronoi region of the closest feature.
-__device__ double pt(const double x[12], double fd[12], double sd[144], double &s_out,
-                     double &t_out) {
-  for (int i = 0; i < 12; i++) fd[i] = 0;
-  for (int i = 0; i < 144; i++) sd[i] = 0;
+// squared distance to the plane through the barycentric foot point
+// (point_plane_distance, :449-492)
+__device__ double plane_dsq(const double x[12]) {
   const double *P = x, *V0 = x + 3, *V1 = x + 6, *V2 = x + 9;
   double e0[3], e1[3], w[3];
   for (int k = 0; k < 3; k++) {
@@ -428,114 +246,143 @@ __device__ double pt(const double x[12], double fd[12], double sd[144], double &
   const double d = w[0] * e0[0] + w[1] * e0[1] + w[2] * e0[2];
   const double e = e1[1] * w[1] + e1[2] * w[2] + w[0] * e1[0];
   const double det = a * c - b * b;
-  double s = b * e - c * d, t = b * d - a * e, r;
+  const double inv = 1. / det;
+  const double s = (b * e - c * d) * inv, t = (b * d - a * e) * inv;
+  const double u = 1 - (s + t);
+  double dist2 = 0;
+  for (int k = 0; k < 3; k++) {
+    const double q = -P[k] + V1[k] * s + V2[k] * t + V0[k] * u;
+    dist2 += q * q;
+  }
+  return dist2;
+}
+
+__device__ pt_cls pt_classify(const double x[12]) {
+  pt_cls r;
+  r.ia = r.ib = 0;
+  const double *P = x, *V0 = x + 3, *V1 = x + 6, *V2 = x + 9;
+  double e0[3], e1[3], w[3];
+  for (int k = 0; k < 3; k++) {
+    e0[k] = -V0[k] + V1[k];
+    e1[k] = -V0[k] + V2[k];
+    w[k] = -P[k] + V0[k];
+  }
+  const double a = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
+  const double b = e1[1] * e0[1] + e1[2] * e0[2] + e0[0] * e1[0];
+  const double c = e1[1] * e1[1] + e1[2] * e1[2] + e1[0] * e1[0];
+  const double d = w[0] * e0[0] + w[1] * e0[1] + w[2] * e0[2];
+  const double e = e1[1] * w[1] + e1[2] * w[2] + w[0] * e1[0];
+  const double det = a * c - b * b;
+  double s = b * e - c * d, t = b * d - a * e;
+  // vertex / edge selectors: vertex k = block k; edge (i, j) as passed by pt
+#define VV(k) do { r.kind = 1; r.ib = (k); r.dsq = vv_dsq(x, 0, (k)); } while (0)
+#define VE(i, j) do { r.kind = 2; r.ia = (i); r.ib = (j); r.dsq = ve_dsq(x, r.ia, r.ib); } while (0)
   if (s + t <= det) {
     if (s < 0) {
       if (t < 0 && d < 0) {
         t = 0;
-        if (-d >= a) { s = 1; r = pt_vv(x, 0, 2, fd, sd); }
-        else { s = -d / a; r = pt_ve(x, 2, 1, fd, sd); }
+        if (-d >= a) { s = 1; VV(2); }
+        else { s = -d / a; VE(2, 1); }
       } else {
         s = 0;
-        if (e >= 0) { t = 0; r = pt_vv(x, 0, 1, fd, sd); }
-        else if (-e >= c) { t = 1; r = pt_vv(x, 0, 3, fd, sd); }
-        else { t = -e / c; r = pt_ve(x, 3, 1, fd, sd); }
+        if (e >= 0) { t = 0; VV(1); }
+        else if (-e >= c) { t = 1; VV(3); }
+        else { t = -e / c; VE(3, 1); }
       }
     } else if (t < 0) {
       t = 0;
-      if (d >= 0) { s = 0; r = pt_vv(x, 0, 1, fd, sd); }
-      else if (-d >= a) { s = 1; r = pt_vv(x, 0, 2, fd, sd); }
-      else { s = -d / a; r = pt_ve(x, 1, 2, fd, sd); }
+      if (d >= 0) { s = 0; VV(1); }
+      else if (-d >= a) { s = 1; VV(2); }
+      else { s = -d / a; VE(1, 2); }
     } else {
       const double inv = (1) / det;
       s *= inv;
       t *= inv;
-      r = pt_plane(x, fd, sd);
+      r.kind = 0;
+      r.dsq = plane_dsq(x);
     }
   } else {
     if (s < 0) {
       const double t0 = b + d, t1 = c + e;
       if (t1 > t0) {
         const double num = t1 - t0, den = a - 2 * b + c;
-        if (num >= den) { s = 1; t = 0; r = pt_vv(x, 0, 2, fd, sd); }
-        else { s = num / den; t = 1 - s; r = pt_ve(x, 2, 3, fd, sd); }
+        if (num >= den) { s = 1; t = 0; VV(2); }
+        else { s = num / den; t = 1 - s; VE(2, 3); }
       } else {
         s = 0;
-        if (t1 <= 0) { t = 1; r = pt_vv(x, 0, 3, fd, sd); }
-        else if (e >= 0) { t = 0; r = pt_vv(x, 0, 1, fd, sd); }
-        else { t = -e / c; r = pt_ve(x, 1, 3, fd, sd); }
+        if (t1 <= 0) { t = 1; VV(3); }
+        else if (e >= 0) { t = 0; VV(1); }
+        else { t = -e / c; VE(1, 3); }
       }
     } else if (t < 0) {
       const double t0 = b + e, t1 = a + d;
       if (t1 > t0) {
         const double num = t1 - t0, den = a - 2 * b + c;
-        if (num >= den) { t = 1; s = 0; r = pt_vv(x, 0, 3, fd, sd); }
-        else { t = num / den; s = 1 - t; r = pt_ve(x, 2, 3, fd, sd); }
+        if (num >= den) { t = 1; s = 0; VV(3); }
+        else { t = num / den; s = 1 - t; VE(2, 3); }
       } else {
         t = 0;
-        if (t1 <= 0) { s = 1; r = pt_vv(x, 0, 2, fd, sd); }
-        else if (d >= 0) { s = 0; r = pt_vv(x, 0, 1, fd, sd); }
-        else { s = -d / a; r = pt_ve(x, 1, 2, fd, sd); }
+        if (t1 <= 0) { s = 1; VV(2); }
+        else if (d >= 0) { s = 0; VV(1); }
+        else { s = -d / a; VE(1, 2); }
       }
     } else {
       const double num = c + e - b - d;
-      if (num <= 0) { s = 0; t = 1; r = pt_vv(x, 0, 3, fd, sd); }
+      if (num <= 0) { s = 0; t = 1; VV(3); }
       else {
         const double den = a - 2 * b + c;
-        if (num >= den) { s = 1; t = 0; r = pt_vv(x, 0, 2, fd, sd); }
-        else { s = num / den; t = 1 - s; r = pt_ve(x, 2, 3, fd, sd); }
+        if (num >= den) { s = 1; t = 0; VV(2); }
+        else { s = num / den; t = 1 - s; VE(2, 3); }
       }
     }
   }
-  s_out = s;
-  t_out = t;
+#undef VV
+#undef VE
+  r.s = s;
+  r.t = t;
   return r;
 }
 
-// Penalty response of one impact: staging = 12x12 LHS then the 12 rhs.
-__global__ void __launch_bounds__(64)
-    k_imp_unit(int n, const int4 *__restrict__ imp, const int *__restrict__ alt,
-               const double4 *__restrict__ xc, double k, double eps2,
-               double *__restrict__ ks, int *__restrict__ counts) {
+// One thread per impact: region, barycentrics, distance and whether the
+// impact produces a response (kCollisionResponseForce, :47-51 and :91).
+__global__ void k_imp_classify(int n, const int4 *__restrict__ imp, const int *__restrict__ alt,
+                               const double4 *__restrict__ xc, double eps2,
+                               int4 *__restrict__ cls_i, double4 *__restrict__ cls_d,
+                               int *__restrict__ counts) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= n) return;
-  double *K = ks + (size_t)u * ICF_IMP_STAGE;
   const int4 id = imp[u];
   const int nid[4] = {id.x, id.y, id.z, id.w};
-  bool any_active = false;
-  for (int i = 0; i < 4; i++) any_active |= (nid[i] >= 0 && alt[nid[i]] >= 0);
-  double x[12];
-  bool ok = any_active && id.y >= 0;
-  if (ok)
-    for (int i = 0; i < 4; i++) {
-      const double4 p = xc[nid[i]];
-      x[3 * i] = p.x; x[3 * i + 1] = p.y; x[3 * i + 2] = p.z;
-    }
-  double fd[12], sd[144], s = 0, t = 0, dsq = 0;
-  if (ok) dsq = pt(x, fd, sd, s, t);
-  if (!ok || !(dsq > eps2)) {
-    for (int i = 0; i < ICF_IMP_STAGE; i++) K[i] = 0;
+  bool any_active = false, valid = true;
+  for (int i = 0; i < 4; i++) {
+    valid &= nid[i] >= 0;
+    any_active |= (nid[i] >= 0 && alt[nid[i]] >= 0);
+  }
+  if (!valid || !any_active) {
+    cls_i[u] = make_int4(-1, 0, 0, 0);
+    cls_d[u] = make_double4(0, 0, 0, 0);
     return;
   }
-  const double w[3] = {1 - (s + t), s, t};
-  const double F[3] = {k * 0.5 * fd[0], k * 0.5 * fd[1], k * 0.5 * fd[2]};
-  for (int i = 0; i < 12; i++)
-    for (int j = i; j < 12; j++) K[i * 12 + j] = K[j * 12 + i] = k * sd[i * 12 + j] / 2;
-  for (int c = 0; c < 3; c++) {
-    K[144 + c] = -F[c];
-    for (int v = 0; v < 3; v++) K[144 + 3 + 3 * v + c] = w[v] * F[c];
+  double x[12];
+  for (int i = 0; i < 4; i++) {
+    const double4 p = xc[nid[i]];
+    x[3 * i] = p.x; x[3 * i + 1] = p.y; x[3 * i + 2] = p.z;
   }
-  atomicAdd(counts + 3, 1);
+  const pt_cls r = pt_classify(x);
+  const bool active = r.dsq > eps2;
+  cls_i[u] = make_int4(active ? r.kind : -1, r.ia, r.ib, 0);
+  cls_d[u] = make_double4(r.s, r.t, r.dsq, 0.0);
+  if (active) atomicAdd(counts + 3, 1);
 }
 
 }  // namespace
 
 int icf_launch_imp_unit(icf_ctx *ctx) {
-  k_imp_unit<<<icf_blocks(ctx->n_imp, 64), 64, 0, ctx->stream>>>(
-      ctx->n_imp, ctx->d_imp, ctx->d_alt, ctx->d_xc, ctx->prm.penaltyK,
-      ctx->prm.DistanceEpsilon * ctx->prm.DistanceEpsilon, ctx->d_ks, ctx->d_counts);
+  k_imp_classify<<<icf_blocks(ctx->n_imp, 128), 128, 0, ctx->stream>>>(
+      ctx->n_imp, ctx->d_imp, ctx->d_alt, ctx->d_xc, ctx->prm.DistanceEpsilon * ctx->prm.DistanceEpsilon,
+      ctx->d_imp_ci, ctx->d_imp_cd, ctx->d_counts);
   ICF_CUDA(ctx, cudaGetLastError());
-  return ICF_OK;
+  return icf_launch_imp_deriv(ctx, ctx->d_imp_ci, ctx->d_imp_cd);
 }
 
 // Narrow phase + set expansion + closest face.  Leaves ctx->d_imp /

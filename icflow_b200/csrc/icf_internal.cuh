@@ -74,6 +74,8 @@ struct icf_ctx {
   std::string err;
   icf_params prm{};
   bool have_prm = false;
+  // PPR axis factors (f, d, dd) at zero opening: normal then tangential
+  double axis0[6] = {0, 0, 0, 0, 0, 0};
   int precision = ICF_FP64;
 
   // sizes
@@ -120,6 +122,15 @@ struct icf_ctx {
   int *d_rc_off = nullptr;
   uint32_t *d_rc = nullptr;
 
+  // gather metadata of the static pattern: start of the CZ codes per slot,
+  // diagonal slot per row (-1 if none), compacted off-diagonal slots
+  int *d_rc_mid = nullptr, *d_diag = nullptr, *d_offd = nullptr;
+  int n_offd = 0;
+  // static -> merged slot (when contact pairs add blocks) and the merged
+  // positions of the contact-only blocks
+  int *d_s2m = nullptr, *d_dynpos = nullptr;
+  int s2m_cap = 0, dynpos_cap = 0, n_dyn = 0;
+
   // merged pattern
   int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;
   int rows_cap = 0, cols_cap = 0;
@@ -128,6 +139,10 @@ struct icf_ctx {
   // impacts and their contributions
   int n_imp = 0, imp_cap = 0;
   int4 *d_imp = nullptr;
+  // per-impact classification {kind, ia, ib, 0} and {s, t, dsq, 0}; same
+  // capacity as the impact staging d_ks (ks_cap)
+  int4 *d_imp_ci = nullptr;
+  double4 *d_imp_cd = nullptr;
   int n_crs = 0;                  // slots touched by impacts
   int *d_cr_slot = nullptr, *d_cr_off = nullptr;
   uint32_t *d_cr = nullptr;
@@ -187,4 +202,5 @@ int icf_launch_add_dx(icf_ctx *ctx, const double *d_dx);
 int icf_launch_accept(icf_ctx *ctx, double h);
 int icf_launch_commit_cz(icf_ctx *ctx);
 int icf_launch_imp_unit(icf_ctx *ctx);
+int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d);
 int icf_get_node_inc(icf_ctx *ctx, icf_node_inc *tets, icf_node_inc *imps);

@@ -133,22 +133,50 @@ __global__ void k_dyn_new(int n, const unsigned long long *__restrict__ dkey,
 
 __global__ void k_merge_static(int nnz_s, const unsigned long long *__restrict__ skey,
                                const unsigned long long *__restrict__ dkey, int nd,
-                               unsigned long long *__restrict__ mkey, int *__restrict__ src) {
+                               unsigned long long *__restrict__ mkey, int *__restrict__ src,
+                               int *__restrict__ s2m) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nnz_s) return;
   const long long p = i + lower_bound_u64(dkey, nd, skey[i]);
   mkey[p] = skey[i];
   src[p] = i;
+  s2m[i] = (int)p;
 }
 
 __global__ void k_merge_dyn(int nd, const unsigned long long *__restrict__ dkey,
                             const unsigned long long *__restrict__ skey, int nnz_s,
-                            unsigned long long *__restrict__ mkey, int *__restrict__ src) {
+                            unsigned long long *__restrict__ mkey, int *__restrict__ src,
+                            int *__restrict__ dynpos) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nd) return;
   const long long p = j + lower_bound_u64(skey, nnz_s, dkey[j]);
   mkey[p] = dkey[j];
   src[p] = -1;
+  dynpos[j] = (int)p;
+}
+
+// Per static slot: where its CZ codes start (tet codes come first in the
+// stable order), and whether it is a diagonal block.  Diagonal slots are
+// listed per row, off-diagonal slots are flagged for compaction.
+__global__ void k_slot_meta(int nnz_s, const unsigned long long *__restrict__ skey,
+                            const int *__restrict__ rc_off, const uint32_t *__restrict__ rc,
+                            int *__restrict__ rc_mid, int *__restrict__ diag_of_row,
+                            int *__restrict__ offflag) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nnz_s) return;
+  const int b = rc_off[s], e = rc_off[s + 1];
+  int m = b;
+  while (m < e && (rc[m] >> 30) == ICF_KIND_TET) m++;
+  rc_mid[s] = m;
+  const unsigned long long k = skey[s];
+  const int row = (int)(k >> 32), col = (int)(k & 0xffffffffull);
+  if (row == col) diag_of_row[row] = s;
+  offflag[s] = row != col;
+}
+
+__global__ void k_iota(int n, int *__restrict__ a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
 }
 
 // impact contributions keyed by their merged slot
@@ -374,6 +402,38 @@ int icf_build_static_pattern(icf_ctx *ctx) {
   ctx->nnz_s = nnz_s;
   ctx->n_rc = nv;
   ctx->N = nnz_s > 0 ? (int)(last >> 32) + 1 : 0;
+
+  // gather metadata: CZ-code start per slot, diagonal slot per row, the
+  // compacted list of off-diagonal slots
+  const int N = ctx->N;
+  cudaFree(ctx->d_rc_mid);
+  cudaFree(ctx->d_diag);
+  cudaFree(ctx->d_offd);
+  ctx->d_rc_mid = ctx->d_diag = ctx->d_offd = nullptr;
+  ICF_CUDA(ctx, cudaMalloc(&ctx->d_rc_mid, sizeof(int) * (size_t)(nnz_s + 1)));
+  ICF_CUDA(ctx, cudaMalloc(&ctx->d_diag, sizeof(int) * (size_t)(N + 1)));
+  ICF_CUDA(ctx, cudaMalloc(&ctx->d_offd, sizeof(int) * (size_t)(nnz_s + 1)));
+  ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_diag, 0xff, sizeof(int) * (size_t)(N + 1), s));
+  ctx->n_offd = 0;
+  if (nnz_s > 0) {
+    int *offflag, *iota, *d_n;
+    ICF_CUDA(ctx, cudaMallocAsync(&offflag, sizeof(int) * nnz_s, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&iota, sizeof(int) * nnz_s, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&d_n, sizeof(int), s));
+    k_slot_meta<<<icf_blocks(nnz_s, 256), 256, 0, s>>>(nnz_s, ctx->d_skeys, ctx->d_rc_off, ctx->d_rc,
+                                                      ctx->d_rc_mid, ctx->d_diag, offflag);
+    k_iota<<<icf_blocks(nnz_s, 256), 256, 0, s>>>(nnz_s, iota);
+    ICF_CUDA(ctx, cudaGetLastError());
+    size_t tb = 0;
+    cub::DeviceSelect::Flagged(nullptr, tb, iota, offflag, ctx->d_offd, d_n, nnz_s, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceSelect::Flagged(ctx->d_tmp, tb, iota, offflag, ctx->d_offd, d_n, nnz_s, s));
+    ICF_CUDA(ctx, cudaMemcpyAsync(&ctx->n_offd, d_n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaFreeAsync(offflag, s));
+    ICF_CUDA(ctx, cudaFreeAsync(iota, s));
+    ICF_CUDA(ctx, cudaFreeAsync(d_n, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  }
   return ICF_OK;
 }
 
@@ -450,12 +510,27 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
                                   cudaMemcpyDeviceToDevice, s));
     ctx->src_identity = true;
   } else {
+    // static -> merged positions and the positions of the contact-only blocks
+    if (!ctx->d_s2m || ctx->s2m_cap < nnz_s + 1) {
+      cudaFree(ctx->d_s2m);
+      ctx->d_s2m = nullptr;
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_s2m, sizeof(int) * (size_t)(nnz_s + 1)));
+      ctx->s2m_cap = nnz_s + 1;
+    }
+    if (!ctx->d_dynpos || ctx->dynpos_cap < nd) {
+      cudaFree(ctx->d_dynpos);
+      ctx->d_dynpos = nullptr;
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_dynpos, sizeof(int) * (size_t)(2 * nd)));
+      ctx->dynpos_cap = 2 * nd;
+    }
     if (nnz_s > 0)
       k_merge_static<<<icf_blocks(nnz_s, 256), 256, 0, s>>>(nnz_s, ctx->d_skeys, dkeys, nd, ctx->d_mkeys,
-                                                           ctx->d_src);
-    k_merge_dyn<<<icf_blocks(nd, 256), 256, 0, s>>>(nd, dkeys, ctx->d_skeys, nnz_s, ctx->d_mkeys, ctx->d_src);
+                                                           ctx->d_src, ctx->d_s2m);
+    k_merge_dyn<<<icf_blocks(nd, 256), 256, 0, s>>>(nd, dkeys, ctx->d_skeys, nnz_s, ctx->d_mkeys, ctx->d_src,
+                                                   ctx->d_dynpos);
     ctx->src_identity = false;
   }
+  ctx->n_dyn = nd;
   if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
   if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
   k_rows<<<icf_blocks((long long)N + 1, 256), 256, 0, s>>>(N, nnz, ctx->d_mkeys, ctx->d_rows);
@@ -519,9 +594,16 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
     // impact staging
     if (ctx->n_imp > ctx->ks_cap) {
       cudaFree(ctx->d_ks);
+      cudaFree(ctx->d_imp_ci);
+      cudaFree(ctx->d_imp_cd);
       ctx->d_ks = nullptr;
-      ICF_CUDA(ctx, cudaMalloc(&ctx->d_ks, sizeof(double) * ICF_IMP_STAGE * (size_t)(2 * ctx->n_imp)));
-      ctx->ks_cap = 2 * ctx->n_imp;
+      ctx->d_imp_ci = nullptr;
+      ctx->d_imp_cd = nullptr;
+      const size_t cap = 2 * (size_t)ctx->n_imp;
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_ks, sizeof(double) * ICF_IMP_STAGE * cap));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_imp_ci, sizeof(int4) * cap));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_imp_cd, sizeof(double4) * cap));
+      ctx->ks_cap = (int)cap;
     }
   }
   // outputs

@@ -98,6 +98,159 @@ struct icf_law {
   bool contact, failed;
 };
 
+// ---- axis form of the law -------------------------------------------------------
+// Every PPR function is a product of one factor per axis (PPR_math.h:2-57):
+//   Tn  = (gam_n/deln)        dN(xn)  fT(xt)      Tt  = (gam_t/delt)        dT(xt)  fN(xn)
+//   Dnn = (gam_n/deln^2)      ddN(xn) fT(xt)      Dtt = (gam_t/delt^2)      ddT(xt) fN(xn)
+//   Dnt = (gam_n gam_t/(deln delt)) dN(xn) dT(xt)
+// with, for the normal axis (alpha, p_m; the tangential one uses beta, p_n),
+//   fN  = gam_n (1-x)^a (p/a+x)^p + <phi_n - phi_t>
+//   dN  = p (1-x)^a (p/a+x)^(p-1) - a (1-x)^(a-1) (p/a+x)^p
+//   ddN = (p^2-p)(1-x)^a (p/a+x)^(p-2) + (a^2-a)(1-x)^(a-2)(p/a+x)^p
+//         - 2 a p (1-x)^(a-1) (p/a+x)^(p-1).
+// The law only ever evaluates an axis at the current opening, at the
+// historical maximum, or at zero, so each Gauss point needs at most four axis
+// evaluations (the zero ones are constants).  (1-x)^(a-k) and (p/a+x)^(p-k)
+// come from one pow each and exact divisions by (1-x) and (p/a+x).
+struct icf_axis {
+  double f, d, dd;
+};
+
+__device__ __forceinline__ icf_axis icf_axis_eval(double a, double p, double gam, double mac,
+                                                  double x) {
+  const double o = 1.0 - x, s = (p / a) + x;
+  double o0, o1, o2;
+  if (o > 0) {
+    o0 = pow(o, a);
+    o1 = o0 / o;
+    o2 = o1 / o;
+  } else {
+    o0 = pow(o, a);
+    o1 = pow(o, a - 1.0);
+    o2 = pow(o, a - 2.0);
+  }
+  const double s0 = pow(s, p), s1 = s0 / s, s2 = s1 / s;
+  icf_axis r;
+  r.f = gam * o0 * s0 + mac;
+  r.d = (p * o0 * s1) - (a * o1 * s0);
+  r.dd = (p * p - p) * o0 * s2 + (a * a - a) * o2 * s0 - 2.0 * a * p * o1 * s1;
+  return r;
+}
+
+struct icf_law_c {
+  double alpha, beta, p_m, p_n, gam_n, gam_t, pMtn, pMnt, rn, rt;
+  icf_axis N0, T0;  // axes at zero opening
+};
+
+// cohesive_law_thermodynamically_consistent (cz_kernels.h:37-174) on the axis
+// factors; pmax and tmax are updated in place.
+__device__ inline icf_law icf_cz_law_axes(const icf_law_c &C, double f_tn, double f_tt,
+                                          double deln, double delt, double &pmax,
+                                          double &tmax, double opn, double opt) {
+  icf_law L;
+  L.Tn = L.Tt = L.Dnn = L.Dtt = L.Dnt = 0;
+  L.contact = false;
+  L.failed = false;
+  if (opn > deln || opt > delt) {
+    L.failed = true;
+    return L;
+  }
+  const double cN = C.gam_n / deln, cT = C.gam_t / delt;
+  const double cNN = C.gam_n / (deln * deln), cTT = C.gam_t / (delt * delt);
+  const double cNT = C.gam_n * C.gam_t / (deln * delt);
+  L.contact = (opn < 0);
+  const double eps_neg = -1e-9;
+  const double thr_t = f_tt * 0.05, thr_n = f_tn * 0.05;
+  const icf_axis Np = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, pmax / deln);
+  const icf_axis Tm = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, tmax / delt);
+  const icf_axis To = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, opt / delt);
+  if (L.contact) {
+    if (pmax != 0) {
+      const double peak = cN * Np.d * Tm.f;           // Tn_(pmax, tmax)
+      L.Tn = peak * opn / pmax;
+      L.Dnn = peak / pmax;
+    } else {
+      L.Dnn = cNN * C.N0.dd * Tm.f;                   // Dnn_(0, tmax)
+      L.Tn = L.Dnn * opn;
+    }
+    L.Tt = cT * To.d * C.N0.f;                        // Tt_(0, opt)
+    if (L.Tt >= eps_neg && !(opt > delt * C.rt / 5 && L.Tt < thr_t)) {
+      if (opt >= tmax) {
+        tmax = opt;
+        L.Dtt = cTT * To.dd * C.N0.f;                 // Dtt_(0, opt)
+      } else {
+        const double peak = cT * Tm.d * C.N0.f;       // Tt_(0, tmax)
+        L.Tt = peak * opt / tmax;
+        L.Dtt = peak / tmax;
+      }
+    } else {
+      L.Tt = L.Dtt = L.Dnt = 0;
+      L.Tn = L.Dnn = 0;
+      L.failed = true;
+    }
+    return L;
+  }
+  const icf_axis No = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, opn / deln);
+  L.Tt = cT * To.d * No.f;                            // Tt_(opn, opt)
+  L.Tn = cN * No.d * To.f;                            // Tn_(opn, opt)
+  if (L.Tt >= eps_neg && L.Tn >= eps_neg && !(opt > delt * C.rt / 5 && L.Tt < thr_t) &&
+      !(opn > deln * C.rn / 5 && L.Tn < thr_n)) {
+    const bool tsoft = (opt >= tmax), nsoft = (opn >= pmax);
+    if (tsoft && nsoft) {
+      tmax = opt;
+      pmax = opn;
+      L.Dnn = cNN * No.dd * To.f;
+      L.Dnt = cNT * No.d * To.d;
+      L.Dtt = cTT * To.dd * No.f;
+    } else if (tsoft && !nsoft) {
+      if (pmax != 0) {
+        const double peak = cN * Np.d * Tm.f;         // Tn_(pmax, tmax)
+        L.Tn = peak * opn / pmax;
+        L.Dnn = peak / pmax;
+      } else {
+        L.Tn = 0;
+        L.Dnn = cNN * C.N0.dd * Tm.f;                 // Dnn_(0, tmax)
+      }
+      tmax = opt;
+      L.Tt = cT * To.d * Np.f;                        // Tt_(pmax, opt)
+      L.Dtt = cTT * To.dd * Np.f;                     // Dtt_(pmax, opt)
+    } else if (!tsoft && nsoft) {
+      if (tmax != 0) {
+        const double peak = cT * Tm.d * Np.f;         // Tt_(pmax, tmax)
+        L.Tt = peak * opt / tmax;
+        L.Dtt = peak / tmax;
+      } else {
+        L.Tt = 0;
+        L.Dtt = cTT * C.T0.dd * Np.f;                 // Dtt_(pmax, 0)
+      }
+      pmax = opn;
+      L.Tn = cN * No.d * Tm.f;                        // Tn_(opn, tmax)
+      L.Dnn = cNN * No.dd * Tm.f;                     // Dnn_(opn, tmax)
+    } else {
+      const double peakN = cN * Np.d * Tm.f;          // Tn_(pmax, tmax)
+      if (pmax != 0) {
+        L.Tn = peakN * opn / pmax;
+        L.Dnn = peakN / pmax;
+      } else {
+        L.Tn = 0;
+        L.Dnn = cNN * C.N0.dd * Tm.f;                 // Dnn_(0, tmax)
+      }
+      if (tmax != 0) {
+        const double peakT = cT * Tm.d * Np.f;        // Tt_(pmax, tmax)
+        L.Tt = peakT * opt / tmax;
+        L.Dtt = peakT / tmax;
+      } else {
+        L.Tt = 0;
+        L.Dtt = cTT * C.T0.dd * Np.f;                 // Dtt_(pmax, 0)
+      }
+    }
+  } else {
+    L.failed = true;
+    L.Tn = L.Tt = L.Dnn = L.Dtt = L.Dnt = 0;
+  }
+  return L;
+}
+
 // cohesive_law_thermodynamically_consistent (cz_kernels.h:37-174); pmax and
 // tmax are updated in place.
 __device__ inline icf_law icf_cz_law(const icf_ppr_c &q, double &pmax,
