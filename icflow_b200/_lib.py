@@ -100,6 +100,7 @@ SIGNATURES = {
     "icf_get_pcsr": (I, [P, I, C.c_longlong, ip]),
     "icf_assemble": (I, [P, D, C.POINTER(icf_counts)]),
     "icf_assemble_async": (I, [P, D]),
+    "icf_set_graph": (I, [P, I]),
     "icf_read_counts": (I, [P, C.POINTER(icf_counts)]),
     "icf_transfer_linear_system": (I, [P, dp, dp]),
     "icf_transfer_updated_state": (I, [P, dp, dp, ip, dp, dp]),

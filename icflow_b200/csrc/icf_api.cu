@@ -173,7 +173,10 @@ int icf_create(int device, icf_ctx **out) {
   icf_ctx *ctx = new (std::nothrow) icf_ctx();
   if (!ctx) return ICF_ERR_SIZE;
   ctx->device = device;
-  if (cudaSetDevice(device) != cudaSuccess ||
+  bool ok = cudaSetDevice(device) == cudaSuccess;
+  for (int i = 0; ok && i < 2; i++) ok = cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking) == cudaSuccess;
+  for (int i = 0; ok && i < 5; i++) ok = cudaEventCreateWithFlags(&ctx->ev[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok ||
       cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&ctx->d_counts, 8 * sizeof(int)) != cudaSuccess ||
       cudaMallocHost(&ctx->h_counts, 8 * sizeof(int)) != cudaSuccess ||
@@ -194,7 +197,7 @@ static void free_all(icf_ctx *c) {
                   c->d_es, c->d_cs, c->d_ks, c->d_skeys, c->d_rc_off, c->d_rc, c->d_rows, c->d_cols,
                   c->d_src, c->d_mkeys, c->d_imp, c->d_cr_slot, c->d_cr_off, c->d_cr, c->d_pairs,
                   c->d_masks, c->d_imp_ci, c->d_imp_cd, c->d_rc_mid, c->d_diag, c->d_offd,
-                  c->d_s2m, c->d_dynpos, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
+                  c->d_s2m, c->d_dynpos, c->d_gdesc_diag, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
                   c->imp_inc.off, c->imp_inc.inc, c->d_tmp};
   for (void *p : ptrs) cudaFree(p);
 }
@@ -203,6 +206,11 @@ int icf_destroy(icf_ctx *ctx) {
   if (!ctx) return ICF_ERR_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  for (int i = 0; i < 2; i++)
+    if (ctx->aux[i]) cudaStreamDestroy(ctx->aux[i]);
+  for (int i = 0; i < 5; i++)
+    if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   free_all(ctx);
   cudaFree(ctx->d_counts);
   cudaFree(ctx->d_norm);
@@ -223,6 +231,7 @@ int icf_set_constants(icf_ctx *ctx, const icf_params *p) {
     return icf_fail(ctx, ICF_ERR_ARG, "parameters give a degenerate PPR law or Newmark scheme");
   ctx->prm = q;
   ctx->have_prm = true;
+  ctx->version++;
   // PPR axis factors at zero opening (the law's constant evaluations)
   const double ax[2][4] = {{q.alpha, q.p_m, q.gam_n, q.pMnt}, {q.beta, q.p_n, q.gam_t, q.pMtn}};
   for (int i = 0; i < 2; i++) {
@@ -241,6 +250,7 @@ int icf_set_precision(icf_ctx *ctx, int precision) {
   if (precision != ICF_FP64 && precision != ICF_FP32_MIXED)
     return icf_fail(ctx, ICF_ERR_ARG, "unknown precision");
   ctx->precision = precision;
+  ctx->version++;
   return ICF_OK;
 }
 
@@ -248,6 +258,7 @@ int icf_set_cz_strength(icf_ctx *ctx, int n_czs, const double *sigma_max, const 
   ICF_CHECK_CTX(ctx);
   if (!ctx->have_prm) return icf_fail(ctx, ICF_ERR_STATE, "icf_set_constants first");
   if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  ctx->version++;
   if (!sigma_max || !tau_max) {
     ctx->per_cz_prm = false;
     return ICF_OK;
@@ -314,7 +325,8 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->d_czavg = nullptr; ctx->d_czprm = nullptr; ctx->d_es = nullptr; ctx->d_cs = nullptr;
   ctx->d_ks = nullptr; ctx->ks_cap = 0; ctx->d_imp_ci = nullptr; ctx->d_imp_cd = nullptr;
   ctx->d_rc_mid = ctx->d_diag = ctx->d_offd = nullptr; ctx->n_offd = 0;
-  ctx->d_s2m = ctx->d_dynpos = nullptr; ctx->s2m_cap = ctx->dynpos_cap = ctx->n_dyn = 0; ctx->d_skeys = nullptr; ctx->d_rc_off = nullptr; ctx->d_rc = nullptr;
+  ctx->d_s2m = ctx->d_dynpos = nullptr; ctx->s2m_cap = ctx->dynpos_cap = ctx->n_dyn = 0;
+  ctx->d_gdesc_diag = ctx->d_gdesc_off = nullptr; ctx->gdesc_cap = 0; ctx->d_skeys = nullptr; ctx->d_rc_off = nullptr; ctx->d_rc = nullptr;
   ctx->d_rows = ctx->d_cols = ctx->d_src = nullptr; ctx->rows_cap = ctx->cols_cap = 0; ctx->d_mkeys = nullptr;
   ctx->d_imp = nullptr; ctx->imp_cap = 0; ctx->n_imp = 0; ctx->d_cr_slot = ctx->d_cr_off = nullptr;
   ctx->d_cr = nullptr; ctx->cr_cap = 0; ctx->n_crs = 0; ctx->d_pairs = ctx->d_masks = nullptr;
@@ -392,6 +404,7 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
     ICF_CUDA(ctx, cudaMemcpy(ctx->d_faces, faces, sizeof(int) * 3 * (size_t)n_faces, cudaMemcpyHostToDevice));
   }
   ctx->have_static = true;
+  ctx->version++;
   return ICF_OK;
 }
 
@@ -495,6 +508,7 @@ int icf_create_structure(icf_ctx *ctx, int *N, int *nnz) {
   if (!ctx->d_skeys) ICF_TRY(icf_build_static_pattern(ctx));
   ICF_TRY(icf_build_merged_pattern(ctx));
   ctx->have_structure = true;
+  ctx->version++;
   if (N) *N = ctx->N;
   if (nnz) *nnz = ctx->nnz;
   return ICF_OK;
@@ -538,6 +552,12 @@ int icf_assemble_async(icf_ctx *ctx, double h) {
   if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
   if (!(h > 0) || !std::isfinite(h)) return icf_fail(ctx, ICF_ERR_ARG, "time step must be positive");
   return icf_launch_assembly(ctx, h);
+}
+
+int icf_set_graph(icf_ctx *ctx, int enable) {
+  ICF_CHECK_CTX(ctx);
+  ctx->use_graph = enable != 0;
+  return ICF_OK;
 }
 
 int icf_read_counts(icf_ctx *ctx, icf_counts *c) {

@@ -466,50 +466,66 @@ __device__ __forceinline__ void add_cz(uint32_t code, const double *__restrict__
   }
 }
 
-// Diagonal blocks: one thread per row.  Every code of a diagonal block has
-// a == b, so the rhs row is summed alongside.  Tet codes precede CZ codes in
-// each block's list; the two loops keep the kinds apart so lanes do not
-// diverge on the kind.
+// Diagonal blocks: four threads per row, each summing every fourth code of the
+// row's diagonal block, combined by a fixed shuffle tree.  Every code of a
+// diagonal block has a == b, so the rhs row is summed alongside.  Tet codes
+// precede CZ codes in each block's list; the two loops keep the kinds apart
+// so lanes do not diverge on the kind.
 __global__ void __launch_bounds__(128)
-    k_gather_diag(int N, const int *__restrict__ diag, const int *__restrict__ rc_off,
-                  const int *__restrict__ rc_mid, const uint32_t *__restrict__ rc,
-                  const int *__restrict__ s2m, int identity, const double4 *__restrict__ es,
-                  const double *__restrict__ cs, double sc, double mc, double lam, double mu,
-                  double *__restrict__ vals, double *__restrict__ rhs) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= N) return;
-  const int st = __ldg(diag + row);
-  if (st < 0) return;
+    k_gather_diag(int N, const int4 *__restrict__ desc, const uint32_t *__restrict__ rc,
+                  const double4 *__restrict__ es, const double *__restrict__ cs, double sc,
+                  double mc, double lam, double mu, double *__restrict__ vals,
+                  double *__restrict__ rhs) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = t >> 2, sub = t & 3;
+  const int4 d = row < N ? desc[row] : make_int4(-1, 0, 0, 0);
   double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, r[3] = {0, 0, 0};
-  const int q0 = __ldg(rc_off + st), qm = __ldg(rc_mid + st), q1 = __ldg(rc_off + st + 1);
-  for (int q = q0; q < qm; q++) add_tet(__ldg(rc + q), es, sc, mc, lam, mu, b, r);
-  for (int q = qm; q < q1; q++) add_cz(__ldg(rc + q), cs, b, r);
-  const int pos = identity ? st : __ldg(s2m + st);
-  double *o = vals + 9 * (size_t)pos;
+  if (d.x >= 0) {
+    for (int q = d.y + sub; q < d.z; q += 4) add_tet(__ldg(rc + q), es, sc, mc, lam, mu, b, r);
+    for (int q = d.z + sub; q < d.w; q += 4) add_cz(__ldg(rc + q), cs, b, r);
+  }
 #pragma unroll
-  for (int k = 0; k < 9; k++) o[k] = b[k];
-  rhs[3 * (size_t)row + 0] = r[0];
-  rhs[3 * (size_t)row + 1] = r[1];
-  rhs[3 * (size_t)row + 2] = r[2];
+  for (int m = 1; m <= 2; m <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) b[k] += __shfl_xor_sync(0xffffffffu, b[k], m);
+#pragma unroll
+    for (int k = 0; k < 3; k++) r[k] += __shfl_xor_sync(0xffffffffu, r[k], m);
+  }
+  if (d.x < 0) return;
+  if (sub == 0) {
+    double *o = vals + 9 * (size_t)d.x;
+#pragma unroll
+    for (int k = 0; k < 9; k++) o[k] = b[k];
+  } else if (sub == 1) {
+    rhs[3 * (size_t)row + 0] = r[0];
+    rhs[3 * (size_t)row + 1] = r[1];
+    rhs[3 * (size_t)row + 2] = r[2];
+  }
 }
 
 // Off-diagonal blocks: one thread per block of the compacted list, so the
-// lanes of a warp have lists of similar length (about three tets each).
+// lanes of a warp have lists of similar length (about three tets each).  The
+// codes are loaded ahead of the staging records they point to.
 __global__ void __launch_bounds__(256)
-    k_gather_off(int n_off, const int *__restrict__ offd, const int *__restrict__ rc_off,
-                 const int *__restrict__ rc_mid, const uint32_t *__restrict__ rc,
-                 const int *__restrict__ s2m, int identity, const double4 *__restrict__ es,
-                 const double *__restrict__ cs, double sc, double mc, double lam, double mu,
-                 double *__restrict__ vals) {
+    k_gather_off(int n_off, const int4 *__restrict__ desc, const uint32_t *__restrict__ rc,
+                 const double4 *__restrict__ es, const double *__restrict__ cs, double sc,
+                 double mc, double lam, double mu, double *__restrict__ vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_off) return;
-  const int st = __ldg(offd + i);
+  const int4 d = desc[i];
   double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  const int q0 = __ldg(rc_off + st), qm = __ldg(rc_mid + st), q1 = __ldg(rc_off + st + 1);
-  for (int q = q0; q < qm; q++) add_tet(__ldg(rc + q), es, sc, mc, lam, mu, b, nullptr);
-  for (int q = qm; q < q1; q++) add_cz(__ldg(rc + q), cs, b, nullptr);
-  const int pos = identity ? st : __ldg(s2m + st);
-  double *o = vals + 9 * (size_t)pos;
+  int q = d.y;
+  for (; q + 4 <= d.z; q += 4) {
+    const uint32_t c0 = __ldg(rc + q), c1 = __ldg(rc + q + 1), c2 = __ldg(rc + q + 2),
+                   c3 = __ldg(rc + q + 3);
+    add_tet(c0, es, sc, mc, lam, mu, b, nullptr);
+    add_tet(c1, es, sc, mc, lam, mu, b, nullptr);
+    add_tet(c2, es, sc, mc, lam, mu, b, nullptr);
+    add_tet(c3, es, sc, mc, lam, mu, b, nullptr);
+  }
+  for (; q < d.z; q++) add_tet(__ldg(rc + q), es, sc, mc, lam, mu, b, nullptr);
+  for (q = d.z; q < d.w; q++) add_cz(__ldg(rc + q), cs, b, nullptr);
+  double *o = vals + 9 * (size_t)d.x;
 #pragma unroll
   for (int k = 0; k < 9; k++) o[k] = b[k];
 }
@@ -700,14 +716,39 @@ __global__ void k_commit_cz(int nc, const double *__restrict__ tent,
 }  // namespace
 
 // ---- host launchers --------------------------------------------------------------
-int icf_launch_assembly(icf_ctx *ctx, double h) {
+// One assembly as a fork/join DAG over three streams:
+//   main : memsets | tets ............ | wait CZ -> diagonal gather | join -> contact add, checks
+//   aux0 :         | CZs | wait tets -> off-diagonal gather ........|
+//   aux1 :         | zero contact-only blocks, impact units .........|
+// The unit kernels are occupancy- or latency-limited on their own, so running
+// them side by side fills the machine; the gathers write disjoint blocks.
+static int enqueue_assembly(icf_ctx *ctx, double h) {
   const icf_dprm P = icf_make_dprm(ctx);
-  cudaStream_t s = ctx->stream;
+  cudaStream_t s = ctx->stream, sa = ctx->aux[0], sb = ctx->aux[1];
+  cudaEvent_t e_fork = ctx->ev[0], e_cz = ctx->ev[1], e_tet = ctx->ev[2], e_a = ctx->ev[3],
+              e_b = ctx->ev[4];
   ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, 8 * sizeof(int), s));
   ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
+  ICF_CUDA(ctx, cudaEventRecord(e_fork, s));
+  ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_fork, 0));
+  ICF_CUDA(ctx, cudaStreamWaitEvent(sb, e_fork, 0));
+
+  // aux1: contact-only blocks start at zero; impact units
+  if (ctx->n_dyn > 0)
+    k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, sb>>>(ctx->n_dyn, ctx->d_dynpos, ctx->d_vals);
+  if (ctx->n_imp > 0) {
+    const int rc = icf_launch_imp_unit(ctx, sb);
+    if (rc) return rc;
+  }
+  ICF_CUDA(ctx, cudaEventRecord(e_b, sb));
+
+  // main: tets
   if (ctx->n_elem > 0)
     k_tet_unit<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0,
                                                           ctx->d_xc, ctx->d_va, P, ctx->d_es);
+  ICF_CUDA(ctx, cudaEventRecord(e_tet, s));
+
+  // aux0: CZs
   if (ctx->n_cz > 0) {
     icf_law_c LC;
     LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
@@ -715,29 +756,37 @@ int icf_launch_assembly(icf_ctx *ctx, double h) {
     LC.rn = P.rn; LC.rt = P.rt;
     LC.N0 = icf_axis{ctx->axis0[0], ctx->axis0[1], ctx->axis0[2]};
     LC.T0 = icf_axis{ctx->axis0[3], ctx->axis0[4], ctx->axis0[5]};
-    k_cz_gp<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, s>>>(
+    auto small_int = [](double v) {
+      return (v == (double)(int)v && v >= 2 && v <= 16) ? (int)v : 0;
+    };
+    LC.alpha_int = small_int(P.alpha);
+    LC.beta_int = small_int(P.beta);
+    k_cz_gp<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, sa>>>(
         ctx->n_cz, ctx->d_cz, ctx->d_xc, ctx->d_czs, ctx->d_czfail,
         ctx->per_cz_prm ? ctx->d_czprm : nullptr, P, LC, ctx->d_cs, ctx->d_cztent, ctx->d_czflags,
         ctx->d_czavg, ctx->d_counts);
   }
-  if (ctx->n_imp > 0) {
-    const int rc = icf_launch_imp_unit(ctx);
-    if (rc) return rc;
-  }
+  ICF_CUDA(ctx, cudaEventRecord(e_cz, sa));
+
   const double nb = ctx->prm.NewmarkBeta, ng = ctx->prm.NewmarkGamma;
   const double sc = 1.0 + ctx->prm.dampingStiffness * ng / (h * nb);
   const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
-  const int ident = ctx->src_identity ? 1 : 0;
-  if (ctx->N > 0)
-    k_gather_diag<<<icf_blocks(ctx->N, 128), 128, 0, s>>>(
-        ctx->N, ctx->d_diag, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_rc, ctx->d_s2m, ident, ctx->d_es,
-        ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals, ctx->d_rhs);
+  // aux0: off-diagonal blocks once the tets are staged
+  ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_tet, 0));
   if (ctx->n_offd > 0)
-    k_gather_off<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(
-        ctx->n_offd, ctx->d_offd, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_rc, ctx->d_s2m, ident, ctx->d_es,
-        ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals);
-  if (ctx->n_dyn > 0)
-    k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, s>>>(ctx->n_dyn, ctx->d_dynpos, ctx->d_vals);
+    k_gather_off<<<icf_blocks(ctx->n_offd, 256), 256, 0, sa>>>(ctx->n_offd, ctx->d_gdesc_off, ctx->d_rc,
+                                                              ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu,
+                                                              ctx->d_vals);
+  ICF_CUDA(ctx, cudaEventRecord(e_a, sa));
+  // main: diagonal blocks and rhs once the CZs are staged
+  ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
+  if (ctx->N > 0)
+    k_gather_diag<<<icf_blocks(4LL * ctx->N, 128), 128, 0, s>>>(ctx->N, ctx->d_gdesc_diag, ctx->d_rc,
+                                                              ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu,
+                                                              ctx->d_vals, ctx->d_rhs);
+  // join
+  ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
+  ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
   if (ctx->n_crs > 0)
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off,
                                                         ctx->d_cr, ctx->d_cols, ctx->d_ks,
@@ -748,6 +797,39 @@ int icf_launch_assembly(icf_ctx *ctx, double h) {
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int),
                                 cudaMemcpyDeviceToHost, s));
+  return ICF_OK;
+}
+
+// Launches the assembly, through the captured graph when enabled.  The graph
+// is captured on first use and whenever the context's version (bumped by any
+// call that changes the pattern, sizes, parameters or buffers) or the time
+// step differs from the captured one.
+int icf_launch_assembly(icf_ctx *ctx, double h) {
+  if (!ctx->use_graph) return enqueue_assembly(ctx, h);
+  if (!ctx->graph_exec || ctx->graph_version != ctx->version || ctx->graph_h != h) {
+    if (ctx->graph_exec) {
+      cudaGraphExecDestroy(ctx->graph_exec);
+      ctx->graph_exec = nullptr;
+    }
+    ICF_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_assembly(ctx, h);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc != ICF_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ec != cudaSuccess) return icf_fail(ctx, ICF_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      ctx->graph_exec = nullptr;
+      return icf_fail(ctx, ICF_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    }
+    ctx->graph_version = ctx->version;
+    ctx->graph_h = h;
+  }
+  ICF_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
   return ICF_OK;
 }
 

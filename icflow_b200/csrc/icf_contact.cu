@@ -377,12 +377,12 @@ __global__ void k_imp_classify(int n, const int4 *__restrict__ imp, const int *_
 
 }  // namespace
 
-int icf_launch_imp_unit(icf_ctx *ctx) {
-  k_imp_classify<<<icf_blocks(ctx->n_imp, 128), 128, 0, ctx->stream>>>(
+int icf_launch_imp_unit(icf_ctx *ctx, cudaStream_t stream) {
+  k_imp_classify<<<icf_blocks(ctx->n_imp, 128), 128, 0, stream>>>(
       ctx->n_imp, ctx->d_imp, ctx->d_alt, ctx->d_xc, ctx->prm.DistanceEpsilon * ctx->prm.DistanceEpsilon,
       ctx->d_imp_ci, ctx->d_imp_cd, ctx->d_counts);
   ICF_CUDA(ctx, cudaGetLastError());
-  return icf_launch_imp_deriv(ctx, ctx->d_imp_ci, ctx->d_imp_cd);
+  return icf_launch_imp_deriv(ctx, ctx->d_imp_ci, ctx->d_imp_cd, stream);
 }
 
 // Narrow phase + set expansion + closest face.  Leaves ctx->d_imp /

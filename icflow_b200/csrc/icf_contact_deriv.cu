@@ -253,8 +253,8 @@ __global__ void __launch_bounds__(32 * WARPS)
 
 }  // namespace
 
-int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d) {
-  k_imp_deriv<<<icf_blocks(ctx->n_imp, WARPS), 32 * WARPS, 0, ctx->stream>>>(
+int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d, cudaStream_t stream) {
+  k_imp_deriv<<<icf_blocks(ctx->n_imp, WARPS), 32 * WARPS, 0, stream>>>(
       ctx->n_imp, ctx->d_imp, ctx->d_xc, cls_i, cls_d, ctx->prm.penaltyK, ctx->d_ks);
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;

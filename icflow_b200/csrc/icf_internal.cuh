@@ -71,6 +71,15 @@ struct icf_dprm {
 struct icf_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // auxiliary streams and events of the assembly's fork/join graph
+  cudaStream_t aux[2] = {nullptr, nullptr};
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // the assembly captured as a CUDA graph; re-captured when anything it
+  // bakes in (pattern, sizes, parameters, buffers, time step) changes
+  bool use_graph = true;
+  cudaGraphExec_t graph_exec = nullptr;
+  double graph_h = 0.0;
+  unsigned long long version = 1, graph_version = 0;
   std::string err;
   icf_params prm{};
   bool have_prm = false;
@@ -130,6 +139,10 @@ struct icf_ctx {
   // positions of the contact-only blocks
   int *d_s2m = nullptr, *d_dynpos = nullptr;
   int s2m_cap = 0, dynpos_cap = 0, n_dyn = 0;
+  // gather descriptors {merged position, first tet code, first CZ code, end}:
+  // N per-row diagonal entries, then one per off-diagonal block (one buffer)
+  int4 *d_gdesc_diag = nullptr, *d_gdesc_off = nullptr;
+  int gdesc_cap = 0;
 
   // merged pattern
   int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;
@@ -201,6 +214,6 @@ int icf_launch_infer(icf_ctx *ctx, double h);
 int icf_launch_add_dx(icf_ctx *ctx, const double *d_dx);
 int icf_launch_accept(icf_ctx *ctx, double h);
 int icf_launch_commit_cz(icf_ctx *ctx);
-int icf_launch_imp_unit(icf_ctx *ctx);
-int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d);
+int icf_launch_imp_unit(icf_ctx *ctx, cudaStream_t stream);
+int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d, cudaStream_t stream);
 int icf_get_node_inc(icf_ctx *ctx, icf_node_inc *tets, icf_node_inc *imps);

@@ -174,6 +174,22 @@ __global__ void k_slot_meta(int nnz_s, const unsigned long long *__restrict__ sk
   offflag[s] = row != col;
 }
 
+// Gather descriptors {merged position, first tet code, first CZ code, end}:
+// per row for the diagonal blocks (position -1 if the row has none) and per
+// off-diagonal block.
+__global__ void k_desc(int n, const int *__restrict__ slot_of, const int *__restrict__ rc_off,
+                       const int *__restrict__ rc_mid, const int *__restrict__ s2m, int identity,
+                       int4 *__restrict__ desc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int st = slot_of[i];
+  if (st < 0) {
+    desc[i] = make_int4(-1, 0, 0, 0);
+    return;
+  }
+  desc[i] = make_int4(identity ? st : s2m[st], rc_off[st], rc_mid[st], rc_off[st + 1]);
+}
+
 __global__ void k_iota(int n, int *__restrict__ a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i;
@@ -531,6 +547,21 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
     ctx->src_identity = false;
   }
   ctx->n_dyn = nd;
+  // gather descriptors for this merge
+  if (!ctx->d_gdesc_diag || ctx->gdesc_cap < N + ctx->n_offd + 2) {
+    cudaFree(ctx->d_gdesc_diag);
+    ctx->d_gdesc_diag = nullptr;
+    ICF_CUDA(ctx, cudaMalloc(&ctx->d_gdesc_diag, sizeof(int4) * (size_t)(N + ctx->n_offd + 2)));
+    ctx->gdesc_cap = N + ctx->n_offd + 2;
+  }
+  ctx->d_gdesc_off = ctx->d_gdesc_diag + N + 1;
+  const int ident = nd == 0 ? 1 : 0;
+  if (N > 0)
+    k_desc<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_diag, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_s2m,
+                                             ident, ctx->d_gdesc_diag);
+  if (ctx->n_offd > 0)
+    k_desc<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_offd, ctx->d_rc_off,
+                                                       ctx->d_rc_mid, ctx->d_s2m, ident, ctx->d_gdesc_off);
   if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
   if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
   k_rows<<<icf_blocks((long long)N + 1, 256), 256, 0, s>>>(N, nnz, ctx->d_mkeys, ctx->d_rows);

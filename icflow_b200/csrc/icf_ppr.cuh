@@ -117,10 +117,15 @@ struct icf_axis {
 };
 
 __device__ __forceinline__ icf_axis icf_axis_eval(double a, double p, double gam, double mac,
-                                                  double x) {
+                                                  double x, int a_int = 0) {
   const double o = 1.0 - x, s = (p / a) + x;
   double o0, o1, o2;
-  if (o > 0) {
+  if (a_int >= 2) {  // integer exponent: (1-x)^(a-2) by repeated products
+    o2 = 1.0;
+    for (int k = 0; k < a_int - 2; k++) o2 *= o;
+    o1 = o2 * o;
+    o0 = o1 * o;
+  } else if (o > 0) {
     o0 = pow(o, a);
     o1 = o0 / o;
     o2 = o1 / o;
@@ -140,6 +145,7 @@ __device__ __forceinline__ icf_axis icf_axis_eval(double a, double p, double gam
 struct icf_law_c {
   double alpha, beta, p_m, p_n, gam_n, gam_t, pMtn, pMnt, rn, rt;
   icf_axis N0, T0;  // axes at zero opening
+  int alpha_int, beta_int;  // alpha, beta when they are integers in [2, 16], else 0
 };
 
 // cohesive_law_thermodynamically_consistent (cz_kernels.h:37-174) on the axis
@@ -161,9 +167,9 @@ __device__ inline icf_law icf_cz_law_axes(const icf_law_c &C, double f_tn, doubl
   L.contact = (opn < 0);
   const double eps_neg = -1e-9;
   const double thr_t = f_tt * 0.05, thr_n = f_tn * 0.05;
-  const icf_axis Np = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, pmax / deln);
-  const icf_axis Tm = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, tmax / delt);
-  const icf_axis To = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, opt / delt);
+  const icf_axis Np = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, pmax / deln, C.alpha_int);
+  const icf_axis Tm = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, tmax / delt, C.beta_int);
+  const icf_axis To = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, opt / delt, C.beta_int);
   if (L.contact) {
     if (pmax != 0) {
       const double peak = cN * Np.d * Tm.f;           // Tn_(pmax, tmax)
@@ -190,7 +196,7 @@ __device__ inline icf_law icf_cz_law_axes(const icf_law_c &C, double f_tn, doubl
     }
     return L;
   }
-  const icf_axis No = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, opn / deln);
+  const icf_axis No = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, opn / deln, C.alpha_int);
   L.Tt = cT * To.d * No.f;                            // Tt_(opn, opt)
   L.Tn = cN * No.d * To.f;                            // Tn_(opn, opt)
   if (L.Tt >= eps_neg && L.Tn >= eps_neg && !(opt > delt * C.rt / 5 && L.Tt < thr_t) &&

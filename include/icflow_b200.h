@@ -180,6 +180,10 @@ int icf_assemble(icf_ctx *ctx, double h, icf_counts *counts);
  * read later with icf_read_counts.  Capturable in a CUDA graph once the
  * pattern is built. */
 int icf_assemble_async(icf_ctx *ctx, double h);
+/* The assembly runs as a fork/join DAG over three streams, captured once as a
+ * CUDA graph (default) and re-captured only when the pattern, parameters,
+ * buffers or time step change; enable = 0 launches the kernels directly. */
+int icf_set_graph(icf_ctx *ctx, int enable);
 int icf_read_counts(icf_ctx *ctx, icf_counts *counts);
 
 /* ---- results ------------------------------------------------------------- */

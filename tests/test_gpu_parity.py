@@ -171,3 +171,29 @@ def test_error_paths():
     gf.CreateStructure()
     assert lib.icf_assemble(gf.ctx, -1.0, None) == _lib.ICF_ERR_ARG
     gf.close()
+
+
+def test_graph_matches_direct_launch(O):
+    """The captured fork/join graph and direct launches give identical bits,
+    and a changed time step or pattern re-captures the graph."""
+    from icflow_b200 import _lib
+
+    coll = M.polycrystal(n=6, grains=5, seed=4, platens=True, gap=-0.3)
+    prms = config_prms(penaltyK=1e8)
+    gf = _gf(coll, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    state = random_state(coll, 2, du=1e-6)
+    pairs = M.candidate_pairs(coll, coll.x0 + state[0])
+    lib = _lib.load()
+    outs = []
+    for graph in (1, 0, 1):
+        _lib.check(gf.ctx, lib.icf_set_graph(gf.ctx, graph))
+        outs.append(gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs))
+    for o in outs[1:]:
+        assert np.array_equal(o["vals"], outs[0]["vals"]) and np.array_equal(o["rhs"], outs[0]["rhs"])
+    a = gpu_assemble(gf, coll, state, 2 * H, pmax, tmax, failed, pairs=pairs)
+    p = orc_prms_from(O, prms)
+    imp = gf.c_itet
+    o = oracle_assemble(O, p, coll, state, 2 * H, pmax, tmax, imp)
+    compare(a, o)
+    gf.close()
