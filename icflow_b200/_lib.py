@@ -102,6 +102,7 @@ SIGNATURES = {
     "icf_assemble_async": (I, [P, D]),
     "icf_set_graph": (I, [P, I]),
     "icf_read_counts": (I, [P, C.POINTER(icf_counts)]),
+    "icf_assemble_noalloc": (I, [P, D, P, P, P, P, P, C.POINTER(icf_counts)]),
     "icf_transfer_linear_system": (I, [P, dp, dp]),
     "icf_transfer_updated_state": (I, [P, dp, dp, ip, dp, dp]),
     "icf_get_cz_tentative": (I, [P, dp, ip, dp]),

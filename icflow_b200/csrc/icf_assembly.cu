@@ -885,3 +885,54 @@ int icf_launch_commit_cz(icf_ctx *ctx) {
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
+
+// ---- launches with caller-chosen buffers (used by the allocation-free entry
+// point in icf_noalloc.cu; the context's own assembly path above is separate)
+int icf_enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cudaStream_t s) {
+  const icf_dprm P = icf_make_dprm(ctx);
+  ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, 8 * sizeof(int), s));
+  ICF_CUDA(ctx, cudaMemsetAsync(B.rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
+  k_pack_nodes<<<icf_blocks(ctx->n_nodes, 256), 256, 0, s>>>(ctx->n_nodes, ctx->d_x0, B.un, B.vn, B.an,
+                                                            B.xc, B.va);
+  if (ctx->n_elem > 0)
+    k_tet_unit<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0, B.xc,
+                                                          B.va, P, B.es);
+  if (ctx->n_cz > 0) {
+    icf_law_c LC;
+    LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
+    LC.gam_n = P.gam_n; LC.gam_t = P.gam_t; LC.pMtn = P.pMtn; LC.pMnt = P.pMnt;
+    LC.rn = P.rn; LC.rt = P.rt;
+    LC.N0 = icf_axis{ctx->axis0[0], ctx->axis0[1], ctx->axis0[2]};
+    LC.T0 = icf_axis{ctx->axis0[3], ctx->axis0[4], ctx->axis0[5]};
+    auto small_int = [](double v) { return (v == (double)(int)v && v >= 2 && v <= 16) ? (int)v : 0; };
+    LC.alpha_int = small_int(P.alpha);
+    LC.beta_int = small_int(P.beta);
+    k_cz_gp<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, s>>>(
+        ctx->n_cz, ctx->d_cz, B.xc, ctx->d_czs, ctx->d_czfail, ctx->per_cz_prm ? ctx->d_czprm : nullptr, P,
+        LC, B.cs, ctx->d_cztent, ctx->d_czflags, ctx->d_czavg, ctx->d_counts);
+  }
+  if (ctx->n_imp > 0) {
+    const int rc = icf_launch_imp_unit_bufs(ctx, B.xc, B.ci, B.cd, B.ks, s);
+    if (rc) return rc;
+  }
+  const double nb = ctx->prm.NewmarkBeta, ng = ctx->prm.NewmarkGamma;
+  const double sc = 1.0 + ctx->prm.dampingStiffness * ng / (h * nb);
+  const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
+  if (ctx->n_dyn > 0)
+    k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, s>>>(ctx->n_dyn, ctx->d_dynpos, B.vals);
+  if (ctx->n_offd > 0)
+    k_gather_off<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_gdesc_off, ctx->d_rc, B.es,
+                                                             B.cs, sc, mc, P.lam, P.mu, B.vals);
+  if (ctx->N > 0)
+    k_gather_diag<<<icf_blocks(4LL * ctx->N, 128), 128, 0, s>>>(ctx->N, ctx->d_gdesc_diag, ctx->d_rc, B.es,
+                                                              B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs);
+  if (ctx->n_crs > 0)
+    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
+                                                        ctx->d_cols, B.ks, B.vals, B.rhs);
+  if (ctx->N > 0)
+    k_finite<<<icf_blocks(3LL * ctx->N, 256) < 1184 ? icf_blocks(3LL * ctx->N, 256) : 1184, 256, 0, s>>>(
+        3 * ctx->N, B.rhs, ctx->d_counts + 4);
+  ICF_CUDA(ctx, cudaGetLastError());
+  ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  return ICF_OK;
+}

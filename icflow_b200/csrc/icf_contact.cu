@@ -448,3 +448,13 @@ int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts) {
   *n_impacts = nu;
   return ICF_OK;
 }
+
+// Impact units with caller-chosen buffers (allocation-free entry point).
+int icf_launch_imp_unit_bufs(icf_ctx *ctx, const double4 *xc, int4 *ci, double4 *cd, double *ks,
+                             cudaStream_t stream) {
+  k_imp_classify<<<icf_blocks(ctx->n_imp, 128), 128, 0, stream>>>(
+      ctx->n_imp, ctx->d_imp, ctx->d_alt, xc, ctx->prm.DistanceEpsilon * ctx->prm.DistanceEpsilon, ci, cd,
+      ctx->d_counts);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return icf_launch_imp_deriv_bufs(ctx, xc, ci, cd, ks, stream);
+}

@@ -259,3 +259,12 @@ int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d, 
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
+
+// Derivative kernel with caller-chosen buffers (allocation-free entry point).
+int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, const int4 *cls_i, const double4 *cls_d,
+                              double *ks, cudaStream_t stream) {
+  k_imp_deriv<<<icf_blocks(ctx->n_imp, WARPS), 32 * WARPS, 0, stream>>>(ctx->n_imp, ctx->d_imp, xc, cls_i,
+                                                                       cls_d, ctx->prm.penaltyK, ks);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}

@@ -185,6 +185,23 @@ int icf_assemble_async(icf_ctx *ctx, double h);
  * buffers or time step change; enable = 0 launches the kernels directly. */
 int icf_set_graph(icf_ctx *ctx, int enable);
 int icf_read_counts(icf_ctx *ctx, icf_counts *counts);
+/* Allocation-free assembly.  No counterpart in the reference: icFlow always
+ * assembles into buffers its GPU class allocated.  For callers that cannot
+ * allocate device memory while they assemble (a host that serves every device
+ * byte from its own pre-sized pool, or a loop that must not enter the
+ * allocator), this computes the same blocks and rhs as icf_assemble from the
+ * caller's device arrays d_un, d_vn, d_an (n_nodes*3 doubles each) into the
+ * caller's device arrays d_vals (nnz*9) and d_rhs (N*3), with every temporary
+ * held in one 8 MiB static device array that each GPU loading the library keeps
+ * until exit.  It calls no cudaMalloc or cudaFree.  Models whose temporaries
+ * exceed 8 MiB (80 B/node + 256 B/tet + 384 B/CZ + 1328 B/impact) get
+ * ICF_ERR_SIZE.  The context must hold constants, static data and a structure
+ * from earlier calls.  The first call on a device looks up the array's device
+ * address (make it before any stream capture).  All calls share the array:
+ * calls that overlap on the GPU race.  Synchronous. */
+int icf_assemble_noalloc(icf_ctx *ctx, double h, const double *d_un, const double *d_vn,
+                         const double *d_an, double *d_vals, double *d_rhs,
+                         icf_counts *counts);
 
 /* ---- results ------------------------------------------------------------- */
 /* TransferLinearSystemToHost :481-485: vals[nnz*9], rhs[N*3] (either may be
