@@ -43,6 +43,18 @@ H = 1e-5
 FLUSH_BYTES = 256 << 20
 
 
+WORKLOADS = {
+    # polycrystal compression, 1 mm cube: (hexes per side, grains)
+    "cfg1": (32, 128),    # 196,608 tets, ~35k CZs
+    "cfg2": (64, 2048),   # 1,572,864 tets, ~390k CZs
+}
+
+
+def workload_name(n: int, grains: int) -> str:
+    return (f"polycrystal compression, 1 mm cube, {n}^3 hex -> 6 tets ({6 * n ** 3} tets), {grains} grains, "
+            "CZs on grain boundaries, rigid platens in contact, dt 1e-5")
+
+
 def build_workload(seed: int, n: int = 32, grains: int = 128):
     from icflow_b200 import mesh as M
 
@@ -142,12 +154,13 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-assembly DRAM bytes from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "assembly_traffic.json"
+def ncu_traffic(kernel: str, workload: str):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary, if it holds a capture of this workload."""
+    p = ROOT / "profiles" / "dram_traffic.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get("dram_bytes_per_assembly")
+            return json.loads(p.read_text()).get(workload, {}).get(kernel)
         except (ValueError, OSError):
             return None
     return None
@@ -163,9 +176,10 @@ def cpu_baseline(coll, state, sig, pairs, bound_s: float = 12.0, nthreads: int =
     from icflow_b200.model_prms import config_prms
 
     prms = config_prms(penaltyK=1e8)
-    from tests.harness import orc_prms_from
-
-    p = orc_prms_from(O, prms)
+    keys = ("Y", "nu", "rho", "dampingMass", "dampingStiffness", "gravity", "NewmarkBeta", "NewmarkGamma",
+            "alpha", "beta", "lambda_n", "lambda_t", "phi_n", "phi_t", "sigma_max", "tau_max", "penaltyK",
+            "DistanceEpsilon")
+    p = O.prms(**{k: getattr(prms, k) for k in keys})
     un, vn, an = state
     xt = coll.x0 + un
     masks = O.narrow_phase(pairs, coll.selem, xt)
@@ -214,7 +228,8 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    coll, state, sig, pairs = build_workload(0)
+    n, grains = WORKLOADS[args.workload]
+    coll, state, sig, pairs = build_workload(0, n, grains)
     steps = max(args.steps, 1)
     rate, threads, kind, sample = cpu_baseline(coll, state, sig, pairs,
                                                bound_s=min(60.0, 2.0 * steps))
@@ -222,8 +237,7 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 / rate, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": "polycrystal compression, 1 mm cube, 196608 tets, 128 grains, "
-                                   "CZs on grain boundaries, rigid platens in contact",
+            "config": {"workload": workload_name(n, grains),
                        "tets": int(len(coll.elems)), "czs": int(len(coll.czs))},
             "cpu_baseline": {"value": rate, "unit": "assemblies/s", "cores": threads, "kind": kind,
                              "sample": sample},
@@ -250,7 +264,8 @@ def run_ours(args):
     dev = local if ws > 1 else 0
     torch.cuda.set_device(dev)
 
-    coll, state, sig, pairs = build_workload(rank)
+    n, grains = WORKLOADS[args.workload]
+    coll, state, sig, pairs = build_workload(rank, n, grains)
     prms = config_prms(penaltyK=1e8)
     gf = GPU_Functionality(dev)
     gf.prms = prms
@@ -321,6 +336,9 @@ def run_ours(args):
         barrier()
         ms_e2e = e0.elapsed_time(e1) / args.steps
     clocks = clk.summary()
+    # per-kernel device times: the same kernels run in the graph's order on
+    # one stream with an event after each (no overlap between streams)
+    kernels = gf.ProfileAssembly(H, reps=max(args.steps, 10))
 
     if ws > 1:
         t = torch.tensor([ms_dev, ms_e2e], device=dev, dtype=torch.float64)
@@ -330,7 +348,13 @@ def run_ours(args):
     B = algorithmic_bytes(nnz, N, len(coll.x0), len(coll.elems), nc, len(imps))
     peak, peak_kind = measured_peak()
     achieved = B / (ms_dev * 1e-3) / 1e9
-    launches_per_step = 4 + (1 if len(imps) else 0) + (1 if len(imps) else 0)
+    launches_per_step = len(kernels)
+    top = max(kernels, key=lambda k: k["ms"])
+    k_sum = sum(k["ms"] for k in kernels)
+    for k in kernels:
+        k["GBps"] = k["bytes"] / (k["ms"] * 1e-3) / 1e9
+        k["share"] = k["ms"] / k_sum
+    top_ach = top["bytes"] / (top["ms"] * 1e-3) / 1e9
     line = None
     if rank == 0:
         line = {
@@ -338,15 +362,21 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded polycrystal; no public dataset exists for this path)",
-            "config": {"workload": "polycrystal compression, 1 mm cube, 32^3 hex -> 6 tets, 128 grains, "
-                                   "CZs on grain boundaries, rigid platens in contact, dt 1e-5",
+            "config": {"workload": workload_name(n, grains),
                        "tets": int(len(coll.elems)), "czs": int(nc), "nodes": int(len(coll.x0)),
                        "active_rows": int(N), "blocks": int(nnz), "impacts": int(len(imps)),
                        "l2": "flushed between steps (256 MiB write), outside the timed region"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": ncu_traffic(),
-                         "algorithmic_bytes": B, "peak_source": peak_kind,
-                         "scope": "whole assembly (all kernels of one step)"},
+            "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": top_ach, "peak": peak,
+                         "unit": "GB/s", "frac": top_ach / peak, "traffic": ncu_traffic(top["name"], args.workload),
+                         "algorithmic_bytes": top["bytes"], "launch_ms": top["ms"],
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback",
+                         "assembly": {"algorithmic_bytes": B, "achieved": achieved, "frac": achieved / peak,
+                                      "scope": "one whole assembly (graph launch), bytes per the "
+                                               "72 nnzb + 24 N_a + 96 N + 56 n_t + 240 n_c + 56 n_i model"},
+                         "kernels": [{"name": k["name"], "ms": round(k["ms"], 5), "share": round(k["share"], 4),
+                                      "bytes": k["bytes"], "GBps": round(k["GBps"], 1),
+                                      "frac": round(k["GBps"] / peak, 4)} for k in kernels]},
             "e2e": {"value": ws * 1000.0 / ms_e2e, "unit": "assemblies/s",
                     "h2d_bytes_per_step": int(3 * un.nbytes), "d2h_bytes_per_step": int(8 * (9 * nnz + 3 * N))},
             "gpu_launches": launches_per_step * args.steps,
@@ -372,6 +402,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", default="cfg1", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

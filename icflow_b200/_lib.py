@@ -65,6 +65,15 @@ class icf_counts(C.Structure):
         "nImpacts", "nImpactsActive", "nonFinite")]
 
 
+class icf_kernel_times(C.Structure):
+    _fields_ = [("n_kernels", C.c_int), ("name", (C.c_char * 32) * 16),
+                ("bytes", C.c_longlong * 16), ("ms", C.c_double * 16)]
+
+    def as_list(self):
+        return [{"name": bytes(self.name[k]).split(b"\0")[0].decode(), "bytes": int(self.bytes[k]),
+                 "ms": float(self.ms[k])} for k in range(self.n_kernels)]
+
+
 class icf_device_buffers(C.Structure):
     _fields_ = [
         ("vals", C.c_void_p), ("rhs", C.c_void_p), ("csr_rows", C.c_void_p),
@@ -102,6 +111,7 @@ SIGNATURES = {
     "icf_assemble_async": (I, [P, D]),
     "icf_set_graph": (I, [P, I]),
     "icf_read_counts": (I, [P, C.POINTER(icf_counts)]),
+    "icf_profile_assembly": (I, [P, D, I, C.POINTER(icf_kernel_times)]),
     "icf_assemble_noalloc": (I, [P, D, P, P, P, P, P, C.POINTER(icf_counts)]),
     "icf_transfer_linear_system": (I, [P, dp, dp]),
     "icf_transfer_updated_state": (I, [P, dp, dp, ip, dp, dp]),

@@ -554,6 +554,27 @@ int icf_assemble_async(icf_ctx *ctx, double h) {
   return icf_launch_assembly(ctx, h);
 }
 
+int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out) {
+  ICF_CHECK_CTX(ctx);
+  if (!out || reps < 1) return icf_fail(ctx, ICF_ERR_ARG, "icf_profile_assembly: out and reps >= 1 required");
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  ICF_CUDA(ctx, cudaSetDevice(ctx->device));
+  const char *names[ICF_PROF_MAX];
+  long long bytes[ICF_PROF_MAX];
+  double ms[ICF_PROF_MAX];
+  int n = 0;
+  const int rc = icf_profile_assembly_impl(ctx, h, reps, &n, names, bytes, ms);
+  if (rc) return rc;
+  memset(out, 0, sizeof(*out));
+  out->n_kernels = n < ICF_MAX_KERNELS ? n : ICF_MAX_KERNELS;
+  for (int k = 0; k < out->n_kernels; k++) {
+    strncpy(out->name[k], names[k], 31);
+    out->bytes[k] = bytes[k];
+    out->ms[k] = ms[k];
+  }
+  return icf_read_counts(ctx, nullptr);
+}
+
 int icf_set_graph(icf_ctx *ctx, int enable) {
   ICF_CHECK_CTX(ctx);
   ctx->use_graph = enable != 0;

@@ -17,6 +17,8 @@
 // Each block is summed in a fixed order and written once, so the result is
 // bit-reproducible; the reference's CAS-loop atomics (atomic_add.h:1-13) have
 // no counterpart.
+#include <vector>
+
 #include "icf_internal.cuh"
 #include "icf_ppr.cuh"
 
@@ -69,14 +71,13 @@ __device__ __forceinline__ void frame3(const double p0[3], const double p1[3],
 //   sum_b Df_ab v_b = V (lam tr(L) I + mu (L + L^T)) h_a,  L = sum_b v_b h_b^T
 // and the consistent mass is M_ab = rho/20 (1 + delta_ab) I.  The staging
 // record of vertex a is {h_a, V} and {rhs_a, 0}; k_gather rebuilds
-// LHS_ab = stiffCoeff Df_ab + massCoeff M_ab from it.
-__global__ void __launch_bounds__(128, 3)
-    k_tet_unit(int ne, const int4 *__restrict__ elem,
-               const double4 *__restrict__ x0, const double4 *__restrict__ xc,
-               const double2 *__restrict__ va, icf_dprm P,
-               double4 *__restrict__ es) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= ne) return;
+// LHS_ab = stiffCoeff Df_ab + massCoeff M_ab from it.  The record (16
+// double2, 256 B) is written to rec in shared memory.
+__device__ __forceinline__ void tet_record(int e, const int4 *__restrict__ elem,
+                                           const double4 *__restrict__ x0,
+                                           const double4 *__restrict__ xc,
+                                           const double2 *__restrict__ va, const icf_dprm &P,
+                                           double2 *rec) {
   const int4 id = __ldg(elem + e);
   const int nid[4] = {id.x, id.y, id.z, id.w};
   double X[4][3], C[4][3], Vn[4][3], An[4][3];
@@ -166,7 +167,6 @@ __global__ void __launch_bounds__(128, 3)
   const double mV = P.rho20 * V;
   const double gz = P.grav_rho * V / 4;
 
-  double4 *out = es + 8 * (size_t)e;
 #pragma unroll
   for (int a = 0; a < 4; a++) {
     double sg[3], f[3], dv[3], r[3];
@@ -186,8 +186,35 @@ __global__ void __launch_bounds__(128, 3)
       const double inert = mV * (An[a][k] + sa[k]);
       r[k] = (k == 2 ? gz : 0.0) - f[k] - damp - inert;
     }
-    out[a] = make_double4(h[a][0], h[a][1], h[a][2], V);
-    out[4 + a] = make_double4(r[0], r[1], r[2], 0.0);
+    rec[2 * a] = make_double2(h[a][0], h[a][1]);
+    rec[2 * a + 1] = make_double2(h[a][2], V);
+    rec[8 + 2 * a] = make_double2(r[0], r[1]);
+    rec[9 + 2 * a] = make_double2(r[2], 0.0);
+  }
+}
+
+// One thread per tetrahedron.  Each warp's 32 records (8 KB) are staged in
+// shared memory (rows padded to 272 B, so both the row-wise writes and the
+// column-wise reads are free of bank conflicts) and stored as 512 B
+// contiguous chunks per instruction.
+__global__ void __launch_bounds__(128, 3)
+    k_tet_unit(int ne, const int4 *__restrict__ elem,
+               const double4 *__restrict__ x0, const double4 *__restrict__ xc,
+               const double2 *__restrict__ va, icf_dprm P,
+               double4 *__restrict__ es) {
+  __shared__ double2 sbuf[4][32][17];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long base = (long long)blockIdx.x * blockDim.x + 32 * w;
+  if (base >= ne) return;
+  const int e = (int)base + lane;
+  if (e < ne) tet_record(e, elem, x0, xc, va, P, sbuf[w][lane]);
+  __syncwarp();
+  const long long nrec = (ne - base) < 32 ? (ne - base) : 32;
+  double2 *o = reinterpret_cast<double2 *>(es) + 16 * base;
+#pragma unroll 4
+  for (int k = 0; k < 16; k++) {
+    const int idx = 32 * k + lane;
+    if (idx < 16 * nrec) o[idx] = sbuf[w][idx >> 4][idx & 15];
   }
 }
 
@@ -506,7 +533,7 @@ __global__ void __launch_bounds__(128)
 // Off-diagonal blocks: one thread per block of the compacted list, so the
 // lanes of a warp have lists of similar length (about three tets each).  The
 // codes are loaded ahead of the staging records they point to.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_gather_off(int n_off, const int4 *__restrict__ desc, const uint32_t *__restrict__ rc,
                  const double4 *__restrict__ es, const double *__restrict__ cs, double sc,
                  double mc, double lam, double mu, double *__restrict__ vals) {
@@ -725,10 +752,12 @@ __global__ void k_commit_cz(int nc, const double *__restrict__ tent,
 static int enqueue_assembly(icf_ctx *ctx, double h) {
   const icf_dprm P = icf_make_dprm(ctx);
   cudaStream_t s = ctx->stream, sa = ctx->aux[0], sb = ctx->aux[1];
+  if (ctx->prof) sa = sb = s;  // per-kernel timing: one stream, in order
   cudaEvent_t e_fork = ctx->ev[0], e_cz = ctx->ev[1], e_tet = ctx->ev[2], e_a = ctx->ev[3],
               e_b = ctx->ev[4];
   ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, 8 * sizeof(int), s));
   ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
+  if (ctx->prof) ICF_CUDA(ctx, cudaEventRecord(ctx->prof->ev[0], s));
   ICF_CUDA(ctx, cudaEventRecord(e_fork, s));
   ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_fork, 0));
   ICF_CUDA(ctx, cudaStreamWaitEvent(sb, e_fork, 0));
@@ -736,6 +765,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   // aux1: contact-only blocks start at zero; impact units
   if (ctx->n_dyn > 0)
     k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, sb>>>(ctx->n_dyn, ctx->d_dynpos, ctx->d_vals);
+  if (ctx->n_dyn > 0) icf_prof_mark(ctx, sb, "k_zero_dyn", 76LL * ctx->n_dyn);
   if (ctx->n_imp > 0) {
     const int rc = icf_launch_imp_unit(ctx, sb);
     if (rc) return rc;
@@ -746,6 +776,8 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   if (ctx->n_elem > 0)
     k_tet_unit<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0,
                                                           ctx->d_xc, ctx->d_va, P, ctx->d_es);
+  // ids, node state (x0, x_t, v, a) once, 256 B record out
+  if (ctx->n_elem > 0) icf_prof_mark(ctx, s, "k_tet_unit", 272LL * ctx->n_elem + 112LL * ctx->n_nodes);
   ICF_CUDA(ctx, cudaEventRecord(e_tet, s));
 
   // aux0: CZs
@@ -765,6 +797,10 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
         ctx->n_cz, ctx->d_cz, ctx->d_xc, ctx->d_czs, ctx->d_czfail,
         ctx->per_cz_prm ? ctx->d_czprm : nullptr, P, LC, ctx->d_cs, ctx->d_cztent, ctx->d_czflags,
         ctx->d_czavg, ctx->d_counts);
+    // ids, six node positions, state in, per-CZ strengths, staging, tentative
+    // state, flags and averages out
+    icf_prof_mark(ctx, sa, "k_cz_gp", (24LL + 192 + 52 + (ctx->per_cz_prm ? 32 : 0) + 8 * ICF_CZ_STAGE + 84) *
+                                          ctx->n_cz);
   }
   ICF_CUDA(ctx, cudaEventRecord(e_cz, sa));
 
@@ -777,6 +813,11 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     k_gather_off<<<icf_blocks(ctx->n_offd, 256), 256, 0, sa>>>(ctx->n_offd, ctx->d_gdesc_off, ctx->d_rc,
                                                               ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu,
                                                               ctx->d_vals);
+  // descriptors, codes, the h records of every tet and the CZ staging once,
+  // blocks out
+  if (ctx->n_offd > 0)
+    icf_prof_mark(ctx, sa, "k_gather_off", 88LL * ctx->n_offd + 4LL * ctx->n_rc_off + 128LL * ctx->n_elem +
+                                               8LL * ICF_CZ_STAGE * ctx->n_cz);
   ICF_CUDA(ctx, cudaEventRecord(e_a, sa));
   // main: diagonal blocks and rhs once the CZs are staged
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
@@ -784,6 +825,9 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     k_gather_diag<<<icf_blocks(4LL * ctx->N, 128), 128, 0, s>>>(ctx->N, ctx->d_gdesc_diag, ctx->d_rc,
                                                               ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu,
                                                               ctx->d_vals, ctx->d_rhs);
+  if (ctx->N > 0)
+    icf_prof_mark(ctx, s, "k_gather_diag", 112LL * ctx->N + 4LL * (ctx->n_rc - ctx->n_rc_off) +
+                                               256LL * ctx->n_elem + 8LL * ICF_CZ_STAGE * ctx->n_cz);
   // join
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
@@ -791,9 +835,12 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off,
                                                         ctx->d_cr, ctx->d_cols, ctx->d_ks,
                                                         ctx->d_vals, ctx->d_rhs);
+  if (ctx->n_crs > 0)
+    icf_prof_mark(ctx, s, "k_imp_add", 8LL * ICF_IMP_STAGE * ctx->n_imp + 172LL * ctx->n_crs + 4LL * 16 * ctx->n_imp);
   if (ctx->N > 0)
     k_finite<<<icf_blocks(3LL * ctx->N, 256) < 1184 ? icf_blocks(3LL * ctx->N, 256) : 1184, 256, 0,
                s>>>(3 * ctx->N, ctx->d_rhs, ctx->d_counts + 4);
+  if (ctx->N > 0) icf_prof_mark(ctx, s, "k_finite", 24LL * ctx->N);
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int),
                                 cudaMemcpyDeviceToHost, s));
@@ -804,6 +851,54 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
 // is captured on first use and whenever the context's version (bumped by any
 // call that changes the pattern, sizes, parameters or buffers) or the time
 // step differs from the captured one.
+void icf_prof_mark(icf_ctx *ctx, cudaStream_t s, const char *name, long long bytes) {
+  icf_prof_state *p = ctx->prof;
+  if (!p || p->n >= ICF_PROF_MAX) return;
+  p->name[p->n] = name;
+  p->bytes[p->n] = bytes;
+  cudaEventRecord(p->ev[p->n + 1], s);
+  p->n++;
+}
+
+// Runs `reps` assemblies without the graph, on one stream, with an event
+// after every kernel; returns each kernel's mean device time.  The
+// kernels, their launch shapes and their order are those of the graph; only
+// the overlap between the streams is given up.
+int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const char **names,
+                              long long *bytes, double *ms) {
+  icf_prof_state st;
+  for (int i = 0; i <= ICF_PROF_MAX; i++) ICF_CUDA(ctx, cudaEventCreate(&st.ev[i]));
+  std::vector<double> acc(ICF_PROF_MAX, 0.0);
+  int rc = ICF_OK;
+  for (int r = 0; r < reps && rc == ICF_OK; r++) {
+    st.n = 0;
+    ctx->prof = &st;
+    rc = enqueue_assembly(ctx, h);
+    ctx->prof = nullptr;
+    if (rc) break;
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      rc = icf_fail(ctx, ICF_ERR_CUDA, std::string("profile: ") + cudaGetErrorString(e));
+      break;
+    }
+    for (int k = 0; k < st.n; k++) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, st.ev[k], st.ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  ctx->prof = nullptr;
+  for (int i = 0; i <= ICF_PROF_MAX; i++) cudaEventDestroy(st.ev[i]);
+  if (rc) return rc;
+  *n = st.n;
+  for (int k = 0; k < st.n; k++) {
+    names[k] = st.name[k];
+    bytes[k] = st.bytes[k];
+    ms[k] = acc[k] / (reps > 0 ? reps : 1);
+  }
+  return ICF_OK;
+}
+
 int icf_launch_assembly(icf_ctx *ctx, double h) {
   if (!ctx->use_graph) return enqueue_assembly(ctx, h);
   if (!ctx->graph_exec || ctx->graph_version != ctx->version || ctx->graph_h != h) {

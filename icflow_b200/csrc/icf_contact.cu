@@ -382,7 +382,12 @@ int icf_launch_imp_unit(icf_ctx *ctx, cudaStream_t stream) {
       ctx->n_imp, ctx->d_imp, ctx->d_alt, ctx->d_xc, ctx->prm.DistanceEpsilon * ctx->prm.DistanceEpsilon,
       ctx->d_imp_ci, ctx->d_imp_cd, ctx->d_counts);
   ICF_CUDA(ctx, cudaGetLastError());
-  return icf_launch_imp_deriv(ctx, ctx->d_imp_ci, ctx->d_imp_cd, stream);
+  // ids, four node positions, classification out
+  icf_prof_mark(ctx, stream, "k_imp_classify", 192LL * ctx->n_imp);
+  const int rc = icf_launch_imp_deriv(ctx, ctx->d_imp_ci, ctx->d_imp_cd, stream);
+  // classification and node positions in, 160-double staging record out
+  icf_prof_mark(ctx, stream, "k_imp_deriv", (48LL + 128 + 8 * ICF_IMP_STAGE) * ctx->n_imp);
+  return rc;
 }
 
 // Narrow phase + set expansion + closest face.  Leaves ctx->d_imp /

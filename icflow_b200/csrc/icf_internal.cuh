@@ -92,6 +92,7 @@ struct icf_ctx {
   int N = 0;          // rows of the pattern
   int nnz_s = 0;      // static blocks
   long long n_rc = 0; // static contribution codes
+  long long n_rc_off = 0; // ... of which to off-diagonal blocks
   int nnz = 0;        // merged blocks
   bool have_static = false, have_nodes = false, have_structure = false;
   bool src_identity = true;
@@ -181,7 +182,23 @@ struct icf_ctx {
   // scratch
   void *d_tmp = nullptr;
   size_t tmp_bytes = 0;
+
+  // per-kernel timing (icf_profile_assembly): when set, the assembly runs
+  // on the main stream only and each kernel is followed by an event
+  struct icf_prof_state *prof = nullptr;
 };
+
+#define ICF_PROF_MAX 16
+struct icf_prof_state {
+  int n = 0;
+  const char *name[ICF_PROF_MAX];
+  long long bytes[ICF_PROF_MAX];
+  cudaEvent_t ev[ICF_PROF_MAX + 1];
+};
+// Records the end of the kernel just launched on `s` (no-op unless profiling).
+void icf_prof_mark(icf_ctx *ctx, cudaStream_t s, const char *name, long long bytes);
+int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const char **names,
+                              long long *bytes, double *ms);
 
 // ---- error plumbing ---------------------------------------------------------
 int icf_fail(icf_ctx *ctx, int code, const std::string &msg);

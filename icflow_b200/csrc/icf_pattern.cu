@@ -190,6 +190,24 @@ __global__ void k_desc(int n, const int *__restrict__ slot_of, const int *__rest
   desc[i] = make_int4(identity ? st : s2m[st], rc_off[st], rc_mid[st], rc_off[st + 1]);
 }
 
+// sort key of a gather descriptor: its tet and CZ list lengths, 8 bits each
+__global__ void k_desc_key(int n, const int4 *__restrict__ desc, uint32_t *__restrict__ key) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 d = desc[i];
+  const int nt = d.z - d.y, nc = d.w - d.z;
+  key[i] = (uint32_t)((nt < 255 ? nt : 255) << 8 | (nc < 255 ? nc : 255));
+}
+
+// number of contribution codes of the off-diagonal slots
+__global__ void k_off_codes(int n, const int *__restrict__ offflag, const int *__restrict__ rc_off,
+                            unsigned long long *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long c = (i < n && offflag[i]) ? (unsigned long long)(rc_off[i + 1] - rc_off[i]) : 0ull;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
 __global__ void k_iota(int n, int *__restrict__ a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i;
@@ -445,10 +463,18 @@ int icf_build_static_pattern(icf_ctx *ctx) {
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
     ICF_CUDA(ctx, cub::DeviceSelect::Flagged(ctx->d_tmp, tb, iota, offflag, ctx->d_offd, d_n, nnz_s, s));
     ICF_CUDA(ctx, cudaMemcpyAsync(&ctx->n_offd, d_n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    unsigned long long *d_c;
+    ICF_CUDA(ctx, cudaMallocAsync(&d_c, sizeof(unsigned long long), s));
+    ICF_CUDA(ctx, cudaMemsetAsync(d_c, 0, sizeof(unsigned long long), s));
+    k_off_codes<<<icf_blocks(nnz_s, 256), 256, 0, s>>>(nnz_s, offflag, ctx->d_rc_off, d_c);
+    unsigned long long n_off_codes = 0;
+    ICF_CUDA(ctx, cudaMemcpyAsync(&n_off_codes, d_c, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaFreeAsync(d_c, s));
     ICF_CUDA(ctx, cudaFreeAsync(offflag, s));
     ICF_CUDA(ctx, cudaFreeAsync(iota, s));
     ICF_CUDA(ctx, cudaFreeAsync(d_n, s));
     ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    ctx->n_rc_off = (long long)n_off_codes;
   }
   return ICF_OK;
 }
@@ -559,9 +585,26 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
   if (N > 0)
     k_desc<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_diag, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_s2m,
                                              ident, ctx->d_gdesc_diag);
-  if (ctx->n_offd > 0)
-    k_desc<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_offd, ctx->d_rc_off,
-                                                       ctx->d_rc_mid, ctx->d_s2m, ident, ctx->d_gdesc_off);
+  if (ctx->n_offd > 0) {
+    // Off-diagonal descriptors ordered by (tet count, CZ count), stable, so
+    // the lanes of a gather warp walk lists of equal length.
+    const int no = ctx->n_offd;
+    int4 *d0;
+    uint32_t *k0, *k1;
+    ICF_CUDA(ctx, cudaMallocAsync(&d0, sizeof(int4) * (size_t)no, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&k0, sizeof(uint32_t) * (size_t)no, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&k1, sizeof(uint32_t) * (size_t)no, s));
+    k_desc<<<icf_blocks(no, 256), 256, 0, s>>>(no, ctx->d_offd, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_s2m,
+                                               ident, d0);
+    k_desc_key<<<icf_blocks(no, 256), 256, 0, s>>>(no, d0, k0);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, d0, ctx->d_gdesc_off, no, 0, 16, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, d0, ctx->d_gdesc_off, no, 0, 16, s));
+    ICF_CUDA(ctx, cudaFreeAsync(d0, s));
+    ICF_CUDA(ctx, cudaFreeAsync(k0, s));
+    ICF_CUDA(ctx, cudaFreeAsync(k1, s));
+  }
   if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
   if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
   k_rows<<<icf_blocks((long long)N + 1, 256), 256, 0, s>>>(N, nnz, ctx->d_mkeys, ctx->d_rows);

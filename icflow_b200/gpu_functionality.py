@@ -179,6 +179,14 @@ class GPU_Functionality:
         self.cf.nImpactsActive = cnt.nImpactsActive
         return cnt
 
+    def ProfileAssembly(self, h: float | None = None, reps: int = 10):
+        """Per-kernel mean device time of the assembly (no reference
+        counterpart): list of {name, bytes, ms}."""
+        h = self.cf.TimeStep if h is None else h
+        t = _lib.icf_kernel_times()
+        check(self.ctx, self.lib.icf_profile_assembly(self.ctx, float(h), int(reps), C.byref(t)))
+        return t.as_list()
+
     # -- collisionResponse (:627-676): folded into the assembly --
     def collisionResponse(self):
         return self.cf.nImpactsActive

@@ -185,6 +185,20 @@ int icf_assemble_async(icf_ctx *ctx, double h);
  * buffers or time step change; enable = 0 launches the kernels directly. */
 int icf_set_graph(icf_ctx *ctx, int enable);
 int icf_read_counts(icf_ctx *ctx, icf_counts *counts);
+/* Per-kernel device times of the assembly.  No counterpart in the reference
+ * (icFlow times whole steps on the host).  Runs `reps` assemblies without the
+ * graph, every kernel on the context stream in the graph's order with an event
+ * after it, and returns per kernel its name, its algorithmic bytes per launch
+ * (every input and output item counted once) and its mean device time.  The
+ * outputs of the last run are those of icf_assemble.  Synchronous. */
+#define ICF_MAX_KERNELS 16
+typedef struct icf_kernel_times {
+  int n_kernels;               /* kernels one assembly launches */
+  char name[ICF_MAX_KERNELS][32];
+  long long bytes[ICF_MAX_KERNELS];
+  double ms[ICF_MAX_KERNELS];
+} icf_kernel_times;
+int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out);
 /* Allocation-free assembly.  No counterpart in the reference: icFlow always
  * assembles into buffers its GPU class allocated.  For callers that cannot
  * allocate device memory while they assemble (a host that serves every device

@@ -197,3 +197,24 @@ def test_graph_matches_direct_launch(O):
     o = oracle_assemble(O, p, coll, state, 2 * H, pmax, tmax, imp)
     compare(a, o)
     gf.close()
+
+
+def test_profile_assembly_kernels(O):
+    """Per-kernel timing runs the same kernels: same bits as the graph, every
+    kernel of the step listed with a positive time and byte count."""
+    coll = M.polycrystal(n=6, grains=5, seed=4, platens=True, gap=-0.3)
+    prms = config_prms(penaltyK=1e8)
+    gf = _gf(coll, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    state = random_state(coll, 2, du=1e-6)
+    pairs = M.candidate_pairs(coll, coll.x0 + state[0])
+    a = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+    ks = gf.ProfileAssembly(H, reps=3)
+    names = [k["name"] for k in ks]
+    assert {"k_tet_unit", "k_cz_gp", "k_gather_off", "k_gather_diag", "k_finite"} <= set(names)
+    if len(gf.c_itet):
+        assert {"k_imp_classify", "k_imp_deriv", "k_imp_add"} <= set(names)
+    assert all(k["ms"] > 0 and k["bytes"] > 0 for k in ks)
+    vals, rhs = gf.TransferLinearSystemToHost()
+    assert np.array_equal(vals.ravel(), a["vals"].ravel()) and np.array_equal(rhs.ravel(), a["rhs"].ravel())
+    gf.close()
