@@ -279,6 +279,7 @@ def run_ours(args):
     gf.TransferPCSR(np.zeros((nc, 3)), np.zeros((nc, 3)), np.zeros(nc, np.int32))
     imps = gf.NarrowPhaseCollisionDetection(pairs)
     N, nnz = gf.CreateStructure(copy_back=False)
+    tune = [] if args.no_tune else gf.Autotune(H, reps=10)
     lib = gf.lib
     bufs = gf.DeviceBuffers()
     stream = torch.cuda.ExternalStream(bufs.stream, device=dev)
@@ -365,7 +366,8 @@ def run_ours(args):
             "config": {"workload": workload_name(n, grains),
                        "tets": int(len(coll.elems)), "czs": int(nc), "nodes": int(len(coll.x0)),
                        "active_rows": int(N), "blocks": int(nnz), "impacts": int(len(imps)),
-                       "l2": "flushed between steps (256 MiB write), outside the timed region"},
+                       "l2": "flushed between steps (256 MiB write), outside the timed region",
+                       "launch_variants": {t["kernel"]: t["variant"] for t in tune if t["chosen"]} or "defaults"},
             "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": top_ach, "peak": peak,
                          "unit": "GB/s", "frac": top_ach / peak, "traffic": ncu_traffic(top["name"], args.workload),
                          "algorithmic_bytes": top["bytes"], "launch_ms": top["ms"],
@@ -380,6 +382,7 @@ def run_ours(args):
             "e2e": {"value": ws * 1000.0 / ms_e2e, "unit": "assemblies/s",
                     "h2d_bytes_per_step": int(3 * un.nbytes), "d2h_bytes_per_step": int(8 * (9 * nnz + 3 * N))},
             "gpu_launches": launches_per_step * args.steps,
+            "autotune": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in t.items()} for t in tune],
             "clocks": clocks,
         }
         if not args.no_cpu:
@@ -403,6 +406,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="cfg1", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch variants")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -74,6 +74,16 @@ class icf_kernel_times(C.Structure):
                  "ms": float(self.ms[k])} for k in range(self.n_kernels)]
 
 
+class icf_tune_report(C.Structure):
+    _fields_ = [("n", C.c_int), ("kernel", (C.c_char * 16) * 32), ("variant", (C.c_char * 32) * 32),
+                ("ms", C.c_double * 32), ("chosen", C.c_int * 32)]
+
+    def as_list(self):
+        s = lambda b: bytes(b).split(b"\0")[0].decode()  # noqa: E731
+        return [{"kernel": s(self.kernel[i]), "variant": s(self.variant[i]), "ms": float(self.ms[i]),
+                 "chosen": bool(self.chosen[i])} for i in range(self.n)]
+
+
 class icf_device_buffers(C.Structure):
     _fields_ = [
         ("vals", C.c_void_p), ("rhs", C.c_void_p), ("csr_rows", C.c_void_p),
@@ -112,6 +122,8 @@ SIGNATURES = {
     "icf_set_graph": (I, [P, I]),
     "icf_read_counts": (I, [P, C.POINTER(icf_counts)]),
     "icf_profile_assembly": (I, [P, D, I, C.POINTER(icf_kernel_times)]),
+    "icf_autotune": (I, [P, D, I, C.POINTER(icf_tune_report)]),
+    "icf_set_variant": (I, [P, I, I]),
     "icf_assemble_noalloc": (I, [P, D, P, P, P, P, P, C.POINTER(icf_counts)]),
     "icf_transfer_linear_system": (I, [P, dp, dp]),
     "icf_transfer_updated_state": (I, [P, dp, dp, ip, dp, dp]),

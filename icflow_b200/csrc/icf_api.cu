@@ -198,7 +198,8 @@ static void free_all(icf_ctx *c) {
                   c->d_src, c->d_mkeys, c->d_imp, c->d_cr_slot, c->d_cr_off, c->d_cr, c->d_pairs,
                   c->d_masks, c->d_imp_ci, c->d_imp_cd, c->d_rc_mid, c->d_diag, c->d_offd,
                   c->d_s2m, c->d_dynpos, c->d_gdesc_diag, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
-                  c->imp_inc.off, c->imp_inc.inc, c->d_tmp};
+                  c->imp_inc.off, c->imp_inc.inc, c->d_tmp, c->sell_off.meta, c->sell_off.unit,
+                  c->sell_off.codes, c->sell_diag.meta, c->sell_diag.unit, c->sell_diag.codes};
   for (void *p : ptrs) cudaFree(p);
 }
 
@@ -332,6 +333,8 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->d_cr = nullptr; ctx->cr_cap = 0; ctx->n_crs = 0; ctx->d_pairs = ctx->d_masks = nullptr;
   ctx->pairs_cap = 0; ctx->n_pairs = 0; ctx->d_vals = ctx->d_rhs = ctx->d_nodeF = nullptr; ctx->vals_cap = 0;
   ctx->tet_inc = icf_node_inc(); ctx->imp_inc = icf_node_inc(); ctx->d_tmp = nullptr; ctx->tmp_bytes = 0;
+  ctx->sell_off = icf_sell();
+  ctx->sell_diag = icf_sell();
   ctx->per_cz_prm = false;
   ctx->have_structure = false;
   ctx->have_nodes = false;
@@ -573,6 +576,20 @@ int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out
     out->ms[k] = ms[k];
   }
   return icf_read_counts(ctx, nullptr);
+}
+
+int icf_autotune(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
+  ICF_CHECK_CTX(ctx);
+  if (reps < 1) return icf_fail(ctx, ICF_ERR_ARG, "icf_autotune: reps >= 1");
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  ICF_CUDA(ctx, cudaSetDevice(ctx->device));
+  return icf_autotune_impl(ctx, h, reps, out);
+}
+
+int icf_set_variant(icf_ctx *ctx, int kind, int variant) {
+  ICF_CHECK_CTX(ctx);
+  ICF_CUDA(ctx, cudaSetDevice(ctx->device));
+  return icf_set_variant_impl(ctx, kind, variant);
 }
 
 int icf_set_graph(icf_ctx *ctx, int enable) {

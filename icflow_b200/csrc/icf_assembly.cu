@@ -197,7 +197,8 @@ __device__ __forceinline__ void tet_record(int e, const int4 *__restrict__ elem,
 // shared memory (rows padded to 272 B, so both the row-wise writes and the
 // column-wise reads are free of bank conflicts) and stored as 512 B
 // contiguous chunks per instruction.
-__global__ void __launch_bounds__(128, 3)
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB)
     k_tet_unit(int ne, const int4 *__restrict__ elem,
                const double4 *__restrict__ x0, const double4 *__restrict__ xc,
                const double2 *__restrict__ va, icf_dprm P,
@@ -440,123 +441,6 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK)
   (void)flag;
 }
 
-// ---- the gather ----------------------------------------------------------------
-__device__ __forceinline__ int sym_pair(int i, int j) {
-  // (0,0)0 (0,1)1 (0,2)2 (1,1)3 (1,2)4 (2,2)5
-  const int lo = i < j ? i : j, hi = i < j ? j : i;
-  return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
-}
-
-// Contribution of one tet code to its block (and, for a diagonal block, to the
-// rhs row): LHS_ab = stiffCoeff Df_ab + massCoeff M_ab rebuilt from the
-// staging record (see k_tet_unit).
-__device__ __forceinline__ void add_tet(uint32_t code, const double4 *__restrict__ es, double sc,
-                                        double mc, double lam, double mu, double b[9], double r[3]) {
-  const uint32_t e = (code >> 4) & 0x3FFFFFFu, a = (code >> 2) & 3u, bb = code & 3u;
-  const double4 A = es[8 * (size_t)e + a];
-  const double4 Bv = es[8 * (size_t)e + bb];
-  const double V = A.w;
-  const double ha[3] = {A.x, A.y, A.z}, hb[3] = {Bv.x, Bv.y, Bv.z};
-  const double dot = ha[0] * hb[0] + ha[1] * hb[1] + ha[2] * hb[2];
-  const double c1 = sc * V * lam, c2 = sc * V * mu;
-  const double cd = c2 * dot + mc * V * (a == bb ? 2.0 : 1.0);
-#pragma unroll
-  for (int k = 0; k < 3; k++)
-#pragma unroll
-    for (int l = 0; l < 3; l++) b[3 * k + l] += c1 * ha[k] * hb[l] + c2 * hb[k] * ha[l] + (k == l ? cd : 0.0);
-  if (r != nullptr) {
-    const double4 Rr = es[8 * (size_t)e + 4 + a];
-    r[0] += Rr.x;
-    r[1] += Rr.y;
-    r[2] += Rr.z;
-  }
-}
-
-// Contribution of one CZ code: +-Kt[a mod 3][b mod 3] (symmetric 3x3) and,
-// for a diagonal block, -+rt[a mod 3].
-__device__ __forceinline__ void add_cz(uint32_t code, const double *__restrict__ cs, double b[9],
-                                       double r[3]) {
-  const uint32_t c = (code >> 6) & 0xFFFFFFu, a = (code >> 3) & 7u, bb = code & 7u;
-  const double *S = cs + (size_t)c * ICF_CZ_STAGE;
-  const int ia = a % 3, ib = bb % 3;
-  const double sg = ((a < 3) == (bb < 3)) ? 1.0 : -1.0;
-  const double2 *K2 = reinterpret_cast<const double2 *>(S + 6 * sym_pair(ia, ib));
-  const double2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
-  b[0] += sg * k01.x; b[1] += sg * k01.y; b[2] += sg * k23.x;
-  b[3] += sg * k01.y; b[4] += sg * k23.y; b[5] += sg * k45.x;
-  b[6] += sg * k23.x; b[7] += sg * k45.x; b[8] += sg * k45.y;
-  if (r != nullptr) {
-    const double sa = (a < 3) ? -1.0 : 1.0;
-    r[0] += sa * __ldg(S + 36 + 3 * ia + 0);
-    r[1] += sa * __ldg(S + 36 + 3 * ia + 1);
-    r[2] += sa * __ldg(S + 36 + 3 * ia + 2);
-  }
-}
-
-// Diagonal blocks: four threads per row, each summing every fourth code of the
-// row's diagonal block, combined by a fixed shuffle tree.  Every code of a
-// diagonal block has a == b, so the rhs row is summed alongside.  Tet codes
-// precede CZ codes in each block's list; the two loops keep the kinds apart
-// so lanes do not diverge on the kind.
-__global__ void __launch_bounds__(128)
-    k_gather_diag(int N, const int4 *__restrict__ desc, const uint32_t *__restrict__ rc,
-                  const double4 *__restrict__ es, const double *__restrict__ cs, double sc,
-                  double mc, double lam, double mu, double *__restrict__ vals,
-                  double *__restrict__ rhs) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int row = t >> 2, sub = t & 3;
-  const int4 d = row < N ? desc[row] : make_int4(-1, 0, 0, 0);
-  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, r[3] = {0, 0, 0};
-  if (d.x >= 0) {
-    for (int q = d.y + sub; q < d.z; q += 4) add_tet(__ldg(rc + q), es, sc, mc, lam, mu, b, r);
-    for (int q = d.z + sub; q < d.w; q += 4) add_cz(__ldg(rc + q), cs, b, r);
-  }
-#pragma unroll
-  for (int m = 1; m <= 2; m <<= 1) {
-#pragma unroll
-    for (int k = 0; k < 9; k++) b[k] += __shfl_xor_sync(0xffffffffu, b[k], m);
-#pragma unroll
-    for (int k = 0; k < 3; k++) r[k] += __shfl_xor_sync(0xffffffffu, r[k], m);
-  }
-  if (d.x < 0) return;
-  if (sub == 0) {
-    double *o = vals + 9 * (size_t)d.x;
-#pragma unroll
-    for (int k = 0; k < 9; k++) o[k] = b[k];
-  } else if (sub == 1) {
-    rhs[3 * (size_t)row + 0] = r[0];
-    rhs[3 * (size_t)row + 1] = r[1];
-    rhs[3 * (size_t)row + 2] = r[2];
-  }
-}
-
-// Off-diagonal blocks: one thread per block of the compacted list, so the
-// lanes of a warp have lists of similar length (about three tets each).  The
-// codes are loaded ahead of the staging records they point to.
-__global__ void __launch_bounds__(256, 4)
-    k_gather_off(int n_off, const int4 *__restrict__ desc, const uint32_t *__restrict__ rc,
-                 const double4 *__restrict__ es, const double *__restrict__ cs, double sc,
-                 double mc, double lam, double mu, double *__restrict__ vals) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_off) return;
-  const int4 d = desc[i];
-  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  int q = d.y;
-  for (; q + 4 <= d.z; q += 4) {
-    const uint32_t c0 = __ldg(rc + q), c1 = __ldg(rc + q + 1), c2 = __ldg(rc + q + 2),
-                   c3 = __ldg(rc + q + 3);
-    add_tet(c0, es, sc, mc, lam, mu, b, nullptr);
-    add_tet(c1, es, sc, mc, lam, mu, b, nullptr);
-    add_tet(c2, es, sc, mc, lam, mu, b, nullptr);
-    add_tet(c3, es, sc, mc, lam, mu, b, nullptr);
-  }
-  for (; q < d.z; q++) add_tet(__ldg(rc + q), es, sc, mc, lam, mu, b, nullptr);
-  for (q = d.z; q < d.w; q++) add_cz(__ldg(rc + q), cs, b, nullptr);
-  double *o = vals + 9 * (size_t)d.x;
-#pragma unroll
-  for (int k = 0; k < 9; k++) o[k] = b[k];
-}
-
 // Blocks that only contact pairs create start at zero.
 __global__ void k_zero_dyn(int nd, const int *__restrict__ pos, double *__restrict__ vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -742,6 +626,31 @@ __global__ void k_commit_cz(int nc, const double *__restrict__ tent,
 
 }  // namespace
 
+namespace {
+struct tet_variant {
+  const char *name;
+  void (*fn)(int, const int4 *, const double4 *, const double4 *, const double2 *, icf_dprm, double4 *);
+};
+const tet_variant TET_VARIANTS[] = {
+    {"t128 minb3", k_tet_unit<3>},
+    {"t128 minb2", k_tet_unit<2>},
+    {"t128 minb4", k_tet_unit<4>},
+};
+constexpr int N_TET = sizeof(TET_VARIANTS) / sizeof(TET_VARIANTS[0]);
+}  // namespace
+
+int icf_tet_variants() { return N_TET; }
+const char *icf_tet_variant_name(int v) { return TET_VARIANTS[v].name; }
+int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *va, double4 *es, cudaStream_t s) {
+  if (ctx->n_elem <= 0) return ICF_OK;
+  if (variant < 0 || variant >= N_TET) variant = 0;
+  const icf_dprm P = icf_make_dprm(ctx);
+  TET_VARIANTS[variant].fn<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0, xc,
+                                                                       va, P, es);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
 // ---- host launchers --------------------------------------------------------------
 // One assembly as a fork/join DAG over three streams:
 //   main : memsets | tets ............ | wait CZ -> diagonal gather | join -> contact add, checks
@@ -774,8 +683,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
 
   // main: tets
   if (ctx->n_elem > 0)
-    k_tet_unit<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0,
-                                                          ctx->d_xc, ctx->d_va, P, ctx->d_es);
+    ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, ctx->d_xc, ctx->d_va, ctx->d_es, s));
   // ids, node state (x0, x_t, v, a) once, 256 B record out
   if (ctx->n_elem > 0) icf_prof_mark(ctx, s, "k_tet_unit", 272LL * ctx->n_elem + 112LL * ctx->n_nodes);
   ICF_CUDA(ctx, cudaEventRecord(e_tet, s));
@@ -810,23 +718,21 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   // aux0: off-diagonal blocks once the tets are staged
   ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_tet, 0));
   if (ctx->n_offd > 0)
-    k_gather_off<<<icf_blocks(ctx->n_offd, 256), 256, 0, sa>>>(ctx->n_offd, ctx->d_gdesc_off, ctx->d_rc,
-                                                              ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu,
-                                                              ctx->d_vals);
+    ICF_TRY_RC(icf_launch_gather_off(ctx, ctx->tune_off, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals,
+                                     sa));
   // descriptors, codes, the h records of every tet and the CZ staging once,
   // blocks out
   if (ctx->n_offd > 0)
-    icf_prof_mark(ctx, sa, "k_gather_off", 88LL * ctx->n_offd + 4LL * ctx->n_rc_off + 128LL * ctx->n_elem +
+    icf_prof_mark(ctx, sa, "k_gather_off", 80LL * ctx->n_offd + 4LL * ctx->n_rc_off + 128LL * ctx->n_elem +
                                                8LL * ICF_CZ_STAGE * ctx->n_cz);
   ICF_CUDA(ctx, cudaEventRecord(e_a, sa));
   // main: diagonal blocks and rhs once the CZs are staged
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
   if (ctx->N > 0)
-    k_gather_diag<<<icf_blocks(4LL * ctx->N, 128), 128, 0, s>>>(ctx->N, ctx->d_gdesc_diag, ctx->d_rc,
-                                                              ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu,
-                                                              ctx->d_vals, ctx->d_rhs);
+    ICF_TRY_RC(icf_launch_gather_diag(ctx, ctx->tune_diag, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals,
+                                      ctx->d_rhs, s));
   if (ctx->N > 0)
-    icf_prof_mark(ctx, s, "k_gather_diag", 112LL * ctx->N + 4LL * (ctx->n_rc - ctx->n_rc_off) +
+    icf_prof_mark(ctx, s, "k_gather_diag", 104LL * ctx->N + 4LL * (ctx->n_rc - ctx->n_rc_off) +
                                                256LL * ctx->n_elem + 8LL * ICF_CZ_STAGE * ctx->n_cz);
   // join
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
@@ -990,8 +896,7 @@ int icf_enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cud
   k_pack_nodes<<<icf_blocks(ctx->n_nodes, 256), 256, 0, s>>>(ctx->n_nodes, ctx->d_x0, B.un, B.vn, B.an,
                                                             B.xc, B.va);
   if (ctx->n_elem > 0)
-    k_tet_unit<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0, B.xc,
-                                                          B.va, P, B.es);
+    ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, B.xc, B.va, B.es, s));
   if (ctx->n_cz > 0) {
     icf_law_c LC;
     LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
@@ -1016,11 +921,9 @@ int icf_enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cud
   if (ctx->n_dyn > 0)
     k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, s>>>(ctx->n_dyn, ctx->d_dynpos, B.vals);
   if (ctx->n_offd > 0)
-    k_gather_off<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_gdesc_off, ctx->d_rc, B.es,
-                                                             B.cs, sc, mc, P.lam, P.mu, B.vals);
+    ICF_TRY_RC(icf_launch_gather_off(ctx, ctx->tune_off, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, s));
   if (ctx->N > 0)
-    k_gather_diag<<<icf_blocks(4LL * ctx->N, 128), 128, 0, s>>>(ctx->N, ctx->d_gdesc_diag, ctx->d_rc, B.es,
-                                                              B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs);
+    ICF_TRY_RC(icf_launch_gather_diag(ctx, ctx->tune_diag, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs, s));
   if (ctx->n_crs > 0)
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
                                                         ctx->d_cols, B.ks, B.vals, B.rhs);

@@ -53,6 +53,24 @@ __host__ __device__ inline uint32_t icf_code_cz(uint32_t u, uint32_t a,
   return (ICF_KIND_CZ << 30) | (u << 6) | (a << 3) | b;
 }
 
+// Sliced-ELL contribution lists of a gather.  The units (blocks, or rows
+// for the diagonal gather) are ordered by (window of 2^wl consecutive units,
+// tet-code count, CZ-code count) and cut into slices of 32 / lanes units;
+// `lanes` threads serve a unit.  Slice s keeps meta[s] = {first code, tet
+// iterations, CZ iterations, 0}; iteration k of lane l reads
+// codes[meta.x + 32 k + l] (one coalesced 128 B load per warp), the tet
+// iterations first.  Lane sub of a unit takes its codes sub, sub + lanes, ...;
+// missing ones are ICF_CODE_PAD.  unit[u] = {output block, row or -1}.
+#define ICF_CODE_PAD 0xFFFFFFFFu
+struct icf_sell {
+  int lanes = 1;
+  int n_units = 0, n_slices = 0, slices_cap = 0;
+  long long n_codes = 0, codes_cap = 0;
+  int4 *meta = nullptr;
+  int2 *unit = nullptr;
+  uint32_t *codes = nullptr;
+};
+
 // Parameters the kernels read, passed by value (they live in the kernel
 // parameter bank, i.e. constant memory).
 struct icf_dprm {
@@ -144,6 +162,8 @@ struct icf_ctx {
   // N per-row diagonal entries, then one per off-diagonal block (one buffer)
   int4 *d_gdesc_diag = nullptr, *d_gdesc_off = nullptr;
   int gdesc_cap = 0;
+  // the gathers' sliced-ELL code lists (built from the descriptors)
+  icf_sell sell_off, sell_diag;
 
   // merged pattern
   int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;
@@ -186,6 +206,8 @@ struct icf_ctx {
   // per-kernel timing (icf_profile_assembly): when set, the assembly runs
   // on the main stream only and each kernel is followed by an event
   struct icf_prof_state *prof = nullptr;
+  // launch variants chosen by the autotuner (indices into the variant tables)
+  int tune_tet = 0, tune_off = 0, tune_diag = 0;
 };
 
 #define ICF_PROF_MAX 16
@@ -197,6 +219,22 @@ struct icf_prof_state {
 };
 // Records the end of the kernel just launched on `s` (no-op unless profiling).
 void icf_prof_mark(icf_ctx *ctx, cudaStream_t s, const char *name, long long bytes);
+// gathers (icf_gather.cu): variant tables and launchers
+int icf_gather_variants(int kind);  // kind 0 off-diagonal, 1 diagonal
+const char *icf_gather_variant_name(int kind, int v);
+int icf_gather_variant_lanes(int v);  // lanes per row of diagonal variant v
+int icf_launch_gather_off(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc, double mc,
+                          double lam, double mu, double *vals, cudaStream_t s);
+int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc,
+                           double mc, double lam, double mu, double *vals, double *rhs, cudaStream_t s);
+// tet kernel variants (icf_assembly.cu)
+int icf_tet_variants();
+const char *icf_tet_variant_name(int v);
+int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *va, double4 *es, cudaStream_t s);
+// rebuilds the diagonal gather lists for `lanes` lanes per row (icf_pattern.cu)
+int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes);
+int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out);
+int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant);
 int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const char **names,
                               long long *bytes, double *ms);
 
@@ -211,6 +249,11 @@ int icf_fail(icf_ctx *ctx, int code, const std::string &msg);
   } while (0)
 
 int icf_scratch(icf_ctx *ctx, size_t bytes);
+#define ICF_TRY_RC(call)        \
+  do {                          \
+    const int rc_ = (call);     \
+    if (rc_ != ICF_OK) return rc_; \
+  } while (0)
 
 inline unsigned icf_blocks(long long n, int bs) {
   return (unsigned)((n + bs - 1) / bs);

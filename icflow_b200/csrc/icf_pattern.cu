@@ -190,13 +190,75 @@ __global__ void k_desc(int n, const int *__restrict__ slot_of, const int *__rest
   desc[i] = make_int4(identity ? st : s2m[st], rc_off[st], rc_mid[st], rc_off[st + 1]);
 }
 
-// sort key of a gather descriptor: its tet and CZ list lengths, 8 bits each
-__global__ void k_desc_key(int n, const int4 *__restrict__ desc, uint32_t *__restrict__ key) {
+// ---- sliced-ELL gather lists (see icf_sell) ---------------------------------
+// sort key of unit i: its window, then its per-lane tet and CZ iteration counts
+__global__ void k_sell_key(int n, int wl, int lanes, const int4 *__restrict__ desc,
+                           uint32_t *__restrict__ key, int *__restrict__ idx) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int4 d = desc[i];
-  const int nt = d.z - d.y, nc = d.w - d.z;
-  key[i] = (uint32_t)((nt < 255 ? nt : 255) << 8 | (nc < 255 ? nc : 255));
+  int mt = d.x >= 0 ? (d.z - d.y + lanes - 1) / lanes : 0;
+  int mc = d.x >= 0 ? (d.w - d.z + lanes - 1) / lanes : 0;
+  mt = mt < 255 ? mt : 255;
+  mc = mc < 255 ? mc : 255;
+  key[i] = (uint32_t)(i >> wl) << 16 | (uint32_t)mt << 8 | (uint32_t)mc;
+  idx[i] = i;
+}
+
+// one warp per slice: iteration counts (the slice's maxima) and unit table
+__global__ void k_sell_count(int n, int n_slices, int lanes, const int *__restrict__ perm,
+                             const int4 *__restrict__ desc, int with_row, int4 *__restrict__ meta,
+                             int *__restrict__ cnt, int2 *__restrict__ unit) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n_slices) return;
+  const int per = 32 / lanes;
+  const int j = lane / lanes, sub = lane % lanes;
+  const int u = w * per + j;
+  int mt = 0, mc = 0;
+  int2 un = make_int2(-1, -1);
+  if (u < n) {
+    const int i = perm[u];
+    const int4 d = desc[i];
+    if (d.x >= 0) {
+      mt = (d.z - d.y + lanes - 1) / lanes;
+      mc = (d.w - d.z + lanes - 1) / lanes;
+    }
+    un = make_int2(d.x, with_row ? i : -1);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mt = max(mt, __shfl_xor_sync(0xffffffffu, mt, o));
+    mc = max(mc, __shfl_xor_sync(0xffffffffu, mc, o));
+  }
+  if (sub == 0) unit[w * per + j] = un;
+  if (lane == 0) {
+    meta[w] = make_int4(0, mt, mc, 0);
+    cnt[w] = 32 * (mt + mc);
+  }
+}
+
+__global__ void k_sell_fill(int n, int n_slices, int lanes, const int *__restrict__ perm,
+                            const int4 *__restrict__ desc, const int *__restrict__ off,
+                            const uint32_t *__restrict__ rc, int4 *__restrict__ meta,
+                            uint32_t *__restrict__ codes) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n_slices) return;
+  const int per = 32 / lanes;
+  const int j = lane / lanes, sub = lane % lanes;
+  const int u = w * per + j;
+  int4 d = make_int4(-1, 0, 0, 0);
+  if (u < n) d = desc[perm[u]];
+  const int4 m = meta[w];
+  const long long o = off[w];
+  const int nt = d.x >= 0 ? d.z - d.y : 0, nc = d.x >= 0 ? d.w - d.z : 0;
+  for (int k = 0; k < m.y; k++) {
+    const int q = k * lanes + sub;
+    codes[o + 32LL * k + lane] = q < nt ? rc[d.y + q] : ICF_CODE_PAD;
+  }
+  for (int k = 0; k < m.z; k++) {
+    const int q = k * lanes + sub;
+    codes[o + 32LL * (m.y + k) + lane] = q < nc ? rc[d.z + q] : ICF_CODE_PAD;
+  }
+  if (lane == 0) meta[w].x = (int)o;
 }
 
 // number of contribution codes of the off-diagonal slots
@@ -479,6 +541,72 @@ int icf_build_static_pattern(icf_ctx *ctx) {
   return ICF_OK;
 }
 
+// Builds the sliced-ELL lists of a gather from its descriptors (n units).
+static int build_sell(icf_ctx *ctx, const int4 *desc, int n, int wl, bool with_row, icf_sell *S,
+                      cudaStream_t s) {
+  const int per = 32 / S->lanes;
+  S->n_units = n;
+  S->n_slices = (n + per - 1) / per;
+  S->n_codes = 0;
+  if (n == 0) return ICF_OK;
+  const int ns = S->n_slices;
+  if (ns > S->slices_cap || !S->meta) {
+    cudaFree(S->meta);
+    cudaFree(S->unit);
+    S->meta = nullptr;
+    S->unit = nullptr;
+    const int cap = ns + ns / 4 + 16;
+    ICF_CUDA(ctx, cudaMalloc(&S->meta, sizeof(int4) * (size_t)cap));
+    ICF_CUDA(ctx, cudaMalloc(&S->unit, sizeof(int2) * (size_t)cap * per));
+    S->slices_cap = cap;
+  }
+  uint32_t *k0, *k1;
+  int *i0, *perm, *cnt, *off;
+  ICF_CUDA(ctx, cudaMallocAsync(&k0, sizeof(uint32_t) * (size_t)n, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&k1, sizeof(uint32_t) * (size_t)n, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&i0, sizeof(int) * (size_t)n, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&perm, sizeof(int) * (size_t)n, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&cnt, sizeof(int) * (size_t)(ns + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&off, sizeof(int) * (size_t)(ns + 1), s));
+  k_sell_key<<<icf_blocks(n, 256), 256, 0, s>>>(n, wl, S->lanes, desc, k0, i0);
+  int end_bit = 16;
+  while ((((long long)n - 1) >> wl) >> (end_bit - 16)) end_bit++;
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, i0, perm, n, 0, end_bit, s);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, i0, perm, n, 0, end_bit, s));
+  ICF_CUDA(ctx, cudaMemsetAsync(S->unit, 0xff, sizeof(int2) * (size_t)ns * per, s));
+  k_sell_count<<<icf_blocks(32LL * ns, 256), 256, 0, s>>>(n, ns, S->lanes, perm, desc, with_row ? 1 : 0,
+                                                         S->meta, cnt, S->unit);
+  ICF_CUDA(ctx, cudaMemsetAsync(cnt + ns, 0, sizeof(int), s));
+  tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, ns + 1, s);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, cnt, off, ns + 1, s));
+  int total = 0;
+  ICF_CUDA(ctx, cudaMemcpyAsync(&total, off + ns, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  if (total < 0) return icf_fail(ctx, ICF_ERR_SIZE, "gather code list exceeds 2^31 entries");
+  if (total > S->codes_cap || !S->codes) {
+    cudaFree(S->codes);
+    S->codes = nullptr;
+    const long long cap = (long long)total + total / 4 + 32;
+    ICF_CUDA(ctx, cudaMalloc(&S->codes, sizeof(uint32_t) * (size_t)cap));
+    S->codes_cap = cap;
+  }
+  k_sell_fill<<<icf_blocks(32LL * ns, 256), 256, 0, s>>>(n, ns, S->lanes, perm, desc, off, ctx->d_rc, S->meta,
+                                                        S->codes);
+  ICF_CUDA(ctx, cudaGetLastError());
+  S->n_codes = total;
+  ICF_CUDA(ctx, cudaFreeAsync(k0, s));
+  ICF_CUDA(ctx, cudaFreeAsync(k1, s));
+  ICF_CUDA(ctx, cudaFreeAsync(i0, s));
+  ICF_CUDA(ctx, cudaFreeAsync(perm, s));
+  ICF_CUDA(ctx, cudaFreeAsync(cnt, s));
+  ICF_CUDA(ctx, cudaFreeAsync(off, s));
+  return ICF_OK;
+}
+
 template <typename T>
 static int grow(icf_ctx *ctx, T **p, int *cap, long long n) {
   if (n <= *cap && *p) return ICF_OK;
@@ -585,26 +713,13 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
   if (N > 0)
     k_desc<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_diag, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_s2m,
                                              ident, ctx->d_gdesc_diag);
-  if (ctx->n_offd > 0) {
-    // Off-diagonal descriptors ordered by (tet count, CZ count), stable, so
-    // the lanes of a gather warp walk lists of equal length.
-    const int no = ctx->n_offd;
-    int4 *d0;
-    uint32_t *k0, *k1;
-    ICF_CUDA(ctx, cudaMallocAsync(&d0, sizeof(int4) * (size_t)no, s));
-    ICF_CUDA(ctx, cudaMallocAsync(&k0, sizeof(uint32_t) * (size_t)no, s));
-    ICF_CUDA(ctx, cudaMallocAsync(&k1, sizeof(uint32_t) * (size_t)no, s));
-    k_desc<<<icf_blocks(no, 256), 256, 0, s>>>(no, ctx->d_offd, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_s2m,
-                                               ident, d0);
-    k_desc_key<<<icf_blocks(no, 256), 256, 0, s>>>(no, d0, k0);
-    size_t tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, d0, ctx->d_gdesc_off, no, 0, 16, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, d0, ctx->d_gdesc_off, no, 0, 16, s));
-    ICF_CUDA(ctx, cudaFreeAsync(d0, s));
-    ICF_CUDA(ctx, cudaFreeAsync(k0, s));
-    ICF_CUDA(ctx, cudaFreeAsync(k1, s));
-  }
+  if (ctx->n_offd > 0)
+    k_desc<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_offd, ctx->d_rc_off,
+                                                       ctx->d_rc_mid, ctx->d_s2m, ident, ctx->d_gdesc_off);
+  ctx->sell_off.lanes = 1;
+  ctx->sell_diag.lanes = icf_gather_variant_lanes(ctx->tune_diag);
+  if (build_sell(ctx, ctx->d_gdesc_off, ctx->n_offd, 12, false, &ctx->sell_off, s)) return ICF_ERR_CUDA;
+  if (build_sell(ctx, ctx->d_gdesc_diag, N, 10, true, &ctx->sell_diag, s)) return ICF_ERR_CUDA;
   if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
   if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
   k_rows<<<icf_blocks((long long)N + 1, 256), 256, 0, s>>>(N, nnz, ctx->d_mkeys, ctx->d_rows);
@@ -707,5 +822,14 @@ int icf_launch_pcsr(icf_ctx *ctx, int kind, int *d_out) {
     k_pcsr<<<icf_blocks(ctx->n_imp, 128), 128, 0, s>>>(ctx->n_imp, 4, reinterpret_cast<const int *>(ctx->d_imp),
                                                       4, ctx->d_alt, ctx->d_mkeys, ctx->nnz, d_out);
   ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
+int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes) {
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  ctx->sell_diag.lanes = lanes;
+  const int wl = lanes >= 4 ? 10 : 11;
+  if (build_sell(ctx, ctx->d_gdesc_diag, ctx->N, wl, true, &ctx->sell_diag, ctx->stream)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ICF_OK;
 }

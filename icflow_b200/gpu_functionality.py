@@ -187,6 +187,17 @@ class GPU_Functionality:
         check(self.ctx, self.lib.icf_profile_assembly(self.ctx, float(h), int(reps), C.byref(t)))
         return t.as_list()
 
+    def Autotune(self, h: float | None = None, reps: int = 10):
+        """Times every launch variant of the tet kernel and the gathers on this
+        model and keeps the fastest (no reference counterpart)."""
+        h = self.cf.TimeStep if h is None else h
+        r = _lib.icf_tune_report()
+        check(self.ctx, self.lib.icf_autotune(self.ctx, float(h), int(reps), C.byref(r)))
+        return r.as_list()
+
+    def SetVariant(self, kind: int, variant: int):
+        check(self.ctx, self.lib.icf_set_variant(self.ctx, int(kind), int(variant)))
+
     # -- collisionResponse (:627-676): folded into the assembly --
     def collisionResponse(self):
         return self.cf.nImpactsActive

@@ -199,6 +199,26 @@ typedef struct icf_kernel_times {
   double ms[ICF_MAX_KERNELS];
 } icf_kernel_times;
 int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out);
+/* Launch-variant autotuner.  No counterpart in the reference (its kernels run
+ * one thread per unit in blocks of 128, GPU_Functionality.cs:38).  The tet
+ * kernel and the two gathers each have several launch variants that compute
+ * the same values (registers per thread, codes per iteration, loads through
+ * registers or cp.async, lanes per row of the diagonal gather).  icf_autotune
+ * times every variant on the current model (`reps` launches each, device
+ * events), keeps the fastest of each kind for the following assemblies and
+ * reports all timings.  Needs a structure; leaves the outputs of a complete
+ * assembly behind.  icf_set_variant pins one variant by index (kind 0 tet,
+ * 1 off-diagonal gather, 2 diagonal gather). */
+#define ICF_MAX_TUNE 32
+typedef struct icf_tune_report {
+  int n;                          /* candidates timed */
+  char kernel[ICF_MAX_TUNE][16];
+  char variant[ICF_MAX_TUNE][32];
+  double ms[ICF_MAX_TUNE];        /* mean device time per launch */
+  int chosen[ICF_MAX_TUNE];       /* 1 for the variant kept */
+} icf_tune_report;
+int icf_autotune(icf_ctx *ctx, double h, int reps, icf_tune_report *out);
+int icf_set_variant(icf_ctx *ctx, int kind, int variant);
 /* Allocation-free assembly.  No counterpart in the reference: icFlow always
  * assembles into buffers its GPU class allocated.  For callers that cannot
  * allocate device memory while they assemble (a host that serves every device

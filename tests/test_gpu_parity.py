@@ -218,3 +218,46 @@ def test_profile_assembly_kernels(O):
     vals, rhs = gf.TransferLinearSystemToHost()
     assert np.array_equal(vals.ravel(), a["vals"].ravel()) and np.array_equal(rhs.ravel(), a["rhs"].ravel())
     gf.close()
+
+
+def test_every_launch_variant_and_autotune(O):
+    """Each launch variant of the tet kernel and of both gathers gives blocks
+    and rhs within the FP64 bar against the oracle; the autotuner reports a
+    timing for every variant and keeps one of each kind."""
+    from icflow_b200 import _lib
+
+    coll = M.polycrystal(n=6, grains=5, seed=4, platens=True, gap=-0.3)
+    prms = config_prms(penaltyK=1e8)
+    gf = _gf(coll, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    state = random_state(coll, 3, du=1e-6)
+    pairs = M.candidate_pairs(coll, coll.x0 + state[0])
+    ref = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+    p = orc_prms_from(O, prms)
+    o = oracle_assemble(O, p, coll, state, H, pmax, tmax, gf.c_itet)
+    compare(ref, o)
+    lib = _lib.load()
+    counts = {}
+    for kind in range(3):
+        v = 0
+        while lib.icf_set_variant(gf.ctx, kind, v) == 0:
+            gf.AssembleElemsAndCZs(H)
+            vals, rhs = gf.TransferLinearSystemToHost()
+            assert rowwise_rel(o["rows"], o["vals"], vals.reshape(-1, 3, 3)) <= FP64_TOL, (kind, v)
+            assert vec_rel(o["rhs"], rhs) <= FP64_TOL, (kind, v)
+            v += 1
+        counts[kind] = v
+        _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, 0))
+    assert all(n >= 2 for n in counts.values()), counts
+    rep = gf.Autotune(H, reps=3)
+    kinds = {r["kernel"] for r in rep}
+    assert kinds == {"k_tet_unit", "k_gather_off", "k_gather_diag"}
+    assert len(rep) == sum(counts.values())
+    for k in kinds:
+        assert sum(r["chosen"] for r in rep if r["kernel"] == k) == 1
+    vals, rhs = gf.TransferLinearSystemToHost()
+    assert rowwise_rel(o["rows"], o["vals"], vals.reshape(-1, 3, 3)) <= FP64_TOL
+    gf.AssembleElemsAndCZs(H)
+    vals2, rhs2 = gf.TransferLinearSystemToHost()
+    assert np.array_equal(vals, vals2) and np.array_equal(rhs, rhs2)
+    gf.close()
