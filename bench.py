@@ -271,6 +271,7 @@ def run_ours(args):
     gf.prms = prms
     gf.mc = coll
     gf.SetConstants()
+    gf.SetPrecision(1 if args.precision == "mixed" else 0)
     gf.TransferStaticDataToDevice()
     gf.SetCZStrengths(sig, sig)
     un, vn, an = state
@@ -361,7 +362,8 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": ws * 1000.0 / ms_dev, "unit": "assemblies/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 Hessians, f64 rotation/law/rhs/accumulation",
             "data": "synthetic (seeded polycrystal; no public dataset exists for this path)",
             "config": {"workload": workload_name(n, grains),
                        "tets": int(len(coll.elems)), "czs": int(nc), "nodes": int(len(coll.x0)),
@@ -407,6 +409,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="cfg1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch variants")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="fp64, or FP32 Hessian arithmetic with FP64 rotation, law, rhs and accumulation")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

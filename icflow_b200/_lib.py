@@ -123,6 +123,18 @@ SIGNATURES = {
     "icf_read_counts": (I, [P, C.POINTER(icf_counts)]),
     "icf_profile_assembly": (I, [P, D, I, C.POINTER(icf_kernel_times)]),
     "icf_autotune": (I, [P, D, I, C.POINTER(icf_tune_report)]),
+    "icf_solve": (I, [P, D, I, P, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "icf_apply_dx": (I, [P, C.POINTER(C.c_double)]),
+    "icf_residual_norm": (I, [P, C.POINTER(C.c_double)]),
+    "icf_mlp_create": (I, [I, C.POINTER(P)]),
+    "icf_mlp_destroy": (I, [P]),
+    "icf_mlp_last_error": (C.c_char_p, [P]),
+    "icf_mlp_param_count": (I, []),
+    "icf_mlp_set_params": (I, [P, P, P]),
+    "icf_mlp_get_params": (I, [P, P, P]),
+    "icf_mlp_forward": (I, [P, I, P, P]),
+    "icf_mlp_grad": (I, [P, I, P, P, P, C.POINTER(C.c_float)]),
+    "icf_mlp_train": (I, [P, I, P, P, I, I, C.c_float, C.c_ulonglong, C.POINTER(C.c_float)]),
     "icf_set_variant": (I, [P, I, I]),
     "icf_assemble_noalloc": (I, [P, D, P, P, P, P, P, C.POINTER(icf_counts)]),
     "icf_transfer_linear_system": (I, [P, dp, dp]),

@@ -191,6 +191,7 @@ int icf_create(int device, icf_ctx **out) {
 }
 
 static void free_all(icf_ctx *c) {
+  icf_free_solver(c);
   void *ptrs[] = {c->d_elem, c->d_cz, c->d_alt, c->d_selem, c->d_adj_off, c->d_adj, c->d_faces,
                   c->d_x0, c->d_xc, c->d_va, c->d_u, c->d_v, c->d_a, c->d_du, c->d_un, c->d_h3,
                   c->d_czs, c->d_czfail, c->d_cztent, c->d_czflags, c->d_czavg, c->d_czprm,
@@ -199,7 +200,7 @@ static void free_all(icf_ctx *c) {
                   c->d_masks, c->d_imp_ci, c->d_imp_cd, c->d_rc_mid, c->d_diag, c->d_offd,
                   c->d_s2m, c->d_dynpos, c->d_gdesc_diag, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
                   c->imp_inc.off, c->imp_inc.inc, c->d_tmp, c->sell_off.meta, c->sell_off.unit,
-                  c->sell_off.codes, c->sell_diag.meta, c->sell_diag.unit, c->sell_diag.codes};
+                  c->sell_off.codes, c->sell_diag.meta, c->sell_diag.unit, c->sell_diag.codes, c->d_czhist};
   for (void *p : ptrs) cudaFree(p);
 }
 
@@ -232,6 +233,7 @@ int icf_set_constants(icf_ctx *ctx, const icf_params *p) {
     return icf_fail(ctx, ICF_ERR_ARG, "parameters give a degenerate PPR law or Newmark scheme");
   ctx->prm = q;
   ctx->have_prm = true;
+  ctx->hist_valid = false;
   ctx->version++;
   // PPR axis factors at zero opening (the law's constant evaluations)
   const double ax[2][4] = {{q.alpha, q.p_m, q.gam_n, q.pMnt}, {q.beta, q.p_n, q.gam_t, q.pMtn}};
@@ -260,6 +262,7 @@ int icf_set_cz_strength(icf_ctx *ctx, int n_czs, const double *sigma_max, const 
   if (!ctx->have_prm) return icf_fail(ctx, ICF_ERR_STATE, "icf_set_constants first");
   if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
   ctx->version++;
+  ctx->hist_valid = false;
   if (!sigma_max || !tau_max) {
     ctx->per_cz_prm = false;
     return ICF_OK;
@@ -335,6 +338,8 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->tet_inc = icf_node_inc(); ctx->imp_inc = icf_node_inc(); ctx->d_tmp = nullptr; ctx->tmp_bytes = 0;
   ctx->sell_off = icf_sell();
   ctx->sell_diag = icf_sell();
+  ctx->d_czhist = nullptr;
+  ctx->hist_valid = false;
   ctx->per_cz_prm = false;
   ctx->have_structure = false;
   ctx->have_nodes = false;
@@ -369,6 +374,7 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ICF_TRY(dalloc(ctx, &ctx->d_czflags, (size_t)n_czs));
   ICF_TRY(dalloc(ctx, &ctx->d_czavg, 4 * (size_t)n_czs));
   ICF_TRY(dalloc(ctx, &ctx->d_cs, ICF_CZ_STAGE * (size_t)n_czs));
+  ICF_TRY(dalloc(ctx, &ctx->d_czhist, 18 * (size_t)n_czs));
 
   std::vector<double4> hx(n);
   for (size_t i = 0; i < n; i++) hx[i] = make_double4(x0[3 * i], x0[3 * i + 1], x0[3 * i + 2], 0.0);
@@ -432,6 +438,7 @@ int icf_transfer_cz_state(icf_ctx *ctx, int n_czs, const double *pmax, const dou
   ICF_CHECK_CTX(ctx);
   if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
   if (n_czs != ctx->n_cz || !pmax || !tmax || !failed) return icf_fail(ctx, ICF_ERR_ARG, "bad CZ arrays");
+  ctx->hist_valid = false;
   std::vector<double> h(8 * (size_t)n_czs, 0.0);
   for (int c = 0; c < n_czs; c++)
     for (int i = 0; i < 3; i++) {
@@ -511,6 +518,7 @@ int icf_create_structure(icf_ctx *ctx, int *N, int *nnz) {
   if (!ctx->d_skeys) ICF_TRY(icf_build_static_pattern(ctx));
   ICF_TRY(icf_build_merged_pattern(ctx));
   ctx->have_structure = true;
+  ctx->struct_gen++;
   ctx->version++;
   if (N) *N = ctx->N;
   if (nnz) *nnz = ctx->nnz;
@@ -739,6 +747,45 @@ int icf_add_dx(icf_ctx *ctx, const double *dx, double *norm) {
   double *d = ctx->d_h3;  // 9 * n_nodes >= 3 * N
   ICF_CUDA(ctx, cudaMemcpyAsync(d, dx, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyHostToDevice, s));
   ICF_TRY(icf_launch_add_dx(ctx, d));
+  ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_norm, ctx->d_norm, sizeof(double), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  if (norm) *norm = ctx->h_norm[0];
+  return ICF_OK;
+}
+
+int icf_solve(icf_ctx *ctx, double rel_tol, int max_iter, double *dx, int *iters, double *relres) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure and icf_assemble first");
+  if (!(rel_tol > 0) || max_iter < 1) return icf_fail(ctx, ICF_ERR_ARG, "rel_tol > 0 and max_iter >= 1");
+  ICF_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (ctx->N == 0) {
+    if (iters) *iters = 0;
+    if (relres) *relres = 0;
+    return ICF_OK;
+  }
+  const int rc = icf_solve_impl(ctx, rel_tol, max_iter, iters, relres);
+  if (rc) return rc;
+  if (dx)
+    ICF_CUDA(ctx, cudaMemcpy(dx, ctx->solver.x, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyDeviceToHost));
+  return ICF_OK;
+}
+
+int icf_residual_norm(icf_ctx *ctx, double *norm2) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_structure || !norm2) return icf_fail(ctx, ICF_ERR_STATE, "icf_assemble first; norm2 required");
+  cudaStream_t s = ctx->stream;
+  ICF_TRY(icf_launch_sumsq(ctx, ctx->d_rhs, 3LL * ctx->N));
+  ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_norm, ctx->d_norm, sizeof(double), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  *norm2 = ctx->h_norm[0];
+  return ICF_OK;
+}
+
+int icf_apply_dx(icf_ctx *ctx, double *norm) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_structure || !ctx->solver.x) return icf_fail(ctx, ICF_ERR_STATE, "icf_solve first");
+  cudaStream_t s = ctx->stream;
+  ICF_TRY(icf_launch_add_dx(ctx, ctx->solver.x));
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_norm, ctx->d_norm, sizeof(double), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaStreamSynchronize(s));
   if (norm) *norm = ctx->h_norm[0];

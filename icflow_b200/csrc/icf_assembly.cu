@@ -73,6 +73,7 @@ __device__ __forceinline__ void frame3(const double p0[3], const double p1[3],
 // record of vertex a is {h_a, V} and {rhs_a, 0}; k_gather rebuilds
 // LHS_ab = stiffCoeff Df_ab + massCoeff M_ab from it.  The record (16
 // double2, 256 B) is written to rec in shared memory.
+template <bool MIXED>
 __device__ __forceinline__ void tet_record(int e, const int4 *__restrict__ elem,
                                            const double4 *__restrict__ x0,
                                            const double4 *__restrict__ xc,
@@ -186,10 +187,18 @@ __device__ __forceinline__ void tet_record(int e, const int4 *__restrict__ elem,
       const double inert = mV * (An[a][k] + sa[k]);
       r[k] = (k == 2 ? gz : 0.0) - f[k] - damp - inert;
     }
-    rec[2 * a] = make_double2(h[a][0], h[a][1]);
-    rec[2 * a + 1] = make_double2(h[a][2], V);
-    rec[8 + 2 * a] = make_double2(r[0], r[1]);
-    rec[9 + 2 * a] = make_double2(r[2], 0.0);
+    if (MIXED) {
+      // FP64 rhs; the Hessian inputs rounded to FP32
+      rec[2 * a] = make_double2(r[0], r[1]);
+      rec[2 * a + 1] = make_double2(r[2], 0.0);
+      *reinterpret_cast<float4 *>(rec + 8 + a) =
+          make_float4((float)h[a][0], (float)h[a][1], (float)h[a][2], (float)V);
+    } else {
+      rec[2 * a] = make_double2(h[a][0], h[a][1]);
+      rec[2 * a + 1] = make_double2(h[a][2], V);
+      rec[8 + 2 * a] = make_double2(r[0], r[1]);
+      rec[9 + 2 * a] = make_double2(r[2], 0.0);
+    }
   }
 }
 
@@ -197,7 +206,14 @@ __device__ __forceinline__ void tet_record(int e, const int4 *__restrict__ elem,
 // shared memory (rows padded to 272 B, so both the row-wise writes and the
 // column-wise reads are free of bank conflicts) and stored as 512 B
 // contiguous chunks per instruction.
-template <int MINB>
+//
+// FP32-mixed (MIXED): the rotation, the force and the rhs stay FP64; the
+// rotated gradients and the volume, which are all the Hessian blocks are
+// built from, are rounded to FP32.  The staging then holds the rhs records
+// compactly, es[4e + a] = {rhs_a, 0}, followed by the FP32 records
+// es32[4e + a] = {h_a, V} with es32 = (float4 *)(es + 4 ne): 192 B per tet in
+// the same buffer.
+template <int MINB, bool MIXED>
 __global__ void __launch_bounds__(128, MINB)
     k_tet_unit(int ne, const int4 *__restrict__ elem,
                const double4 *__restrict__ x0, const double4 *__restrict__ xc,
@@ -208,14 +224,29 @@ __global__ void __launch_bounds__(128, MINB)
   const long long base = (long long)blockIdx.x * blockDim.x + 32 * w;
   if (base >= ne) return;
   const int e = (int)base + lane;
-  if (e < ne) tet_record(e, elem, x0, xc, va, P, sbuf[w][lane]);
+  if (e < ne) tet_record<MIXED>(e, elem, x0, xc, va, P, sbuf[w][lane]);
   __syncwarp();
   const long long nrec = (ne - base) < 32 ? (ne - base) : 32;
-  double2 *o = reinterpret_cast<double2 *>(es) + 16 * base;
+  if (!MIXED) {
+    double2 *o = reinterpret_cast<double2 *>(es) + 16 * base;
 #pragma unroll 4
-  for (int k = 0; k < 16; k++) {
-    const int idx = 32 * k + lane;
-    if (idx < 16 * nrec) o[idx] = sbuf[w][idx >> 4][idx & 15];
+    for (int k = 0; k < 16; k++) {
+      const int idx = 32 * k + lane;
+      if (idx < 16 * nrec) o[idx] = sbuf[w][idx >> 4][idx & 15];
+    }
+  } else {
+    double2 *o = reinterpret_cast<double2 *>(es) + 8 * base;
+#pragma unroll 4
+    for (int k = 0; k < 8; k++) {
+      const int idx = 32 * k + lane;
+      if (idx < 8 * nrec) o[idx] = sbuf[w][idx >> 3][idx & 7];
+    }
+    float4 *oh = reinterpret_cast<float4 *>(es + 4 * (size_t)ne) + 4 * base;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int idx = 32 * k + lane;
+      if (idx < 4 * nrec) oh[idx] = *reinterpret_cast<const float4 *>(&sbuf[w][idx >> 2][8 + (idx & 3)]);
+    }
   }
 }
 
@@ -270,10 +301,17 @@ __device__ __forceinline__ void cz_frame(const double m0[3], const double m1[3],
 // opening and the law; the three combine through shared memory in Gauss point
 // order 0, 1, 2 (the reference's accumulation order).
 constexpr int CZ_PER_BLOCK = 32;
+// FP32-mixed (MIXED): geometry, law and tractions stay FP64 (the PPR law,
+// including its softening branch near separation, is FP64 throughout); the
+// Gauss-point tangents Q and their combination into the 3x3 blocks Kt are
+// FP32.  The staging then holds rt compactly, cs[12c + 0..8] (FP64), followed
+// by the FP32 blocks cs32[36c + 0..35] with cs32 = (float *)(cs + 12 nc):
+// 240 B per CZ in the same buffer.
+template <bool MIXED>
 __global__ void __launch_bounds__(3 * CZ_PER_BLOCK)
     k_cz_gp(int nc, const int *__restrict__ cz, const double4 *__restrict__ xc,
             const double *__restrict__ czs, const int *__restrict__ czfail,
-            const double4 *__restrict__ czprm, icf_dprm P, icf_law_c LC,
+            const double4 *__restrict__ czprm, const double *__restrict__ hist, icf_dprm P, icf_law_c LC,
             double *__restrict__ cs, double *__restrict__ cztent, int *__restrict__ czflags,
             double *__restrict__ czavg, int *__restrict__ counts) {
   __shared__ double sQ[3 * CZ_PER_BLOCK][6];
@@ -322,7 +360,11 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK)
     }
     const double opn = o[2];
     const double opt = sqrt(add(mul(o[0], o[0]), mul(o[1], o[1])));
-    const icf_law Lw = icf_cz_law_axes(LC, f_tn, f_tt, deln, delt, pmax, tmax, opn, opt);
+    // history axes from the cache (k_cz_hist), 6 doubles per Gauss point
+    const double2 *hp = reinterpret_cast<const double2 *>(hist + 18 * (size_t)c + 6 * gp);
+    const double2 h01 = __ldg(hp), h23 = __ldg(hp + 1), h45 = __ldg(hp + 2);
+    const icf_axis Np{h01.x, h01.y, h23.x}, Tm{h23.y, h45.x, h45.y};
+    const icf_law Lw = icf_cz_law_hist(LC, f_tn, f_tt, deln, delt, Np, Tm, pmax, tmax, opn, opt);
 
     // local traction and its (symmetric) tangent (:301-340)
     double T[3], Td[3][3];
@@ -349,17 +391,37 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK)
     const double cw = (1.0 / 3.0) * aJ;
 #pragma unroll
     for (int k = 0; k < 3; k++) sTw[t][k] = cw * (R[0][k] * T[0] + R[1][k] * T[1] + R[2][k] * T[2]);
-    double TR[3][3];
+    if (MIXED) {
+      float Rf[3][3], TRf[3][3];
 #pragma unroll
-    for (int m = 0; m < 3; m++)
+      for (int m = 0; m < 3; m++)
 #pragma unroll
-      for (int l = 0; l < 3; l++) TR[m][l] = Td[m][0] * R[0][l] + Td[m][1] * R[1][l] + Td[m][2] * R[2][l];
-    int p = 0;
+        for (int l = 0; l < 3; l++) Rf[m][l] = (float)R[m][l];
 #pragma unroll
-    for (int k = 0; k < 3; k++)
+      for (int m = 0; m < 3; m++)
 #pragma unroll
-      for (int l = k; l < 3; l++)
-        sQ[t][p++] = cw * (R[0][k] * TR[0][l] + R[1][k] * TR[1][l] + R[2][k] * TR[2][l]);
+        for (int l = 0; l < 3; l++)
+          TRf[m][l] = (float)Td[m][0] * Rf[0][l] + (float)Td[m][1] * Rf[1][l] + (float)Td[m][2] * Rf[2][l];
+      const float cwf = (float)cw;
+      int p = 0;
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int l = k; l < 3; l++)
+          sQ[t][p++] = cwf * (Rf[0][k] * TRf[0][l] + Rf[1][k] * TRf[1][l] + Rf[2][k] * TRf[2][l]);
+    } else {
+      double TR[3][3];
+#pragma unroll
+      for (int m = 0; m < 3; m++)
+#pragma unroll
+        for (int l = 0; l < 3; l++) TR[m][l] = Td[m][0] * R[0][l] + Td[m][1] * R[1][l] + Td[m][2] * R[2][l];
+      int p = 0;
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int l = k; l < 3; l++)
+          sQ[t][p++] = cw * (R[0][k] * TR[0][l] + R[1][k] * TR[1][l] + R[2][k] * TR[2][l]);
+    }
     sAv[t][0] = opn;
     sAv[t][1] = opt;
     sAv[t][2] = Lw.Tn;
@@ -382,8 +444,16 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK)
         const int pr = v / 6, comp = v - 6 * pr;
         const int pi = pr < 3 ? 0 : (pr < 5 ? 1 : 2);
         const int pj = pr < 3 ? pr : (pr < 5 ? pr - 2 : 2);
+        if (MIXED) {
+          float vf = 0.f;
 #pragma unroll
-        for (int g = 0; g < 3; g++) val += (P.sf[pi * 3 + g] * P.sf[pj * 3 + g]) * sQ[b3 + g][comp];
+          for (int g = 0; g < 3; g++)
+            vf += (float)(P.sf[pi * 3 + g] * P.sf[pj * 3 + g]) * (float)sQ[b3 + g][comp];
+          val = vf;
+        } else {
+#pragma unroll
+          for (int g = 0; g < 3; g++) val += (P.sf[pi * 3 + g] * P.sf[pj * 3 + g]) * sQ[b3 + g][comp];
+        }
       } else if (v < 45) {
         const int i = (v - 36) / 3, k = (v - 36) - 3 * i;
 #pragma unroll
@@ -411,9 +481,23 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK)
   __syncthreads();
   // coalesced store of the block's staging records
   const int c0 = blockIdx.x * CZ_PER_BLOCK;
-  const int nvals = min(CZ_PER_BLOCK, nc - c0) * ICF_CZ_STAGE;
-  double *dst = cs + (size_t)c0 * ICF_CZ_STAGE;
-  for (int i = t; i < nvals; i += 3 * CZ_PER_BLOCK) dst[i] = sOut[i];
+  const int ncz = min(CZ_PER_BLOCK, nc - c0);
+  if (!MIXED) {
+    const int nvals = ncz * ICF_CZ_STAGE;
+    double *dst = cs + (size_t)c0 * ICF_CZ_STAGE;
+    for (int i = t; i < nvals; i += 3 * CZ_PER_BLOCK) dst[i] = sOut[i];
+  } else {
+    double *dr = cs + 12 * (size_t)c0;
+    for (int i = t; i < 12 * ncz; i += 3 * CZ_PER_BLOCK) {
+      const int jj = i / 12, q = i - 12 * jj;
+      dr[i] = q < 9 ? sOut[jj * ICF_CZ_STAGE + 36 + q] : 0.0;
+    }
+    float *dk = reinterpret_cast<float *>(cs + 12 * (size_t)nc) + 36 * (size_t)c0;
+    for (int i = t; i < 36 * ncz; i += 3 * CZ_PER_BLOCK) {
+      const int jj = i / 36, q = i - 36 * jj;
+      dk[i] = (float)sOut[jj * ICF_CZ_STAGE + q];
+    }
+  }
   // counters (integer atomics: order-independent)
   if (t < 32) {
     int dm = 0, fa = 0, ct = 0;
@@ -495,14 +579,14 @@ __global__ void k_node_force(int n, const int *__restrict__ off,
                              const double4 *__restrict__ es,
                              const int *__restrict__ ioff,
                              const int *__restrict__ iinc,
-                             const double *__restrict__ ks,
+                             const double *__restrict__ ks, int rstride, int roff,
                              double *__restrict__ F) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double f[3] = {0, 0, 0};
   for (int q = off[i]; q < off[i + 1]; q++) {
     const int code = inc[q];
-    const double4 r = es[8 * (size_t)(code >> 2) + 4 + (code & 3)];
+    const double4 r = es[rstride * (size_t)(code >> 2) + roff + (code & 3)];
     f[0] += r.x;
     f[1] += r.y;
     f[2] += r.z;
@@ -612,6 +696,26 @@ __global__ void k_accept(int n, double h, const double4 *__restrict__ x0,
 }
 
 // Commit of the tentative CZ state (TransferUpdatedStateToHost, :496-516).
+// History axes N(pmax/deln), T(tmax/delt) of every CZ Gauss point from the
+// committed state: {Np.f, Np.d, Np.dd, Tm.f, Tm.d, Tm.dd} at hist[18c + 6gp].
+__global__ void k_cz_hist(int nc, const double *__restrict__ czs, const double4 *__restrict__ czprm,
+                          double deln0, double delt0, icf_law_c LC, double *__restrict__ hist) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * nc) return;
+  const int c = t / 3, gp = t - 3 * c;
+  double deln = deln0, delt = delt0;
+  if (czprm) {
+    const double4 w = czprm[c];
+    deln = w.z;
+    delt = w.w;
+  }
+  icf_axis Np, Tm;
+  icf_cz_hist_axes(LC, deln, delt, czs[8 * (size_t)c + gp], czs[8 * (size_t)c + 3 + gp], Np, Tm);
+  double *o = hist + 18 * (size_t)c + 6 * gp;
+  o[0] = Np.f; o[1] = Np.d; o[2] = Np.dd;
+  o[3] = Tm.f; o[4] = Tm.d; o[5] = Tm.dd;
+}
+
 __global__ void k_commit_cz(int nc, const double *__restrict__ tent,
                             const int *__restrict__ flags, double *__restrict__ czs,
                             int *__restrict__ fail) {
@@ -631,22 +735,22 @@ struct tet_variant {
   const char *name;
   void (*fn)(int, const int4 *, const double4 *, const double4 *, const double2 *, icf_dprm, double4 *);
 };
-const tet_variant TET_VARIANTS[] = {
-    {"t128 minb3", k_tet_unit<3>},
-    {"t128 minb2", k_tet_unit<2>},
-    {"t128 minb4", k_tet_unit<4>},
+const tet_variant TET_VARIANTS[2][3] = {
+    {{"t128 minb3", k_tet_unit<3, false>}, {"t128 minb2", k_tet_unit<2, false>}, {"t128 minb4", k_tet_unit<4, false>}},
+    {{"t128 minb3", k_tet_unit<3, true>}, {"t128 minb2", k_tet_unit<2, true>}, {"t128 minb4", k_tet_unit<4, true>}},
 };
-constexpr int N_TET = sizeof(TET_VARIANTS) / sizeof(TET_VARIANTS[0]);
+constexpr int N_TET = 3;
 }  // namespace
 
 int icf_tet_variants() { return N_TET; }
-const char *icf_tet_variant_name(int v) { return TET_VARIANTS[v].name; }
+const char *icf_tet_variant_name(int v) { return TET_VARIANTS[0][v].name; }
 int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *va, double4 *es, cudaStream_t s) {
   if (ctx->n_elem <= 0) return ICF_OK;
   if (variant < 0 || variant >= N_TET) variant = 0;
   const icf_dprm P = icf_make_dprm(ctx);
-  TET_VARIANTS[variant].fn<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem, ctx->d_x0, xc,
-                                                                       va, P, es);
+  const int mixed = ctx->precision == ICF_FP32_MIXED ? 1 : 0;
+  TET_VARIANTS[mixed][variant].fn<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem,
+                                                                              ctx->d_x0, xc, va, P, es);
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
@@ -658,6 +762,32 @@ int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *
 //   aux1 :         | zero contact-only blocks, impact units .........|
 // The unit kernels are occupancy- or latency-limited on their own, so running
 // them side by side fills the machine; the gathers write disjoint blocks.
+static icf_law_c make_law_c(const icf_ctx *ctx, const icf_dprm &P) {
+  icf_law_c LC;
+  LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
+  LC.gam_n = P.gam_n; LC.gam_t = P.gam_t; LC.pMtn = P.pMtn; LC.pMnt = P.pMnt;
+  LC.rn = P.rn; LC.rt = P.rt;
+  LC.N0 = icf_axis{ctx->axis0[0], ctx->axis0[1], ctx->axis0[2]};
+  LC.T0 = icf_axis{ctx->axis0[3], ctx->axis0[4], ctx->axis0[5]};
+  auto small_int = [](double v) { return (v == (double)(int)v && v >= 2 && v <= 16) ? (int)v : 0; };
+  LC.alpha_int = small_int(P.alpha);
+  LC.beta_int = small_int(P.beta);
+  return LC;
+}
+
+// Refreshes the history-axis cache of the CZs when the damage state, the
+// strengths or the constants changed since it was filled.
+int icf_ensure_cz_hist(icf_ctx *ctx, cudaStream_t s) {
+  if (ctx->hist_valid || ctx->n_cz == 0) return ICF_OK;
+  const icf_dprm P = icf_make_dprm(ctx);
+  k_cz_hist<<<icf_blocks(3LL * ctx->n_cz, 256), 256, 0, s>>>(ctx->n_cz, ctx->d_czs,
+                                                           ctx->per_cz_prm ? ctx->d_czprm : nullptr, P.deln,
+                                                           P.delt, make_law_c(ctx, P), ctx->d_czhist);
+  ICF_CUDA(ctx, cudaGetLastError());
+  ctx->hist_valid = true;
+  return ICF_OK;
+}
+
 static int enqueue_assembly(icf_ctx *ctx, double h) {
   const icf_dprm P = icf_make_dprm(ctx);
   cudaStream_t s = ctx->stream, sa = ctx->aux[0], sb = ctx->aux[1];
@@ -685,30 +815,21 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   if (ctx->n_elem > 0)
     ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, ctx->d_xc, ctx->d_va, ctx->d_es, s));
   // ids, node state (x0, x_t, v, a) once, 256 B record out
-  if (ctx->n_elem > 0) icf_prof_mark(ctx, s, "k_tet_unit", 272LL * ctx->n_elem + 112LL * ctx->n_nodes);
+  const bool mixed = ctx->precision == ICF_FP32_MIXED;
+  const long long tet_rec = mixed ? 192 : 256, tet_h = mixed ? 64 : 128, cz_rec = mixed ? 240 : 8 * ICF_CZ_STAGE;
+  if (ctx->n_elem > 0) icf_prof_mark(ctx, s, "k_tet_unit", (16 + tet_rec) * ctx->n_elem + 112LL * ctx->n_nodes);
   ICF_CUDA(ctx, cudaEventRecord(e_tet, s));
 
   // aux0: CZs
   if (ctx->n_cz > 0) {
-    icf_law_c LC;
-    LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
-    LC.gam_n = P.gam_n; LC.gam_t = P.gam_t; LC.pMtn = P.pMtn; LC.pMnt = P.pMnt;
-    LC.rn = P.rn; LC.rt = P.rt;
-    LC.N0 = icf_axis{ctx->axis0[0], ctx->axis0[1], ctx->axis0[2]};
-    LC.T0 = icf_axis{ctx->axis0[3], ctx->axis0[4], ctx->axis0[5]};
-    auto small_int = [](double v) {
-      return (v == (double)(int)v && v >= 2 && v <= 16) ? (int)v : 0;
-    };
-    LC.alpha_int = small_int(P.alpha);
-    LC.beta_int = small_int(P.beta);
-    k_cz_gp<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, sa>>>(
+    const icf_law_c LC = make_law_c(ctx, P);
+    (ctx->precision == ICF_FP32_MIXED ? k_cz_gp<true> : k_cz_gp<false>)<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, sa>>>(
         ctx->n_cz, ctx->d_cz, ctx->d_xc, ctx->d_czs, ctx->d_czfail,
-        ctx->per_cz_prm ? ctx->d_czprm : nullptr, P, LC, ctx->d_cs, ctx->d_cztent, ctx->d_czflags,
+        ctx->per_cz_prm ? ctx->d_czprm : nullptr, ctx->d_czhist, P, LC, ctx->d_cs, ctx->d_cztent, ctx->d_czflags,
         ctx->d_czavg, ctx->d_counts);
     // ids, six node positions, state in, per-CZ strengths, staging, tentative
     // state, flags and averages out
-    icf_prof_mark(ctx, sa, "k_cz_gp", (24LL + 192 + 52 + (ctx->per_cz_prm ? 32 : 0) + 8 * ICF_CZ_STAGE + 84) *
-                                          ctx->n_cz);
+    icf_prof_mark(ctx, sa, "k_cz_gp", (24LL + 192 + 52 + (ctx->per_cz_prm ? 32 : 0) + cz_rec + 84) * ctx->n_cz);
   }
   ICF_CUDA(ctx, cudaEventRecord(e_cz, sa));
 
@@ -723,8 +844,8 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   // descriptors, codes, the h records of every tet and the CZ staging once,
   // blocks out
   if (ctx->n_offd > 0)
-    icf_prof_mark(ctx, sa, "k_gather_off", 80LL * ctx->n_offd + 4LL * ctx->n_rc_off + 128LL * ctx->n_elem +
-                                               8LL * ICF_CZ_STAGE * ctx->n_cz);
+    icf_prof_mark(ctx, sa, "k_gather_off", 80LL * ctx->n_offd + 4LL * ctx->n_rc_off + tet_h * ctx->n_elem +
+                                               cz_rec * ctx->n_cz);
   ICF_CUDA(ctx, cudaEventRecord(e_a, sa));
   // main: diagonal blocks and rhs once the CZs are staged
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
@@ -733,7 +854,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
                                       ctx->d_rhs, s));
   if (ctx->N > 0)
     icf_prof_mark(ctx, s, "k_gather_diag", 104LL * ctx->N + 4LL * (ctx->n_rc - ctx->n_rc_off) +
-                                               256LL * ctx->n_elem + 8LL * ICF_CZ_STAGE * ctx->n_cz);
+                                               tet_rec * ctx->n_elem + cz_rec * ctx->n_cz);
   // join
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
@@ -776,6 +897,7 @@ int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const ch
   for (int i = 0; i <= ICF_PROF_MAX; i++) ICF_CUDA(ctx, cudaEventCreate(&st.ev[i]));
   std::vector<double> acc(ICF_PROF_MAX, 0.0);
   int rc = ICF_OK;
+  rc = icf_ensure_cz_hist(ctx, ctx->stream);
   for (int r = 0; r < reps && rc == ICF_OK; r++) {
     st.n = 0;
     ctx->prof = &st;
@@ -806,6 +928,7 @@ int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const ch
 }
 
 int icf_launch_assembly(icf_ctx *ctx, double h) {
+  ICF_TRY_RC(icf_ensure_cz_hist(ctx, ctx->stream));
   if (!ctx->use_graph) return enqueue_assembly(ctx, h);
   if (!ctx->graph_exec || ctx->graph_version != ctx->version || ctx->graph_h != h) {
     if (ctx->graph_exec) {
@@ -840,7 +963,7 @@ int icf_launch_node_force(icf_ctx *ctx) {
   if (rc) return rc;
   k_node_force<<<icf_blocks(ctx->n_nodes, 128), 128, 0, ctx->stream>>>(
       ctx->n_nodes, t.off, t.inc, ctx->d_es, ctx->n_imp > 0 ? m.off : nullptr, m.inc, ctx->d_ks,
-      ctx->d_nodeF);
+      ctx->precision == ICF_FP32_MIXED ? 4 : 8, ctx->precision == ICF_FP32_MIXED ? 0 : 4, ctx->d_nodeF);
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
@@ -872,6 +995,13 @@ int icf_launch_add_dx(icf_ctx *ctx, const double *d_dx) {
   return ICF_OK;
 }
 
+int icf_launch_sumsq(icf_ctx *ctx, const double *d_x, long long n) {
+  k_sumsq<<<256, 256, 0, ctx->stream>>>((int)n, d_x, ctx->d_norm + 1);
+  k_sum_parts<<<1, 32, 0, ctx->stream>>>(256, ctx->d_norm + 1, ctx->d_norm);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
 int icf_launch_accept(icf_ctx *ctx, double h) {
   k_accept<<<icf_blocks(ctx->n_nodes, 256), 256, 0, ctx->stream>>>(
       ctx->n_nodes, h, ctx->d_x0, ctx->d_u, ctx->d_v, ctx->d_a, ctx->d_un, ctx->d_du, ctx->d_xc);
@@ -883,6 +1013,7 @@ int icf_launch_commit_cz(icf_ctx *ctx) {
   if (ctx->n_cz == 0) return ICF_OK;
   k_commit_cz<<<icf_blocks(ctx->n_cz, 256), 256, 0, ctx->stream>>>(
       ctx->n_cz, ctx->d_cztent, ctx->d_czflags, ctx->d_czs, ctx->d_czfail);
+  ctx->hist_valid = false;
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
@@ -890,6 +1021,7 @@ int icf_launch_commit_cz(icf_ctx *ctx) {
 // ---- launches with caller-chosen buffers (used by the allocation-free entry
 // point in icf_noalloc.cu; the context's own assembly path above is separate)
 int icf_enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cudaStream_t s) {
+  ICF_TRY_RC(icf_ensure_cz_hist(ctx, s));
   const icf_dprm P = icf_make_dprm(ctx);
   ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, 8 * sizeof(int), s));
   ICF_CUDA(ctx, cudaMemsetAsync(B.rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
@@ -898,18 +1030,10 @@ int icf_enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cud
   if (ctx->n_elem > 0)
     ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, B.xc, B.va, B.es, s));
   if (ctx->n_cz > 0) {
-    icf_law_c LC;
-    LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
-    LC.gam_n = P.gam_n; LC.gam_t = P.gam_t; LC.pMtn = P.pMtn; LC.pMnt = P.pMnt;
-    LC.rn = P.rn; LC.rt = P.rt;
-    LC.N0 = icf_axis{ctx->axis0[0], ctx->axis0[1], ctx->axis0[2]};
-    LC.T0 = icf_axis{ctx->axis0[3], ctx->axis0[4], ctx->axis0[5]};
-    auto small_int = [](double v) { return (v == (double)(int)v && v >= 2 && v <= 16) ? (int)v : 0; };
-    LC.alpha_int = small_int(P.alpha);
-    LC.beta_int = small_int(P.beta);
-    k_cz_gp<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, s>>>(
-        ctx->n_cz, ctx->d_cz, B.xc, ctx->d_czs, ctx->d_czfail, ctx->per_cz_prm ? ctx->d_czprm : nullptr, P,
-        LC, B.cs, ctx->d_cztent, ctx->d_czflags, ctx->d_czavg, ctx->d_counts);
+    const icf_law_c LC = make_law_c(ctx, P);
+    (ctx->precision == ICF_FP32_MIXED ? k_cz_gp<true> : k_cz_gp<false>)<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, s>>>(
+        ctx->n_cz, ctx->d_cz, B.xc, ctx->d_czs, ctx->d_czfail, ctx->per_cz_prm ? ctx->d_czprm : nullptr,
+        ctx->d_czhist, P, LC, B.cs, ctx->d_cztent, ctx->d_czflags, ctx->d_czavg, ctx->d_counts);
   }
   if (ctx->n_imp > 0) {
     const int rc = icf_launch_imp_unit_bufs(ctx, B.xc, B.ci, B.cd, B.ks, s);

@@ -8,10 +8,14 @@
 // so the result is identical on every run.
 //
 // Every gather has several launch variants (registers per thread, codes per
-// iteration, loads through registers or through cp.async into shared memory,
-// lanes per row).  They compute the same sums in the same order; the
-// autotuner (icf_tune.cu) times them on the model at hand and keeps the
-// fastest.
+// iteration, lanes per row).  They compute the same sums; the autotuner
+// (icf_tune.cu) times them on the model at hand and keeps the fastest.
+//
+// Two precisions share the code.  FP64: staging records as k_tet_unit and
+// k_cz_gp write them in FP64.  FP32-mixed: the Hessian inputs are FP32
+// records (tet {h, V} as float4, CZ blocks Kt as float) and each block's tet
+// and CZ terms are formed and summed in FP32, then written to the FP64 matrix;
+// the rhs records and their sums stay FP64.
 #include <cstdint>
 
 #include "icf_internal.cuh"
@@ -24,8 +28,56 @@ __device__ __forceinline__ int sym_pair(int i, int j) {
   return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
 }
 
+__device__ __forceinline__ void tet_code(uint32_t code, uint32_t &e, uint32_t &a, uint32_t &b) {
+  e = (code >> 4) & 0x3FFFFFFu;
+  a = (code >> 2) & 3u;
+  b = code & 3u;
+}
+
+__device__ __forceinline__ void cz_code(uint32_t code, uint32_t &c, int &ia, int &ib, bool &same, bool &a_lo) {
+  c = (code >> 6) & 0xFFFFFFu;
+  const uint32_t a = (code >> 3) & 7u, bb = code & 7u;
+  ia = a % 3;
+  ib = bb % 3;
+  same = (a < 3) == (bb < 3);
+  a_lo = a < 3;
+}
+
+// Staging views and arithmetic of one precision.
+struct fp64 {
+  typedef double real;
+  typedef double4 rec;
+  const double4 *es;  // tet records: {h_a, V} at 8e + a, {rhs_a, 0} at 8e + 4 + a
+  const double *cs;   // CZ records: Kt (6 x 6) at 48c, rt[3][3] at 48c + 36
+  __device__ __forceinline__ rec hrec(uint32_t e, uint32_t a) const { return es[8 * (size_t)e + a]; }
+  __device__ __forceinline__ double4 rrec(uint32_t e, uint32_t a) const { return es[8 * (size_t)e + 4 + a]; }
+  __device__ __forceinline__ void kt(uint32_t c, int pair, real k[6]) const {
+    const double2 *K2 = reinterpret_cast<const double2 *>(cs + (size_t)c * ICF_CZ_STAGE + 6 * pair);
+    const double2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
+    k[0] = k01.x; k[1] = k01.y; k[2] = k23.x; k[3] = k23.y; k[4] = k45.x; k[5] = k45.y;
+  }
+  __device__ __forceinline__ const double *rt(uint32_t c) const { return cs + (size_t)c * ICF_CZ_STAGE + 36; }
+};
+struct fp32mixed {
+  typedef float real;
+  typedef float4 rec;
+  const float4 *es32;  // {h_a, V} at 4e + a
+  const double4 *esr;  // {rhs_a, 0} at 4e + a
+  const float *cs32;   // Kt at 36c
+  const double *csr;   // rt at 12c
+  __device__ __forceinline__ rec hrec(uint32_t e, uint32_t a) const { return es32[4 * (size_t)e + a]; }
+  __device__ __forceinline__ double4 rrec(uint32_t e, uint32_t a) const { return esr[4 * (size_t)e + a]; }
+  __device__ __forceinline__ void kt(uint32_t c, int pair, real k[6]) const {
+    const float2 *K2 = reinterpret_cast<const float2 *>(cs32 + (size_t)c * 36 + 6 * pair);
+    const float2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
+    k[0] = k01.x; k[1] = k01.y; k[2] = k23.x; k[3] = k23.y; k[4] = k45.x; k[5] = k45.y;
+  }
+  __device__ __forceinline__ const double *rt(uint32_t c) const { return csr + (size_t)c * 12; }
+};
+
+template <typename R>
 struct gargs {
-  double sc, mc, lam, mu;
+  R sc, mc, lam, mu;
 };
 
 // LHS_ab = stiffCoeff Df_ab + massCoeff M_ab rebuilt from the staging records
@@ -33,153 +85,139 @@ struct gargs {
 //   Df_ab = V (lam h_a h_b^T + mu h_b h_a^T + mu (h_a.h_b) I),
 //   M_ab = rho/20 (1 + delta_ab) V I.
 // A zero record (a padding code) adds nothing.
-__device__ __forceinline__ void acc_tet(const double4 &A, const double4 &B, bool diag, const gargs &g,
-                                        double b[9]) {
-  const double V = A.w;
-  const double ha[3] = {A.x, A.y, A.z}, hb[3] = {B.x, B.y, B.z};
-  const double dot = ha[0] * hb[0] + ha[1] * hb[1] + ha[2] * hb[2];
-  const double c1 = g.sc * V * g.lam, c2 = g.sc * V * g.mu;
-  const double cd = c2 * dot + g.mc * V * (diag ? 2.0 : 1.0);
+template <typename R, typename V4>
+__device__ __forceinline__ void acc_tet(const V4 &A, const V4 &B, bool diag, const gargs<R> &g, R b[9]) {
+  const R V = A.w;
+  const R ha[3] = {A.x, A.y, A.z}, hb[3] = {B.x, B.y, B.z};
+  const R dot = ha[0] * hb[0] + ha[1] * hb[1] + ha[2] * hb[2];
+  const R c1 = g.sc * V * g.lam, c2 = g.sc * V * g.mu;
+  const R cd = c2 * dot + g.mc * V * (diag ? R(2) : R(1));
 #pragma unroll
   for (int k = 0; k < 3; k++)
 #pragma unroll
-    for (int l = 0; l < 3; l++) b[3 * k + l] += c1 * ha[k] * hb[l] + c2 * hb[k] * ha[l] + (k == l ? cd : 0.0);
-}
-
-__device__ __forceinline__ void tet_code(uint32_t code, uint32_t &e, uint32_t &a, uint32_t &b) {
-  e = (code >> 4) & 0x3FFFFFFu;
-  a = (code >> 2) & 3u;
-  b = code & 3u;
+    for (int l = 0; l < 3; l++) b[3 * k + l] += c1 * ha[k] * hb[l] + c2 * hb[k] * ha[l] + (k == l ? cd : R(0));
 }
 
 // Contribution of one CZ code: +-Kt[a mod 3][b mod 3] (symmetric 3x3) and,
-// for a diagonal block, -+rt[a mod 3].
-__device__ __forceinline__ void add_cz(uint32_t code, const double *__restrict__ cs, double b[9],
-                                       double *r) {
-  const uint32_t c = (code >> 6) & 0xFFFFFFu, a = (code >> 3) & 7u, bb = code & 7u;
-  const double *S = cs + (size_t)c * ICF_CZ_STAGE;
-  const int ia = a % 3, ib = bb % 3;
-  const double sg = ((a < 3) == (bb < 3)) ? 1.0 : -1.0;
-  const double2 *K2 = reinterpret_cast<const double2 *>(S + 6 * sym_pair(ia, ib));
-  const double2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
-  b[0] += sg * k01.x; b[1] += sg * k01.y; b[2] += sg * k23.x;
-  b[3] += sg * k01.y; b[4] += sg * k23.y; b[5] += sg * k45.x;
-  b[6] += sg * k23.x; b[7] += sg * k45.x; b[8] += sg * k45.y;
+// for a diagonal block, -+rt[a mod 3] (FP64).
+template <typename S>
+__device__ __forceinline__ void add_cz(const S &st, uint32_t code, typename S::real b[9], double *r) {
+  typedef typename S::real R;
+  uint32_t c;
+  int ia, ib;
+  bool same, a_lo;
+  cz_code(code, c, ia, ib, same, a_lo);
+  R k[6];
+  st.kt(c, sym_pair(ia, ib), k);
+  const R sg = same ? R(1) : R(-1);
+  b[0] += sg * k[0]; b[1] += sg * k[1]; b[2] += sg * k[2];
+  b[3] += sg * k[1]; b[4] += sg * k[3]; b[5] += sg * k[4];
+  b[6] += sg * k[2]; b[7] += sg * k[4]; b[8] += sg * k[5];
   if (r != nullptr) {
-    const double sa = (a < 3) ? -1.0 : 1.0;
-    r[0] += sa * __ldg(S + 36 + 3 * ia + 0);
-    r[1] += sa * __ldg(S + 36 + 3 * ia + 1);
-    r[2] += sa * __ldg(S + 36 + 3 * ia + 2);
+    const double sa = a_lo ? -1.0 : 1.0;
+    const double *rt = st.rt(c);
+    r[0] += sa * __ldg(rt + 3 * ia + 0);
+    r[1] += sa * __ldg(rt + 3 * ia + 1);
+    r[2] += sa * __ldg(rt + 3 * ia + 2);
   }
 }
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_rec(double4 *smem, const double4 *gmem) {
-  cp_async16(smem, gmem);
-  cp_async16(reinterpret_cast<char *>(smem) + 16, reinterpret_cast<const char *>(gmem) + 16);
-}
+template <typename V4>
+__device__ __forceinline__ V4 zero4();
+template <>
+__device__ __forceinline__ double4 zero4<double4>() { return make_double4(0, 0, 0, 0); }
+template <>
+__device__ __forceinline__ float4 zero4<float4>() { return make_float4(0, 0, 0, 0); }
 
 // ---- off-diagonal blocks: one lane per block --------------------------------
-
-// Records through registers: U codes per iteration, their 2U records loaded
-// before any is used.
-template <int MINB, int U>
+// U codes per iteration; their 2U records are loaded before any is used.
+template <typename S, int MINB, int U>
 __global__ void __launch_bounds__(256, MINB)
-    k_gather_off_reg(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
-                     const uint32_t *__restrict__ codes, const double4 *__restrict__ es,
-                     const double *__restrict__ cs, gargs g, double *__restrict__ vals) {
+    k_gather_off(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
+                 const uint32_t *__restrict__ codes, S st, gargs<typename S::real> g,
+                 double *__restrict__ vals) {
+  typedef typename S::real R;
+  typedef typename S::rec V4;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= n_slices) return;
   const int4 m = meta[w];
   const uint32_t *c = codes + m.x + lane;
-  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int k = 0; k < m.y; k += U) {
     uint32_t cc[U];
 #pragma unroll
     for (int j = 0; j < U; j++) cc[j] = (k + j < m.y) ? __ldg(c + 32 * (k + j)) : ICF_CODE_PAD;
-    double4 A[U], B[U];
+    V4 A[U], B[U];
 #pragma unroll
     for (int j = 0; j < U; j++) {
-      A[j] = B[j] = make_double4(0, 0, 0, 0);
+      A[j] = B[j] = zero4<V4>();
       if (cc[j] != ICF_CODE_PAD) {
         uint32_t e, a, bb;
         tet_code(cc[j], e, a, bb);
-        A[j] = es[8 * (size_t)e + a];
-        B[j] = es[8 * (size_t)e + bb];
+        A[j] = st.hrec(e, a);
+        B[j] = st.hrec(e, bb);
       }
     }
 #pragma unroll
-    for (int j = 0; j < U; j++) acc_tet(A[j], B[j], false, g, b);
+    for (int j = 0; j < U; j++) acc_tet<R, V4>(A[j], B[j], false, g, b);
   }
   for (int k = m.y; k < m.y + m.z; k++) {
     const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz(c0, cs, b, nullptr);
+    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
   }
   const int2 u = unit[32 * w + lane];
   if (u.x < 0) return;
   double *o = vals + 9 * (size_t)u.x;
 #pragma unroll
-  for (int q = 0; q < 9; q++) o[q] = b[q];
-}
-
-// Records through shared memory: the 2U records of an iteration are copied
-// with cp.async (no registers held while they are in flight), then read back
-// conflict-free (record j of the 32 lanes is contiguous).
-template <int T, int U>
-__global__ void __launch_bounds__(T)
-    k_gather_off_async(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
-                       const uint32_t *__restrict__ codes, const double4 *__restrict__ es,
-                       const double *__restrict__ cs, gargs g, double *__restrict__ vals) {
-  extern __shared__ double4 sm_rec[];
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= n_slices) return;
-  double4 *my = sm_rec + (size_t)(threadIdx.x >> 5) * (2 * U * 32);
-  const int4 m = meta[w];
-  const uint32_t *c = codes + m.x + lane;
-  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int k = 0; k < m.y; k += U) {
-    uint32_t cc[U];
-#pragma unroll
-    for (int j = 0; j < U; j++) cc[j] = (k + j < m.y) ? __ldg(c + 32 * (k + j)) : ICF_CODE_PAD;
-#pragma unroll
-    for (int j = 0; j < U; j++)
-      if (cc[j] != ICF_CODE_PAD) {
-        uint32_t e, a, bb;
-        tet_code(cc[j], e, a, bb);
-        cp_async_rec(my + (2 * j) * 32 + lane, es + 8 * (size_t)e + a);
-        cp_async_rec(my + (2 * j + 1) * 32 + lane, es + 8 * (size_t)e + bb);
-      }
-    cp_async_wait_all();
-#pragma unroll
-    for (int j = 0; j < U; j++)
-      if (cc[j] != ICF_CODE_PAD) acc_tet(my[(2 * j) * 32 + lane], my[(2 * j + 1) * 32 + lane], false, g, b);
-  }
-  for (int k = m.y; k < m.y + m.z; k++) {
-    const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz(c0, cs, b, nullptr);
-  }
-  const int2 u = unit[32 * w + lane];
-  if (u.x < 0) return;
-  double *o = vals + 9 * (size_t)u.x;
-#pragma unroll
-  for (int q = 0; q < 9; q++) o[q] = b[q];
+  for (int q = 0; q < 9; q++) o[q] = (double)b[q];
 }
 
 // ---- diagonal blocks and rhs rows: L lanes per row --------------------------
 // Every code of a diagonal block has a == b: one {h, V} record for the block
 // and one {rhs, 0} record for the row.  The L partial sums are combined by a
 // fixed shuffle tree.
-template <int L>
-__device__ __forceinline__ void diag_finish(int w, int lane, const int2 *__restrict__ unit, double b[9],
-                                            double r[3], double *__restrict__ vals,
-                                            double *__restrict__ rhs) {
+template <typename S, int L, int MINB, int U>
+__global__ void __launch_bounds__(256, MINB)
+    k_gather_diag(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
+                  const uint32_t *__restrict__ codes, S st, gargs<typename S::real> g,
+                  double *__restrict__ vals, double *__restrict__ rhs) {
+  typedef typename S::real R;
+  typedef typename S::rec V4;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n_slices) return;
+  const int4 m = meta[w];
+  const uint32_t *c = codes + m.x + lane;
+  R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double r[3] = {0, 0, 0};
+  for (int k = 0; k < m.y; k += U) {
+    uint32_t cc[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) cc[j] = (k + j < m.y) ? __ldg(c + 32 * (k + j)) : ICF_CODE_PAD;
+    V4 A[U];
+    double4 Rr[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      A[j] = zero4<V4>();
+      Rr[j] = make_double4(0, 0, 0, 0);
+      if (cc[j] != ICF_CODE_PAD) {
+        uint32_t e, a, bb;
+        tet_code(cc[j], e, a, bb);
+        A[j] = st.hrec(e, a);
+        Rr[j] = st.rrec(e, a);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      acc_tet<R, V4>(A[j], A[j], true, g, b);
+      r[0] += Rr[j].x;
+      r[1] += Rr[j].y;
+      r[2] += Rr[j].z;
+    }
+  }
+  for (int k = m.y; k < m.y + m.z; k++) {
+    const uint32_t c0 = __ldg(c + 32 * k);
+    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, r);
+  }
 #pragma unroll
   for (int o = 1; o < L; o <<= 1) {
 #pragma unroll
@@ -189,141 +227,56 @@ __device__ __forceinline__ void diag_finish(int w, int lane, const int2 *__restr
   }
   const int sub = lane % L;
   const int2 u = unit[(32 / L) * w + lane / L];
-  const bool wb = (sub == 0), wr = (L == 1) ? true : (sub == 1);
-  if (wb && u.x >= 0) {
+  if (sub == 0 && u.x >= 0) {
     double *o = vals + 9 * (size_t)u.x;
 #pragma unroll
-    for (int q = 0; q < 9; q++) o[q] = b[q];
+    for (int q = 0; q < 9; q++) o[q] = (double)b[q];
   }
-  if (wr && u.y >= 0) {
+  if (sub == (L > 1 ? 1 : 0) && u.y >= 0) {
     rhs[3 * (size_t)u.y + 0] = r[0];
     rhs[3 * (size_t)u.y + 1] = r[1];
     rhs[3 * (size_t)u.y + 2] = r[2];
   }
 }
 
-template <int L, int MINB, int U>
-__global__ void __launch_bounds__(256, MINB)
-    k_gather_diag_reg(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
-                      const uint32_t *__restrict__ codes, const double4 *__restrict__ es,
-                      const double *__restrict__ cs, gargs g, double *__restrict__ vals,
-                      double *__restrict__ rhs) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= n_slices) return;
-  const int4 m = meta[w];
-  const uint32_t *c = codes + m.x + lane;
-  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, r[3] = {0, 0, 0};
-  for (int k = 0; k < m.y; k += U) {
-    uint32_t cc[U];
-#pragma unroll
-    for (int j = 0; j < U; j++) cc[j] = (k + j < m.y) ? __ldg(c + 32 * (k + j)) : ICF_CODE_PAD;
-    double4 A[U], R[U];
-#pragma unroll
-    for (int j = 0; j < U; j++) {
-      A[j] = R[j] = make_double4(0, 0, 0, 0);
-      if (cc[j] != ICF_CODE_PAD) {
-        uint32_t e, a, bb;
-        tet_code(cc[j], e, a, bb);
-        A[j] = es[8 * (size_t)e + a];
-        R[j] = es[8 * (size_t)e + 4 + a];
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < U; j++) {
-      acc_tet(A[j], A[j], true, g, b);
-      r[0] += R[j].x;
-      r[1] += R[j].y;
-      r[2] += R[j].z;
-    }
-  }
-  for (int k = m.y; k < m.y + m.z; k++) {
-    const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz(c0, cs, b, r);
-  }
-  diag_finish<L>(w, lane, unit, b, r, vals, rhs);
-}
-
-template <int T, int L, int U>
-__global__ void __launch_bounds__(T)
-    k_gather_diag_async(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
-                        const uint32_t *__restrict__ codes, const double4 *__restrict__ es,
-                        const double *__restrict__ cs, gargs g, double *__restrict__ vals,
-                        double *__restrict__ rhs) {
-  extern __shared__ double4 sm_rec[];
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= n_slices) return;
-  double4 *my = sm_rec + (size_t)(threadIdx.x >> 5) * (2 * U * 32);
-  const int4 m = meta[w];
-  const uint32_t *c = codes + m.x + lane;
-  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, r[3] = {0, 0, 0};
-  for (int k = 0; k < m.y; k += U) {
-    uint32_t cc[U];
-#pragma unroll
-    for (int j = 0; j < U; j++) cc[j] = (k + j < m.y) ? __ldg(c + 32 * (k + j)) : ICF_CODE_PAD;
-#pragma unroll
-    for (int j = 0; j < U; j++)
-      if (cc[j] != ICF_CODE_PAD) {
-        uint32_t e, a, bb;
-        tet_code(cc[j], e, a, bb);
-        cp_async_rec(my + (2 * j) * 32 + lane, es + 8 * (size_t)e + a);
-        cp_async_rec(my + (2 * j + 1) * 32 + lane, es + 8 * (size_t)e + 4 + a);
-      }
-    cp_async_wait_all();
-#pragma unroll
-    for (int j = 0; j < U; j++)
-      if (cc[j] != ICF_CODE_PAD) {
-        const double4 A = my[(2 * j) * 32 + lane], R = my[(2 * j + 1) * 32 + lane];
-        acc_tet(A, A, true, g, b);
-        r[0] += R.x;
-        r[1] += R.y;
-        r[2] += R.z;
-      }
-  }
-  for (int k = m.y; k < m.y + m.z; k++) {
-    const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz(c0, cs, b, r);
-  }
-  diag_finish<L>(w, lane, unit, b, r, vals, rhs);
-}
-
 // ---- variant tables ---------------------------------------------------------
-typedef void (*off_fn)(int, const int4 *, const int2 *, const uint32_t *, const double4 *, const double *, gargs,
-                       double *);
-typedef void (*diag_fn)(int, const int4 *, const int2 *, const uint32_t *, const double4 *, const double *,
-                        gargs, double *, double *);
+template <typename S>
+using off_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, S, gargs<typename S::real>, double *);
+template <typename S>
+using diag_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, S, gargs<typename S::real>, double *,
+                         double *);
 
 struct off_variant {
   const char *name;
-  off_fn fn;
-  int threads;
-  int smem;  // dynamic shared memory per block
+  off_fn<fp64> f64;
+  off_fn<fp32mixed> f32;
 };
 struct diag_variant {
   const char *name;
-  diag_fn fn;
-  int threads, smem, lanes;
+  int lanes;
+  diag_fn<fp64> f64;
+  diag_fn<fp32mixed> f32;
 };
 
-const off_variant OFF_VARIANTS[] = {
-    {"reg minb4 u4", k_gather_off_reg<4, 4>, 256, 0},
-    {"reg minb2 u4", k_gather_off_reg<2, 4>, 256, 0},
-    {"reg minb3 u2", k_gather_off_reg<3, 2>, 256, 0},
-    {"async t128 u4", k_gather_off_async<128, 4>, 128, 4 * 2 * 4 * 32 * 32},
-    {"async t128 u8", k_gather_off_async<128, 8>, 128, 4 * 2 * 8 * 32 * 32},
-    {"async t256 u4", k_gather_off_async<256, 4>, 256, 8 * 2 * 4 * 32 * 32},
-};
-const diag_variant DIAG_VARIANTS[] = {
-    {"reg L4 minb4 u4", k_gather_diag_reg<4, 4, 4>, 256, 0, 4},
-    {"reg L4 minb2 u4", k_gather_diag_reg<4, 2, 4>, 256, 0, 4},
-    {"reg L2 minb3 u4", k_gather_diag_reg<2, 3, 4>, 256, 0, 2},
-    {"reg L8 minb4 u2", k_gather_diag_reg<8, 4, 2>, 256, 0, 8},
-    {"async t128 L4 u4", k_gather_diag_async<128, 4, 4>, 128, 4 * 2 * 4 * 32 * 32, 4},
-    {"async t128 L2 u8", k_gather_diag_async<128, 2, 8>, 128, 4 * 2 * 8 * 32 * 32, 2},
-};
+#define OFFV(MB, U) {"reg minb" #MB " u" #U, k_gather_off<fp64, MB, U>, k_gather_off<fp32mixed, MB, U>}
+#define DIAGV(L, MB, U) \
+  {"reg L" #L " minb" #MB " u" #U, L, k_gather_diag<fp64, L, MB, U>, k_gather_diag<fp32mixed, L, MB, U>}
+const off_variant OFF_VARIANTS[] = {OFFV(4, 4), OFFV(3, 2), OFFV(2, 4), OFFV(4, 2)};
+const diag_variant DIAG_VARIANTS[] = {DIAGV(4, 4, 4), DIAGV(2, 3, 4), DIAGV(4, 2, 4), DIAGV(8, 4, 2),
+                                      DIAGV(2, 4, 2)};
+#undef OFFV
+#undef DIAGV
 constexpr int N_OFF = sizeof(OFF_VARIANTS) / sizeof(OFF_VARIANTS[0]);
 constexpr int N_DIAG = sizeof(DIAG_VARIANTS) / sizeof(DIAG_VARIANTS[0]);
 
-bool g_attrs_set[64] = {false};
+fp32mixed mixed_views(const icf_ctx *ctx, const double4 *es, const double *cs) {
+  fp32mixed m;
+  m.esr = es;
+  m.es32 = reinterpret_cast<const float4 *>(es + 4 * (size_t)ctx->n_elem);
+  m.csr = cs;
+  m.cs32 = reinterpret_cast<const float *>(cs + 12 * (size_t)ctx->n_cz);
+  return m;
+}
 
 }  // namespace
 
@@ -333,32 +286,23 @@ const char *icf_gather_variant_name(int kind, int v) {
 }
 int icf_gather_variant_lanes(int v) { return DIAG_VARIANTS[v].lanes; }
 
-// Opts the shared-memory variants into more than 48 KB of dynamic shared
-// memory (once per device).
-static int set_smem_attrs(icf_ctx *ctx) {
-  if (ctx->device < 0 || ctx->device >= 64 || g_attrs_set[ctx->device]) return ICF_OK;
-  for (int v = 0; v < N_OFF; v++)
-    if (OFF_VARIANTS[v].smem > 0)
-      ICF_CUDA(ctx, cudaFuncSetAttribute(reinterpret_cast<const void *>(OFF_VARIANTS[v].fn),
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, OFF_VARIANTS[v].smem));
-  for (int v = 0; v < N_DIAG; v++)
-    if (DIAG_VARIANTS[v].smem > 0)
-      ICF_CUDA(ctx, cudaFuncSetAttribute(reinterpret_cast<const void *>(DIAG_VARIANTS[v].fn),
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, DIAG_VARIANTS[v].smem));
-  g_attrs_set[ctx->device] = true;
-  return ICF_OK;
-}
-
 int icf_launch_gather_off(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc, double mc,
                           double lam, double mu, double *vals, cudaStream_t s) {
   const icf_sell &S = ctx->sell_off;
   if (S.n_slices == 0) return ICF_OK;
   if (variant < 0 || variant >= N_OFF) variant = 0;
-  if (set_smem_attrs(ctx)) return ICF_ERR_CUDA;
-  const off_variant &V = OFF_VARIANTS[variant];
-  const gargs g{sc, mc, lam, mu};
-  V.fn<<<icf_blocks(32LL * S.n_slices, V.threads), V.threads, V.smem, s>>>(S.n_slices, S.meta, S.unit, S.codes,
-                                                                          es, cs, g, vals);
+  const unsigned grid = icf_blocks(32LL * S.n_slices, 256);
+  if (ctx->precision == ICF_FP32_MIXED) {
+    const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
+    OFF_VARIANTS[variant].f32<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, mixed_views(ctx, es, cs),
+                                                  g, vals);
+  } else {
+    fp64 st;
+    st.es = es;
+    st.cs = cs;
+    const gargs<double> g{sc, mc, lam, mu};
+    OFF_VARIANTS[variant].f64<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, st, g, vals);
+  }
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
@@ -374,11 +318,18 @@ int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const d
       if (DIAG_VARIANTS[v].lanes == S.lanes) variant = v;
     if (variant < 0) return icf_fail(ctx, ICF_ERR_STATE, "no diagonal gather for this list layout");
   }
-  if (set_smem_attrs(ctx)) return ICF_ERR_CUDA;
-  const diag_variant &V = DIAG_VARIANTS[variant];
-  const gargs g{sc, mc, lam, mu};
-  V.fn<<<icf_blocks(32LL * S.n_slices, V.threads), V.threads, V.smem, s>>>(S.n_slices, S.meta, S.unit, S.codes,
-                                                                          es, cs, g, vals, rhs);
+  const unsigned grid = icf_blocks(32LL * S.n_slices, 256);
+  if (ctx->precision == ICF_FP32_MIXED) {
+    const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
+    DIAG_VARIANTS[variant].f32<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes,
+                                                   mixed_views(ctx, es, cs), g, vals, rhs);
+  } else {
+    fp64 st;
+    st.es = es;
+    st.cs = cs;
+    const gargs<double> g{sc, mc, lam, mu};
+    DIAG_VARIANTS[variant].f64<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, st, g, vals, rhs);
+  }
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }

@@ -71,6 +71,17 @@ struct icf_sell {
   uint32_t *codes = nullptr;
 };
 
+// Device CG solver state (icf_solve.cu).
+struct icf_solver {
+  long long gen = -1;  // structure generation the lower-block index belongs to
+  int *lrows = nullptr, *lcols = nullptr, *lslot = nullptr;
+  long long rows_cap = 0, l_cap = 0, ls_cap = 0;
+  double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
+  long long x_cap = 0, r_cap = 0, z_cap = 0, p_cap = 0, q_cap = 0, d_cap = 0;
+  double *part = nullptr, *sc = nullptr;
+  double *h_sc = nullptr;  // pinned
+};
+
 // Parameters the kernels read, passed by value (they live in the kernel
 // parameter bank, i.e. constant memory).
 struct icf_dprm {
@@ -208,6 +219,13 @@ struct icf_ctx {
   struct icf_prof_state *prof = nullptr;
   // launch variants chosen by the autotuner (indices into the variant tables)
   int tune_tet = 0, tune_off = 0, tune_diag = 0;
+  // CZ history axes at the committed pmax/tmax (k_cz_hist), 18 doubles per CZ;
+  // refilled before the next assembly whenever hist_valid is false
+  double *d_czhist = nullptr;
+  bool hist_valid = false;
+  // linear solve; struct_gen counts structure builds
+  icf_solver solver;
+  long long struct_gen = 0;
 };
 
 #define ICF_PROF_MAX 16
@@ -233,6 +251,10 @@ const char *icf_tet_variant_name(int v);
 int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *va, double4 *es, cudaStream_t s);
 // rebuilds the diagonal gather lists for `lanes` lanes per row (icf_pattern.cu)
 int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes);
+int icf_ensure_cz_hist(icf_ctx *ctx, cudaStream_t s);
+int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, double *relres);
+void icf_free_solver(icf_ctx *ctx);
+int icf_launch_sumsq(icf_ctx *ctx, const double *d_x, long long n);
 int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out);
 int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant);
 int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const char **names,

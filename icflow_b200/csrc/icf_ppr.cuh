@@ -148,10 +148,20 @@ struct icf_law_c {
   int alpha_int, beta_int;  // alpha, beta when they are integers in [2, 16], else 0
 };
 
+// The axes at the committed history, N(pmax/deln) and T(tmax/delt).  They only
+// change when the damage state does, so the assembly reads them from a cache
+// (k_cz_hist) instead of evaluating two of its four axes every iteration.
+__device__ __forceinline__ void icf_cz_hist_axes(const icf_law_c &C, double deln, double delt, double pmax,
+                                                 double tmax, icf_axis &Np, icf_axis &Tm) {
+  Np = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, pmax / deln, C.alpha_int);
+  Tm = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, tmax / delt, C.beta_int);
+}
+
 // cohesive_law_thermodynamically_consistent (cz_kernels.h:37-174) on the axis
-// factors; pmax and tmax are updated in place.
-__device__ inline icf_law icf_cz_law_axes(const icf_law_c &C, double f_tn, double f_tt,
-                                          double deln, double delt, double &pmax,
+// factors, given the history axes Np, Tm of the incoming pmax, tmax; pmax and
+// tmax are updated in place.
+__device__ inline icf_law icf_cz_law_hist(const icf_law_c &C, double f_tn, double f_tt, double deln,
+                                          double delt, const icf_axis &Np, const icf_axis &Tm, double &pmax,
                                           double &tmax, double opn, double opt) {
   icf_law L;
   L.Tn = L.Tt = L.Dnn = L.Dtt = L.Dnt = 0;
@@ -167,8 +177,6 @@ __device__ inline icf_law icf_cz_law_axes(const icf_law_c &C, double f_tn, doubl
   L.contact = (opn < 0);
   const double eps_neg = -1e-9;
   const double thr_t = f_tt * 0.05, thr_n = f_tn * 0.05;
-  const icf_axis Np = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, pmax / deln, C.alpha_int);
-  const icf_axis Tm = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, tmax / delt, C.beta_int);
   const icf_axis To = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, opt / delt, C.beta_int);
   if (L.contact) {
     if (pmax != 0) {
@@ -255,6 +263,15 @@ __device__ inline icf_law icf_cz_law_axes(const icf_law_c &C, double f_tn, doubl
     L.Tn = L.Tt = L.Dnn = L.Dtt = L.Dnt = 0;
   }
   return L;
+}
+
+// The same, evaluating the history axes itself.
+__device__ inline icf_law icf_cz_law_axes(const icf_law_c &C, double f_tn, double f_tt,
+                                          double deln, double delt, double &pmax,
+                                          double &tmax, double opn, double opt) {
+  icf_axis Np, Tm;
+  icf_cz_hist_axes(C, deln, delt, pmax, tmax, Np, Tm);
+  return icf_cz_law_hist(C, f_tn, f_tt, deln, delt, Np, Tm, pmax, tmax, opn, opt);
 }
 
 // cohesive_law_thermodynamically_consistent (cz_kernels.h:37-174); pmax and

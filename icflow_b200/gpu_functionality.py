@@ -262,5 +262,27 @@ class GPU_Functionality:
         check(self.ctx, self.lib.icf_add_dx(self.ctx, dptr(dx), C.byref(nrm)))
         return nrm.value
 
+    def Solve(self, rel_tol: float = 1e-12, max_iter: int = 20000, want_dx: bool = False):
+        """Device CG solve of the last assembled system (replaces
+        LinearSystem.Solve / PARDISO).  Returns (iterations, relative residual,
+        dx or None)."""
+        it, rr = C.c_int(), C.c_double()
+        dx = np.zeros((self.linearSystem.N, 3)) if want_dx else None
+        check(self.ctx, self.lib.icf_solve(self.ctx, float(rel_tol), int(max_iter), dptr(dx), C.byref(it),
+                                           C.byref(rr)))
+        return it.value, rr.value, dx
+
+    def ApplyDx(self) -> float:
+        """_XtoDU with the device solution; returns NormOfDx (sum of dx^2)."""
+        nrm = C.c_double()
+        check(self.ctx, self.lib.icf_apply_dx(self.ctx, C.byref(nrm)))
+        return nrm.value
+
+    def ResidualNorm(self) -> float:
+        """||rhs|| of the last assembly."""
+        n2 = C.c_double()
+        check(self.ctx, self.lib.icf_residual_norm(self.ctx, C.byref(n2)))
+        return float(np.sqrt(n2.value))
+
     def AcceptTentativeValues(self, h: float):
         check(self.ctx, self.lib.icf_accept_tentative(self.ctx, float(h)))

@@ -1,0 +1,148 @@
+"""The learned Newton warm start (no counterpart in the reference).
+
+icFlow starts every Newton loop from du = v h (ImplicitModel3.cs:149-156).
+LearnedWarmStart replaces that guess for the active nodes with
+
+    du = v h + out_scale * net(x),   x = (u, v, a, du_{n-1}, du_{n-2})
+
+where net is the per-node MLP of the library (icf_mlp: 15 -> 64 -> 64 -> 3,
+GELU, BF16 weights, FP32 accumulation, trained on the GPU by the library's own
+forward and backward kernels).  Training data are the method's own
+trajectories: every accepted step contributes, per active node, the inputs
+seen at the start of the step and the correction the Newton loop found,
+du_accepted - v h.  A zero network gives back the plain guess, which stays
+the fallback (and the judge: both are run to the same residual tolerance).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from icflow_b200 import _lib
+
+NI, NO = 15, 3
+
+
+def features(u, v, a, du1, du2) -> np.ndarray:
+    return np.concatenate([u, v, a, du1, du2], axis=1).astype(np.float32)
+
+
+class MLP:
+    """Handle on the library's network (icf_mlp)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        rc = self.lib.icf_mlp_create(device, C.byref(h))
+        if rc:
+            raise _lib.ICFError(rc, "icf_mlp_create failed")
+        self.h = h
+        self.npar = self.lib.icf_mlp_param_count()
+
+    def _check(self, rc):
+        if rc:
+            raise _lib.ICFError(rc, self.lib.icf_mlp_last_error(self.h).decode())
+
+    def set_params(self, params: np.ndarray, norm: np.ndarray | None = None):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == self.npar
+        n = None if norm is None else np.ascontiguousarray(norm, np.float32)
+        self._check(self.lib.icf_mlp_set_params(self.h, p.ctypes.data_as(C.c_void_p),
+                                                 None if n is None else n.ctypes.data_as(C.c_void_p)))
+
+    def get_params(self):
+        p = np.zeros(self.npar, np.float32)
+        n = np.zeros(2 * NI + NO, np.float32)
+        self._check(self.lib.icf_mlp_get_params(self.h, p.ctypes.data_as(C.c_void_p), n.ctypes.data_as(C.c_void_p)))
+        return p, n
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, NI)
+        y = np.zeros((len(x), NO), np.float32)
+        self._check(self.lib.icf_mlp_forward(self.h, len(x), x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p)))
+        return y
+
+    def grad(self, x: np.ndarray, y: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, NI)
+        y = np.ascontiguousarray(y, np.float32).reshape(-1, NO)
+        g = np.zeros(self.npar, np.float32)
+        loss = C.c_float()
+        self._check(self.lib.icf_mlp_grad(self.h, len(x), x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
+                                          g.ctypes.data_as(C.c_void_p), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, x, y, epochs=20, batch=4096, lr=1e-3, seed=0) -> float:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, NI)
+        y = np.ascontiguousarray(y, np.float32).reshape(-1, NO)
+        loss = C.c_float()
+        self._check(self.lib.icf_mlp_train(self.h, len(x), x.ctypes.data_as(C.c_void_p),
+                                           y.ctypes.data_as(C.c_void_p), int(epochs), int(batch), float(lr),
+                                           int(seed), C.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if self.h:
+            self.lib.icf_mlp_destroy(self.h)
+            self.h = None
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-style initialisation, last layer zero (the untrained guess is the
+    plain one)."""
+    rng = np.random.default_rng(seed)
+    p = []
+    p.append(rng.normal(0, np.sqrt(2 / NI), (64, NI)))
+    p.append(np.zeros(64))
+    p.append(rng.normal(0, np.sqrt(2 / 64), (64, 64)))
+    p.append(np.zeros(64))
+    p.append(np.zeros((NO, 64)))
+    p.append(np.zeros(NO))
+    return np.concatenate([a.ravel() for a in p]).astype(np.float32)
+
+
+class LearnedWarmStart:
+    """Records trajectories, trains the network and serves as the `warm_start`
+    of ImplicitModel3.Step."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        self.net = MLP(device)
+        self.net.set_params(init_params(seed))
+        self.xs: list[np.ndarray] = []
+        self.ys: list[np.ndarray] = []
+        self.norm = None
+        self.seed = seed
+
+    # ---- data -----------------------------------------------------------------
+    def record(self, model, h, u, v, a, du1, du2, du_acc):
+        act = model.active
+        self.xs.append(features(u, v, a, du1, du2)[act])
+        self.ys.append((du_acc - v * h)[act].astype(np.float32))
+
+    def dataset(self):
+        return np.concatenate(self.xs), np.concatenate(self.ys)
+
+    # ---- training ---------------------------------------------------------------
+    def fit(self, epochs=30, batch=4096, lr=2e-3) -> float:
+        x, y = self.dataset()
+        shift = x.mean(axis=0)
+        sd = x.std(axis=0)
+        scale = 1.0 / np.where(sd > 0, sd, 1.0)
+        osd = y.std(axis=0)
+        out_scale = np.where(osd > 0, osd, 1.0)
+        self.norm = np.concatenate([shift, scale, out_scale]).astype(np.float32)
+        p, _ = self.net.get_params()
+        self.net.set_params(p, self.norm)
+        return self.net.train(x, y / out_scale, epochs=epochs, batch=min(batch, len(x)), lr=lr, seed=self.seed)
+
+    # ---- the guess --------------------------------------------------------------
+    def __call__(self, model, h, u, v, a):
+        du = v * h
+        if self.norm is None:
+            return du
+        x = features(u, v, a, model.du_prev, model.du_prev2)
+        corr = self.net.forward(x).astype(np.float64) * self.norm[2 * NI:]
+        return du + corr
+
+    def close(self):
+        self.net.close()

@@ -267,8 +267,49 @@ int icf_infer_tentative(icf_ctx *ctx, double h);
 /* _XtoDU (ImplicitModel3.cs:247-256): du += dx[altId] for active nodes;
  * dx has N*3 entries.  Returns sum(dx^2) in *norm (NormOfDx). */
 int icf_add_dx(icf_ctx *ctx, const double *dx, double *norm);
+/* The Newton linear solve on the device, replacing LinearSystem.Solve
+ * (LinearSystem.cs:48-64, MKL PARDISO on the host, after the D2H of
+ * :481-485).  Solves A dx = rhs for the matrix and rhs of the last assembly
+ * (A symmetric, stored as its upper blocks) by conjugate gradients with a
+ * 3x3 block-Jacobi preconditioner, to ||rhs - A dx|| <= rel_tol ||rhs||.
+ * dx[N*3] (nullable) receives the solution, which also stays on the device
+ * for icf_apply_dx.  ICF_ERR_NUMERIC if it does not converge in max_iter
+ * iterations or the matrix is not positive definite. */
+int icf_solve(icf_ctx *ctx, double rel_tol, int max_iter, double *dx, int *iters, double *relres);
+/* Sum of squares of the rhs of the last assembly (the Newton residual norm,
+ * squared).  No counterpart in the reference, whose convergence test is on
+ * the increment (LinearSystem.NormOfDx). */
+int icf_residual_norm(icf_ctx *ctx, double *norm2);
+/* _XtoDU with the device solution of icf_solve: du += dx for active nodes;
+ * *norm = sum(dx^2) (LinearSystem.NormOfDx, LinearSystem.cs:69-74). */
+int icf_apply_dx(icf_ctx *ctx, double *norm);
 /* AcceptTentativeValues (Node.cs:62-77). */
 int icf_accept_tentative(icf_ctx *ctx, double h);
+
+/* ---- learned Newton warm start (no counterpart in the reference) ----------
+ * icFlow starts each Newton loop from du = v h (ImplicitModel3.cs:149-156).
+ * icf_mlp is a per-node network 15 -> 64 -> 64 -> 3 with GELU, BF16 weights
+ * and FP32 accumulation (tensor-core mma), with its own training.  Inputs per
+ * node: u, v, a, du of the previous step, du of the step before (15 floats);
+ * they are normalised as (x - shift) * scale; the output is in units of
+ * out_scale.  norm = {shift[15], scale[15], out_scale[3]}.  Parameters
+ * (icf_mlp_param_count floats): W1[64][15] b1[64] W2[64][64] b2[64] W3[3][64]
+ * b3[3].  All calls are synchronous; host arrays are row-major per node. */
+typedef struct icf_mlp icf_mlp;
+int icf_mlp_create(int device, icf_mlp **out);
+int icf_mlp_destroy(icf_mlp *m);
+const char *icf_mlp_last_error(const icf_mlp *m);
+int icf_mlp_param_count(void);
+int icf_mlp_set_params(icf_mlp *m, const float *params, const float *norm);
+int icf_mlp_get_params(icf_mlp *m, float *params, float *norm);
+/* y[n*3] = network(x[n*15]) */
+int icf_mlp_forward(icf_mlp *m, int n, const float *x, float *y);
+/* gradient of the mean squared error over n nodes and 3 outputs */
+int icf_mlp_grad(icf_mlp *m, int n, const float *x, const float *y, float *grad, float *loss);
+/* minibatch Adam on the device; epochs over a seeded shuffle; *loss = final
+ * mean squared error over all n */
+int icf_mlp_train(icf_mlp *m, int n, const float *x, const float *y, int epochs, int batch, float lr,
+                  unsigned long long seed, float *loss);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,92 @@
+"""The learned warm start on the GPU: the network's forward and gradient
+kernels against the CPU restatement, training on the device, and what the
+trained network gains over the plain guess du = v h at the same residual
+tolerance."""
+import numpy as np
+import pytest
+
+from icflow_b200.implicit_model import ImplicitModel3
+from icflow_b200.warm_start import MLP, LearnedWarmStart, init_params
+from oracle.mlp_oracle import NI, NO, forward, loss_and_grad
+from tests.test_gpu_newton import _prms, fast_cantilever
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(seed=0, n=3000):
+    rng = np.random.default_rng(seed)
+    p = init_params(seed)
+    p[-(NO * 64 + NO):] = rng.normal(0, 0.2, NO * 64 + NO).astype(np.float32)
+    norm = np.concatenate([rng.normal(size=NI), rng.uniform(0.5, 2, NI), np.ones(NO)]).astype(np.float32)
+    x = rng.normal(size=(n, NI)).astype(np.float32) / norm[NI:2 * NI] + norm[:NI]
+    return p, norm, x
+
+
+def test_forward_matches_cpu():
+    p, norm, x = _setup(0, 1037)  # not a multiple of 16
+    net = MLP()
+    net.set_params(p, norm)
+    y = net.forward(x)
+    ref = forward(p, norm, x)["y"]
+    err = np.abs(y - ref).max() / np.abs(ref).max()
+    assert err <= 2e-3, err
+    net.close()
+
+
+def test_gradient_matches_cpu():
+    p, norm, x = _setup(1, 777)
+    t = np.random.default_rng(2).normal(size=(len(x), NO)).astype(np.float32)
+    net = MLP()
+    net.set_params(p, norm)
+    g, loss = net.grad(x, t)
+    lref, gref = loss_and_grad(p, norm, x, t)
+    assert abs(loss - lref) <= 1e-3 * lref
+    err = np.abs(g - gref).max() / np.abs(gref).max()
+    print(f"MLP gradient vs CPU restatement: {err:.2e} (max-norm relative)")
+    assert err <= 1e-2, err
+    # identical on a second run (fixed-order reductions)
+    g2, _ = net.grad(x, t)
+    assert np.array_equal(g, g2)
+    net.close()
+
+
+def test_training_fits_a_smooth_map():
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=(20000, NI)).astype(np.float32)
+    t = np.stack([np.sin(x[:, 0]) + 0.5 * x[:, 3], x[:, 6] * x[:, 9] * 0.3, np.tanh(x[:, 12] - x[:, 1])], 1)
+    net = MLP()
+    net.set_params(init_params(0), np.concatenate([np.zeros(NI), np.ones(NI), np.ones(NO)]).astype(np.float32))
+    _, l0 = net.grad(x, t)
+    l1 = net.train(x, t, epochs=40, batch=1024, lr=3e-3, seed=1)
+    print(f"training: loss {l0:.3e} -> {l1:.3e}")
+    assert l1 < 0.05 * l0
+    net.close()
+
+
+def test_learned_warm_start_reduces_newton_iterations():
+    """Train on the method's own trajectory (tip driven at 0.2 m/s), then run a
+    new trajectory (0.25 m/s) with both guesses to a residual tolerance of
+    1e-8 of the zero-increment residual, minIterations 1."""
+    p = _prms()
+    p.minIterations = 1
+    p.maxIterations = 20
+    ws = LearnedWarmStart(seed=0)
+    g = ImplicitModel3(fast_cantilever(0.2), p, convergence="residual", res_tol=1e-8)
+    g.recorder = ws
+    for _ in range(60):
+        g.Step()
+    g.close()
+    loss = ws.fit(epochs=150, batch=2048, lr=2e-3)
+    its = {}
+    for name, warm in (("plain", None), ("learned", ws)):
+        m = ImplicitModel3(fast_cantilever(0.25), p, convergence="residual", res_tol=1e-8)
+        for _ in range(40):
+            s = m.Step(warm_start=warm)
+            assert s.converged
+        its[name] = np.mean([s.iterations for s in m.history[2:]])
+        m.close()
+    red = 1 - its["learned"] / its["plain"]
+    print(f"warm start: training loss {loss:.3e}; Newton iterations/step plain {its['plain']:.2f}, "
+          f"learned {its['learned']:.2f} ({100 * red:.0f}% fewer)")
+    assert its["learned"] <= its["plain"]
+    ws.close()

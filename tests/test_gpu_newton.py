@@ -1,0 +1,92 @@
+"""Whole time steps on the device (ImplicitModel3 mirror): N-step parity of
+displacements and damage state with the CPU twin (oracle assembly + direct
+solve), FP32-mixed against FP64 at equal converged displacements, and a
+contact run."""
+import numpy as np
+import pytest
+
+from icflow_b200 import mesh as M
+from icflow_b200.implicit_model import ImplicitModel3
+from icflow_b200.model_prms import config_prms
+from tests.newton_oracle import OracleModel
+
+pytestmark = pytest.mark.gpu
+
+
+def fast_cantilever(rate=0.2):
+    """cfg0 beam with the tip driven at `rate` m/s so that the mid-span CZs
+    damage within a few dozen steps."""
+    c = M.cantilever()
+    m = c.meshes[0]
+    tip = np.isclose(m.x0[:, 0], 0.6)
+    m.forced = [(tip, 0.0, 0.0, rate, 1.0)]
+    return c
+
+
+def _prms(eps=0.005):
+    p = config_prms()
+    p.InitialTimeStep = 1e-4
+    p.ConvergenceEpsilon = eps
+    return p
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def test_newton_steps_match_oracle():
+    """40 steps: per-step iteration counts equal; displacements, velocities
+    and CZ damage state (pmax, tmax, failed) match the CPU twin."""
+    c = fast_cantilever()
+    p = _prms()
+    g = ImplicitModel3(c, p)
+    o = OracleModel(c, p)
+    for _ in range(40):
+        sg = g.Step()
+        so = o.Step()
+        assert sg.iterations == so
+    u, v, a, cz = g.state()
+    assert _rel(u, o.u) <= 1e-8, _rel(u, o.u)
+    assert _rel(v, o.v) <= 1e-6, _rel(v, o.v)
+    assert o.pmax.max() > 0, "no damage developed; the case does not test the CZ commit"
+    assert _rel(cz["pmax"], o.pmax) <= 1e-8 and _rel(cz["tmax"], o.tmax) <= 1e-8
+    assert np.array_equal(cz["failed"], o.failed)
+    g.close()
+
+
+def test_fp32_mixed_equal_converged_displacements():
+    """FP32 Hessians converge to the FP64 displacements within 1e-6 relative
+    (the rhs, and so the converged solution, is FP64 in both)."""
+    c = fast_cantilever()
+    p = _prms(eps=1e-9)
+    runs = []
+    for prec in (0, 1):
+        g = ImplicitModel3(c, p, precision=prec)
+        for _ in range(30):
+            g.Step()
+        u, _, _, cz = g.state()
+        runs.append((u, cz, [s.iterations for s in g.history]))
+        g.close()
+    (u64, cz64, it64), (u32, cz32, it32) = runs
+    err = _rel(u32, u64)
+    print(f"FP32-mixed vs FP64 after 30 steps: displacement {err:.2e}; iterations {sum(it32)} vs {sum(it64)}")
+    assert err <= 1e-6
+    assert _rel(cz32["pmax"], cz64["pmax"]) <= 1e-5
+    assert np.array_equal(cz32["failed"], cz64["failed"])
+
+
+def test_contact_steps_converge():
+    """Polycrystal between closing platens: the Newton loop with device narrow
+    phase, pattern rebuild, assembly and CG converges every step."""
+    c = M.polycrystal(n=6, grains=6, seed=1, platens=True, gap=-0.2)
+    p = config_prms(penaltyK=1e8)
+    p.InitialTimeStep = 1e-5
+    p.ConvergenceEpsilon = 1e-6
+    p.CollisionScheme = 1
+    sig = M.lognormal_strengths(len(c.czs), seed=1, granule_pairs=c.meshes[0].cz_grains)
+    g = ImplicitModel3(c, p, strengths=sig, contact=True)
+    for _ in range(8):
+        s = g.Step()
+        assert s.converged and not s.diverged, s
+    assert any(s.n_impacts > 0 for s in g.history)
+    g.close()

@@ -261,3 +261,42 @@ def test_every_launch_variant_and_autotune(O):
     vals2, rhs2 = gf.TransferLinearSystemToHost()
     assert np.array_equal(vals, vals2) and np.array_equal(rhs, rhs2)
     gf.close()
+
+
+FP32_TOL = 1e-5  # FP32-mixed blocks, normwise per block row against the FP64 oracle
+
+
+@pytest.mark.parametrize("case", ["cantilever_damaged", "polycrystal_contact"])
+def test_fp32_mixed_error_report(O, case):
+    """FP32-mixed assembly against the FP64 oracle, per field: Hessian blocks
+    within FP32_TOL normwise per block row; rhs, tentative CZ state and flags
+    as in FP64 (the law, tractions, forces and rhs stay FP64)."""
+    from icflow_b200 import _lib
+
+    prms = config_prms(penaltyK=1e8)
+    if case == "cantilever_damaged":
+        coll = M.cantilever()
+        state = random_state(coll, 7, du=8e-6)
+        pairs = None
+    else:
+        coll = M.polycrystal(n=8, grains=6, seed=2, platens=True, gap=-0.3)
+        state = random_state(coll, 8, du=2e-6)
+        pairs = M.candidate_pairs(coll, coll.x0 + state[0])
+    gf = _gf(coll, prms)
+    _lib.check(gf.ctx, gf.lib.icf_set_precision(gf.ctx, 1))
+    pmax, tmax, failed = _zeros_cz(coll)
+    a = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+    p = orc_prms_from(O, prms)
+    o = oracle_assemble(O, p, coll, state, H, pmax, tmax, gf.c_itet if pairs is not None else
+                        np.zeros((0, 4), np.int32))
+    assert np.array_equal(a["rows"], o["rows"]) and np.array_equal(a["cols"], o["cols"])
+    err_vals = rowwise_rel(o["rows"], o["vals"], a["vals"])
+    err_rhs = vec_rel(o["rhs"], a["rhs"])
+    assert 0 < err_vals <= FP32_TOL, err_vals
+    assert err_rhs <= FP64_TOL, err_rhs
+    sel = o["czsel"]
+    if len(sel):
+        assert np.array_equal(a["flags"][sel], o["flags"])
+        assert vec_rel(o["tent"], a["tent"][sel]) <= FP64_TOL
+    print(f"{case}: FP32-mixed vs FP64 oracle: blocks {err_vals:.2e} (rowwise), rhs {err_rhs:.2e}")
+    gf.close()
