@@ -2,11 +2,17 @@
 
 One step = one Newton assembly (zero + tetrahedra + cohesive zones with damage
 state and flags + contact response -> BCSR values and rhs) of a fixed
-structure, on the polycrystal-compression workload: 1 mm cube, 32^3
-hexahedra split into 196,608 tets, 128 Voronoi grains with cohesive zones on
-every grain boundary (per-boundary lognormal strengths, mean 1 MPa, cv 0.2),
-two rigid platens overlapping the cube by a quarter cell (penalty 1e8),
-dt = 1e-5 s, FP64.  Inputs are synthetic (seeded), as icFlow ships no setups.
+structure.  Workloads (--workload):
+  cfg1 (default)  polycrystal compression: 1 mm cube, 32^3 hexahedra split into
+                  196,608 tets, 128 Voronoi grains with cohesive zones on every
+                  grain boundary (per-boundary lognormal strengths, mean 1 MPa,
+                  cv 0.2), two rigid platens overlapping the cube by a quarter
+                  cell (penalty 1e8), dt = 1e-5 s, FP64;
+  cfg2            the same at 64^3 hexahedra (1,572,864 tets), 2048 grains;
+  cfg3            64 independent cubes of uneven size (tets U[5k, 60k], grains
+                  U[8, 64]) assembled together in one graph launch, launch
+                  variants autotuned, FP32-mixed by default.
+Inputs are synthetic (seeded), as icFlow ships no setups.
 
   value  assemblies/s with inputs resident in HBM (device events around each
          step; L2 is flushed between steps by writing a 256 MiB buffer, outside
@@ -16,9 +22,10 @@ dt = 1e-5 s, FP64.  Inputs are synthetic (seeded), as icFlow ships no setups.
          rhs into pinned memory, every step
 
 `--impl reference` times the reference's own kernels compiled for the host
-(oracle/_ref, all host threads) on the same workload.  Under torchrun each rank
-assembles its own specimen (seed = rank, weak scaling, no collective in the
-data path); timing is max over ranks.
+(oracle/_ref, all host threads) on the same workload.  Under torchrun, for
+cfg1/cfg2 each rank assembles its own specimen (seed = rank, weak scaling);
+for cfg3 the 64 specimens are split across the ranks (strong scaling).  No
+collective touches the data path; timing is max over ranks.
 """
 from __future__ import annotations
 
@@ -44,24 +51,29 @@ FLUSH_BYTES = 256 << 20
 
 
 WORKLOADS = {
-    # polycrystal compression, 1 mm cube: (hexes per side, grains)
+    # polycrystal compression, 1 mm cube: (hexes per side, grains); one
+    # specimen per rank (weak scaling)
     "cfg1": (32, 128),    # 196,608 tets, ~35k CZs
-    "cfg2": (64, 2048),   # 1,572,864 tets, ~390k CZs
+    "cfg2": (64, 2048),   # 1,572,864 tets, ~396k CZs
+    # 64 uneven specimens (tets U[5k, 60k], grains U[8, 64]) assembled together
+    # in one graph launch; the specimens are split across ranks (strong scaling)
+    "cfg3": None,
 }
+N_SPECIMENS = 64
 
 
-def workload_name(n: int, grains: int) -> str:
+def workload_name(workload: str, n: int = 0, grains: int = 0) -> str:
+    if workload == "cfg3":
+        return (f"{N_SPECIMENS} independent polycrystal cubes, tets U[5k,60k], grains U[8,64], CZs on grain "
+                "boundaries, per-boundary lognormal strengths, one graph launch per assembly, dt 1e-5")
     return (f"polycrystal compression, 1 mm cube, {n}^3 hex -> 6 tets ({6 * n ** 3} tets), {grains} grains, "
             "CZs on grain boundaries, rigid platens in contact, dt 1e-5")
 
 
-def build_workload(seed: int, n: int = 32, grains: int = 128):
-    from icflow_b200 import mesh as M
-
-    coll = M.polycrystal(n=n, grains=grains, seed=seed, platens=True, gap=-0.25)
+def _state(coll, seed):
     rng = np.random.default_rng(seed + 101)
     nn = len(coll.x0)
-    # a compressed state: uniform strain 1e-4 toward the mid-plane plus noise
+    # a compressed state: uniform strain 1e-4 toward each specimen's mid-plane plus noise
     zc = 0.5e-3
     un = np.zeros((nn, 3))
     un[:, 2] = -1e-4 * (coll.x0[:, 2] - zc)
@@ -69,9 +81,29 @@ def build_workload(seed: int, n: int = 32, grains: int = 128):
     un[coll.anchored] = 0.0
     vn = (rng.random((nn, 3)) - 0.5) * 1e-3
     an = (rng.random((nn, 3)) - 0.5) * 1e-1
+    return un, vn, an
+
+
+def build_workload(workload: str, seed: int, rank: int = 0, world: int = 1):
+    """(collection, (un, vn, an), per-CZ strengths, candidate pairs, units of
+    the metric this rank's collection holds)."""
+    from icflow_b200 import mesh as M
+
+    if workload == "cfg3":
+        from icflow_b200.shard import shard
+
+        mine = shard(N_SPECIMENS, rank, world)
+        coll, info = M.batched_specimens(N_SPECIMENS, seed=seed, only=mine)
+        sig = np.concatenate([M.lognormal_strengths(len(m.czs), seed=1000 * seed + i, granule_pairs=m.cz_grains)
+                              for (i, _, _), m in zip(info, coll.meshes)])
+        pairs = np.zeros((0, 2), np.int32)
+        return coll, _state(coll, seed), sig, pairs, len(mine) / N_SPECIMENS
+    n, grains = WORKLOADS[workload]
+    coll = M.polycrystal(n=n, grains=grains, seed=seed, platens=True, gap=-0.25)
+    un, vn, an = _state(coll, seed)
     sig = M.lognormal_strengths(len(coll.czs), seed=seed, granule_pairs=coll.meshes[0].cz_grains)
     pairs = M.candidate_pairs(coll, coll.x0 + un)
-    return coll, (un, vn, an), sig, pairs
+    return coll, (un, vn, an), sig, pairs, 1.0
 
 
 def algorithmic_bytes(nnz, n_active, n_nodes, n_tet, n_cz, n_imp) -> int:
@@ -140,10 +172,9 @@ class ClockSampler:
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from icflow_b200.shard import dist_env as env
+
+    return env()
 
 
 def measured_peak():
@@ -228,8 +259,7 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    n, grains = WORKLOADS[args.workload]
-    coll, state, sig, pairs = build_workload(0, n, grains)
+    coll, state, sig, pairs, _ = build_workload(args.workload, 0)
     steps = max(args.steps, 1)
     rate, threads, kind, sample = cpu_baseline(coll, state, sig, pairs,
                                                bound_s=min(60.0, 2.0 * steps))
@@ -237,7 +267,7 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 / rate, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": workload_name(n, grains),
+            "config": {"workload": workload_name(args.workload, *(WORKLOADS[args.workload] or ())),
                        "tets": int(len(coll.elems)), "czs": int(len(coll.czs))},
             "cpu_baseline": {"value": rate, "unit": "assemblies/s", "cores": threads, "kind": kind,
                              "sample": sample},
@@ -264,14 +294,17 @@ def run_ours(args):
     dev = local if ws > 1 else 0
     torch.cuda.set_device(dev)
 
-    n, grains = WORKLOADS[args.workload]
-    coll, state, sig, pairs = build_workload(rank, n, grains)
+    # cfg1/cfg2: one specimen per rank (seed = rank); cfg3: this rank's share
+    # of the 64 specimens (seed 0 for all ranks)
+    batched = args.workload == "cfg3"
+    coll, state, sig, pairs, units = build_workload(args.workload, 0 if batched else rank, rank, ws)
     prms = config_prms(penaltyK=1e8)
     gf = GPU_Functionality(dev)
     gf.prms = prms
     gf.mc = coll
     gf.SetConstants()
-    gf.SetPrecision(1 if args.precision == "mixed" else 0)
+    precision = args.precision or ("mixed" if batched else "fp64")
+    gf.SetPrecision(1 if precision == "mixed" else 0)
     gf.TransferStaticDataToDevice()
     gf.SetCZStrengths(sig, sig)
     un, vn, an = state
@@ -342,10 +375,10 @@ def run_ours(args):
     # one stream with an event after each (no overlap between streams)
     kernels = gf.ProfileAssembly(H, reps=max(args.steps, 10))
 
-    if ws > 1:
-        t = torch.tensor([ms_dev, ms_e2e], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_dev, ms_e2e = float(t[0]), float(t[1])
+    from icflow_b200.shard import reduce_max, reduce_sum
+
+    ms_dev, ms_e2e = reduce_max([ms_dev, ms_e2e], device=dev)
+    total_units = reduce_sum([units], device=dev)[0]
 
     B = algorithmic_bytes(nnz, N, len(coll.x0), len(coll.elems), nc, len(imps))
     peak, peak_kind = measured_peak()
@@ -360,12 +393,14 @@ def run_ours(args):
     line = None
     if rank == 0:
         line = {
-            "metric": METRIC, "value": ws * 1000.0 / ms_dev, "unit": "assemblies/s", "n_gpus": ws,
+            "metric": METRIC, "value": total_units * 1000.0 / ms_dev, "unit": "assemblies/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32 Hessians, f64 rotation/law/rhs/accumulation",
+            "higher_is_better": True, "scaling": "strong" if batched else "weak", "vs_baseline": None,
+            "dtype": "f64" if precision == "fp64" else "f32 Hessians, f64 rotation/law/rhs/accumulation",
             "data": "synthetic (seeded polycrystal; no public dataset exists for this path)",
-            "config": {"workload": workload_name(n, grains),
+            "config": {"workload": workload_name(args.workload, *(WORKLOADS[args.workload] or ())),
+                       "specimens_per_assembly": N_SPECIMENS if batched else 1,
+                       "specimens_rank0": int(len(coll.meshes)) if batched else 1,
                        "tets": int(len(coll.elems)), "czs": int(nc), "nodes": int(len(coll.x0)),
                        "active_rows": int(N), "blocks": int(nnz), "impacts": int(len(imps)),
                        "l2": "flushed between steps (256 MiB write), outside the timed region",
@@ -381,7 +416,7 @@ def run_ours(args):
                          "kernels": [{"name": k["name"], "ms": round(k["ms"], 5), "share": round(k["share"], 4),
                                       "bytes": k["bytes"], "GBps": round(k["GBps"], 1),
                                       "frac": round(k["GBps"] / peak, 4)} for k in kernels]},
-            "e2e": {"value": ws * 1000.0 / ms_e2e, "unit": "assemblies/s",
+            "e2e": {"value": total_units * 1000.0 / ms_e2e, "unit": "assemblies/s",
                     "h2d_bytes_per_step": int(3 * un.nbytes), "d2h_bytes_per_step": int(8 * (9 * nnz + 3 * N))},
             "gpu_launches": launches_per_step * args.steps,
             "autotune": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in t.items()} for t in tune],
@@ -409,8 +444,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="cfg1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch variants")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                    help="fp64, or FP32 Hessian arithmetic with FP64 rotation, law, rhs and accumulation")
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="fp64, or FP32 Hessian arithmetic with FP64 rotation, law, rhs and accumulation "
+                         "(default: fp64 for cfg1/cfg2, mixed for cfg3)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

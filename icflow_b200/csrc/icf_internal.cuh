@@ -71,13 +71,14 @@ struct icf_sell {
   uint32_t *codes = nullptr;
 };
 
-// Device CG solver state (icf_solve.cu).
+// Device MINRES solver state (icf_solve.cu).
 struct icf_solver {
   long long gen = -1;  // structure generation the lower-block index belongs to
   int *lrows = nullptr, *lcols = nullptr, *lslot = nullptr;
   long long rows_cap = 0, l_cap = 0, ls_cap = 0;
   double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
-  long long x_cap = 0, r_cap = 0, z_cap = 0, p_cap = 0, q_cap = 0, d_cap = 0;
+  double *w = nullptr, *w2 = nullptr;
+  long long x_cap = 0, r_cap = 0, z_cap = 0, p_cap = 0, q_cap = 0, d_cap = 0, w_cap = 0, w2_cap = 0;
   double *part = nullptr, *sc = nullptr;
   double *h_sc = nullptr;  // pinned
 };

@@ -3,15 +3,17 @@
 // The reference copies the upper-triangular BCSR matrix and the rhs to the
 // host every Newton iteration and solves them with MKL PARDISO (symmetric,
 // mtype -2, BSR 3x3; LinearSystem.cs:45-64, PardisoLoader2/dllmain.cpp:30-79).
-// Here the system stays where it was assembled and is solved by conjugate
-// gradients with a block-Jacobi (3x3) preconditioner:
+// Here the system stays where it was assembled and is solved by
+// the minimal residual method (MINRES: the matrix is symmetric but, with
+// softening cohesive zones, may be indefinite, as PARDISO's mtype -2 allows)
+// with a block-Jacobi (3x3) preconditioner:
 //   - A x uses the stored upper blocks directly and their transposes through
 //     a per-structure index of the lower blocks (row = column of the upper
 //     block), four lanes per row and a fixed shuffle tree, so every product
 //     is deterministic;
 //   - dot products reduce per block and then in one block, in a fixed order;
-//   - the CG scalars live on the device; the host reads the residual every
-//     few iterations only to stop.
+//   - the MINRES scalars and plane rotations live on the device; the host
+//     reads the residual estimate every few iterations only to stop.
 // The solution stays on the device for icf_apply_dx (du += dx, the
 // reference's _XtoDU, ImplicitModel3.cs:247-256).
 #include <cub/cub.cuh>
@@ -128,98 +130,167 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return s;
 }
 
-// partial sums of a.b (and of c.d when c != nullptr) per block
-__global__ void __launch_bounds__(256) k_dot2(int n, const double *__restrict__ a, const double *__restrict__ b,
-                                              const double *__restrict__ c, const double *__restrict__ d,
-                                              double *__restrict__ part) {
-  __shared__ double sh[8];
-  double s1 = 0, s2 = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    s1 += a[i] * b[i];
-    if (c) s2 += c[i] * d[i];
-  }
-  const double t1 = block_sum(s1, sh);
-  const double t2 = block_sum(s2, sh);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = t1;
-    part[RED_BLOCKS + blockIdx.x] = t2;
-  }
+// ---- preconditioned MINRES (Paige & Saunders 1975), the matrix symmetric and
+// possibly indefinite (softening cohesive zones), the preconditioner the SPD
+// 3x3 block-Jacobi M.  Scalars live on the device:
+//   sc[0] beta  [1] oldb  [2] alfa  [3] dbar  [4] epsln  [5] oldeps
+//   sc[6] cs    [7] sn    [8] phibar [9] beta1 [10] phi   [11] delta
+//   sc[12] gamma [13] breakdown flag
+constexpr int NSC = 16;
+
+// y = Dinv r for 3-vectors of N rows
+__device__ __forceinline__ void apply_dinv(const double *D, const double r[3], double z[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) z[k] = D[3 * k] * r[0] + D[3 * k + 1] * r[1] + D[3 * k + 2] * r[2];
 }
 
-// scalars: [0] rz  [1] alpha  [2] beta  [3] rr  [4] bb  [5] breakdown
-__global__ void k_alpha(const double *__restrict__ part, double *__restrict__ sc) {
-  if (threadIdx.x != 0) return;
-  double pq = 0;
-  for (int i = 0; i < RED_BLOCKS; i++) pq += part[i];
-  if (!(pq > 0) || !isfinite(pq)) {
-    sc[1] = 0;
-    sc[5] = 1;
-  } else {
-    sc[1] = sc[0] / pq;
-  }
-}
-__global__ void k_beta(const double *__restrict__ part, double *__restrict__ sc, int init) {
-  if (threadIdx.x != 0) return;
-  double rz = 0, rr = 0;
-  for (int i = 0; i < RED_BLOCKS; i++) rz += part[i];
-  for (int i = 0; i < RED_BLOCKS; i++) rr += part[RED_BLOCKS + i];
-  if (init) {
-    sc[4] = rr;
-    sc[5] = 0;
-    sc[2] = 0;
-  } else {
-    sc[2] = sc[0] > 0 ? rz / sc[0] : 0;
-  }
-  sc[0] = rz;
-  sc[3] = rr;
-}
-
-// x += alpha p; r -= alpha q; z = Dinv r
-__global__ void k_update(int N, const double *__restrict__ sc, const double *__restrict__ p,
-                         const double *__restrict__ q, const double *__restrict__ dinv, double *__restrict__ x,
-                         double *__restrict__ r, double *__restrict__ z) {
+// start: x = 0, r1 = r2 = b, y = Dinv b, w = w2 = 0
+__global__ void k_mr_start(int N, const double *__restrict__ b, const double *__restrict__ dinv,
+                           double *__restrict__ x, double *__restrict__ r1, double *__restrict__ r2,
+                           double *__restrict__ y, double *__restrict__ w, double *__restrict__ w2) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  const double al = sc[1];
-  double rv[3];
+  double rv[3], z[3];
 #pragma unroll
-  for (int k = 0; k < 3; k++) {
-    const size_t j = 3 * (size_t)i + k;
-    x[j] += al * p[j];
-    rv[k] = r[j] - al * q[j];
-    r[j] = rv[k];
-  }
-  const double *D = dinv + 9 * (size_t)i;
-#pragma unroll
-  for (int k = 0; k < 3; k++) z[3 * (size_t)i + k] = D[3 * k] * rv[0] + D[3 * k + 1] * rv[1] + D[3 * k + 2] * rv[2];
-}
-
-// start: x = 0, r = b, z = Dinv r
-__global__ void k_start(int N, const double *__restrict__ b, const double *__restrict__ dinv, double *__restrict__ x,
-                        double *__restrict__ r, double *__restrict__ z, double *__restrict__ p) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  double rv[3];
+  for (int k = 0; k < 3; k++) rv[k] = b[3 * (size_t)i + k];
+  apply_dinv(dinv + 9 * (size_t)i, rv, z);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const size_t j = 3 * (size_t)i + k;
     x[j] = 0;
-    rv[k] = b[j];
-    r[j] = rv[k];
-  }
-  const double *D = dinv + 9 * (size_t)i;
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    const double zk = D[3 * k] * rv[0] + D[3 * k + 1] * rv[1] + D[3 * k + 2] * rv[2];
-    z[3 * (size_t)i + k] = zk;
-    p[3 * (size_t)i + k] = zk;
+    r1[j] = rv[k];
+    r2[j] = rv[k];
+    y[j] = z[k];
+    w[j] = 0;
+    w2[j] = 0;
   }
 }
 
-__global__ void k_newp(int n, const double *__restrict__ sc, const double *__restrict__ z, double *__restrict__ p) {
+__global__ void k_mr_init(const double *__restrict__ part, double *__restrict__ sc) {
+  if (threadIdx.x != 0) return;
+  double b2 = 0;
+  for (int i = 0; i < RED_BLOCKS; i++) b2 += part[i];
+  for (int k = 0; k < NSC; k++) sc[k] = 0;
+  if (b2 < 0 || !isfinite(b2)) sc[13] = 1;
+  const double beta1 = b2 > 0 ? sqrt(b2) : 0.0;
+  sc[0] = beta1;  // beta
+  sc[1] = 0;      // oldb
+  sc[6] = -1;     // cs
+  sc[7] = 0;      // sn
+  sc[8] = beta1;  // phibar
+  sc[9] = beta1;  // beta1
+}
+
+// v = y / beta
+__global__ void k_mr_v(int n, const double *__restrict__ sc, const double *__restrict__ y, double *__restrict__ v) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  p[i] = z[i] + sc[2] * p[i];
+  v[i] = sc[0] > 0 ? y[i] / sc[0] : 0.0;  // beta = 0: converged exactly, nothing left to add
+}
+
+// y -= (beta / oldb) r1 (after the first iteration); partial sums of v.y
+__global__ void __launch_bounds__(256) k_mr_a(int n, int first, const double *__restrict__ sc,
+                                              const double *__restrict__ r1, const double *__restrict__ v,
+                                              double *__restrict__ y, double *__restrict__ part) {
+  __shared__ double sh[8];
+  const double f = (first || !(sc[1] > 0)) ? 0.0 : sc[0] / sc[1];
+  double acc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double yi = y[i] - f * r1[i];
+    y[i] = yi;
+    acc += v[i] * yi;
+  }
+  const double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void k_mr_alfa(const double *__restrict__ part, double *__restrict__ sc) {
+  if (threadIdx.x != 0) return;
+  double a = 0;
+  for (int i = 0; i < RED_BLOCKS; i++) a += part[i];
+  sc[2] = a;
+}
+
+// y -= (alfa / beta) r2; r1 = r2; r2 = y; y = Dinv r2; partial sums of r2.y
+__global__ void __launch_bounds__(256) k_mr_b(int N, const double *__restrict__ sc, const double *__restrict__ dinv,
+                                              double *__restrict__ r1, double *__restrict__ r2,
+                                              double *__restrict__ y, double *__restrict__ part) {
+  __shared__ double sh[8];
+  const double f = sc[0] > 0 ? sc[2] / sc[0] : 0.0;
+  double acc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    double yv[3], z[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const size_t j = 3 * (size_t)i + k;
+      yv[k] = y[j] - f * r2[j];
+      r1[j] = r2[j];
+      r2[j] = yv[k];
+    }
+    apply_dinv(dinv + 9 * (size_t)i, yv, z);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      y[3 * (size_t)i + k] = z[k];
+      acc += yv[k] * z[k];
+    }
+  }
+  const double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// the plane rotation of this iteration
+__global__ void k_mr_rot(const double *__restrict__ part, double *__restrict__ sc) {
+  if (threadIdx.x != 0) return;
+  double b2 = 0;
+  for (int i = 0; i < RED_BLOCKS; i++) b2 += part[i];
+  if (b2 < 0 || !isfinite(b2)) {
+    sc[13] = 1;
+    b2 = 0;
+  }
+  const double oldb = sc[0], beta = sqrt(b2), alfa = sc[2];
+  const double cs = sc[6], sn = sc[7], dbar = sc[3];
+  const double oldeps = sc[4];
+  const double delta = cs * dbar + sn * alfa;
+  const double gbar = sn * dbar - cs * alfa;
+  const double epsln = sn * beta;
+  const double dbar2 = -cs * beta;
+  double gamma = sqrt(gbar * gbar + beta * beta);
+  if (gamma < 1e-300) gamma = 1e-300;
+  const double cs2 = gbar / gamma, sn2 = beta / gamma;
+  const double phi = cs2 * sc[8];
+  sc[8] = sn2 * sc[8];  // phibar
+  sc[1] = oldb;
+  sc[0] = beta;
+  sc[3] = dbar2;
+  sc[4] = epsln;
+  sc[5] = oldeps;
+  sc[6] = cs2;
+  sc[7] = sn2;
+  sc[10] = phi;
+  sc[11] = delta;
+  sc[12] = gamma;
+}
+
+// w1 = w2; w2 = w; w = (v - oldeps w1 - delta w2) / gamma; x += phi w
+__global__ void k_mr_x(int n, const double *__restrict__ sc, const double *__restrict__ v, double *__restrict__ w,
+                       double *__restrict__ w2, double *__restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double w1 = w2[i], wo = w[i];
+  const double wn = (v[i] - sc[5] * w1 - sc[11] * wo) / sc[12];
+  w2[i] = wo;
+  w[i] = wn;
+  x[i] += sc[10] * wn;
+}
+
+// partial sums of b.y (the start's preconditioned norm)
+__global__ void __launch_bounds__(256) k_dot(int n, const double *__restrict__ a, const double *__restrict__ b,
+                                             double *__restrict__ part) {
+  __shared__ double sh[8];
+  double s1 = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s1 += a[i] * b[i];
+  const double t = block_sum(s1, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
 template <typename T>
@@ -237,7 +308,7 @@ int grow(icf_ctx *ctx, T **p, long long *cap, long long n) {
 
 void icf_free_solver(icf_ctx *ctx) {
   icf_solver &S = ctx->solver;
-  void *ptrs[] = {S.lrows, S.lcols, S.lslot, S.x, S.r, S.z, S.p, S.q, S.dinv, S.part, S.sc};
+  void *ptrs[] = {S.lrows, S.lcols, S.lslot, S.x, S.r, S.z, S.p, S.q, S.w, S.w2, S.dinv, S.part, S.sc};
   for (void *p : ptrs) cudaFree(p);
   if (S.h_sc) cudaFreeHost(S.h_sc);
   S = icf_solver();
@@ -276,44 +347,47 @@ int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, doubl
   const int N = ctx->N;
   const long long n3 = 3LL * N;
   if (S.gen != ctx->struct_gen) ICF_TRY_RC(build_lower(ctx));
+  // vectors: x, r1 (r), r2 (z), y (p), v (q), w, w2
   ICF_TRY_RC(grow(ctx, &S.x, &S.x_cap, n3));
   ICF_TRY_RC(grow(ctx, &S.r, &S.r_cap, n3));
   ICF_TRY_RC(grow(ctx, &S.z, &S.z_cap, n3));
   ICF_TRY_RC(grow(ctx, &S.p, &S.p_cap, n3));
   ICF_TRY_RC(grow(ctx, &S.q, &S.q_cap, n3));
+  ICF_TRY_RC(grow(ctx, &S.w, &S.w_cap, n3));
+  ICF_TRY_RC(grow(ctx, &S.w2, &S.w2_cap, n3));
   ICF_TRY_RC(grow(ctx, &S.dinv, &S.d_cap, 9LL * N));
   if (!S.part) ICF_CUDA(ctx, cudaMalloc(&S.part, sizeof(double) * 2 * RED_BLOCKS));
-  if (!S.sc) ICF_CUDA(ctx, cudaMalloc(&S.sc, sizeof(double) * 8 + sizeof(int)));
-  if (!S.h_sc) ICF_CUDA(ctx, cudaMallocHost(&S.h_sc, sizeof(double) * 8));
-  int *bad = reinterpret_cast<int *>(S.sc + 8);
+  if (!S.sc) ICF_CUDA(ctx, cudaMalloc(&S.sc, sizeof(double) * NSC + sizeof(int)));
+  if (!S.h_sc) ICF_CUDA(ctx, cudaMallocHost(&S.h_sc, sizeof(double) * NSC));
+  double *x = S.x, *r1 = S.r, *r2 = S.z, *y = S.p, *v = S.q;
+  int *bad = reinterpret_cast<int *>(S.sc + NSC);
   ICF_CUDA(ctx, cudaMemsetAsync(bad, 0, sizeof(int), s));
   k_dinv<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_rows, ctx->d_vals, S.dinv, bad);
-  k_start<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_rhs, S.dinv, S.x, S.r, S.z, S.p);
-  k_dot2<<<RED_BLOCKS, 256, 0, s>>>((int)n3, S.r, S.z, S.r, S.r, S.part);
-  k_beta<<<1, 32, 0, s>>>(S.part, S.sc, 1);
+  k_mr_start<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_rhs, S.dinv, x, r1, r2, y, S.w, S.w2);
+  k_dot<<<RED_BLOCKS, 256, 0, s>>>((int)n3, r1, y, S.part);
+  k_mr_init<<<1, 32, 0, s>>>(S.part, S.sc);
   ICF_CUDA(ctx, cudaGetLastError());
   int it = 0;
   double rel = 0;
   const int check_every = 4;
-  bool done = false;
-  while (!done) {
-    ICF_CUDA(ctx, cudaMemcpyAsync(S.h_sc, S.sc, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));
+  while (true) {
+    ICF_CUDA(ctx, cudaMemcpyAsync(S.h_sc, S.sc, sizeof(double) * NSC, cudaMemcpyDeviceToHost, s));
     ICF_CUDA(ctx, cudaStreamSynchronize(s));
-    const double rr = S.h_sc[3], bb = S.h_sc[4];
-    rel = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+    const double phibar = S.h_sc[8], beta1 = S.h_sc[9];
+    if (S.h_sc[13] != 0)
+      return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: the block-Jacobi preconditioner is not positive definite");
+    rel = beta1 > 0 ? phibar / beta1 : 0.0;
     if (!std::isfinite(rel)) return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: non-finite residual");
-    if (S.h_sc[5] != 0) return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: CG breakdown (matrix not positive definite)");
-    if (rel <= rel_tol || bb == 0) break;
-    if (it >= max_iter) break;
+    if (rel <= rel_tol || beta1 == 0 || it >= max_iter) break;
     for (int k = 0; k < check_every && it < max_iter; k++, it++) {
+      k_mr_v<<<icf_blocks(n3, 256), 256, 0, s>>>((int)n3, S.sc, y, v);
       k_spmv<<<icf_blocks(4LL * N, 256), 256, 0, s>>>(N, ctx->d_rows, ctx->d_cols, S.lrows, S.lcols, S.lslot,
-                                                      ctx->d_vals, S.p, S.q);
-      k_dot2<<<RED_BLOCKS, 256, 0, s>>>((int)n3, S.p, S.q, nullptr, nullptr, S.part);
-      k_alpha<<<1, 32, 0, s>>>(S.part, S.sc);
-      k_update<<<icf_blocks(N, 256), 256, 0, s>>>(N, S.sc, S.p, S.q, S.dinv, S.x, S.r, S.z);
-      k_dot2<<<RED_BLOCKS, 256, 0, s>>>((int)n3, S.r, S.z, S.r, S.r, S.part);
-      k_beta<<<1, 32, 0, s>>>(S.part, S.sc, 0);
-      k_newp<<<icf_blocks(n3, 256), 256, 0, s>>>((int)n3, S.sc, S.z, S.p);
+                                                      ctx->d_vals, v, y);
+      k_mr_a<<<RED_BLOCKS, 256, 0, s>>>((int)n3, it == 0 ? 1 : 0, S.sc, r1, v, y, S.part);
+      k_mr_alfa<<<1, 32, 0, s>>>(S.part, S.sc);
+      k_mr_b<<<RED_BLOCKS, 256, 0, s>>>(N, S.sc, S.dinv, r1, r2, y, S.part);
+      k_mr_rot<<<1, 32, 0, s>>>(S.part, S.sc);
+      k_mr_x<<<icf_blocks(n3, 256), 256, 0, s>>>((int)n3, S.sc, v, S.w, S.w2, x);
     }
     ICF_CUDA(ctx, cudaGetLastError());
   }

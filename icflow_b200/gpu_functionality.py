@@ -263,7 +263,7 @@ class GPU_Functionality:
         return nrm.value
 
     def Solve(self, rel_tol: float = 1e-12, max_iter: int = 20000, want_dx: bool = False):
-        """Device CG solve of the last assembled system (replaces
+        """Device MINRES solve of the last assembled system (replaces
         LinearSystem.Solve / PARDISO).  Returns (iterations, relative residual,
         dx or None)."""
         it, rr = C.c_int(), C.c_double()

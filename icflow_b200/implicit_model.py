@@ -10,7 +10,7 @@ Per step (ImplicitModel3.Step, :369-435):
                               warm start (warm_start.LearnedWarmStart);
   Newton loop                 InferTentativeValues (device) -> contact pairs
                               and narrow phase -> CreateStructure -> assembly
-                              -> linear solve (device CG in place of PARDISO)
+                              -> linear solve (device MINRES for PARDISO)
                               -> _checkDivergence (:214-245) -> _XtoDU, until
                               minIterations are done and the increment norm
                               converged, diverged or maxIterations ran out;
@@ -137,6 +137,37 @@ class ImplicitModel3:
         rel = float(np.sqrt(norm / st["E0"]))
         st["rel"] = rel
         return rel <= p.ConvergenceEpsilon, rel > 1.01
+
+    def guess_residuals(self, guesses) -> list[float]:
+        """Residual norm of the first Newton iterate for each initial guess (du
+        of the active nodes, all nodes' shape), relative to the residual at
+        zero increment, at the start of the next step; the state is left as
+        it was (used to calibrate initial guesses)."""
+        gf, p, coll = self.gf, self.prms, self.coll
+        h = p.InitialTimeStep
+        u, v, a, _ = gf.GetNodeState()
+        pres = coll.anchored
+        base = np.zeros_like(u)
+        base[pres] = prescribed_displacement(coll, self.t + h)[pres] - u[pres]
+
+        def resid(du):
+            gf.SetDU(du)
+            gf.InferTentativeValues(h)
+            if self.contact:
+                uu, _, _, duc = gf.GetNodeState()
+                gf.NarrowPhaseCollisionDetection(M.candidate_pairs(coll, coll.x0 + uu + duc))
+            gf.CreateStructure(copy_back=False)
+            gf.AssembleElemsAndCZs(h)
+            return gf.ResidualNorm()
+
+        r0 = resid(base)
+        out = []
+        for g in guesses:
+            du = base.copy()
+            du[self.active] = g[self.active]
+            out.append(resid(du) / r0 if r0 > 0 else 0.0)
+        gf.SetDU(np.zeros_like(u))
+        return out
 
     def Step(self, warm_start=None) -> StepStats:
         t0 = time.perf_counter()

@@ -371,6 +371,33 @@ def polycrystal(n: int = 32, grains: int = 128, edge: float = 1e-3, seed: int = 
     return Collection(meshes).prepare()
 
 
+def batched_specimens(n_specimens: int = 64, seed: int = 0, tets=(5000, 60000), grains=(8, 64),
+                      edge: float = 1e-3, spacing: float = 2.0, only: list | None = None):
+    """Independent polycrystal cubes of uneven size: specimen i has about
+    U[tets] tetrahedra (a cube of n^3 hexahedra, n = round((t / 6)^(1/3))) and
+    U[grains] Voronoi grains with CZs on every grain boundary, placed
+    `spacing` edges apart along x so that they never touch.  `only` keeps a
+    subset of the specimen indices (the draw for every index is the same
+    whether or not it is kept).  Returns the collection and, per kept
+    specimen, (index, tets, grains)."""
+    rng = np.random.default_rng(seed)
+    draws = [(int(rng.integers(tets[0], tets[1] + 1)), int(rng.integers(grains[0], grains[1] + 1)))
+             for _ in range(n_specimens)]
+    keep = range(n_specimens) if only is None else sorted(only)
+    meshes, info = [], []
+    for i in keep:
+        t, g = draws[i]
+        n = max(2, int(round((t / 6.0) ** (1.0 / 3.0))))
+        m = box_mesh((n, n, n), (edge, edge, edge), (i * spacing * edge, 0.0, 0.0), name=f"specimen{i}")
+        lo = (i * spacing * edge, 0.0, 0.0)
+        hi = (i * spacing * edge + edge, edge, edge)
+        gr = voronoi_grains(m.x0, m.elems, g, seed * 1000 + i, lo=lo, hi=hi)
+        m = insert_czs(m, gr)
+        meshes.append(m)
+        info.append((i, 6 * n ** 3, g))
+    return Collection(meshes).prepare(), info
+
+
 def lognormal_strengths(n_cz: int, mean: float = 1e6, cv: float = 0.2, seed: int = 0,
                         granule_pairs: np.ndarray | None = None) -> np.ndarray:
     """Per-CZ strength, lognormal with the given mean and coefficient of

@@ -3,15 +3,24 @@
 icFlow starts every Newton loop from du = v h (ImplicitModel3.cs:149-156).
 LearnedWarmStart replaces that guess for the active nodes with
 
-    du = v h + out_scale * net(x),   x = (u, v, a, du_{n-1}, du_{n-2})
+    du = v h + (du_{n-1} - du_{n-2}) + gain * out_scale * net(x),
+    x = (u, v, a, du_{n-1}, du_{n-2})
 
 where net is the per-node MLP of the library (icf_mlp: 15 -> 64 -> 64 -> 3,
 GELU, BF16 weights, FP32 accumulation, trained on the GPU by the library's own
 forward and backward kernels).  Training data are the method's own
 trajectories: every accepted step contributes, per active node, the inputs
-seen at the start of the step and the correction the Newton loop found,
-du_accepted - v h.  A zero network gives back the plain guess, which stays
-the fallback (and the judge: both are run to the same residual tolerance).
+seen at the start of the step and the correction the Newton loop found
+beyond the second-order extrapolation, du_accepted - v h - (du_{n-1} -
+du_{n-2}).  (With the reference's accept, v h = du_{n-1}, so the first two
+terms extrapolate the increments linearly.)  The network is trained per node
+on displacements, but what the Newton loop pays for is the force residual of
+the guess, and per-node prediction errors that are not spatially coherent
+cost far more force than they save displacement; `gain` is therefore
+calibrated on a separate trajectory by the first-iterate residual
+(calibrate) and may come out 0, leaving the extrapolation alone.  The plain
+guess v h stays the fallback and the judge: both run to the same residual
+tolerance.
 """
 from __future__ import annotations
 
@@ -112,12 +121,13 @@ class LearnedWarmStart:
         self.ys: list[np.ndarray] = []
         self.norm = None
         self.seed = seed
+        self.gain = 1.0
 
     # ---- data -----------------------------------------------------------------
     def record(self, model, h, u, v, a, du1, du2, du_acc):
         act = model.active
         self.xs.append(features(u, v, a, du1, du2)[act])
-        self.ys.append((du_acc - v * h)[act].astype(np.float32))
+        self.ys.append((du_acc - v * h - (du1 - du2))[act].astype(np.float32))
 
     def dataset(self):
         return np.concatenate(self.xs), np.concatenate(self.ys)
@@ -136,13 +146,33 @@ class LearnedWarmStart:
         return self.net.train(x, y / out_scale, epochs=epochs, batch=min(batch, len(x)), lr=lr, seed=self.seed)
 
     # ---- the guess --------------------------------------------------------------
-    def __call__(self, model, h, u, v, a):
-        du = v * h
-        if self.norm is None:
+    def guess(self, model, h, u, v, a, gain=None):
+        g = self.gain if gain is None else gain
+        du = v * h + (model.du_prev - model.du_prev2)
+        if self.norm is None or g == 0:
             return du
         x = features(u, v, a, model.du_prev, model.du_prev2)
         corr = self.net.forward(x).astype(np.float64) * self.norm[2 * NI:]
-        return du + corr
+        return du + g * corr
+
+    def __call__(self, model, h, u, v, a):
+        return self.guess(model, h, u, v, a)
+
+    def calibrate(self, model, steps: int, gains=(0.0, 0.05, 0.2, 0.5, 1.0)) -> dict:
+        """Runs `steps` steps of `model` (plain guess) and, before each, the
+        first-iterate residual of the learned guess at each gain; keeps the
+        gain with the smallest mean log residual.  Returns that mean per gain."""
+        h = model.prms.InitialTimeStep
+        logs = {g: [] for g in gains}
+        for _ in range(steps):
+            u, v, a, _ = model.gf.GetNodeState()
+            rs = model.guess_residuals([self.guess(model, h, u, v, a, gain=g) for g in gains])
+            for g, r in zip(gains, rs):
+                logs[g].append(np.log10(max(r, 1e-300)))
+            model.Step()
+        mean = {g: float(np.mean(logs[g])) for g in gains}
+        self.gain = min(mean, key=mean.get)
+        return mean
 
     def close(self):
         self.net.close()

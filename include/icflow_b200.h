@@ -270,11 +270,12 @@ int icf_add_dx(icf_ctx *ctx, const double *dx, double *norm);
 /* The Newton linear solve on the device, replacing LinearSystem.Solve
  * (LinearSystem.cs:48-64, MKL PARDISO on the host, after the D2H of
  * :481-485).  Solves A dx = rhs for the matrix and rhs of the last assembly
- * (A symmetric, stored as its upper blocks) by conjugate gradients with a
- * 3x3 block-Jacobi preconditioner, to ||rhs - A dx|| <= rel_tol ||rhs||.
+ * (A symmetric, stored as its upper blocks, possibly indefinite as PARDISO's
+ * mtype -2 allows) by MINRES with a 3x3 block-Jacobi preconditioner, until the
+ * preconditioned residual is at most rel_tol times its initial value.
  * dx[N*3] (nullable) receives the solution, which also stays on the device
  * for icf_apply_dx.  ICF_ERR_NUMERIC if it does not converge in max_iter
- * iterations or the matrix is not positive definite. */
+ * iterations or the block-Jacobi preconditioner is not positive definite. */
 int icf_solve(icf_ctx *ctx, double rel_tol, int max_iter, double *dx, int *iters, double *relres);
 /* Sum of squares of the rhs of the last assembly (the Newton residual norm,
  * squared).  No counterpart in the reference, whose convergence test is on

@@ -64,29 +64,37 @@ def test_training_fits_a_smooth_map():
 
 
 def test_learned_warm_start_reduces_newton_iterations():
-    """Train on the method's own trajectory (tip driven at 0.2 m/s), then run a
-    new trajectory (0.25 m/s) with both guesses to a residual tolerance of
-    1e-8 of the zero-increment residual, minIterations 1."""
+    """Train on the method's own trajectory (tip driven at 0.02 m/s), calibrate
+    the network's gain on another (0.022 m/s), then run a third (0.025 m/s)
+    with the plain guess du = v h and with the learned one, both to a
+    residual tolerance of 1e-8 of the zero-increment residual, minIterations
+    1, and compare Newton iterations per step."""
     p = _prms()
     p.minIterations = 1
     p.maxIterations = 20
     ws = LearnedWarmStart(seed=0)
-    g = ImplicitModel3(fast_cantilever(0.2), p, convergence="residual", res_tol=1e-8)
+    g = ImplicitModel3(fast_cantilever(0.02), p, convergence="residual", res_tol=1e-8)
     g.recorder = ws
     for _ in range(60):
-        g.Step()
+        assert g.Step().converged
     g.close()
     loss = ws.fit(epochs=150, batch=2048, lr=2e-3)
+    cal = ImplicitModel3(fast_cantilever(0.022), p, convergence="residual", res_tol=1e-8)
+    for _ in range(3):
+        cal.Step()
+    by_gain = ws.calibrate(cal, 12)
+    cal.close()
     its = {}
     for name, warm in (("plain", None), ("learned", ws)):
-        m = ImplicitModel3(fast_cantilever(0.25), p, convergence="residual", res_tol=1e-8)
+        m = ImplicitModel3(fast_cantilever(0.025), p, convergence="residual", res_tol=1e-8)
         for _ in range(40):
             s = m.Step(warm_start=warm)
             assert s.converged
         its[name] = np.mean([s.iterations for s in m.history[2:]])
         m.close()
     red = 1 - its["learned"] / its["plain"]
-    print(f"warm start: training loss {loss:.3e}; Newton iterations/step plain {its['plain']:.2f}, "
-          f"learned {its['learned']:.2f} ({100 * red:.0f}% fewer)")
+    print(f"warm start: training loss {loss:.3e}; first-iterate log10 residual by gain "
+          f"{ {k: round(v, 2) for k, v in by_gain.items()} }, gain {ws.gain}; Newton iterations/step "
+          f"plain {its['plain']:.2f}, learned {its['learned']:.2f} ({100 * red:.0f}% fewer)")
     assert its["learned"] <= its["plain"]
     ws.close()
