@@ -731,6 +731,79 @@ __global__ void k_commit_cz(int nc, const double *__restrict__ tent,
 }  // namespace
 
 namespace {
+// Contribution layout (ICF_LAYOUT_CONTRIB): besides the compact rhs records
+// es[4e + a] = {rhs_a, 0} (node forces), every tet writes each of its upper
+// block contributions straight into the gather position tetpos[16e + 4a + b]:
+//   off-diagonal (a != b): {h_a, V}, {h_b, 0}   FP64 64 B / FP32-mixed 32 B
+//   diagonal (a == a):     {h_a, V}, {rhs_a, 0}  FP64 64 B / mixed 48 B
+//                                                 ({h_a, V} FP32, rhs FP64)
+// so the gathers read their inputs as contiguous streams.
+template <int MINB, bool MIXED>
+__global__ void __launch_bounds__(128, MINB)
+    k_tet_contrib(int ne, const int4 *__restrict__ elem, const double4 *__restrict__ x0,
+                  const double4 *__restrict__ xc, const double2 *__restrict__ va, icf_dprm P,
+                  const int *__restrict__ tetpos, double4 *__restrict__ es, char *__restrict__ soff,
+                  char *__restrict__ sdiag) {
+  __shared__ double2 sbuf[4][32][17];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long base = (long long)blockIdx.x * blockDim.x + 32 * w;
+  if (base >= ne) return;
+  const int e = (int)base + lane;
+  if (e < ne) {
+    double2 *rec = sbuf[w][lane];
+    tet_record<false>(e, elem, x0, xc, va, P, rec);
+    const int4 *tp4 = reinterpret_cast<const int4 *>(tetpos + 16 * (size_t)e);
+    int pos[16];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int4 t = __ldg(tp4 + q);
+      pos[4 * q] = t.x; pos[4 * q + 1] = t.y; pos[4 * q + 2] = t.z; pos[4 * q + 3] = t.w;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const double2 ha01 = rec[2 * a], ha2V = rec[2 * a + 1];
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const int p = pos[4 * a + b];
+        if (p < 0) continue;
+        if (a == b) {
+          const double2 r01 = rec[8 + 2 * a], r2 = rec[9 + 2 * a];
+          if (MIXED) {
+            char *d = sdiag + 48 * (size_t)p;
+            *reinterpret_cast<float4 *>(d) = make_float4((float)ha01.x, (float)ha01.y, (float)ha2V.x, (float)ha2V.y);
+            *reinterpret_cast<double2 *>(d + 16) = r01;
+            *reinterpret_cast<double2 *>(d + 32) = r2;
+          } else {
+            double4 *d = reinterpret_cast<double4 *>(sdiag) + 2 * (size_t)p;
+            d[0] = make_double4(ha01.x, ha01.y, ha2V.x, ha2V.y);
+            d[1] = make_double4(r01.x, r01.y, r2.x, 0.0);
+          }
+        } else {
+          const double2 hb01 = rec[2 * b], hb2V = rec[2 * b + 1];
+          if (MIXED) {
+            float4 *d = reinterpret_cast<float4 *>(soff) + 2 * (size_t)p;
+            d[0] = make_float4((float)ha01.x, (float)ha01.y, (float)ha2V.x, (float)ha2V.y);
+            d[1] = make_float4((float)hb01.x, (float)hb01.y, (float)hb2V.x, 0.f);
+          } else {
+            double4 *d = reinterpret_cast<double4 *>(soff) + 2 * (size_t)p;
+            d[0] = make_double4(ha01.x, ha01.y, ha2V.x, ha2V.y);
+            d[1] = make_double4(hb01.x, hb01.y, hb2V.x, 0.0);
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+  // compact rhs records, coalesced through shared memory
+  const long long nrec = (ne - base) < 32 ? (ne - base) : 32;
+  double2 *o = reinterpret_cast<double2 *>(es) + 8 * base;
+#pragma unroll 4
+  for (int k = 0; k < 8; k++) {
+    const int idx = 32 * k + lane;
+    if (idx < 8 * nrec) o[idx] = sbuf[w][idx >> 3][8 + (idx & 7)];
+  }
+}
+
 struct tet_variant {
   const char *name;
   void (*fn)(int, const int4 *, const double4 *, const double4 *, const double2 *, icf_dprm, double4 *);
@@ -738,6 +811,12 @@ struct tet_variant {
 const tet_variant TET_VARIANTS[2][3] = {
     {{"t128 minb3", k_tet_unit<3, false>}, {"t128 minb2", k_tet_unit<2, false>}, {"t128 minb4", k_tet_unit<4, false>}},
     {{"t128 minb3", k_tet_unit<3, true>}, {"t128 minb2", k_tet_unit<2, true>}, {"t128 minb4", k_tet_unit<4, true>}},
+};
+typedef void (*tet_contrib_fn)(int, const int4 *, const double4 *, const double4 *, const double2 *, icf_dprm,
+                               const int *, double4 *, char *, char *);
+const tet_contrib_fn TET_CONTRIB[2][3] = {
+    {k_tet_contrib<3, false>, k_tet_contrib<2, false>, k_tet_contrib<4, false>},
+    {k_tet_contrib<3, true>, k_tet_contrib<2, true>, k_tet_contrib<4, true>},
 };
 constexpr int N_TET = 3;
 }  // namespace
@@ -749,8 +828,13 @@ int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *
   if (variant < 0 || variant >= N_TET) variant = 0;
   const icf_dprm P = icf_make_dprm(ctx);
   const int mixed = ctx->precision == ICF_FP32_MIXED ? 1 : 0;
-  TET_VARIANTS[mixed][variant].fn<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem,
-                                                                              ctx->d_x0, xc, va, P, es);
+  if (ctx->layout == ICF_LAYOUT_CONTRIB)
+    TET_CONTRIB[mixed][variant]<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(
+        ctx->n_elem, ctx->d_elem, ctx->d_x0, xc, va, P, ctx->d_tetpos, es,
+        static_cast<char *>(ctx->d_stage_off), static_cast<char *>(ctx->d_stage_diag));
+  else
+    TET_VARIANTS[mixed][variant].fn<<<icf_blocks(ctx->n_elem, 128), 128, 0, s>>>(ctx->n_elem, ctx->d_elem,
+                                                                                ctx->d_x0, xc, va, P, es);
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
@@ -816,8 +900,23 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, ctx->d_xc, ctx->d_va, ctx->d_es, s));
   // ids, node state (x0, x_t, v, a) once, 256 B record out
   const bool mixed = ctx->precision == ICF_FP32_MIXED;
-  const long long tet_rec = mixed ? 192 : 256, tet_h = mixed ? 64 : 128, cz_rec = mixed ? 240 : 8 * ICF_CZ_STAGE;
-  if (ctx->n_elem > 0) icf_prof_mark(ctx, s, "k_tet_unit", (16 + tet_rec) * ctx->n_elem + 112LL * ctx->n_nodes);
+  const bool contrib = ctx->layout == ICF_LAYOUT_CONTRIB;
+  // per tet: the staging it writes (records, or rhs + contribution records)
+  // and the part of it the off-diagonal and diagonal gathers read back
+  const long long n_doff = ctx->n_rc_off, n_ddiag = ctx->n_rc - ctx->n_rc_off;  // tet + CZ codes
+  long long tet_out, off_in, diag_in;
+  if (contrib) {
+    const long long ro = mixed ? 32 : 64, rd = mixed ? 48 : 64;
+    tet_out = 64 * ctx->n_elem + 128 * ctx->n_elem + ro * 6 * ctx->n_elem + rd * 4 * ctx->n_elem;
+    off_in = ro * 6 * ctx->n_elem;
+    diag_in = rd * 4 * ctx->n_elem;
+  } else {
+    tet_out = (mixed ? 192 : 256) * ctx->n_elem;
+    off_in = (mixed ? 64 : 128) * ctx->n_elem + 4 * n_doff;
+    diag_in = (mixed ? 192 : 256) * ctx->n_elem + 4 * n_ddiag;
+  }
+  const long long cz_rec = mixed ? 240 : 8 * ICF_CZ_STAGE;
+  if (ctx->n_elem > 0) icf_prof_mark(ctx, s, "k_tet_unit", 16 * ctx->n_elem + tet_out + 112LL * ctx->n_nodes);
   ICF_CUDA(ctx, cudaEventRecord(e_tet, s));
 
   // aux0: CZs
@@ -844,8 +943,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   // descriptors, codes, the h records of every tet and the CZ staging once,
   // blocks out
   if (ctx->n_offd > 0)
-    icf_prof_mark(ctx, sa, "k_gather_off", 80LL * ctx->n_offd + 4LL * ctx->n_rc_off + tet_h * ctx->n_elem +
-                                               cz_rec * ctx->n_cz);
+    icf_prof_mark(ctx, sa, "k_gather_off", 80LL * ctx->n_offd + off_in + cz_rec * ctx->n_cz);
   ICF_CUDA(ctx, cudaEventRecord(e_a, sa));
   // main: diagonal blocks and rhs once the CZs are staged
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
@@ -853,8 +951,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     ICF_TRY_RC(icf_launch_gather_diag(ctx, ctx->tune_diag, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals,
                                       ctx->d_rhs, s));
   if (ctx->N > 0)
-    icf_prof_mark(ctx, s, "k_gather_diag", 104LL * ctx->N + 4LL * (ctx->n_rc - ctx->n_rc_off) +
-                                               tet_rec * ctx->n_elem + cz_rec * ctx->n_cz);
+    icf_prof_mark(ctx, s, "k_gather_diag", 104LL * ctx->N + diag_in + cz_rec * ctx->n_cz);
   // join
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
@@ -963,7 +1060,8 @@ int icf_launch_node_force(icf_ctx *ctx) {
   if (rc) return rc;
   k_node_force<<<icf_blocks(ctx->n_nodes, 128), 128, 0, ctx->stream>>>(
       ctx->n_nodes, t.off, t.inc, ctx->d_es, ctx->n_imp > 0 ? m.off : nullptr, m.inc, ctx->d_ks,
-      ctx->precision == ICF_FP32_MIXED ? 4 : 8, ctx->precision == ICF_FP32_MIXED ? 0 : 4, ctx->d_nodeF);
+      (ctx->precision == ICF_FP32_MIXED || ctx->layout == ICF_LAYOUT_CONTRIB) ? 4 : 8,
+      (ctx->precision == ICF_FP32_MIXED || ctx->layout == ICF_LAYOUT_CONTRIB) ? 0 : 4, ctx->d_nodeF);
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
@@ -1020,7 +1118,19 @@ int icf_launch_commit_cz(icf_ctx *ctx) {
 
 // ---- launches with caller-chosen buffers (used by the allocation-free entry
 // point in icf_noalloc.cu; the context's own assembly path above is separate)
+static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cudaStream_t s);
+
+// The caller-buffer path keeps the per-tet record layout (its scratch holds
+// 256 B per tet; the contribution layout's staging lives in the context).
 int icf_enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cudaStream_t s) {
+  const int saved = ctx->layout;
+  ctx->layout = ICF_LAYOUT_RECORDS;
+  const int rc = enqueue_assembly_bufs(ctx, h, B, s);
+  ctx->layout = saved;
+  return rc;
+}
+
+static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cudaStream_t s) {
   ICF_TRY_RC(icf_ensure_cz_hist(ctx, s));
   const icf_dprm P = icf_make_dprm(ctx);
   ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, 8 * sizeof(int), s));

@@ -239,6 +239,134 @@ __global__ void __launch_bounds__(256, MINB)
   }
 }
 
+// ---- contribution layout (ICF_LAYOUT_CONTRIB) --------------------------------
+// The tet kernel wrote each contribution's inputs at its list position, so
+// iteration k of lane l reads record (meta.x + 32 k + l): one contiguous
+// stream per warp, no codes and no random loads for the tet part.
+// Positions of padding codes hold zero records.
+template <bool MIXED>
+struct crec;
+template <>
+struct crec<false> {
+  typedef double4 V4;
+  static __device__ __forceinline__ void off(const char *st, long long p, V4 &A, V4 &B) {
+    const double4 *r = reinterpret_cast<const double4 *>(st) + 2 * p;
+    A = r[0];
+    B = r[1];
+  }
+  static __device__ __forceinline__ void diag(const char *st, long long p, V4 &A, double4 &R) {
+    const double4 *r = reinterpret_cast<const double4 *>(st) + 2 * p;
+    A = r[0];
+    R = r[1];
+  }
+};
+template <>
+struct crec<true> {
+  typedef float4 V4;
+  static __device__ __forceinline__ void off(const char *st, long long p, V4 &A, V4 &B) {
+    const float4 *r = reinterpret_cast<const float4 *>(st) + 2 * p;
+    A = r[0];
+    B = r[1];
+  }
+  static __device__ __forceinline__ void diag(const char *st, long long p, V4 &A, double4 &R) {
+    const char *r = st + 48 * p;
+    A = *reinterpret_cast<const float4 *>(r);
+    const double2 r01 = *reinterpret_cast<const double2 *>(r + 16);
+    const double2 r2 = *reinterpret_cast<const double2 *>(r + 32);
+    R = make_double4(r01.x, r01.y, r2.x, 0.0);
+  }
+};
+
+template <typename S, bool MIXED, int MINB, int U>
+__global__ void __launch_bounds__(256, MINB)
+    k_gather_off_c(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
+                   const uint32_t *__restrict__ codes, const char *__restrict__ stage, S st,
+                   gargs<typename S::real> g, double *__restrict__ vals) {
+  typedef typename S::real R;
+  typedef typename crec<MIXED>::V4 V4;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n_slices) return;
+  const int4 m = meta[w];
+  R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const long long p0 = (long long)m.x + lane;
+  for (int k = 0; k < m.y; k += U) {
+    V4 A[U], B[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      A[j] = B[j] = zero4<V4>();
+      if (k + j < m.y) crec<MIXED>::off(stage, p0 + 32LL * (k + j), A[j], B[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) acc_tet<R, V4>(A[j], B[j], false, g, b);
+  }
+  const uint32_t *c = codes + m.x + lane;
+  for (int k = m.y; k < m.y + m.z; k++) {
+    const uint32_t c0 = __ldg(c + 32 * k);
+    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
+  }
+  const int2 u = unit[32 * w + lane];
+  if (u.x < 0) return;
+  double *o = vals + 9 * (size_t)u.x;
+#pragma unroll
+  for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+}
+
+template <typename S, bool MIXED, int L, int MINB, int U>
+__global__ void __launch_bounds__(256, MINB)
+    k_gather_diag_c(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
+                    const uint32_t *__restrict__ codes, const char *__restrict__ stage, S st,
+                    gargs<typename S::real> g, double *__restrict__ vals, double *__restrict__ rhs) {
+  typedef typename S::real R;
+  typedef typename crec<MIXED>::V4 V4;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n_slices) return;
+  const int4 m = meta[w];
+  R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double r[3] = {0, 0, 0};
+  const long long p0 = (long long)m.x + lane;
+  for (int k = 0; k < m.y; k += U) {
+    V4 A[U];
+    double4 Rr[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      A[j] = zero4<V4>();
+      Rr[j] = make_double4(0, 0, 0, 0);
+      if (k + j < m.y) crec<MIXED>::diag(stage, p0 + 32LL * (k + j), A[j], Rr[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      acc_tet<R, V4>(A[j], A[j], true, g, b);
+      r[0] += Rr[j].x;
+      r[1] += Rr[j].y;
+      r[2] += Rr[j].z;
+    }
+  }
+  const uint32_t *c = codes + m.x + lane;
+  for (int k = m.y; k < m.y + m.z; k++) {
+    const uint32_t c0 = __ldg(c + 32 * k);
+    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, r);
+  }
+#pragma unroll
+  for (int o = 1; o < L; o <<= 1) {
+#pragma unroll
+    for (int q = 0; q < 9; q++) b[q] += __shfl_xor_sync(0xffffffffu, b[q], o);
+#pragma unroll
+    for (int q = 0; q < 3; q++) r[q] += __shfl_xor_sync(0xffffffffu, r[q], o);
+  }
+  const int sub = lane % L;
+  const int2 u = unit[(32 / L) * w + lane / L];
+  if (sub == 0 && u.x >= 0) {
+    double *o = vals + 9 * (size_t)u.x;
+#pragma unroll
+    for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+  }
+  if (sub == (L > 1 ? 1 : 0) && u.y >= 0) {
+    rhs[3 * (size_t)u.y + 0] = r[0];
+    rhs[3 * (size_t)u.y + 1] = r[1];
+    rhs[3 * (size_t)u.y + 2] = r[2];
+  }
+}
+
 // ---- variant tables ---------------------------------------------------------
 template <typename S>
 using off_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, S, gargs<typename S::real>, double *);
@@ -246,21 +374,35 @@ template <typename S>
 using diag_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, S, gargs<typename S::real>, double *,
                          double *);
 
+template <typename S>
+using offc_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, const char *, S,
+                         gargs<typename S::real>, double *);
+template <typename S>
+using diagc_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, const char *, S,
+                          gargs<typename S::real>, double *, double *);
+
 struct off_variant {
   const char *name;
   off_fn<fp64> f64;
   off_fn<fp32mixed> f32;
+  offc_fn<fp64> c64;
+  offc_fn<fp32mixed> c32;
 };
 struct diag_variant {
   const char *name;
   int lanes;
   diag_fn<fp64> f64;
   diag_fn<fp32mixed> f32;
+  diagc_fn<fp64> c64;
+  diagc_fn<fp32mixed> c32;
 };
 
-#define OFFV(MB, U) {"reg minb" #MB " u" #U, k_gather_off<fp64, MB, U>, k_gather_off<fp32mixed, MB, U>}
-#define DIAGV(L, MB, U) \
-  {"reg L" #L " minb" #MB " u" #U, L, k_gather_diag<fp64, L, MB, U>, k_gather_diag<fp32mixed, L, MB, U>}
+#define OFFV(MB, U)                                                                                   \
+  {"reg minb" #MB " u" #U, k_gather_off<fp64, MB, U>, k_gather_off<fp32mixed, MB, U>,                \
+   k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>}
+#define DIAGV(L, MB, U)                                                                               \
+  {"reg L" #L " minb" #MB " u" #U, L, k_gather_diag<fp64, L, MB, U>, k_gather_diag<fp32mixed, L, MB, U>, \
+   k_gather_diag_c<fp64, false, L, MB, U>, k_gather_diag_c<fp32mixed, true, L, MB, U>}
 const off_variant OFF_VARIANTS[] = {OFFV(4, 4), OFFV(3, 2), OFFV(2, 4), OFFV(4, 2)};
 const diag_variant DIAG_VARIANTS[] = {DIAGV(4, 4, 4), DIAGV(2, 3, 4), DIAGV(4, 2, 4), DIAGV(8, 4, 2),
                                       DIAGV(2, 4, 2)};
@@ -292,7 +434,18 @@ int icf_launch_gather_off(icf_ctx *ctx, int variant, const double4 *es, const do
   if (S.n_slices == 0) return ICF_OK;
   if (variant < 0 || variant >= N_OFF) variant = 0;
   const unsigned grid = icf_blocks(32LL * S.n_slices, 256);
-  if (ctx->precision == ICF_FP32_MIXED) {
+  const char *stage = static_cast<const char *>(ctx->d_stage_off);
+  if (ctx->layout == ICF_LAYOUT_CONTRIB && ctx->precision == ICF_FP32_MIXED) {
+    const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
+    OFF_VARIANTS[variant].c32<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, stage,
+                                                  mixed_views(ctx, es, cs), g, vals);
+  } else if (ctx->layout == ICF_LAYOUT_CONTRIB) {
+    fp64 st;
+    st.es = es;
+    st.cs = cs;
+    const gargs<double> g{sc, mc, lam, mu};
+    OFF_VARIANTS[variant].c64<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, stage, st, g, vals);
+  } else if (ctx->precision == ICF_FP32_MIXED) {
     const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
     OFF_VARIANTS[variant].f32<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, mixed_views(ctx, es, cs),
                                                   g, vals);
@@ -319,7 +472,19 @@ int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const d
     if (variant < 0) return icf_fail(ctx, ICF_ERR_STATE, "no diagonal gather for this list layout");
   }
   const unsigned grid = icf_blocks(32LL * S.n_slices, 256);
-  if (ctx->precision == ICF_FP32_MIXED) {
+  const char *stage = static_cast<const char *>(ctx->d_stage_diag);
+  if (ctx->layout == ICF_LAYOUT_CONTRIB && ctx->precision == ICF_FP32_MIXED) {
+    const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
+    DIAG_VARIANTS[variant].c32<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, stage,
+                                                   mixed_views(ctx, es, cs), g, vals, rhs);
+  } else if (ctx->layout == ICF_LAYOUT_CONTRIB) {
+    fp64 st;
+    st.es = es;
+    st.cs = cs;
+    const gargs<double> g{sc, mc, lam, mu};
+    DIAG_VARIANTS[variant].c64<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, stage, st, g, vals,
+                                                   rhs);
+  } else if (ctx->precision == ICF_FP32_MIXED) {
     const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
     DIAG_VARIANTS[variant].f32<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes,
                                                    mixed_views(ctx, es, cs), g, vals, rhs);

@@ -62,6 +62,9 @@ __host__ __device__ inline uint32_t icf_code_cz(uint32_t u, uint32_t a,
 // iterations first.  Lane sub of a unit takes its codes sub, sub + lanes, ...;
 // missing ones are ICF_CODE_PAD.  unit[u] = {output block, row or -1}.
 #define ICF_CODE_PAD 0xFFFFFFFFu
+#define ICF_LAYOUT_RECORDS 0
+#define ICF_LAYOUT_CONTRIB 1
+#define ICF_CONTRIB_BYTES 64  // bytes per contribution record
 struct icf_sell {
   int lanes = 1;
   int n_units = 0, n_slices = 0, slices_cap = 0;
@@ -220,6 +223,18 @@ struct icf_ctx {
   struct icf_prof_state *prof = nullptr;
   // launch variants chosen by the autotuner (indices into the variant tables)
   int tune_tet = 0, tune_off = 0, tune_diag = 0;
+  // staging layout of the tet contributions:
+  //   ICF_LAYOUT_RECORDS  per-tet records es[8e + ...] read at random by the
+  //                       gathers through the contribution codes;
+  //   ICF_LAYOUT_CONTRIB  per-contribution records written by the tet kernel
+  //                       straight into the gathers' sliced-ELL positions
+  //                       (d_stage_off / d_stage_diag, 64 B each, position
+  //                       map d_tetpos[16 e + 4 a + b]), read as streams.
+  int layout = 1;
+  int *d_tetpos = nullptr;
+  long long tetpos_cap = 0;
+  void *d_stage_off = nullptr, *d_stage_diag = nullptr;
+  long long stage_off_cap = 0, stage_diag_cap = 0;  // bytes
   // CZ history axes at the committed pmax/tmax (k_cz_hist), 18 doubles per CZ;
   // refilled before the next assembly whenever hist_valid is false
   double *d_czhist = nullptr;
@@ -252,6 +267,8 @@ const char *icf_tet_variant_name(int v);
 int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *va, double4 *es, cudaStream_t s);
 // rebuilds the diagonal gather lists for `lanes` lanes per row (icf_pattern.cu)
 int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes);
+// position map and zeroed contribution staging for the current lists
+int icf_build_contrib(icf_ctx *ctx);
 int icf_ensure_cz_hist(icf_ctx *ctx, cudaStream_t s);
 int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, double *relres);
 void icf_free_solver(icf_ctx *ctx);

@@ -720,6 +720,7 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
   ctx->sell_diag.lanes = icf_gather_variant_lanes(ctx->tune_diag);
   if (build_sell(ctx, ctx->d_gdesc_off, ctx->n_offd, 12, false, &ctx->sell_off, s)) return ICF_ERR_CUDA;
   if (build_sell(ctx, ctx->d_gdesc_diag, N, 10, true, &ctx->sell_diag, s)) return ICF_ERR_CUDA;
+  if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
   if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
   if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
   k_rows<<<icf_blocks((long long)N + 1, 256), 256, 0, s>>>(N, nnz, ctx->d_mkeys, ctx->d_rows);
@@ -830,6 +831,49 @@ int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes) {
   ctx->sell_diag.lanes = lanes;
   const int wl = lanes >= 4 ? 10 : 11;
   if (build_sell(ctx, ctx->d_gdesc_diag, ctx->N, wl, true, &ctx->sell_diag, ctx->stream)) return ICF_ERR_CUDA;
+  if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ICF_OK;
+}
+
+// tetpos[16 e + 4 a + b] = position of tet code (e, a, b) in a gather list
+__global__ void k_tetpos(long long n, const uint32_t *__restrict__ codes, int *__restrict__ tetpos) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const uint32_t c = codes[p];
+  if (c == ICF_CODE_PAD || (c >> 30) != ICF_KIND_TET) return;
+  const uint32_t e = (c >> 4) & 0x3FFFFFFu, a = (c >> 2) & 3u, b = c & 3u;
+  tetpos[16 * (size_t)e + 4 * a + b] = (int)p;
+}
+
+int icf_build_contrib(icf_ctx *ctx) {
+  cudaStream_t s = ctx->stream;
+  const long long ne = ctx->n_elem;
+  if (ne == 0) return ICF_OK;
+  if (16 * ne > ctx->tetpos_cap || !ctx->d_tetpos) {
+    cudaFree(ctx->d_tetpos);
+    ctx->d_tetpos = nullptr;
+    ICF_CUDA(ctx, cudaMalloc(&ctx->d_tetpos, sizeof(int) * 16 * (size_t)ne));
+    ctx->tetpos_cap = 16 * ne;
+  }
+  ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_tetpos, 0xff, sizeof(int) * 16 * (size_t)ne, s));
+  const icf_sell *L[2] = {&ctx->sell_off, &ctx->sell_diag};
+  void **stage[2] = {&ctx->d_stage_off, &ctx->d_stage_diag};
+  long long *cap[2] = {&ctx->stage_off_cap, &ctx->stage_diag_cap};
+  for (int k = 0; k < 2; k++) {
+    const long long n = L[k]->n_codes;
+    const long long bytes = (n > 0 ? n : 1) * (long long)ICF_CONTRIB_BYTES;
+    if (bytes > *cap[k] || !*stage[k]) {
+      cudaFree(*stage[k]);
+      *stage[k] = nullptr;
+      const long long c = bytes + bytes / 4;
+      ICF_CUDA(ctx, cudaMalloc(stage[k], (size_t)c));
+      *cap[k] = c;
+    }
+    // positions no tet writes (padding, CZ iterations) must read as zero
+    ICF_CUDA(ctx, cudaMemsetAsync(*stage[k], 0, (size_t)bytes, s));
+    if (n > 0) k_tetpos<<<icf_blocks(n, 256), 256, 0, s>>>(n, L[k]->codes, ctx->d_tetpos);
+  }
+  ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }

@@ -55,9 +55,11 @@ static int time_launches(icf_ctx *ctx, timer &t, int reps, F launch, double *ms)
 }
 
 int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant) {
-  const int n = kind == 0 ? icf_tet_variants() : (kind == 1 ? icf_gather_variants(0) : icf_gather_variants(1));
-  if (kind < 0 || kind > 2 || variant < 0 || variant >= n)
-    return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..2 and a variant index of that kind");
+  const int n = kind == 0 ? icf_tet_variants()
+                          : (kind == 1 ? icf_gather_variants(0) : (kind == 2 ? icf_gather_variants(1) : 2));
+  if (kind < 0 || kind > 3 || variant < 0 || variant >= n)
+    return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..3 and a variant index of that kind");
+  if (kind == 3) ctx->layout = variant;
   if (kind == 0) ctx->tune_tet = variant;
   if (kind == 1) ctx->tune_off = variant;
   if (kind == 2) {
@@ -82,6 +84,25 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
   const double sc = 1.0 + ctx->prm.dampingStiffness * ng / (h * nb);
   const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
 
+  // staging layout: whole assemblies (graph launches) with each layout
+  {
+    const char *names[2] = {"per-tet records", "per-contribution stream"};
+    double best = 1e30;
+    int bl = ctx->layout;
+    for (int l = 0; l < 2; l++) {
+      ctx->layout = l;
+      ctx->version++;
+      double ms = 0;
+      ICF_TRY_RC(time_launches(ctx, t, reps, [&] { return icf_launch_assembly(ctx, h); }, &ms));
+      report(out, "layout", names[l], ms);
+      if (ms < best) best = ms, bl = l;
+    }
+    ctx->layout = bl;
+    ctx->version++;
+    mark_chosen(out, "layout", names[bl]);
+    ICF_TRY_RC(icf_launch_assembly(ctx, h));
+    ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   // tets
   if (ctx->n_elem > 0) {
     double best = 1e30;
@@ -120,6 +141,8 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
       for (int v = 0; v < icf_gather_variants(1); v++) any |= icf_gather_variant_lanes(v) == lanes_list[li];
       if (!any) continue;
       ICF_TRY_RC(icf_rebuild_sell_diag(ctx, lanes_list[li]));
+      // new list positions: the contribution staging is refilled by the tets
+      ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, ctx->d_xc, ctx->d_va, ctx->d_es, ctx->stream));
       for (int v = 0; v < icf_gather_variants(1); v++) {
         if (icf_gather_variant_lanes(v) != lanes_list[li]) continue;
         double ms = 0;

@@ -238,7 +238,7 @@ def test_every_launch_variant_and_autotune(O):
     compare(ref, o)
     lib = _lib.load()
     counts = {}
-    for kind in range(3):
+    for kind in (3, 0, 1, 2):
         v = 0
         while lib.icf_set_variant(gf.ctx, kind, v) == 0:
             gf.AssembleElemsAndCZs(H)
@@ -249,9 +249,20 @@ def test_every_launch_variant_and_autotune(O):
         counts[kind] = v
         _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, 0))
     assert all(n >= 2 for n in counts.values()), counts
+    # the other layout with every gather variant
+    _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 3, 0))
+    for kind in (1, 2):
+        for v in range(counts[kind]):
+            _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, v))
+            gf.AssembleElemsAndCZs(H)
+            vals, rhs = gf.TransferLinearSystemToHost()
+            assert rowwise_rel(o["rows"], o["vals"], vals.reshape(-1, 3, 3)) <= FP64_TOL, ("records", kind, v)
+            assert vec_rel(o["rhs"], rhs) <= FP64_TOL
+        _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, 0))
+    _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 3, 1))
     rep = gf.Autotune(H, reps=3)
     kinds = {r["kernel"] for r in rep}
-    assert kinds == {"k_tet_unit", "k_gather_off", "k_gather_diag"}
+    assert kinds == {"layout", "k_tet_unit", "k_gather_off", "k_gather_diag"}
     assert len(rep) == sum(counts.values())
     for k in kinds:
         assert sum(r["chosen"] for r in rep if r["kernel"] == k) == 1
