@@ -9,10 +9,10 @@
 //                 the CZ staging, tentative damage state and flags
 //                 (cz_kernels.h:210-434)
 //   k_imp_*       impacts (icf_contact.cu, icf_contact_deriv.cu)
-//   k_gather_*    one thread per BCSR block (diagonal blocks by row, then the
-//                 off-diagonal ones): sums the contributions listed for the
-//                 block in the pattern's slot-sorted code list and writes it
-//                 once (and the rhs row of a diagonal block)
+//   k_gather_*    (icf_gather.cu) the lanes that own a BCSR block sum the
+//                 contributions listed for it in the pattern's sliced-ELL
+//                 lists and write it once (and the rhs row of a diagonal
+//                 block, with the NaN/Inf check of the row)
 //   k_imp_add     adds impact contributions to the blocks they touch
 // Each block is summed in a fixed order and written once, so the result is
 // bit-reproducible; the reference's CAS-loop atomics (atomic_add.h:1-13) have
@@ -307,8 +307,8 @@ constexpr int CZ_PER_BLOCK = 32;
 // FP32.  The staging then holds rt compactly, cs[12c + 0..8] (FP64), followed
 // by the FP32 blocks cs32[36c + 0..35] with cs32 = (float *)(cs + 12 nc):
 // 240 B per CZ in the same buffer.
-template <bool MIXED>
-__global__ void __launch_bounds__(3 * CZ_PER_BLOCK)
+template <bool MIXED, int MINB>
+__global__ void __launch_bounds__(3 * CZ_PER_BLOCK, MINB)
     k_cz_gp(int nc, const int *__restrict__ cz, const double4 *__restrict__ xc,
             const double *__restrict__ czs, const int *__restrict__ czfail,
             const double4 *__restrict__ czprm, const double *__restrict__ hist, icf_dprm P, icf_law_c LC,
@@ -538,7 +538,7 @@ __global__ void k_imp_add(int n_slots, const int *__restrict__ slot,
                           const uint32_t *__restrict__ code,
                           const int *__restrict__ cols,
                           const double *__restrict__ ks,
-                          double *__restrict__ vals, double *__restrict__ rhs) {
+                          double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_slots) return;
   const int s = slot[g];
@@ -556,21 +556,21 @@ __global__ void k_imp_add(int n_slots, const int *__restrict__ slot,
     }
   }
   double *o = vals + 9 * (size_t)s;
-  for (int k = 0; k < 9; k++) o[k] += b[k];
+  bool bad = false;
+  for (int k = 0; k < 9; k++) {
+    o[k] += b[k];
+    bad |= !isfinite(b[k]);
+  }
   if (diag) {
     const int row = cols[s];
-    for (int k = 0; k < 3; k++) rhs[3 * (size_t)row + k] += r[k];
+    for (int k = 0; k < 3; k++) {
+      rhs[3 * (size_t)row + k] += r[k];
+      bad |= !isfinite(r[k]);
+    }
   }
+  if (bad) atomicOr(nonfinite, 1);
 }
 
-// NaN/Inf scan of the rhs (cheap; the matrix inherits non-finite values from
-// the same units).
-__global__ void k_finite(int n, const double *__restrict__ x, int *flag) {
-  int bad = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    if (!isfinite(x[i])) bad = 1;
-  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
-}
 
 // Node forces (the F field of the node array, GPU_Functionality.cs:519-527):
 // per node the sum of the rhs of every tet vertex on it plus impact forces.
@@ -821,7 +821,37 @@ const tet_contrib_fn TET_CONTRIB[2][3] = {
 constexpr int N_TET = 3;
 }  // namespace
 
+typedef void (*cz_fn)(int, const int *, const double4 *, const double *, const int *, const double4 *,
+                      const double *, icf_dprm, icf_law_c, double *, double *, int *, double *, int *);
+struct cz_variant {
+  const char *name;
+  cz_fn f64, f32;
+};
+const cz_variant CZ_VARIANTS[] = {
+    {"96 thr minb1", k_cz_gp<false, 1>, k_cz_gp<true, 1>},
+    {"96 thr minb6", k_cz_gp<false, 6>, k_cz_gp<true, 6>},
+    {"96 thr minb8", k_cz_gp<false, 8>, k_cz_gp<true, 8>},
+};
+constexpr int N_CZV = sizeof(CZ_VARIANTS) / sizeof(CZ_VARIANTS[0]);
+
 int icf_tet_variants() { return N_TET; }
+int icf_cz_variants() { return N_CZV; }
+const char *icf_cz_variant_name(int v) { return CZ_VARIANTS[v].name; }
+
+static icf_law_c make_law_c(const icf_ctx *ctx, const icf_dprm &P);
+
+int icf_launch_cz(icf_ctx *ctx, int variant, const double4 *xc, double *cs, cudaStream_t s) {
+  if (ctx->n_cz <= 0) return ICF_OK;
+  if (variant < 0 || variant >= N_CZV) variant = 0;
+  const icf_dprm P = icf_make_dprm(ctx);
+  const icf_law_c LC = make_law_c(ctx, P);
+  const cz_fn f = ctx->precision == ICF_FP32_MIXED ? CZ_VARIANTS[variant].f32 : CZ_VARIANTS[variant].f64;
+  f<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, s>>>(
+      ctx->n_cz, ctx->d_cz, xc, ctx->d_czs, ctx->d_czfail, ctx->per_cz_prm ? ctx->d_czprm : nullptr, ctx->d_czhist,
+      P, LC, cs, ctx->d_cztent, ctx->d_czflags, ctx->d_czavg, ctx->d_counts);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
 const char *icf_tet_variant_name(int v) { return TET_VARIANTS[0][v].name; }
 int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *va, double4 *es, cudaStream_t s) {
   if (ctx->n_elem <= 0) return ICF_OK;
@@ -921,11 +951,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
 
   // aux0: CZs
   if (ctx->n_cz > 0) {
-    const icf_law_c LC = make_law_c(ctx, P);
-    (ctx->precision == ICF_FP32_MIXED ? k_cz_gp<true> : k_cz_gp<false>)<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, sa>>>(
-        ctx->n_cz, ctx->d_cz, ctx->d_xc, ctx->d_czs, ctx->d_czfail,
-        ctx->per_cz_prm ? ctx->d_czprm : nullptr, ctx->d_czhist, P, LC, ctx->d_cs, ctx->d_cztent, ctx->d_czflags,
-        ctx->d_czavg, ctx->d_counts);
+    ICF_TRY_RC(icf_launch_cz(ctx, ctx->tune_cz, ctx->d_xc, ctx->d_cs, sa));
     // ids, six node positions, state in, per-CZ strengths, staging, tentative
     // state, flags and averages out
     icf_prof_mark(ctx, sa, "k_cz_gp", (24LL + 192 + 52 + (ctx->per_cz_prm ? 32 : 0) + cz_rec + 84) * ctx->n_cz);
@@ -958,13 +984,10 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   if (ctx->n_crs > 0)
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off,
                                                         ctx->d_cr, ctx->d_cols, ctx->d_ks,
-                                                        ctx->d_vals, ctx->d_rhs);
+                                                        ctx->d_vals, ctx->d_rhs, ctx->d_counts + 4);
   if (ctx->n_crs > 0)
     icf_prof_mark(ctx, s, "k_imp_add", 8LL * ICF_IMP_STAGE * ctx->n_imp + 172LL * ctx->n_crs + 4LL * 16 * ctx->n_imp);
-  if (ctx->N > 0)
-    k_finite<<<icf_blocks(3LL * ctx->N, 256) < 1184 ? icf_blocks(3LL * ctx->N, 256) : 1184, 256, 0,
-               s>>>(3 * ctx->N, ctx->d_rhs, ctx->d_counts + 4);
-  if (ctx->N > 0) icf_prof_mark(ctx, s, "k_finite", 24LL * ctx->N);
+
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int),
                                 cudaMemcpyDeviceToHost, s));
@@ -1140,10 +1163,7 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
   if (ctx->n_elem > 0)
     ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, B.xc, B.va, B.es, s));
   if (ctx->n_cz > 0) {
-    const icf_law_c LC = make_law_c(ctx, P);
-    (ctx->precision == ICF_FP32_MIXED ? k_cz_gp<true> : k_cz_gp<false>)<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, s>>>(
-        ctx->n_cz, ctx->d_cz, B.xc, ctx->d_czs, ctx->d_czfail, ctx->per_cz_prm ? ctx->d_czprm : nullptr,
-        ctx->d_czhist, P, LC, B.cs, ctx->d_cztent, ctx->d_czflags, ctx->d_czavg, ctx->d_counts);
+    ICF_TRY_RC(icf_launch_cz(ctx, ctx->tune_cz, B.xc, B.cs, s));
   }
   if (ctx->n_imp > 0) {
     const int rc = icf_launch_imp_unit_bufs(ctx, B.xc, B.ci, B.cd, B.ks, s);
@@ -1160,10 +1180,8 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
     ICF_TRY_RC(icf_launch_gather_diag(ctx, ctx->tune_diag, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs, s));
   if (ctx->n_crs > 0)
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
-                                                        ctx->d_cols, B.ks, B.vals, B.rhs);
-  if (ctx->N > 0)
-    k_finite<<<icf_blocks(3LL * ctx->N, 256) < 1184 ? icf_blocks(3LL * ctx->N, 256) : 1184, 256, 0, s>>>(
-        3 * ctx->N, B.rhs, ctx->d_counts + 4);
+                                                        ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4);
+
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
   return ICF_OK;

@@ -180,7 +180,7 @@ template <typename S, int L, int MINB, int U>
 __global__ void __launch_bounds__(256, MINB)
     k_gather_diag(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
                   const uint32_t *__restrict__ codes, S st, gargs<typename S::real> g,
-                  double *__restrict__ vals, double *__restrict__ rhs) {
+                  double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite) {
   typedef typename S::real R;
   typedef typename S::rec V4;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -237,6 +237,13 @@ __global__ void __launch_bounds__(256, MINB)
     rhs[3 * (size_t)u.y + 1] = r[1];
     rhs[3 * (size_t)u.y + 2] = r[2];
   }
+  // NaN/Inf check of the row (its rhs and diagonal block), one vote per warp
+  bool bad = false;
+  if (sub == 0)
+#pragma unroll
+    for (int q = 0; q < 9; q++) bad |= !isfinite((double)b[q]);
+  bad |= !(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]));
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
 }
 
 // ---- contribution layout (ICF_LAYOUT_CONTRIB) --------------------------------
@@ -315,7 +322,8 @@ template <typename S, bool MIXED, int L, int MINB, int U>
 __global__ void __launch_bounds__(256, MINB)
     k_gather_diag_c(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
                     const uint32_t *__restrict__ codes, const char *__restrict__ stage, S st,
-                    gargs<typename S::real> g, double *__restrict__ vals, double *__restrict__ rhs) {
+                    gargs<typename S::real> g, double *__restrict__ vals, double *__restrict__ rhs,
+                    int *__restrict__ nonfinite) {
   typedef typename S::real R;
   typedef typename crec<MIXED>::V4 V4;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -365,6 +373,13 @@ __global__ void __launch_bounds__(256, MINB)
     rhs[3 * (size_t)u.y + 1] = r[1];
     rhs[3 * (size_t)u.y + 2] = r[2];
   }
+  // NaN/Inf check of the row (its rhs and diagonal block), one vote per warp
+  bool bad = false;
+  if (sub == 0)
+#pragma unroll
+    for (int q = 0; q < 9; q++) bad |= !isfinite((double)b[q]);
+  bad |= !(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]));
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
 }
 
 // ---- variant tables ---------------------------------------------------------
@@ -372,14 +387,14 @@ template <typename S>
 using off_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, S, gargs<typename S::real>, double *);
 template <typename S>
 using diag_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, S, gargs<typename S::real>, double *,
-                         double *);
+                         double *, int *);
 
 template <typename S>
 using offc_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, const char *, S,
                          gargs<typename S::real>, double *);
 template <typename S>
 using diagc_fn = void (*)(int, const int4 *, const int2 *, const uint32_t *, const char *, S,
-                          gargs<typename S::real>, double *, double *);
+                          gargs<typename S::real>, double *, double *, int *);
 
 struct off_variant {
   const char *name;
@@ -476,24 +491,25 @@ int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const d
   if (ctx->layout == ICF_LAYOUT_CONTRIB && ctx->precision == ICF_FP32_MIXED) {
     const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
     DIAG_VARIANTS[variant].c32<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, stage,
-                                                   mixed_views(ctx, es, cs), g, vals, rhs);
+                                                   mixed_views(ctx, es, cs), g, vals, rhs, ctx->d_counts + 4);
   } else if (ctx->layout == ICF_LAYOUT_CONTRIB) {
     fp64 st;
     st.es = es;
     st.cs = cs;
     const gargs<double> g{sc, mc, lam, mu};
     DIAG_VARIANTS[variant].c64<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, stage, st, g, vals,
-                                                   rhs);
+                                                   rhs, ctx->d_counts + 4);
   } else if (ctx->precision == ICF_FP32_MIXED) {
     const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
     DIAG_VARIANTS[variant].f32<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes,
-                                                   mixed_views(ctx, es, cs), g, vals, rhs);
+                                                   mixed_views(ctx, es, cs), g, vals, rhs, ctx->d_counts + 4);
   } else {
     fp64 st;
     st.es = es;
     st.cs = cs;
     const gargs<double> g{sc, mc, lam, mu};
-    DIAG_VARIANTS[variant].f64<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, st, g, vals, rhs);
+    DIAG_VARIANTS[variant].f64<<<grid, 256, 0, s>>>(S.n_slices, S.meta, S.unit, S.codes, st, g, vals, rhs,
+                                                   ctx->d_counts + 4);
   }
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;

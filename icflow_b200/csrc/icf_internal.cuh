@@ -222,7 +222,7 @@ struct icf_ctx {
   // on the main stream only and each kernel is followed by an event
   struct icf_prof_state *prof = nullptr;
   // launch variants chosen by the autotuner (indices into the variant tables)
-  int tune_tet = 0, tune_off = 0, tune_diag = 0;
+  int tune_tet = 0, tune_off = 0, tune_diag = 0, tune_cz = 0;
   // staging layout of the tet contributions:
   //   ICF_LAYOUT_RECORDS  per-tet records es[8e + ...] read at random by the
   //                       gathers through the contribution codes;
@@ -265,6 +265,9 @@ int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const d
 int icf_tet_variants();
 const char *icf_tet_variant_name(int v);
 int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *va, double4 *es, cudaStream_t s);
+int icf_cz_variants();
+const char *icf_cz_variant_name(int v);
+int icf_launch_cz(icf_ctx *ctx, int variant, const double4 *xc, double *cs, cudaStream_t s);
 // rebuilds the diagonal gather lists for `lanes` lanes per row (icf_pattern.cu)
 int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes);
 // position map and zeroed contribution staging for the current lists

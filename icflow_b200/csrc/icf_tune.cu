@@ -1,13 +1,14 @@
 // icf_tune.cu -- the launch-variant autotuner.
 //
-// The tet kernel and the two gathers each come in several launch variants
-// (registers per thread, codes per iteration, loads through registers or
-// cp.async, lanes per row).  Every variant computes the same values.  Which one
-// is fastest depends on the model's size and on its code-count
-// distribution, so the tuner times each variant on the model at hand (device
-// events around `reps` back-to-back launches on the context stream, after one
-// untimed launch) and keeps the fastest.  The choice stays with the context
-// and is baked into the assembly graph at its next capture.
+// The tet kernel, the CZ kernel and the two gathers each come in several
+// launch variants (registers per thread, codes per iteration, lanes per row),
+// and the tet contributions have two staging layouts.  Every variant computes
+// the same values.  Which one is fastest depends on the model's size, on its
+// code-count distribution and on what runs beside it in the graph, so the
+// tuner times whole assemblies on the model at hand (device events around
+// `reps` back-to-back graph launches on the context stream, after one untimed
+// launch that re-captures the graph) and keeps the fastest choice of each
+// kind in turn.  The choice stays with the context.
 #include <cstring>
 #include <string>
 
@@ -56,10 +57,14 @@ static int time_launches(icf_ctx *ctx, timer &t, int reps, F launch, double *ms)
 
 int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant) {
   const int n = kind == 0 ? icf_tet_variants()
-                          : (kind == 1 ? icf_gather_variants(0) : (kind == 2 ? icf_gather_variants(1) : 2));
-  if (kind < 0 || kind > 3 || variant < 0 || variant >= n)
-    return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..3 and a variant index of that kind");
+                          : kind == 1 ? icf_gather_variants(0)
+                          : kind == 2 ? icf_gather_variants(1)
+                          : kind == 3 ? 2
+                                      : icf_cz_variants();
+  if (kind < 0 || kind > 4 || variant < 0 || variant >= n)
+    return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..4 and a variant index of that kind");
   if (kind == 3) ctx->layout = variant;
+  if (kind == 4) ctx->tune_cz = variant;
   if (kind == 0) ctx->tune_tet = variant;
   if (kind == 1) ctx->tune_off = variant;
   if (kind == 2) {
@@ -71,93 +76,54 @@ int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant) {
   return ICF_OK;
 }
 
+// Coordinate descent over the launch choices, each candidate judged by the
+// time of whole assemblies (the captured graph, re-captured per candidate).
+// Timing kernels alone misleads: the graph runs the tet, CZ and impact
+// kernels concurrently, and a variant that wins alone (say, a CZ kernel that
+// packs more blocks per SM) can slow its neighbours down more than it gains.
 int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
   if (out) memset(out, 0, sizeof(*out));
-  // one assembly so that every staging buffer holds this model's values
-  ICF_TRY_RC(icf_launch_assembly(ctx, h));
-  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   timer t;
   ICF_CUDA(ctx, cudaEventCreate(&t.a));
   ICF_CUDA(ctx, cudaEventCreate(&t.b));
-  const icf_dprm P = icf_make_dprm(ctx);
-  const double nb = ctx->prm.NewmarkBeta, ng = ctx->prm.NewmarkGamma;
-  const double sc = 1.0 + ctx->prm.dampingStiffness * ng / (h * nb);
-  const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
-
-  // staging layout: whole assemblies (graph launches) with each layout
-  {
-    const char *names[2] = {"per-tet records", "per-contribution stream"};
+  auto assembly_ms = [&](double *ms) {
+    ctx->version++;  // re-capture with the candidate's kernels
+    return time_launches(ctx, t, reps, [&] { return icf_launch_assembly(ctx, h); }, ms);
+  };
+  struct kind_desc {
+    const char *name;
+    int kind, n;
+    int *cur;
+  };
+  const kind_desc kinds[] = {
+      {"layout", 3, 2, &ctx->layout},
+      {"k_tet_unit", 0, ctx->n_elem > 0 ? icf_tet_variants() : 0, &ctx->tune_tet},
+      {"k_cz_gp", 4, ctx->n_cz > 0 ? icf_cz_variants() : 0, &ctx->tune_cz},
+      {"k_gather_off", 1, ctx->sell_off.n_slices > 0 ? icf_gather_variants(0) : 0, &ctx->tune_off},
+      {"k_gather_diag", 2, ctx->N > 0 ? icf_gather_variants(1) : 0, &ctx->tune_diag},
+  };
+  const char *layout_names[2] = {"per-tet records", "per-contribution stream"};
+  for (const kind_desc &k : kinds) {
+    if (k.n < 2) continue;
     double best = 1e30;
-    int bl = ctx->layout;
-    for (int l = 0; l < 2; l++) {
-      ctx->layout = l;
-      ctx->version++;
+    int bv = *k.cur;
+    for (int v = 0; v < k.n; v++) {
+      ICF_TRY_RC(icf_set_variant_impl(ctx, k.kind, v));
       double ms = 0;
-      ICF_TRY_RC(time_launches(ctx, t, reps, [&] { return icf_launch_assembly(ctx, h); }, &ms));
-      report(out, "layout", names[l], ms);
-      if (ms < best) best = ms, bl = l;
-    }
-    ctx->layout = bl;
-    ctx->version++;
-    mark_chosen(out, "layout", names[bl]);
-    ICF_TRY_RC(icf_launch_assembly(ctx, h));
-    ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  }
-  // tets
-  if (ctx->n_elem > 0) {
-    double best = 1e30;
-    int bv = 0;
-    for (int v = 0; v < icf_tet_variants(); v++) {
-      double ms = 0;
-      ICF_TRY_RC(time_launches(ctx, t, reps, [&] { return icf_launch_tet(ctx, v, ctx->d_xc, ctx->d_va, ctx->d_es, ctx->stream); }, &ms));
-      report(out, "k_tet_unit", icf_tet_variant_name(v), ms);
+      ICF_TRY_RC(assembly_ms(&ms));
+      const char *vn = k.kind == 3 ? layout_names[v]
+                       : k.kind == 0 ? icf_tet_variant_name(v)
+                       : k.kind == 4 ? icf_cz_variant_name(v)
+                                     : icf_gather_variant_name(k.kind == 1 ? 0 : 1, v);
+      report(out, k.name, vn, ms);
       if (ms < best) best = ms, bv = v;
     }
-    ctx->tune_tet = bv;
-    mark_chosen(out, "k_tet_unit", icf_tet_variant_name(bv));
-  }
-  // off-diagonal gather
-  if (ctx->sell_off.n_slices > 0) {
-    double best = 1e30;
-    int bv = 0;
-    for (int v = 0; v < icf_gather_variants(0); v++) {
-      double ms = 0;
-      ICF_TRY_RC(time_launches(ctx, t, reps, [&] {
-        return icf_launch_gather_off(ctx, v, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals, ctx->stream);
-      }, &ms));
-      report(out, "k_gather_off", icf_gather_variant_name(0, v), ms);
-      if (ms < best) best = ms, bv = v;
-    }
-    ctx->tune_off = bv;
-    mark_chosen(out, "k_gather_off", icf_gather_variant_name(0, bv));
-  }
-  // diagonal gather: each lanes-per-row layout needs its own lists
-  if (ctx->N > 0) {
-    double best = 1e30;
-    int bv = 0;
-    const int lanes_list[3] = {2, 4, 8};
-    for (int li = 0; li < 3; li++) {
-      bool any = false;
-      for (int v = 0; v < icf_gather_variants(1); v++) any |= icf_gather_variant_lanes(v) == lanes_list[li];
-      if (!any) continue;
-      ICF_TRY_RC(icf_rebuild_sell_diag(ctx, lanes_list[li]));
-      // new list positions: the contribution staging is refilled by the tets
-      ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, ctx->d_xc, ctx->d_va, ctx->d_es, ctx->stream));
-      for (int v = 0; v < icf_gather_variants(1); v++) {
-        if (icf_gather_variant_lanes(v) != lanes_list[li]) continue;
-        double ms = 0;
-        ICF_TRY_RC(time_launches(ctx, t, reps, [&] {
-          return icf_launch_gather_diag(ctx, v, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals,
-                                        ctx->d_rhs, ctx->stream);
-        }, &ms));
-        report(out, "k_gather_diag", icf_gather_variant_name(1, v), ms);
-        if (ms < best) best = ms, bv = v;
-      }
-    }
-    ctx->tune_diag = bv;
-    if (ctx->sell_diag.lanes != icf_gather_variant_lanes(bv))
-      ICF_TRY_RC(icf_rebuild_sell_diag(ctx, icf_gather_variant_lanes(bv)));
-    mark_chosen(out, "k_gather_diag", icf_gather_variant_name(1, bv));
+    ICF_TRY_RC(icf_set_variant_impl(ctx, k.kind, bv));
+    const char *vn = k.kind == 3 ? layout_names[bv]
+                     : k.kind == 0 ? icf_tet_variant_name(bv)
+                     : k.kind == 4 ? icf_cz_variant_name(bv)
+                                   : icf_gather_variant_name(k.kind == 1 ? 0 : 1, bv);
+    mark_chosen(out, k.name, vn);
   }
   ctx->version++;
   // leave the outputs of a complete assembly behind

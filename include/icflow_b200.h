@@ -208,7 +208,7 @@ int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out
  * events), keeps the fastest of each kind for the following assemblies and
  * reports all timings.  Needs a structure; leaves the outputs of a complete
  * assembly behind.  icf_set_variant pins one variant by index (kind 0 tet,
- * 1 off-diagonal gather, 2 diagonal gather) or the staging layout (kind 3:
+ * 1 off-diagonal gather, 2 diagonal gather, 4 CZ kernel) or the staging layout (kind 3:
  * 0 per-tet records gathered through contribution codes, 1 per-contribution
  * records written at their gather positions and read as streams, the
  * default).  The tuner also times whole assemblies with each layout first. */

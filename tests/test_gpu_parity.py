@@ -1,4 +1,6 @@
 """CUDA path vs the CPU oracle through the C ABI (needs a B200)."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -173,6 +175,35 @@ def test_error_paths():
     gf.close()
 
 
+def test_non_finite_state_is_reported():
+    """A NaN in the node state reaches the matrix: the assembly returns
+    ICF_ERR_NUMERIC (counts.nonFinite = 1) and the context stays usable."""
+    from icflow_b200 import _lib
+
+    coll = M.cantilever()
+    prms = config_prms()
+    gf = _gf(coll, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    un, vn, an = random_state(coll, 5, du=1e-6)
+    gf.TransferPCSR(pmax, tmax, failed)
+    gf.CreateStructure()
+    bad_v = vn.copy()
+    bad_v[np.nonzero(coll.alt >= 0)[0][7]] = np.nan
+    lib = _lib.load()
+    try:
+        gf.TransferNodesToGPU(un, bad_v, an)
+    except _lib.ICFError as e:  # rejected on the host: also acceptable
+        assert e.code == _lib.ICF_ERR_ARG
+    else:
+        cnt = _lib.icf_counts()
+        assert lib.icf_assemble(gf.ctx, H, C.byref(cnt)) == _lib.ICF_ERR_NUMERIC
+        assert cnt.nonFinite == 1 or b"non-finite" in lib.icf_last_error(gf.ctx)
+    gf.TransferNodesToGPU(un, vn, an)
+    cnt = gf.AssembleElemsAndCZs(H)
+    assert cnt.nonFinite == 0
+    gf.close()
+
+
 def test_graph_matches_direct_launch(O):
     """The captured fork/join graph and direct launches give identical bits,
     and a changed time step or pattern re-captures the graph."""
@@ -211,7 +242,7 @@ def test_profile_assembly_kernels(O):
     a = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
     ks = gf.ProfileAssembly(H, reps=3)
     names = [k["name"] for k in ks]
-    assert {"k_tet_unit", "k_cz_gp", "k_gather_off", "k_gather_diag", "k_finite"} <= set(names)
+    assert {"k_tet_unit", "k_cz_gp", "k_gather_off", "k_gather_diag"} <= set(names)
     if len(gf.c_itet):
         assert {"k_imp_classify", "k_imp_deriv", "k_imp_add"} <= set(names)
     assert all(k["ms"] > 0 and k["bytes"] > 0 for k in ks)
@@ -238,7 +269,7 @@ def test_every_launch_variant_and_autotune(O):
     compare(ref, o)
     lib = _lib.load()
     counts = {}
-    for kind in (3, 0, 1, 2):
+    for kind in (3, 0, 1, 2, 4):
         v = 0
         while lib.icf_set_variant(gf.ctx, kind, v) == 0:
             gf.AssembleElemsAndCZs(H)
@@ -262,7 +293,7 @@ def test_every_launch_variant_and_autotune(O):
     _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 3, 1))
     rep = gf.Autotune(H, reps=3)
     kinds = {r["kernel"] for r in rep}
-    assert kinds == {"layout", "k_tet_unit", "k_gather_off", "k_gather_diag"}
+    assert kinds == {"layout", "k_tet_unit", "k_cz_gp", "k_gather_off", "k_gather_diag"}
     assert len(rep) == sum(counts.values())
     for k in kinds:
         assert sum(r["chosen"] for r in rep if r["kernel"] == k) == 1
