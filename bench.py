@@ -313,6 +313,8 @@ def run_ours(args):
     gf.TransferPCSR(np.zeros((nc, 3)), np.zeros((nc, 3)), np.zeros(nc, np.int32))
     imps = gf.NarrowPhaseCollisionDetection(pairs)
     N, nnz = gf.CreateStructure(copy_back=False)
+    if args.layout != "auto":
+        _lib.check(gf.ctx, gf.lib.icf_set_variant(gf.ctx, 3, 0 if args.layout == "records" else 1))
     tune = [] if args.no_tune else gf.Autotune(H, reps=10)
     lib = gf.lib
     bufs = gf.DeviceBuffers()
@@ -444,6 +446,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="cfg1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch variants")
+    ap.add_argument("--layout", default="auto", choices=["auto", "records", "contrib"],
+                    help="staging layout of the tet contributions (auto: the autotuner's choice)")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="fp64, or FP32 Hessian arithmetic with FP64 rotation, law, rhs and accumulation "
                          "(default: fp64 for cfg1/cfg2, mixed for cfg3)")

@@ -174,6 +174,7 @@ int icf_create(int device, icf_ctx **out) {
   if (!ctx) return ICF_ERR_SIZE;
   ctx->device = device;
   bool ok = cudaSetDevice(device) == cudaSuccess;
+  if (ok) ok = cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device) == cudaSuccess;
   for (int i = 0; ok && i < 2; i++) ok = cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking) == cudaSuccess;
   for (int i = 0; ok && i < 5; i++) ok = cudaEventCreateWithFlags(&ctx->ev[i], cudaEventDisableTiming) == cudaSuccess;
   if (!ok ||

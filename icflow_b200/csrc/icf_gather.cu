@@ -246,6 +246,280 @@ __global__ void __launch_bounds__(256, MINB)
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
 }
 
+// ---- streaming cache hints ------------------------------------------------------
+// Same as k_gather_off, but the list codes, units and the output blocks are
+// touched once and go through L2 as evict-first (ld/st .cs), so that the
+// staging records, which several blocks read, stay in L2 longer.
+template <typename S, int MINB, int U>
+__global__ void __launch_bounds__(256, MINB)
+    k_gather_off_cs(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
+                    const uint32_t *__restrict__ codes, S st, gargs<typename S::real> g,
+                    double *__restrict__ vals) {
+  typedef typename S::real R;
+  typedef typename S::rec V4;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n_slices) return;
+  const int4 m = __ldcs(meta + w);
+  const uint32_t *c = codes + m.x + lane;
+  R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < m.y; k += U) {
+    uint32_t cc[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) cc[j] = (k + j < m.y) ? __ldcs(c + 32 * (k + j)) : ICF_CODE_PAD;
+    V4 A[U], B[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      A[j] = B[j] = zero4<V4>();
+      if (cc[j] != ICF_CODE_PAD) {
+        uint32_t e, a, bb;
+        tet_code(cc[j], e, a, bb);
+        A[j] = st.hrec(e, a);
+        B[j] = st.hrec(e, bb);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) acc_tet<R, V4>(A[j], B[j], false, g, b);
+  }
+  for (int k = m.y; k < m.y + m.z; k++) {
+    const uint32_t c0 = __ldcs(c + 32 * k);
+    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
+  }
+  const int2 u = __ldcs(unit + 32 * w + lane);
+  if (u.x < 0) return;
+  double *o = vals + 9 * (size_t)u.x;
+#pragma unroll
+  for (int q = 0; q < 9; q++) __stcs(o + q, (double)b[q]);
+}
+
+// ---- natural-order lists with coalesced block stores ---------------------------
+// The slices hold 32 consecutive off-diagonal blocks, so their outputs are
+// (nearly) contiguous in vals.  The lanes put their 9 values in shared memory
+// and the warp stores the 288 values so that consecutive lanes write
+// consecutive doubles: a few L2 write requests per warp instead of one per
+// sector.  The price is divergence: a slice runs as many iterations as its
+// longest list.
+template <typename S, int MINB, int U>
+__global__ void __launch_bounds__(256, MINB)
+    k_gather_off_nat(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
+                     const uint32_t *__restrict__ codes, S st, gargs<typename S::real> g,
+                     double *__restrict__ vals) {
+  typedef typename S::real R;
+  typedef typename S::rec V4;
+  __shared__ double sb[8][32 * 9];
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n_slices) return;
+  const int wl = threadIdx.x >> 5;
+  const int4 m = meta[w];
+  const int2 u = unit[32 * w + lane];
+  const uint32_t *c = codes + m.x + lane;
+  R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < m.y; k += U) {
+    uint32_t cc[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) cc[j] = (k + j < m.y) ? __ldg(c + 32 * (k + j)) : ICF_CODE_PAD;
+    V4 A[U], B[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      A[j] = B[j] = zero4<V4>();
+      if (cc[j] != ICF_CODE_PAD) {
+        uint32_t e, a, bb;
+        tet_code(cc[j], e, a, bb);
+        A[j] = st.hrec(e, a);
+        B[j] = st.hrec(e, bb);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) acc_tet<R, V4>(A[j], B[j], false, g, b);
+  }
+  for (int k = m.y; k < m.y + m.z; k++) {
+    const uint32_t c0 = __ldg(c + 32 * k);
+    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
+  }
+#pragma unroll
+  for (int q = 0; q < 9; q++) sb[wl][9 * lane + q] = (double)b[q];
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const int idx = 32 * k + lane;
+    const int blk = idx / 9, q = idx - 9 * blk;
+    const int slot = __shfl_sync(0xffffffffu, u.x, blk);
+    if (slot >= 0) vals[9 * (size_t)slot + q] = sb[wl][idx];
+  }
+}
+
+// ---- persistent, software-pipelined variants --------------------------------
+// A warp walks slices w, w + W, ... (W = warps in the grid).  While the
+// records of slice w are in flight it already loads the next slice's meta,
+// unit and first codes, so the dependent chain meta -> codes -> records is
+// paid about once per slice instead of three times.
+template <typename S, int MINB, int U>
+__global__ void __launch_bounds__(256, MINB)
+    k_gather_off_pipe(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
+                      const uint32_t *__restrict__ codes, S st, gargs<typename S::real> g,
+                      double *__restrict__ vals) {
+  typedef typename S::real R;
+  typedef typename S::rec V4;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= n_slices) return;
+  int4 m = meta[w];
+  int2 u = unit[32 * w + lane];
+  uint32_t cc[U];
+#pragma unroll
+  for (int j = 0; j < U; j++) cc[j] = j < m.y ? __ldg(codes + m.x + 32 * j + lane) : ICF_CODE_PAD;
+  while (true) {
+    const int wn = w + nw;
+    int4 mn = make_int4(0, 0, 0, 0);
+    int2 un = make_int2(-1, -1);
+    if (wn < n_slices) {
+      mn = meta[wn];
+      un = unit[32 * wn + lane];
+    }
+    V4 A[U], B[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      A[j] = B[j] = zero4<V4>();
+      if (cc[j] != ICF_CODE_PAD) {
+        uint32_t e, a, bb;
+        tet_code(cc[j], e, a, bb);
+        A[j] = st.hrec(e, a);
+        B[j] = st.hrec(e, bb);
+      }
+    }
+    uint32_t cn[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) cn[j] = (wn < n_slices && j < mn.y) ? __ldg(codes + mn.x + 32 * j + lane) : ICF_CODE_PAD;
+    R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < U; j++) acc_tet<R, V4>(A[j], B[j], false, g, b);
+    const uint32_t *c = codes + m.x + lane;
+    for (int k = U; k < m.y; k++) {
+      const uint32_t c0 = __ldg(c + 32 * k);
+      if (c0 != ICF_CODE_PAD) {
+        uint32_t e, a, bb;
+        tet_code(c0, e, a, bb);
+        acc_tet<R, V4>(st.hrec(e, a), st.hrec(e, bb), false, g, b);
+      }
+    }
+    for (int k = m.y; k < m.y + m.z; k++) {
+      const uint32_t c0 = __ldg(c + 32 * k);
+      if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
+    }
+    if (u.x >= 0) {
+      double *o = vals + 9 * (size_t)u.x;
+#pragma unroll
+      for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+    }
+    if (wn >= n_slices) break;
+    w = wn;
+    m = mn;
+    u = un;
+#pragma unroll
+    for (int j = 0; j < U; j++) cc[j] = cn[j];
+  }
+}
+
+template <typename S, int L, int MINB, int U>
+__global__ void __launch_bounds__(256, MINB)
+    k_gather_diag_pipe(int n_slices, const int4 *__restrict__ meta, const int2 *__restrict__ unit,
+                       const uint32_t *__restrict__ codes, S st, gargs<typename S::real> g,
+                       double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite) {
+  typedef typename S::real R;
+  typedef typename S::rec V4;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= n_slices) return;
+  int4 m = meta[w];
+  int2 u = unit[(32 / L) * w + lane / L];
+  uint32_t cc[U];
+#pragma unroll
+  for (int j = 0; j < U; j++) cc[j] = j < m.y ? __ldg(codes + m.x + 32 * j + lane) : ICF_CODE_PAD;
+  bool bad = false;
+  while (true) {
+    const int wn = w + nw;
+    int4 mn = make_int4(0, 0, 0, 0);
+    int2 un = make_int2(-1, -1);
+    if (wn < n_slices) {
+      mn = meta[wn];
+      un = unit[(32 / L) * wn + lane / L];
+    }
+    V4 A[U];
+    double4 Rr[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      A[j] = zero4<V4>();
+      Rr[j] = make_double4(0, 0, 0, 0);
+      if (cc[j] != ICF_CODE_PAD) {
+        uint32_t e, a, bb;
+        tet_code(cc[j], e, a, bb);
+        A[j] = st.hrec(e, a);
+        Rr[j] = st.rrec(e, a);
+      }
+    }
+    uint32_t cn[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) cn[j] = (wn < n_slices && j < mn.y) ? __ldg(codes + mn.x + 32 * j + lane) : ICF_CODE_PAD;
+    R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double r[3] = {0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      acc_tet<R, V4>(A[j], A[j], true, g, b);
+      r[0] += Rr[j].x;
+      r[1] += Rr[j].y;
+      r[2] += Rr[j].z;
+    }
+    const uint32_t *c = codes + m.x + lane;
+    for (int k = U; k < m.y; k++) {
+      const uint32_t c0 = __ldg(c + 32 * k);
+      if (c0 != ICF_CODE_PAD) {
+        uint32_t e, a, bb;
+        tet_code(c0, e, a, bb);
+        const V4 A1 = st.hrec(e, a);
+        const double4 R1 = st.rrec(e, a);
+        acc_tet<R, V4>(A1, A1, true, g, b);
+        r[0] += R1.x;
+        r[1] += R1.y;
+        r[2] += R1.z;
+      }
+    }
+    for (int k = m.y; k < m.y + m.z; k++) {
+      const uint32_t c0 = __ldg(c + 32 * k);
+      if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, r);
+    }
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1) {
+#pragma unroll
+      for (int q = 0; q < 9; q++) b[q] += __shfl_xor_sync(0xffffffffu, b[q], o);
+#pragma unroll
+      for (int q = 0; q < 3; q++) r[q] += __shfl_xor_sync(0xffffffffu, r[q], o);
+    }
+    const int sub = lane % L;
+    if (sub == 0 && u.x >= 0) {
+      double *o = vals + 9 * (size_t)u.x;
+#pragma unroll
+      for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+    }
+    if (sub == (L > 1 ? 1 : 0) && u.y >= 0) {
+      rhs[3 * (size_t)u.y + 0] = r[0];
+      rhs[3 * (size_t)u.y + 1] = r[1];
+      rhs[3 * (size_t)u.y + 2] = r[2];
+    }
+    if (sub == 0)
+#pragma unroll
+      for (int q = 0; q < 9; q++) bad |= !isfinite((double)b[q]);
+    bad |= !(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]));
+    if (wn >= n_slices) break;
+    w = wn;
+    m = mn;
+    u = un;
+#pragma unroll
+    for (int j = 0; j < U; j++) cc[j] = cn[j];
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
+}
+
 // ---- contribution layout (ICF_LAYOUT_CONTRIB) --------------------------------
 // The tet kernel wrote each contribution's inputs at its list position, so
 // iteration k of lane l reads record (meta.x + 32 k + l): one contiguous
@@ -402,6 +676,8 @@ struct off_variant {
   off_fn<fp32mixed> f32;
   offc_fn<fp64> c64;
   offc_fn<fp32mixed> c32;
+  int persistent_minb;  // > 0: persistent grid of n_sm * this many blocks (record layout)
+  bool natural;         // reads natural-order lists
 };
 struct diag_variant {
   const char *name;
@@ -410,19 +686,38 @@ struct diag_variant {
   diag_fn<fp32mixed> f32;
   diagc_fn<fp64> c64;
   diagc_fn<fp32mixed> c32;
+  int persistent_minb;
 };
 
 #define OFFV(MB, U)                                                                                   \
   {"reg minb" #MB " u" #U, k_gather_off<fp64, MB, U>, k_gather_off<fp32mixed, MB, U>,                \
-   k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>}
+   k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, 0, false}
+#define OFFN(MB, U)                                                                                   \
+  {"natural minb" #MB " u" #U, k_gather_off_nat<fp64, MB, U>, k_gather_off_nat<fp32mixed, MB, U>,   \
+   k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, 0, true}
+#define OFFS(MB, U)                                                                                   \
+  {"stream minb" #MB " u" #U, k_gather_off_cs<fp64, MB, U>, k_gather_off_cs<fp32mixed, MB, U>,      \
+   k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, 0, false}
+#define OFFP(MB, U)                                                                                   \
+  {"pipe minb" #MB " u" #U, k_gather_off_pipe<fp64, MB, U>, k_gather_off_pipe<fp32mixed, MB, U>,     \
+   k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, MB, false}
 #define DIAGV(L, MB, U)                                                                               \
   {"reg L" #L " minb" #MB " u" #U, L, k_gather_diag<fp64, L, MB, U>, k_gather_diag<fp32mixed, L, MB, U>, \
-   k_gather_diag_c<fp64, false, L, MB, U>, k_gather_diag_c<fp32mixed, true, L, MB, U>}
-const off_variant OFF_VARIANTS[] = {OFFV(4, 4), OFFV(3, 2), OFFV(2, 4), OFFV(4, 2)};
+   k_gather_diag_c<fp64, false, L, MB, U>, k_gather_diag_c<fp32mixed, true, L, MB, U>, 0}
+#define DIAGP(L, MB, U)                                                                               \
+  {"pipe L" #L " minb" #MB " u" #U, L, k_gather_diag_pipe<fp64, L, MB, U>,                           \
+   k_gather_diag_pipe<fp32mixed, L, MB, U>, k_gather_diag_c<fp64, false, L, MB, U>,                  \
+   k_gather_diag_c<fp32mixed, true, L, MB, U>, MB}
+const off_variant OFF_VARIANTS[] = {OFFV(4, 4), OFFV(3, 2), OFFV(2, 4), OFFV(4, 2), OFFP(4, 2), OFFP(3, 4),
+                                    OFFN(4, 2), OFFN(4, 4), OFFN(3, 2), OFFS(4, 2), OFFS(4, 4)};
 const diag_variant DIAG_VARIANTS[] = {DIAGV(4, 4, 4), DIAGV(2, 3, 4), DIAGV(4, 2, 4), DIAGV(8, 4, 2),
-                                      DIAGV(2, 4, 2)};
+                                      DIAGV(2, 4, 2), DIAGP(4, 4, 2), DIAGP(8, 4, 2)};
 #undef OFFV
+#undef OFFN
+#undef OFFS
+#undef OFFP
 #undef DIAGV
+#undef DIAGP
 constexpr int N_OFF = sizeof(OFF_VARIANTS) / sizeof(OFF_VARIANTS[0]);
 constexpr int N_DIAG = sizeof(DIAG_VARIANTS) / sizeof(DIAG_VARIANTS[0]);
 
@@ -442,13 +737,16 @@ const char *icf_gather_variant_name(int kind, int v) {
   return kind == 0 ? OFF_VARIANTS[v].name : DIAG_VARIANTS[v].name;
 }
 int icf_gather_variant_lanes(int v) { return DIAG_VARIANTS[v].lanes; }
+bool icf_gather_variant_natural(int v) { return OFF_VARIANTS[v].natural; }
 
 int icf_launch_gather_off(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc, double mc,
                           double lam, double mu, double *vals, cudaStream_t s) {
   const icf_sell &S = ctx->sell_off;
   if (S.n_slices == 0) return ICF_OK;
   if (variant < 0 || variant >= N_OFF) variant = 0;
-  const unsigned grid = icf_blocks(32LL * S.n_slices, 256);
+  unsigned grid = icf_blocks(32LL * S.n_slices, 256);
+  const int pm = OFF_VARIANTS[variant].persistent_minb;
+  if (pm > 0 && ctx->layout == ICF_LAYOUT_RECORDS && grid > (unsigned)(ctx->n_sm * pm)) grid = ctx->n_sm * pm;
   const char *stage = static_cast<const char *>(ctx->d_stage_off);
   if (ctx->layout == ICF_LAYOUT_CONTRIB && ctx->precision == ICF_FP32_MIXED) {
     const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
@@ -486,7 +784,9 @@ int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const d
       if (DIAG_VARIANTS[v].lanes == S.lanes) variant = v;
     if (variant < 0) return icf_fail(ctx, ICF_ERR_STATE, "no diagonal gather for this list layout");
   }
-  const unsigned grid = icf_blocks(32LL * S.n_slices, 256);
+  unsigned grid = icf_blocks(32LL * S.n_slices, 256);
+  const int pm = DIAG_VARIANTS[variant].persistent_minb;
+  if (pm > 0 && ctx->layout == ICF_LAYOUT_RECORDS && grid > (unsigned)(ctx->n_sm * pm)) grid = ctx->n_sm * pm;
   const char *stage = static_cast<const char *>(ctx->d_stage_diag);
   if (ctx->layout == ICF_LAYOUT_CONTRIB && ctx->precision == ICF_FP32_MIXED) {
     const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};

@@ -67,6 +67,7 @@ __host__ __device__ inline uint32_t icf_code_cz(uint32_t u, uint32_t a,
 #define ICF_CONTRIB_BYTES 64  // bytes per contribution record
 struct icf_sell {
   int lanes = 1;
+  bool natural = false;  // units in their own order (no count sort): slices of consecutive units
   int n_units = 0, n_slices = 0, slices_cap = 0;
   long long n_codes = 0, codes_cap = 0;
   int4 *meta = nullptr;
@@ -103,6 +104,7 @@ struct icf_dprm {
 
 struct icf_ctx {
   int device = 0;
+  int n_sm = 148;  // multiprocessors of the device (persistent launch grids)
   cudaStream_t stream = nullptr;
   // auxiliary streams and events of the assembly's fork/join graph
   cudaStream_t aux[2] = {nullptr, nullptr};
@@ -257,6 +259,7 @@ void icf_prof_mark(icf_ctx *ctx, cudaStream_t s, const char *name, long long byt
 int icf_gather_variants(int kind);  // kind 0 off-diagonal, 1 diagonal
 const char *icf_gather_variant_name(int kind, int v);
 int icf_gather_variant_lanes(int v);  // lanes per row of diagonal variant v
+bool icf_gather_variant_natural(int v);  // off-diagonal variant v reads natural-order lists
 int icf_launch_gather_off(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc, double mc,
                           double lam, double mu, double *vals, cudaStream_t s);
 int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc,
@@ -270,6 +273,7 @@ const char *icf_cz_variant_name(int v);
 int icf_launch_cz(icf_ctx *ctx, int variant, const double4 *xc, double *cs, cudaStream_t s);
 // rebuilds the diagonal gather lists for `lanes` lanes per row (icf_pattern.cu)
 int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes);
+int icf_rebuild_sell_off(icf_ctx *ctx, bool natural);
 // position map and zeroed contribution staging for the current lists
 int icf_build_contrib(icf_ctx *ctx);
 int icf_ensure_cz_hist(icf_ctx *ctx, cudaStream_t s);

@@ -568,13 +568,17 @@ static int build_sell(icf_ctx *ctx, const int4 *desc, int n, int wl, bool with_r
   ICF_CUDA(ctx, cudaMallocAsync(&perm, sizeof(int) * (size_t)n, s));
   ICF_CUDA(ctx, cudaMallocAsync(&cnt, sizeof(int) * (size_t)(ns + 1), s));
   ICF_CUDA(ctx, cudaMallocAsync(&off, sizeof(int) * (size_t)(ns + 1), s));
-  k_sell_key<<<icf_blocks(n, 256), 256, 0, s>>>(n, wl, S->lanes, desc, k0, i0);
-  int end_bit = 16;
-  while ((((long long)n - 1) >> wl) >> (end_bit - 16)) end_bit++;
   size_t tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, i0, perm, n, 0, end_bit, s);
-  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-  ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, i0, perm, n, 0, end_bit, s));
+  if (S->natural) {
+    k_iota<<<icf_blocks(n, 256), 256, 0, s>>>(n, perm);
+  } else {
+    k_sell_key<<<icf_blocks(n, 256), 256, 0, s>>>(n, wl, S->lanes, desc, k0, i0);
+    int end_bit = 16;
+    while ((((long long)n - 1) >> wl) >> (end_bit - 16)) end_bit++;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, i0, perm, n, 0, end_bit, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, i0, perm, n, 0, end_bit, s));
+  }
   ICF_CUDA(ctx, cudaMemsetAsync(S->unit, 0xff, sizeof(int2) * (size_t)ns * per, s));
   k_sell_count<<<icf_blocks(32LL * ns, 256), 256, 0, s>>>(n, ns, S->lanes, perm, desc, with_row ? 1 : 0,
                                                          S->meta, cnt, S->unit);
@@ -717,6 +721,7 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
     k_desc<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_offd, ctx->d_rc_off,
                                                        ctx->d_rc_mid, ctx->d_s2m, ident, ctx->d_gdesc_off);
   ctx->sell_off.lanes = 1;
+  ctx->sell_off.natural = icf_gather_variant_natural(ctx->tune_off);
   ctx->sell_diag.lanes = icf_gather_variant_lanes(ctx->tune_diag);
   if (build_sell(ctx, ctx->d_gdesc_off, ctx->n_offd, 12, false, &ctx->sell_off, s)) return ICF_ERR_CUDA;
   if (build_sell(ctx, ctx->d_gdesc_diag, N, 10, true, &ctx->sell_diag, s)) return ICF_ERR_CUDA;
@@ -831,6 +836,15 @@ int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes) {
   ctx->sell_diag.lanes = lanes;
   const int wl = lanes >= 4 ? 10 : 11;
   if (build_sell(ctx, ctx->d_gdesc_diag, ctx->N, wl, true, &ctx->sell_diag, ctx->stream)) return ICF_ERR_CUDA;
+  if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ICF_OK;
+}
+
+int icf_rebuild_sell_off(icf_ctx *ctx, bool natural) {
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  ctx->sell_off.natural = natural;
+  if (build_sell(ctx, ctx->d_gdesc_off, ctx->n_offd, 12, false, &ctx->sell_off, ctx->stream)) return ICF_ERR_CUDA;
   if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ICF_OK;

@@ -66,7 +66,11 @@ int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant) {
   if (kind == 3) ctx->layout = variant;
   if (kind == 4) ctx->tune_cz = variant;
   if (kind == 0) ctx->tune_tet = variant;
-  if (kind == 1) ctx->tune_off = variant;
+  if (kind == 1) {
+    ctx->tune_off = variant;
+    const bool nat = icf_gather_variant_natural(variant);
+    if (ctx->have_structure && nat != ctx->sell_off.natural) ICF_TRY_RC(icf_rebuild_sell_off(ctx, nat));
+  }
   if (kind == 2) {
     ctx->tune_diag = variant;
     const int lanes = icf_gather_variant_lanes(variant);
