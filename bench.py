@@ -177,6 +177,16 @@ def dist_env():
     return env()
 
 
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip() + f" ({os.cpu_count()} logical CPUs)"
+    except OSError:
+        pass
+    return f"{os.cpu_count()} logical CPUs"
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -376,6 +386,28 @@ def run_ours(args):
     # per-kernel device times: the same kernels run in the graph's order on
     # one stream with an event after each (no overlap between streams)
     kernels = gf.ProfileAssembly(H, reps=max(args.steps, 10))
+    mixed_error = None
+    if precision == "mixed":
+        # the same assembly in FP64: normwise error of the FP32-mixed result
+        gf.AssembleElemsAndCZs(H)
+        v32, r32 = gf.TransferLinearSystemToHost()
+        gf.SetPrecision(0)
+        gf.AssembleElemsAndCZs(H)
+        v64, r64 = gf.TransferLinearSystemToHost()
+        gf.SetPrecision(1)
+        rows = np.zeros(N + 1, np.int32)
+        cols = np.zeros(nnz, np.int32)
+        _lib.check(gf.ctx, lib.icf_get_structure(gf.ctx, _lib.iptr(rows), _lib.iptr(cols)))
+        b64 = v64.reshape(-1, 9)
+        b32 = v32.reshape(-1, 9)
+        rid = np.repeat(np.arange(N), np.diff(rows))
+        num = np.zeros(N)
+        den = np.zeros(N)
+        np.maximum.at(num, rid, np.abs(b32 - b64).max(axis=1))
+        np.maximum.at(den, rid, np.abs(b64).max(axis=1))
+        mixed_error = {"blocks_rowwise_max": float((num / np.where(den > 0, den, 1)).max()),
+                       "rhs_max_rel": float(np.abs(r32 - r64).max() / np.abs(r64).max()),
+                       "scope": "same inputs assembled in FP64 on the device; per block row max|diff|/max|FP64|"}
 
     from icflow_b200.shard import reduce_max, reduce_sum
 
@@ -422,12 +454,15 @@ def run_ours(args):
                     "h2d_bytes_per_step": int(3 * un.nbytes), "d2h_bytes_per_step": int(8 * (9 * nnz + 3 * N))},
             "gpu_launches": launches_per_step * args.steps,
             "autotune": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in t.items()} for t in tune],
+            "mixed_error": mixed_error,
             "clocks": clocks,
         }
         if not args.no_cpu:
             rate, threads, kind, sample = cpu_baseline(coll, state, sig, pairs, bound_s=args.cpu_seconds)
+            rate1, _, _, sample1 = cpu_baseline(coll, state, sig, pairs, bound_s=args.cpu_seconds, nthreads=1)
             line["cpu_baseline"] = {"value": rate, "unit": "assemblies/s", "cores": threads, "kind": kind,
-                                    "sample": sample}
+                                    "sample": sample, "cpu_model": cpu_model(),
+                                    "single_core": {"value": rate1, "sample": sample1}}
     gf.close()
     if ws > 1:
         torch.distributed.barrier()
