@@ -383,6 +383,36 @@ def run_ours(args):
         barrier()
         ms_e2e = e0.elapsed_time(e1) / args.steps
     clocks = clk.summary()
+    # full Newton iteration without the solve: device broad phase, narrow
+    # phase, structure rebuild (pattern merge, lists), assembly; wall clock
+    full_iter = None
+    if not batched:
+        reps = 5
+        for _ in range(2):
+            gf.BroadPhase()
+            gf.NarrowPhaseCollisionDetection(None)
+            gf.CreateStructure(copy_back=False)
+            gf.AssembleElemsAndCZs(H)
+        torch.cuda.synchronize(dev)
+        t_s = [0.0, 0.0]
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            gf.BroadPhase()
+            gf.NarrowPhaseCollisionDetection(None)
+            gf.CreateStructure(copy_back=False)
+            torch.cuda.synchronize(dev)
+            t1 = time.perf_counter()
+            gf.AssembleElemsAndCZs(H)
+            torch.cuda.synchronize(dev)
+            t2 = time.perf_counter()
+            t_s[0] += t1 - t0
+            t_s[1] += t2 - t1
+        full_iter = {"value": reps / (t_s[0] + t_s[1]), "unit": "iterations/s",
+                     "structure_ms": 1000 * t_s[0] / reps, "assembly_ms": 1000 * t_s[1] / reps,
+                     "pairs": gf.nPairs, "impacts": gf.nImpacts,
+                     "scope": "device broad phase + narrow phase + structure rebuild + synchronous assembly, "
+                              "host wall clock; no linear solve"}
+
     # per-kernel device times: the same kernels run in the graph's order on
     # one stream with an event after each (no overlap between streams)
     kernels = gf.ProfileAssembly(H, reps=max(args.steps, 10))
@@ -455,6 +485,7 @@ def run_ours(args):
             "gpu_launches": launches_per_step * args.steps,
             "autotune": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in t.items()} for t in tune],
             "mixed_error": mixed_error,
+            "full_iteration": full_iter,
             "clocks": clocks,
         }
         if not args.no_cpu:

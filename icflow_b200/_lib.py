@@ -126,6 +126,9 @@ SIGNATURES = {
     "icf_solve": (I, [P, D, I, P, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "icf_apply_dx": (I, [P, C.POINTER(C.c_double)]),
     "icf_residual_norm": (I, [P, C.POINTER(C.c_double)]),
+    "icf_set_surface_groups": (I, [P, I, P]),
+    "icf_broad_phase": (I, [P, D, C.POINTER(C.c_int)]),
+    "icf_get_pairs": (I, [P, I, P]),
     "icf_mlp_create": (I, [I, C.POINTER(P)]),
     "icf_mlp_destroy": (I, [P]),
     "icf_mlp_last_error": (C.c_char_p, [P]),

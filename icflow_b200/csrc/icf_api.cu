@@ -202,7 +202,7 @@ static void free_all(icf_ctx *c) {
                   c->d_s2m, c->d_dynpos, c->d_gdesc_diag, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
                   c->imp_inc.off, c->imp_inc.inc, c->d_tmp, c->sell_off.meta, c->sell_off.unit,
                   c->sell_off.codes, c->sell_diag.meta, c->sell_diag.unit, c->sell_diag.codes, c->d_czhist,
-                  c->d_tetpos, c->d_stage_off, c->d_stage_diag};
+                  c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup};
   for (void *p : ptrs) cudaFree(p);
 }
 
@@ -346,6 +346,8 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->tetpos_cap = 0;
   ctx->d_stage_off = ctx->d_stage_diag = nullptr;
   ctx->stage_off_cap = ctx->stage_diag_cap = 0;
+  ctx->d_sgroup = nullptr;
+  ctx->pairs_from_broad = false;
   ctx->per_cz_prm = false;
   ctx->have_structure = false;
   ctx->have_nodes = false;
@@ -458,9 +460,53 @@ int icf_transfer_cz_state(icf_ctx *ctx, int n_czs, const double *pmax, const dou
   return ICF_OK;
 }
 
+int icf_set_surface_groups(icf_ctx *ctx, int n_surface, const int *group) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  cudaFree(ctx->d_sgroup);
+  ctx->d_sgroup = nullptr;
+  if (!group) return ICF_OK;
+  if (n_surface != ctx->n_surf) return icf_fail(ctx, ICF_ERR_ARG, "n_surface does not match the static data");
+  ICF_TRY(dalloc(ctx, &ctx->d_sgroup, (size_t)n_surface));
+  ICF_CUDA(ctx, cudaMemcpy(ctx->d_sgroup, group, sizeof(int) * (size_t)n_surface, cudaMemcpyHostToDevice));
+  return ICF_OK;
+}
+
+int icf_broad_phase(icf_ctx *ctx, double pad, int *n_pairs) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static || !ctx->have_nodes) return icf_fail(ctx, ICF_ERR_STATE, "static data and node state first");
+  if (!n_pairs || !(pad >= 0) || !std::isfinite(pad)) return icf_fail(ctx, ICF_ERR_ARG, "pad >= 0 and n_pairs required");
+  ICF_CUDA(ctx, cudaSetDevice(ctx->device));
+  ICF_TRY(icf_broad_phase_impl(ctx, pad, ctx->d_sgroup, n_pairs));
+  ctx->pairs_from_broad = true;
+  return ICF_OK;
+}
+
+int icf_get_pairs(icf_ctx *ctx, int capacity, int *pairs) {
+  ICF_CHECK_CTX(ctx);
+  if (!pairs || capacity < ctx->n_pairs) return icf_fail(ctx, ICF_ERR_SIZE, "pair buffer too small");
+  if (ctx->n_pairs)
+    ICF_CUDA(ctx, cudaMemcpy(pairs, ctx->d_pairs, sizeof(int) * 2 * (size_t)ctx->n_pairs, cudaMemcpyDeviceToHost));
+  return ICF_OK;
+}
+
 int icf_narrow_phase(icf_ctx *ctx, int n_pairs, const int *pairs, int *n_impacts) {
   ICF_CHECK_CTX(ctx);
   if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  if (n_pairs < 0 && pairs == nullptr && n_impacts) {
+    // the pairs of the last icf_broad_phase, already on the device
+    if (!ctx->pairs_from_broad) return icf_fail(ctx, ICF_ERR_STATE, "icf_broad_phase first");
+    if (ctx->prm.CollisionScheme == 0 || ctx->n_pairs == 0) {
+      ctx->n_imp = 0;
+      *n_impacts = 0;
+      ctx->have_structure = false;
+      return ICF_OK;
+    }
+    ICF_TRY(icf_run_narrow_phase(ctx, ctx->n_pairs, n_impacts));
+    ctx->have_structure = false;
+    return ICF_OK;
+  }
+  ctx->pairs_from_broad = false;
   if (n_pairs < 0 || (n_pairs && !pairs) || !n_impacts) return icf_fail(ctx, ICF_ERR_ARG, "bad pair list");
   if (ctx->prm.CollisionScheme == 0 || n_pairs == 0) {
     ctx->n_imp = 0;

@@ -1,0 +1,261 @@
+// icf_broad.cu -- broad phase on the device: candidate surface-element pairs.
+//
+// The reference builds a k-DOP-24 bounding-volume tree on the host every few
+// steps, refits it otherwise and self-collides it to list the element pairs
+// its narrow phase tests (BVHT.cs:29-77, BVHN.cs:39-194, kDOP24.cs:69-169).
+// Only that pair list crosses into the assembly path.  Here it is built where
+// the positions already are, with a uniform grid:
+//   1. axis-aligned box of every surface element at the current positions
+//      (x0 + un), widened by `pad`;
+//   2. cell size = the largest box extent, so a box covers at most 2x2x2 cells;
+//      every (cell, element) entry is listed and the entries are sorted by cell
+//      (CUB radix sort);
+//   3. within each cell, every pair a < b of elements of different groups
+//      whose boxes overlap (closed intervals) is a candidate;
+//   4. the pairs are sorted (a, b) ascending, a pair found in several cells
+//      is kept once, and the list stays on the device for the narrow phase.
+// The cell size, the cell ranges (the lowest cell and the next along each
+// axis) and the overlap test are those of the host candidate generator the
+// tests compare against, so both give the same set.
+// Groups are the meshes: elements of one mesh never pair (the reference's
+// narrow phase would drop most of them anyway for sharing nodes).
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <cstdint>
+
+#include "icf_internal.cuh"
+
+namespace {
+
+struct box {
+  double lo[3], hi[3];
+};
+
+__device__ __forceinline__ box elem_box(const int4 *selem, const double4 *xc, int i, double pad) {
+  const int4 id = selem[i];
+  const int n[4] = {id.x, id.y, id.z, id.w};
+  box b;
+  for (int k = 0; k < 3; k++) {
+    b.lo[k] = 1e300;
+    b.hi[k] = -1e300;
+  }
+  for (int v = 0; v < 4; v++) {
+    const double4 p = xc[n[v]];
+    const double c[3] = {p.x, p.y, p.z};
+    for (int k = 0; k < 3; k++) {
+      b.lo[k] = fmin(b.lo[k], c[k]);
+      b.hi[k] = fmax(b.hi[k], c[k]);
+    }
+  }
+  for (int k = 0; k < 3; k++) {
+    b.lo[k] -= pad;
+    b.hi[k] += pad;
+  }
+  return b;
+}
+
+__global__ void k_boxes(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc, double pad,
+                        double *__restrict__ lohi, double *__restrict__ ext) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0;
+  if (i < n) {
+    const box b = elem_box(selem, xc, i, pad);
+    for (int k = 0; k < 3; k++) {
+      lohi[6 * (size_t)i + k] = b.lo[k];
+      lohi[6 * (size_t)i + 3 + k] = b.hi[k];
+      e = fmax(e, b.hi[k] - b.lo[k]);
+    }
+  }
+  if (i < n) ext[i] = e;
+}
+
+// per element: its lowest cell and which of the next cells along each axis
+// its box also reaches (cells c0 + {0, 1} per axis, those <= the highest)
+__global__ void k_cells(int n, const double *__restrict__ lohi, const double *__restrict__ red, int *__restrict__ cnt,
+                        int4 *__restrict__ clo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double cell = red[0];
+  int c0[3], s[3];
+  for (int k = 0; k < 3; k++) {
+    c0[k] = (int)floor((lohi[6 * (size_t)i + k] - red[1 + k]) / cell);
+    const int c1 = (int)floor((lohi[6 * (size_t)i + 3 + k] - red[1 + k]) / cell);
+    s[k] = c1 > c0[k] ? 1 : 0;
+  }
+  cnt[i] = (s[0] + 1) * (s[1] + 1) * (s[2] + 1);
+  clo[i] = make_int4(c0[0], c0[1], c0[2], s[0] | s[1] << 1 | s[2] << 2);
+}
+
+__device__ __forceinline__ unsigned long long cell_key(int x, int y, int z) {
+  return ((unsigned long long)(unsigned)x << 42) | ((unsigned long long)(unsigned)y << 21) | (unsigned)z;
+}
+
+__global__ void k_entries(int n, const int4 *__restrict__ clo, const int *__restrict__ off,
+                          unsigned long long *__restrict__ key, int *__restrict__ elem) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 c = clo[i];
+  int o = off[i];
+  for (int dz = 0; dz <= ((c.w >> 2) & 1); dz++)
+    for (int dy = 0; dy <= ((c.w >> 1) & 1); dy++)
+      for (int dx = 0; dx <= (c.w & 1); dx++) {
+        key[o] = cell_key(c.x + dx, c.y + dy, c.z + dz);
+        elem[o] = i;
+        o++;
+      }
+}
+
+__device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, const int *group) {
+  if (group && group[a] == group[b]) return false;
+  for (int k = 0; k < 3; k++)
+    if (!(lohi[6 * (size_t)a + k] <= lohi[6 * (size_t)b + 3 + k] && lohi[6 * (size_t)b + k] <= lohi[6 * (size_t)a + 3 + k]))
+      return false;
+  return true;
+}
+
+// entry i pairs with the later entries of its cell; count, then write
+__global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const int *__restrict__ elem,
+                        const double *__restrict__ lohi, const int *__restrict__ group, const int *__restrict__ off,
+                        int *__restrict__ cnt, unsigned long long *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const unsigned long long here = key[i];
+  const int a0 = elem[i];
+  int c = 0;
+  int o = off ? off[i] : 0;
+  for (int j = i + 1; j < m && key[j] == here; j++) {
+    const int b0 = elem[j];
+    const int a = a0 < b0 ? a0 : b0, b = a0 < b0 ? b0 : a0;
+    if (keep_pair(a, b, lohi, group)) {
+      if (out) out[o++] = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
+      c++;
+    }
+  }
+  if (cnt) cnt[i] = c;
+}
+
+__global__ void k_unpack_pairs(int n, const unsigned long long *__restrict__ in, int *__restrict__ pairs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  pairs[2 * (size_t)i] = (int)(in[i] >> 32);
+  pairs[2 * (size_t)i + 1] = (int)(in[i] & 0xffffffffull);
+}
+
+struct min_op {
+  __device__ double operator()(double a, double b) const { return a < b ? a : b; }
+};
+struct max_op {
+  __device__ double operator()(double a, double b) const { return a > b ? a : b; }
+};
+
+// red[0] = cell size (largest extent), red[1..3] = lowest corner
+__global__ void k_strided(int n, const double *__restrict__ lohi, int k, double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = lohi[6 * (size_t)i + k];
+}
+
+}  // namespace
+
+int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pairs_out) {
+  cudaStream_t s = ctx->stream;
+  const int n = ctx->n_surf;
+  *n_pairs_out = 0;
+  ctx->n_pairs = 0;
+  if (n < 2) return ICF_OK;
+  double *lohi, *ext, *red, *tmpv;
+  int *cnt, *off;
+  int4 *clo;
+  ICF_CUDA(ctx, cudaMallocAsync(&lohi, sizeof(double) * 6 * (size_t)n, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&ext, sizeof(double) * (size_t)n, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&tmpv, sizeof(double) * (size_t)n, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&red, sizeof(double) * 4, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&cnt, sizeof(int) * (size_t)(n + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&off, sizeof(int) * (size_t)(n + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&clo, sizeof(int4) * (size_t)n, s));
+  ICF_CUDA(ctx, cudaMemsetAsync(ext, 0, sizeof(double), s));
+  k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, lohi, ext);
+  size_t tb = 0;
+  cub::DeviceReduce::Reduce(nullptr, tb, ext, red, n, max_op(), 0.0, s);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceReduce::Reduce(ctx->d_tmp, tb, ext, red, n, max_op(), 0.0, s));
+  for (int k = 0; k < 3; k++) {
+    k_strided<<<icf_blocks(n, 256), 256, 0, s>>>(n, lohi, k, tmpv);
+    tb = 0;
+    cub::DeviceReduce::Reduce(nullptr, tb, tmpv, red + 1 + k, n, min_op(), 1e300, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceReduce::Reduce(ctx->d_tmp, tb, tmpv, red + 1 + k, n, min_op(), 1e300, s));
+  }
+  double h_red[4];
+  ICF_CUDA(ctx, cudaMemcpyAsync(h_red, red, sizeof(h_red), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  if (!(h_red[0] > 0) || !std::isfinite(h_red[0])) return icf_fail(ctx, ICF_ERR_NUMERIC, "broad phase: degenerate boxes");
+  k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, lohi, red, cnt, clo);
+  ICF_CUDA(ctx, cudaMemsetAsync(cnt + n, 0, sizeof(int), s));
+  tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, n + 1, s);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, cnt, off, n + 1, s));
+  int m = 0;
+  ICF_CUDA(ctx, cudaMemcpyAsync(&m, off + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  unsigned long long *k0, *k1;
+  int *e0, *e1, *pc, *po;
+  ICF_CUDA(ctx, cudaMallocAsync(&k0, sizeof(unsigned long long) * (size_t)m, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&k1, sizeof(unsigned long long) * (size_t)m, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&e0, sizeof(int) * (size_t)m, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&e1, sizeof(int) * (size_t)m, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&pc, sizeof(int) * (size_t)(m + 1), s));
+  ICF_CUDA(ctx, cudaMallocAsync(&po, sizeof(int) * (size_t)(m + 1), s));
+  k_entries<<<icf_blocks(n, 256), 256, 0, s>>>(n, clo, off, k0, e0);
+  tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, e0, e1, m, 0, 63, s);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, e0, e1, m, 0, 63, s));
+  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, k1, e1, lohi, d_group, nullptr, pc, nullptr);
+  ICF_CUDA(ctx, cudaMemsetAsync(pc + m, 0, sizeof(int), s));
+  tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, pc, po, m + 1, s);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, pc, po, m + 1, s));
+  int nall = 0, np = 0;
+  ICF_CUDA(ctx, cudaMemcpyAsync(&nall, po + m, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  if (nall > 0) {
+    unsigned long long *p0, *p1;
+    int *d_np;
+    ICF_CUDA(ctx, cudaMallocAsync(&p0, sizeof(unsigned long long) * (size_t)nall, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&p1, sizeof(unsigned long long) * (size_t)nall, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&d_np, sizeof(int), s));
+    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, k1, e1, lohi, d_group, po, nullptr, p0);
+    tb = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, p0, p1, nall, 0, 64, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, p0, p1, nall, 0, 64, s));
+    tb = 0;
+    cub::DeviceSelect::Unique(nullptr, tb, p1, p0, d_np, nall, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, p1, p0, d_np, nall, s));
+    ICF_CUDA(ctx, cudaMemcpyAsync(&np, d_np, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    ICF_CUDA(ctx, cudaFreeAsync(d_np, s));
+    if (np > ctx->pairs_cap || !ctx->d_pairs) {
+      cudaFree(ctx->d_pairs);
+      cudaFree(ctx->d_masks);
+      ctx->d_pairs = ctx->d_masks = nullptr;
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_pairs, sizeof(int) * 2 * (size_t)np));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_masks, sizeof(int) * (size_t)np));
+      ctx->pairs_cap = np;
+    }
+    k_unpack_pairs<<<icf_blocks(np, 256), 256, 0, s>>>(np, p0, ctx->d_pairs);
+    ICF_CUDA(ctx, cudaFreeAsync(p0, s));
+    ICF_CUDA(ctx, cudaFreeAsync(p1, s));
+  }
+  ICF_CUDA(ctx, cudaGetLastError());
+  void *tmp[] = {lohi, ext, tmpv, red, cnt, off, clo, k0, k1, e0, e1, pc, po};
+  for (void *p : tmp) ICF_CUDA(ctx, cudaFreeAsync(p, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  ctx->n_pairs = np;
+  *n_pairs_out = np;
+  return ICF_OK;
+}

@@ -202,6 +202,8 @@ struct icf_ctx {
   // narrow phase
   int n_pairs = 0, pairs_cap = 0;
   int *d_pairs = nullptr, *d_masks = nullptr;
+  int *d_sgroup = nullptr;  // group (mesh) of every surface element, or null
+  bool pairs_from_broad = false;
 
   // node incidence lists for the node forces
   icf_node_inc tet_inc, imp_inc;
@@ -280,6 +282,7 @@ int icf_ensure_cz_hist(icf_ctx *ctx, cudaStream_t s);
 int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, double *relres);
 void icf_free_solver(icf_ctx *ctx);
 int icf_launch_sumsq(icf_ctx *ctx, const double *d_x, long long n);
+int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pairs_out);
 int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out);
 int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant);
 int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const char **names,

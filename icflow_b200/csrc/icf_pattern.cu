@@ -863,7 +863,8 @@ __global__ void k_tetpos(long long n, const uint32_t *__restrict__ codes, int *_
 int icf_build_contrib(icf_ctx *ctx) {
   cudaStream_t s = ctx->stream;
   const long long ne = ctx->n_elem;
-  if (ne == 0) return ICF_OK;
+  // only the contribution layout needs the map and its staging
+  if (ne == 0 || ctx->layout != ICF_LAYOUT_CONTRIB) return ICF_OK;
   if (16 * ne > ctx->tetpos_cap || !ctx->d_tetpos) {
     cudaFree(ctx->d_tetpos);
     ctx->d_tetpos = nullptr;

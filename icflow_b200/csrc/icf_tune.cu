@@ -63,7 +63,14 @@ int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant) {
                                       : icf_cz_variants();
   if (kind < 0 || kind > 4 || variant < 0 || variant >= n)
     return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..4 and a variant index of that kind");
-  if (kind == 3) ctx->layout = variant;
+  if (kind == 3) {
+    const bool build = ctx->layout != variant && variant == ICF_LAYOUT_CONTRIB;
+    ctx->layout = variant;
+    if (build && ctx->have_structure) {
+      ICF_TRY_RC(icf_build_contrib(ctx));
+      ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+  }
   if (kind == 4) ctx->tune_cz = variant;
   if (kind == 0) ctx->tune_tet = variant;
   if (kind == 1) {

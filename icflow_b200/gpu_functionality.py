@@ -103,6 +103,7 @@ class GPU_Functionality:
 
     # -- TransferStaticDataToDevice (:255-302) --
     def TransferStaticDataToDevice(self):
+        self._groups_set = False
         mc = self.mc
         x0 = np.ascontiguousarray(mc.x0, np.float64)
         el = np.ascontiguousarray(mc.elems, np.int32)
@@ -128,11 +129,35 @@ class GPU_Functionality:
         check(self.ctx, self.lib.icf_transfer_cz_state(self.ctx, len(failed), dptr(pmax), dptr(tmax),
                                                        iptr(failed)))
 
-    # -- NarrowPhaseCollisionDetection (:539-616) --
-    def NarrowPhaseCollisionDetection(self, narrowList: np.ndarray):
-        pairs = np.ascontiguousarray(narrowList, np.int32).reshape(-1, 2)
+    # -- broad phase on the device (replaces the host BVH, BVHT.cs:29-77) --
+    def BroadPhase(self, pad: float = 0.0) -> int:
+        """Candidate surface-element pairs of different meshes with
+        overlapping boxes at the current positions; they stay on the device
+        for NarrowPhaseCollisionDetection(None)."""
+        if not getattr(self, "_groups_set", False):
+            grp = np.ascontiguousarray(self.mc.selem_mesh, np.int32)
+            check(self.ctx, self.lib.icf_set_surface_groups(self.ctx, len(grp), iptr(grp)))
+            self._groups_set = True
         n = C.c_int()
-        check(self.ctx, self.lib.icf_narrow_phase(self.ctx, len(pairs), iptr(pairs), C.byref(n)))
+        check(self.ctx, self.lib.icf_broad_phase(self.ctx, float(pad), C.byref(n)))
+        self.nPairs = n.value
+        return n.value
+
+    def GetPairs(self) -> np.ndarray:
+        out = np.zeros((max(self.nPairs, 1), 2), np.int32)
+        check(self.ctx, self.lib.icf_get_pairs(self.ctx, len(out), iptr(out)))
+        return out[:self.nPairs]
+
+    # -- NarrowPhaseCollisionDetection (:539-616) --
+    def NarrowPhaseCollisionDetection(self, narrowList: np.ndarray | None):
+        """narrowList: [n, 2] surface-element pairs, or None for the pairs of
+        the last BroadPhase (already on the device)."""
+        n = C.c_int()
+        if narrowList is None:
+            check(self.ctx, self.lib.icf_narrow_phase(self.ctx, -1, None, C.byref(n)))
+        else:
+            pairs = np.ascontiguousarray(narrowList, np.int32).reshape(-1, 2)
+            check(self.ctx, self.lib.icf_narrow_phase(self.ctx, len(pairs), iptr(pairs), C.byref(n)))
         self.nImpacts = self.cf.nCollisions = n.value
         self.c_itet = np.zeros((n.value, 4), np.int32)
         if n.value:

@@ -19,9 +19,10 @@ Per step (ImplicitModel3.Step, :369-435):
 
 The time step is fixed: _adjustTimeStep's time-scale factor (:259-287) and the
 damage-explosion frame discard are not reproduced.  The node state, the
-matrix and the Newton increment stay on the device; the host reads v once per
-step (for the guess) and, with contact, the tentative positions once per
-iteration (for the candidate pairs of the broad phase).
+contact pairs, the matrix and the Newton increment stay on the device; the
+host reads v once per step (for the guess).  broad_phase="host" swaps the
+device broad phase for the host grid generator (the tentative positions then
+cross to the host every iteration).
 """
 from __future__ import annotations
 
@@ -78,7 +79,8 @@ class ImplicitModel3:
 
     def __init__(self, coll: M.Collection, prms: ModelPrms, strengths: np.ndarray | None = None,
                  device: int = 0, precision: int = 0, contact: bool = False, rel_tol: float = 1e-12,
-                 v0: np.ndarray | None = None, convergence: str = "increment", res_tol: float = 1e-8):
+                 v0: np.ndarray | None = None, convergence: str = "increment", res_tol: float = 1e-8,
+                 broad_phase: str = "device"):
         """convergence: "increment" is the reference's test on NormOfDx
         (_checkDivergence); "residual" stops when ||rhs|| <= res_tol * ||rhs
         at zero increment||, a scale that does not depend on the initial
@@ -87,6 +89,9 @@ class ImplicitModel3:
             raise ValueError("convergence is 'increment' or 'residual'")
         self.convergence = convergence
         self.res_tol = res_tol
+        if broad_phase not in ("device", "host"):
+            raise ValueError("broad_phase is 'device' or 'host'")
+        self.broad_phase = broad_phase
         self.coll = coll
         self.prms = prms
         self.contact = contact
@@ -154,8 +159,7 @@ class ImplicitModel3:
             gf.SetDU(du)
             gf.InferTentativeValues(h)
             if self.contact:
-                uu, _, _, duc = gf.GetNodeState()
-                gf.NarrowPhaseCollisionDetection(M.candidate_pairs(coll, coll.x0 + uu + duc))
+                self._contact()
             gf.CreateStructure(copy_back=False)
             gf.AssembleElemsAndCZs(h)
             return gf.ResidualNorm()
@@ -168,6 +172,17 @@ class ImplicitModel3:
             out.append(resid(du) / r0 if r0 > 0 else 0.0)
         gf.SetDU(np.zeros_like(u))
         return out
+
+    def _contact(self):
+        """Broad and narrow phase at the tentative positions: on the device
+        (pairs never leave it), or with the host grid generator."""
+        gf = self.gf
+        if self.broad_phase == "device":
+            gf.BroadPhase()
+            gf.NarrowPhaseCollisionDetection(None)
+        else:
+            uu, _, _, duc = gf.GetNodeState()
+            gf.NarrowPhaseCollisionDetection(M.candidate_pairs(self.coll, self.coll.x0 + uu + duc))
 
     def Step(self, warm_start=None) -> StepStats:
         t0 = time.perf_counter()
@@ -189,9 +204,7 @@ class ImplicitModel3:
         def assemble():
             gf.InferTentativeValues(h)
             if self.contact:
-                uu, _, _, duc = gf.GetNodeState()
-                pairs = M.candidate_pairs(coll, coll.x0 + uu + duc)
-                gf.NarrowPhaseCollisionDetection(pairs)
+                self._contact()
                 self._n_imp = gf.nImpacts
             gf.CreateStructure(copy_back=False)
             return gf.AssembleElemsAndCZs(h)

@@ -151,6 +151,17 @@ int icf_transfer_cz_state(icf_ctx *ctx, int n_czs, const double *pmax,
  * closest adjacent face.  The impacts become part of the next structure. */
 int icf_narrow_phase(icf_ctx *ctx, int n_pairs, const int *pairs,
                      int *n_impacts);
+/* Broad phase on the device (replaces the host k-DOP BVH, BVHT.cs:29-77,
+ * BVHN.cs:39-194, whose element-pair list NarrowPhaseCollisionDetection
+ * receives): surface-element pairs a < b of different groups whose
+ * axis-aligned boxes at the current positions, widened by pad, overlap.
+ * Groups (e.g. the mesh of each surface element) come from
+ * icf_set_surface_groups; without them every pair qualifies.  The pairs stay
+ * on the device: icf_narrow_phase(ctx, -1, NULL, &n) uses them; icf_get_pairs
+ * copies them out (pairs[n*2], ascending). */
+int icf_set_surface_groups(icf_ctx *ctx, int n_surface, const int *group);
+int icf_broad_phase(icf_ctx *ctx, double pad, int *n_pairs);
+int icf_get_pairs(icf_ctx *ctx, int capacity, int *pairs);
 /* impacts[n*4] = (node, face vertex 0, 1, 2), the c_itet rows of :611. */
 int icf_get_impacts(icf_ctx *ctx, int capacity, int *impacts);
 /* Supply an impact list directly (e.g. one read back with ReadImpacts). */

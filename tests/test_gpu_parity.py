@@ -342,3 +342,22 @@ def test_fp32_mixed_error_report(O, case):
         assert vec_rel(o["tent"], a["tent"][sel]) <= FP64_TOL
     print(f"{case}: FP32-mixed vs FP64 oracle: blocks {err_vals:.2e} (rowwise), rhs {err_rhs:.2e}")
     gf.close()
+
+
+def test_device_broad_phase_matches_host_pairs(O):
+    """The device broad phase gives the host generator's pair set, and the
+    narrow phase from those device-resident pairs gives the same impacts."""
+    for seed, gap in ((1, -0.3), (2, -0.05), (3, 0.2)):
+        coll = M.polycrystal(n=7, grains=5, seed=seed, platens=True, gap=gap)
+        prms = config_prms(penaltyK=1e8)
+        gf = _gf(coll, prms)
+        un, vn, an = random_state(coll, seed, du=3e-6)
+        gf.TransferNodesToGPU(un, vn, an)
+        n = gf.BroadPhase()
+        dev = gf.GetPairs()
+        host = M.candidate_pairs(coll, coll.x0 + un)
+        assert n == len(host) and np.array_equal(dev, host), (seed, n, len(host))
+        imps_dev = gf.NarrowPhaseCollisionDetection(None).copy()
+        imps_host = gf.NarrowPhaseCollisionDetection(host).copy()
+        assert np.array_equal(imps_dev, imps_host)
+        gf.close()
