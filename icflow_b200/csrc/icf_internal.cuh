@@ -234,7 +234,7 @@ struct icf_ctx {
   //                       straight into the gathers' sliced-ELL positions
   //                       (d_stage_off / d_stage_diag, 64 B each, position
   //                       map d_tetpos[16 e + 4 a + b]), read as streams.
-  int layout = 1;
+  int layout = ICF_LAYOUT_RECORDS;
   int *d_tetpos = nullptr;
   long long tetpos_cap = 0;
   void *d_stage_off = nullptr, *d_stage_diag = nullptr;

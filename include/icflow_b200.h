@@ -220,9 +220,9 @@ int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out
  * reports all timings.  Needs a structure; leaves the outputs of a complete
  * assembly behind.  icf_set_variant pins one variant by index (kind 0 tet,
  * 1 off-diagonal gather, 2 diagonal gather, 4 CZ kernel) or the staging layout (kind 3:
- * 0 per-tet records gathered through contribution codes, 1 per-contribution
- * records written at their gather positions and read as streams, the
- * default).  The tuner also times whole assemblies with each layout first. */
+ * 0 per-tet records gathered through contribution codes, the default; 1
+ * per-contribution records written at their gather positions and read as
+ * streams).  The tuner also times whole assemblies with each layout first. */
 #define ICF_MAX_TUNE 32
 typedef struct icf_tune_report {
   int n;                          /* candidates timed */
