@@ -138,6 +138,8 @@ SIGNATURES = {
     "icf_mlp_forward": (I, [P, I, P, P]),
     "icf_mlp_grad": (I, [P, I, P, P, P, C.POINTER(C.c_float)]),
     "icf_mlp_train": (I, [P, I, P, P, I, I, C.c_float, C.c_ulonglong, C.POINTER(C.c_float)]),
+    "icf_mlp_grad_dy": (I, [P, I, P, P, P]),
+    "icf_mlp_adam_step": (I, [P, P, C.c_float]),
     "icf_set_variant": (I, [P, I, I]),
     "icf_assemble_noalloc": (I, [P, D, P, P, P, P, P, C.POINTER(icf_counts)]),
     "icf_transfer_linear_system": (I, [P, dp, dp]),

@@ -234,13 +234,15 @@ __global__ void __launch_bounds__(256) k_mlp_fwd_train(int n, const float *__res
         }
       }
     const float inv = 2.0f / (float)(n * NO);
+    if (tgt != nullptr) {  // tgt == nullptr: dy was supplied by the caller
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const int r = r0 + g + (e >= 2 ? 8 : 0), c = 2 * t + (e & 1);
-      if (r < n && c < NO) {
-        const float d = f.y[e] - tgt[(size_t)r * NO + c];
-        dy[(size_t)r * NO + c] = inv * d;
-        l += d * d;
+      for (int e = 0; e < 4; e++) {
+        const int r = r0 + g + (e >= 2 ? 8 : 0), c = 2 * t + (e & 1);
+        if (r < n && c < NO) {
+          const float d = f.y[e] - tgt[(size_t)r * NO + c];
+          dy[(size_t)r * NO + c] = inv * d;
+          l += d * d;
+        }
       }
     }
   }
@@ -433,14 +435,15 @@ int ensure_cap(icf_mlp *m, int n) {
   return ICF_OK;
 }
 
-// forward + backward of the data already in d_x, d_y (n nodes): d_grad, loss
-int grad_on_device(icf_mlp *m, int n, float *loss_host) {
+// forward + backward of the data already in d_x, d_y (n nodes): d_grad, loss.
+// dy_given: d_dy already holds dL/dy (the caller's loss), d_y is unused.
+int grad_on_device(icf_mlp *m, int n, float *loss_host, bool dy_given = false) {
   cudaStream_t s = m->stream;
   const int tiles = (n + 15) / 16;
   const int blocks = (tiles + 7) / 8;
   float *loss_part = m->d_loss + 1;
-  k_mlp_fwd_train<<<blocks, 256, 0, s>>>(n, m->d_x, m->d_y, m->d_wb, m->d_master, m->d_norm, m->d_z1, m->d_h1,
-                                          m->d_z2, m->d_h2, m->d_dy, loss_part);
+  k_mlp_fwd_train<<<blocks, 256, 0, s>>>(n, m->d_x, dy_given ? nullptr : m->d_y, m->d_wb, m->d_master, m->d_norm,
+                                          m->d_z1, m->d_h1, m->d_z2, m->d_h2, m->d_dy, loss_part);
   // warps beyond the last tile wrote zero partials: count them in
   k_mlp_bwd_act<<<icf_blocks(n, 128), 128, 0, s>>>(n, m->d_wb, m->d_z1, m->d_z2, m->d_dy, m->d_dz1, m->d_dz2);
   const int nch = (n + CHUNK - 1) / CHUNK;
@@ -553,6 +556,33 @@ int icf_mlp_grad(icf_mlp *m, int n, const float *x, const float *y, float *grad,
   if (grad_on_device(m, n, &l)) return ICF_ERR_CUDA;
   MLP_CUDA(m, cudaMemcpy(grad, m->d_grad, sizeof(float) * NPAR, cudaMemcpyDeviceToHost));
   if (loss) *loss = l;
+  return ICF_OK;
+}
+
+int icf_mlp_grad_dy(icf_mlp *m, int n, const float *x, const float *dy, float *grad) {
+  if (!m || n <= 0 || !x || !dy) return ICF_ERR_ARG;
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  if (ensure_cap(m, n)) return ICF_ERR_CUDA;
+  cudaStream_t s = m->stream;
+  MLP_CUDA(m, cudaMemcpyAsync(m->d_x, x, sizeof(float) * NI * (size_t)n, cudaMemcpyHostToDevice, s));
+  MLP_CUDA(m, cudaMemcpyAsync(m->d_dy, dy, sizeof(float) * NO * (size_t)n, cudaMemcpyHostToDevice, s));
+  if (grad_on_device(m, n, nullptr, true)) return ICF_ERR_CUDA;
+  if (grad) MLP_CUDA(m, cudaMemcpyAsync(grad, m->d_grad, sizeof(float) * NPAR, cudaMemcpyDeviceToHost, s));
+  MLP_CUDA(m, cudaStreamSynchronize(s));
+  return ICF_OK;
+}
+
+int icf_mlp_adam_step(icf_mlp *m, const float *grad, float lr) {
+  if (!m || !(lr > 0)) return ICF_ERR_ARG;
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  cudaStream_t s = m->stream;
+  if (grad) MLP_CUDA(m, cudaMemcpyAsync(m->d_grad, grad, sizeof(float) * NPAR, cudaMemcpyHostToDevice, s));
+  m->adam_t++;
+  const float b1c = 1.f - powf(0.9f, (float)m->adam_t), b2c = 1.f - powf(0.999f, (float)m->adam_t);
+  k_mlp_adam<<<icf_blocks(NPAR, 256), 256, 0, s>>>(m->d_master, m->d_m, m->d_v, m->d_grad, lr, b1c, b2c);
+  k_mlp_pack<<<icf_blocks(WB_N, 256), 256, 0, s>>>(m->d_master, m->d_wb);
+  MLP_CUDA(m, cudaGetLastError());
+  MLP_CUDA(m, cudaStreamSynchronize(s));
   return ICF_OK;
 }
 

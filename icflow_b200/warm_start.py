@@ -81,6 +81,17 @@ class MLP:
                                           g.ctypes.data_as(C.c_void_p), C.byref(loss)))
         return g, loss.value
 
+    def grad_dy(self, x: np.ndarray, dy: np.ndarray):
+        """Backward pass for a caller-defined loss (dy = dL/d output); the
+        gradient stays on the device for adam_step."""
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, NI)
+        dy = np.ascontiguousarray(dy, np.float32).reshape(-1, NO)
+        self._check(self.lib.icf_mlp_grad_dy(self.h, len(x), x.ctypes.data_as(C.c_void_p),
+                                             dy.ctypes.data_as(C.c_void_p), None))
+
+    def adam_step(self, lr: float):
+        self._check(self.lib.icf_mlp_adam_step(self.h, None, float(lr)))
+
     def train(self, x, y, epochs=20, batch=4096, lr=1e-3, seed=0) -> float:
         x = np.ascontiguousarray(x, np.float32).reshape(-1, NI)
         y = np.ascontiguousarray(y, np.float32).reshape(-1, NO)
@@ -119,6 +130,7 @@ class LearnedWarmStart:
         self.net.set_params(init_params(seed))
         self.xs: list[np.ndarray] = []
         self.ys: list[np.ndarray] = []
+        self.mats: list = []
         self.norm = None
         self.seed = seed
         self.gain = 1.0
@@ -128,6 +140,15 @@ class LearnedWarmStart:
         act = model.active
         self.xs.append(features(u, v, a, du1, du2)[act])
         self.ys.append((du_acc - v * h - (du1 - du2))[act].astype(np.float32))
+        # the step's last assembled matrix (at the accepted iterate), for the
+        # residual-weighted loss
+        gf = model.gf
+        vals, _ = gf.TransferLinearSystemToHost()
+        N = gf.linearSystem.N
+        rows = np.zeros(N + 1, np.int32)
+        cols = np.zeros(gf.linearSystem.nnz, np.int32)
+        _lib.check(gf.ctx, gf.lib.icf_get_structure(gf.ctx, _lib.iptr(rows), _lib.iptr(cols)))
+        self.mats.append((N, rows, cols, vals.copy(), model.coll.alt[act].copy()))
 
     def dataset(self):
         return np.concatenate(self.xs), np.concatenate(self.ys)
@@ -144,6 +165,59 @@ class LearnedWarmStart:
         p, _ = self.net.get_params()
         self.net.set_params(p, self.norm)
         return self.net.train(x, y / out_scale, epochs=epochs, batch=min(batch, len(x)), lr=lr, seed=self.seed)
+
+    def fit_residual(self, epochs=40, lr=3e-4, warm_epochs=0) -> float:
+        """Training on what the Newton loop pays for: per recorded step, the
+        force residual the prediction error causes, ||A e||^2, with A the
+        step's assembled matrix (symmetric, from its upper blocks) and e the
+        error of the predicted correction, normalised by the mean over the
+        steps of ||A y||^2 for the true corrections y (so 1.0 is the zero
+        network, i.e. the extrapolation alone).  The matrix products run on
+        the host (scipy); the network's forward and backward run on the
+        device.  Returns the mean loss of the last epoch."""
+        import scipy.sparse as sp
+
+        x_all, y_all = self.dataset()
+        shift = x_all.mean(axis=0)
+        sd = x_all.std(axis=0)
+        scale = 1.0 / np.where(sd > 0, sd, 1.0)
+        osd = y_all.std(axis=0)
+        out_scale = np.where(osd > 0, osd, 1.0)
+        self.norm = np.concatenate([shift, scale, out_scale]).astype(np.float32)
+        p, _ = self.net.get_params()
+        self.net.set_params(p, self.norm)
+        if warm_epochs:
+            self.net.train(x_all, y_all / out_scale, epochs=warm_epochs, batch=min(2048, len(x_all)), lr=lr,
+                           seed=self.seed)
+        mats = []
+        for (N, rows, cols, vals, alt) in self.mats:
+            U = sp.bsr_matrix((vals.reshape(-1, 3, 3), cols, rows), shape=(3 * N, 3 * N)).tocsr()
+            diag = cols == np.repeat(np.arange(N), np.diff(rows))
+            D = sp.bsr_matrix((vals.reshape(-1, 3, 3) * diag[:, None, None], cols, rows), shape=(3 * N, 3 * N)).tocsr()
+            mats.append(((U + U.T - D).tocsr(), N, alt))
+        dens = []
+        for (A, N, alt), y in zip(mats, self.ys):
+            yy = np.zeros((N, 3))
+            yy[alt] = y
+            dens.append(float(np.square(A @ yy.ravel()).sum()))
+        den = float(np.mean(dens)) + 1e-300
+        rng = np.random.default_rng(self.seed)
+        last = 0.0
+        for _ in range(epochs):
+            tot = 0.0
+            for s in rng.permutation(len(self.xs)):
+                A, N, alt = mats[s]
+                x, y = self.xs[s], self.ys[s].astype(np.float64)
+                pred = self.net.forward(x).astype(np.float64) * out_scale
+                e = np.zeros((N, 3))
+                e[alt] = pred - y
+                r = A @ e.ravel()
+                tot += float(r @ r) / den
+                g = (2.0 / den) * (A @ r).reshape(N, 3)[alt]
+                self.net.grad_dy(x, g * out_scale)
+                self.net.adam_step(lr)
+            last = tot / len(self.xs)
+        return last
 
     # ---- the guess --------------------------------------------------------------
     def guess(self, model, h, u, v, a, gain=None):

@@ -321,6 +321,13 @@ int icf_mlp_get_params(icf_mlp *m, float *params, float *norm);
 int icf_mlp_forward(icf_mlp *m, int n, const float *x, float *y);
 /* gradient of the mean squared error over n nodes and 3 outputs */
 int icf_mlp_grad(icf_mlp *m, int n, const float *x, const float *y, float *grad, float *loss);
+/* gradient for a loss the caller defines: dy[n*3] = dL/d(output), so that
+ * any loss on the outputs (e.g. the force residual of the predicted
+ * increments) trains through the same backward kernels; grad may be NULL
+ * (kept on the device for icf_mlp_adam_step) */
+int icf_mlp_grad_dy(icf_mlp *m, int n, const float *x, const float *dy, float *grad);
+/* one Adam step with grad (NULL: the gradient of the last icf_mlp_grad_dy) */
+int icf_mlp_adam_step(icf_mlp *m, const float *grad, float lr);
 /* minibatch Adam on the device; epochs over a seeded shuffle; *loss = final
  * mean squared error over all n */
 int icf_mlp_train(icf_mlp *m, int n, const float *x, const float *y, int epochs, int batch, float lr,
