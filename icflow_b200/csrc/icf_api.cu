@@ -201,7 +201,9 @@ static void free_all(icf_ctx *c) {
                   c->d_masks, c->d_imp_ci, c->d_imp_cd, c->d_rc_mid, c->d_diag, c->d_offd,
                   c->d_s2m, c->d_dynpos, c->d_gdesc_diag, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
                   c->imp_inc.off, c->imp_inc.inc, c->d_tmp, c->sell_off.meta, c->sell_off.unit,
-                  c->sell_off.codes, c->sell_diag.meta, c->sell_diag.unit, c->sell_diag.codes, c->d_czhist,
+                  c->sell_off.codes, c->sell_diag.meta, c->sell_diag.unit, c->sell_diag.codes,
+                  c->sell_off_cz.meta, c->sell_off_cz.unit, c->sell_off_cz.codes, c->sell_diag_cz.meta,
+                  c->sell_diag_cz.unit, c->sell_diag_cz.codes, c->d_czhist,
                   c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup};
   for (void *p : ptrs) cudaFree(p);
 }
@@ -340,6 +342,8 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->tet_inc = icf_node_inc(); ctx->imp_inc = icf_node_inc(); ctx->d_tmp = nullptr; ctx->tmp_bytes = 0;
   ctx->sell_off = icf_sell();
   ctx->sell_diag = icf_sell();
+  ctx->sell_off_cz = icf_sell();
+  ctx->sell_diag_cz = icf_sell();
   ctx->d_czhist = nullptr;
   ctx->hist_valid = false;
   ctx->d_tetpos = nullptr;

@@ -923,7 +923,6 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     const int rc = icf_launch_imp_unit(ctx, sb);
     if (rc) return rc;
   }
-  ICF_CUDA(ctx, cudaEventRecord(e_b, sb));
 
   // main: tets
   if (ctx->n_elem > 0)
@@ -933,17 +932,16 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   const bool contrib = ctx->layout == ICF_LAYOUT_CONTRIB;
   // per tet: the staging it writes (records, or rhs + contribution records)
   // and the part of it the off-diagonal and diagonal gathers read back
-  const long long n_doff = ctx->n_rc_off, n_ddiag = ctx->n_rc - ctx->n_rc_off;  // tet + CZ codes
-  long long tet_out, off_in, diag_in;
+  long long tet_out, off_rec, diag_rec;
   if (contrib) {
     const long long ro = mixed ? 32 : 64, rd = mixed ? 48 : 64;
     tet_out = 64 * ctx->n_elem + 128 * ctx->n_elem + ro * 6 * ctx->n_elem + rd * 4 * ctx->n_elem;
-    off_in = ro * 6 * ctx->n_elem;
-    diag_in = rd * 4 * ctx->n_elem;
+    off_rec = ro * 6 * ctx->n_elem;
+    diag_rec = rd * 4 * ctx->n_elem;
   } else {
     tet_out = (mixed ? 192 : 256) * ctx->n_elem;
-    off_in = (mixed ? 64 : 128) * ctx->n_elem + 4 * n_doff;
-    diag_in = (mixed ? 192 : 256) * ctx->n_elem + 4 * n_ddiag;
+    off_rec = (mixed ? 64 : 128) * ctx->n_elem;
+    diag_rec = (mixed ? 192 : 256) * ctx->n_elem;
   }
   const long long cz_rec = mixed ? 240 : 8 * ICF_CZ_STAGE;
   if (ctx->n_elem > 0) icf_prof_mark(ctx, s, "k_tet_unit", 16 * ctx->n_elem + tet_out + 112LL * ctx->n_nodes);
@@ -961,23 +959,53 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   const double nb = ctx->prm.NewmarkBeta, ng = ctx->prm.NewmarkGamma;
   const double sc = 1.0 + ctx->prm.dampingStiffness * ng / (h * nb);
   const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
-  // aux0: off-diagonal blocks once the tets are staged
-  ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_tet, 0));
-  if (ctx->n_offd > 0)
-    ICF_TRY_RC(icf_launch_gather_off(ctx, ctx->tune_off, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals,
-                                     sa));
-  // descriptors, codes, the h records of every tet and the CZ staging once,
-  // blocks out
-  if (ctx->n_offd > 0)
-    icf_prof_mark(ctx, sa, "k_gather_off", 80LL * ctx->n_offd + off_in + cz_rec * ctx->n_cz);
+  // The gathers.  Algorithmic bytes of one list: its descriptors and blocks
+  // (80 B per off-diagonal block, 104 B per row with its rhs), its codes, its
+  // share (by codes) of the tet records and, for a list with CZ codes, the
+  // CZ staging once.
+  const icf_sell &OA = ctx->sell_off, &OB = ctx->sell_off_cz, &DA = ctx->sell_diag, &DB = ctx->sell_diag_cz;
+  auto list_bytes = [&](const icf_sell &L, long long per_unit, long long rec, long long n_codes_all,
+                        bool cz) {
+    const double share = n_codes_all > 0 ? (double)L.n_real / (double)n_codes_all : 0.0;
+    return per_unit * L.n_units + 4LL * L.n_real + (long long)(share * rec) + (cz ? cz_rec * ctx->n_cz : 0);
+  };
+  const long long codes_off = OA.n_real + OB.n_real, codes_diag = DA.n_real + DB.n_real;
+  auto gather_off = [&](const icf_sell &L, cudaStream_t q, const char *name, bool cz) -> int {
+    if (L.n_units == 0) return ICF_OK;
+    ICF_TRY_RC(icf_launch_gather_off(ctx, L, ctx->tune_off, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu,
+                                     ctx->d_vals, q));
+    icf_prof_mark(ctx, q, name, list_bytes(L, 80, off_rec, codes_off, cz));
+    return ICF_OK;
+  };
+  auto gather_diag = [&](const icf_sell &L, cudaStream_t q, const char *name, bool cz) -> int {
+    if (L.n_units == 0) return ICF_OK;
+    ICF_TRY_RC(icf_launch_gather_diag(ctx, L, ctx->tune_diag, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu,
+                                      ctx->d_vals, ctx->d_rhs, q));
+    icf_prof_mark(ctx, q, name, list_bytes(L, 104, diag_rec, codes_diag, cz));
+    return ICF_OK;
+  };
+  if (OB.n_units > 0 || DB.n_units > 0) {
+    // split lists: the units without CZ codes run as soon as the tets are
+    // staged, beside the CZ kernel (off-diagonal on aux1, diagonal on main);
+    // the units with CZ codes wait for the CZs (off-diagonal on aux0,
+    // diagonal on main)
+    ICF_CUDA(ctx, cudaStreamWaitEvent(sb, e_tet, 0));
+    ICF_TRY_RC(gather_off(OA, sb, "k_gather_off", false));
+    ICF_TRY_RC(gather_diag(DA, s, "k_gather_diag", false));
+    ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_tet, 0));
+    ICF_TRY_RC(gather_off(OB, sa, "k_gather_off_cz", true));
+    ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
+    ICF_TRY_RC(gather_diag(DB, s, "k_gather_diag_cz", true));
+  } else {
+    // one list per gather: off-diagonal on aux0 once the tets are staged,
+    // diagonal on main once the CZs are
+    ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_tet, 0));
+    ICF_TRY_RC(gather_off(OA, sa, "k_gather_off", true));
+    ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
+    ICF_TRY_RC(gather_diag(DA, s, "k_gather_diag", true));
+  }
   ICF_CUDA(ctx, cudaEventRecord(e_a, sa));
-  // main: diagonal blocks and rhs once the CZs are staged
-  ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
-  if (ctx->N > 0)
-    ICF_TRY_RC(icf_launch_gather_diag(ctx, ctx->tune_diag, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals,
-                                      ctx->d_rhs, s));
-  if (ctx->N > 0)
-    icf_prof_mark(ctx, s, "k_gather_diag", 104LL * ctx->N + diag_in + cz_rec * ctx->n_cz);
+  ICF_CUDA(ctx, cudaEventRecord(e_b, sb));
   // join
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
@@ -1174,10 +1202,13 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
   const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
   if (ctx->n_dyn > 0)
     k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, s>>>(ctx->n_dyn, ctx->d_dynpos, B.vals);
-  if (ctx->n_offd > 0)
-    ICF_TRY_RC(icf_launch_gather_off(ctx, ctx->tune_off, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, s));
-  if (ctx->N > 0)
-    ICF_TRY_RC(icf_launch_gather_diag(ctx, ctx->tune_diag, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs, s));
+  for (const icf_sell *L : {&ctx->sell_off, &ctx->sell_off_cz})
+    if (L->n_units > 0)
+      ICF_TRY_RC(icf_launch_gather_off(ctx, *L, ctx->tune_off, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, s));
+  for (const icf_sell *L : {&ctx->sell_diag, &ctx->sell_diag_cz})
+    if (L->n_units > 0)
+      ICF_TRY_RC(icf_launch_gather_diag(ctx, *L, ctx->tune_diag, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs,
+                                        s));
   if (ctx->n_crs > 0)
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
                                                         ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4);

@@ -739,9 +739,8 @@ const char *icf_gather_variant_name(int kind, int v) {
 int icf_gather_variant_lanes(int v) { return DIAG_VARIANTS[v].lanes; }
 bool icf_gather_variant_natural(int v) { return OFF_VARIANTS[v].natural; }
 
-int icf_launch_gather_off(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc, double mc,
-                          double lam, double mu, double *vals, cudaStream_t s) {
-  const icf_sell &S = ctx->sell_off;
+int icf_launch_gather_off(icf_ctx *ctx, const icf_sell &S, int variant, const double4 *es, const double *cs,
+                          double sc, double mc, double lam, double mu, double *vals, cudaStream_t s) {
   if (S.n_slices == 0) return ICF_OK;
   if (variant < 0 || variant >= N_OFF) variant = 0;
   unsigned grid = icf_blocks(32LL * S.n_slices, 256);
@@ -773,9 +772,8 @@ int icf_launch_gather_off(icf_ctx *ctx, int variant, const double4 *es, const do
   return ICF_OK;
 }
 
-int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc,
-                           double mc, double lam, double mu, double *vals, double *rhs, cudaStream_t s) {
-  const icf_sell &S = ctx->sell_diag;
+int icf_launch_gather_diag(icf_ctx *ctx, const icf_sell &S, int variant, const double4 *es, const double *cs,
+                           double sc, double mc, double lam, double mu, double *vals, double *rhs, cudaStream_t s) {
   if (S.n_slices == 0) return ICF_OK;
   if (variant < 0 || variant >= N_DIAG || DIAG_VARIANTS[variant].lanes != S.lanes) {
     // the lists were built for S.lanes: take the first variant that reads them

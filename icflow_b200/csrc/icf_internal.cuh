@@ -69,7 +69,8 @@ struct icf_sell {
   int lanes = 1;
   bool natural = false;  // units in their own order (no count sort): slices of consecutive units
   int n_units = 0, n_slices = 0, slices_cap = 0;
-  long long n_codes = 0, codes_cap = 0;
+  long long n_codes = 0, codes_cap = 0;  // code slots, padding included
+  long long n_real = 0;                   // contribution codes of the units (no padding)
   int4 *meta = nullptr;
   int2 *unit = nullptr;
   uint32_t *codes = nullptr;
@@ -179,8 +180,13 @@ struct icf_ctx {
   // N per-row diagonal entries, then one per off-diagonal block (one buffer)
   int4 *d_gdesc_diag = nullptr, *d_gdesc_off = nullptr;
   int gdesc_cap = 0;
-  // the gathers' sliced-ELL code lists (built from the descriptors)
-  icf_sell sell_off, sell_diag;
+  // the gathers' sliced-ELL code lists (built from the descriptors).  With
+  // split_cz the units without CZ codes (sell_off / sell_diag) and those with
+  // CZ codes (sell_off_cz / sell_diag_cz) are separate lists, so the first
+  // can be gathered while the CZ kernel still runs; otherwise everything is
+  // in sell_off / sell_diag.
+  icf_sell sell_off, sell_diag, sell_off_cz, sell_diag_cz;
+  bool split_cz = false;
 
   // merged pattern
   int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;
@@ -262,10 +268,10 @@ int icf_gather_variants(int kind);  // kind 0 off-diagonal, 1 diagonal
 const char *icf_gather_variant_name(int kind, int v);
 int icf_gather_variant_lanes(int v);  // lanes per row of diagonal variant v
 bool icf_gather_variant_natural(int v);  // off-diagonal variant v reads natural-order lists
-int icf_launch_gather_off(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc, double mc,
-                          double lam, double mu, double *vals, cudaStream_t s);
-int icf_launch_gather_diag(icf_ctx *ctx, int variant, const double4 *es, const double *cs, double sc,
-                           double mc, double lam, double mu, double *vals, double *rhs, cudaStream_t s);
+int icf_launch_gather_off(icf_ctx *ctx, const icf_sell &S, int variant, const double4 *es, const double *cs,
+                          double sc, double mc, double lam, double mu, double *vals, cudaStream_t s);
+int icf_launch_gather_diag(icf_ctx *ctx, const icf_sell &S, int variant, const double4 *es, const double *cs,
+                           double sc, double mc, double lam, double mu, double *vals, double *rhs, cudaStream_t s);
 // tet kernel variants (icf_assembly.cu)
 int icf_tet_variants();
 const char *icf_tet_variant_name(int v);
@@ -274,6 +280,7 @@ int icf_cz_variants();
 const char *icf_cz_variant_name(int v);
 int icf_launch_cz(icf_ctx *ctx, int variant, const double4 *xc, double *cs, cudaStream_t s);
 // rebuilds the diagonal gather lists for `lanes` lanes per row (icf_pattern.cu)
+int icf_rebuild_lists(icf_ctx *ctx);  // both gathers' lists for the current layout and split
 int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes);
 int icf_rebuild_sell_off(icf_ctx *ctx, bool natural);
 // position map and zeroed contribution staging for the current lists

@@ -207,8 +207,8 @@ __global__ void k_sell_key(int n, int wl, int lanes, const int4 *__restrict__ de
 
 // one warp per slice: iteration counts (the slice's maxima) and unit table
 __global__ void k_sell_count(int n, int n_slices, int lanes, const int *__restrict__ perm,
-                             const int4 *__restrict__ desc, int with_row, int4 *__restrict__ meta,
-                             int *__restrict__ cnt, int2 *__restrict__ unit) {
+                             const int4 *__restrict__ desc, int with_row, const int *__restrict__ row_of,
+                             int4 *__restrict__ meta, int *__restrict__ cnt, int2 *__restrict__ unit) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= n_slices) return;
   const int per = 32 / lanes;
@@ -223,7 +223,7 @@ __global__ void k_sell_count(int n, int n_slices, int lanes, const int *__restri
       mt = (d.z - d.y + lanes - 1) / lanes;
       mc = (d.w - d.z + lanes - 1) / lanes;
     }
-    un = make_int2(d.x, with_row ? i : -1);
+    un = make_int2(d.x, with_row ? (row_of ? row_of[i] : i) : -1);
   }
   for (int o = 16; o > 0; o >>= 1) {
     mt = max(mt, __shfl_xor_sync(0xffffffffu, mt, o));
@@ -541,13 +541,26 @@ int icf_build_static_pattern(icf_ctx *ctx) {
   return ICF_OK;
 }
 
+// total contribution codes of n descriptors
+__global__ void k_real_codes(int n, const int4 *__restrict__ desc, unsigned long long *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long c = 0;
+  if (i < n) {
+    const int4 d = desc[i];
+    if (d.x >= 0) c = (unsigned long long)(d.w - d.y);
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
 // Builds the sliced-ELL lists of a gather from its descriptors (n units).
 static int build_sell(icf_ctx *ctx, const int4 *desc, int n, int wl, bool with_row, icf_sell *S,
-                      cudaStream_t s) {
+                      cudaStream_t s, const int *row_of = nullptr) {
   const int per = 32 / S->lanes;
   S->n_units = n;
   S->n_slices = (n + per - 1) / per;
   S->n_codes = 0;
+  S->n_real = 0;
   if (n == 0) return ICF_OK;
   const int ns = S->n_slices;
   if (ns > S->slices_cap || !S->meta) {
@@ -580,16 +593,24 @@ static int build_sell(icf_ctx *ctx, const int4 *desc, int n, int wl, bool with_r
     ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, i0, perm, n, 0, end_bit, s));
   }
   ICF_CUDA(ctx, cudaMemsetAsync(S->unit, 0xff, sizeof(int2) * (size_t)ns * per, s));
-  k_sell_count<<<icf_blocks(32LL * ns, 256), 256, 0, s>>>(n, ns, S->lanes, perm, desc, with_row ? 1 : 0,
+  k_sell_count<<<icf_blocks(32LL * ns, 256), 256, 0, s>>>(n, ns, S->lanes, perm, desc, with_row ? 1 : 0, row_of,
                                                          S->meta, cnt, S->unit);
   ICF_CUDA(ctx, cudaMemsetAsync(cnt + ns, 0, sizeof(int), s));
   tb = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, ns + 1, s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, cnt, off, ns + 1, s));
+  unsigned long long *d_real;
+  ICF_CUDA(ctx, cudaMallocAsync(&d_real, sizeof(unsigned long long), s));
+  ICF_CUDA(ctx, cudaMemsetAsync(d_real, 0, sizeof(unsigned long long), s));
+  k_real_codes<<<icf_blocks(n, 256), 256, 0, s>>>(n, desc, d_real);
   int total = 0;
+  unsigned long long real = 0;
   ICF_CUDA(ctx, cudaMemcpyAsync(&total, off + ns, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(&real, d_real, sizeof(real), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  ICF_CUDA(ctx, cudaFreeAsync(d_real, s));
+  S->n_real = (long long)real;
   if (total < 0) return icf_fail(ctx, ICF_ERR_SIZE, "gather code list exceeds 2^31 entries");
   if (total > S->codes_cap || !S->codes) {
     cudaFree(S->codes);
@@ -608,6 +629,68 @@ static int build_sell(icf_ctx *ctx, const int4 *desc, int n, int wl, bool with_r
   ICF_CUDA(ctx, cudaFreeAsync(perm, s));
   ICF_CUDA(ctx, cudaFreeAsync(cnt, s));
   ICF_CUDA(ctx, cudaFreeAsync(off, s));
+  return ICF_OK;
+}
+
+// 1 for a descriptor with CZ codes
+__global__ void k_has_cz(int n, const int4 *__restrict__ desc, int *__restrict__ flag, int *__restrict__ noflag,
+                         int *__restrict__ idx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 d = desc[i];
+  const int f = (d.x >= 0 && d.w > d.z) ? 1 : 0;
+  flag[i] = f;
+  noflag[i] = 1 - f;
+  idx[i] = i;
+}
+
+// The gather lists of the current descriptors.  With split_cz (and the
+// per-tet record layout) the units split into those without CZ codes
+// (sell_off / sell_diag) and those with (sell_off_cz / sell_diag_cz); the
+// diagonal lists carry each unit's row explicitly.
+static int build_lists(icf_ctx *ctx, bool off, bool diag) {
+  cudaStream_t s = ctx->stream;
+  const bool split = ctx->split_cz && ctx->layout == ICF_LAYOUT_RECORDS && ctx->n_cz > 0;
+  for (int k = 0; k < 2; k++) {
+    if ((k == 0 && !off) || (k == 1 && !diag)) continue;
+    const int4 *desc = k == 0 ? ctx->d_gdesc_off : ctx->d_gdesc_diag;
+    const int n = k == 0 ? ctx->n_offd : ctx->N;
+    icf_sell *A = k == 0 ? &ctx->sell_off : &ctx->sell_diag;
+    icf_sell *B = k == 0 ? &ctx->sell_off_cz : &ctx->sell_diag_cz;
+    const int wl = k == 0 ? 12 : (A->lanes >= 4 ? 10 : 11);
+    if (!split || n == 0) {
+      if (build_sell(ctx, desc, n, wl, k == 1, A, s)) return ICF_ERR_CUDA;
+      B->n_units = B->n_slices = 0;
+      B->n_codes = 0;
+      continue;
+    }
+    int *flag, *noflag, *idx, *ia, *ib, *d_n;
+    int4 *da, *db;
+    ICF_CUDA(ctx, cudaMallocAsync(&flag, sizeof(int) * (size_t)n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&noflag, sizeof(int) * (size_t)n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&idx, sizeof(int) * (size_t)n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&ia, sizeof(int) * (size_t)n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&ib, sizeof(int) * (size_t)n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&da, sizeof(int4) * (size_t)n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&db, sizeof(int4) * (size_t)n, s));
+    ICF_CUDA(ctx, cudaMallocAsync(&d_n, sizeof(int) * 4, s));
+    k_has_cz<<<icf_blocks(n, 256), 256, 0, s>>>(n, desc, flag, noflag, idx);
+    size_t tb = 0;
+    cub::DeviceSelect::Flagged(nullptr, tb, desc, noflag, da, d_n, n, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceSelect::Flagged(ctx->d_tmp, tb, desc, noflag, da, d_n, n, s));
+    ICF_CUDA(ctx, cub::DeviceSelect::Flagged(ctx->d_tmp, tb, desc, flag, db, d_n + 1, n, s));
+    ICF_CUDA(ctx, cub::DeviceSelect::Flagged(ctx->d_tmp, tb, idx, noflag, ia, d_n + 2, n, s));
+    ICF_CUDA(ctx, cub::DeviceSelect::Flagged(ctx->d_tmp, tb, idx, flag, ib, d_n + 3, n, s));
+    int h_n[4] = {0, 0, 0, 0};
+    ICF_CUDA(ctx, cudaMemcpyAsync(h_n, d_n, sizeof(h_n), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    if (build_sell(ctx, da, h_n[0], wl, k == 1, A, s, k == 1 ? ia : nullptr)) return ICF_ERR_CUDA;
+    if (build_sell(ctx, db, h_n[1], wl, k == 1, B, s, k == 1 ? ib : nullptr)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    void *tmp[] = {flag, noflag, idx, ia, ib, da, db, d_n};
+    for (void *q : tmp) ICF_CUDA(ctx, cudaFreeAsync(q, s));
+  }
   return ICF_OK;
 }
 
@@ -720,11 +803,10 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
   if (ctx->n_offd > 0)
     k_desc<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_offd, ctx->d_rc_off,
                                                        ctx->d_rc_mid, ctx->d_s2m, ident, ctx->d_gdesc_off);
-  ctx->sell_off.lanes = 1;
-  ctx->sell_off.natural = icf_gather_variant_natural(ctx->tune_off);
-  ctx->sell_diag.lanes = icf_gather_variant_lanes(ctx->tune_diag);
-  if (build_sell(ctx, ctx->d_gdesc_off, ctx->n_offd, 12, false, &ctx->sell_off, s)) return ICF_ERR_CUDA;
-  if (build_sell(ctx, ctx->d_gdesc_diag, N, 10, true, &ctx->sell_diag, s)) return ICF_ERR_CUDA;
+  ctx->sell_off.lanes = ctx->sell_off_cz.lanes = 1;
+  ctx->sell_off.natural = ctx->sell_off_cz.natural = icf_gather_variant_natural(ctx->tune_off);
+  ctx->sell_diag.lanes = ctx->sell_diag_cz.lanes = icf_gather_variant_lanes(ctx->tune_diag);
+  if (build_lists(ctx, true, true)) return ICF_ERR_CUDA;
   if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
   if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
   if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
@@ -831,11 +913,18 @@ int icf_launch_pcsr(icf_ctx *ctx, int kind, int *d_out) {
   return ICF_OK;
 }
 
+int icf_rebuild_lists(icf_ctx *ctx) {
+  if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
+  if (build_lists(ctx, true, true)) return ICF_ERR_CUDA;
+  if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
+  ctx->version++;
+  return ICF_OK;
+}
+
 int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes) {
   if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
-  ctx->sell_diag.lanes = lanes;
-  const int wl = lanes >= 4 ? 10 : 11;
-  if (build_sell(ctx, ctx->d_gdesc_diag, ctx->N, wl, true, &ctx->sell_diag, ctx->stream)) return ICF_ERR_CUDA;
+  ctx->sell_diag.lanes = ctx->sell_diag_cz.lanes = lanes;
+  if (build_lists(ctx, false, true)) return ICF_ERR_CUDA;
   if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ICF_OK;
@@ -843,8 +932,8 @@ int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes) {
 
 int icf_rebuild_sell_off(icf_ctx *ctx, bool natural) {
   if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
-  ctx->sell_off.natural = natural;
-  if (build_sell(ctx, ctx->d_gdesc_off, ctx->n_offd, 12, false, &ctx->sell_off, ctx->stream)) return ICF_ERR_CUDA;
+  ctx->sell_off.natural = ctx->sell_off_cz.natural = natural;
+  if (build_lists(ctx, true, false)) return ICF_ERR_CUDA;
   if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ICF_OK;

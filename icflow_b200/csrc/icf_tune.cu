@@ -60,14 +60,17 @@ int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant) {
                           : kind == 1 ? icf_gather_variants(0)
                           : kind == 2 ? icf_gather_variants(1)
                           : kind == 3 ? 2
+                          : kind == 5 ? 2
                                       : icf_cz_variants();
-  if (kind < 0 || kind > 4 || variant < 0 || variant >= n)
-    return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..4 and a variant index of that kind");
-  if (kind == 3) {
-    const bool build = ctx->layout != variant && variant == ICF_LAYOUT_CONTRIB;
-    ctx->layout = variant;
-    if (build && ctx->have_structure) {
-      ICF_TRY_RC(icf_build_contrib(ctx));
+  if (kind < 0 || kind > 5 || variant < 0 || variant >= n)
+    return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..5 and a variant index of that kind");
+  if (kind == 3 || kind == 5) {
+    // the staging layout and the split decide which lists exist
+    const bool changed = kind == 3 ? ctx->layout != variant : ctx->split_cz != (variant == 1);
+    if (kind == 3) ctx->layout = variant;
+    else ctx->split_cz = variant == 1;
+    if (changed && ctx->have_structure) {
+      ICF_TRY_RC(icf_rebuild_lists(ctx));
       ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     }
   }
@@ -101,6 +104,7 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
     ctx->version++;  // re-capture with the candidate's kernels
     return time_launches(ctx, t, reps, [&] { return icf_launch_assembly(ctx, h); }, ms);
   };
+  int split = ctx->split_cz ? 1 : 0;
   struct kind_desc {
     const char *name;
     int kind, n;
@@ -108,12 +112,14 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
   };
   const kind_desc kinds[] = {
       {"layout", 3, 2, &ctx->layout},
+      {"split", 5, ctx->n_cz > 0 ? 2 : 0, &split},
       {"k_tet_unit", 0, ctx->n_elem > 0 ? icf_tet_variants() : 0, &ctx->tune_tet},
       {"k_cz_gp", 4, ctx->n_cz > 0 ? icf_cz_variants() : 0, &ctx->tune_cz},
-      {"k_gather_off", 1, ctx->sell_off.n_slices > 0 ? icf_gather_variants(0) : 0, &ctx->tune_off},
+      {"k_gather_off", 1, ctx->n_offd > 0 ? icf_gather_variants(0) : 0, &ctx->tune_off},
       {"k_gather_diag", 2, ctx->N > 0 ? icf_gather_variants(1) : 0, &ctx->tune_diag},
   };
   const char *layout_names[2] = {"per-tet records", "per-contribution stream"};
+  const char *split_names[2] = {"one list per gather", "CZ-free units apart"};
   for (const kind_desc &k : kinds) {
     if (k.n < 2) continue;
     double best = 1e30;
@@ -123,6 +129,7 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
       double ms = 0;
       ICF_TRY_RC(assembly_ms(&ms));
       const char *vn = k.kind == 3 ? layout_names[v]
+                       : k.kind == 5 ? split_names[v]
                        : k.kind == 0 ? icf_tet_variant_name(v)
                        : k.kind == 4 ? icf_cz_variant_name(v)
                                      : icf_gather_variant_name(k.kind == 1 ? 0 : 1, v);
@@ -131,6 +138,7 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
     }
     ICF_TRY_RC(icf_set_variant_impl(ctx, k.kind, bv));
     const char *vn = k.kind == 3 ? layout_names[bv]
+                     : k.kind == 5 ? split_names[bv]
                      : k.kind == 0 ? icf_tet_variant_name(bv)
                      : k.kind == 4 ? icf_cz_variant_name(bv)
                                    : icf_gather_variant_name(k.kind == 1 ? 0 : 1, bv);

@@ -222,7 +222,10 @@ int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out
  * 1 off-diagonal gather, 2 diagonal gather, 4 CZ kernel) or the staging layout (kind 3:
  * 0 per-tet records gathered through contribution codes, the default; 1
  * per-contribution records written at their gather positions and read as
- * streams).  The tuner also times whole assemblies with each layout first. */
+ * streams) or the list split (kind 5, per-tet records only: 0, the default,
+ * one list per gather; 1 keeps the units without CZ contributions in lists of
+ * their own that run beside the CZ kernel).  The tuner also times whole
+ * assemblies with each layout and split first. */
 #define ICF_MAX_TUNE 32
 typedef struct icf_tune_report {
   int n;                          /* candidates timed */

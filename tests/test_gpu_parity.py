@@ -269,7 +269,7 @@ def test_every_launch_variant_and_autotune(O):
     compare(ref, o)
     lib = _lib.load()
     counts = {}
-    for kind in (3, 0, 1, 2, 4):
+    for kind in (3, 5, 0, 1, 2, 4):
         v = 0
         while lib.icf_set_variant(gf.ctx, kind, v) == 0:
             gf.AssembleElemsAndCZs(H)
@@ -280,20 +280,33 @@ def test_every_launch_variant_and_autotune(O):
         counts[kind] = v
         _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, 0))
     assert all(n >= 2 for n in counts.values()), counts
-    # the other layout with every gather variant
+    # the per-tet record layout, split and single lists, with every gather variant
     _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 3, 0))
-    for kind in (1, 2):
-        for v in range(counts[kind]):
-            _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, v))
-            gf.AssembleElemsAndCZs(H)
-            vals, rhs = gf.TransferLinearSystemToHost()
-            assert rowwise_rel(o["rows"], o["vals"], vals.reshape(-1, 3, 3)) <= FP64_TOL, ("records", kind, v)
-            assert vec_rel(o["rhs"], rhs) <= FP64_TOL
-        _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, 0))
+    for split in (0, 1):
+        _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 5, split))
+        for kind in (1, 2):
+            for v in range(counts[kind]):
+                _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, v))
+                gf.AssembleElemsAndCZs(H)
+                vals, rhs = gf.TransferLinearSystemToHost()
+                assert rowwise_rel(o["rows"], o["vals"], vals.reshape(-1, 3, 3)) <= FP64_TOL, ("records", split, kind, v)
+                assert vec_rel(o["rhs"], rhs) <= FP64_TOL
+            _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, kind, 0))
+    # the split lists give the same bits as the single ones
+    _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 5, 0))
+    gf.AssembleElemsAndCZs(H)
+    v0, r0 = gf.TransferLinearSystemToHost()
+    v0, r0 = v0.copy(), r0.copy()
+    _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 5, 1))
+    gf.AssembleElemsAndCZs(H)
+    v1, r1 = gf.TransferLinearSystemToHost()
+    assert np.array_equal(v0, v1) and np.array_equal(r0, r1)
+    names = {k["name"] for k in gf.ProfileAssembly(H, reps=2)}
+    assert {"k_gather_off", "k_gather_off_cz", "k_gather_diag", "k_gather_diag_cz"} <= names
     _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 3, 1))
     rep = gf.Autotune(H, reps=3)
     kinds = {r["kernel"] for r in rep}
-    assert kinds == {"layout", "k_tet_unit", "k_cz_gp", "k_gather_off", "k_gather_diag"}
+    assert kinds == {"layout", "split", "k_tet_unit", "k_cz_gp", "k_gather_off", "k_gather_diag"}
     assert len(rep) == sum(counts.values())
     for k in kinds:
         assert sum(r["chosen"] for r in rep if r["kernel"] == k) == 1
