@@ -24,7 +24,8 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # without fused multiply-add so that every operation rounds on its own.
 NO_FMA = {"icf_contact.cu"}
 SOURCES = ["icf_api.cu", "icf_assembly.cu", "icf_pattern.cu", "icf_contact.cu", "icf_contact_deriv.cu",
-           "icf_noalloc.cu", "icf_gather.cu", "icf_tune.cu", "icf_solve.cu", "icf_broad.cu", "icf_mlp.cu"]
+           "icf_noalloc.cu", "icf_gather.cu", "icf_tune.cu", "icf_solve.cu", "icf_broad.cu", "icf_mlp.cu",
+           "icf_tile.cu"]
 
 
 def nvcc() -> str:

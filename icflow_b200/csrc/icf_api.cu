@@ -193,6 +193,7 @@ int icf_create(int device, icf_ctx **out) {
 
 static void free_all(icf_ctx *c) {
   icf_free_solver(c);
+  icf_free_tiles(c);
   void *ptrs[] = {c->d_elem, c->d_cz, c->d_alt, c->d_selem, c->d_adj_off, c->d_adj, c->d_faces,
                   c->d_x0, c->d_xc, c->d_va, c->d_u, c->d_v, c->d_a, c->d_du, c->d_un, c->d_h3,
                   c->d_czs, c->d_czfail, c->d_cztent, c->d_czflags, c->d_czavg, c->d_czprm,
@@ -573,6 +574,7 @@ int icf_create_structure(icf_ctx *ctx, int *N, int *nnz) {
   if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
   if (!ctx->d_skeys) ICF_TRY(icf_build_static_pattern(ctx));
   ICF_TRY(icf_build_merged_pattern(ctx));
+  if (ctx->gather_tiles && !ctx->tiles.built) ICF_TRY(icf_build_tiles(ctx));
   ctx->have_structure = true;
   ctx->struct_gen++;
   ctx->version++;

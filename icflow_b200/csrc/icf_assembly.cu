@@ -984,7 +984,15 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     icf_prof_mark(ctx, q, name, list_bytes(L, 104, diag_rec, codes_diag, cz));
     return ICF_OK;
   };
-  if (OB.n_units > 0 || DB.n_units > 0) {
+  if (icf_tiles_active(ctx)) {
+    // one tiled gather for every block, once the tets and the CZs are staged;
+    // algorithmic bytes: units, codes, the tet records and the CZ staging once
+    const icf_tiles &T = ctx->tiles;
+    ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
+    ICF_TRY_RC(icf_launch_gather_tile(ctx, ctx->d_es, ctx->d_cs, sc, mc, P.lam, P.mu, ctx->d_vals, ctx->d_rhs, s));
+    icf_prof_mark(ctx, s, "k_gather_tile",
+                  80 * T.n_off_units + 104 * T.n_diag_units + 4 * T.n_real + diag_rec + cz_rec * ctx->n_cz);
+  } else if (OB.n_units > 0 || DB.n_units > 0) {
     // split lists: the units without CZ codes run as soon as the tets are
     // staged, beside the CZ kernel (off-diagonal on aux1, diagonal on main);
     // the units with CZ codes wait for the CZs (off-diagonal on aux0,
@@ -1202,13 +1210,17 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
   const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
   if (ctx->n_dyn > 0)
     k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, s>>>(ctx->n_dyn, ctx->d_dynpos, B.vals);
-  for (const icf_sell *L : {&ctx->sell_off, &ctx->sell_off_cz})
-    if (L->n_units > 0)
-      ICF_TRY_RC(icf_launch_gather_off(ctx, *L, ctx->tune_off, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, s));
-  for (const icf_sell *L : {&ctx->sell_diag, &ctx->sell_diag_cz})
-    if (L->n_units > 0)
-      ICF_TRY_RC(icf_launch_gather_diag(ctx, *L, ctx->tune_diag, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs,
-                                        s));
+  if (icf_tiles_active(ctx)) {
+    ICF_TRY_RC(icf_launch_gather_tile(ctx, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs, s));
+  } else {
+    for (const icf_sell *L : {&ctx->sell_off, &ctx->sell_off_cz})
+      if (L->n_units > 0)
+        ICF_TRY_RC(icf_launch_gather_off(ctx, *L, ctx->tune_off, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, s));
+    for (const icf_sell *L : {&ctx->sell_diag, &ctx->sell_diag_cz})
+      if (L->n_units > 0)
+        ICF_TRY_RC(icf_launch_gather_diag(ctx, *L, ctx->tune_diag, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals,
+                                          B.rhs, s));
+  }
   if (ctx->n_crs > 0)
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
                                                         ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4);

@@ -22,6 +22,10 @@
 
 namespace {
 
+#ifndef CZ_UNROLL
+#define CZ_UNROLL 2  // CZ codes per group in the gathers
+#endif
+
 __device__ __forceinline__ int sym_pair(int i, int j) {
   // (0,0)0 (0,1)1 (0,2)2 (1,1)3 (1,2)4 (2,2)5
   const int lo = i < j ? i : j, hi = i < j ? j : i;
@@ -50,6 +54,9 @@ struct fp64 {
   const double4 *es;  // tet records: {h_a, V} at 8e + a, {rhs_a, 0} at 8e + 4 + a
   const double *cs;   // CZ records: Kt (6 x 6) at 48c, rt[3][3] at 48c + 36
   __device__ __forceinline__ rec hrec(uint32_t e, uint32_t a) const { return es[8 * (size_t)e + a]; }
+  __device__ __forceinline__ const char *hsrc(uint32_t e) const {  // the 4 h records of tet e
+    return reinterpret_cast<const char *>(es + 8 * (size_t)e);
+  }
   __device__ __forceinline__ double4 rrec(uint32_t e, uint32_t a) const { return es[8 * (size_t)e + 4 + a]; }
   __device__ __forceinline__ void kt(uint32_t c, int pair, real k[6]) const {
     const double2 *K2 = reinterpret_cast<const double2 *>(cs + (size_t)c * ICF_CZ_STAGE + 6 * pair);
@@ -66,6 +73,9 @@ struct fp32mixed {
   const float *cs32;   // Kt at 36c
   const double *csr;   // rt at 12c
   __device__ __forceinline__ rec hrec(uint32_t e, uint32_t a) const { return es32[4 * (size_t)e + a]; }
+  __device__ __forceinline__ const char *hsrc(uint32_t e) const {
+    return reinterpret_cast<const char *>(es32 + 4 * (size_t)e);
+  }
   __device__ __forceinline__ double4 rrec(uint32_t e, uint32_t a) const { return esr[4 * (size_t)e + a]; }
   __device__ __forceinline__ void kt(uint32_t c, int pair, real k[6]) const {
     const float2 *K2 = reinterpret_cast<const float2 *>(cs32 + (size_t)c * 36 + 6 * pair);
@@ -122,6 +132,59 @@ __device__ __forceinline__ void add_cz(const S &st, uint32_t code, typename S::r
   }
 }
 
+// The CZ codes k0 .. k1 - 1 of a lane (stride 32), UC at a time: first the
+// codes, then all their staging loads, then the terms in code order (the same
+// terms and order as add_cz, code by code).
+template <typename S, int UC>
+__device__ __forceinline__ void cz_codes(const S &st, const uint32_t *c, int k0, int k1, typename S::real b[9],
+                                         double *r) {
+  typedef typename S::real R;
+  for (int k = k0; k < k1; k += UC) {
+    uint32_t cc[UC];
+#pragma unroll
+    for (int j = 0; j < UC; j++) cc[j] = (k + j < k1) ? __ldg(c + 32 * (k + j)) : ICF_CODE_PAD;
+    R kk[UC][6], sg[UC];
+    double rt[UC][3], sa[UC];
+#pragma unroll
+    for (int j = 0; j < UC; j++) {
+      sg[j] = R(0);
+      sa[j] = 0.0;
+#pragma unroll
+      for (int q = 0; q < 6; q++) kk[j][q] = R(0);
+      rt[j][0] = rt[j][1] = rt[j][2] = 0.0;
+      if (cc[j] != ICF_CODE_PAD) {
+        uint32_t cz;
+        int ia, ib;
+        bool same, a_lo;
+        cz_code(cc[j], cz, ia, ib, same, a_lo);
+        st.kt(cz, sym_pair(ia, ib), kk[j]);
+        sg[j] = same ? R(1) : R(-1);
+        if (r != nullptr) {
+          const double *p = st.rt(cz) + 3 * ia;
+          rt[j][0] = __ldg(p);
+          rt[j][1] = __ldg(p + 1);
+          rt[j][2] = __ldg(p + 2);
+          sa[j] = a_lo ? -1.0 : 1.0;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < UC; j++) {
+      if (cc[j] == ICF_CODE_PAD) continue;
+      const R g = sg[j];
+      const R *K = kk[j];
+      b[0] += g * K[0]; b[1] += g * K[1]; b[2] += g * K[2];
+      b[3] += g * K[1]; b[4] += g * K[3]; b[5] += g * K[4];
+      b[6] += g * K[2]; b[7] += g * K[4]; b[8] += g * K[5];
+      if (r != nullptr) {
+        r[0] += sa[j] * rt[j][0];
+        r[1] += sa[j] * rt[j][1];
+        r[2] += sa[j] * rt[j][2];
+      }
+    }
+  }
+}
+
 template <typename V4>
 __device__ __forceinline__ V4 zero4();
 template <>
@@ -161,10 +224,7 @@ __global__ void __launch_bounds__(256, MINB)
 #pragma unroll
     for (int j = 0; j < U; j++) acc_tet<R, V4>(A[j], B[j], false, g, b);
   }
-  for (int k = m.y; k < m.y + m.z; k++) {
-    const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
-  }
+  cz_codes<S, CZ_UNROLL>(st, c, m.y, m.y + m.z, b, nullptr);
   const int2 u = unit[32 * w + lane];
   if (u.x < 0) return;
   double *o = vals + 9 * (size_t)u.x;
@@ -214,10 +274,7 @@ __global__ void __launch_bounds__(256, MINB)
       r[2] += Rr[j].z;
     }
   }
-  for (int k = m.y; k < m.y + m.z; k++) {
-    const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, r);
-  }
+  cz_codes<S, 1>(st, c, m.y, m.y + m.z, b, r);
 #pragma unroll
   for (int o = 1; o < L; o <<= 1) {
 #pragma unroll
@@ -331,10 +388,7 @@ __global__ void __launch_bounds__(256, MINB)
 #pragma unroll
     for (int j = 0; j < U; j++) acc_tet<R, V4>(A[j], B[j], false, g, b);
   }
-  for (int k = m.y; k < m.y + m.z; k++) {
-    const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
-  }
+  cz_codes<S, CZ_UNROLL>(st, c, m.y, m.y + m.z, b, nullptr);
 #pragma unroll
   for (int q = 0; q < 9; q++) sb[wl][9 * lane + q] = (double)b[q];
   __syncwarp();
@@ -402,10 +456,7 @@ __global__ void __launch_bounds__(256, MINB)
         acc_tet<R, V4>(st.hrec(e, a), st.hrec(e, bb), false, g, b);
       }
     }
-    for (int k = m.y; k < m.y + m.z; k++) {
-      const uint32_t c0 = __ldg(c + 32 * k);
-      if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
-    }
+    cz_codes<S, CZ_UNROLL>(st, c, m.y, m.y + m.z, b, nullptr);
     if (u.x >= 0) {
       double *o = vals + 9 * (size_t)u.x;
 #pragma unroll
@@ -484,10 +535,7 @@ __global__ void __launch_bounds__(256, MINB)
         r[2] += R1.z;
       }
     }
-    for (int k = m.y; k < m.y + m.z; k++) {
-      const uint32_t c0 = __ldg(c + 32 * k);
-      if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, r);
-    }
+    cz_codes<S, 1>(st, c, m.y, m.y + m.z, b, r);
 #pragma unroll
     for (int o = 1; o < L; o <<= 1) {
 #pragma unroll
@@ -581,10 +629,7 @@ __global__ void __launch_bounds__(256, MINB)
     for (int j = 0; j < U; j++) acc_tet<R, V4>(A[j], B[j], false, g, b);
   }
   const uint32_t *c = codes + m.x + lane;
-  for (int k = m.y; k < m.y + m.z; k++) {
-    const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, nullptr);
-  }
+  cz_codes<S, CZ_UNROLL>(st, c, m.y, m.y + m.z, b, nullptr);
   const int2 u = unit[32 * w + lane];
   if (u.x < 0) return;
   double *o = vals + 9 * (size_t)u.x;
@@ -624,10 +669,7 @@ __global__ void __launch_bounds__(256, MINB)
     }
   }
   const uint32_t *c = codes + m.x + lane;
-  for (int k = m.y; k < m.y + m.z; k++) {
-    const uint32_t c0 = __ldg(c + 32 * k);
-    if (c0 != ICF_CODE_PAD) add_cz<S>(st, c0, b, r);
-  }
+  cz_codes<S, 1>(st, c, m.y, m.y + m.z, b, r);
 #pragma unroll
   for (int o = 1; o < L; o <<= 1) {
 #pragma unroll
@@ -689,6 +731,128 @@ struct diag_variant {
   int persistent_minb;
 };
 
+// ---- row tiles (icf_tiles): every block of a set of rows per CTA ---------------
+__device__ __forceinline__ void cp16(void *smem, const void *gmem) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The CTA first copies, with asynchronous 16 B copies, the tile's slice
+// metadata, units and 16-bit tet codes (contiguous ranges) and the {h_a, V}
+// records of its tets (one 128 B / 64 B line per tet) into shared memory.
+// Its warps then take the tile's slices in turn, one lane per block.  A tet
+// code names the tet's position in the tile; CZ codes are read from global
+// memory.  Diagonal blocks (unit row >= 0) also sum their vertices' rhs
+// records and the CZ rt terms.  Per block, the sum runs over the codes in the
+// order of the static code list, as in the list gathers.
+#define TILE_THREADS 256
+template <typename S, int MINB, int U>
+__global__ void __launch_bounds__(TILE_THREADS, MINB)
+    k_gather_tile(const int4 *__restrict__ tiles, const int2 *__restrict__ trange, const int *__restrict__ ttet,
+                  const int4 *__restrict__ meta, const int2 *__restrict__ unit, const uint16_t *__restrict__ tcodes,
+                  const uint32_t *__restrict__ czcodes, S st, gargs<typename S::real> g,
+                  double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite) {
+  typedef typename S::real R;
+  typedef typename S::rec V4;
+  constexpr int CH = 4 * (int)sizeof(V4) / 16;  // 16 B chunks per tet
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  __shared__ int next_slice;
+  const int4 t = tiles[blockIdx.x];
+  const int2 tr = trange[blockIdx.x];
+  V4 *sh = reinterpret_cast<V4 *>(tile_smem);
+  int4 *smeta = reinterpret_cast<int4 *>(sh + 4 * t.y);
+  int2 *sunit = reinterpret_cast<int2 *>(smeta + t.w);
+  uint16_t *scode = reinterpret_cast<uint16_t *>(sunit + 32 * t.w);
+  int *gid = reinterpret_cast<int *>(scode + tr.y);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (int q = tid; q < t.w; q += nth) cp16(smeta + q, meta + t.z + q);
+  for (int q = tid; q < 16 * t.w; q += nth) cp16(sunit + 2 * q, unit + 32 * (size_t)t.z + 2 * q);
+  for (int q = tid; q < tr.y / 8; q += nth) cp16(scode + 8 * q, tcodes + tr.x + 8 * q);
+  {
+    // thread tid copies chunk tid % CH of tets tid / CH, tid / CH + nth / CH, ...
+    const int ch = tid % CH, step = nth / CH;
+    int k = tid / CH;
+    for (; k + 3 * step < t.y; k += 4 * step) {
+      int e[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) e[j] = __ldg(ttet + t.x + k + j * step);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        cp16(reinterpret_cast<char *>(sh + 4 * (k + j * step)) + 16 * ch, st.hsrc((uint32_t)e[j]) + 16 * ch);
+        if (ch == 0) gid[k + j * step] = e[j];
+      }
+    }
+    for (; k < t.y; k += step) {
+      const int e = __ldg(ttet + t.x + k);
+      cp16(reinterpret_cast<char *>(sh + 4 * k) + 16 * ch, st.hsrc((uint32_t)e) + 16 * ch);
+      if (ch == 0) gid[k] = e;
+    }
+  }
+  if (tid == 0) next_slice = nth >> 5;
+  cp_wait_all();
+  __syncthreads();
+  const int lane = tid & 31;
+  bool bad = false;
+  int w = tid >> 5;
+  while (w < t.w) {
+    const int4 m = smeta[w];
+    const int2 u = sunit[32 * w + lane];
+    const bool dg = u.y >= 0;
+    const uint16_t *c = scode + (m.x - tr.x) + lane;
+    R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double r[3] = {0, 0, 0};
+    for (int k = 0; k < m.y; k += U) {
+      uint32_t cc[U];
+#pragma unroll
+      for (int j = 0; j < U; j++) cc[j] = (k + j < m.y) ? (uint32_t)c[32 * (k + j)] : 0xFFFFu;
+      // the rhs records (global memory) of the group's diagonal codes are
+      // requested before any Hessian term is formed from shared memory
+      double qx[U], qy[U], qz[U];
+#pragma unroll
+      for (int j = 0; j < U; j++) {
+        qx[j] = qy[j] = qz[j] = 0.0;
+        const uint32_t lt = cc[j] >> 4, a = (cc[j] >> 2) & 3u, bb = cc[j] & 3u;
+        if (cc[j] != 0xFFFFu && a == bb && lt < (uint32_t)t.y) {
+          const double4 q = st.rrec((uint32_t)gid[lt], a);
+          qx[j] = q.x;
+          qy[j] = q.y;
+          qz[j] = q.z;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < U; j++) {
+        const uint32_t lt = cc[j] >> 4, a = (cc[j] >> 2) & 3u, bb = cc[j] & 3u;
+        if (cc[j] == 0xFFFFu || lt >= (uint32_t)t.y) continue;  // padding (the builder checks every code)
+        acc_tet<R, V4>(sh[4 * lt + a], sh[4 * lt + bb], a == bb, g, b);
+        r[0] += qx[j];
+        r[1] += qy[j];
+        r[2] += qz[j];
+      }
+    }
+    cz_codes<S, CZ_UNROLL>(st, czcodes + m.w + lane, 0, m.z, b, dg ? r : nullptr);
+    if (u.x >= 0) {
+      double *o = vals + 9 * (size_t)u.x;
+#pragma unroll
+      for (int q = 0; q < 9; q++) {
+        o[q] = (double)b[q];
+        bad |= !isfinite((double)b[q]);
+      }
+    }
+    if (dg) {
+      rhs[3 * (size_t)u.y + 0] = r[0];
+      rhs[3 * (size_t)u.y + 1] = r[1];
+      rhs[3 * (size_t)u.y + 2] = r[2];
+      bad |= !(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]));
+    }
+    int nw = 0;
+    if (lane == 0) nw = atomicAdd(&next_slice, 1);
+    w = __shfl_sync(0xffffffffu, nw, 0);
+  }
+  // no barrier at the end: each warp reports on its own
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
+}
+
 #define OFFV(MB, U)                                                                                   \
   {"reg minb" #MB " u" #U, k_gather_off<fp64, MB, U>, k_gather_off<fp32mixed, MB, U>,                \
    k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, 0, false}
@@ -731,6 +895,38 @@ fp32mixed mixed_views(const icf_ctx *ctx, const double4 *es, const double *cs) {
 }
 
 }  // namespace
+
+// Shared memory of the tiled gather for the largest tile (outside any capture).
+int icf_gather_tile_setup(icf_ctx *ctx) {
+  const icf_tiles &T = ctx->tiles;
+  ICF_CUDA(ctx, cudaFuncSetAttribute(k_gather_tile<fp32mixed, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)T.smem32));
+  ICF_CUDA(ctx, cudaFuncSetAttribute(k_gather_tile<fp64, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)T.smem64));
+  return ICF_OK;
+}
+
+int icf_launch_gather_tile(icf_ctx *ctx, const double4 *es, const double *cs, double sc, double mc, double lam,
+                           double mu, double *vals, double *rhs, cudaStream_t s) {
+  const icf_tiles &T = ctx->tiles;
+  if (T.n_tiles == 0) return ICF_OK;
+  if (ctx->precision == ICF_FP32_MIXED) {
+    const gargs<float> g{(float)sc, (float)mc, (float)lam, (float)mu};
+    k_gather_tile<fp32mixed, 4, 2><<<T.n_tiles, TILE_THREADS, T.smem32, s>>>(
+        T.tiles, T.trange, T.ttet, T.meta, T.unit, T.tcodes, T.czcodes, mixed_views(ctx, es, cs), g, vals, rhs,
+        ctx->d_counts + 4);
+  } else {
+    fp64 st;
+    st.es = es;
+    st.cs = cs;
+    const gargs<double> g{sc, mc, lam, mu};
+    k_gather_tile<fp64, 3, 2><<<T.n_tiles, TILE_THREADS, T.smem64, s>>>(T.tiles, T.trange, T.ttet, T.meta, T.unit,
+                                                               T.tcodes, T.czcodes, st, g, vals, rhs,
+                                                               ctx->d_counts + 4);
+  }
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
 
 int icf_gather_variants(int kind) { return kind == 0 ? N_OFF : N_DIAG; }
 const char *icf_gather_variant_name(int kind, int v) {

@@ -76,6 +76,37 @@ struct icf_sell {
   uint32_t *codes = nullptr;
 };
 
+// Row tiles of the static pattern (icf_tile.cu): the rows cut, in Morton
+// order of their nodes, into tiles whose tets (those with a vertex on one of
+// the tile's rows) number at most ICF_TILE_TETS.  One CTA of k_gather_tile
+// stages a tile in shared memory and writes every block of its rows.
+//   tiles[t]  = {first tet in ttet, tets, first slice, slices}
+//   trange[t] = {first tet code, tet codes} of the tile's slices
+//   ttet      = each tile's tets, ascending
+//   meta[s]   = {first tet code, tet iterations, CZ iterations, first CZ code}
+//   unit      = 32 per slice: {block, row or -1} (unit_s: static slots; unit:
+//               merged slots of the current structure)
+//   tcodes    = 16-bit tet codes (position in the tile << 4 | a << 2 | b),
+//               sliced ELL: iteration k of lane l at first + 32 k + l; 0xFFFF pads
+//   czcodes   = the CZ codes, sliced ELL likewise
+#define ICF_TILE_TETS 384
+#define ICF_TILE_CODES 8192  // tet codes of a tile, before padding
+struct icf_tiles {
+  bool built = false;  // for the current static pattern
+  bool ok = false;     // false: some row has more tets than a tile holds
+  int n_tiles = 0, n_slices = 0;
+  long long n_ttet = 0, n_tcodes = 0, n_czcodes = 0, n_real = 0;
+  long long n_diag_units = 0, n_off_units = 0;
+  size_t smem64 = 0, smem32 = 0;  // shared memory of the largest tile
+  int4 *tiles = nullptr;
+  int2 *trange = nullptr;
+  int *ttet = nullptr;
+  int4 *meta = nullptr;
+  int2 *unit_s = nullptr, *unit = nullptr;
+  uint16_t *tcodes = nullptr;
+  uint32_t *czcodes = nullptr;
+};
+
 // Device MINRES solver state (icf_solve.cu).
 struct icf_solver {
   long long gen = -1;  // structure generation the lower-block index belongs to
@@ -187,6 +218,9 @@ struct icf_ctx {
   // in sell_off / sell_diag.
   icf_sell sell_off, sell_diag, sell_off_cz, sell_diag_cz;
   bool split_cz = false;
+  // row-tile gather (one kernel for all blocks) instead of the two list gathers
+  icf_tiles tiles;
+  bool gather_tiles = false;
 
   // merged pattern
   int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;
@@ -280,6 +314,13 @@ int icf_cz_variants();
 const char *icf_cz_variant_name(int v);
 int icf_launch_cz(icf_ctx *ctx, int variant, const double4 *xc, double *cs, cudaStream_t s);
 // rebuilds the diagonal gather lists for `lanes` lanes per row (icf_pattern.cu)
+int icf_build_tiles(icf_ctx *ctx);       // host-built, once per static pattern
+int icf_remap_tiles(icf_ctx *ctx);       // unit slots for the current structure
+void icf_free_tiles(icf_ctx *ctx);
+int icf_gather_tile_setup(icf_ctx *ctx);
+bool icf_tiles_active(const icf_ctx *ctx);
+int icf_launch_gather_tile(icf_ctx *ctx, const double4 *es, const double *cs, double sc, double mc, double lam,
+                           double mu, double *vals, double *rhs, cudaStream_t s);
 int icf_rebuild_lists(icf_ctx *ctx);  // both gathers' lists for the current layout and split
 int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes);
 int icf_rebuild_sell_off(icf_ctx *ctx, bool natural);

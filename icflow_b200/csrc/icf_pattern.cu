@@ -808,6 +808,7 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
   ctx->sell_diag.lanes = ctx->sell_diag_cz.lanes = icf_gather_variant_lanes(ctx->tune_diag);
   if (build_lists(ctx, true, true)) return ICF_ERR_CUDA;
   if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
+  if (ctx->tiles.built && icf_remap_tiles(ctx)) return ICF_ERR_CUDA;
   if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
   if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
   k_rows<<<icf_blocks((long long)N + 1, 256), 256, 0, s>>>(N, nnz, ctx->d_mkeys, ctx->d_rows);

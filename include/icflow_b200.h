@@ -224,7 +224,11 @@ int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out
  * per-contribution records written at their gather positions and read as
  * streams) or the list split (kind 5, per-tet records only: 0, the default,
  * one list per gather; 1 keeps the units without CZ contributions in lists of
- * their own that run beside the CZ kernel).  The tuner also times whole
+ * their own that run beside the CZ kernel) or the gather scheme (kind 6,
+ * per-tet records only: 0, the default, the off-diagonal and diagonal list
+ * gathers; 1 one row-tile gather, a CTA per set of rows with the rows' tet
+ * records and codes staged in shared memory, built on the host at the first
+ * structure that needs it).  The tuner also times whole
  * assemblies with each layout and split first. */
 #define ICF_MAX_TUNE 32
 typedef struct icf_tune_report {

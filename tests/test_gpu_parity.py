@@ -269,7 +269,7 @@ def test_every_launch_variant_and_autotune(O):
     compare(ref, o)
     lib = _lib.load()
     counts = {}
-    for kind in (3, 5, 0, 1, 2, 4):
+    for kind in (3, 6, 5, 0, 1, 2, 4):
         v = 0
         while lib.icf_set_variant(gf.ctx, kind, v) == 0:
             gf.AssembleElemsAndCZs(H)
@@ -306,8 +306,12 @@ def test_every_launch_variant_and_autotune(O):
     _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 3, 1))
     rep = gf.Autotune(H, reps=3)
     kinds = {r["kernel"] for r in rep}
-    assert kinds == {"layout", "split", "k_tet_unit", "k_cz_gp", "k_gather_off", "k_gather_diag"}
-    assert len(rep) == sum(counts.values())
+    assert {"layout", "k_tet_unit", "k_cz_gp"} <= kinds
+    layout = [r["variant"] for r in rep if r["kernel"] == "layout" and r["chosen"]]
+    assert ("gather" in kinds) == (layout == ["per-tet records"]), (layout, kinds)
+    if "split" in kinds:  # the list gathers' choices are timed only when the lists run
+        assert {"k_gather_off", "k_gather_diag"} <= kinds
+        assert len(rep) == sum(counts.values()) - (0 if "gather" in kinds else counts[6])
     for k in kinds:
         assert sum(r["chosen"] for r in rep if r["kernel"] == k) == 1
     vals, rhs = gf.TransferLinearSystemToHost()
@@ -354,6 +358,46 @@ def test_fp32_mixed_error_report(O, case):
         assert np.array_equal(a["flags"][sel], o["flags"])
         assert vec_rel(o["tent"], a["tent"][sel]) <= FP64_TOL
     print(f"{case}: FP32-mixed vs FP64 oracle: blocks {err_vals:.2e} (rowwise), rhs {err_rhs:.2e}")
+    gf.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_tiled_gather(O, precision):
+    """The row-tile gather (one CTA per tile, tet records and codes staged in
+    shared memory) against the oracle, in both precisions, for two structures
+    of the same model (the contact blocks move the merged slots); its
+    off-diagonal blocks equal the list gather's bit for bit (one lane per
+    block, same code order)."""
+    from icflow_b200 import _lib
+
+    prms = config_prms(penaltyK=1e8)
+    coll = M.polycrystal(n=8, grains=6, seed=2, platens=True, gap=-0.3)
+    gf = _gf(coll, prms)
+    lib = _lib.load()
+    _lib.check(gf.ctx, lib.icf_set_precision(gf.ctx, precision))
+    p = orc_prms_from(O, prms)
+    tol = FP64_TOL if precision == 0 else FP32_TOL
+    for seed in (8, 9):
+        state = random_state(coll, seed, du=2e-6)
+        pmax, tmax, failed = _zeros_cz(coll)
+        pairs = M.candidate_pairs(coll, coll.x0 + state[0])
+        _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 6, 0))
+        a = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+        _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 6, 1))
+        gf.AssembleElemsAndCZs(H)
+        vals, rhs = gf.TransferLinearSystemToHost()
+        vals = vals.reshape(-1, 3, 3)
+        names = {k["name"] for k in gf.ProfileAssembly(H, reps=2)}
+        assert "k_gather_tile" in names and "k_gather_off" not in names, names
+        o = oracle_assemble(O, p, coll, state, H, pmax, tmax, gf.c_itet)
+        assert np.array_equal(a["rows"], o["rows"]) and np.array_equal(a["cols"], o["cols"])
+        assert rowwise_rel(o["rows"], o["vals"], vals) <= tol
+        assert vec_rel(o["rhs"], rhs) <= FP64_TOL
+        row_of = np.repeat(np.arange(len(a["rows"]) - 1), np.diff(a["rows"]))
+        off = a["cols"] != row_of
+        assert np.array_equal(vals[off], a["vals"][off])
+        cnt = gf.AssembleElemsAndCZs(H)
+        assert cnt.nonFinite == 0
     gf.close()
 
 
