@@ -268,6 +268,10 @@ __device__ __forceinline__ void cz_frame(const double m0[3], const double m1[3],
     p1[k] = sub(m1[k], m0[k]);
     p2[k] = sub(m0[k], m2[k]);
   }
+  // the reference's operation order and rounding (no contraction): the
+  // opening is a difference of nearly equal rotated coordinates, so a
+  // rounding change in R moves it by far more than its own size at small
+  // openings
   const double l1 = sqrt(add(add(mul(p1[0], p1[0]), mul(p1[1], p1[1])), mul(p1[2], p1[2])));
   for (int k = 0; k < 3; k++) R[0][k] = p1[k] / l1;
   n[0] = add(mul(-p1[2], p2[1]), mul(p1[1], p2[2]));
