@@ -25,12 +25,14 @@
 namespace {
 
 // ---- small vector helpers ---------------------------------------------------
+// A node position (32 B, 32 B aligned: node arrays start on 256 B) in one
+// 256-bit read-only load.
 __device__ __forceinline__ void ld_node(const double4 *__restrict__ p, int i,
                                         double o[3]) {
-  const double4 v = p[i];
-  o[0] = v.x;
-  o[1] = v.y;
-  o[2] = v.z;
+  double w;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(w)
+      : "l"(p + i));
 }
 
 // Orthonormal frame of three points as in fastRotationMatrix

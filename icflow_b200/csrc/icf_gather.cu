@@ -47,17 +47,28 @@ __device__ __forceinline__ void cz_code(uint32_t code, uint32_t &c, int &ia, int
   a_lo = a < 3;
 }
 
+// One 32 B staging record in a single 256-bit read-only load (the record
+// starts on a 32 B boundary: the staging buffer is 256 B aligned and every
+// record is 32 B).
+__device__ __forceinline__ double4 ld_rec(const double4 *p) {
+  double4 v;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+  return v;
+}
+
 // Staging views and arithmetic of one precision.
 struct fp64 {
   typedef double real;
   typedef double4 rec;
   const double4 *es;  // tet records: {h_a, V} at 8e + a, {rhs_a, 0} at 8e + 4 + a
   const double *cs;   // CZ records: Kt (6 x 6) at 48c, rt[3][3] at 48c + 36
-  __device__ __forceinline__ rec hrec(uint32_t e, uint32_t a) const { return es[8 * (size_t)e + a]; }
+  __device__ __forceinline__ rec hrec(uint32_t e, uint32_t a) const { return ld_rec(es + 8 * (size_t)e + a); }
   __device__ __forceinline__ const char *hsrc(uint32_t e) const {  // the 4 h records of tet e
     return reinterpret_cast<const char *>(es + 8 * (size_t)e);
   }
-  __device__ __forceinline__ double4 rrec(uint32_t e, uint32_t a) const { return es[8 * (size_t)e + 4 + a]; }
+  __device__ __forceinline__ double4 rrec(uint32_t e, uint32_t a) const {
+    return ld_rec(es + 8 * (size_t)e + 4 + a);
+  }
   __device__ __forceinline__ void kt(uint32_t c, int pair, real k[6]) const {
     const double2 *K2 = reinterpret_cast<const double2 *>(cs + (size_t)c * ICF_CZ_STAGE + 6 * pair);
     const double2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
