@@ -326,7 +326,43 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK, MINB)
   __shared__ double sPT[3 * CZ_PER_BLOCK][2];
   __shared__ int sFl[3 * CZ_PER_BLOCK];
   __shared__ double sOut[CZ_PER_BLOCK * ICF_CZ_STAGE];
+  __shared__ double sD[CZ_PER_BLOCK][9];   // per CZ: (R x_n - R x_{n+3})[k] at 3 n + k
+  __shared__ double sRJ[CZ_PER_BLOCK][10]; // per CZ: R (row-major), aJ
   const int t = threadIdx.x;
+  // per CZ, once (the first warp, one CZ per lane): node positions, the
+  // mid-plane, its frame and the rotated face differences (:243-290)
+  if (t < CZ_PER_BLOCK) {
+    const int cc = blockIdx.x * CZ_PER_BLOCK + t;
+    if (cc < nc && __ldg(czfail + cc) == 0) {
+      const int4 i0 = __ldg(reinterpret_cast<const int4 *>(cz) + 2 * cc);
+      const int2 i1 = __ldg(reinterpret_cast<const int2 *>(cz) + 4 * cc + 2);
+      const int nid[6] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y};
+      double x[6][3];
+#pragma unroll
+      for (int i = 0; i < 6; i++) ld_node(xc, nid[i], x[i]);
+      double mp[3][3], R[3][3], aJ;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) mp[i][k] = mul(add(x[i][k], x[i + 3][k]), 0.5);
+      cz_frame(mp[0], mp[1], mp[2], R, aJ);
+#pragma unroll
+      for (int n = 0; n < 3; n++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const double xa = add(add(mul(x[n][0], R[k][0]), mul(x[n][1], R[k][1])), mul(x[n][2], R[k][2]));
+          const double xb =
+              add(add(mul(x[n + 3][0], R[k][0]), mul(x[n + 3][1], R[k][1])), mul(x[n + 3][2], R[k][2]));
+          sD[t][3 * n + k] = sub(xa, xb);
+        }
+#pragma unroll
+      for (int m = 0; m < 3; m++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) sRJ[t][3 * m + k] = R[m][k];
+      sRJ[t][9] = aJ;
+    }
+  }
+  __syncthreads();
   const int j = t / 3, gp = t - 3 * j;
   const int c = blockIdx.x * CZ_PER_BLOCK + j;
   const bool live = c < nc && __ldg(czfail + c) == 0;
@@ -337,32 +373,21 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK, MINB)
       const double4 w = czprm[c];
       f_tn = w.x; f_tt = w.y; deln = w.z; delt = w.w;
     }
-    const int4 i0 = __ldg(reinterpret_cast<const int4 *>(cz) + 2 * c);
-    const int2 i1 = __ldg(reinterpret_cast<const int2 *>(cz) + 4 * c + 2);
-    const int nid[6] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y};
-    double x[6][3];
-#pragma unroll
-    for (int i = 0; i < 6; i++) ld_node(xc, nid[i], x[i]);
     double pmax = __ldg(czs + 8 * (size_t)c + gp);
     double tmax = __ldg(czs + 8 * (size_t)c + 3 + gp);
-
-    // mid-plane, its frame, local coordinates and the opening (:243-290)
-    double mp[3][3], R[3][3], aJ;
+    double R[3][3];
 #pragma unroll
-    for (int i = 0; i < 3; i++)
+    for (int m = 0; m < 3; m++)
 #pragma unroll
-      for (int k = 0; k < 3; k++) mp[i][k] = mul(add(x[i][k], x[i + 3][k]), 0.5);
-    cz_frame(mp[0], mp[1], mp[2], R, aJ);
+      for (int k = 0; k < 3; k++) R[m][k] = sRJ[j][3 * m + k];
+    const double aJ = sRJ[j][9];
+    // this Gauss point's opening
     double o[3] = {0, 0, 0};
 #pragma unroll
     for (int n = 0; n < 3; n++) {
       const double sfn = P.sf[n * 3 + gp];
 #pragma unroll
-      for (int k = 0; k < 3; k++) {
-        const double xa = add(add(mul(x[n][0], R[k][0]), mul(x[n][1], R[k][1])), mul(x[n][2], R[k][2]));
-        const double xb = add(add(mul(x[n + 3][0], R[k][0]), mul(x[n + 3][1], R[k][1])), mul(x[n + 3][2], R[k][2]));
-        o[k] = add(o[k], mul(sub(xa, xb), sfn));
-      }
+      for (int k = 0; k < 3; k++) o[k] = add(o[k], mul(sD[j][3 * n + k], sfn));
     }
     const double opn = o[2];
     const double opt = sqrt(add(mul(o[0], o[0]), mul(o[1], o[1])));
@@ -440,34 +465,46 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK, MINB)
   sFl[t] = fl;
   __syncthreads();
 
-  // combine the three Gauss points of CZ j; thread gp builds 16 of the 48 values
+  // combine the three Gauss points of CZ j: thread gp builds the Kt pairs
+  // 2 gp and 2 gp + 1 (12 values), the rt row gp (3) and one pad value
   const int b3 = 3 * j;
   const bool failed = live && (((sFl[b3] | sFl[b3 + 1] | sFl[b3 + 2]) & 4) != 0);
-  for (int v = 16 * gp; v < 16 * gp + 16; v++) {
-    double val = 0.0;
-    if (live && !failed) {
-      if (v < 36) {
-        const int pr = v / 6, comp = v - 6 * pr;
-        const int pi = pr < 3 ? 0 : (pr < 5 ? 1 : 2);
-        const int pj = pr < 3 ? pr : (pr < 5 ? pr - 2 : 2);
+  const bool on = live && !failed;
+  double *so = sOut + j * ICF_CZ_STAGE;
+#pragma unroll
+  for (int hh = 0; hh < 2; hh++) {
+    const int pr = 2 * gp + hh;
+    const int pi = pr < 3 ? 0 : (pr < 5 ? 1 : 2);
+    const int pj = pr < 3 ? pr : (pr < 5 ? pr - 2 : 2);
+    double cf[3];
+#pragma unroll
+    for (int g = 0; g < 3; g++) cf[g] = P.sf[pi * 3 + g] * P.sf[pj * 3 + g];
+#pragma unroll
+    for (int comp = 0; comp < 6; comp++) {
+      double val = 0.0;
+      if (on) {
         if (MIXED) {
           float vf = 0.f;
 #pragma unroll
-          for (int g = 0; g < 3; g++)
-            vf += (float)(P.sf[pi * 3 + g] * P.sf[pj * 3 + g]) * (float)sQ[b3 + g][comp];
+          for (int g = 0; g < 3; g++) vf += (float)cf[g] * (float)sQ[b3 + g][comp];
           val = vf;
         } else {
 #pragma unroll
-          for (int g = 0; g < 3; g++) val += (P.sf[pi * 3 + g] * P.sf[pj * 3 + g]) * sQ[b3 + g][comp];
+          for (int g = 0; g < 3; g++) val += cf[g] * sQ[b3 + g][comp];
         }
-      } else if (v < 45) {
-        const int i = (v - 36) / 3, k = (v - 36) - 3 * i;
-#pragma unroll
-        for (int g = 0; g < 3; g++) val += P.sf[i * 3 + g] * sTw[b3 + g][k];
       }
+      so[6 * pr + comp] = val;
     }
-    sOut[j * ICF_CZ_STAGE + v] = val;
   }
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double val = 0.0;
+    if (on)
+#pragma unroll
+      for (int g = 0; g < 3; g++) val += P.sf[gp * 3 + g] * sTw[b3 + g][k];
+    so[36 + 3 * gp + k] = val;
+  }
+  so[45 + gp] = 0.0;
   int flag = 0;
   if (gp == 0 && live) {
     const int f0 = sFl[b3], f1 = sFl[b3 + 1], f2 = sFl[b3 + 2];
