@@ -1049,9 +1049,12 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     ICF_TRY_RC(gather_diag(DB, s, "k_gather_diag_cz", true));
   } else {
     // one list per gather: off-diagonal on aux0 once the tets are staged,
-    // diagonal on main once the CZs are
-    ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_tet, 0));
-    ICF_TRY_RC(gather_off(OA, sa, "k_gather_off", true));
+    // diagonal on main once the CZs are; or (serial_gathers) both on main,
+    // one after the other
+    cudaStream_t so = ctx->serial_gathers ? s : sa;
+    if (ctx->serial_gathers) ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
+    else ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_tet, 0));
+    ICF_TRY_RC(gather_off(OA, so, "k_gather_off", true));
     ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_cz, 0));
     ICF_TRY_RC(gather_diag(DA, s, "k_gather_diag", true));
   }

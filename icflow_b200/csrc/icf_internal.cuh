@@ -221,6 +221,9 @@ struct icf_ctx {
   // row-tile gather (one kernel for all blocks) instead of the two list gathers
   icf_tiles tiles;
   bool gather_tiles = false;
+  // the two list gathers one after the other on the main stream instead of
+  // side by side
+  bool serial_gathers = false;
 
   // merged pattern
   int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;

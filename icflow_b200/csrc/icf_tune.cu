@@ -62,9 +62,11 @@ int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant) {
                           : kind == 3 ? 2
                           : kind == 5 ? 2
                           : kind == 6 ? 2
+                          : kind == 7 ? 2
                                       : icf_cz_variants();
-  if (kind < 0 || kind > 6 || variant < 0 || variant >= n)
-    return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..6 and a variant index of that kind");
+  if (kind < 0 || kind > 7 || variant < 0 || variant >= n)
+    return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..7 and a variant index of that kind");
+  if (kind == 7) ctx->serial_gathers = variant == 1;
   if (kind == 6) {
     ctx->gather_tiles = variant == 1;
     if (ctx->gather_tiles && ctx->have_structure && !ctx->tiles.built) {
@@ -112,7 +114,7 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
     ctx->version++;  // re-capture with the candidate's kernels
     return time_launches(ctx, t, reps, [&] { return icf_launch_assembly(ctx, h); }, ms);
   };
-  int split = ctx->split_cz ? 1 : 0, tiles = ctx->gather_tiles ? 1 : 0;
+  int split = ctx->split_cz ? 1 : 0, tiles = ctx->gather_tiles ? 1 : 0, serial = ctx->serial_gathers ? 1 : 0;
   struct kind_desc {
     const char *name;
     int kind, n;
@@ -122,6 +124,7 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
       {"layout", 3, 2, &ctx->layout},
       {"gather", 6, 2, &tiles},
       {"split", 5, ctx->n_cz > 0 ? 2 : 0, &split},
+      {"streams", 7, 2, &serial},
       {"k_tet_unit", 0, ctx->n_elem > 0 ? icf_tet_variants() : 0, &ctx->tune_tet},
       {"k_cz_gp", 4, ctx->n_cz > 0 ? icf_cz_variants() : 0, &ctx->tune_cz},
       {"k_gather_off", 1, ctx->n_offd > 0 ? icf_gather_variants(0) : 0, &ctx->tune_off},
@@ -130,10 +133,13 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
   const char *layout_names[2] = {"per-tet records", "per-contribution stream"};
   const char *split_names[2] = {"one list per gather", "CZ-free units apart"};
   const char *gather_names[2] = {"off-diagonal + diagonal lists", "row tiles"};
+  const char *stream_names[2] = {"gathers side by side", "gathers one after other"};
   for (const kind_desc &k : kinds) {
     if (k.n < 2) continue;
     // the list gathers' choices do not matter while the tiled gather runs
-    if ((k.kind == 1 || k.kind == 2 || k.kind == 5) && icf_tiles_active(ctx)) continue;
+    if ((k.kind == 1 || k.kind == 2 || k.kind == 5 || k.kind == 7) && icf_tiles_active(ctx)) continue;
+    // the stream placement matters only for one list per gather
+    if (k.kind == 7 && ctx->split_cz && ctx->layout == ICF_LAYOUT_RECORDS) continue;
     // nor the tiled gather under the per-contribution layout
     if (k.kind == 6 && ctx->layout != ICF_LAYOUT_RECORDS) continue;
     double best = 1e30;
@@ -145,6 +151,7 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
       const char *vn = k.kind == 3 ? layout_names[v]
                        : k.kind == 5 ? split_names[v]
                        : k.kind == 6 ? gather_names[v]
+                       : k.kind == 7 ? stream_names[v]
                        : k.kind == 0 ? icf_tet_variant_name(v)
                        : k.kind == 4 ? icf_cz_variant_name(v)
                                      : icf_gather_variant_name(k.kind == 1 ? 0 : 1, v);
@@ -155,6 +162,7 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
     const char *vn = k.kind == 3 ? layout_names[bv]
                      : k.kind == 5 ? split_names[bv]
                      : k.kind == 6 ? gather_names[bv]
+                     : k.kind == 7 ? stream_names[bv]
                      : k.kind == 0 ? icf_tet_variant_name(bv)
                      : k.kind == 4 ? icf_cz_variant_name(bv)
                                    : icf_gather_variant_name(k.kind == 1 ? 0 : 1, bv);

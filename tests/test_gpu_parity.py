@@ -269,7 +269,7 @@ def test_every_launch_variant_and_autotune(O):
     compare(ref, o)
     lib = _lib.load()
     counts = {}
-    for kind in (3, 6, 5, 0, 1, 2, 4):
+    for kind in (3, 6, 5, 7, 0, 1, 2, 4):
         v = 0
         while lib.icf_set_variant(gf.ctx, kind, v) == 0:
             gf.AssembleElemsAndCZs(H)
@@ -311,7 +311,10 @@ def test_every_launch_variant_and_autotune(O):
     assert ("gather" in kinds) == (layout == ["per-tet records"]), (layout, kinds)
     if "split" in kinds:  # the list gathers' choices are timed only when the lists run
         assert {"k_gather_off", "k_gather_diag"} <= kinds
-        assert len(rep) == sum(counts.values()) - (0 if "gather" in kinds else counts[6])
+    kind_of = {"layout": 3, "gather": 6, "split": 5, "streams": 7, "k_tet_unit": 0, "k_gather_off": 1,
+               "k_gather_diag": 2, "k_cz_gp": 4}
+    for k in kinds:  # every variant of a timed kind is timed
+        assert sum(r["kernel"] == k for r in rep) == counts[kind_of[k]], k
     for k in kinds:
         assert sum(r["chosen"] for r in rep if r["kernel"] == k) == 1
     vals, rhs = gf.TransferLinearSystemToHost()
