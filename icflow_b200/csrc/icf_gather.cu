@@ -69,10 +69,19 @@ struct fp64 {
   __device__ __forceinline__ double4 rrec(uint32_t e, uint32_t a) const {
     return ld_rec(es + 8 * (size_t)e + 4 + a);
   }
+  // Kt pair p sits at byte 384 c + 48 p: 32 B aligned for even p, 16 B past
+  // a 32 B boundary for odd p, so two loads (32 B + 16 B) read its 48 B.
   __device__ __forceinline__ void kt(uint32_t c, int pair, real k[6]) const {
-    const double2 *K2 = reinterpret_cast<const double2 *>(cs + (size_t)c * ICF_CZ_STAGE + 6 * pair);
-    const double2 k01 = __ldg(K2), k23 = __ldg(K2 + 1), k45 = __ldg(K2 + 2);
-    k[0] = k01.x; k[1] = k01.y; k[2] = k23.x; k[3] = k23.y; k[4] = k45.x; k[5] = k45.y;
+    const double *K = cs + (size_t)c * ICF_CZ_STAGE + 6 * pair;
+    if ((pair & 1) == 0) {
+      const double4 a = ld_rec(reinterpret_cast<const double4 *>(K));
+      const double2 b = __ldg(reinterpret_cast<const double2 *>(K + 4));
+      k[0] = a.x; k[1] = a.y; k[2] = a.z; k[3] = a.w; k[4] = b.x; k[5] = b.y;
+    } else {
+      const double2 a = __ldg(reinterpret_cast<const double2 *>(K));
+      const double4 b = ld_rec(reinterpret_cast<const double4 *>(K + 2));
+      k[0] = a.x; k[1] = a.y; k[2] = b.x; k[3] = b.y; k[4] = b.z; k[5] = b.w;
+    }
   }
   __device__ __forceinline__ const double *rt(uint32_t c) const { return cs + (size_t)c * ICF_CZ_STAGE + 36; }
 };
@@ -196,6 +205,37 @@ __device__ __forceinline__ void cz_codes(const S &st, const uint32_t *c, int k0,
   }
 }
 
+// A 3x3 block (72 B, 8 B aligned) in five stores instead of nine: four
+// 16 B stores from whichever of its first two doubles is 16 B aligned, and an
+// rhs row (24 B) in two stores instead of three.
+template <typename R>
+__device__ __forceinline__ void st_block(double *__restrict__ vals, int s, const R b[9]) {
+  double *o = vals + 9 * (size_t)s;
+  if ((reinterpret_cast<uintptr_t>(o) & 8) == 0) {
+    reinterpret_cast<double2 *>(o)[0] = make_double2((double)b[0], (double)b[1]);
+    reinterpret_cast<double2 *>(o)[1] = make_double2((double)b[2], (double)b[3]);
+    reinterpret_cast<double2 *>(o)[2] = make_double2((double)b[4], (double)b[5]);
+    reinterpret_cast<double2 *>(o)[3] = make_double2((double)b[6], (double)b[7]);
+    o[8] = (double)b[8];
+  } else {
+    o[0] = (double)b[0];
+    reinterpret_cast<double2 *>(o + 1)[0] = make_double2((double)b[1], (double)b[2]);
+    reinterpret_cast<double2 *>(o + 1)[1] = make_double2((double)b[3], (double)b[4]);
+    reinterpret_cast<double2 *>(o + 1)[2] = make_double2((double)b[5], (double)b[6]);
+    reinterpret_cast<double2 *>(o + 1)[3] = make_double2((double)b[7], (double)b[8]);
+  }
+}
+__device__ __forceinline__ void st_rhs(double *__restrict__ rhs, int row, const double r[3]) {
+  double *o = rhs + 3 * (size_t)row;
+  if ((reinterpret_cast<uintptr_t>(o) & 8) == 0) {
+    reinterpret_cast<double2 *>(o)[0] = make_double2(r[0], r[1]);
+    o[2] = r[2];
+  } else {
+    o[0] = r[0];
+    reinterpret_cast<double2 *>(o + 1)[0] = make_double2(r[1], r[2]);
+  }
+}
+
 template <typename V4>
 __device__ __forceinline__ V4 zero4();
 template <>
@@ -238,9 +278,7 @@ __global__ void __launch_bounds__(256, MINB)
   cz_codes<S, CZ_UNROLL>(st, c, m.y, m.y + m.z, b, nullptr);
   const int2 u = unit[32 * w + lane];
   if (u.x < 0) return;
-  double *o = vals + 9 * (size_t)u.x;
-#pragma unroll
-  for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+  st_block(vals, u.x, b);
 }
 
 // ---- diagonal blocks and rhs rows: L lanes per row --------------------------
@@ -296,14 +334,10 @@ __global__ void __launch_bounds__(256, MINB)
   const int sub = lane % L;
   const int2 u = unit[(32 / L) * w + lane / L];
   if (sub == 0 && u.x >= 0) {
-    double *o = vals + 9 * (size_t)u.x;
-#pragma unroll
-    for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+    st_block(vals, u.x, b);
   }
   if (sub == (L > 1 ? 1 : 0) && u.y >= 0) {
-    rhs[3 * (size_t)u.y + 0] = r[0];
-    rhs[3 * (size_t)u.y + 1] = r[1];
-    rhs[3 * (size_t)u.y + 2] = r[2];
+    st_rhs(rhs, u.y, r);
   }
   // NaN/Inf check of the row (its rhs and diagonal block), one vote per warp
   bool bad = false;
@@ -469,9 +503,7 @@ __global__ void __launch_bounds__(256, MINB)
     }
     cz_codes<S, CZ_UNROLL>(st, c, m.y, m.y + m.z, b, nullptr);
     if (u.x >= 0) {
-      double *o = vals + 9 * (size_t)u.x;
-#pragma unroll
-      for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+      st_block(vals, u.x, b);
     }
     if (wn >= n_slices) break;
     w = wn;
@@ -556,14 +588,10 @@ __global__ void __launch_bounds__(256, MINB)
     }
     const int sub = lane % L;
     if (sub == 0 && u.x >= 0) {
-      double *o = vals + 9 * (size_t)u.x;
-#pragma unroll
-      for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+      st_block(vals, u.x, b);
     }
     if (sub == (L > 1 ? 1 : 0) && u.y >= 0) {
-      rhs[3 * (size_t)u.y + 0] = r[0];
-      rhs[3 * (size_t)u.y + 1] = r[1];
-      rhs[3 * (size_t)u.y + 2] = r[2];
+      st_rhs(rhs, u.y, r);
     }
     if (sub == 0)
 #pragma unroll
@@ -643,9 +671,7 @@ __global__ void __launch_bounds__(256, MINB)
   cz_codes<S, CZ_UNROLL>(st, c, m.y, m.y + m.z, b, nullptr);
   const int2 u = unit[32 * w + lane];
   if (u.x < 0) return;
-  double *o = vals + 9 * (size_t)u.x;
-#pragma unroll
-  for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+  st_block(vals, u.x, b);
 }
 
 template <typename S, bool MIXED, int L, int MINB, int U>
@@ -691,14 +717,10 @@ __global__ void __launch_bounds__(256, MINB)
   const int sub = lane % L;
   const int2 u = unit[(32 / L) * w + lane / L];
   if (sub == 0 && u.x >= 0) {
-    double *o = vals + 9 * (size_t)u.x;
-#pragma unroll
-    for (int q = 0; q < 9; q++) o[q] = (double)b[q];
+    st_block(vals, u.x, b);
   }
   if (sub == (L > 1 ? 1 : 0) && u.y >= 0) {
-    rhs[3 * (size_t)u.y + 0] = r[0];
-    rhs[3 * (size_t)u.y + 1] = r[1];
-    rhs[3 * (size_t)u.y + 2] = r[2];
+    st_rhs(rhs, u.y, r);
   }
   // NaN/Inf check of the row (its rhs and diagonal block), one vote per warp
   bool bad = false;
@@ -843,17 +865,12 @@ __global__ void __launch_bounds__(TILE_THREADS, MINB)
     }
     cz_codes<S, CZ_UNROLL>(st, czcodes + m.w + lane, 0, m.z, b, dg ? r : nullptr);
     if (u.x >= 0) {
-      double *o = vals + 9 * (size_t)u.x;
+      st_block(vals, u.x, b);
 #pragma unroll
-      for (int q = 0; q < 9; q++) {
-        o[q] = (double)b[q];
-        bad |= !isfinite((double)b[q]);
-      }
+      for (int q = 0; q < 9; q++) bad |= !isfinite((double)b[q]);
     }
     if (dg) {
-      rhs[3 * (size_t)u.y + 0] = r[0];
-      rhs[3 * (size_t)u.y + 1] = r[1];
-      rhs[3 * (size_t)u.y + 2] = r[2];
+      st_rhs(rhs, u.y, r);
       bad |= !(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]));
     }
     int nw = 0;
