@@ -582,36 +582,37 @@ __global__ void k_imp_add(int n_slots, const int *__restrict__ slot,
                           const int *__restrict__ cols,
                           const double *__restrict__ ks,
                           double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n_slots) return;
-  const int s = slot[g];
-  double b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, r[3] = {0, 0, 0};
-  bool diag = false;
-  for (int q = off[g]; q < off[g + 1]; q++) {
-    const uint32_t cd = code[q];
-    const uint32_t u = (cd >> 4) & 0x3FFFFFFu, a = (cd >> 2) & 3u, bb = cd & 3u;
-    const double *K = ks + (size_t)u * ICF_IMP_STAGE;
-    for (int k = 0; k < 3; k++)
-      for (int l = 0; l < 3; l++) b[3 * k + l] += K[(3 * a + k) * 12 + 3 * bb + l];
-    if (a == bb) {
-      for (int k = 0; k < 3; k++) r[k] += K[144 + 3 * a + k];
-      diag = true;
+  // one warp per touched block: lane 12 h + e (h = 0, 1; e < 12) reads entry
+  // e (9 block values, then 3 rhs values) of the codes h, h + 2, ... of the
+  // block, in code order; the two halves then add up, and lanes 0..11 add the
+  // sums to the block and rhs row.  A few thousand blocks: the short
+  // dependent chains per lane keep this off the critical path's tail.
+  const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= n_slots) return;
+  const int s = slot[w], q0 = off[w], q1 = off[w + 1];
+  const int h = lane / 12, e = lane - 12 * h;
+  double v = 0.0;
+  bool dg = false;
+  if (h < 2)
+    for (int q = q0 + h; q < q1; q += 2) {
+      const uint32_t cd = __ldg(code + q);
+      const uint32_t u = (cd >> 4) & 0x3FFFFFFu, a = (cd >> 2) & 3u, bb = cd & 3u;
+      const double *K = ks + (size_t)u * ICF_IMP_STAGE;
+      dg |= a == bb;
+      if (e < 9) v += __ldg(K + (3 * a + e / 3) * 12 + 3 * bb + e % 3);
+      else if (a == bb) v += __ldg(K + 144 + 3 * a + (e - 9));
     }
-  }
-  double *o = vals + 9 * (size_t)s;
+  v += __shfl_down_sync(0xffffffffu, v, 12);
+  dg = __any_sync(0xffffffffu, dg);
   bool bad = false;
-  for (int k = 0; k < 9; k++) {
-    o[k] += b[k];
-    bad |= !isfinite(b[k]);
+  if (lane < 9) {
+    vals[9 * (size_t)s + lane] += v;
+    bad = !isfinite(v);
+  } else if (lane < 12 && dg) {
+    rhs[3 * (size_t)cols[s] + (lane - 9)] += v;
+    bad = !isfinite(v);
   }
-  if (diag) {
-    const int row = cols[s];
-    for (int k = 0; k < 3; k++) {
-      rhs[3 * (size_t)row + k] += r[k];
-      bad |= !isfinite(r[k]);
-    }
-  }
-  if (bad) atomicOr(nonfinite, 1);
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
 }
 
 
@@ -1064,7 +1065,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
   if (ctx->n_crs > 0)
-    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off,
+    k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off,
                                                         ctx->d_cr, ctx->d_cols, ctx->d_ks,
                                                         ctx->d_vals, ctx->d_rhs, ctx->d_counts + 4);
   if (ctx->n_crs > 0)
@@ -1268,7 +1269,7 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
                                           B.rhs, s));
   }
   if (ctx->n_crs > 0)
-    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
+    k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
                                                         ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4);
 
   ICF_CUDA(ctx, cudaGetLastError());
