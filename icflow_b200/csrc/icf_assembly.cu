@@ -581,7 +581,11 @@ __global__ void k_imp_add(int n_slots, const int *__restrict__ slot,
                           const uint32_t *__restrict__ code,
                           const int *__restrict__ cols,
                           const double *__restrict__ ks,
-                          double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite) {
+                          double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite,
+                          const unsigned long long *__restrict__ mkey, const int *__restrict__ src,
+                          int identity, int which) {
+  // which: 0 every touched block; 1 those the off-diagonal gather does not
+  // write (diagonal or contact-only); 2 those it does (static, off-diagonal).
   // one warp per touched block: lane 12 h + e (h = 0, 1; e < 12) reads entry
   // e (9 block values, then 3 rhs values) of the codes h, h + 2, ... of the
   // block, in code order; the two halves then add up, and lanes 0..11 add the
@@ -590,6 +594,7 @@ __global__ void k_imp_add(int n_slots, const int *__restrict__ slot,
   const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (w >= n_slots) return;
   const int s = slot[w], q0 = off[w], q1 = off[w + 1];
+  if (which != 0 && icf_off_static(mkey, src, identity, s) != (which == 2)) return;
   const int h = lane / 12, e = lane - 12 * h;
   double v = 0.0;
   bool dg = false;
@@ -1061,13 +1066,20 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   }
   ICF_CUDA(ctx, cudaEventRecord(e_a, sa));
   ICF_CUDA(ctx, cudaEventRecord(e_b, sb));
-  // join
-  ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
+  // impact terms: the blocks that the off-diagonal gather does not write
+  // (diagonal blocks, written on main, and contact-only blocks, zeroed on
+  // aux1) as soon as the impacts are staged; the others after the join
+  const int ident = ctx->src_identity ? 1 : 0;
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
-  if (ctx->n_crs > 0)
-    k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off,
-                                                        ctx->d_cr, ctx->d_cols, ctx->d_ks,
-                                                        ctx->d_vals, ctx->d_rhs, ctx->d_counts + 4);
+  if (ctx->n_crs > ctx->n_crs_off)
+    k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(
+        ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
+        ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 1);
+  ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
+  if (ctx->n_crs_off > 0)
+    k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(
+        ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
+        ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 2);
   if (ctx->n_crs > 0)
     icf_prof_mark(ctx, s, "k_imp_add", 8LL * ICF_IMP_STAGE * ctx->n_imp + 172LL * ctx->n_crs + 4LL * 16 * ctx->n_imp);
 
@@ -1270,7 +1282,8 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
   }
   if (ctx->n_crs > 0)
     k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
-                                                        ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4);
+                                                        ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4,
+                                                        ctx->d_mkeys, ctx->d_src, 1, 0);
 
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -224,6 +224,9 @@ struct icf_ctx {
   // the two list gathers one after the other on the main stream instead of
   // side by side
   bool serial_gathers = false;
+  // touched blocks of the impacts that the off-diagonal list gather writes
+  // (static, off the diagonal): their impact terms wait for that gather
+  int n_crs_off = 0;
 
   // merged pattern
   int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;
@@ -324,7 +327,12 @@ int icf_gather_tile_setup(icf_ctx *ctx);
 bool icf_tiles_active(const icf_ctx *ctx);
 int icf_launch_gather_tile(icf_ctx *ctx, const double4 *es, const double *cs, double sc, double mc, double lam,
                            double mu, double *vals, double *rhs, cudaStream_t s);
-int icf_rebuild_lists(icf_ctx *ctx);  // both gathers' lists for the current layout and split
+int icf_rebuild_lists(icf_ctx *ctx);
+// 1 for a merged slot that the off-diagonal gather writes: static, off the diagonal
+__host__ __device__ inline bool icf_off_static(const unsigned long long *mkey, const int *src, int identity, int s) {
+  const unsigned long long k = mkey[s];
+  return (identity || src[s] >= 0) && (k >> 32) != (k & 0xffffffffull);
+}  // both gathers' lists for the current layout and split
 int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes);
 int icf_rebuild_sell_off(icf_ctx *ctx, bool natural);
 // position map and zeroed contribution staging for the current lists

@@ -276,6 +276,14 @@ __global__ void k_iota(int n, int *__restrict__ a) {
 }
 
 // impact contributions keyed by their merged slot
+__global__ void k_count_off_static(int n, const int *__restrict__ slot, const unsigned long long *__restrict__ mkey,
+                                   const int *__restrict__ src, int identity, int *__restrict__ out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool f = g < n && icf_off_static(mkey, src, identity, slot[g]);
+  const unsigned m = __ballot_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(out, __popc(m));
+}
+
 __global__ void k_cand_imp_rc(int ni, const int4 *__restrict__ imp, const int *__restrict__ alt,
                               const unsigned long long *__restrict__ mkey, int nnz,
                               int *__restrict__ slot, uint32_t *__restrict__ code) {
@@ -869,6 +877,18 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
     ICF_CUDA(ctx, cudaFreeAsync(cnt, s));
     ICF_CUDA(ctx, cudaFreeAsync(d_nr, s));
     ctx->n_crs = nvalid;
+    // how many of them the off-diagonal gather writes
+    ctx->n_crs_off = 0;
+    if (nvalid > 0) {
+      int *d_c;
+      ICF_CUDA(ctx, cudaMallocAsync(&d_c, sizeof(int), s));
+      ICF_CUDA(ctx, cudaMemsetAsync(d_c, 0, sizeof(int), s));
+      k_count_off_static<<<icf_blocks(nvalid, 256), 256, 0, s>>>(nvalid, ctx->d_cr_slot, ctx->d_mkeys, ctx->d_src,
+                                                                  ctx->src_identity ? 1 : 0, d_c);
+      ICF_CUDA(ctx, cudaMemcpyAsync(&ctx->n_crs_off, d_c, sizeof(int), cudaMemcpyDeviceToHost, s));
+      ICF_CUDA(ctx, cudaFreeAsync(d_c, s));
+      ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    }
     // impact staging
     if (ctx->n_imp > ctx->ks_cap) {
       cudaFree(ctx->d_ks);
