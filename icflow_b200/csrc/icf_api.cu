@@ -9,6 +9,8 @@
 #include <cstring>
 #include <new>
 
+#include <cstdint>
+
 #include "icf_internal.cuh"
 
 // ---- helpers -----------------------------------------------------------------
@@ -175,6 +177,16 @@ int icf_create(int device, icf_ctx **out) {
   ctx->device = device;
   bool ok = cudaSetDevice(device) == cudaSuccess;
   if (ok) ok = cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device) == cudaSuccess;
+  // the structure build and the broad phase take their temporaries from the
+  // device's default memory pool (cudaMallocAsync); keep what they release
+  // in the pool instead of unmapping it at every synchronisation (the default
+  // threshold 0 makes each later allocation map memory afresh)
+  if (ok) {
+    cudaMemPool_t pool;
+    ok = cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess;
+    uint64_t keep = UINT64_MAX;
+    if (ok) ok = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess;
+  }
   for (int i = 0; ok && i < 2; i++) ok = cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking) == cudaSuccess;
   for (int i = 0; ok && i < 5; i++) ok = cudaEventCreateWithFlags(&ctx->ev[i], cudaEventDisableTiming) == cudaSuccess;
   if (!ok ||
@@ -204,7 +216,8 @@ static void free_all(icf_ctx *c) {
                   c->imp_inc.off, c->imp_inc.inc, c->d_tmp, c->sell_off.meta, c->sell_off.unit,
                   c->sell_off.codes, c->sell_diag.meta, c->sell_diag.unit, c->sell_diag.codes,
                   c->sell_off_cz.meta, c->sell_off_cz.unit, c->sell_off_cz.codes, c->sell_diag_cz.meta,
-                  c->sell_diag_cz.unit, c->sell_diag_cz.codes, c->d_czhist,
+                  c->sell_diag_cz.unit, c->sell_diag_cz.codes, c->sell_off.unit_s, c->sell_diag.unit_s,
+                  c->sell_off_cz.unit_s, c->sell_diag_cz.unit_s, c->d_czhist,
                   c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup};
   for (void *p : ptrs) cudaFree(p);
 }
@@ -345,6 +358,7 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->sell_diag = icf_sell();
   ctx->sell_off_cz = icf_sell();
   ctx->sell_diag_cz = icf_sell();
+  ctx->lists_static = false;
   ctx->d_czhist = nullptr;
   ctx->hist_valid = false;
   ctx->d_tetpos = nullptr;
@@ -470,10 +484,22 @@ int icf_set_surface_groups(icf_ctx *ctx, int n_surface, const int *group) {
   if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
   cudaFree(ctx->d_sgroup);
   ctx->d_sgroup = nullptr;
+  ctx->sgroup_bits = -1;
   if (!group) return ICF_OK;
   if (n_surface != ctx->n_surf) return icf_fail(ctx, ICF_ERR_ARG, "n_surface does not match the static data");
   ICF_TRY(dalloc(ctx, &ctx->d_sgroup, (size_t)n_surface));
   ICF_CUDA(ctx, cudaMemcpy(ctx->d_sgroup, group, sizeof(int) * (size_t)n_surface, cudaMemcpyHostToDevice));
+  // bits of the largest group id (for the broad phase's (cell, group) keys);
+  // -1 when some id is negative
+  int gmax = 0;
+  bool neg = false;
+  for (int i = 0; i < n_surface; i++) {
+    neg |= group[i] < 0;
+    gmax = group[i] > gmax ? group[i] : gmax;
+  }
+  int bits = 0;
+  while (bits < 31 && (1LL << bits) <= (long long)gmax) bits++;
+  ctx->sgroup_bits = neg ? -1 : bits;
   return ICF_OK;
 }
 

@@ -1146,10 +1146,6 @@ int icf_launch_assembly(icf_ctx *ctx, double h) {
   ICF_TRY_RC(icf_ensure_cz_hist(ctx, ctx->stream));
   if (!ctx->use_graph) return enqueue_assembly(ctx, h);
   if (!ctx->graph_exec || ctx->graph_version != ctx->version || ctx->graph_h != h) {
-    if (ctx->graph_exec) {
-      cudaGraphExecDestroy(ctx->graph_exec);
-      ctx->graph_exec = nullptr;
-    }
     ICF_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     const int rc = enqueue_assembly(ctx, h);
     cudaGraph_t g = nullptr;
@@ -1159,6 +1155,22 @@ int icf_launch_assembly(icf_ctx *ctx, double h) {
       return rc;
     }
     if (ec != cudaSuccess) return icf_fail(ctx, ICF_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+    // a new structure usually changes sizes and pointers only: update the
+    // instantiated graph in place when its topology still matches, which
+    // costs far less than instantiating anew
+    if (ctx->graph_exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(ctx->graph_exec, g, &info) == cudaSuccess) {
+        cudaGraphDestroy(g);
+        ctx->graph_version = ctx->version;
+        ctx->graph_h = h;
+        ICF_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+        return ICF_OK;
+      }
+      cudaGetLastError();  // the failed update leaves an error state behind
+      cudaGraphExecDestroy(ctx->graph_exec);
+      ctx->graph_exec = nullptr;
+    }
     const cudaError_t ei = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
     cudaGraphDestroy(g);
     if (ei != cudaSuccess) {

@@ -91,19 +91,39 @@ __device__ __forceinline__ unsigned long long cell_key(int x, int y, int z) {
   return ((unsigned long long)(unsigned)x << 42) | ((unsigned long long)(unsigned)y << 21) | (unsigned)z;
 }
 
-__global__ void k_entries(int n, const int4 *__restrict__ clo, const int *__restrict__ off,
-                          unsigned long long *__restrict__ key, int *__restrict__ elem) {
+// With groups packed into the key (gbits >= 0), an entry's key is
+// (x << 2 nb | y << nb | z) << gbits | group: sorted, the entries of a cell
+// come in runs of one group each.
+__global__ void k_entries(int n, const int4 *__restrict__ clo, const int *__restrict__ off, int nb, int gbits,
+                          const int *__restrict__ group, unsigned long long *__restrict__ key,
+                          int *__restrict__ elem) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int4 c = clo[i];
   int o = off[i];
+  const unsigned long long g = gbits >= 0 ? (unsigned long long)(unsigned)group[i] : 0ull;
   for (int dz = 0; dz <= ((c.w >> 2) & 1); dz++)
     for (int dy = 0; dy <= ((c.w >> 1) & 1); dy++)
       for (int dx = 0; dx <= (c.w & 1); dx++) {
-        key[o] = cell_key(c.x + dx, c.y + dy, c.z + dz);
+        if (gbits >= 0)
+          key[o] = ((((unsigned long long)(unsigned)(c.x + dx) << (2 * nb)) |
+                     ((unsigned long long)(unsigned)(c.y + dy) << nb) | (unsigned long long)(unsigned)(c.z + dz))
+                    << gbits) | g;
+        else
+          key[o] = cell_key(c.x + dx, c.y + dy, c.z + dz);
         elem[o] = i;
         o++;
       }
+}
+
+// first index in [lo, hi) whose key is > v
+__device__ __forceinline__ int upper_key(const unsigned long long *key, int lo, int hi, unsigned long long v) {
+  while (lo < hi) {
+    const int mid = lo + ((hi - lo) >> 1);
+    if (key[mid] <= v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
 }
 
 __device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, const int *group) {
@@ -114,17 +134,25 @@ __device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, cons
   return true;
 }
 
-// entry i pairs with the later entries of its cell; count, then write
+// entry i pairs with the later entries of its cell; count, then write.  With
+// group keys (gbits >= 0) the later entries of its own group are skipped: the
+// candidates are the entries from the end of its (cell, group) run to the end
+// of its cell, found by binary search.
 __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const int *__restrict__ elem,
-                        const double *__restrict__ lohi, const int *__restrict__ group, const int *__restrict__ off,
-                        int *__restrict__ cnt, unsigned long long *__restrict__ out) {
+                        const double *__restrict__ lohi, const int *__restrict__ group, int gbits,
+                        const int *__restrict__ off, int *__restrict__ cnt, unsigned long long *__restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const unsigned long long here = key[i];
   const int a0 = elem[i];
   int c = 0;
   int o = off ? off[i] : 0;
-  for (int j = i + 1; j < m && key[j] == here; j++) {
+  int j0 = i + 1, j1 = m;
+  if (gbits >= 0) {
+    j0 = upper_key(key, i + 1, m, here);  // end of the run of this cell and group
+    j1 = upper_key(key, j0, m, here | ((1ull << gbits) - 1));  // end of the cell
+  }
+  for (int j = j0; j < j1 && (gbits >= 0 || key[j] == here); j++) {
     const int b0 = elem[j];
     const int a = a0 < b0 ? a0 : b0, b = a0 < b0 ? b0 : a0;
     if (keep_pair(a, b, lohi, group)) {
@@ -169,7 +197,7 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
   ICF_CUDA(ctx, cudaMallocAsync(&lohi, sizeof(double) * 6 * (size_t)n, s));
   ICF_CUDA(ctx, cudaMallocAsync(&ext, sizeof(double) * (size_t)n, s));
   ICF_CUDA(ctx, cudaMallocAsync(&tmpv, sizeof(double) * (size_t)n, s));
-  ICF_CUDA(ctx, cudaMallocAsync(&red, sizeof(double) * 4, s));
+  ICF_CUDA(ctx, cudaMallocAsync(&red, sizeof(double) * 7, s));
   ICF_CUDA(ctx, cudaMallocAsync(&cnt, sizeof(int) * (size_t)(n + 1), s));
   ICF_CUDA(ctx, cudaMallocAsync(&off, sizeof(int) * (size_t)(n + 1), s));
   ICF_CUDA(ctx, cudaMallocAsync(&clo, sizeof(int4) * (size_t)n, s));
@@ -185,11 +213,26 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     cub::DeviceReduce::Reduce(nullptr, tb, tmpv, red + 1 + k, n, min_op(), 1e300, s);
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
     ICF_CUDA(ctx, cub::DeviceReduce::Reduce(ctx->d_tmp, tb, tmpv, red + 1 + k, n, min_op(), 1e300, s));
+    // the highest corner, for the cell-index range of the group keys
+    k_strided<<<icf_blocks(n, 256), 256, 0, s>>>(n, lohi, 3 + k, tmpv);
+    tb = 0;
+    cub::DeviceReduce::Reduce(nullptr, tb, tmpv, red + 4 + k, n, max_op(), -1e300, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceReduce::Reduce(ctx->d_tmp, tb, tmpv, red + 4 + k, n, max_op(), -1e300, s));
   }
-  double h_red[4];
+  double h_red[7];
   ICF_CUDA(ctx, cudaMemcpyAsync(h_red, red, sizeof(h_red), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaStreamSynchronize(s));
   if (!(h_red[0] > 0) || !std::isfinite(h_red[0])) return icf_fail(ctx, ICF_ERR_NUMERIC, "broad phase: degenerate boxes");
+  // (cell, group) keys when the cell indices and group ids fit in 63 bits
+  int nb = 1;
+  {
+    double span = 0;
+    for (int k = 0; k < 3; k++) span = fmax(span, (h_red[4 + k] - h_red[1 + k]) / h_red[0]);
+    const double cells = std::isfinite(span) ? span + 2.0 : 1e30;
+    while (nb < 40 && (double)(1ull << nb) < cells) nb++;
+  }
+  const int gbits = (d_group && ctx->sgroup_bits >= 0 && 3 * nb + ctx->sgroup_bits <= 63) ? ctx->sgroup_bits : -1;
   k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, lohi, red, cnt, clo);
   ICF_CUDA(ctx, cudaMemsetAsync(cnt + n, 0, sizeof(int), s));
   tb = 0;
@@ -207,12 +250,13 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
   ICF_CUDA(ctx, cudaMallocAsync(&e1, sizeof(int) * (size_t)m, s));
   ICF_CUDA(ctx, cudaMallocAsync(&pc, sizeof(int) * (size_t)(m + 1), s));
   ICF_CUDA(ctx, cudaMallocAsync(&po, sizeof(int) * (size_t)(m + 1), s));
-  k_entries<<<icf_blocks(n, 256), 256, 0, s>>>(n, clo, off, k0, e0);
+  k_entries<<<icf_blocks(n, 256), 256, 0, s>>>(n, clo, off, nb, gbits, d_group, k0, e0);
+  const int end_bit = gbits >= 0 ? 3 * nb + gbits : 63;
   tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, e0, e1, m, 0, 63, s);
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, e0, e1, m, 0, end_bit, s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-  ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, e0, e1, m, 0, 63, s));
-  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, k1, e1, lohi, d_group, nullptr, pc, nullptr);
+  ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, e0, e1, m, 0, end_bit, s));
+  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, k1, e1, lohi, d_group, gbits, nullptr, pc, nullptr);
   ICF_CUDA(ctx, cudaMemsetAsync(pc + m, 0, sizeof(int), s));
   tb = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb, pc, po, m + 1, s);
@@ -227,7 +271,7 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     ICF_CUDA(ctx, cudaMallocAsync(&p0, sizeof(unsigned long long) * (size_t)nall, s));
     ICF_CUDA(ctx, cudaMallocAsync(&p1, sizeof(unsigned long long) * (size_t)nall, s));
     ICF_CUDA(ctx, cudaMallocAsync(&d_np, sizeof(int), s));
-    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, k1, e1, lohi, d_group, po, nullptr, p0);
+    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, k1, e1, lohi, d_group, gbits, po, nullptr, p0);
     tb = 0;
     cub::DeviceRadixSort::SortKeys(nullptr, tb, p0, p1, nall, 0, 64, s);
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;

@@ -72,7 +72,8 @@ struct icf_sell {
   long long n_codes = 0, codes_cap = 0;  // code slots, padding included
   long long n_real = 0;                   // contribution codes of the units (no padding)
   int4 *meta = nullptr;
-  int2 *unit = nullptr;
+  int2 *unit = nullptr;    // merged slots of the current structure
+  int2 *unit_s = nullptr;  // static slots (the lists are built once per static pattern)
   uint32_t *codes = nullptr;
 };
 
@@ -227,6 +228,9 @@ struct icf_ctx {
   // touched blocks of the impacts that the off-diagonal list gather writes
   // (static, off the diagonal): their impact terms wait for that gather
   int n_crs_off = 0;
+  // the gather lists exist for the current static pattern, layout and split
+  // (their units in static slots; each structure only remaps the slots)
+  bool lists_static = false;
 
   // merged pattern
   int *d_rows = nullptr, *d_cols = nullptr, *d_src = nullptr;
@@ -249,6 +253,7 @@ struct icf_ctx {
   int n_pairs = 0, pairs_cap = 0;
   int *d_pairs = nullptr, *d_masks = nullptr;
   int *d_sgroup = nullptr;  // group (mesh) of every surface element, or null
+  int sgroup_bits = -1;     // bits of the largest group id; -1: none set or some negative
   bool pairs_from_broad = false;
 
   // node incidence lists for the node forces
@@ -327,7 +332,8 @@ int icf_gather_tile_setup(icf_ctx *ctx);
 bool icf_tiles_active(const icf_ctx *ctx);
 int icf_launch_gather_tile(icf_ctx *ctx, const double4 *es, const double *cs, double sc, double mc, double lam,
                            double mu, double *vals, double *rhs, cudaStream_t s);
-int icf_rebuild_lists(icf_ctx *ctx);
+int icf_rebuild_lists(icf_ctx *ctx);  // both gathers' lists for the current layout and split
+int icf_remap_lists(icf_ctx *ctx);    // their units' slots for the current structure
 // 1 for a merged slot that the off-diagonal gather writes: static, off the diagonal
 __host__ __device__ inline bool icf_off_static(const unsigned long long *mkey, const int *src, int identity, int s) {
   const unsigned long long k = mkey[s];

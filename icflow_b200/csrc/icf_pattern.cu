@@ -574,11 +574,14 @@ static int build_sell(icf_ctx *ctx, const int4 *desc, int n, int wl, bool with_r
   if (ns > S->slices_cap || !S->meta) {
     cudaFree(S->meta);
     cudaFree(S->unit);
+    cudaFree(S->unit_s);
+    S->unit_s = nullptr;
     S->meta = nullptr;
     S->unit = nullptr;
     const int cap = ns + ns / 4 + 16;
     ICF_CUDA(ctx, cudaMalloc(&S->meta, sizeof(int4) * (size_t)cap));
     ICF_CUDA(ctx, cudaMalloc(&S->unit, sizeof(int2) * (size_t)cap * per));
+    ICF_CUDA(ctx, cudaMalloc(&S->unit_s, sizeof(int2) * (size_t)cap * per));
     S->slices_cap = cap;
   }
   uint32_t *k0, *k1;
@@ -600,9 +603,9 @@ static int build_sell(icf_ctx *ctx, const int4 *desc, int n, int wl, bool with_r
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
     ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, i0, perm, n, 0, end_bit, s));
   }
-  ICF_CUDA(ctx, cudaMemsetAsync(S->unit, 0xff, sizeof(int2) * (size_t)ns * per, s));
+  ICF_CUDA(ctx, cudaMemsetAsync(S->unit_s, 0xff, sizeof(int2) * (size_t)ns * per, s));
   k_sell_count<<<icf_blocks(32LL * ns, 256), 256, 0, s>>>(n, ns, S->lanes, perm, desc, with_row ? 1 : 0, row_of,
-                                                         S->meta, cnt, S->unit);
+                                                         S->meta, cnt, S->unit_s);
   ICF_CUDA(ctx, cudaMemsetAsync(cnt + ns, 0, sizeof(int), s));
   tb = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, ns + 1, s);
@@ -804,18 +807,23 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
     ctx->gdesc_cap = N + ctx->n_offd + 2;
   }
   ctx->d_gdesc_off = ctx->d_gdesc_diag + N + 1;
-  const int ident = nd == 0 ? 1 : 0;
-  if (N > 0)
-    k_desc<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_diag, ctx->d_rc_off, ctx->d_rc_mid, ctx->d_s2m,
-                                             ident, ctx->d_gdesc_diag);
-  if (ctx->n_offd > 0)
-    k_desc<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_offd, ctx->d_rc_off,
-                                                       ctx->d_rc_mid, ctx->d_s2m, ident, ctx->d_gdesc_off);
-  ctx->sell_off.lanes = ctx->sell_off_cz.lanes = 1;
-  ctx->sell_off.natural = ctx->sell_off_cz.natural = icf_gather_variant_natural(ctx->tune_off);
-  ctx->sell_diag.lanes = ctx->sell_diag_cz.lanes = icf_gather_variant_lanes(ctx->tune_diag);
-  if (build_lists(ctx, true, true)) return ICF_ERR_CUDA;
-  if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
+  // the gather lists depend on the static pattern only: built once, in
+  // static slots, then mapped to the merged slots of every structure
+  if (!ctx->lists_static) {
+    if (N > 0)
+      k_desc<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_diag, ctx->d_rc_off, ctx->d_rc_mid, nullptr, 1,
+                                               ctx->d_gdesc_diag);
+    if (ctx->n_offd > 0)
+      k_desc<<<icf_blocks(ctx->n_offd, 256), 256, 0, s>>>(ctx->n_offd, ctx->d_offd, ctx->d_rc_off,
+                                                         ctx->d_rc_mid, nullptr, 1, ctx->d_gdesc_off);
+    ctx->sell_off.lanes = ctx->sell_off_cz.lanes = 1;
+    ctx->sell_off.natural = ctx->sell_off_cz.natural = icf_gather_variant_natural(ctx->tune_off);
+    ctx->sell_diag.lanes = ctx->sell_diag_cz.lanes = icf_gather_variant_lanes(ctx->tune_diag);
+    if (build_lists(ctx, true, true)) return ICF_ERR_CUDA;
+    if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
+    ctx->lists_static = true;
+  }
+  if (icf_remap_lists(ctx)) return ICF_ERR_CUDA;
   if (ctx->tiles.built && icf_remap_tiles(ctx)) return ICF_ERR_CUDA;
   if (dkeys) ICF_CUDA(ctx, cudaFreeAsync(dkeys, s));
   if (nnz > 0) k_cols<<<icf_blocks(nnz, 256), 256, 0, s>>>(nnz, ctx->d_mkeys, ctx->d_cols);
@@ -934,10 +942,31 @@ int icf_launch_pcsr(icf_ctx *ctx, int kind, int *d_out) {
   return ICF_OK;
 }
 
+__global__ void k_remap_units(long long n, const int2 *__restrict__ us, const int *__restrict__ s2m, int identity,
+                              int2 *__restrict__ u) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int2 v = us[i];
+  if (v.x >= 0 && !identity) v.x = s2m[v.x];
+  u[i] = v;
+}
+
+int icf_remap_lists(icf_ctx *ctx) {
+  const int ident = (ctx->src_identity || !ctx->d_s2m) ? 1 : 0;
+  for (icf_sell *L : {&ctx->sell_off, &ctx->sell_diag, &ctx->sell_off_cz, &ctx->sell_diag_cz}) {
+    if (L->n_slices == 0) continue;
+    const long long n = (long long)(32 / L->lanes) * L->n_slices;  // units per slice: 32 / lanes
+    k_remap_units<<<icf_blocks(n, 256), 256, 0, ctx->stream>>>(n, L->unit_s, ctx->d_s2m, ident, L->unit);
+  }
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
 int icf_rebuild_lists(icf_ctx *ctx) {
   if (!ctx->have_structure) return icf_fail(ctx, ICF_ERR_STATE, "icf_create_structure first");
   if (build_lists(ctx, true, true)) return ICF_ERR_CUDA;
   if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
+  if (icf_remap_lists(ctx)) return ICF_ERR_CUDA;
   ctx->version++;
   return ICF_OK;
 }
@@ -947,6 +976,7 @@ int icf_rebuild_sell_diag(icf_ctx *ctx, int lanes) {
   ctx->sell_diag.lanes = ctx->sell_diag_cz.lanes = lanes;
   if (build_lists(ctx, false, true)) return ICF_ERR_CUDA;
   if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
+  if (icf_remap_lists(ctx)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ICF_OK;
 }
@@ -956,6 +986,7 @@ int icf_rebuild_sell_off(icf_ctx *ctx, bool natural) {
   ctx->sell_off.natural = ctx->sell_off_cz.natural = natural;
   if (build_lists(ctx, true, false)) return ICF_ERR_CUDA;
   if (icf_build_contrib(ctx)) return ICF_ERR_CUDA;
+  if (icf_remap_lists(ctx)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ICF_OK;
 }
