@@ -33,6 +33,7 @@ __device__ __forceinline__ void ld_node(const double4 *__restrict__ p, int i,
   asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
       : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(w)
       : "l"(p + i));
+  asm("" ::"d"(w));  // the fourth component is padding
 }
 
 // Orthonormal frame of three points as in fastRotationMatrix

@@ -21,6 +21,7 @@
 // narrow phase would drop most of them anyway for sharing nodes).
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 
@@ -170,17 +171,65 @@ __global__ void k_unpack_pairs(int n, const unsigned long long *__restrict__ in,
   pairs[2 * (size_t)i + 1] = (int)(in[i] & 0xffffffffull);
 }
 
-struct min_op {
-  __device__ double operator()(double a, double b) const { return a < b ? a : b; }
-};
-struct max_op {
-  __device__ double operator()(double a, double b) const { return a > b ? a : b; }
-};
 
-// red[0] = cell size (largest extent), red[1..3] = lowest corner
-__global__ void k_strided(int n, const double *__restrict__ lohi, int k, double *__restrict__ out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = lohi[6 * (size_t)i + k];
+
+// red[0] = cell size (largest extent), red[1..3] = lowest corner, red[4..6] =
+// highest corner: one pass, per block then one block over the partials
+// (min and max are exact, so the order does not matter)
+__device__ __forceinline__ void red7_block(double v[7]) {
+  __shared__ double sh[7][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 7; q++) {
+    const bool mn = q >= 1 && q <= 3;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double t = __shfl_xor_sync(0xffffffffu, v[q], o);
+      v[q] = mn ? fmin(v[q], t) : fmax(v[q], t);
+    }
+    if (lane == 0) sh[q][w] = v[q];
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 7; q++) {
+      const bool mn = q >= 1 && q <= 3;
+      v[q] = lane < nw ? sh[q][lane] : (mn ? 1e300 : -1e300);
+      for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, v[q], o);
+        v[q] = mn ? fmin(v[q], t) : fmax(v[q], t);
+      }
+    }
+  }
+}
+__global__ void k_red7(int n, const double *__restrict__ lohi, const double *__restrict__ ext,
+                       double *__restrict__ part) {
+  double v[7] = {-1e300, 1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    v[0] = fmax(v[0], ext[i]);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      v[1 + k] = fmin(v[1 + k], lohi[6 * (size_t)i + k]);
+      v[4 + k] = fmax(v[4 + k], lohi[6 * (size_t)i + 3 + k]);
+    }
+  }
+  red7_block(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 7; q++) part[7 * (size_t)blockIdx.x + q] = v[q];
+}
+__global__ void k_red7_final(int nb, const double *__restrict__ part, double *__restrict__ red) {
+  double v[7] = {-1e300, 1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < 7; q++) {
+      const bool mn = q >= 1 && q <= 3;
+      v[q] = mn ? fmin(v[q], part[7 * (size_t)b + q]) : fmax(v[q], part[7 * (size_t)b + q]);
+    }
+  red7_block(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 7; q++) red[q] = v[q];
 }
 
 }  // namespace
@@ -196,7 +245,8 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
   int4 *clo;
   ICF_CUDA(ctx, cudaMallocAsync(&lohi, sizeof(double) * 6 * (size_t)n, s));
   ICF_CUDA(ctx, cudaMallocAsync(&ext, sizeof(double) * (size_t)n, s));
-  ICF_CUDA(ctx, cudaMallocAsync(&tmpv, sizeof(double) * (size_t)n, s));
+  // per-block partials of the corner and extent reduction
+  ICF_CUDA(ctx, cudaMallocAsync(&tmpv, sizeof(double) * 7 * (size_t)(2 * ctx->n_sm + 1), s));
   ICF_CUDA(ctx, cudaMallocAsync(&red, sizeof(double) * 7, s));
   ICF_CUDA(ctx, cudaMallocAsync(&cnt, sizeof(int) * (size_t)(n + 1), s));
   ICF_CUDA(ctx, cudaMallocAsync(&off, sizeof(int) * (size_t)(n + 1), s));
@@ -204,21 +254,10 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
   ICF_CUDA(ctx, cudaMemsetAsync(ext, 0, sizeof(double), s));
   k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, lohi, ext);
   size_t tb = 0;
-  cub::DeviceReduce::Reduce(nullptr, tb, ext, red, n, max_op(), 0.0, s);
-  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-  ICF_CUDA(ctx, cub::DeviceReduce::Reduce(ctx->d_tmp, tb, ext, red, n, max_op(), 0.0, s));
-  for (int k = 0; k < 3; k++) {
-    k_strided<<<icf_blocks(n, 256), 256, 0, s>>>(n, lohi, k, tmpv);
-    tb = 0;
-    cub::DeviceReduce::Reduce(nullptr, tb, tmpv, red + 1 + k, n, min_op(), 1e300, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceReduce::Reduce(ctx->d_tmp, tb, tmpv, red + 1 + k, n, min_op(), 1e300, s));
-    // the highest corner, for the cell-index range of the group keys
-    k_strided<<<icf_blocks(n, 256), 256, 0, s>>>(n, lohi, 3 + k, tmpv);
-    tb = 0;
-    cub::DeviceReduce::Reduce(nullptr, tb, tmpv, red + 4 + k, n, max_op(), -1e300, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceReduce::Reduce(ctx->d_tmp, tb, tmpv, red + 4 + k, n, max_op(), -1e300, s));
+  {
+    const int nbk = (int)std::min<long long>((n + 255) / 256, 2LL * ctx->n_sm);
+    k_red7<<<nbk, 256, 0, s>>>(n, lohi, ext, tmpv);
+    k_red7_final<<<1, 256, 0, s>>>(nbk, tmpv, red);
   }
   double h_red[7];
   ICF_CUDA(ctx, cudaMemcpyAsync(h_red, red, sizeof(h_red), cudaMemcpyDeviceToHost, s));
