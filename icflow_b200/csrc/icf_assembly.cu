@@ -921,11 +921,14 @@ int icf_launch_tet(icf_ctx *ctx, int variant, const double4 *xc, const double2 *
 
 // ---- host launchers --------------------------------------------------------------
 // One assembly as a fork/join DAG over three streams:
-//   main : memsets | tets ............ | wait CZ -> diagonal gather | join -> contact add, checks
+//   main : memsets | tets ............ | wait CZ -> diagonal gather | wait aux1 -> contact add
+//          (diagonal and contact-only blocks) | join -> contact add (static off-diagonal blocks)
 //   aux0 :         | CZs | wait tets -> off-diagonal gather ........|
 //   aux1 :         | zero contact-only blocks, impact units .........|
-// The unit kernels are occupancy- or latency-limited on their own, so running
-// them side by side fills the machine; the gathers write disjoint blocks.
+// (or, per the tuner, both gathers on main, or one tiled gather, or split
+// lists).  The unit kernels are occupancy- or latency-limited on their own, so
+// running them side by side fills the machine; the gathers write disjoint
+// blocks.
 static icf_law_c make_law_c(const icf_ctx *ctx, const icf_dprm &P) {
   icf_law_c LC;
   LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
