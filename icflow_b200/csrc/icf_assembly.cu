@@ -962,7 +962,10 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   cudaEvent_t e_fork = ctx->ev[0], e_cz = ctx->ev[1], e_tet = ctx->ev[2], e_a = ctx->ev[3],
               e_b = ctx->ev[4];
   ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, 8 * sizeof(int), s));
-  ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
+  // the diagonal list gathers write every row's rhs (rows without a diagonal
+  // block too); the row tiles hold only rows with one
+  if (icf_tiles_active(ctx))
+    ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
   if (ctx->prof) ICF_CUDA(ctx, cudaEventRecord(ctx->prof->ev[0], s));
   ICF_CUDA(ctx, cudaEventRecord(e_fork, s));
   ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_fork, 0));
@@ -1268,7 +1271,8 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
   ICF_TRY_RC(icf_ensure_cz_hist(ctx, s));
   const icf_dprm P = icf_make_dprm(ctx);
   ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, 8 * sizeof(int), s));
-  ICF_CUDA(ctx, cudaMemsetAsync(B.rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
+  if (icf_tiles_active(ctx))
+    ICF_CUDA(ctx, cudaMemsetAsync(B.rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
   k_pack_nodes<<<icf_blocks(ctx->n_nodes, 256), 256, 0, s>>>(ctx->n_nodes, ctx->d_x0, B.un, B.vn, B.an,
                                                             B.xc, B.va);
   if (ctx->n_elem > 0)
