@@ -1077,18 +1077,24 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   // (diagonal blocks, written on main, and contact-only blocks, zeroed on
   // aux1) as soon as the impacts are staged; the others after the join
   const int ident = ctx->src_identity ? 1 : 0;
+  // algorithmic bytes: the impact staging once, 172 B per touched block and
+  // 4 B per code, split between the two launches by their blocks
+  const long long imp_in = 8LL * ICF_IMP_STAGE * ctx->n_imp + 4LL * 16 * ctx->n_imp;
+  const int n_a = ctx->n_crs - ctx->n_crs_off;
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
-  if (ctx->n_crs > ctx->n_crs_off)
+  if (n_a > 0) {
     k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(
         ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
         ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 1);
+    icf_prof_mark(ctx, s, "k_imp_add", imp_in * n_a / ctx->n_crs + 172LL * n_a);
+  }
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
-  if (ctx->n_crs_off > 0)
+  if (ctx->n_crs_off > 0) {
     k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(
         ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
         ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 2);
-  if (ctx->n_crs > 0)
-    icf_prof_mark(ctx, s, "k_imp_add", 8LL * ICF_IMP_STAGE * ctx->n_imp + 172LL * ctx->n_crs + 4LL * 16 * ctx->n_imp);
+    icf_prof_mark(ctx, s, "k_imp_add_off", imp_in * ctx->n_crs_off / ctx->n_crs + 172LL * ctx->n_crs_off);
+  }
 
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int),
