@@ -75,8 +75,8 @@ class icf_kernel_times(C.Structure):
 
 
 class icf_tune_report(C.Structure):
-    _fields_ = [("n", C.c_int), ("kernel", (C.c_char * 16) * 32), ("variant", (C.c_char * 32) * 32),
-                ("ms", C.c_double * 32), ("chosen", C.c_int * 32)]
+    _fields_ = [("n", C.c_int), ("kernel", (C.c_char * 16) * 64), ("variant", (C.c_char * 32) * 64),
+                ("ms", C.c_double * 64), ("chosen", C.c_int * 64)]
 
     def as_list(self):
         s = lambda b: bytes(b).split(b"\0")[0].decode()  # noqa: E731

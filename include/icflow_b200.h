@@ -230,7 +230,7 @@ int icf_profile_assembly(icf_ctx *ctx, double h, int reps, icf_kernel_times *out
  * records and codes staged in shared memory, built on the host at the first
  * structure that needs it).  The tuner also times whole
  * assemblies with each layout and split first. */
-#define ICF_MAX_TUNE 32
+#define ICF_MAX_TUNE 64
 typedef struct icf_tune_report {
   int n;                          /* candidates timed */
   char kernel[ICF_MAX_TUNE][16];
