@@ -884,11 +884,6 @@ __global__ void __launch_bounds__(TILE_THREADS, MINB)
 #define OFFV(MB, U)                                                                                   \
   {"reg minb" #MB " u" #U, k_gather_off<fp64, MB, U>, k_gather_off<fp32mixed, MB, U>,                \
    k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, 0, false}
-// FP32-mixed records are half the size: twice the codes per iteration in the
-// same registers (FP64 keeps U)
-#define OFFW(MB, U)                                                                                   \
-  {"reg minb" #MB " u" #U " (x2 mixed)", k_gather_off<fp64, MB, U>, k_gather_off<fp32mixed, MB, 2 * U>, \
-   k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, 0, false}
 #define OFFN(MB, U)                                                                                   \
   {"natural minb" #MB " u" #U, k_gather_off_nat<fp64, MB, U>, k_gather_off_nat<fp32mixed, MB, U>,   \
    k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, 0, true}
@@ -905,12 +900,11 @@ __global__ void __launch_bounds__(TILE_THREADS, MINB)
   {"pipe L" #L " minb" #MB " u" #U, L, k_gather_diag_pipe<fp64, L, MB, U>,                           \
    k_gather_diag_pipe<fp32mixed, L, MB, U>, k_gather_diag_c<fp64, false, L, MB, U>,                  \
    k_gather_diag_c<fp32mixed, true, L, MB, U>, MB}
-const off_variant OFF_VARIANTS[] = {OFFV(4, 4), OFFV(3, 2), OFFV(2, 4), OFFV(4, 2), OFFW(4, 4), OFFP(4, 2), OFFP(3, 4),
+const off_variant OFF_VARIANTS[] = {OFFV(4, 4), OFFV(3, 2), OFFV(2, 4), OFFV(4, 2), OFFP(4, 2), OFFP(3, 4),
                                     OFFN(4, 2), OFFN(4, 4), OFFN(3, 2), OFFS(4, 2), OFFS(4, 4)};
 const diag_variant DIAG_VARIANTS[] = {DIAGV(4, 4, 4), DIAGV(2, 3, 4), DIAGV(4, 2, 4), DIAGV(8, 4, 2),
                                       DIAGV(2, 4, 2), DIAGP(4, 4, 2), DIAGP(8, 4, 2)};
 #undef OFFV
-#undef OFFW
 #undef OFFN
 #undef OFFS
 #undef OFFP
