@@ -420,4 +420,12 @@ def test_device_broad_phase_matches_host_pairs(O):
         imps_dev = gf.NarrowPhaseCollisionDetection(None).copy()
         imps_host = gf.NarrowPhaseCollisionDetection(host).copy()
         assert np.array_equal(imps_dev, imps_host)
+        # group ids that do not fit the (cell, group) keys (a negative one)
+        # take the per-cell scan; the pair set is the same
+        from icflow_b200 import _lib
+        grp = np.ascontiguousarray(coll.selem_mesh, np.int32) - 1
+        _lib.check(gf.ctx, gf.lib.icf_set_surface_groups(gf.ctx, len(grp), _lib.iptr(grp)))
+        n2 = C.c_int()
+        _lib.check(gf.ctx, gf.lib.icf_broad_phase(gf.ctx, 0.0, C.byref(n2)))
+        assert n2.value == len(host) and np.array_equal(gf.GetPairs(), host)
         gf.close()
