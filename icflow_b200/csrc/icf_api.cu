@@ -218,7 +218,7 @@ static void free_all(icf_ctx *c) {
                   c->sell_off_cz.meta, c->sell_off_cz.unit, c->sell_off_cz.codes, c->sell_diag_cz.meta,
                   c->sell_diag_cz.unit, c->sell_diag_cz.codes, c->sell_off.unit_s, c->sell_diag.unit_s,
                   c->sell_off_cz.unit_s, c->sell_diag_cz.unit_s, c->d_czhist,
-                  c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup};
+                  c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup, c->d_imp_built};
   for (void *p : ptrs) cudaFree(p);
 }
 
@@ -359,6 +359,9 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->sell_off_cz = icf_sell();
   ctx->sell_diag_cz = icf_sell();
   ctx->lists_static = false;
+  ctx->d_imp_built = nullptr;
+  ctx->imp_built_cap = 0;
+  ctx->n_imp_built = -1;
   ctx->d_czhist = nullptr;
   ctx->hist_valid = false;
   ctx->d_tetpos = nullptr;
@@ -595,12 +598,61 @@ int icf_set_impacts(icf_ctx *ctx, int n_impacts, const int *impacts) {
   return ICF_OK;
 }
 
+__global__ void k_imp_differ(int n, const int4 *__restrict__ a, const int4 *__restrict__ b, int *__restrict__ flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 x = a[i], y = b[i];
+  if (x.x != y.x || x.y != y.y || x.z != y.z || x.w != y.w) *flag = 1;
+}
+
+// 1 when the current impacts are those the merged structure was built from.
+static int same_impacts(icf_ctx *ctx, bool *same) {
+  *same = false;
+  if (ctx->n_imp_built < 0 || ctx->n_imp != ctx->n_imp_built) return ICF_OK;
+  if (ctx->n_imp == 0) {
+    *same = true;
+    return ICF_OK;
+  }
+  ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_norm, 0, sizeof(int), ctx->stream));
+  k_imp_differ<<<icf_blocks(ctx->n_imp, 256), 256, 0, ctx->stream>>>(ctx->n_imp, ctx->d_imp, ctx->d_imp_built,
+                                                                    reinterpret_cast<int *>(ctx->d_norm));
+  int differ = 1;
+  ICF_CUDA(ctx, cudaMemcpyAsync(&differ, ctx->d_norm, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *same = differ == 0;
+  return ICF_OK;
+}
+
 int icf_create_structure(icf_ctx *ctx, int *N, int *nnz) {
   ICF_CHECK_CTX(ctx);
   if (!ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "icf_transfer_static first");
+  // The reference rebuilds the structure every Newton iteration
+  // (ImplicitModel3.cs:389).  The structure depends only on the static
+  // pattern and the impact list, so when the list is the one the current
+  // structure was built from, the structure, the gather lists and the
+  // captured assembly graph all stay as they are.
+  bool same = false;
+  if (ctx->d_skeys) ICF_TRY(same_impacts(ctx, &same));
+  if (same) {
+    ctx->have_structure = true;
+    if (N) *N = ctx->N;
+    if (nnz) *nnz = ctx->nnz;
+    return ICF_OK;
+  }
   if (!ctx->d_skeys) ICF_TRY(icf_build_static_pattern(ctx));
   ICF_TRY(icf_build_merged_pattern(ctx));
   if (ctx->gather_tiles && !ctx->tiles.built) ICF_TRY(icf_build_tiles(ctx));
+  // remember the impacts this structure holds
+  if (ctx->n_imp > ctx->imp_built_cap) {
+    cudaFree(ctx->d_imp_built);
+    ctx->d_imp_built = nullptr;
+    ICF_TRY(dalloc(ctx, &ctx->d_imp_built, 2 * (size_t)ctx->n_imp));
+    ctx->imp_built_cap = 2 * ctx->n_imp;
+  }
+  if (ctx->n_imp)
+    ICF_CUDA(ctx, cudaMemcpyAsync(ctx->d_imp_built, ctx->d_imp, sizeof(int4) * (size_t)ctx->n_imp,
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+  ctx->n_imp_built = ctx->n_imp;
   ctx->have_structure = true;
   ctx->struct_gen++;
   ctx->version++;

@@ -240,6 +240,10 @@ struct icf_ctx {
   // impacts and their contributions
   int n_imp = 0, imp_cap = 0;
   int4 *d_imp = nullptr;
+  // the impact list the current merged structure was built from (-1: none);
+  // a structure request with the same list keeps the structure
+  int n_imp_built = -1, imp_built_cap = 0;
+  int4 *d_imp_built = nullptr;
   // per-impact classification {kind, ia, ib, 0} and {s, t, dsq, 0}; same
   // capacity as the impact staging d_ks (ks_cap)
   int4 *d_imp_ci = nullptr;
