@@ -230,6 +230,32 @@ def test_graph_matches_direct_launch(O):
     gf.close()
 
 
+def test_structure_kept_for_the_same_impacts(O):
+    """A structure request with the impact list the current structure holds
+    keeps it (same pattern, same bits); a different list rebuilds it, and
+    the assembly matches the oracle either way."""
+    coll = M.polycrystal(n=6, grains=5, seed=4, platens=True, gap=-0.3)
+    prms = config_prms(penaltyK=1e8)
+    gf = _gf(coll, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    p = orc_prms_from(O, prms)
+    state = random_state(coll, 2, du=1e-6)
+    pairs = M.candidate_pairs(coll, coll.x0 + state[0])
+    a = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+    assert len(gf.c_itet) > 0
+    b = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)  # same impacts
+    for k in ("rows", "cols", "vals", "rhs", "ipcsr"):
+        assert np.array_equal(a[k], b[k]), k
+    # fewer pairs, fewer impacts: a new structure
+    c = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs[: len(pairs) // 2])
+    compare(c, oracle_assemble(O, p, coll, state, H, pmax, tmax, gf.c_itet))
+    # and back to the first list
+    d = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
+    for k in ("rows", "cols", "vals", "rhs"):
+        assert np.array_equal(a[k], d[k]), k
+    gf.close()
+
+
 def test_profile_assembly_kernels(O):
     """Per-kernel timing runs the same kernels: same bits as the graph, every
     kernel of the step listed with a positive time and byte count."""
