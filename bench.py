@@ -410,8 +410,8 @@ def run_ours(args):
         full_iter = {"value": reps / (t_s[0] + t_s[1]), "unit": "iterations/s",
                      "structure_ms": 1000 * t_s[0] / reps, "assembly_ms": 1000 * t_s[1] / reps,
                      "pairs": gf.nPairs, "impacts": gf.nImpacts,
-                     "scope": "device broad phase + narrow phase + structure rebuild + synchronous assembly, "
-                              "host wall clock; no linear solve"}
+                     "scope": "device broad phase + narrow phase + structure request (kept when the impact list "
+                              "is unchanged, as here) + synchronous assembly, host wall clock; no linear solve"}
 
     # per-kernel device times: the same kernels run in the graph's order on
     # one stream with an event after each (no overlap between streams)
