@@ -3,12 +3,14 @@
 One step = one Newton assembly (zero + tetrahedra + cohesive zones with damage
 state and flags + contact response -> BCSR values and rhs) of a fixed
 structure.  Workloads (--workload):
-  cfg1 (default)  polycrystal compression: 1 mm cube, 32^3 hexahedra split into
+  cfg1            polycrystal compression: 1 mm cube, 32^3 hexahedra split into
                   196,608 tets, 128 Voronoi grains with cohesive zones on every
                   grain boundary (per-boundary lognormal strengths, mean 1 MPa,
                   cv 0.2), two rigid platens overlapping the cube by a quarter
                   cell (penalty 1e8), dt = 1e-5 s, FP64;
-  cfg2            the same at 64^3 hexahedra (1,572,864 tets), 2048 grains;
+  cfg2 (default)  the same at 64^3 hexahedra (1,572,864 tets), 2048 grains: the
+                  1.5M-tet size the throughput target is stated at; the line
+                  also carries the FP32-mixed measurement of the same workload;
   cfg3            64 independent cubes of uneven size (tets U[5k, 60k], grains
                   U[8, 64]) assembled together in one graph launch, launch
                   variants autotuned, FP32-mixed by default.
@@ -114,6 +116,22 @@ def algorithmic_bytes(nnz, n_active, n_nodes, n_tet, n_cz, n_imp) -> int:
     return 72 * nnz + 24 * n_active + 96 * n_nodes + 56 * n_tet + 240 * n_cz + 56 * n_imp
 
 
+def kernel_share_bytes(name, nnz, n_rows, n_nodes, n_tet, n_cz, n_imp) -> int:
+    """The part of algorithmic_bytes a kernel is responsible for: the node
+    state and tet ids to the tet kernel, the CZ items to the CZ kernel, the
+    off-diagonal blocks (contact-only ones included) to the off-diagonal
+    gather, the diagonal blocks and rhs rows to the diagonal gather, the
+    impact items to the impact derivatives; the row-tile gather writes both
+    kinds of blocks.  Summed over one assembly's kernels this is
+    algorithmic_bytes."""
+    return {"k_tet_unit": 96 * n_nodes + 56 * n_tet,
+            "k_cz_gp": 240 * n_cz,
+            "k_gather_off": 72 * (nnz - n_rows),
+            "k_gather_diag": 72 * n_rows + 24 * n_rows,
+            "k_gather_tile": 72 * nnz + 24 * n_rows,
+            "k_imp_deriv": 56 * n_imp}.get(name, 0)
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
 
@@ -195,16 +213,18 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str, workload: str):
-    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
-    summary, if it holds a capture of this workload."""
+def ncu_traffic(workload: str, precision: str):
+    """DRAM bytes (read + write) per launch of each kernel, from the committed
+    summary of an ncu capture of this workload (profiles/dram_traffic.json,
+    which names the command and the code it was taken on), or {}."""
     p = ROOT / "profiles" / "dram_traffic.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get(workload, {}).get(kernel)
+            d = json.loads(p.read_text()).get(workload, {})
+            return d.get(precision, {}) if isinstance(d.get(precision), dict) else {}
         except (ValueError, OSError):
-            return None
-    return None
+            return {}
+    return {}
 
 
 def cpu_baseline(coll, state, sig, pairs, bound_s: float = 12.0, nthreads: int = 0):
@@ -286,6 +306,36 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _device_ms(gf, lib, stream, flush, steps, warmup, barrier, H_):
+    """Mean device time of `steps` assemblies (graph launches) with the inputs
+    resident in HBM: CUDA events on the launching stream around each launch, L2
+    flushed by a 256 MiB write between launches, outside the events."""
+    import torch
+
+    from icflow_b200 import _lib
+
+    for _ in range(warmup):
+        rc = lib.icf_assemble_async(gf.ctx, H_)
+        if rc:
+            _lib.check(gf.ctx, rc)
+    cnt = _lib.icf_counts()
+    _lib.check(gf.ctx, lib.icf_read_counts(gf.ctx, C.byref(cnt)))
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    barrier()
+    with torch.cuda.stream(stream):
+        for i in range(steps):
+            flush.zero_()
+            starts[i].record(stream)
+            rc = lib.icf_assemble_async(gf.ctx, H_)
+            if rc:
+                _lib.check(gf.ctx, rc)
+            ends[i].record(stream)
+    barrier()
+    _lib.check(gf.ctx, lib.icf_read_counts(gf.ctx, C.byref(cnt)))
+    return float(np.mean([a.elapsed_time(b) for a, b in zip(starts, ends)])), cnt
+
+
 def run_ours(args):
     import torch
 
@@ -314,6 +364,7 @@ def run_ours(args):
     gf.mc = coll
     gf.SetConstants()
     precision = args.precision or ("mixed" if batched else "fp64")
+    other = "fp64" if precision == "mixed" else "mixed"
     gf.SetPrecision(1 if precision == "mixed" else 0)
     gf.TransferStaticDataToDevice()
     gf.SetCZStrengths(sig, sig)
@@ -331,38 +382,16 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(bufs.stream, device=dev)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
 
-    def assemble_async():
-        rc = lib.icf_assemble_async(gf.ctx, H)
-        if rc:
-            _lib.check(gf.ctx, rc)
-
-    # warm-up
-    for _ in range(args.warmup):
-        assemble_async()
-    cnt = _lib.icf_counts()
-    _lib.check(gf.ctx, lib.icf_read_counts(gf.ctx, C.byref(cnt)))
-
     def barrier():
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize(dev)
 
-    # device-resident timing, L2 flushed between steps outside the events
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with ClockSampler(dev) as clk:
-        barrier()
-        with torch.cuda.stream(stream):
-            for i in range(args.steps):
-                flush.zero_()
-                starts[i].record(stream)
-                assemble_async()
-                ends[i].record(stream)
-        barrier()
-        ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-        ms_dev = float(np.mean(ms))
+        ms_dev, cnt = _device_ms(gf, lib, stream, flush, args.steps, args.warmup, barrier, H)
 
-        # end to end through the C ABI with pinned host buffers
+        # end to end through the C ABI with pinned host buffers: H2D of un, vn,
+        # an; the assembly; D2H of vals and rhs, every step
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
         hun, hvn, han = pin(un), pin(vn), pin(an)
         hvals = torch.empty(9 * nnz, dtype=torch.float64).pin_memory().numpy()
@@ -383,8 +412,29 @@ def run_ours(args):
         barrier()
         ms_e2e = e0.elapsed_time(e1) / args.steps
     clocks = clk.summary()
-    # full Newton iteration without the solve: device broad phase, narrow
-    # phase, structure rebuild (pattern merge, lists), assembly; wall clock
+
+    # per-kernel device times: the same kernels in the graph's order on one
+    # stream with an event after each (no overlap between streams); the last
+    # entry is the per-commit CZ history refresh
+    kernels = gf.ProfileAssembly(H, reps=max(args.steps, 10))
+    hist = [k for k in kernels if k["name"] == "k_cz_hist"]
+    kernels = [k for k in kernels if k["name"] != "k_cz_hist"]
+
+    # the same workload in the other precision, measured the same way
+    other_line = None
+    if not args.no_other:
+        gf.SetPrecision(1 if other == "mixed" else 0)
+        tune_o = [] if args.no_tune else gf.Autotune(H, reps=10)
+        with ClockSampler(dev) as clk_o:
+            ms_o, _ = _device_ms(gf, lib, stream, flush, args.steps, args.warmup, barrier, H)
+        k_o = [k for k in gf.ProfileAssembly(H, reps=max(args.steps, 10)) if k["name"] != "k_cz_hist"]
+        gf.SetPrecision(1 if precision == "mixed" else 0)
+        other_line = {"precision": other, "ms_per_step": ms_o, "clocks": clk_o.summary(),
+                      "launch_variants": {t["kernel"]: t["variant"] for t in tune_o if t["chosen"]} or "defaults",
+                      "kernels": [{"name": k["name"], "ms": round(k["ms"], 5)} for k in k_o]}
+
+    # a whole Newton iteration without the solve: device broad phase, narrow
+    # phase, structure request, assembly; host wall clock
     full_iter = None
     if not batched:
         reps = 5
@@ -413,49 +463,29 @@ def run_ours(args):
                      "scope": "device broad phase + narrow phase + structure request (kept when the impact list "
                               "is unchanged, as here) + synchronous assembly, host wall clock; no linear solve"}
 
-    # per-kernel device times: the same kernels run in the graph's order on
-    # one stream with an event after each (no overlap between streams)
-    kernels = gf.ProfileAssembly(H, reps=max(args.steps, 10))
-    mixed_error = None
-    if precision == "mixed":
-        # the same assembly in FP64: normwise error of the FP32-mixed result
-        gf.AssembleElemsAndCZs(H)
-        v32, r32 = gf.TransferLinearSystemToHost()
-        gf.SetPrecision(0)
-        gf.AssembleElemsAndCZs(H)
-        v64, r64 = gf.TransferLinearSystemToHost()
-        gf.SetPrecision(1)
-        rows = np.zeros(N + 1, np.int32)
-        cols = np.zeros(nnz, np.int32)
-        _lib.check(gf.ctx, lib.icf_get_structure(gf.ctx, _lib.iptr(rows), _lib.iptr(cols)))
-        b64 = v64.reshape(-1, 9)
-        b32 = v32.reshape(-1, 9)
-        rid = np.repeat(np.arange(N), np.diff(rows))
-        num = np.zeros(N)
-        den = np.zeros(N)
-        np.maximum.at(num, rid, np.abs(b32 - b64).max(axis=1))
-        np.maximum.at(den, rid, np.abs(b64).max(axis=1))
-        mixed_error = {"blocks_rowwise_max": float((num / np.where(den > 0, den, 1)).max()),
-                       "rhs_max_rel": float(np.abs(r32 - r64).max() / np.abs(r64).max()),
-                       "scope": "same inputs assembled in FP64 on the device; per block row max|diff|/max|FP64|"}
-
     from icflow_b200.shard import reduce_max, reduce_sum
 
-    ms_dev, ms_e2e = reduce_max([ms_dev, ms_e2e], device=dev)
+    ms_list = [ms_dev, ms_e2e] + ([other_line["ms_per_step"]] if other_line else [])
+    ms_list = reduce_max(ms_list, device=dev)
+    ms_dev, ms_e2e = ms_list[0], ms_list[1]
+    if other_line:
+        other_line["ms_per_step"] = ms_list[2]
     total_units = reduce_sum([units], device=dev)[0]
 
-    B = algorithmic_bytes(nnz, N, len(coll.x0), len(coll.elems), nc, len(imps))
+    n_nodes, n_tet = len(coll.x0), len(coll.elems)
+    B = algorithmic_bytes(nnz, N, n_nodes, n_tet, nc, len(imps))
     peak, peak_kind = measured_peak()
     achieved = B / (ms_dev * 1e-3) / 1e9
-    launches_per_step = len(kernels)
+    traffic = ncu_traffic(args.workload, precision)
     top = max(kernels, key=lambda k: k["ms"])
     k_sum = sum(k["ms"] for k in kernels)
     for k in kernels:
-        k["GBps"] = k["bytes"] / (k["ms"] * 1e-3) / 1e9
+        k["alg"] = kernel_share_bytes(k["name"], nnz, N, n_nodes, n_tet, nc, len(imps))
         k["share"] = k["ms"] / k_sum
-    top_ach = top["bytes"] / (top["ms"] * 1e-3) / 1e9
     line = None
     if rank == 0:
+        top_ach = top["alg"] / (top["ms"] * 1e-3) / 1e9
+        traffic_asm = sum(v for v in traffic.values()) if traffic else None
         line = {
             "metric": METRIC, "value": total_units * 1000.0 / ms_dev, "unit": "assemblies/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev,
@@ -465,29 +495,51 @@ def run_ours(args):
             "config": {"workload": workload_name(args.workload, *(WORKLOADS[args.workload] or ())),
                        "specimens_per_assembly": N_SPECIMENS if batched else 1,
                        "specimens_rank0": int(len(coll.meshes)) if batched else 1,
-                       "tets": int(len(coll.elems)), "czs": int(nc), "nodes": int(len(coll.x0)),
+                       "tets": int(n_tet), "czs": int(nc), "nodes": int(n_nodes),
                        "active_rows": int(N), "blocks": int(nnz), "impacts": int(len(imps)),
                        "l2": "flushed between steps (256 MiB write), outside the timed region",
                        "launch_variants": {t["kernel"]: t["variant"] for t in tune if t["chosen"]} or "defaults"},
-            "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": top_ach, "peak": peak,
-                         "unit": "GB/s", "frac": top_ach / peak, "traffic": ncu_traffic(top["name"], args.workload),
-                         "algorithmic_bytes": top["bytes"], "launch_ms": top["ms"],
+            # whole assembly against the HBM roofline: the compulsory bytes of
+            # one assembly (72 nnzb + 24 N_a + 96 N + 56 n_t + 240 n_c + 56 n_i)
+            # over the device time of one graph launch
+            "roofline": {"bound": "hbm", "kernel": "one assembly (graph launch)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic_asm,
+                         "algorithmic_bytes": B,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback",
-                         "assembly": {"algorithmic_bytes": B, "achieved": achieved, "frac": achieved / peak,
-                                      "scope": "one whole assembly (graph launch), bytes per the "
-                                               "72 nnzb + 24 N_a + 96 N + 56 n_t + 240 n_c + 56 n_i model"},
+                         "traffic_source": "profiles/dram_traffic.json: sum over one assembly's kernels of ncu "
+                                           "dram__bytes_read.sum + dram__bytes_write.sum" if traffic else None,
+                         "dominant_kernel": {
+                             "name": top["name"], "launch_ms": top["ms"], "algorithmic_bytes": top["alg"],
+                             "achieved": top_ach, "frac": top_ach / peak, "touched_bytes": top["bytes"],
+                             "traffic": traffic.get(top["name"]),
+                             "scope": "its share of the assembly's compulsory bytes over its serialised launch "
+                                      "time; touched_bytes counts the staging records it reads back as well"},
                          "kernels": [{"name": k["name"], "ms": round(k["ms"], 5), "share": round(k["share"], 4),
-                                      "bytes": k["bytes"], "GBps": round(k["GBps"], 1),
-                                      "frac": round(k["GBps"] / peak, 4)} for k in kernels]},
+                                      "algorithmic_bytes": k["alg"], "touched_bytes": k["bytes"],
+                                      "frac": round(k["alg"] / (k["ms"] * 1e-3) / 1e9 / peak, 4),
+                                      "traffic": traffic.get(k["name"])} for k in kernels]},
             "e2e": {"value": total_units * 1000.0 / ms_e2e, "unit": "assemblies/s",
-                    "h2d_bytes_per_step": int(3 * un.nbytes), "d2h_bytes_per_step": int(8 * (9 * nnz + 3 * N))},
-            "gpu_launches": launches_per_step * args.steps,
+                    "h2d_bytes_per_step": int(un.nbytes + vn.nbytes + an.nbytes),
+                    "d2h_bytes_per_step": int(8 * (9 * nnz + 3 * N))},
+            "gpu_launches": len(kernels) * args.steps,
             "autotune": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in t.items()} for t in tune],
-            "mixed_error": mixed_error,
             "full_iteration": full_iter,
             "clocks": clocks,
         }
+        if cnt.nLawExact:
+            line["law_exact_repeats"] = int(cnt.nLawExact)
+        if hist:
+            # once per committed step; the reference's minimum of three Newton
+            # iterations per step (ModelPrms.cs:206) bounds its share per assembly
+            line["cz_history_refresh"] = {"ms_per_commit": hist[0]["ms"],
+                                          "ms_per_assembly_at_3_iterations": hist[0]["ms"] / 3,
+                                          "scope": "k_cz_hist runs when the committed damage state changes "
+                                                   "(once per accepted step), outside the assembly's graph"}
+        if other_line:
+            other_line["value"] = total_units * 1000.0 / other_line["ms_per_step"]
+            other_line["speedup_vs_line"] = ms_dev / other_line["ms_per_step"]
+            line[other] = other_line
         if not args.no_cpu:
             rate, threads, kind, sample = cpu_baseline(coll, state, sig, pairs, bound_s=args.cpu_seconds)
             rate1, _, _, sample1 = cpu_baseline(coll, state, sig, pairs, bound_s=args.cpu_seconds, nthreads=1)
@@ -510,13 +562,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="cfg1", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-other", action="store_true",
+                    help="skip the measurement of the same workload in the other precision")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch variants")
     ap.add_argument("--layout", default="auto", choices=["auto", "records", "contrib"],
                     help="staging layout of the tet contributions (auto: the autotuner's choice)")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="fp64, or FP32 Hessian arithmetic with FP64 rotation, law, rhs and accumulation "
-                         "(default: fp64 for cfg1/cfg2, mixed for cfg3)")
+                         "(default: fp64 for cfg1/cfg2, mixed for cfg3); the line also carries the other")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

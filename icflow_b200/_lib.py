@@ -62,7 +62,7 @@ class icf_params(C.Structure):
 class icf_counts(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         "nElems", "nCZ", "nCZDamaged", "nCZFailedThisStep", "nCZContact",
-        "nImpacts", "nImpactsActive", "nonFinite")]
+        "nImpacts", "nImpactsActive", "nonFinite", "nLawExact")]
 
 
 class icf_kernel_times(C.Structure):
@@ -145,6 +145,7 @@ SIGNATURES = {
     "icf_transfer_linear_system": (I, [P, dp, dp]),
     "icf_transfer_updated_state": (I, [P, dp, dp, ip, dp, dp]),
     "icf_get_cz_tentative": (I, [P, dp, ip, dp]),
+    "icf_cz_law_eval": (I, [P, I, dp, dp, dp, dp, dp, dp, dp, dp, ip]),
     "icf_get_device_buffers": (I, [P, C.POINTER(icf_device_buffers)]),
     "icf_set_node_state": (I, [P, I, dp, dp, dp]),
     "icf_get_node_state": (I, [P, dp, dp, dp, dp]),

@@ -66,13 +66,6 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
-def build_oracle() -> None:
-    """Builds the CPU checkers under oracle/ (test infrastructure)."""
-    root = PKG.parent / "oracle"
-    if (root / "Makefile").exists():
-        subprocess.run(["make", "-s", "-C", str(root)], check=True)
-
-
 if __name__ == "__main__":
     build_library(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(LIB)

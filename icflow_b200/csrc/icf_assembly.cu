@@ -314,7 +314,7 @@ constexpr int CZ_PER_BLOCK = 32;
 // FP32.  The staging then holds rt compactly, cs[12c + 0..8] (FP64), followed
 // by the FP32 blocks cs32[36c + 0..35] with cs32 = (float *)(cs + 12 nc):
 // 240 B per CZ in the same buffer.
-template <bool MIXED, int MINB>
+template <bool MIXED, int MINB, bool EXACT = false>
 __global__ void __launch_bounds__(3 * CZ_PER_BLOCK, MINB)
     k_cz_gp(int nc, const int *__restrict__ cz, const double4 *__restrict__ xc,
             const double *__restrict__ czs, const int *__restrict__ czfail,
@@ -396,7 +396,11 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK, MINB)
     const double2 *hp = reinterpret_cast<const double2 *>(hist + 18 * (size_t)c + 6 * gp);
     const double2 h01 = __ldg(hp), h23 = __ldg(hp + 1), h45 = __ldg(hp + 2);
     const icf_axis Np{h01.x, h01.y, h23.x}, Tm{h23.y, h45.x, h45.y};
-    const icf_law Lw = icf_cz_law_hist(LC, f_tn, f_tt, deln, delt, Np, Tm, pmax, tmax, opn, opt);
+    bool undecided = false;
+    const icf_law Lw = icf_cz_law_hist<EXACT>(LC, f_tn, f_tt, deln, delt, Np, Tm, pmax, tmax, opn, opt, undecided);
+    // a failure comparison within rounding of its threshold: the library
+    // repeats this assembly with the EXACT kernel (icf_read_counts)
+    if (undecided) atomicAdd(counts + 5, 1);
 
     // local traction and its (symmetric) tangent (:301-340)
     double T[3], Td[3][3];
@@ -882,6 +886,9 @@ const cz_variant CZ_VARIANTS[] = {
     {"96 thr minb6", k_cz_gp<false, 6>, k_cz_gp<true, 6>},
     {"96 thr minb8", k_cz_gp<false, 8>, k_cz_gp<true, 8>},
 };
+// the kernel that settles every failure comparison with the reference's
+// rounding (the repeat of an assembly that left one undecided)
+const cz_variant CZ_EXACT = {"96 thr exact", k_cz_gp<false, 1, true>, k_cz_gp<true, 1, true>};
 constexpr int N_CZV = sizeof(CZ_VARIANTS) / sizeof(CZ_VARIANTS[0]);
 
 int icf_tet_variants() { return N_TET; }
@@ -895,7 +902,8 @@ int icf_launch_cz(icf_ctx *ctx, int variant, const double4 *xc, double *cs, cuda
   if (variant < 0 || variant >= N_CZV) variant = 0;
   const icf_dprm P = icf_make_dprm(ctx);
   const icf_law_c LC = make_law_c(ctx, P);
-  const cz_fn f = ctx->precision == ICF_FP32_MIXED ? CZ_VARIANTS[variant].f32 : CZ_VARIANTS[variant].f64;
+  const cz_variant &V = ctx->cz_exact ? CZ_EXACT : CZ_VARIANTS[variant];
+  const cz_fn f = ctx->precision == ICF_FP32_MIXED ? V.f32 : V.f64;
   f<<<icf_blocks(ctx->n_cz, CZ_PER_BLOCK), 3 * CZ_PER_BLOCK, 0, s>>>(
       ctx->n_cz, ctx->d_cz, xc, ctx->d_czs, ctx->d_czfail, ctx->per_cz_prm ? ctx->d_czprm : nullptr, ctx->d_czhist,
       P, LC, cs, ctx->d_cztent, ctx->d_czflags, ctx->d_czavg, ctx->d_counts);
@@ -934,8 +942,11 @@ static icf_law_c make_law_c(const icf_ctx *ctx, const icf_dprm &P) {
   LC.alpha = P.alpha; LC.beta = P.beta; LC.p_m = P.p_m; LC.p_n = P.p_n;
   LC.gam_n = P.gam_n; LC.gam_t = P.gam_t; LC.pMtn = P.pMtn; LC.pMnt = P.pMnt;
   LC.rn = P.rn; LC.rt = P.rt;
-  LC.N0 = icf_axis{ctx->axis0[0], ctx->axis0[1], ctx->axis0[2]};
-  LC.T0 = icf_axis{ctx->axis0[3], ctx->axis0[4], ctx->axis0[5]};
+  const double *a0 = ctx->axis0;
+  LC.N0 = icf_axis{a0[0], a0[1], a0[2], a0[3], a0[4], a0[5]};
+  LC.T0 = icf_axis{a0[6], a0[7], a0[8], a0[9], a0[10], a0[11]};
+  LC.zN = ctx->z0[0];
+  LC.zT = ctx->z0[1];
   auto small_int = [](double v) { return (v == (double)(int)v && v >= 2 && v <= 16) ? (int)v : 0; };
   LC.alpha_int = small_int(P.alpha);
   LC.beta_int = small_int(P.beta);
@@ -1144,6 +1155,21 @@ int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const ch
     }
   }
   ctx->prof = nullptr;
+  // the CZ history-axis refresh, which runs once per committed step (before
+  // the next assembly), not once per assembly: timed on its own, reported last
+  double hist_ms = 0.0;
+  if (rc == ICF_OK && ctx->n_cz > 0 && st.n < ICF_PROF_MAX) {
+    for (int r = 0; r < reps && rc == ICF_OK; r++) {
+      ctx->hist_valid = false;
+      cudaEventRecord(st.ev[0], ctx->stream);
+      rc = icf_ensure_cz_hist(ctx, ctx->stream);
+      cudaEventRecord(st.ev[1], ctx->stream);
+      if (cudaEventSynchronize(st.ev[1]) != cudaSuccess) rc = icf_fail(ctx, ICF_ERR_CUDA, "profile: k_cz_hist");
+      float t = 0.f;
+      cudaEventElapsedTime(&t, st.ev[0], st.ev[1]);
+      hist_ms += t;
+    }
+  }
   for (int i = 0; i <= ICF_PROF_MAX; i++) cudaEventDestroy(st.ev[i]);
   if (rc) return rc;
   *n = st.n;
@@ -1152,10 +1178,18 @@ int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const ch
     bytes[k] = st.bytes[k];
     ms[k] = acc[k] / (reps > 0 ? reps : 1);
   }
+  if (ctx->n_cz > 0 && st.n < ICF_PROF_MAX) {
+    names[st.n] = "k_cz_hist";
+    bytes[st.n] = 64LL * ctx->n_cz + 144LL * ctx->n_cz;  // committed state in, history axes out
+    ms[st.n] = hist_ms / (reps > 0 ? reps : 1);
+    *n = st.n + 1;
+  }
   return ICF_OK;
 }
 
 int icf_launch_assembly(icf_ctx *ctx, double h) {
+  ctx->last_h = h;
+  ctx->n_law_exact = 0;
   ICF_TRY_RC(icf_ensure_cz_hist(ctx, ctx->stream));
   if (!ctx->use_graph) return enqueue_assembly(ctx, h);
   if (!ctx->graph_exec || ctx->graph_version != ctx->version || ctx->graph_h != h) {
@@ -1313,5 +1347,49 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
 
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  return ICF_OK;
+}
+
+// ---- the cohesive law alone (icf_cz_law_eval) -------------------------------------
+// One thread per Gauss-point state in[4i..4i+3] = {pmax, tmax, opn, opt}, with
+// the history axes and the law exactly as k_cz_hist and k_cz_gp evaluate
+// them: the fast law, and where it leaves a comparison undecided the exact
+// one, as the repeated assembly would; out[7i..] = {pmax', tmax', Tn, Tt, Dnn,
+// Dtt, Dnt}, fl[3i..] = {contact, failed, exact decision used}.
+__global__ void k_cz_law_eval(int n, const double *__restrict__ in, const double4 *__restrict__ prm, icf_dprm P,
+                              icf_law_c LC, double *__restrict__ out, int *__restrict__ fl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double f_tn = P.f_tn, f_tt = P.f_tt, deln = P.deln, delt = P.delt;
+  if (prm) {
+    const double4 w = prm[i];
+    f_tn = w.x; f_tt = w.y; deln = w.z; delt = w.w;
+  }
+  double pmax = in[4 * (size_t)i], tmax = in[4 * (size_t)i + 1];
+  const double opn = in[4 * (size_t)i + 2], opt = in[4 * (size_t)i + 3];
+  icf_axis Np, Tm;
+  icf_cz_hist_axes(LC, deln, delt, pmax, tmax, Np, Tm);
+  // the assembly reads the history axes back from the cache as {f, d, dd}
+  const icf_axis Npc{Np.f, Np.d, Np.dd}, Tmc{Tm.f, Tm.d, Tm.dd};
+  const double pmax0 = pmax, tmax0 = tmax;
+  bool undecided = false;
+  icf_law L = icf_cz_law_hist<false>(LC, f_tn, f_tt, deln, delt, Npc, Tmc, pmax, tmax, opn, opt, undecided);
+  if (undecided) {
+    pmax = pmax0;
+    tmax = tmax0;
+    bool u2 = false;
+    L = icf_cz_law_hist<true>(LC, f_tn, f_tt, deln, delt, Npc, Tmc, pmax, tmax, opn, opt, u2);
+  }
+  double *o = out + 7 * (size_t)i;
+  o[0] = pmax; o[1] = tmax; o[2] = L.Tn; o[3] = L.Tt; o[4] = L.Dnn; o[5] = L.Dtt; o[6] = L.Dnt;
+  fl[3 * i] = L.contact ? 1 : 0;
+  fl[3 * i + 1] = L.failed ? 1 : 0;
+  fl[3 * i + 2] = undecided ? 1 : 0;
+}
+
+int icf_launch_law_eval(icf_ctx *ctx, int n, const double *in, const double4 *prm, double *out, int *fl) {
+  const icf_dprm P = icf_make_dprm(ctx);
+  k_cz_law_eval<<<icf_blocks(n, 128), 128, 0, ctx->stream>>>(n, in, prm, P, make_law_c(ctx, P), out, fl);
+  ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }

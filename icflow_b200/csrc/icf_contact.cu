@@ -438,6 +438,7 @@ int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts) {
       ctx->d_imp = nullptr;
       ICF_CUDA(ctx, cudaMalloc(&ctx->d_imp, sizeof(int4) * (size_t)(2 * nu)));
       ctx->imp_cap = 2 * nu;
+      ctx->imp_gen++;
     }
     k_closest<<<icf_blocks(nu, 128), 128, 0, s>>>(nu, k0, ctx->d_adj_off, ctx->d_adj, ctx->d_faces,
                                                  ctx->d_xc, ctx->d_imp);

@@ -26,6 +26,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -151,8 +152,17 @@ struct icf_ctx {
   std::string err;
   icf_params prm{};
   bool have_prm = false;
-  // PPR axis factors (f, d, dd) at zero opening: normal then tangential
-  double axis0[6] = {0, 0, 0, 0, 0, 0};
+  // PPR axis factors at zero opening, normal then tangential: f, d, dd and
+  // the term magnitudes md, mf and rounding count k of the decision bounds
+  double axis0[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  // the reference's dN, dT at zero opening (its rounding noise), normal then
+  // tangential, from the host C library's pow
+  double z0[2] = {0, 0};
+  // the CZ kernel settles every failure comparison with the reference's
+  // rounding (set while an assembly with an undecided comparison is repeated)
+  bool cz_exact = false;
+  double last_h = 0.0;  // time step of the last assembly
+  int n_law_exact = 0;  // comparisons the last assembly settled exactly
   int precision = ICF_FP64;
 
   // sizes
@@ -244,6 +254,9 @@ struct icf_ctx {
   // a structure request with the same list keeps the structure
   int n_imp_built = -1, imp_built_cap = 0;
   int4 *d_imp_built = nullptr;
+  // bumped whenever d_imp is reallocated: a kept structure (and the graph
+  // captured over it) holds the d_imp pointer it was built with
+  unsigned long long imp_gen = 0, imp_gen_built = 0;
   // per-impact classification {kind, ia, ib, 0} and {s, t, dsq, 0}; same
   // capacity as the impact staging d_ks (ks_cap)
   int4 *d_imp_ci = nullptr;
@@ -268,6 +281,7 @@ struct icf_ctx {
   int vals_cap = 0;
 
   // counters: [0] damaged [1] failed [2] contact [3] active impacts [4] nonfinite
+  // [5] undecided CZ law comparisons
   int *d_counts = nullptr;
   int *h_counts = nullptr; // pinned
   double *d_norm = nullptr;
@@ -348,6 +362,12 @@ int icf_rebuild_sell_off(icf_ctx *ctx, bool natural);
 // position map and zeroed contribution staging for the current lists
 int icf_build_contrib(icf_ctx *ctx);
 int icf_ensure_cz_hist(icf_ctx *ctx, cudaStream_t s);
+// the cohesive law alone on device arrays (icf_cz_law_eval): in[4n], prm[n]
+// or null, out[7n], fl[2n]
+int icf_launch_law_eval(icf_ctx *ctx, int n, const double *in, const double4 *prm, double *out, int *fl);
+// after an assembly left a law comparison undecided (counts[5]), repeats it
+// with the exact CZ kernel; `rerun` enqueues the same assembly again
+int icf_settle_law(icf_ctx *ctx, const std::function<int()> &rerun);
 int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, double *relres);
 void icf_free_solver(icf_ctx *ctx);
 int icf_launch_sumsq(icf_ctx *ctx, const double *d_x, long long n);

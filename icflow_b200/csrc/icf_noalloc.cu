@@ -111,6 +111,9 @@ extern "C" int icf_assemble_noalloc(icf_ctx *ctx, double h, const double *d_un, 
   if (rc != ICF_OK) return rc;
   e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return icf_fail(ctx, ICF_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString(e));
+  ctx->n_law_exact = 0;
+  const int rs = icf_settle_law(ctx, [&] { return icf_enqueue_assembly_bufs(ctx, h, B, ctx->stream); });
+  if (rs != ICF_OK) return rs;
   if (counts) {
     counts->nElems = ctx->n_elem;
     counts->nCZ = ctx->n_cz;
@@ -120,6 +123,7 @@ extern "C" int icf_assemble_noalloc(icf_ctx *ctx, double h, const double *d_un, 
     counts->nImpacts = ctx->n_imp;
     counts->nImpactsActive = ctx->h_counts[3];
     counts->nonFinite = ctx->h_counts[4];
+    counts->nLawExact = ctx->n_law_exact;
   }
   if (ctx->h_counts[4]) return icf_fail(ctx, ICF_ERR_NUMERIC, "non-finite value in the assembled rhs");
   return ICF_OK;

@@ -8,6 +8,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "icf_exact.cuh"
+
 // Law outputs for one Gauss point.
 struct icf_law {
   double Tn, Tt, Dnn, Dtt, Dnt;
@@ -30,6 +32,11 @@ struct icf_law {
 // come from one pow each and exact divisions by (1-x) and (p/a+x).
 struct icf_axis {
   double f, d, dd;
+  // for the decision bounds (icf_law_bound): md = |p o0 s1| + |a o1 s0| and
+  // mf = |gam o0 s0| + |mac|, the magnitudes of the terms of d and f, and k,
+  // the rounding error of this evaluation of d and f in units of 2^-53 of
+  // those magnitudes
+  double md, mf, k;
 };
 
 __device__ __forceinline__ icf_axis icf_axis_eval(double a, double p, double gam, double mac,
@@ -54,19 +61,66 @@ __device__ __forceinline__ icf_axis icf_axis_eval(double a, double p, double gam
   // s = p/a + x > 0 wherever the law evaluates an axis (x >= 0), so s^p is
   // 2^(p log2 s): two library calls, cheaper than the general pow
   const double is = 1.0 / s;
-  const double s0 = exp2(p * log2(s)), s1 = s0 * is, s2 = s1 * is;
+  const double E = p * log2(s);
+  const double s0 = exp2(E), s1 = s0 * is, s2 = s1 * is;
   icf_axis r;
   r.f = gam * o0 * s0 + mac;
   r.d = (p * o0 * s1) - (a * o1 * s0);
   r.dd = (p * p - p) * o0 * s2 + (a * a - a) * o2 * s0 - 2.0 * a * p * o1 * s1;
+  // o^(a-k): a - 2 products or pow (2 ulp) and a division; s^p: log2 (1 ulp),
+  // the product with p and exp2 (2 ulp) give 2 ulp + 3 ulp |p log2 s|
+  r.md = fabs(p * o0 * s1) + fabs(a * o1 * s0);
+  r.mf = fabs(gam * o0 * s0) + fabs(mac);
+  r.k = fabs(a) + 24.0 + 3.0 * fabs(E);
   return r;
 }
 
 struct icf_law_c {
   double alpha, beta, p_m, p_n, gam_n, gam_t, pMtn, pMnt, rn, rt;
   icf_axis N0, T0;  // axes at zero opening
+  // the reference's dN and dT at zero opening, p S1 - a S0 with S_k =
+  // pow(p/a, p - k) from the host C library (PPR_math.h:8-9, 20): the exact
+  // difference is 0, so this constant is pure rounding and is taken as the
+  // reference computes it
+  double zN, zT;
   int alpha_int, beta_int;  // alpha, beta when they are integers in [2, 16], else 0
 };
+
+// ---- the law's decisions ----------------------------------------------------------
+// The reference compares Tt_ and Tn_ (at the current opening) with -1e-9 and,
+// past a fifth of the characteristic opening, with 5 % of the strength
+// (cz_kernels.h:43-47, 90-95).  The fast values here are the axis products
+// cT dT(xt) fN(xn) and cN dN(xn) fT(xt); their distance from the reference's
+// values is bounded by the term magnitudes times the rounding counts of both
+// evaluations (the reference's: pow within an ulp, three products).  At a
+// zero opening the axis difference dT or dN is pure rounding noise (about
+// 1e-10 in traction, against the -1e-9 threshold), so there it is replaced
+// by the reference's own constant zT or zN and only the other, well
+// conditioned factor is approximate.  A comparison that the bound still
+// cannot settle is "undecided": the assembly's CZ kernel counts it
+// (EXACT = false) and the library then repeats that assembly with the
+// EXACT = true kernel, which settles it on icf_ref_Tt/icf_ref_Tn, the
+// reference's expressions with pow correctly rounded (icf_exact.cuh).
+__device__ __forceinline__ double icf_law_bound(double c, const icf_axis &own, const icf_axis &other) {
+  const double u = 1.1102230246251565e-16;  // 2^-53
+  return 2.0 * fabs(c) * own.md * other.mf * (own.k + other.k + 18.0) * u;
+}
+// the decision value at a zero opening of its own axis: (g/del) z f_other
+// with the products rounded as the reference rounds them
+__device__ __forceinline__ double icf_law_zero(double g, double del, double z, const icf_axis &other, double &e) {
+  const double u = 1.1102230246251565e-16;
+  const double pr12 = __dmul_rn(__ddiv_rn(g, del), z);
+  e = 2.0 * fabs(pr12) * other.mf * (other.k + 8.0) * u;
+  return __dmul_rn(pr12, other.f);
+}
+__device__ __forceinline__ bool icf_near(double v, double e, double thr) { return fabs(v - thr) <= e; }
+
+// Tn_ and Tt_ at (dn, dt) by the reference expressions (icf_exact.cuh).
+__device__ __forceinline__ double2 icf_law_exact_T(const icf_law_c &C, double deln, double delt, double dn,
+                                                   double dt) {
+  const icf_ppr_k K{C.alpha, C.beta, C.p_m, C.p_n, C.gam_n, C.gam_t, C.pMtn, C.pMnt};
+  return make_double2(icf_ref_Tn(K, deln, delt, dn, dt), icf_ref_Tt(K, deln, delt, dn, dt));
+}
 
 // The axes at the committed history, N(pmax/deln) and T(tmax/delt).  They only
 // change when the damage state does, so the assembly reads them from a cache
@@ -79,10 +133,12 @@ __device__ __forceinline__ void icf_cz_hist_axes(const icf_law_c &C, double deln
 
 // cohesive_law_thermodynamically_consistent (cz_kernels.h:37-174) on the axis
 // factors, given the history axes Np, Tm of the incoming pmax, tmax; pmax and
-// tmax are updated in place.
+// tmax are updated in place.  `undecided` is set when a failure comparison
+// could not be settled without the reference's rounding (EXACT = false).
+template <bool EXACT>
 __device__ inline icf_law icf_cz_law_hist(const icf_law_c &C, double f_tn, double f_tt, double deln,
                                           double delt, const icf_axis &Np, const icf_axis &Tm, double &pmax,
-                                          double &tmax, double opn, double opt) {
+                                          double &tmax, double opn, double opt, bool &undecided) {
   icf_law L;
   L.Tn = L.Tt = L.Dnn = L.Dtt = L.Dnt = 0;
   L.contact = false;
@@ -99,6 +155,7 @@ __device__ inline icf_law icf_cz_law_hist(const icf_law_c &C, double f_tn, doubl
   const double eps_neg = -1e-9;
   const double thr_t = f_tt * 0.05, thr_n = f_tn * 0.05;
   const icf_axis To = icf_axis_eval(C.beta, C.p_n, C.gam_t, C.pMtn, opt * idelt, C.beta_int);
+  const bool t_past = opt > delt * C.rt / 5;
   if (L.contact) {
     if (pmax != 0) {
       const double peak = cN * Np.d * Tm.f;           // Tn_(pmax, tmax)
@@ -109,7 +166,14 @@ __device__ inline icf_law icf_cz_law_hist(const icf_law_c &C, double f_tn, doubl
       L.Tn = L.Dnn * opn;
     }
     L.Tt = cT * To.d * C.N0.f;                        // Tt_(0, opt)
-    if (L.Tt >= eps_neg && !(opt > delt * C.rt / 5 && L.Tt < thr_t)) {
+    double Tt_d = L.Tt, e;
+    if (opt == 0.0) Tt_d = icf_law_zero(C.gam_t, delt, C.zT, C.N0, e);
+    else e = icf_law_bound(cT, To, C.N0);
+    if (icf_near(Tt_d, e, eps_neg) || (t_past && icf_near(Tt_d, e, thr_t))) {
+      if (EXACT) Tt_d = icf_law_exact_T(C, deln, delt, 0.0, opt).y;
+      else undecided = true;
+    }
+    if (Tt_d >= eps_neg && !(t_past && Tt_d < thr_t)) {
       if (opt >= tmax) {
         tmax = opt;
         L.Dtt = cTT * To.dd * C.N0.f;                 // Dtt_(0, opt)
@@ -128,8 +192,23 @@ __device__ inline icf_law icf_cz_law_hist(const icf_law_c &C, double f_tn, doubl
   const icf_axis No = icf_axis_eval(C.alpha, C.p_m, C.gam_n, C.pMnt, opn * ideln, C.alpha_int);
   L.Tt = cT * To.d * No.f;                            // Tt_(opn, opt)
   L.Tn = cN * No.d * To.f;                            // Tn_(opn, opt)
-  if (L.Tt >= eps_neg && L.Tn >= eps_neg && !(opt > delt * C.rt / 5 && L.Tt < thr_t) &&
-      !(opn > deln * C.rn / 5 && L.Tn < thr_n)) {
+  const bool n_past = opn > deln * C.rn / 5;
+  double Tt_d = L.Tt, Tn_d = L.Tn, et, en;
+  if (opt == 0.0) Tt_d = icf_law_zero(C.gam_t, delt, C.zT, No, et);
+  else et = icf_law_bound(cT, To, No);
+  if (opn == 0.0) Tn_d = icf_law_zero(C.gam_n, deln, C.zN, To, en);
+  else en = icf_law_bound(cN, No, To);
+  if (icf_near(Tt_d, et, eps_neg) || icf_near(Tn_d, en, eps_neg) || (t_past && icf_near(Tt_d, et, thr_t)) ||
+      (n_past && icf_near(Tn_d, en, thr_n))) {
+    if (EXACT) {
+      const double2 x = icf_law_exact_T(C, deln, delt, opn, opt);
+      Tn_d = x.x;
+      Tt_d = x.y;
+    } else {
+      undecided = true;
+    }
+  }
+  if (Tt_d >= eps_neg && Tn_d >= eps_neg && !(t_past && Tt_d < thr_t) && !(n_past && Tn_d < thr_n)) {
     const bool tsoft = (opt >= tmax), nsoft = (opn >= pmax);
     if (tsoft && nsoft) {
       tmax = opt;

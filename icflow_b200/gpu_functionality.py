@@ -258,6 +258,23 @@ class GPU_Functionality:
         check(self.ctx, self.lib.icf_get_cz_tentative(self.ctx, dptr(tent), iptr(flags), dptr(avg)))
         return tent[:nc], flags[:nc], avg[:nc]
 
+    def CZLaw(self, pmax, tmax, opn, opt, strength=None):
+        """The cohesive law of the CZ kernel (cz_kernels.h:37-174) evaluated on
+        the device for arrays of Gauss-point states; strength[n, 2] =
+        (sigma_max, tau_max) per state or None for the constants.  Returns
+        pmax', tmax', law[n, 5] (Tn, Tt, Dnn, Dtt, Dnt), flags[n, 3]
+        (contact, failed, settled with the reference's rounding)."""
+        pmax, tmax, opn, opt = (np.ascontiguousarray(z, np.float64).ravel() for z in (pmax, tmax, opn, opt))
+        n = len(pmax)
+        st = None if strength is None else np.ascontiguousarray(strength, np.float64).reshape(n, 2)
+        pm, tm = np.zeros(n), np.zeros(n)
+        law = np.zeros((n, 5))
+        fl = np.zeros((n, 3), np.int32)
+        check(self.ctx, self.lib.icf_cz_law_eval(self.ctx, n, dptr(pmax), dptr(tmax), dptr(opn), dptr(opt),
+                                                 dptr(st) if st is not None else None, dptr(pm), dptr(tm),
+                                                 dptr(law), iptr(fl)))
+        return pm, tm, law, fl
+
     def DeviceBuffers(self) -> _lib.icf_device_buffers:
         b = _lib.icf_device_buffers()
         check(self.ctx, self.lib.icf_get_device_buffers(self.ctx, C.byref(b)))

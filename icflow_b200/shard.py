@@ -1,8 +1,8 @@
 """Multi-GPU plumbing for the assembly path: one process per GPU, no
 collective in the data path.
 
-The path shards only as independent units (SURVEY: batched specimens, or
-one specimen per rank).  Each rank assembles its own share on its own GPU;
+The path shards only as independent units (batched specimens, or one
+specimen per rank).  Each rank assembles its own share on its own GPU;
 the only communication is the timing, reduced as the maximum over ranks, and
 the counts, summed, after the timed region.  Ranks take specimens
 round-robin, so uneven specimen sizes spread evenly enough without a

@@ -83,6 +83,10 @@ typedef struct icf_counts {
   int nImpacts;          /* impacts in the current structure */
   int nImpactsActive;    /* impacts that produced a penalty response */
   int nonFinite;         /* 1 if a NaN/Inf reached the matrix or rhs */
+  int nLawExact;         /* CZ Gauss points whose failure test lay within
+                            rounding of its threshold; the assembly was then
+                            repeated with the reference's rounding for them
+                            (0 in practice; no reference counterpart) */
 } icf_counts;
 
 /* Device buffers, for callers that chain device work (graphs, solvers).
@@ -188,8 +192,9 @@ int icf_get_pcsr(icf_ctx *ctx, int kind, long long capacity, int *out);
  * contributions into the device BCSR values and rhs.  Synchronous. */
 int icf_assemble(icf_ctx *ctx, double h, icf_counts *counts);
 /* Same work, enqueued on the context stream without waiting; counters are
- * read later with icf_read_counts.  Capturable in a CUDA graph once the
- * pattern is built. */
+ * read later with icf_read_counts, which first repeats the assembly if its CZ
+ * law left a failure test undecided (see nLawExact).  Capturable in a CUDA
+ * graph once the pattern is built. */
 int icf_assemble_async(icf_ctx *ctx, double h);
 /* The assembly runs as a fork/join DAG over three streams, captured once as a
  * CUDA graph (default) and re-captured only when the pattern, parameters,
@@ -201,7 +206,10 @@ int icf_read_counts(icf_ctx *ctx, icf_counts *counts);
  * graph, every kernel on the context stream in the graph's order with an event
  * after it, and returns per kernel its name, its algorithmic bytes per launch
  * (every input and output item counted once) and its mean device time.  The
- * outputs of the last run are those of icf_assemble.  Synchronous. */
+ * last entry, k_cz_hist, is the refresh of the CZ history-axis cache, which
+ * runs once per committed damage state (before the next assembly), not once
+ * per assembly.  The outputs of the last run are those of icf_assemble.
+ * Synchronous. */
 #define ICF_MAX_KERNELS 16
 typedef struct icf_kernel_times {
   int n_kernels;               /* kernels one assembly launches */
@@ -272,6 +280,20 @@ int icf_transfer_updated_state(icf_ctx *ctx, double *pmax, double *tmax,
  * tent[n*2] = pmax_, tmax_; flags[n*3] = contact, damaged, failed;
  * avg4[n*4] = avgDn, avgDt, avgTn, avgTt. */
 int icf_get_cz_tentative(icf_ctx *ctx, double *tent, int *flags, double *avg4);
+/* The cohesive law alone, on the device, as the assembly's CZ kernel
+ * evaluates it at one Gauss point: cohesive_law_thermodynamically_consistent
+ * (cz_kernels9/cz_kernels.h:37-174) on the PPR functions (PPR_math.h:2-57).
+ * In the reference the law is a __device__ function with no entry point of
+ * its own; this one exists so that the device law can be checked case by
+ * case.  For n states: committed pmax[i], tmax[i] and openings opn[i], opt[i]
+ * -> updated pmax_out[i], tmax_out[i], law[i*5] = Tn, Tt, Dnn, Dtt, Dnt and
+ * flags[i*3] = contact, failed, and 1 where a failure test was settled with
+ * the reference's rounding (as a repeated assembly settles it).  strength[i*2] = sigma_max, tau_max of each
+ * state (deln, delt derived as for icf_set_cz_strength), or NULL for the
+ * constants of icf_set_constants.  Host arrays; synchronous. */
+int icf_cz_law_eval(icf_ctx *ctx, int n, const double *pmax, const double *tmax,
+                    const double *opn, const double *opt, const double *strength,
+                    double *pmax_out, double *tmax_out, double *law, int *flags);
 int icf_get_device_buffers(icf_ctx *ctx, icf_device_buffers *out);
 
 /* ---- Newmark kinematics on the device, Node.cs:62-97 --------------------- */

@@ -6,8 +6,10 @@ It must produce what icf_assemble produces, from the caller's device arrays
 into the caller's device arrays, with its temporaries in the library's fixed
 static device array.  Checked on two calls in a row (two different node
 states, so the second call cannot reuse anything the first left in the shared
-array), on the cantilever and on a small polycrystal pressed by platens.  This
-file is collected last so a failure here cannot hide the other tests.
+array), on the cantilever and on a small polycrystal pressed by platens, in
+FP64 and FP32-mixed precision, with the list gathers and with the row-tile
+gather.  This file is collected last so a failure here cannot hide the other
+tests.
 """
 import ctypes as C
 
@@ -24,11 +26,12 @@ pytestmark = pytest.mark.gpu
 H = 1e-4
 
 
-def _setup(coll, prms, state, pairs=None):
+def _setup(coll, prms, state, pairs=None, precision=0, tiles=False):
     gf = GPU_Functionality(0)
     gf.prms = prms
     gf.mc = coll
     gf.SetConstants()
+    gf.SetPrecision(precision)
     gf.TransferStaticDataToDevice()
     nc = len(coll.czs)
     gf.TransferPCSR(np.zeros((nc, 3)), np.zeros((nc, 3)), np.zeros(nc, np.int32))
@@ -36,11 +39,17 @@ def _setup(coll, prms, state, pairs=None):
     if pairs is not None:
         gf.NarrowPhaseCollisionDetection(pairs)
     gf.CreateStructure()
+    if tiles:
+        gf.SetVariant(6, 1)
+        names = [k["name"] for k in gf.ProfileAssembly(H, reps=1)]
+        assert "k_gather_tile" in names, names
     return gf
 
 
-@pytest.mark.parametrize("case", ["cantilever", "polycrystal_contact"])
-def test_noalloc_matches_assemble_twice(case):
+@pytest.mark.parametrize("case,precision,tiles", [("cantilever", 0, False), ("polycrystal_contact", 0, False),
+                                                  ("cantilever", 1, False), ("polycrystal_contact", 1, True),
+                                                  ("polycrystal_contact", 0, True)])
+def test_noalloc_matches_assemble_twice(case, precision, tiles):
     import torch
 
     if case == "cantilever":
@@ -55,7 +64,7 @@ def test_noalloc_matches_assemble_twice(case):
     pairs = None
     if case != "cantilever":
         pairs = M.candidate_pairs(coll, coll.x0 + states[0][0])
-    gf = _setup(coll, prms, states[0], pairs)
+    gf = _setup(coll, prms, states[0], pairs, precision, tiles)
     lib = _lib.load()
     ls = gf.linearSystem
     dev = torch.device("cuda", 0)
