@@ -206,6 +206,7 @@ int icf_create(int device, icf_ctx **out) {
 static void free_all(icf_ctx *c) {
   icf_free_solver(c);
   icf_free_tiles(c);
+  icf_free_contact_ws(c);
   void *ptrs[] = {c->d_elem, c->d_cz, c->d_alt, c->d_selem, c->d_adj_off, c->d_adj, c->d_faces,
                   c->d_x0, c->d_xc, c->d_va, c->d_u, c->d_v, c->d_a, c->d_du, c->d_un, c->d_h3,
                   c->d_czs, c->d_czfail, c->d_cztent, c->d_czflags, c->d_czavg, c->d_czprm,
@@ -609,6 +610,7 @@ int icf_narrow_phase(icf_ctx *ctx, int n_pairs, const int *pairs, int *n_impacts
       ctx->n_imp = 0;
       *n_impacts = 0;
       ctx->have_structure = false;
+      ctx->imp_cmp_valid = false;
       return ICF_OK;
     }
     ICF_TRY(icf_run_narrow_phase(ctx, ctx->n_pairs, n_impacts));
@@ -622,6 +624,7 @@ int icf_narrow_phase(icf_ctx *ctx, int n_pairs, const int *pairs, int *n_impacts
     ctx->n_pairs = 0;
     *n_impacts = 0;
     ctx->have_structure = false;
+    ctx->imp_cmp_valid = false;
     return ICF_OK;
   }
   if (ctx->n_surf == 0) return icf_fail(ctx, ICF_ERR_STATE, "no surface elements were transferred");
@@ -671,6 +674,7 @@ int icf_set_impacts(icf_ctx *ctx, int n_impacts, const int *impacts) {
   if (n_impacts)
     ICF_CUDA(ctx, cudaMemcpy(ctx->d_imp, impacts, sizeof(int4) * (size_t)n_impacts, cudaMemcpyHostToDevice));
   ctx->n_imp = n_impacts;
+  ctx->imp_cmp_valid = false;
   ctx->have_structure = false;
   return ICF_OK;
 }
@@ -686,6 +690,10 @@ __global__ void k_imp_differ(int n, const int4 *__restrict__ a, const int4 *__re
 static int same_impacts(icf_ctx *ctx, bool *same) {
   *same = false;
   if (ctx->n_imp_built < 0 || ctx->n_imp != ctx->n_imp_built || ctx->imp_gen != ctx->imp_gen_built) return ICF_OK;
+  if (ctx->imp_cmp_valid) {  // the narrow phase compared the lists on the device
+    *same = ctx->imp_differ == 0;
+    return ICF_OK;
+  }
   if (ctx->n_imp == 0) {
     *same = true;
     return ICF_OK;
@@ -718,6 +726,7 @@ int icf_create_structure(icf_ctx *ctx, int *N, int *nnz) {
   }
   // a rebuild that fails part way must not leave the old list looking current
   ctx->n_imp_built = -1;
+  ctx->imp_cmp_valid = false;
   if (!ctx->d_skeys) ICF_TRY(icf_build_static_pattern(ctx));
   ICF_TRY(icf_build_merged_pattern(ctx));
   if (ctx->gather_tiles && !ctx->tiles.built) ICF_TRY(icf_build_tiles(ctx));

@@ -141,7 +141,8 @@ __device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, cons
 // of its cell, found by binary search.
 __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const int *__restrict__ elem,
                         const double *__restrict__ lohi, const int *__restrict__ group, int gbits,
-                        const int *__restrict__ off, int *__restrict__ cnt, unsigned long long *__restrict__ out) {
+                        const int *__restrict__ off, int *__restrict__ cnt, unsigned long long *__restrict__ out,
+                        long long cap) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const unsigned long long here = key[i];
@@ -157,16 +158,25 @@ __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const
     const int b0 = elem[j];
     const int a = a0 < b0 ? a0 : b0, b = a0 < b0 ? b0 : a0;
     if (keep_pair(a, b, lohi, group)) {
-      if (out) out[o++] = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
+      // beyond the capacity nothing is written; the host sees the total
+      // and repeats with a larger buffer
+      if (out && o < cap) out[o] = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
+      o++;
       c++;
     }
   }
   if (cnt) cnt[i] = c;
 }
 
-__global__ void k_unpack_pairs(int n, const unsigned long long *__restrict__ in, int *__restrict__ pairs) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// The unique pairs (in[0 .. *n_dev), the all-ones padding key dropped) into
+// the pair list; n_dev[0] becomes the pair count.
+__global__ void k_unpack_pairs(long long cap, int *__restrict__ n_dev, const unsigned long long *__restrict__ in,
+                               int *__restrict__ pairs) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int n = *n_dev;
+  if (n > 0 && in[n - 1] == ~0ull) n--;  // the padding, sorted last
+  if (i == 0) n_dev[1] = n;
+  if (i >= n || i >= cap) return;
   pairs[2 * (size_t)i] = (int)(in[i] >> 32);
   pairs[2 * (size_t)i + 1] = (int)(in[i] & 0xffffffffull);
 }
@@ -234,35 +244,69 @@ __global__ void k_red7_final(int nb, const double *__restrict__ part, double *__
 
 }  // namespace
 
+template <typename T>
+static int grow(icf_ctx *ctx, T **p, long long n) {
+  cudaFree(*p);
+  *p = nullptr;
+  ICF_CUDA(ctx, cudaMalloc(p, sizeof(T) * (size_t)(n > 0 ? n : 1)));
+  return ICF_OK;
+}
+
+void icf_free_contact_ws(icf_ctx *ctx) {
+  icf_contact_ws &W = ctx->cws;
+  void *d[] = {W.lohi, W.ext, W.tmpv, W.red, W.bcnt, W.boff, W.clo, W.ek0, W.ek1, W.ee0, W.ee1, W.pc, W.po,
+               W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small};
+  for (void *q : d) cudaFree(q);
+  cudaFreeHost(W.h_small);
+  cudaFreeHost(W.h_red);
+  W = icf_contact_ws();
+}
+
+static int ensure_small(icf_ctx *ctx) {
+  icf_contact_ws &W = ctx->cws;
+  if (!W.d_small) ICF_CUDA(ctx, cudaMalloc(&W.d_small, 8 * sizeof(int)));
+  if (!W.h_small) ICF_CUDA(ctx, cudaMallocHost(&W.h_small, 8 * sizeof(int)));
+  if (!W.h_red) ICF_CUDA(ctx, cudaMallocHost(&W.h_red, 8 * sizeof(double)));
+  return ICF_OK;
+}
+
+// Two synchronisations: one for the grid (cell size and corners, which set
+// the key layout) and the entry count, one for the result.  Buffers live in
+// the context's workspace; only growth beyond the high-water mark allocates.
 int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pairs_out) {
   cudaStream_t s = ctx->stream;
   const int n = ctx->n_surf;
+  icf_contact_ws &W = ctx->cws;
   *n_pairs_out = 0;
   ctx->n_pairs = 0;
   if (n < 2) return ICF_OK;
-  double *lohi, *ext, *red, *tmpv;
-  int *cnt, *off;
-  int4 *clo;
-  ICF_CUDA(ctx, cudaMallocAsync(&lohi, sizeof(double) * 6 * (size_t)n, s));
-  ICF_CUDA(ctx, cudaMallocAsync(&ext, sizeof(double) * (size_t)n, s));
-  // per-block partials of the corner and extent reduction
-  ICF_CUDA(ctx, cudaMallocAsync(&tmpv, sizeof(double) * 7 * (size_t)(2 * ctx->n_sm + 1), s));
-  ICF_CUDA(ctx, cudaMallocAsync(&red, sizeof(double) * 7, s));
-  ICF_CUDA(ctx, cudaMallocAsync(&cnt, sizeof(int) * (size_t)(n + 1), s));
-  ICF_CUDA(ctx, cudaMallocAsync(&off, sizeof(int) * (size_t)(n + 1), s));
-  ICF_CUDA(ctx, cudaMallocAsync(&clo, sizeof(int4) * (size_t)n, s));
-  ICF_CUDA(ctx, cudaMemsetAsync(ext, 0, sizeof(double), s));
-  k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, lohi, ext);
-  size_t tb = 0;
-  {
-    const int nbk = (int)std::min<long long>((n + 255) / 256, 2LL * ctx->n_sm);
-    k_red7<<<nbk, 256, 0, s>>>(n, lohi, ext, tmpv);
-    k_red7_final<<<1, 256, 0, s>>>(nbk, tmpv, red);
+  ICF_TRY_RC(ensure_small(ctx));
+  const int nbk = (int)std::min<long long>((n + 255) / 256, 2LL * ctx->n_sm);
+  if (n > W.b_cap) {
+    ICF_TRY_RC(grow(ctx, &W.lohi, 6LL * n));
+    ICF_TRY_RC(grow(ctx, &W.ext, n));
+    ICF_TRY_RC(grow(ctx, &W.bcnt, n + 1LL));
+    ICF_TRY_RC(grow(ctx, &W.boff, n + 1LL));
+    ICF_TRY_RC(grow(ctx, &W.clo, n));
+    W.b_cap = n;
   }
-  double h_red[7];
-  ICF_CUDA(ctx, cudaMemcpyAsync(h_red, red, sizeof(h_red), cudaMemcpyDeviceToHost, s));
+  if (!W.tmpv) ICF_TRY_RC(grow(ctx, &W.tmpv, 7LL * (2 * ctx->n_sm + 1)));
+  if (!W.red) ICF_TRY_RC(grow(ctx, &W.red, 8));
+  k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext);
+  k_red7<<<nbk, 256, 0, s>>>(n, W.lohi, W.ext, W.tmpv);
+  k_red7_final<<<1, 256, 0, s>>>(nbk, W.tmpv, W.red);
+  k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
+  ICF_CUDA(ctx, cudaMemsetAsync(W.bcnt + n, 0, sizeof(int), s));
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, W.bcnt, W.boff, n + 1, s);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.bcnt, W.boff, n + 1, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(W.h_red, W.red, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 3, W.boff + n, sizeof(int), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  const double *h_red = W.h_red;
   if (!(h_red[0] > 0) || !std::isfinite(h_red[0])) return icf_fail(ctx, ICF_ERR_NUMERIC, "broad phase: degenerate boxes");
+  const int m = W.h_small[3];
   // (cell, group) keys when the cell indices and group ids fit in 63 bits
   int nb = 1;
   {
@@ -272,73 +316,71 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     while (nb < 40 && (double)(1ull << nb) < cells) nb++;
   }
   const int gbits = (d_group && ctx->sgroup_bits >= 0 && 3 * nb + ctx->sgroup_bits <= 63) ? ctx->sgroup_bits : -1;
-  k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, lohi, red, cnt, clo);
-  ICF_CUDA(ctx, cudaMemsetAsync(cnt + n, 0, sizeof(int), s));
-  tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, n + 1, s);
-  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, cnt, off, n + 1, s));
-  int m = 0;
-  ICF_CUDA(ctx, cudaMemcpyAsync(&m, off + n, sizeof(int), cudaMemcpyDeviceToHost, s));
-  ICF_CUDA(ctx, cudaStreamSynchronize(s));
-  unsigned long long *k0, *k1;
-  int *e0, *e1, *pc, *po;
-  ICF_CUDA(ctx, cudaMallocAsync(&k0, sizeof(unsigned long long) * (size_t)m, s));
-  ICF_CUDA(ctx, cudaMallocAsync(&k1, sizeof(unsigned long long) * (size_t)m, s));
-  ICF_CUDA(ctx, cudaMallocAsync(&e0, sizeof(int) * (size_t)m, s));
-  ICF_CUDA(ctx, cudaMallocAsync(&e1, sizeof(int) * (size_t)m, s));
-  ICF_CUDA(ctx, cudaMallocAsync(&pc, sizeof(int) * (size_t)(m + 1), s));
-  ICF_CUDA(ctx, cudaMallocAsync(&po, sizeof(int) * (size_t)(m + 1), s));
-  k_entries<<<icf_blocks(n, 256), 256, 0, s>>>(n, clo, off, nb, gbits, d_group, k0, e0);
+  if (m > W.ent_cap) {
+    const long long c = m + m / 4 + 64;
+    ICF_TRY_RC(grow(ctx, &W.ek0, c));
+    ICF_TRY_RC(grow(ctx, &W.ek1, c));
+    ICF_TRY_RC(grow(ctx, &W.ee0, c));
+    ICF_TRY_RC(grow(ctx, &W.ee1, c));
+    ICF_TRY_RC(grow(ctx, &W.pc, c + 1));
+    ICF_TRY_RC(grow(ctx, &W.po, c + 1));
+    W.ent_cap = c;
+  }
+  k_entries<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.clo, W.boff, nb, gbits, d_group, W.ek0, W.ee0);
   const int end_bit = gbits >= 0 ? 3 * nb + gbits : 63;
   tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, e0, e1, m, 0, end_bit, s);
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, W.ek0, W.ek1, W.ee0, W.ee1, m, 0, end_bit, s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-  ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, k0, k1, e0, e1, m, 0, end_bit, s));
-  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, k1, e1, lohi, d_group, gbits, nullptr, pc, nullptr);
-  ICF_CUDA(ctx, cudaMemsetAsync(pc + m, 0, sizeof(int), s));
+  ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, W.ek0, W.ek1, W.ee0, W.ee1, m, 0, end_bit, s));
+  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, d_group, gbits, nullptr, W.pc, nullptr, 0);
+  ICF_CUDA(ctx, cudaMemsetAsync(W.pc + m, 0, sizeof(int), s));
   tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, pc, po, m + 1, s);
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, W.pc, W.po, m + 1, s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, pc, po, m + 1, s));
-  int nall = 0, np = 0;
-  ICF_CUDA(ctx, cudaMemcpyAsync(&nall, po + m, sizeof(int), cudaMemcpyDeviceToHost, s));
-  ICF_CUDA(ctx, cudaStreamSynchronize(s));
-  if (nall > 0) {
-    unsigned long long *p0, *p1;
-    int *d_np;
-    ICF_CUDA(ctx, cudaMallocAsync(&p0, sizeof(unsigned long long) * (size_t)nall, s));
-    ICF_CUDA(ctx, cudaMallocAsync(&p1, sizeof(unsigned long long) * (size_t)nall, s));
-    ICF_CUDA(ctx, cudaMallocAsync(&d_np, sizeof(int), s));
-    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, k1, e1, lohi, d_group, gbits, po, nullptr, p0);
-    tb = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb, p0, p1, nall, 0, 64, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, p0, p1, nall, 0, 64, s));
-    tb = 0;
-    cub::DeviceSelect::Unique(nullptr, tb, p1, p0, d_np, nall, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, p1, p0, d_np, nall, s));
-    ICF_CUDA(ctx, cudaMemcpyAsync(&np, d_np, sizeof(int), cudaMemcpyDeviceToHost, s));
-    ICF_CUDA(ctx, cudaStreamSynchronize(s));
-    ICF_CUDA(ctx, cudaFreeAsync(d_np, s));
-    if (np > ctx->pairs_cap || !ctx->d_pairs) {
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.pc, W.po, m + 1, s));
+  for (int attempt = 0; attempt < 2; attempt++) {
+    if (W.pair_cap == 0) {
+      const long long c = std::max<long long>(4LL * n, 1024);
+      ICF_TRY_RC(grow(ctx, &W.p0, c));
+      ICF_TRY_RC(grow(ctx, &W.p1, c));
+      W.pair_cap = c;
+    }
+    const long long P = W.pair_cap;
+    if (P > ctx->pairs_cap || !ctx->d_pairs) {
       cudaFree(ctx->d_pairs);
       cudaFree(ctx->d_masks);
       ctx->d_pairs = ctx->d_masks = nullptr;
-      ICF_CUDA(ctx, cudaMalloc(&ctx->d_pairs, sizeof(int) * 2 * (size_t)np));
-      ICF_CUDA(ctx, cudaMalloc(&ctx->d_masks, sizeof(int) * (size_t)np));
-      ctx->pairs_cap = np;
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_pairs, sizeof(int) * 2 * (size_t)P));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_masks, sizeof(int) * (size_t)P));
+      ctx->pairs_cap = (int)P;
     }
-    k_unpack_pairs<<<icf_blocks(np, 256), 256, 0, s>>>(np, p0, ctx->d_pairs);
-    ICF_CUDA(ctx, cudaFreeAsync(p0, s));
-    ICF_CUDA(ctx, cudaFreeAsync(p1, s));
+    // pad with all-ones keys: they sort after every pair and form one run
+    ICF_CUDA(ctx, cudaMemsetAsync(W.p0, 0xFF, sizeof(unsigned long long) * (size_t)P, s));
+    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, d_group, gbits, W.po, nullptr, W.p0, P);
+    tb = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, W.p0, W.p1, (int)P, 0, 64, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, W.p0, W.p1, (int)P, 0, 64, s));
+    tb = 0;
+    cub::DeviceSelect::Unique(nullptr, tb, W.p1, W.p0, W.d_small, (int)P, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, W.p1, W.p0, W.d_small, (int)P, s));
+    k_unpack_pairs<<<icf_blocks(P, 256), 256, 0, s>>>(P, W.d_small, W.p0, ctx->d_pairs);
+    ICF_CUDA(ctx, cudaGetLastError());
+    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 2, W.po + m, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 1, W.d_small + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    const long long nall = W.h_small[2];
+    if (nall <= P) {
+      ctx->n_pairs = W.h_small[1];
+      *n_pairs_out = ctx->n_pairs;
+      return ICF_OK;
+    }
+    // more candidate pairs than the buffer holds: grow it and write them again
+    const long long c = nall + nall / 4 + 1024;
+    ICF_TRY_RC(grow(ctx, &W.p0, c));
+    ICF_TRY_RC(grow(ctx, &W.p1, c));
+    W.pair_cap = c;
   }
-  ICF_CUDA(ctx, cudaGetLastError());
-  void *tmp[] = {lohi, ext, tmpv, red, cnt, off, clo, k0, k1, e0, e1, pc, po};
-  for (void *p : tmp) ICF_CUDA(ctx, cudaFreeAsync(p, s));
-  ICF_CUDA(ctx, cudaStreamSynchronize(s));
-  ctx->n_pairs = np;
-  *n_pairs_out = np;
-  return ICF_OK;
+  return icf_fail(ctx, ICF_ERR_SIZE, "broad phase: pair buffer growth did not converge");
 }

@@ -150,12 +150,12 @@ __device__ double dtn(const double f[9], const double p[3]) {
   return r;
 }
 
-__global__ void k_closest(int n, const unsigned long long *__restrict__ keys,
+__global__ void k_closest(int n, const int *__restrict__ n_dev, const unsigned long long *__restrict__ keys,
                           const int *__restrict__ adj_off, const int *__restrict__ adj,
                           const int *__restrict__ faces, const double4 *__restrict__ xc,
                           int4 *__restrict__ imp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || i >= *n_dev) return;
   const unsigned long long key = keys[i];
   const int node = (int)(key >> 32), el = (int)(key & 0xffffffffULL);
   const double4 pp = xc[node];
@@ -375,6 +375,18 @@ __global__ void k_imp_classify(int n, const int4 *__restrict__ imp, const int *_
   if (active) atomicAdd(counts + 3, 1);
 }
 
+// flag[0] = 1 unless the new list (n_dev[0] impacts) equals the n_built
+// impacts the current structure was built from
+__global__ void k_imp_same(int cap, const int *__restrict__ n_dev, int n_built, const int4 *__restrict__ a,
+                           const int4 *__restrict__ b, int *__restrict__ flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = *n_dev;
+  if (i == 0 && n != n_built) *flag = 1;
+  if (i >= cap || i >= n || i >= n_built) return;
+  const int4 x = a[i], y = b[i];
+  if (x.x != y.x || x.y != y.y || x.z != y.z || x.w != y.w) *flag = 1;
+}
+
 }  // namespace
 
 int icf_launch_imp_unit(icf_ctx *ctx, cudaStream_t stream) {
@@ -391,65 +403,88 @@ int icf_launch_imp_unit(icf_ctx *ctx, cudaStream_t stream) {
 }
 
 // Narrow phase + set expansion + closest face.  Leaves ctx->d_imp /
-// ctx->n_imp set; the pattern must be rebuilt afterwards.
+// ctx->n_imp set; the pattern must be rebuilt afterwards.  Two
+// synchronisations (the expanded tuple count, which sizes the sort, and the
+// result); the buffers are the context's workspace.  The new list is also
+// compared, on the device, with the list the current structure was built
+// from, so that the structure request that follows needs no round trip.
+template <typename T>
+static int grow_buf(icf_ctx *ctx, T **p, long long n) {
+  cudaFree(*p);
+  *p = nullptr;
+  ICF_CUDA(ctx, cudaMalloc(p, sizeof(T) * (size_t)(n > 0 ? n : 1)));
+  return ICF_OK;
+}
+
 int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts) {
   cudaStream_t s = ctx->stream;
+  icf_contact_ws &W = ctx->cws;
+  ctx->imp_cmp_valid = false;
   if (n_pairs == 0) {
     ctx->n_imp = 0;
     *n_impacts = 0;
     return ICF_OK;
   }
+  if (!W.d_small) ICF_CUDA(ctx, cudaMalloc(&W.d_small, 8 * sizeof(int)));
+  if (!W.h_small) ICF_CUDA(ctx, cudaMallocHost(&W.h_small, 8 * sizeof(int)));
+  if (n_pairs + 1LL > W.ncnt_cap) {
+    ICF_TRY_RC(grow_buf(ctx, &W.ncnt, n_pairs + 1LL));
+    ICF_TRY_RC(grow_buf(ctx, &W.noff, n_pairs + 1LL));
+    W.ncnt_cap = n_pairs + 1LL;
+  }
   // counts and offsets of the set bits
-  int *d_cnt = nullptr, *d_off = nullptr;
-  ICF_CUDA(ctx, cudaMallocAsync(&d_cnt, sizeof(int) * (n_pairs + 1), s));
-  ICF_CUDA(ctx, cudaMallocAsync(&d_off, sizeof(int) * (n_pairs + 1), s));
   k_narrow<<<icf_blocks(n_pairs, 128), 128, 0, s>>>(n_pairs, ctx->d_pairs, ctx->d_selem, ctx->d_xc,
-                                                   ctx->d_masks, d_cnt);
+                                                   ctx->d_masks, W.ncnt);
   ICF_CUDA(ctx, cudaGetLastError());
-  ICF_CUDA(ctx, cudaMemsetAsync(d_cnt + n_pairs, 0, sizeof(int), s));
+  ICF_CUDA(ctx, cudaMemsetAsync(W.ncnt + n_pairs, 0, sizeof(int), s));
   size_t tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, d_cnt, d_off, n_pairs + 1, s);
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, W.ncnt, W.noff, n_pairs + 1, s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, d_cnt, d_off, n_pairs + 1, s));
-  int total = 0;
-  ICF_CUDA(ctx, cudaMemcpyAsync(&total, d_off + n_pairs, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.ncnt, W.noff, n_pairs + 1, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 4, W.noff + n_pairs, sizeof(int), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  const int total = W.h_small[4];
+  const bool cmp = ctx->n_imp_built >= 0 && ctx->imp_gen == ctx->imp_gen_built;
   int nu = 0;
   if (total > 0) {
-    unsigned long long *k0 = nullptr, *k1 = nullptr;
-    int *d_nu = nullptr;
-    ICF_CUDA(ctx, cudaMallocAsync(&k0, sizeof(unsigned long long) * total, s));
-    ICF_CUDA(ctx, cudaMallocAsync(&k1, sizeof(unsigned long long) * total, s));
-    ICF_CUDA(ctx, cudaMallocAsync(&d_nu, sizeof(int), s));
-    k_expand<<<icf_blocks(n_pairs, 128), 128, 0, s>>>(n_pairs, ctx->d_pairs, ctx->d_selem,
-                                                     ctx->d_masks, d_off, k0);
-    tb = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb, k0, k1, total, 0, 64, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, k0, k1, total, 0, 64, s));
-    tb = 0;
-    cub::DeviceSelect::Unique(nullptr, tb, k1, k0, d_nu, total, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, k1, k0, d_nu, total, s));
-    ICF_CUDA(ctx, cudaMemcpyAsync(&nu, d_nu, sizeof(int), cudaMemcpyDeviceToHost, s));
-    ICF_CUDA(ctx, cudaStreamSynchronize(s));
-    if (nu > ctx->imp_cap) {
-      if (ctx->d_imp) cudaFree(ctx->d_imp);
-      ctx->d_imp = nullptr;
-      ICF_CUDA(ctx, cudaMalloc(&ctx->d_imp, sizeof(int4) * (size_t)(2 * nu)));
-      ctx->imp_cap = 2 * nu;
+    if (total > W.nkey_cap) {
+      const long long c = total + total / 4 + 64;
+      ICF_TRY_RC(grow_buf(ctx, &W.nk0, c));
+      ICF_TRY_RC(grow_buf(ctx, &W.nk1, c));
+      W.nkey_cap = c;
+    }
+    // the impact list holds at most `total` entries
+    if (total > ctx->imp_cap) {
+      ICF_TRY_RC(grow_buf(ctx, &ctx->d_imp, 2LL * total));
+      ctx->imp_cap = 2 * total;
       ctx->imp_gen++;
     }
-    k_closest<<<icf_blocks(nu, 128), 128, 0, s>>>(nu, k0, ctx->d_adj_off, ctx->d_adj, ctx->d_faces,
-                                                 ctx->d_xc, ctx->d_imp);
+    k_expand<<<icf_blocks(n_pairs, 128), 128, 0, s>>>(n_pairs, ctx->d_pairs, ctx->d_selem, ctx->d_masks, W.noff,
+                                                     W.nk0);
+    tb = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, W.nk0, W.nk1, total, 0, 64, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, W.nk0, W.nk1, total, 0, 64, s));
+    tb = 0;
+    cub::DeviceSelect::Unique(nullptr, tb, W.nk1, W.nk0, W.d_small, total, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, W.nk1, W.nk0, W.d_small, total, s));
+    k_closest<<<icf_blocks(total, 128), 128, 0, s>>>(total, W.d_small, W.nk0, ctx->d_adj_off, ctx->d_adj,
+                                                    ctx->d_faces, ctx->d_xc, ctx->d_imp);
     ICF_CUDA(ctx, cudaGetLastError());
-    ICF_CUDA(ctx, cudaFreeAsync(k0, s));
-    ICF_CUDA(ctx, cudaFreeAsync(k1, s));
-    ICF_CUDA(ctx, cudaFreeAsync(d_nu, s));
+    ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 1, 0, sizeof(int), s));
+    if (cmp && ctx->imp_gen == ctx->imp_gen_built)
+      k_imp_same<<<icf_blocks(total, 256), 256, 0, s>>>(total, W.d_small, ctx->n_imp_built, ctx->d_imp,
+                                                       ctx->d_imp_built, W.d_small + 1);
+    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small, W.d_small, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    nu = W.h_small[0];
+    ctx->imp_cmp_valid = cmp && ctx->imp_gen == ctx->imp_gen_built;
+    ctx->imp_differ = W.h_small[1];
+  } else {
+    ctx->imp_cmp_valid = cmp;
+    ctx->imp_differ = ctx->n_imp_built != 0;
   }
-  ICF_CUDA(ctx, cudaFreeAsync(d_cnt, s));
-  ICF_CUDA(ctx, cudaFreeAsync(d_off, s));
-  ICF_CUDA(ctx, cudaStreamSynchronize(s));
   ctx->n_imp = nu;
   *n_impacts = nu;
   return ICF_OK;

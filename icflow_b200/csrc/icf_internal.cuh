@@ -109,6 +109,33 @@ struct icf_tiles {
   uint32_t *czcodes = nullptr;
 };
 
+// Workspace of the broad and narrow phases, kept across calls and grown to the
+// high-water mark, so that a call allocates nothing in the usual case.
+struct icf_contact_ws {
+  // broad phase, per surface element (capacity b_cap)
+  double *lohi = nullptr, *ext = nullptr, *tmpv = nullptr, *red = nullptr;
+  int *bcnt = nullptr, *boff = nullptr;
+  int4 *clo = nullptr;
+  long long b_cap = 0;
+  // (cell, element) entries (capacity ent_cap) and their pair counts/offsets
+  unsigned long long *ek0 = nullptr, *ek1 = nullptr;
+  int *ee0 = nullptr, *ee1 = nullptr, *pc = nullptr, *po = nullptr;
+  long long ent_cap = 0;
+  // candidate pairs before de-duplication (capacity pair_cap, padded with
+  // all-ones keys that sort last)
+  unsigned long long *p0 = nullptr, *p1 = nullptr;
+  long long pair_cap = 0;
+  // narrow phase: per pair counts/offsets and the (node, element) keys
+  int *ncnt = nullptr, *noff = nullptr;
+  long long ncnt_cap = 0;
+  unsigned long long *nk0 = nullptr, *nk1 = nullptr;
+  long long nkey_cap = 0;
+  // small device results and their pinned host copy: [0] unique count,
+  // [1] impact list differs from the built one, [2] pairs before de-duplication
+  int *d_small = nullptr, *h_small = nullptr;
+  double *h_red = nullptr;  // pinned: the broad phase's grid reduction (7)
+};
+
 // Device MINRES solver state (icf_solve.cu).
 struct icf_solver {
   long long gen = -1;  // structure generation the lower-block index belongs to
@@ -257,6 +284,11 @@ struct icf_ctx {
   // bumped whenever d_imp is reallocated: a kept structure (and the graph
   // captured over it) holds the d_imp pointer it was built with
   unsigned long long imp_gen = 0, imp_gen_built = 0;
+  // set by the narrow phase, which compares its new list with the built one
+  // on the device: imp_cmp_valid while that comparison is current
+  bool imp_cmp_valid = false;
+  int imp_differ = 1;
+  icf_contact_ws cws;
   // per-impact classification {kind, ia, ib, 0} and {s, t, dsq, 0}; same
   // capacity as the impact staging d_ks (ks_cap)
   int4 *d_imp_ci = nullptr;
@@ -372,6 +404,7 @@ int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, doubl
 void icf_free_solver(icf_ctx *ctx);
 int icf_launch_sumsq(icf_ctx *ctx, const double *d_x, long long n);
 int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pairs_out);
+void icf_free_contact_ws(icf_ctx *ctx);
 int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out);
 int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant);
 int icf_profile_assembly_impl(icf_ctx *ctx, double h, int reps, int *n, const char **names,

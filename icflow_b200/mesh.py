@@ -372,14 +372,17 @@ def polycrystal(n: int = 32, grains: int = 128, edge: float = 1e-3, seed: int = 
 
 
 def batched_specimens(n_specimens: int = 64, seed: int = 0, tets=(5000, 60000), grains=(8, 64),
-                      edge: float = 1e-3, spacing: float = 2.0, only: list | None = None):
+                      edge: float = 1e-3, spacing: float = 0.0, only: list | None = None):
     """Independent polycrystal cubes of uneven size: specimen i has about
     U[tets] tetrahedra (a cube of n^3 hexahedra, n = round((t / 6)^(1/3))) and
-    U[grains] Voronoi grains with CZs on every grain boundary, placed
-    `spacing` edges apart along x so that they never touch.  `only` keeps a
-    subset of the specimen indices (the draw for every index is the same
-    whether or not it is kept).  Returns the collection and, per kept
-    specimen, (index, tets, grains)."""
+    U[grains] Voronoi grains with CZs on every grain boundary.  Specimen i
+    sits at x = i * spacing * edge.  The default 0 keeps every specimen in its
+    own frame at the origin: the specimens never interact, and a frame far
+    from the origin costs accuracy, because the corotational forces subtract
+    rest coordinates from rotated current ones (xr = R^T xc - x0) and lose the
+    digits of the offset.  `only` keeps a subset of the specimen indices (the
+    draw for every index is the same whether or not it is kept).  Returns the
+    collection and, per kept specimen, (index, tets, grains)."""
     rng = np.random.default_rng(seed)
     draws = [(int(rng.integers(tets[0], tets[1] + 1)), int(rng.integers(grains[0], grains[1] + 1)))
              for _ in range(n_specimens)]
