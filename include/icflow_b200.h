@@ -261,7 +261,10 @@ int icf_set_variant(icf_ctx *ctx, int kind, int variant);
  * ICF_ERR_SIZE.  The context must hold constants, static data and a structure
  * from earlier calls.  The first call on a device looks up the array's device
  * address (make it before any stream capture).  All calls share the array:
- * calls that overlap on the GPU race.  Synchronous. */
+ * calls that overlap on the GPU race.  The node forces of
+ * icf_transfer_updated_state stay those of the last icf_assemble; the
+ * tentative CZ state is that of the last assembly of either kind.
+ * Synchronous. */
 int icf_assemble_noalloc(icf_ctx *ctx, double h, const double *d_un, const double *d_vn,
                          const double *d_an, double *d_vals, double *d_rhs,
                          icf_counts *counts);
