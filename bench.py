@@ -88,7 +88,10 @@ def _state(coll, seed):
 
 def build_workload(workload: str, seed: int, rank: int = 0, world: int = 1):
     """(collection, (un, vn, an), per-CZ strengths, candidate pairs, units of
-    the metric this rank's collection holds)."""
+    the metric this rank's collection holds).  The polycrystal workloads'
+    pairs are None: they come from the broad phase at the state's positions
+    (every overlapping surface-element pair sharing no node, same mesh
+    included, as the reference's BVH lists them)."""
     from icflow_b200 import mesh as M
 
     if workload == "cfg3":
@@ -104,8 +107,7 @@ def build_workload(workload: str, seed: int, rank: int = 0, world: int = 1):
     coll = M.polycrystal(n=n, grains=grains, seed=seed, platens=True, gap=-0.25)
     un, vn, an = _state(coll, seed)
     sig = M.lognormal_strengths(len(coll.czs), seed=seed, granule_pairs=coll.meshes[0].cz_grains)
-    pairs = M.candidate_pairs(coll, coll.x0 + un)
-    return coll, (un, vn, an), sig, pairs, 1.0
+    return coll, (un, vn, an), sig, None, 1.0
 
 
 def algorithmic_bytes(nnz, n_active, n_nodes, n_tet, n_cz, n_imp) -> int:
@@ -243,6 +245,8 @@ def cpu_baseline(coll, state, sig, pairs, bound_s: float = 12.0, nthreads: int =
     p = O.prms(**{k: getattr(prms, k) for k in keys})
     un, vn, an = state
     xt = coll.x0 + un
+    if pairs is None:  # the broad phase's rule, on the host
+        pairs = O.candidate_pairs(coll.selem, xt)
     masks = O.narrow_phase(pairs, coll.selem, xt)
     imps = O.impacts(pairs, masks, coll.selem, coll.adj_off, coll.adj, coll.faces, xt)
     N, rows, cols = O.build_structure(coll.alt, coll.elems, coll.czs, imps)
@@ -372,7 +376,12 @@ def run_ours(args):
     gf.TransferNodesToGPU(un, vn, an)
     nc = len(coll.czs)
     gf.TransferPCSR(np.zeros((nc, 3)), np.zeros((nc, 3)), np.zeros(nc, np.int32))
-    imps = gf.NarrowPhaseCollisionDetection(pairs)
+    if pairs is None:  # the device broad phase at the state's positions
+        gf.BroadPhase()
+        imps = gf.NarrowPhaseCollisionDetection(None)
+        pairs = gf.GetPairs()
+    else:
+        imps = gf.NarrowPhaseCollisionDetection(pairs)
     N, nnz = gf.CreateStructure(copy_back=False)
     if args.layout != "auto":
         _lib.check(gf.ctx, gf.lib.icf_set_variant(gf.ctx, 3, 0 if args.layout == "records" else 1))
@@ -497,6 +506,7 @@ def run_ours(args):
                        "specimens_rank0": int(len(coll.meshes)) if batched else 1,
                        "tets": int(n_tet), "czs": int(nc), "nodes": int(n_nodes),
                        "active_rows": int(N), "blocks": int(nnz), "impacts": int(len(imps)),
+                       "pairs": int(len(pairs)),
                        "l2": "flushed between steps (256 MiB write), outside the timed region",
                        "launch_variants": {t["kernel"]: t["variant"] for t in tune if t["chosen"]} or "defaults"},
             # whole assembly against the HBM roofline: the compulsory bytes of

@@ -21,189 +21,9 @@
 
 #include "icf_internal.cuh"
 #include "icf_ppr.cuh"
+#include "icf_tet.cuh"
 
 namespace {
-
-// ---- small vector helpers ---------------------------------------------------
-// A node position (32 B, 32 B aligned: node arrays start on 256 B) in one
-// 256-bit read-only load.
-__device__ __forceinline__ void ld_node(const double4 *__restrict__ p, int i,
-                                        double o[3]) {
-  double w;
-  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
-      : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(w)
-      : "l"(p + i));
-  asm("" ::"d"(w));  // the fourth component is padding
-}
-
-// Orthonormal frame of three points as in fastRotationMatrix
-// (elem_kernels9/matrix_math1.h:32-71): columns unit(p1-p0),
-// unit((p1-p0) x (p2-p0)), unit(col1 x col0).
-__device__ __forceinline__ void frame3(const double p0[3], const double p1[3],
-                                       const double p2[3], double R[3][3]) {
-  double d[3], w[3];
-  for (int k = 0; k < 3; k++) {
-    d[k] = p1[k] - p0[k];
-    w[k] = p2[k] - p0[k];
-  }
-  double r = rsqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-  for (int k = 0; k < 3; k++) R[k][0] = d[k] * r;
-  double c0 = -d[2] * w[1] + d[1] * w[2];
-  double c1 = d[2] * w[0] - d[0] * w[2];
-  double c2 = -d[1] * w[0] + d[0] * w[1];
-  r = rsqrt(c0 * c0 + c1 * c1 + c2 * c2);
-  R[0][1] = c0 * r;
-  R[1][1] = c1 * r;
-  R[2][1] = c2 * r;
-  c0 = R[1][1] * R[2][0] - R[1][0] * R[2][1];
-  c1 = -R[0][1] * R[2][0] + R[0][0] * R[2][1];
-  c2 = R[0][1] * R[1][0] - R[0][0] * R[1][1];
-  r = rsqrt(c0 * c0 + c1 * c1 + c2 * c2);
-  R[0][2] = c0 * r;
-  R[1][2] = c1 * r;
-  R[2][2] = c2 * r;
-}
-
-// ---- tetrahedra ---------------------------------------------------------------
-// Closed form of the reference's K = V B^T E B for isotropic E:
-//   K_ab = V (lam g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I)
-// so that, with h_b = R g_b (R = R1 R0^T, the corotational rotation),
-//   Df_ab = R K_ab R^T = V (lam h_a h_b^T + mu h_b h_a^T + mu (h_a.h_b) I)
-//   f_a   = R sum_b K_ab xr_b = V R sigma(F) g_a,  F = sum_b xr_b g_b^T,
-//           sigma(F) = lam tr(F) I + mu (F + F^T),  xr_b = R^T xc_b - x0_b
-//   sum_b Df_ab v_b = V (lam tr(L) I + mu (L + L^T)) h_a,  L = sum_b v_b h_b^T
-// and the consistent mass is M_ab = rho/20 (1 + delta_ab) I.  The staging
-// record of vertex a is {h_a, V} and {rhs_a, 0}; k_gather rebuilds
-// LHS_ab = stiffCoeff Df_ab + massCoeff M_ab from it.  The record (16
-// double2, 256 B) is written to rec in shared memory.
-template <bool MIXED>
-__device__ __forceinline__ void tet_record(int e, const int4 *__restrict__ elem,
-                                           const double4 *__restrict__ x0,
-                                           const double4 *__restrict__ xc,
-                                           const double2 *__restrict__ va, const icf_dprm &P,
-                                           double2 *rec) {
-  const int4 id = __ldg(elem + e);
-  const int nid[4] = {id.x, id.y, id.z, id.w};
-  double X[4][3], C[4][3], Vn[4][3], An[4][3];
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    ld_node(x0, nid[i], X[i]);
-    ld_node(xc, nid[i], C[i]);
-    const double2 q0 = __ldg(va + 3 * nid[i]), q1 = __ldg(va + 3 * nid[i] + 1),
-                  q2 = __ldg(va + 3 * nid[i] + 2);
-    Vn[i][0] = q0.x; Vn[i][1] = q0.y; Vn[i][2] = q1.x;
-    An[i][0] = q1.y; An[i][1] = q2.x; An[i][2] = q2.y;
-  }
-  // rest volume and shape-function gradients (element_kernels2.h:38-57)
-  const double x12 = X[0][0] - X[1][0], x13 = X[0][0] - X[2][0], x14 = X[0][0] - X[3][0];
-  const double x23 = X[1][0] - X[2][0], x24 = X[1][0] - X[3][0], x34 = X[2][0] - X[3][0];
-  const double y12 = X[0][1] - X[1][1], y13 = X[0][1] - X[2][1], y14 = X[0][1] - X[3][1];
-  const double y23 = X[1][1] - X[2][1], y24 = X[1][1] - X[3][1], y34 = X[2][1] - X[3][1];
-  const double z12 = X[0][2] - X[1][2], z13 = X[0][2] - X[2][2], z14 = X[0][2] - X[3][2];
-  const double z23 = X[1][2] - X[2][2], z24 = X[1][2] - X[3][2], z34 = X[2][2] - X[3][2];
-  const double Jdet = -x12 * (y23 * z34 - y34 * z23) - x23 * (y34 * z12 - y12 * z34) -
-                      x34 * (y12 * z23 - y23 * z12);
-  const double V = Jdet / 6.;
-  const double iJ = 1.0 / Jdet;
-  double g[4][3];
-  g[0][0] = (y24 * z23 - y23 * z24) * iJ;  // a1 = y42 z32 - y32 z42
-  g[0][1] = (x23 * z24 - x24 * z23) * iJ;  // b1 = x32 z42 - x42 z32
-  g[0][2] = (x24 * y23 - x23 * y24) * iJ;  // c1 = x42 y32 - x32 y42
-  g[1][0] = (y13 * z34 - y34 * z13) * iJ;  // a2 = y31 z43 - y34 z13
-  g[1][1] = (x34 * z13 - x13 * z34) * iJ;  // b2 = x43 z31 - x13 z34
-  g[1][2] = (x13 * y34 - x34 * y13) * iJ;  // c2 = x31 y43 - x34 y13
-  g[2][0] = (y24 * z14 - y14 * z24) * iJ;  // a3
-  g[2][1] = (x14 * z24 - x24 * z14) * iJ;  // b3
-  g[2][2] = (x24 * y14 - x14 * y24) * iJ;  // c3
-  g[3][0] = (y12 * z13 - y13 * z12) * iJ;  // a4 = y13 z21 - y12 z31
-  g[3][1] = (x13 * z12 - x12 * z13) * iJ;  // b4 = x21 z13 - x31 z12
-  g[3][2] = (x12 * y13 - x13 * y12) * iJ;  // c4 = x13 y21 - x12 y31
-
-  // corotational rotation R = R1 R0^T (:175-201)
-  double R0[3][3], R1[3][3], R[3][3];
-  frame3(X[0], X[1], X[2], R0);
-  frame3(C[0], C[1], C[2], R1);
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++)
-      R[i][j] = R1[i][0] * R0[j][0] + R1[i][1] * R0[j][1] + R1[i][2] * R0[j][2];
-
-  // F = sum_b (R^T xc_b - x0_b) g_b^T and the stress sigma(F)
-  double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll
-  for (int b = 0; b < 4; b++) {
-    double xr[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-      xr[k] = (C[b][0] * R[0][k] + C[b][1] * R[1][k] + C[b][2] * R[2][k]) - X[b][k];
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-#pragma unroll
-      for (int l = 0; l < 3; l++) F[k][l] += xr[k] * g[b][l];
-  }
-  const double trF = F[0][0] + F[1][1] + F[2][2];
-  double S[3][3];
-#pragma unroll
-  for (int k = 0; k < 3; k++)
-#pragma unroll
-    for (int l = 0; l < 3; l++)
-      S[k][l] = P.mu * (F[k][l] + F[l][k]) + (k == l ? P.lam * trF : 0.0);
-
-  // rotated gradients h_b = R g_b and L = sum_b v_b h_b^T
-  double h[4][3];
-  double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-  double sv[3] = {0, 0, 0}, sa[3] = {0, 0, 0};
-#pragma unroll
-  for (int b = 0; b < 4; b++) {
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-      h[b][k] = R[k][0] * g[b][0] + R[k][1] * g[b][1] + R[k][2] * g[b][2];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      sv[k] += Vn[b][k];
-      sa[k] += An[b][k];
-#pragma unroll
-      for (int l = 0; l < 3; l++) L[k][l] += Vn[b][k] * h[b][l];
-    }
-  }
-  const double trL = L[0][0] + L[1][1] + L[2][2];
-  const double mV = P.rho20 * V;
-  const double gz = P.grav_rho * V / 4;
-
-#pragma unroll
-  for (int a = 0; a < 4; a++) {
-    double sg[3], f[3], dv[3], r[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) sg[k] = S[k][0] * g[a][0] + S[k][1] * g[a][1] + S[k][2] * g[a][2];
-#pragma unroll
-    for (int k = 0; k < 3; k++) f[k] = V * (R[k][0] * sg[0] + R[k][1] * sg[1] + R[k][2] * sg[2]);
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const double Lh = (L[k][0] + L[0][k]) * h[a][0] + (L[k][1] + L[1][k]) * h[a][1] +
-                        (L[k][2] + L[2][k]) * h[a][2];
-      dv[k] = V * (P.lam * trL * h[a][k] + P.mu * Lh);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const double damp = mV * P.dm * (Vn[a][k] + sv[k]) + P.ds * dv[k];
-      const double inert = mV * (An[a][k] + sa[k]);
-      r[k] = (k == 2 ? gz : 0.0) - f[k] - damp - inert;
-    }
-    if (MIXED) {
-      // FP64 rhs; the Hessian inputs rounded to FP32
-      rec[2 * a] = make_double2(r[0], r[1]);
-      rec[2 * a + 1] = make_double2(r[2], 0.0);
-      *reinterpret_cast<float4 *>(rec + 8 + a) =
-          make_float4((float)h[a][0], (float)h[a][1], (float)h[a][2], (float)V);
-    } else {
-      rec[2 * a] = make_double2(h[a][0], h[a][1]);
-      rec[2 * a + 1] = make_double2(h[a][2], V);
-      rec[8 + 2 * a] = make_double2(r[0], r[1]);
-      rec[9 + 2 * a] = make_double2(r[2], 0.0);
-    }
-  }
-}
 
 // One thread per tetrahedron.  Each warp's 32 records (8 KB) are staged in
 // shared memory (rows padded to 272 B, so both the row-wise writes and the
@@ -991,8 +811,9 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     if (rc) return rc;
   }
 
-  // main: tets
-  if (ctx->n_elem > 0)
+  // main: tets (the fused row tiles compute them in place)
+  const bool fused = icf_fused_active(ctx);
+  if (ctx->n_elem > 0 && !fused)
     ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, ctx->d_xc, ctx->d_va, ctx->d_es, s));
   // ids, node state (x0, x_t, v, a) once, 256 B record out
   const bool mixed = ctx->precision == ICF_FP32_MIXED;
@@ -1011,15 +832,17 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     diag_rec = (mixed ? 192 : 256) * ctx->n_elem;
   }
   const long long cz_rec = mixed ? 240 : 8 * ICF_CZ_STAGE;
-  if (ctx->n_elem > 0) icf_prof_mark(ctx, s, "k_tet_unit", 16 * ctx->n_elem + tet_out + 112LL * ctx->n_nodes);
+  if (ctx->n_elem > 0 && !fused)
+    icf_prof_mark(ctx, s, "k_tet_unit", 16 * ctx->n_elem + tet_out + 112LL * ctx->n_nodes);
   ICF_CUDA(ctx, cudaEventRecord(e_tet, s));
 
-  // aux0: CZs
+  // aux0: CZs (on main ahead of the fused tiles, which need their staging)
+  cudaStream_t scz = fused ? s : sa;
   if (ctx->n_cz > 0) {
-    ICF_TRY_RC(icf_launch_cz(ctx, ctx->tune_cz, ctx->d_xc, ctx->d_cs, sa));
+    ICF_TRY_RC(icf_launch_cz(ctx, ctx->tune_cz, ctx->d_xc, ctx->d_cs, scz));
     // ids, six node positions, state in, per-CZ strengths, staging, tentative
     // state, flags and averages out
-    icf_prof_mark(ctx, sa, "k_cz_gp", (24LL + 192 + 52 + (ctx->per_cz_prm ? 32 : 0) + cz_rec + 84) * ctx->n_cz);
+    icf_prof_mark(ctx, scz, "k_cz_gp", (24LL + 192 + 52 + (ctx->per_cz_prm ? 32 : 0) + cz_rec + 84) * ctx->n_cz);
   }
   ICF_CUDA(ctx, cudaEventRecord(e_cz, sa));
 
@@ -1051,7 +874,16 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     icf_prof_mark(ctx, q, name, list_bytes(L, 104, diag_rec, codes_diag, cz));
     return ICF_OK;
   };
-  if (icf_tiles_active(ctx)) {
+  if (fused) {
+    // one kernel computes the tets of each row tile and writes every block;
+    // algorithmic bytes: units, codes, the tets' ids and node state, the CZ
+    // staging once
+    const icf_tiles &T = ctx->tiles;
+    ICF_TRY_RC(icf_launch_tile_fused(ctx, ctx->d_xc, ctx->d_va, ctx->d_cs, sc, mc, ctx->d_vals, ctx->d_rhs, s));
+    icf_prof_mark(ctx, s, "k_tile_fused",
+                  80 * T.n_off_units + 104 * T.n_diag_units + 4 * T.n_real + 16 * T.n_ttet + 112LL * ctx->n_nodes +
+                      cz_rec * ctx->n_cz);
+  } else if (icf_tiles_active(ctx)) {
     // one tiled gather for every block, once the tets and the CZs are staged;
     // algorithmic bytes: units, codes, the tet records and the CZ staging once
     const icf_tiles &T = ctx->tiles;
@@ -1232,6 +1064,10 @@ int icf_launch_assembly(icf_ctx *ctx, double h) {
 }
 
 int icf_launch_node_force(icf_ctx *ctx) {
+  // the fused row tiles keep the tet rhs in shared memory: stage it for the
+  // node sums (the node state is the last assembly's)
+  if (icf_fused_active(ctx) && ctx->n_elem > 0)
+    ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, ctx->d_xc, ctx->d_va, ctx->d_es, ctx->stream));
   icf_node_inc t, m;
   int rc = icf_get_node_inc(ctx, &t, &m);
   if (rc) return rc;
@@ -1315,7 +1151,8 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
     ICF_CUDA(ctx, cudaMemsetAsync(B.rhs, 0, sizeof(double) * 3 * (size_t)ctx->N, s));
   k_pack_nodes<<<icf_blocks(ctx->n_nodes, 256), 256, 0, s>>>(ctx->n_nodes, ctx->d_x0, B.un, B.vn, B.an,
                                                             B.xc, B.va);
-  if (ctx->n_elem > 0)
+  const bool fused = icf_fused_active(ctx);
+  if (ctx->n_elem > 0 && !fused)
     ICF_TRY_RC(icf_launch_tet(ctx, ctx->tune_tet, B.xc, B.va, B.es, s));
   if (ctx->n_cz > 0) {
     ICF_TRY_RC(icf_launch_cz(ctx, ctx->tune_cz, B.xc, B.cs, s));
@@ -1329,7 +1166,9 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
   const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
   if (ctx->n_dyn > 0)
     k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, s>>>(ctx->n_dyn, ctx->d_dynpos, B.vals);
-  if (icf_tiles_active(ctx)) {
+  if (fused) {
+    ICF_TRY_RC(icf_launch_tile_fused(ctx, B.xc, B.va, B.cs, sc, mc, B.vals, B.rhs, s));
+  } else if (icf_tiles_active(ctx)) {
     ICF_TRY_RC(icf_launch_gather_tile(ctx, B.es, B.cs, sc, mc, P.lam, P.mu, B.vals, B.rhs, s));
   } else {
     for (const icf_sell *L : {&ctx->sell_off, &ctx->sell_off_cz})

@@ -10,15 +10,20 @@
 //   2. cell size = the largest box extent, so a box covers at most 2x2x2 cells;
 //      every (cell, element) entry is listed and the entries are sorted by cell
 //      (CUB radix sort);
-//   3. within each cell, every pair a < b of elements of different groups
-//      whose boxes overlap (closed intervals) is a candidate;
+//   3. within each cell, every pair a < b of elements whose boxes overlap
+//      (closed intervals), that share no node and where a vertex of one lies
+//      in the other's box is a candidate (with groups set, only pairs of
+//      different groups);
 //   4. the pairs are sorted (a, b) ascending, a pair found in several cells
 //      is kept once, and the list stays on the device for the narrow phase.
 // The cell size, the cell ranges (the lowest cell and the next along each
 // axis) and the overlap test are those of the host candidate generator the
 // tests compare against, so both give the same set.
-// Groups are the meshes: elements of one mesh never pair (the reference's
-// narrow phase would drop most of them anyway for sharing nodes).
+// Like the reference's BVH, which holds every surface element of every mesh,
+// pairs of one mesh are candidates: across a grain boundary the split node
+// copies let two grains of one mesh interpenetrate, and the narrow phase turns
+// that into impacts.  Optional groups (icf_set_surface_groups) restrict the
+// pairs to different groups.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -127,12 +132,35 @@ __device__ __forceinline__ int upper_key(const unsigned long long *key, int lo, 
   return lo;
 }
 
-__device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, const int *group) {
+// A vertex of one element inside the other's box (closed).
+__device__ __forceinline__ bool vertex_in_box(const int n[4], const double4 *xc, const double *lh) {
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const double4 p = xc[n[v]];
+    if (p.x >= lh[0] && p.x <= lh[3] && p.y >= lh[1] && p.y <= lh[4] && p.z >= lh[2] && p.z <= lh[5])
+      return true;
+  }
+  return false;
+}
+
+// A candidate pair: boxes overlap, no node in common (the narrow phase skips
+// such pairs, kNarrowPhase_new, narrowphase.h:67-70), a vertex of one inside
+// the other's box (an impact needs a vertex inside the other tet, so this
+// drops no pair that can give one), and different groups when groups are set.
+__device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, const int *group,
+                                          const int4 *selem, const double4 *xc) {
   if (group && group[a] == group[b]) return false;
   for (int k = 0; k < 3; k++)
     if (!(lohi[6 * (size_t)a + k] <= lohi[6 * (size_t)b + 3 + k] && lohi[6 * (size_t)b + k] <= lohi[6 * (size_t)a + 3 + k]))
       return false;
-  return true;
+  const int4 p = selem[a], q = selem[b];
+  const int pa[4] = {p.x, p.y, p.z, p.w}, qb[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (pa[i] == qb[j]) return false;
+  return vertex_in_box(pa, xc, lohi + 6 * (size_t)b) || vertex_in_box(qb, xc, lohi + 6 * (size_t)a);
 }
 
 // entry i pairs with the later entries of its cell; count, then write.  With
@@ -141,8 +169,8 @@ __device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, cons
 // of its cell, found by binary search.
 __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const int *__restrict__ elem,
                         const double *__restrict__ lohi, const int *__restrict__ group, int gbits,
-                        const int *__restrict__ off, int *__restrict__ cnt, unsigned long long *__restrict__ out,
-                        long long cap) {
+                        const int4 *__restrict__ selem, const double4 *__restrict__ xc, const int *__restrict__ off,
+                        int *__restrict__ cnt, unsigned long long *__restrict__ out, long long cap) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const unsigned long long here = key[i];
@@ -157,7 +185,7 @@ __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const
   for (int j = j0; j < j1 && (gbits >= 0 || key[j] == here); j++) {
     const int b0 = elem[j];
     const int a = a0 < b0 ? a0 : b0, b = a0 < b0 ? b0 : a0;
-    if (keep_pair(a, b, lohi, group)) {
+    if (keep_pair(a, b, lohi, group, selem, xc)) {
       // beyond the capacity nothing is written; the host sees the total
       // and repeats with a larger buffer
       if (out && o < cap) out[o] = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
@@ -332,7 +360,8 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
   cub::DeviceRadixSort::SortPairs(nullptr, tb, W.ek0, W.ek1, W.ee0, W.ee1, m, 0, end_bit, s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, W.ek0, W.ek1, W.ee0, W.ee1, m, 0, end_bit, s));
-  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, d_group, gbits, nullptr, W.pc, nullptr, 0);
+  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, d_group, gbits, ctx->d_selem, ctx->d_xc,
+                                              nullptr, W.pc, nullptr, 0);
   ICF_CUDA(ctx, cudaMemsetAsync(W.pc + m, 0, sizeof(int), s));
   tb = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb, W.pc, W.po, m + 1, s);
@@ -356,7 +385,8 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     }
     // pad with all-ones keys: they sort after every pair and form one run
     ICF_CUDA(ctx, cudaMemsetAsync(W.p0, 0xFF, sizeof(unsigned long long) * (size_t)P, s));
-    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, d_group, gbits, W.po, nullptr, W.p0, P);
+    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, d_group, gbits, ctx->d_selem, ctx->d_xc,
+                                                W.po, nullptr, W.p0, P);
     tb = 0;
     cub::DeviceRadixSort::SortKeys(nullptr, tb, W.p0, W.p1, (int)P, 0, 64, s);
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;

@@ -19,6 +19,7 @@
 #include <cstdint>
 
 #include "icf_internal.cuh"
+#include "icf_tet.cuh"
 
 namespace {
 
@@ -881,6 +882,98 @@ __global__ void __launch_bounds__(TILE_THREADS, MINB)
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
 }
 
+// ---- the fused row-tile kernel: tets computed in shared memory ---------------------
+// As k_gather_tile, but the CTA computes the records of its tile's tets itself
+// (tet_eval, the arithmetic of k_tet_unit) instead of copying them from the
+// staging the tet kernel writes, so the tet records never reach global
+// memory: no 256 B/tet store and no re-reads by the gathers.  A tet with
+// vertices in several tiles is computed once per tile (about twice).  Shared
+// memory per tet: the four {h_a, V} records (FP64 double4, or FP32-mixed
+// float4) and the 12 FP64 rhs values; then the slice metadata, units and
+// 16-bit tet codes of the tile.  The blocks are summed in the same order
+// from the same values as in k_gather_tile: the results are bit-identical.
+template <typename S, int MINB>
+__global__ void __launch_bounds__(TILE_THREADS, MINB)
+    k_tile_fused(const int4 *__restrict__ tiles, const int2 *__restrict__ trange, const int *__restrict__ ttet,
+                 const int4 *__restrict__ meta, const int2 *__restrict__ unit, const uint16_t *__restrict__ tcodes,
+                 const uint32_t *__restrict__ czcodes, S st, gargs<typename S::real> g,
+                 const int4 *__restrict__ elem, const double4 *__restrict__ x0, const double4 *__restrict__ xc,
+                 const double2 *__restrict__ va, icf_dprm P, double *__restrict__ vals, double *__restrict__ rhs,
+                 int *__restrict__ nonfinite) {
+  typedef typename S::real R;
+  typedef typename S::rec V4;
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  __shared__ int next_slice;
+  const int4 t = tiles[blockIdx.x];
+  const int2 tr = trange[blockIdx.x];
+  V4 *sh = reinterpret_cast<V4 *>(tile_smem);
+  double *srhs = reinterpret_cast<double *>(sh + 4 * t.y);
+  int4 *smeta = reinterpret_cast<int4 *>(srhs + 12 * t.y);
+  int2 *sunit = reinterpret_cast<int2 *>(smeta + t.w);
+  uint16_t *scode = reinterpret_cast<uint16_t *>(sunit + 32 * t.w);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  // the tile's lists arrive by cp.async while the tets are computed
+  for (int q = tid; q < t.w; q += nth) cp16(smeta + q, meta + t.z + q);
+  for (int q = tid; q < 16 * t.w; q += nth) cp16(sunit + 2 * q, unit + 32 * (size_t)t.z + 2 * q);
+  for (int q = tid; q < tr.y / 8; q += nth) cp16(scode + 8 * q, tcodes + tr.x + 8 * q);
+  for (int k = tid; k < t.y; k += nth) {
+    const int e = __ldg(ttet + t.x + k);
+    icf_tet_out o;
+    tet_eval(e, elem, x0, xc, va, P, o);
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      V4 r;
+      r.x = (R)o.h[a][0];
+      r.y = (R)o.h[a][1];
+      r.z = (R)o.h[a][2];
+      r.w = (R)o.V;
+      sh[4 * k + a] = r;
+#pragma unroll
+      for (int c = 0; c < 3; c++) srhs[12 * k + 3 * a + c] = o.r[a][c];
+    }
+  }
+  if (tid == 0) next_slice = nth >> 5;
+  cp_wait_all();
+  __syncthreads();
+  const int lane = tid & 31;
+  bool bad = false;
+  int w = tid >> 5;
+  while (w < t.w) {
+    const int4 m = smeta[w];
+    const int2 u = sunit[32 * w + lane];
+    const bool dg = u.y >= 0;
+    const uint16_t *c = scode + (m.x - tr.x) + lane;
+    R b[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double r[3] = {0, 0, 0};
+    for (int k = 0; k < m.y; k++) {
+      const uint32_t cc = (uint32_t)c[32 * k];
+      const uint32_t lt = cc >> 4, a = (cc >> 2) & 3u, bb = cc & 3u;
+      if (cc == 0xFFFFu || lt >= (uint32_t)t.y) continue;  // padding (the builder checks every code)
+      acc_tet<R, V4>(sh[4 * lt + a], sh[4 * lt + bb], a == bb, g, b);
+      if (a == bb) {
+        const double *q = srhs + 12 * lt + 3 * a;
+        r[0] += q[0];
+        r[1] += q[1];
+        r[2] += q[2];
+      }
+    }
+    cz_codes<S, CZ_UNROLL>(st, czcodes + m.w + lane, 0, m.z, b, dg ? r : nullptr);
+    if (u.x >= 0) {
+      st_block(vals, u.x, b);
+#pragma unroll
+      for (int q = 0; q < 9; q++) bad |= !isfinite((double)b[q]);
+    }
+    if (dg) {
+      st_rhs(rhs, u.y, r);
+      bad |= !(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]));
+    }
+    int nw = 0;
+    if (lane == 0) nw = atomicAdd(&next_slice, 1);
+    w = __shfl_sync(0xffffffffu, nw, 0);
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
+}
+
 #define OFFV(MB, U)                                                                                   \
   {"reg minb" #MB " u" #U, k_gather_off<fp64, MB, U>, k_gather_off<fp32mixed, MB, U>,                \
    k_gather_off_c<fp64, false, MB, U>, k_gather_off_c<fp32mixed, true, MB, U>, 0, false}
@@ -927,6 +1020,10 @@ fp32mixed mixed_views(const icf_ctx *ctx, const double4 *es, const double *cs) {
 // Shared memory of the tiled gather for the largest tile (outside any capture).
 int icf_gather_tile_setup(icf_ctx *ctx) {
   const icf_tiles &T = ctx->tiles;
+  ICF_CUDA(ctx, cudaFuncSetAttribute(k_tile_fused<fp32mixed, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)T.smemf32));
+  ICF_CUDA(ctx, cudaFuncSetAttribute(k_tile_fused<fp64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)T.smemf64));
   ICF_CUDA(ctx, cudaFuncSetAttribute(k_gather_tile<fp32mixed, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)T.smem32));
   ICF_CUDA(ctx, cudaFuncSetAttribute(k_gather_tile<fp64, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -951,6 +1048,29 @@ int icf_launch_gather_tile(icf_ctx *ctx, const double4 *es, const double *cs, do
     k_gather_tile<fp64, 3, 2><<<T.n_tiles, TILE_THREADS, T.smem64, s>>>(T.tiles, T.trange, T.ttet, T.meta, T.unit,
                                                                T.tcodes, T.czcodes, st, g, vals, rhs,
                                                                ctx->d_counts + 4);
+  }
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
+int icf_launch_tile_fused(icf_ctx *ctx, const double4 *xc, const double2 *va, const double *cs, double sc,
+                          double mc, double *vals, double *rhs, cudaStream_t s) {
+  const icf_tiles &T = ctx->tiles;
+  if (T.n_tiles == 0) return ICF_OK;
+  const icf_dprm P = icf_make_dprm(ctx);
+  if (ctx->precision == ICF_FP32_MIXED) {
+    const gargs<float> g{(float)sc, (float)mc, (float)P.lam, (float)P.mu};
+    k_tile_fused<fp32mixed, 2><<<T.n_tiles, TILE_THREADS, T.smemf32, s>>>(
+        T.tiles, T.trange, T.ttet, T.meta, T.unit, T.tcodes, T.czcodes, mixed_views(ctx, ctx->d_es, cs), g,
+        ctx->d_elem, ctx->d_x0, xc, va, P, vals, rhs, ctx->d_counts + 4);
+  } else {
+    fp64 st;
+    st.es = nullptr;
+    st.cs = cs;
+    const gargs<double> g{sc, mc, P.lam, P.mu};
+    k_tile_fused<fp64, 2><<<T.n_tiles, TILE_THREADS, T.smemf64, s>>>(
+        T.tiles, T.trange, T.ttet, T.meta, T.unit, T.tcodes, T.czcodes, st, g, ctx->d_elem, ctx->d_x0, xc, va, P,
+        vals, rhs, ctx->d_counts + 4);
   }
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;

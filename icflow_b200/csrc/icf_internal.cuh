@@ -100,6 +100,7 @@ struct icf_tiles {
   long long n_ttet = 0, n_tcodes = 0, n_czcodes = 0, n_real = 0;
   long long n_diag_units = 0, n_off_units = 0;
   size_t smem64 = 0, smem32 = 0;  // shared memory of the largest tile
+  size_t smemf64 = 0, smemf32 = 0;  // ... for the fused kernel (tets computed in place)
   int4 *tiles = nullptr;
   int2 *trange = nullptr;
   int *ttet = nullptr;
@@ -256,9 +257,10 @@ struct icf_ctx {
   // in sell_off / sell_diag.
   icf_sell sell_off, sell_diag, sell_off_cz, sell_diag_cz;
   bool split_cz = false;
-  // row-tile gather (one kernel for all blocks) instead of the two list gathers
+  // row-tile gather (one kernel for all blocks) instead of the two list gathers;
+  // fused_tiles: the tile kernel computes its tets itself (no tet kernel)
   icf_tiles tiles;
-  bool gather_tiles = false;
+  bool gather_tiles = false, fused_tiles = false;
   // the two list gathers one after the other on the main stream instead of
   // side by side
   bool serial_gathers = false;
@@ -382,6 +384,10 @@ int icf_gather_tile_setup(icf_ctx *ctx);
 bool icf_tiles_active(const icf_ctx *ctx);
 int icf_launch_gather_tile(icf_ctx *ctx, const double4 *es, const double *cs, double sc, double mc, double lam,
                            double mu, double *vals, double *rhs, cudaStream_t s);
+// the fused row-tile kernel (tets computed in shared memory) over node state xc, va
+int icf_launch_tile_fused(icf_ctx *ctx, const double4 *xc, const double2 *va, const double *cs, double sc,
+                          double mc, double *vals, double *rhs, cudaStream_t s);
+inline bool icf_fused_active(const icf_ctx *ctx) { return ctx->fused_tiles && icf_tiles_active(ctx); }
 int icf_rebuild_lists(icf_ctx *ctx);  // both gathers' lists for the current layout and split
 int icf_remap_lists(icf_ctx *ctx);    // their units' slots for the current structure
 // 1 for a merged slot that the off-diagonal gather writes: static, off the diagonal

@@ -164,7 +164,7 @@ int icf_build_tiles(icf_ctx *ctx) {
   std::vector<int> tets;
   std::vector<unit_rec> units;
   long long n_real = 0, n_dg = 0, n_off = 0;
-  size_t smem64 = 0, smem32 = 0;
+  size_t smem64 = 0, smem32 = 0, smemf64 = 0, smemf32 = 0;
   for (int t = 0; t < nt_tiles; t++) {
     tets.clear();
     units.clear();
@@ -221,6 +221,9 @@ int icf_build_tiles(icf_ctx *ctx) {
     const size_t rest = 16 * (size_t)ns + 256 * (size_t)ns + 2 * nc16 + 4 * tets.size();
     smem64 = std::max(smem64, 128 * tets.size() + rest);
     smem32 = std::max(smem32, 64 * tets.size() + rest);
+    // fused: the records and 12 rhs values per tet, no tet ids
+    smemf64 = std::max(smemf64, (128 + 96) * tets.size() + rest - 4 * tets.size());
+    smemf32 = std::max(smemf32, (64 + 96) * tets.size() + rest - 4 * tets.size());
   }
   if (h_tcodes.size() >= (size_t)INT32_MAX || h_czcodes.size() >= (size_t)INT32_MAX || smem64 > 200 * 1024)
     return ICF_OK;  // offsets are 32-bit, shared memory bounded: the list gathers serve
@@ -250,6 +253,8 @@ int icf_build_tiles(icf_ctx *ctx) {
   T.n_off_units = n_off;
   T.smem64 = smem64;
   T.smem32 = smem32;
+  T.smemf64 = smemf64;
+  T.smemf32 = smemf32;
   T.ok = true;
   ICF_TRY_RC(icf_gather_tile_setup(ctx));
   return icf_remap_tiles(ctx);

@@ -61,14 +61,16 @@ int icf_set_variant_impl(icf_ctx *ctx, int kind, int variant) {
                           : kind == 2 ? icf_gather_variants(1)
                           : kind == 3 ? 2
                           : kind == 5 ? 2
-                          : kind == 6 ? 2
+                          : kind == 6 ? 3
                           : kind == 7 ? 2
                                       : icf_cz_variants();
   if (kind < 0 || kind > 7 || variant < 0 || variant >= n)
     return icf_fail(ctx, ICF_ERR_ARG, "icf_set_variant: kind 0..7 and a variant index of that kind");
   if (kind == 7) ctx->serial_gathers = variant == 1;
   if (kind == 6) {
-    ctx->gather_tiles = variant == 1;
+    ctx->gather_tiles = variant >= 1;
+    if (ctx->fused_tiles != (variant == 2)) ctx->version++;
+    ctx->fused_tiles = variant == 2;
     if (ctx->gather_tiles && ctx->have_structure && !ctx->tiles.built) {
       ICF_TRY_RC(icf_build_tiles(ctx));
       ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -114,7 +116,8 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
     ctx->version++;  // re-capture with the candidate's kernels
     return time_launches(ctx, t, reps, [&] { return icf_launch_assembly(ctx, h); }, ms);
   };
-  int split = ctx->split_cz ? 1 : 0, tiles = ctx->gather_tiles ? 1 : 0, serial = ctx->serial_gathers ? 1 : 0;
+  int split = ctx->split_cz ? 1 : 0, tiles = ctx->fused_tiles ? 2 : (ctx->gather_tiles ? 1 : 0),
+      serial = ctx->serial_gathers ? 1 : 0;
   struct kind_desc {
     const char *name;
     int kind, n;
@@ -122,7 +125,7 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
   };
   const kind_desc kinds[] = {
       {"layout", 3, 2, &ctx->layout},
-      {"gather", 6, 2, &tiles},
+      {"gather", 6, 3, &tiles},
       {"split", 5, ctx->n_cz > 0 ? 2 : 0, &split},
       {"streams", 7, 2, &serial},
       {"k_tet_unit", 0, ctx->n_elem > 0 ? icf_tet_variants() : 0, &ctx->tune_tet},
@@ -132,12 +135,14 @@ int icf_autotune_impl(icf_ctx *ctx, double h, int reps, icf_tune_report *out) {
   };
   const char *layout_names[2] = {"per-tet records", "per-contribution stream"};
   const char *split_names[2] = {"one list per gather", "CZ-free units apart"};
-  const char *gather_names[2] = {"off-diagonal + diagonal lists", "row tiles"};
+  const char *gather_names[3] = {"off-diagonal + diagonal lists", "row tiles", "fused row tiles"};
   const char *stream_names[2] = {"gathers side by side", "gathers one after other"};
   for (const kind_desc &k : kinds) {
     if (k.n < 2) continue;
     // the list gathers' choices do not matter while the tiled gather runs
     if ((k.kind == 1 || k.kind == 2 || k.kind == 5 || k.kind == 7) && icf_tiles_active(ctx)) continue;
+    // the fused tiles compute the tets themselves: no tet kernel to tune
+    if (k.kind == 0 && icf_fused_active(ctx)) continue;
     // the stream placement matters only for one list per gather
     if (k.kind == 7 && ctx->split_cz && ctx->layout == ICF_LAYOUT_RECORDS) continue;
     // nor the tiled gather under the per-contribution layout

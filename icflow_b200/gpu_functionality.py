@@ -103,7 +103,7 @@ class GPU_Functionality:
 
     # -- TransferStaticDataToDevice (:255-302) --
     def TransferStaticDataToDevice(self):
-        self._groups_set = False
+        self._groups_same_mesh = True  # a new context has no groups: every pair
         mc = self.mc
         x0 = np.ascontiguousarray(mc.x0, np.float64)
         el = np.ascontiguousarray(mc.elems, np.int32)
@@ -130,14 +130,17 @@ class GPU_Functionality:
                                                        iptr(failed)))
 
     # -- broad phase on the device (replaces the host BVH, BVHT.cs:29-77) --
-    def BroadPhase(self, pad: float = 0.0) -> int:
-        """Candidate surface-element pairs of different meshes with
-        overlapping boxes at the current positions; they stay on the device
-        for NarrowPhaseCollisionDetection(None)."""
-        if not getattr(self, "_groups_set", False):
-            grp = np.ascontiguousarray(self.mc.selem_mesh, np.int32)
-            check(self.ctx, self.lib.icf_set_surface_groups(self.ctx, len(grp), iptr(grp)))
-            self._groups_set = True
+    def BroadPhase(self, pad: float = 0.0, same_mesh: bool = True) -> int:
+        """Candidate surface-element pairs with overlapping boxes at the
+        current positions that share no node, as the reference's BVH lists
+        them (BVHT.cs:29-77: every surface element of every mesh, so pairs of
+        one mesh too); same_mesh=False keeps only pairs of different meshes.
+        The pairs stay on the device for NarrowPhaseCollisionDetection(None)."""
+        if getattr(self, "_groups_same_mesh", None) != same_mesh:
+            grp = None if same_mesh else np.ascontiguousarray(self.mc.selem_mesh, np.int32)
+            check(self.ctx, self.lib.icf_set_surface_groups(self.ctx, len(self.mc.selem_mesh),
+                                                            iptr(grp) if grp is not None else None))
+            self._groups_same_mesh = same_mesh
         n = C.c_int()
         check(self.ctx, self.lib.icf_broad_phase(self.ctx, float(pad), C.byref(n)))
         self.nPairs = n.value

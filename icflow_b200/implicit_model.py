@@ -118,6 +118,8 @@ class ImplicitModel3:
         # object with record(model, h, u, v, a, du_prev, du_prev2, du_accepted),
         # called after every accepted step (training data for a warm start)
         self.recorder = None
+        # when a list: the impact list of every Newton iteration (contact runs)
+        self.trace = None
         # accepted increments of the two previous steps (learned warm start inputs)
         self.du_prev = np.zeros((n, 3))
         self.du_prev2 = np.zeros((n, 3))
@@ -206,6 +208,8 @@ class ImplicitModel3:
             if self.contact:
                 self._contact()
                 self._n_imp = gf.nImpacts
+                if self.trace is not None:
+                    self.trace.append(gf.c_itet.copy())
             gf.CreateStructure(copy_back=False)
             return gf.AssembleElemsAndCZs(h)
 

@@ -285,12 +285,19 @@ def _adjacent_faces(el: np.ndarray, faces: np.ndarray, n_nodes: int):
 
 
 def candidate_pairs(coll: Collection, xt: np.ndarray, pad: float = 0.0,
-                    max_pairs: int | None = None) -> np.ndarray:
-    """Surface-element pairs of different meshes whose bounding boxes overlap.
+                    max_pairs: int | None = None, same_mesh: bool = True,
+                    vertex_in_box: bool = True) -> np.ndarray:
+    """Surface-element pairs whose bounding boxes overlap, that share no node
+    and where a vertex of one lies in the other's box; with same_mesh=False
+    only pairs of different meshes.
 
-    Stand-in for the k-DOP broad phase (v3Library/Collisions/BVH), which is not
-    part of the assembly path; only the pair list it hands to the narrow phase
-    matters here.  Returns [n, 2] int32 surface-element ids."""
+    Host stand-in for the reference's k-DOP broad phase (v3Library/Collisions/
+    BVH), whose tree holds every surface element of every mesh: pairs of one
+    mesh are candidates too, and across a grain boundary (split nodes) they
+    give impacts.  Pairs are also dropped unless a vertex of one element lies
+    in the other's box, which every impact needs.  A k-DOP contains the box's
+    slabs, so these pairs include every k-DOP pair that can give an impact.
+    Returns [n, 2] int32 surface-element ids, ascending."""
     se = coll.selem
     lo = xt[se].min(axis=1) - pad
     hi = xt[se].max(axis=1) + pad
@@ -320,9 +327,20 @@ def candidate_pairs(coll: Collection, xt: np.ndarray, pad: float = 0.0,
             continue
         a, b = np.meshgrid(m, m, indexing="ij")
         a, b = a.ravel(), b.ravel()
-        k = (a < b) & (mesh_of[a] != mesh_of[b])
+        k = a < b
+        if not same_mesh:
+            k &= mesh_of[a] != mesh_of[b]
         a, b = a[k], b[k]
         ov = np.all((lo[a] <= hi[b]) & (lo[b] <= hi[a]), axis=1)
+        a, b = a[ov], b[ov]
+        ov = ~(se[a][:, :, None] == se[b][:, None, :]).any(axis=(1, 2))
+        if vertex_in_box:
+            # a vertex of one inside the other's box: an impact needs a vertex
+            # inside the other tet
+            a, b = a[ov], b[ov]
+            va, vb = xt[se[a]], xt[se[b]]
+            ov = (np.all((va >= lo[b][:, None]) & (va <= hi[b][:, None]), axis=2).any(axis=1) |
+                  np.all((vb >= lo[a][:, None]) & (vb <= hi[a][:, None]), axis=2).any(axis=1))
         if ov.any():
             out.append(np.stack([a[ov], b[ov]], 1))
     if not out:

@@ -15,6 +15,7 @@
  */
 #include "icf_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1072,6 +1073,169 @@ void orc_narrow_phase(int n_pairs, const int *pairs, const int *selem,
       }
     masks[i] = orc_narrow_mask(xa, xb, na, nb);
   }
+}
+
+/* kDOP24.Expand(x, y, z) (kDOP24.cs:115-141): the 12 slab directions in the
+ * reference's order, lower bounds d0..d11, upper bounds d12..d23. */
+static void kdop_expand(double d[24], double x, double y, double z) {
+  const double pr[12] = {x, y, z, x + y, x + z, y + z, x - y, x - z, y - z, x + y - z, x + z - y, y + z - x};
+  for (int k = 0; k < 12; k++) {
+    if (pr[k] < d[k]) d[k] = pr[k];
+    if (pr[k] > d[12 + k]) d[12 + k] = pr[k];
+  }
+}
+
+/* kDOP24.Overlaps (kDOP24.cs:84-113). */
+static int kdop_overlaps(const double *a, const double *b) {
+  for (int k = 0; k < 12; k++)
+    if (a[k] > b[12 + k] || a[12 + k] < b[k]) return 0;
+  return 1;
+}
+
+int orc_kdop_pairs(int n_selem, const int *selem, const double *xt, int *out, long long cap) {
+  double *d = (double *)malloc(sizeof(double) * 24 * (size_t)(n_selem > 0 ? n_selem : 1));
+  if (!d) return -1;
+  for (int e = 0; e < n_selem; e++) {
+    double *q = d + 24 * (size_t)e;
+    for (int k = 0; k < 12; k++) {  /* Reset(): +max / -max (kDOP24.cs:60-64) */
+      q[k] = DBL_MAX;
+      q[12 + k] = -DBL_MAX;
+    }
+    for (int v = 0; v < 4; v++) {
+      const int n = selem[4 * e + v];
+      kdop_expand(q, xt[3 * n], xt[3 * n + 1], xt[3 * n + 2]);
+    }
+  }
+  long long np = 0;
+  for (int a = 0; a < n_selem; a++)
+    for (int b = a + 1; b < n_selem; b++)
+      if (kdop_overlaps(d + 24 * (size_t)a, d + 24 * (size_t)b)) {
+        if (np >= cap) {
+          free(d);
+          return -1;
+        }
+        out[2 * np] = a;
+        out[2 * np + 1] = b;
+        np++;
+      }
+  free(d);
+  return (int)np;
+}
+
+typedef struct {
+  unsigned long long key;
+  int elem;
+} cell_entry;
+static int cmp_entry(const void *a, const void *b) {
+  const cell_entry *x = (const cell_entry *)a, *y = (const cell_entry *)b;
+  if (x->key != y->key) return (x->key > y->key) - (x->key < y->key);
+  return (x->elem > y->elem) - (x->elem < y->elem);
+}
+static int cmp_ull(const void *a, const void *b) {
+  const unsigned long long x = *(const unsigned long long *)a, y = *(const unsigned long long *)b;
+  return (x > y) - (x < y);
+}
+
+static int vert_in_box(const int *n, const double *xt, const double *lo, const double *hi) {
+  for (int v = 0; v < 4; v++) {
+    const double *p = xt + 3 * n[v];
+    if (p[0] >= lo[0] && p[0] <= hi[0] && p[1] >= lo[1] && p[1] <= hi[1] && p[2] >= lo[2] && p[2] <= hi[2])
+      return 1;
+  }
+  return 0;
+}
+
+long long orc_candidate_pairs(int n, const int *selem, const int *group, const double *xt, double pad,
+                              int *out, long long cap) {
+  if (n < 2) return 0;
+  double *lo = (double *)malloc(sizeof(double) * 6 * (size_t)n), *hi = lo + 3 * (size_t)n;
+  cell_entry *ent = (cell_entry *)malloc(sizeof(cell_entry) * 8 * (size_t)n);
+  if (!lo || !ent) {
+    free(lo);
+    free(ent);
+    return -1;
+  }
+  double cell = 0.0, base[3] = {DBL_MAX, DBL_MAX, DBL_MAX};
+  for (int e = 0; e < n; e++)
+    for (int k = 0; k < 3; k++) {
+      double a = DBL_MAX, b = -DBL_MAX;
+      for (int v = 0; v < 4; v++) {
+        const double x = xt[3 * selem[4 * e + v] + k];
+        a = x < a ? x : a;
+        b = x > b ? x : b;
+      }
+      lo[3 * e + k] = a - pad;
+      hi[3 * e + k] = b + pad;
+      if (hi[3 * e + k] - lo[3 * e + k] > cell) cell = hi[3 * e + k] - lo[3 * e + k];
+      if (lo[3 * e + k] < base[k]) base[k] = lo[3 * e + k];
+    }
+  if (!(cell > 0)) cell = 1.0;
+  long long m = 0;
+  for (int e = 0; e < n; e++) {
+    long long c0[3], c1[3];
+    for (int k = 0; k < 3; k++) {
+      c0[k] = (long long)floor((lo[3 * e + k] - base[k]) / cell);
+      c1[k] = (long long)floor((hi[3 * e + k] - base[k]) / cell);
+    }
+    for (long long x = c0[0]; x <= c1[0] && x <= c0[0] + 1; x++)
+      for (long long y = c0[1]; y <= c1[1] && y <= c0[1] + 1; y++)
+        for (long long z = c0[2]; z <= c1[2] && z <= c0[2] + 1; z++) {
+          ent[m].key = ((unsigned long long)x << 42) | ((unsigned long long)y << 21) | (unsigned long long)z;
+          ent[m].elem = e;
+          m++;
+        }
+  }
+  qsort(ent, (size_t)m, sizeof(cell_entry), cmp_entry);
+  long long np = 0, pcap = 16 * (long long)n + 1024;
+  unsigned long long *pk = (unsigned long long *)malloc(sizeof(unsigned long long) * (size_t)pcap);
+  for (long long i = 0; i < m && pk; i++)
+    for (long long j = i + 1; j < m && ent[j].key == ent[i].key; j++) {
+      int a = ent[i].elem, b = ent[j].elem;
+      if (a > b) {
+        const int t = a;
+        a = b;
+        b = t;
+      }
+      if (group && group[a] == group[b]) continue;
+      int ov = 1;
+      for (int k = 0; k < 3; k++)
+        if (!(lo[3 * a + k] <= hi[3 * b + k] && lo[3 * b + k] <= hi[3 * a + k])) ov = 0;
+      if (!ov) continue;
+      const int *na = selem + 4 * a, *nb = selem + 4 * b;
+      int shared = 0;
+      for (int p = 0; p < 4; p++)
+        for (int q = 0; q < 4; q++) shared |= na[p] == nb[q];
+      if (shared) continue;
+      if (!vert_in_box(na, xt, lo + 3 * b, hi + 3 * b) && !vert_in_box(nb, xt, lo + 3 * a, hi + 3 * a)) continue;
+      if (np == pcap) {
+        pcap *= 2;
+        unsigned long long *q = (unsigned long long *)realloc(pk, sizeof(unsigned long long) * (size_t)pcap);
+        if (!q) {
+          free(pk);
+          pk = NULL;
+          break;
+        }
+        pk = q;
+      }
+      pk[np++] = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
+    }
+  free(lo);
+  free(ent);
+  if (!pk) return -1;
+  qsort(pk, (size_t)np, sizeof(unsigned long long), cmp_ull);
+  long long u = 0;
+  for (long long i = 0; i < np; i++) {
+    if (i > 0 && pk[i] == pk[i - 1]) continue;
+    if (u >= cap) {
+      free(pk);
+      return -1;
+    }
+    out[2 * u] = (int)(pk[i] >> 32);
+    out[2 * u + 1] = (int)(pk[i] & 0xffffffffu);
+    u++;
+  }
+  free(pk);
+  return u;
 }
 
 static int cmp_ll(const void *a, const void *b) {

@@ -127,6 +127,23 @@ int orc_impacts(int n_pairs, const int *pairs, const int *masks,
                 const int *selem, const int *adj_off, const int *adj_faces,
                 const int *faces, const double *xt, int *out, int cap);
 
+/* Broad phase of the reference: the element pairs its k-DOP-24 bounding
+ * volume hierarchy reports (BVHT.cs:29-77).  Every surface element gets the
+ * 24-plane k-DOP of its tentative vertices (kDOP24.cs:69-141); a node's box
+ * contains its children's (BVHN.cs:39-161), so the self-collide traversal
+ * (BVHN.cs:166-194) lists exactly the unordered leaf pairs whose k-DOPs
+ * overlap (kDOP24.cs:84-113), whatever the tree's shape.  out[2*i] < out[2*i+1],
+ * pairs ascending.  Returns the pair count, or -1 if cap is exceeded. */
+int orc_kdop_pairs(int n_selem, const int *selem, const double *xt, int *out, long long cap);
+
+/* The candidate pairs the device broad phase hands the narrow phase, by a
+ * uniform grid on the host: surface elements a < b whose boxes at xt overlap
+ * (closed), that share no node and where a vertex of one lies in the other's
+ * box; with group != NULL only pairs of different groups.  out[2*i] <
+ * out[2*i+1], ascending.  Returns the count, or -1 if cap is exceeded. */
+long long orc_candidate_pairs(int n_selem, const int *selem, const int *group, const double *xt,
+                              double pad, int *out, long long cap);
+
 /* Newmark predictor (Node.cs:89-97 with :79-87) and commit (Node.cs:62-77). */
 void orc_newmark_infer(int n, double h, double beta, double gamma,
                        const double *x0, const double *u, const double *v,

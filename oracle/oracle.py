@@ -219,6 +219,30 @@ class Oracle:
                                 _d(np.ascontiguousarray(xt, np.float64)), _i(masks))
         return masks[:len(pairs)]
 
+    def candidate_pairs(self, selem, xt, group=None, pad: float = 0.0, cap: int = 80_000_000):
+        """The device broad phase's pair rule on the host (grid; boxes
+        overlap, no shared node, a vertex of one in the other's box)."""
+        selem = np.ascontiguousarray(selem, np.int32)
+        out = np.zeros(2 * cap, np.int32)
+        g = None if group is None else np.ascontiguousarray(group, np.int32)
+        self.L.orc_candidate_pairs.restype = C.c_longlong
+        n = self.L.orc_candidate_pairs(len(selem), _i(selem), _i(g), _d(np.ascontiguousarray(xt, np.float64)),
+                                       C.c_double(pad), _i(out), C.c_longlong(cap))
+        if n < 0:
+            raise RuntimeError("candidate pair buffer too small")
+        return out[:2 * n].reshape(-1, 2).copy()
+
+    def kdop_pairs(self, selem, xt, cap: int = 20_000_000):
+        """The element pairs the reference's k-DOP-24 BVH reports (all
+        unordered surface-element pairs whose k-DOPs overlap), ascending."""
+        selem = np.ascontiguousarray(selem, np.int32)
+        out = np.zeros(2 * cap, np.int32)
+        n = self.L.orc_kdop_pairs(len(selem), _i(selem), _d(np.ascontiguousarray(xt, np.float64)), _i(out),
+                                  C.c_longlong(cap))
+        if n < 0:
+            raise RuntimeError("k-DOP pair buffer too small")
+        return out[:2 * n].reshape(-1, 2).copy()
+
     def impacts(self, pairs, masks, selem, adj_off, adj, faces, xt):
         pairs = np.ascontiguousarray(pairs, np.int32)
         cap = 8 * max(len(pairs), 1)

@@ -128,7 +128,7 @@ def main():
     un = (r3.random((nn, 3)) - 0.5) * 2e-7
     un[c.anchored] = 0
     xt = c.x0 + un
-    pairs = M.candidate_pairs(c, xt)
+    pairs = M.candidate_pairs(c, xt, same_mesh=False, vertex_in_box=False)
     st = R.pack_nodes(c.x0, un, np.zeros((nn, 3)), np.zeros((nn, 3)))
     masks, ie, el_stride = R.narrow_phase_kernel(st, nn, pairs, c.selem, c.adj_off, c.adj)
     keys = set()

@@ -2,8 +2,11 @@
 the same time step (ImplicitModel3.Step, ImplicitModel3.cs:369-435) with the
 oracle's assembly (oracle/icf_oracle.c), the oracle's Newmark predictor and
 commit (Node.cs:62-97) and a direct sparse solve (SuperLU on the symmetric
-matrix, standing in for PARDISO, LinearSystem.cs:48-64).  Test
-infrastructure only."""
+matrix, standing in for PARDISO, LinearSystem.cs:48-64).  With contact, every
+Newton iteration runs the oracle's narrow phase and closest-face search on the
+candidate pairs of the tentative positions, adds the impacts to the structure
+(_addCollidingNodesToStructure, :177-196) and assembles their penalty terms.
+Test infrastructure only."""
 from __future__ import annotations
 
 import numpy as np
@@ -23,7 +26,7 @@ def full_matrix(N: int, rows: np.ndarray, cols: np.ndarray, vals: np.ndarray) ->
 
 
 class OracleModel:
-    def __init__(self, coll, prms, strengths=None, v0=None):
+    def __init__(self, coll, prms, strengths=None, v0=None, contact=False):
         self.O = O = Oracle()
         keys = ("Y", "nu", "rho", "dampingMass", "dampingStiffness", "gravity", "NewmarkBeta", "NewmarkGamma",
                 "alpha", "beta", "lambda_n", "lambda_t", "phi_n", "phi_t", "sigma_max", "tau_max", "penaltyK",
@@ -44,6 +47,10 @@ class OracleModel:
         self.t = 0.0
         self.active = ~coll.anchored
         self.iterations = []
+        self.contact = contact
+        self.trace = []  # per Newton iteration: the impact list
+        # per step: CZs newly damaged and failed (the counters _checkDamage reads)
+        self.damage_counts = []
         imps = np.zeros((0, 4), np.int32)
         # static pattern from every CZ (never shrinks), as the device keeps it
         self.N, self.rows, self.cols = O.build_structure(coll.alt, coll.elems, coll.czs, imps)
@@ -74,13 +81,28 @@ class OracleModel:
         ip = np.zeros((0, 20), np.int32)
         alt = c.alt
         act = np.nonzero(alt >= 0)[0]
+        N, rows, cols, ep, cp = self.N, self.rows, self.cols, self.ep, self.cp
         while True:
             un, vn, an, xt = O.newmark_infer(h, p.NewmarkBeta, p.NewmarkGamma, c.x0, self.u, self.v, self.a, du)
+            if self.contact:
+                from icflow_b200 import mesh as M
+
+                pairs = M.candidate_pairs(c, xt)
+                if len(pairs):
+                    masks = O.narrow_phase(pairs, c.selem, xt)
+                    imps = O.impacts(pairs, masks, c.selem, c.adj_off, c.adj, c.faces, xt)
+                else:
+                    imps = np.zeros((0, 4), np.int32)
+                self.trace.append(imps.copy())
+                N, rows, cols = O.build_structure(c.alt, c.elems, c.czs, imps)
+                ep = O.pcsr(c.elems, 4, c.alt, rows, cols, N)
+                cp = O.pcsr(c.czs, 6, c.alt, rows, cols, N)
+                ip = O.pcsr(imps, 4, c.alt, rows, cols, N)
             live = np.nonzero(self.failed == 0)[0]
-            res = O.assemble(self.p, h, c.x0, un, vn, an, c.elems, self.ep, c.czs[live], self.cp[live],
-                             self.pmax[live], self.tmax[live], imps, ip, len(self.cols), self.N,
+            res = O.assemble(self.p, h, c.x0, un, vn, an, c.elems, ep, c.czs[live], cp[live],
+                             self.pmax[live], self.tmax[live], imps, ip, len(cols), N,
                              cz_ppr=None if self.q is None else [self.q[i] for i in live])
-            A = full_matrix(self.N, self.rows, self.cols, res["vals"])
+            A = full_matrix(N, rows, cols, res["vals"])
             dx = spla.spsolve(A, res["rhs"].ravel()).reshape(-1, 3)
             du[act] += dx[alt[act]]
             norm = float((dx * dx).sum())
@@ -90,6 +112,7 @@ class OracleModel:
                 break
         self.u, self.v, self.a, _, _ = O.newmark_accept(h, c.x0, self.u, self.v, self.a, un, du)
         tent, flags = res["tent"], res["flags"]
+        self.damage_counts.append((int((flags[:, 1] != 0).sum()), int((flags[:, 2] != 0).sum())))
         self.pmax[live] = tent[:, :1]
         self.tmax[live] = tent[:, 1:2]
         self.failed[live] |= (flags[:, 2] != 0).astype(np.int32)

@@ -5,8 +5,10 @@ compressed state, per-boundary strengths, broad-phase pairs); these tests
 assemble the same inputs through the C ABI, with the launch variants the
 autotuner picks (as bench.py does), and compare with the CPU oracle:
 
-  cfg1  polycrystal compression, 196,608 tets, 34,819 CZs, 3,011 impacts:
-        masks, impacts, csr_rows/cols and every slot map bit-exact; blocks
+  cfg1  polycrystal compression, 196,608 tets, 34,819 CZs, ~22,700 impacts
+        (platens and grain boundaries): the device broad phase's pair set
+        equals the host rule's; masks, impacts, csr_rows/cols and every slot
+        map bit-exact; blocks
         within 1e-12 per block row; rhs within 1e-12; CZ flags equal;
         tentative state and averages within 1e-12.
   cfg2  the same at 1,572,864 tets in FP64 (same bar), then in FP32-mixed with
@@ -48,6 +50,7 @@ def _gf(coll, sig, precision, tune):
 
 
 def _oracle(O, prms, coll, state, sig, pairs):
+    """The oracle's narrow phase, impacts and assembly on the given pairs."""
     p = orc_prms_from(O, prms)
     xt = coll.x0 + state[0]
     masks = O.narrow_phase(pairs, coll.selem, xt) if len(pairs) else np.zeros(0, np.int32)
@@ -56,6 +59,15 @@ def _oracle(O, prms, coll, state, sig, pairs):
     nc = len(coll.czs)
     o = oracle_assemble(O, p, coll, state, H, np.zeros((nc, 3)), np.zeros((nc, 3)), imps, cz_sigma=(sig, sig))
     return o, masks, imps
+
+
+def _device_pairs(gf, coll, state):
+    """The device broad phase's pairs at the state's positions (as bench.py
+    builds the workload)."""
+    un, vn, an = state
+    gf.TransferNodesToGPU(un, vn, an)
+    gf.BroadPhase()
+    return gf.GetPairs()
 
 
 def _gpu(gf, coll, state, pairs, tune):
@@ -92,9 +104,12 @@ def _mixed_report(g, o):
 
 @pytest.mark.gpu
 def test_cfg1_bench_workload_parity():
-    coll, state, sig, pairs, _ = bench.build_workload("cfg1", 0)
+    coll, state, sig, _, _ = bench.build_workload("cfg1", 0)
     O = Oracle()
     gf, prms = _gf(coll, sig, 0, True)
+    pairs = _device_pairs(gf, coll, state)
+    # the broad phase's pair set is the host rule's (oracle/icf_oracle.c)
+    assert np.array_equal(pairs, O.candidate_pairs(coll.selem, coll.x0 + state[0]))
     g = _gpu(gf, coll, state, pairs, tune=True)
     o, masks, imps = _oracle(O, prms, coll, state, sig, pairs)
     assert np.array_equal(gf.NarrowPhaseMasks(len(pairs)), masks)
@@ -107,9 +122,10 @@ def test_cfg1_bench_workload_parity():
 
 @pytest.mark.gpu
 def test_cfg2_bench_workload_fp64_parity_and_mixed_error():
-    coll, state, sig, pairs, _ = bench.build_workload("cfg2", 0)
+    coll, state, sig, _, _ = bench.build_workload("cfg2", 0)
     O = Oracle()
     gf, prms = _gf(coll, sig, 0, True)
+    pairs = _device_pairs(gf, coll, state)
     g = _gpu(gf, coll, state, pairs, tune=False)
     o, masks, imps = _oracle(O, prms, coll, state, sig, pairs)
     assert np.array_equal(gf.NarrowPhaseMasks(len(pairs)), masks)

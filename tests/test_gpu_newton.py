@@ -1,7 +1,7 @@
 """Whole time steps on the device (ImplicitModel3 mirror): N-step parity of
 displacements and damage state with the CPU twin (oracle assembly + direct
-solve), FP32-mixed against FP64 at equal converged displacements, and a
-contact run."""
+solve), without and with contact, FP32-mixed against FP64 at equal converged
+displacements."""
 import numpy as np
 import pytest
 
@@ -94,4 +94,48 @@ def test_contact_steps_converge():
         s = g.Step()
         assert s.converged and not s.diverged, s
     assert any(s.n_impacts > 0 for s in g.history)
+    g.close()
+
+
+def test_contact_steps_match_oracle():
+    """20 steps of a polycrystal pressed between closing platens, contact on:
+    every Newton iteration's impact list (device broad phase, narrow phase and
+    closest face) equals the CPU twin's (host candidate pairs, oracle narrow
+    phase and closest face), the iteration counts are equal, and the
+    displacements and CZ damage state match.  The reference would discard a
+    step and shrink the time step when more than 1 % of the CZs newly damage
+    or fail in it, or when Newton does not converge (_checkDamage,
+    _adjustTimeStep, ImplicitModel3.cs:198-212, 259-287); the run stays below
+    both triggers, which the test asserts, so a fixed time step is the
+    reference's behaviour here."""
+    c = M.polycrystal(n=6, grains=6, seed=1, platens=True, gap=-0.01)
+    p = config_prms(penaltyK=1e3)
+    p.InitialTimeStep = 1e-5
+    p.CollisionScheme = 1
+    sig = M.lognormal_strengths(len(c.czs), seed=1, granule_pairs=c.meshes[0].cz_grains)
+    g = ImplicitModel3(c, p, strengths=sig, contact=True)
+    g.trace = []
+    o = OracleModel(c, p, strengths=sig, contact=True)
+    nc = len(c.czs)
+    damaged_prev = 0
+    for step in range(20):
+        sg = g.Step()
+        so = o.Step()
+        assert sg.iterations == so, (step, sg.iterations, so)
+        assert sg.converged and not sg.diverged, (step, sg)
+        dmg, fail = o.damage_counts[-1]
+        assert (dmg - damaged_prev) / nc <= p.maxDamagePerStep and fail / nc <= p.maxFailPerStep, (step, dmg, fail)
+        damaged_prev = dmg
+    assert len(g.trace) == len(o.trace)
+    for i, (a, b) in enumerate(zip(g.trace, o.trace)):
+        assert np.array_equal(a, b), f"impact lists differ at iteration {i}"
+    assert sum(len(t) for t in o.trace) > 0, "no contact: the case does not test the contact path"
+    u, v, a, cz = g.state()
+    assert _rel(u, o.u) <= 1e-8, _rel(u, o.u)
+    assert _rel(v, o.v) <= 1e-6, _rel(v, o.v)
+    if o.pmax.max() > 0:
+        assert _rel(cz["pmax"], o.pmax) <= 1e-8 and _rel(cz["tmax"], o.tmax) <= 1e-8
+    assert np.array_equal(cz["failed"], o.failed)
+    print(f"contact parity: 20 steps, {sum(o.iterations)} iterations, "
+          f"{sum(len(t) for t in o.trace)} impacts over the iterations, u {_rel(u, o.u):.1e}")
     g.close()

@@ -396,7 +396,8 @@ def test_tiled_gather(O, precision):
     shared memory) against the oracle, in both precisions, for two structures
     of the same model (the contact blocks move the merged slots); its
     off-diagonal blocks equal the list gather's bit for bit (one lane per
-    block, same code order)."""
+    block, same code order).  The fused tiles (tets computed in shared
+    memory, no tet kernel) give the tile gather's bits, node forces included."""
     from icflow_b200 import _lib
 
     prms = config_prms(penaltyK=1e8)
@@ -427,6 +428,20 @@ def test_tiled_gather(O, precision):
         assert np.array_equal(vals[off], a["vals"][off])
         cnt = gf.AssembleElemsAndCZs(H)
         assert cnt.nonFinite == 0
+        # the fused tiles compute the tets in shared memory with the tet
+        # kernel's arithmetic and sum the same values in the same order
+        _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 6, 2))
+        gf.AssembleElemsAndCZs(H)
+        vf, rf = gf.TransferLinearSystemToHost()
+        names = {k["name"] for k in gf.ProfileAssembly(H, reps=2)}
+        assert "k_tile_fused" in names and "k_tet_unit" not in names, names
+        assert np.array_equal(vf.reshape(-1, 3, 3), vals) and np.array_equal(rf, rhs)
+        # node forces need the tet rhs, which the fused tiles never stage
+        F_fused = gf.TransferUpdatedStateToHost(want_forces=True)["nodeF"]
+        _lib.check(gf.ctx, lib.icf_set_variant(gf.ctx, 6, 0))
+        gf.AssembleElemsAndCZs(H)
+        F_lists = gf.TransferUpdatedStateToHost(want_forces=True)["nodeF"]
+        assert np.array_equal(F_fused, F_lists)
     gf.close()
 
 
@@ -446,12 +461,89 @@ def test_device_broad_phase_matches_host_pairs(O):
         imps_dev = gf.NarrowPhaseCollisionDetection(None).copy()
         imps_host = gf.NarrowPhaseCollisionDetection(host).copy()
         assert np.array_equal(imps_dev, imps_host)
-        # group ids that do not fit the (cell, group) keys (a negative one)
-        # take the per-cell scan; the pair set is the same
+        # pairs of different meshes only, through (cell, group) keys and,
+        # for group ids that do not fit them (a negative one), the per-cell scan
         from icflow_b200 import _lib
-        grp = np.ascontiguousarray(coll.selem_mesh, np.int32) - 1
-        _lib.check(gf.ctx, gf.lib.icf_set_surface_groups(gf.ctx, len(grp), _lib.iptr(grp)))
-        n2 = C.c_int()
-        _lib.check(gf.ctx, gf.lib.icf_broad_phase(gf.ctx, 0.0, C.byref(n2)))
-        assert n2.value == len(host) and np.array_equal(gf.GetPairs(), host)
+        cross = M.candidate_pairs(coll, coll.x0 + un, same_mesh=False)
+        assert 0 < len(cross) < len(host)
+        for shift in (0, -1):
+            grp = np.ascontiguousarray(coll.selem_mesh, np.int32) + shift
+            _lib.check(gf.ctx, gf.lib.icf_set_surface_groups(gf.ctx, len(grp), _lib.iptr(grp)))
+            n2 = C.c_int()
+            _lib.check(gf.ctx, gf.lib.icf_broad_phase(gf.ctx, 0.0, C.byref(n2)))
+            assert n2.value == len(cross) and np.array_equal(gf.GetPairs(), cross), shift
+        gf.close()
+
+
+def _rotate(coll, R, mesh=None):
+    """A copy of the collection with the nodes of one mesh (all meshes when
+    None) rotated by R about that part's centroid."""
+    import copy
+
+    c = copy.deepcopy(coll)
+    off = 0
+    for i, m in enumerate(c.meshes):
+        n = m.n_nodes
+        if mesh is None or i == mesh:
+            sl = slice(off, off + n)
+            cen = c.x0[sl].mean(axis=0) if mesh is not None else coll.x0.mean(axis=0)
+            c.x0[sl] = cen + (c.x0[sl] - cen) @ R.T
+            m.x0 = c.x0[sl].copy()
+        off += n
+    return c
+
+
+def _rot(axis, deg):
+    a = np.asarray(axis, float) / np.linalg.norm(axis)
+    t = np.radians(deg)
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    return np.eye(3) + np.sin(t) * K + (1 - np.cos(t)) * K @ K
+
+
+def test_broad_phase_covers_the_reference_kdop_pairs(O):
+    """The reference's broad phase is a k-DOP-24 BVH over all surface elements
+    (BVHT.cs:29-77, BVHN.cs:39-194, kDOP24.cs:69-169); its self-collide lists
+    every unordered pair of overlapping k-DOPs, same-mesh pairs included (and
+    across a grain boundary those give impacts).  The device grid broad phase
+    lists the pairs with overlapping boxes that share no node and where a
+    vertex of one lies in the other's box.  An impact needs a vertex of one
+    element inside the other, so such a pair overlaps in every k-DOP
+    direction, shares no node (the narrow phase skips those) and has that
+    vertex in the other's box: every k-DOP pair that can give an impact must
+    be a device pair.  Checked: that containment, and equal impact lists from
+    the two pair sets (the oracle's narrow phase on all k-DOP pairs against
+    the device's on its own), with rotated meshes, where boxes and k-DOPs
+    differ most."""
+    cases = [(1, -0.3, None, None), (2, -0.05, _rot([1, 1, 0], 35), None),
+             (3, -0.2, _rot([0, 1, 0], 10), 1), (4, -0.25, _rot([1, 0, 2], 60), None)]
+    for seed, gap, R, mesh in cases:
+        coll = M.polycrystal(n=7, grains=5, seed=seed, platens=True, gap=gap)
+        if R is not None:
+            coll = _rotate(coll, R, mesh)
+        prms = config_prms(penaltyK=1e8)
+        gf = _gf(coll, prms)
+        un, vn, an = random_state(coll, seed, du=3e-6)
+        gf.TransferNodesToGPU(un, vn, an)
+        xt = coll.x0 + un
+        n_dev = gf.BroadPhase()
+        dev = gf.GetPairs()
+        kd = O.kdop_pairs(coll.selem, xt)
+        se = coll.selem
+        lo, hi = xt[se].min(axis=1), xt[se].max(axis=1)
+        a, b = kd[:, 0], kd[:, 1]
+        shared = (se[a][:, :, None] == se[b][:, None, :]).any(axis=(1, 2))
+        va, vb = xt[se[a]], xt[se[b]]
+        vib = (np.all((va >= lo[b][:, None]) & (va <= hi[b][:, None]), axis=2).any(axis=1) |
+               np.all((vb >= lo[a][:, None]) & (vb <= hi[a][:, None]), axis=2).any(axis=1))
+        can = kd[~shared & vib]
+        dev_set = set(map(tuple, dev.tolist()))
+        assert all(tuple(p) in dev_set for p in can.tolist()), (seed, "k-DOP pair missing from the device set")
+        cross = kd[coll.selem_mesh[a] != coll.selem_mesh[b]]
+        imp_dev = gf.NarrowPhaseCollisionDetection(None).copy()
+        masks = O.narrow_phase(kd, coll.selem, xt)
+        imp_ref = O.impacts(kd, masks, coll.selem, coll.adj_off, coll.adj, coll.faces, xt)
+        assert len(imp_ref) > 0, seed
+        assert np.array_equal(imp_dev, imp_ref), (seed, len(imp_dev), len(imp_ref))
+        print(f"seed {seed}: device pairs {n_dev}, k-DOP pairs {len(kd)} ({len(cross)} across meshes, "
+              f"{len(can)} that can give an impact), impacts {len(imp_ref)}")
         gf.close()

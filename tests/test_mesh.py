@@ -40,14 +40,22 @@ def test_polycrystal_cz_faces_and_adjacency():
     assert np.all(V > 0)
 
 
-def test_candidate_pairs_are_cross_mesh_and_overlap():
+def test_candidate_pairs_overlap_share_no_node_and_cover_the_meshes():
     c = M.polycrystal(n=6, grains=4, seed=1, platens=True, gap=-0.3)
-    pr = M.candidate_pairs(c, c.x0)
-    assert len(pr) > 0
-    assert np.all(c.selem_mesh[pr[:, 0]] != c.selem_mesh[pr[:, 1]])
-    lo = c.x0[c.selem].min(1)
-    hi = c.x0[c.selem].max(1)
-    assert np.all((lo[pr[:, 0]] <= hi[pr[:, 1]]) & (lo[pr[:, 1]] <= hi[pr[:, 0]]))
+    rng = np.random.default_rng(0)
+    xt = c.x0 + (rng.random(c.x0.shape) - 0.5) * 1e-6
+    lo = xt[c.selem].min(1)
+    hi = xt[c.selem].max(1)
+    for same in (True, False):
+        pr = M.candidate_pairs(c, xt, same_mesh=same)
+        assert len(pr) > 0 and np.all(pr[:, 0] < pr[:, 1])
+        assert np.all((lo[pr[:, 0]] <= hi[pr[:, 1]]) & (lo[pr[:, 1]] <= hi[pr[:, 0]]))
+        assert not (c.selem[pr[:, 0]][:, :, None] == c.selem[pr[:, 1]][:, None, :]).any()
+        cross = c.selem_mesh[pr[:, 0]] != c.selem_mesh[pr[:, 1]]
+        assert cross.all() if not same else (~cross).any()
+    # every pair of the cross-mesh list is in the full one
+    full = set(map(tuple, M.candidate_pairs(c, xt).tolist()))
+    assert all(tuple(p) in full for p in M.candidate_pairs(c, xt, same_mesh=False).tolist())
 
 
 def test_lognormal_strengths():
