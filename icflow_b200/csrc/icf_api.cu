@@ -219,7 +219,7 @@ static void free_all(icf_ctx *c) {
                   c->sell_off_cz.meta, c->sell_off_cz.unit, c->sell_off_cz.codes, c->sell_diag_cz.meta,
                   c->sell_diag_cz.unit, c->sell_diag_cz.codes, c->sell_off.unit_s, c->sell_diag.unit_s,
                   c->sell_off_cz.unit_s, c->sell_diag_cz.unit_s, c->d_czhist,
-                  c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup, c->d_imp_built};
+                  c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup, c->d_imp_built, c->d_imp_pos};
   for (void *p : ptrs) cudaFree(p);
 }
 
@@ -435,6 +435,8 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->lists_static = false;
   ctx->d_imp_built = nullptr;
   ctx->imp_built_cap = 0;
+  ctx->d_imp_pos = nullptr;
+  ctx->imp_pos_cap = 0;
   ctx->n_imp_built = -1;
   ctx->d_czhist = nullptr;
   ctx->hist_valid = false;

@@ -400,49 +400,51 @@ __global__ void k_zero_dyn(int nd, const int *__restrict__ pos, double *__restri
   vals[9 * (size_t)pos[i / 9] + (i % 9)] = 0.0;
 }
 
-// Impact contributions, one thread per block they touch (sorted by slot).
-__global__ void k_imp_add(int n_slots, const int *__restrict__ slot,
-                          const int *__restrict__ off,
-                          const uint32_t *__restrict__ code,
-                          const int *__restrict__ cols,
-                          const double *__restrict__ ks,
+// Impact contributions, one thread per block they touch: the records of the
+// block's codes (k_imp_deriv writes them at the codes' positions in the
+// slot-sorted list, so a block's records are contiguous) are summed in code
+// order and added to the block, and to the rhs row for a diagonal block.
+__global__ void k_imp_add(int n_slots, const int *__restrict__ slot, const int *__restrict__ off,
+                          const int *__restrict__ cols, const double *__restrict__ rec,
                           double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite,
                           const unsigned long long *__restrict__ mkey, const int *__restrict__ src,
                           int identity, int which) {
   // which: 0 every touched block; 1 those the off-diagonal gather does not
   // write (diagonal or contact-only); 2 those it does (static, off-diagonal).
-  // one warp per touched block: lane 12 h + e (h = 0, 1; e < 12) reads entry
-  // e (9 block values, then 3 rhs values) of the codes h, h + 2, ... of the
-  // block, in code order; the two halves then add up, and lanes 0..11 add the
-  // sums to the block and rhs row.  A few thousand blocks: the short
-  // dependent chains per lane keep this off the critical path's tail.
-  const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (w >= n_slots) return;
-  const int s = slot[w], q0 = off[w], q1 = off[w + 1];
-  if (which != 0 && icf_off_static(mkey, src, identity, s) != (which == 2)) return;
-  const int h = lane / 12, e = lane - 12 * h;
-  double v = 0.0;
-  bool dg = false;
-  if (h < 2)
-    for (int q = q0 + h; q < q1; q += 2) {
-      const uint32_t cd = __ldg(code + q);
-      const uint32_t u = (cd >> 4) & 0x3FFFFFFu, a = (cd >> 2) & 3u, bb = cd & 3u;
-      const double *K = ks + (size_t)u * ICF_IMP_STAGE;
-      dg |= a == bb;
-      if (e < 9) v += __ldg(K + (3 * a + e / 3) * 12 + 3 * bb + e % 3);
-      else if (a == bb) v += __ldg(K + 144 + 3 * a + (e - 9));
-    }
-  v += __shfl_down_sync(0xffffffffu, v, 12);
-  dg = __any_sync(0xffffffffu, dg);
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
   bool bad = false;
-  if (lane < 9) {
-    vals[9 * (size_t)s + lane] += v;
-    bad = !isfinite(v);
-  } else if (lane < 12 && dg) {
-    rhs[3 * (size_t)cols[s] + (lane - 9)] += v;
-    bad = !isfinite(v);
+  if (w < n_slots) {
+    const int s = slot[w];
+    if (which == 0 || icf_off_static(mkey, src, identity, s) == (which == 2)) {
+      const int q0 = off[w], q1 = off[w + 1];
+      double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int q = q0; q < q1; q++) {
+        const double2 *R = reinterpret_cast<const double2 *>(rec + ICF_IMP_REC * (size_t)q);
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          const double2 t = __ldg(R + k);
+          v[2 * k] += t.x;
+          v[2 * k + 1] += t.y;
+        }
+      }
+      double *o = vals + 9 * (size_t)s;
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        o[k] += v[k];
+        bad |= !isfinite(v[k]);
+      }
+      const unsigned long long key = mkey[s];
+      if ((key >> 32) == (key & 0xffffffffull)) {
+        double *r = rhs + 3 * (size_t)cols[s];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          r[k] += v[9 + k];
+          bad |= !isfinite(v[9 + k]);
+        }
+      }
+    }
   }
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(nonfinite, 1);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(nonfinite, 1);
 }
 
 
@@ -468,7 +470,7 @@ __global__ void k_node_force(int n, const int *__restrict__ off,
   if (ioff)
     for (int q = ioff[i]; q < ioff[i + 1]; q++) {
       const int code = iinc[q];
-      const double *K = ks + (size_t)(code >> 2) * ICF_IMP_STAGE + 144 + 3 * (code & 3);
+      const double *K = ks + (size_t)(code >> 2) * 12 + 3 * (code & 3);
       f[0] += K[0];
       f[1] += K[1];
       f[2] += K[2];
@@ -922,21 +924,22 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   const int ident = ctx->src_identity ? 1 : 0;
   // algorithmic bytes: the impact staging once, 172 B per touched block and
   // 4 B per code, split between the two launches by their blocks
-  const long long imp_in = 8LL * ICF_IMP_STAGE * ctx->n_imp + 4LL * 16 * ctx->n_imp;
+  const long long n_codes = 10LL * ctx->n_imp;  // at most; records of 12 doubles
+  const long long imp_in = 8LL * ICF_IMP_REC * n_codes + 8LL * ctx->n_crs;
   const int n_a = ctx->n_crs - ctx->n_crs_off;
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
   if (n_a > 0) {
-    k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(
-        ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
+    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(
+        ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
         ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 1);
-    icf_prof_mark(ctx, s, "k_imp_add", imp_in * n_a / ctx->n_crs + 172LL * n_a);
+    icf_prof_mark(ctx, s, "k_imp_add", imp_in * n_a / ctx->n_crs + 144LL * n_a);
   }
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   if (ctx->n_crs_off > 0) {
-    k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(
-        ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
+    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(
+        ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
         ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 2);
-    icf_prof_mark(ctx, s, "k_imp_add_off", imp_in * ctx->n_crs_off / ctx->n_crs + 172LL * ctx->n_crs_off);
+    icf_prof_mark(ctx, s, "k_imp_add_off", imp_in * ctx->n_crs_off / ctx->n_crs + 144LL * ctx->n_crs_off);
   }
 
   ICF_CUDA(ctx, cudaGetLastError());
@@ -1072,7 +1075,8 @@ int icf_launch_node_force(icf_ctx *ctx) {
   int rc = icf_get_node_inc(ctx, &t, &m);
   if (rc) return rc;
   k_node_force<<<icf_blocks(ctx->n_nodes, 128), 128, 0, ctx->stream>>>(
-      ctx->n_nodes, t.off, t.inc, ctx->d_es, ctx->n_imp > 0 ? m.off : nullptr, m.inc, ctx->d_ks,
+      ctx->n_nodes, t.off, t.inc, ctx->d_es, ctx->n_imp > 0 ? m.off : nullptr, m.inc,
+      ctx->n_imp > 0 ? icf_imp_forces(ctx->d_ks, ctx->n_imp) : nullptr,
       (ctx->precision == ICF_FP32_MIXED || ctx->layout == ICF_LAYOUT_CONTRIB) ? 4 : 8,
       (ctx->precision == ICF_FP32_MIXED || ctx->layout == ICF_LAYOUT_CONTRIB) ? 0 : 4, ctx->d_nodeF);
   ICF_CUDA(ctx, cudaGetLastError());
@@ -1180,9 +1184,9 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
                                           B.rhs, s));
   }
   if (ctx->n_crs > 0)
-    k_imp_add<<<icf_blocks(32LL * ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cr,
-                                                        ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4,
-                                                        ctx->d_mkeys, ctx->d_src, 1, 0);
+    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols,
+                                                        B.ks, B.vals, B.rhs, ctx->d_counts + 4, ctx->d_mkeys,
+                                                        ctx->d_src, ctx->src_identity ? 1 : 0, 0);
 
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -7,18 +7,19 @@
 // the positions already are, with a uniform grid:
 //   1. axis-aligned box of every surface element at the current positions
 //      (x0 + un), widened by `pad`;
-//   2. cell size = the largest box extent, so a box covers at most 2x2x2 cells;
-//      every (cell, element) entry is listed and the entries are sorted by cell
-//      (CUB radix sort);
+//   2. cell size = the mean box extent (at least a sixteenth of the largest);
+//      every (cell, element) entry of every cell a box reaches is listed and
+//      the entries are sorted by cell (CUB radix sort);
 //   3. within each cell, every pair a < b of elements whose boxes overlap
 //      (closed intervals), that share no node and where a vertex of one lies
 //      in the other's box is a candidate (with groups set, only pairs of
 //      different groups);
-//   4. the pairs are sorted (a, b) ascending, a pair found in several cells
-//      is kept once, and the list stays on the device for the narrow phase.
-// The cell size, the cell ranges (the lowest cell and the next along each
-// axis) and the overlap test are those of the host candidate generator the
-// tests compare against, so both give the same set.
+//   4. a pair is reported only in the cell that holds the low corner of the
+//      two boxes' intersection (so once), the pairs are sorted (a, b)
+//      ascending, and the list stays on the device for the narrow phase.
+// The pair set does not depend on the cell size: two overlapping boxes
+// share the cell of their intersection's low corner; the host pair rule the
+// tests compare against (a grid of its own) gives the same set.
 // Like the reference's BVH, which holds every surface element of every mesh,
 // pairs of one mesh are candidates: across a grain boundary the split node
 // copies let two grains of one mesh interpenetrate, and the narrow phase turns
@@ -76,26 +77,25 @@ __global__ void k_boxes(int n, const int4 *__restrict__ selem, const double4 *__
   if (i < n) ext[i] = e;
 }
 
-// per element: its lowest cell and which of the next cells along each axis
-// its box also reaches (cells c0 + {0, 1} per axis, those <= the highest)
+// per element: its lowest cell and how many more it spans along each axis
+// (every cell its box reaches; at most 16 more, the cell size being at least
+// a sixteenth of the largest box): clo = {c0x, c0y, c0z, sx | sy << 10 | sz << 20}
+__device__ __forceinline__ int cell_of(double v, double base, double cell) { return (int)floor((v - base) / cell); }
 __global__ void k_cells(int n, const double *__restrict__ lohi, const double *__restrict__ red, int *__restrict__ cnt,
                         int4 *__restrict__ clo) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double cell = red[0];
-  int c0[3], s[3];
+  int c0[3], sp[3];
   for (int k = 0; k < 3; k++) {
-    c0[k] = (int)floor((lohi[6 * (size_t)i + k] - red[1 + k]) / cell);
-    const int c1 = (int)floor((lohi[6 * (size_t)i + 3 + k] - red[1 + k]) / cell);
-    s[k] = c1 > c0[k] ? 1 : 0;
+    c0[k] = cell_of(lohi[6 * (size_t)i + k], red[1 + k], cell);
+    const int c1 = cell_of(lohi[6 * (size_t)i + 3 + k], red[1 + k], cell);
+    sp[k] = c1 - c0[k];
   }
-  cnt[i] = (s[0] + 1) * (s[1] + 1) * (s[2] + 1);
-  clo[i] = make_int4(c0[0], c0[1], c0[2], s[0] | s[1] << 1 | s[2] << 2);
+  cnt[i] = (sp[0] + 1) * (sp[1] + 1) * (sp[2] + 1);
+  clo[i] = make_int4(c0[0], c0[1], c0[2], sp[0] | sp[1] << 10 | sp[2] << 20);
 }
 
-__device__ __forceinline__ unsigned long long cell_key(int x, int y, int z) {
-  return ((unsigned long long)(unsigned)x << 42) | ((unsigned long long)(unsigned)y << 21) | (unsigned)z;
-}
 
 // With groups packed into the key (gbits >= 0), an entry's key is
 // (x << 2 nb | y << nb | z) << gbits | group: sorted, the entries of a cell
@@ -108,15 +108,16 @@ __global__ void k_entries(int n, const int4 *__restrict__ clo, const int *__rest
   const int4 c = clo[i];
   int o = off[i];
   const unsigned long long g = gbits >= 0 ? (unsigned long long)(unsigned)group[i] : 0ull;
-  for (int dz = 0; dz <= ((c.w >> 2) & 1); dz++)
-    for (int dy = 0; dy <= ((c.w >> 1) & 1); dy++)
-      for (int dx = 0; dx <= (c.w & 1); dx++) {
-        if (gbits >= 0)
-          key[o] = ((((unsigned long long)(unsigned)(c.x + dx) << (2 * nb)) |
-                     ((unsigned long long)(unsigned)(c.y + dy) << nb) | (unsigned long long)(unsigned)(c.z + dz))
-                    << gbits) | g;
-        else
-          key[o] = cell_key(c.x + dx, c.y + dy, c.z + dz);
+  const int sx = c.w & 1023, sy = (c.w >> 10) & 1023, sz = (c.w >> 20) & 1023;
+  for (int dz = 0; dz <= sz; dz++)
+    for (int dy = 0; dy <= sy; dy++)
+      for (int dx = 0; dx <= sx; dx++) {
+        // (x << 2 nb | y << nb | z) << gbits | group, or without groups the
+        // cell alone (gbits < 0)
+        const unsigned long long ck = ((unsigned long long)(unsigned)(c.x + dx) << (2 * nb)) |
+                                      ((unsigned long long)(unsigned)(c.y + dy) << nb) |
+                                      (unsigned long long)(unsigned)(c.z + dz);
+        key[o] = gbits >= 0 ? (ck << gbits) | g : ck;
         elem[o] = i;
         o++;
       }
@@ -168,9 +169,10 @@ __device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, cons
 // candidates are the entries from the end of its (cell, group) run to the end
 // of its cell, found by binary search.
 __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const int *__restrict__ elem,
-                        const double *__restrict__ lohi, const int *__restrict__ group, int gbits,
+                        const double *__restrict__ lohi, const double *__restrict__ red, int nb,
+                        const int *__restrict__ group, int gbits,
                         const int4 *__restrict__ selem, const double4 *__restrict__ xc, const int *__restrict__ off,
-                        int *__restrict__ cnt, unsigned long long *__restrict__ out, long long cap) {
+                        int *__restrict__ cnt, unsigned long long *__restrict__ out, long long cap, int pb) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const unsigned long long here = key[i];
@@ -182,13 +184,21 @@ __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const
     j0 = upper_key(key, i + 1, m, here);  // end of the run of this cell and group
     j1 = upper_key(key, j0, m, here | ((1ull << gbits) - 1));  // end of the cell
   }
+  // this entry's cell, to report a pair only in the cell that holds the low
+  // corner of the two boxes' intersection (each pair once)
+  const unsigned long long ck = gbits >= 0 ? here >> gbits : here, mk = (1ull << nb) - 1;
+  const int cx = (int)(ck >> (2 * nb)), cy = (int)((ck >> nb) & mk), cz = (int)(ck & mk);
   for (int j = j0; j < j1 && (gbits >= 0 || key[j] == here); j++) {
     const int b0 = elem[j];
     const int a = a0 < b0 ? a0 : b0, b = a0 < b0 ? b0 : a0;
+    const double *la = lohi + 6 * (size_t)a, *lb = lohi + 6 * (size_t)b;
+    if (cell_of(fmax(la[0], lb[0]), red[1], red[0]) != cx || cell_of(fmax(la[1], lb[1]), red[2], red[0]) != cy ||
+        cell_of(fmax(la[2], lb[2]), red[3], red[0]) != cz)
+      continue;
     if (keep_pair(a, b, lohi, group, selem, xc)) {
       // beyond the capacity nothing is written; the host sees the total
       // and repeats with a larger buffer
-      if (out && o < cap) out[o] = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
+      if (out && o < cap) out[o] = ((unsigned long long)(unsigned)a << pb) | (unsigned)b;
       o++;
       c++;
     }
@@ -196,33 +206,34 @@ __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const
   if (cnt) cnt[i] = c;
 }
 
-// The unique pairs (in[0 .. *n_dev), the all-ones padding key dropped) into
-// the pair list; n_dev[0] becomes the pair count.
-__global__ void k_unpack_pairs(long long cap, int *__restrict__ n_dev, const unsigned long long *__restrict__ in,
-                               int *__restrict__ pairs) {
+// The sorted pairs in[0 .. *n_all) (each reported once; the all-ones padding
+// sorts after them) into the pair list; n_out[0] = the pair count.
+__global__ void k_unpack_pairs(long long cap, const int *__restrict__ n_all, int *__restrict__ n_out,
+                               const unsigned long long *__restrict__ in, int pb, int *__restrict__ pairs) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int n = *n_dev;
-  if (n > 0 && in[n - 1] == ~0ull) n--;  // the padding, sorted last
-  if (i == 0) n_dev[1] = n;
-  if (i >= n || i >= cap) return;
-  pairs[2 * (size_t)i] = (int)(in[i] >> 32);
-  pairs[2 * (size_t)i + 1] = (int)(in[i] & 0xffffffffull);
+  const long long n = *n_all < cap ? *n_all : cap;
+  if (i == 0) *n_out = (int)n;
+  if (i >= n) return;
+  pairs[2 * (size_t)i] = (int)(in[i] >> pb);
+  pairs[2 * (size_t)i + 1] = (int)(in[i] & ((1ull << pb) - 1));
 }
 
 
 
-// red[0] = cell size (largest extent), red[1..3] = lowest corner, red[4..6] =
-// highest corner: one pass, per block then one block over the partials
-// (min and max are exact, so the order does not matter)
-__device__ __forceinline__ void red7_block(double v[7]) {
-  __shared__ double sh[7][32];
+// The grid: v[0] = largest extent, v[1..3] = lowest corner, v[4..6] = highest
+// corner, v[7] = sum of extents, per block then one block over the partials
+// (min and max are exact; the sum's order is fixed by the launch); the final
+// block turns v[0] into the cell size, the mean extent but at least a
+// sixteenth of the largest one, so that a box spans at most 17 cells per axis.
+__device__ __forceinline__ void red8_block(double v[8]) {
+  __shared__ double sh[8][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-  for (int q = 0; q < 7; q++) {
-    const bool mn = q >= 1 && q <= 3;
+  for (int q = 0; q < 8; q++) {
+    const bool mn = q >= 1 && q <= 3, sum = q == 7;
     for (int o = 16; o > 0; o >>= 1) {
       const double t = __shfl_xor_sync(0xffffffffu, v[q], o);
-      v[q] = mn ? fmin(v[q], t) : fmax(v[q], t);
+      v[q] = sum ? v[q] + t : (mn ? fmin(v[q], t) : fmax(v[q], t));
     }
     if (lane == 0) sh[q][w] = v[q];
   }
@@ -230,44 +241,49 @@ __device__ __forceinline__ void red7_block(double v[7]) {
   if (w == 0) {
     const int nw = blockDim.x >> 5;
 #pragma unroll
-    for (int q = 0; q < 7; q++) {
-      const bool mn = q >= 1 && q <= 3;
-      v[q] = lane < nw ? sh[q][lane] : (mn ? 1e300 : -1e300);
+    for (int q = 0; q < 8; q++) {
+      const bool mn = q >= 1 && q <= 3, sum = q == 7;
+      v[q] = lane < nw ? sh[q][lane] : (sum ? 0.0 : (mn ? 1e300 : -1e300));
       for (int o = 16; o > 0; o >>= 1) {
         const double t = __shfl_xor_sync(0xffffffffu, v[q], o);
-        v[q] = mn ? fmin(v[q], t) : fmax(v[q], t);
+        v[q] = sum ? v[q] + t : (mn ? fmin(v[q], t) : fmax(v[q], t));
       }
     }
   }
 }
 __global__ void k_red7(int n, const double *__restrict__ lohi, const double *__restrict__ ext,
                        double *__restrict__ part) {
-  double v[7] = {-1e300, 1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+  double v[8] = {-1e300, 1e300, 1e300, 1e300, -1e300, -1e300, -1e300, 0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     v[0] = fmax(v[0], ext[i]);
+    v[7] += ext[i];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       v[1 + k] = fmin(v[1 + k], lohi[6 * (size_t)i + k]);
       v[4 + k] = fmax(v[4 + k], lohi[6 * (size_t)i + 3 + k]);
     }
   }
-  red7_block(v);
+  red8_block(v);
   if (threadIdx.x == 0)
 #pragma unroll
-    for (int q = 0; q < 7; q++) part[7 * (size_t)blockIdx.x + q] = v[q];
+    for (int q = 0; q < 8; q++) part[8 * (size_t)blockIdx.x + q] = v[q];
 }
-__global__ void k_red7_final(int nb, const double *__restrict__ part, double *__restrict__ red) {
-  double v[7] = {-1e300, 1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+__global__ void k_red7_final(int nb, int n, const double *__restrict__ part, double *__restrict__ red) {
+  double v[8] = {-1e300, 1e300, 1e300, 1e300, -1e300, -1e300, -1e300, 0.0};
   for (int b = threadIdx.x; b < nb; b += blockDim.x)
 #pragma unroll
-    for (int q = 0; q < 7; q++) {
-      const bool mn = q >= 1 && q <= 3;
-      v[q] = mn ? fmin(v[q], part[7 * (size_t)b + q]) : fmax(v[q], part[7 * (size_t)b + q]);
+    for (int q = 0; q < 8; q++) {
+      const bool mn = q >= 1 && q <= 3, sum = q == 7;
+      const double x = part[8 * (size_t)b + q];
+      v[q] = sum ? v[q] + x : (mn ? fmin(v[q], x) : fmax(v[q], x));
     }
-  red7_block(v);
-  if (threadIdx.x == 0)
+  red8_block(v);
+  if (threadIdx.x == 0) {
+    const double mean = v[7] / n;
+    v[0] = fmax(mean, v[0] / 16.0);
 #pragma unroll
-    for (int q = 0; q < 7; q++) red[q] = v[q];
+    for (int q = 0; q < 8; q++) red[q] = v[q];
+  }
 }
 
 }  // namespace
@@ -318,11 +334,11 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     ICF_TRY_RC(grow(ctx, &W.clo, n));
     W.b_cap = n;
   }
-  if (!W.tmpv) ICF_TRY_RC(grow(ctx, &W.tmpv, 7LL * (2 * ctx->n_sm + 1)));
+  if (!W.tmpv) ICF_TRY_RC(grow(ctx, &W.tmpv, 8LL * (2 * ctx->n_sm + 1)));
   if (!W.red) ICF_TRY_RC(grow(ctx, &W.red, 8));
   k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext);
   k_red7<<<nbk, 256, 0, s>>>(n, W.lohi, W.ext, W.tmpv);
-  k_red7_final<<<1, 256, 0, s>>>(nbk, W.tmpv, W.red);
+  k_red7_final<<<1, 256, 0, s>>>(nbk, n, W.tmpv, W.red);
   k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
   ICF_CUDA(ctx, cudaMemsetAsync(W.bcnt + n, 0, sizeof(int), s));
   size_t tb = 0;
@@ -343,7 +359,12 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     const double cells = std::isfinite(span) ? span + 2.0 : 1e30;
     while (nb < 40 && (double)(1ull << nb) < cells) nb++;
   }
+  if (3 * nb > 63) return icf_fail(ctx, ICF_ERR_SIZE, "broad phase: more grid cells than 63-bit keys hold");
   const int gbits = (d_group && ctx->sgroup_bits >= 0 && 3 * nb + ctx->sgroup_bits <= 63) ? ctx->sgroup_bits : -1;
+  // pair keys a << pb | b over the bits of the element ids (the all-ones
+  // padding sorts after every pair)
+  int pb = 1;
+  while ((1LL << pb) < (long long)n) pb++;
   if (m > W.ent_cap) {
     const long long c = m + m / 4 + 64;
     ICF_TRY_RC(grow(ctx, &W.ek0, c));
@@ -355,13 +376,13 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     W.ent_cap = c;
   }
   k_entries<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.clo, W.boff, nb, gbits, d_group, W.ek0, W.ee0);
-  const int end_bit = gbits >= 0 ? 3 * nb + gbits : 63;
+  const int end_bit = gbits >= 0 ? 3 * nb + gbits : 3 * nb;
   tb = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tb, W.ek0, W.ek1, W.ee0, W.ee1, m, 0, end_bit, s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, W.ek0, W.ek1, W.ee0, W.ee1, m, 0, end_bit, s));
-  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, d_group, gbits, ctx->d_selem, ctx->d_xc,
-                                              nullptr, W.pc, nullptr, 0);
+  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, W.red, nb, d_group, gbits, ctx->d_selem, ctx->d_xc,
+                                              nullptr, W.pc, nullptr, 0, 0);
   ICF_CUDA(ctx, cudaMemsetAsync(W.pc + m, 0, sizeof(int), s));
   tb = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb, W.pc, W.po, m + 1, s);
@@ -385,17 +406,15 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     }
     // pad with all-ones keys: they sort after every pair and form one run
     ICF_CUDA(ctx, cudaMemsetAsync(W.p0, 0xFF, sizeof(unsigned long long) * (size_t)P, s));
-    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, d_group, gbits, ctx->d_selem, ctx->d_xc,
-                                                W.po, nullptr, W.p0, P);
+    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, W.red, nb, d_group, gbits, ctx->d_selem, ctx->d_xc,
+                                                W.po, nullptr, W.p0, P, pb);
     tb = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb, W.p0, W.p1, (int)P, 0, 64, s);
+    // the padding is all ones in every bit, so sorting the low 2 pb bits
+    // still puts it after the pairs
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, W.p0, W.p1, (int)P, 0, 2 * pb, s);
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, W.p0, W.p1, (int)P, 0, 64, s));
-    tb = 0;
-    cub::DeviceSelect::Unique(nullptr, tb, W.p1, W.p0, W.d_small, (int)P, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, W.p1, W.p0, W.d_small, (int)P, s));
-    k_unpack_pairs<<<icf_blocks(P, 256), 256, 0, s>>>(P, W.d_small, W.p0, ctx->d_pairs);
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, W.p0, W.p1, (int)P, 0, 2 * pb, s));
+    k_unpack_pairs<<<icf_blocks(P, 256), 256, 0, s>>>(P, W.po + m, W.d_small + 1, W.p1, pb, ctx->d_pairs);
     ICF_CUDA(ctx, cudaGetLastError());
     ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 2, W.po + m, sizeof(int), cudaMemcpyDeviceToHost, s));
     ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 1, W.d_small + 1, sizeof(int), cudaMemcpyDeviceToHost, s));

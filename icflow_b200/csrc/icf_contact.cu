@@ -398,7 +398,9 @@ int icf_launch_imp_unit(icf_ctx *ctx, cudaStream_t stream) {
   icf_prof_mark(ctx, stream, "k_imp_classify", 192LL * ctx->n_imp);
   const int rc = icf_launch_imp_deriv(ctx, ctx->d_imp_ci, ctx->d_imp_cd, stream);
   // classification and node positions in, 160-double staging record out
-  icf_prof_mark(ctx, stream, "k_imp_deriv", (48LL + 128 + 8 * ICF_IMP_STAGE) * ctx->n_imp);
+  // classification and node positions in; up to ten 96 B records, the
+  // 64 B position map and a 96 B force record per impact
+  icf_prof_mark(ctx, stream, "k_imp_deriv", (48LL + 128 + 64 + 96 + 8LL * ICF_IMP_REC * 10) * ctx->n_imp);
   return rc;
 }
 

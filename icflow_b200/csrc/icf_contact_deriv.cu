@@ -10,9 +10,13 @@
 //                  barycentrics s(x), t(x) of the foot point
 //                  (point_plane_distance, :449-582)
 // The 32 lanes of a warp share the per-impact setup through shared memory and
-// each evaluates 4-5 of the 144 Hessian entries.  The staging record is
-//   K[12x12] = k/2 d2'' (upper triangle mirrored, :111-114) and
-//   K[144..155] = (-F, w0 F, w1 F, w2 F),  F = k/2 d(d2)/dp,  w = (1-s-t, s, t).
+// each evaluates 2-3 of the 78 entries of the symmetric Hessian (:111-114).
+// K = k/2 d2'' goes straight to the records of the impact's contribution
+// codes, at their positions in the slot-sorted list (icf_internal.cuh,
+// ICF_IMP_REC): the 3x3 block of each code's vertex pair, and, on the
+// diagonal codes, the vertex's rhs from (-F, w0 F, w1 F, w2 F),
+// F = k/2 d(d2)/dp, w = (1-s-t, s, t); the four vertex forces also go to a
+// per-impact force record (for the node forces).
 #include "icf_internal.cuh"
 
 namespace {
@@ -98,10 +102,29 @@ __device__ double line_entry(const LineSetup &L, int i, int j) {
   return t1 + t2 + f1dd + t4 + t5;
 }
 
+// Upper-triangle entry e (0..77) of a 12x12 matrix: (I, J), I <= J.
+__device__ __forceinline__ void upper_ij(int e, int &I, int &J) {
+  int i = 0, start = 0;
+  while (e >= start + 12 - i) {
+    start += 12 - i;
+    i++;
+  }
+  I = i;
+  J = i + (e - start);
+}
+
+// Entry (I, J) of the staged Hessian goes to the record of the code of vertex
+// pair (I/3, J/3) at (I%3, J%3); pairs without a code (an anchored vertex, or
+// the pair taken the other way round) are skipped.
+__device__ __forceinline__ void put(const int *P, double *rec, int I, int J, double v) {
+  const int q = P[4 * (I / 3) + J / 3];
+  if (q >= 0) rec[ICF_IMP_REC * (size_t)q + 3 * (I % 3) + (J % 3)] = v;
+}
+
 __global__ void __launch_bounds__(32 * WARPS)
     k_imp_deriv(int n, const int4 *__restrict__ imp, const double4 *__restrict__ xc,
                 const int4 *__restrict__ ci, const double4 *__restrict__ cd, double kpen,
-                double *__restrict__ ks) {
+                const int *__restrict__ pos, double *__restrict__ rec, double *__restrict__ frc) {
   __shared__ PlaneSetup sP[WARPS];
   __shared__ LineSetup sL[WARPS];
   __shared__ double sx[WARPS][12];
@@ -109,10 +132,14 @@ __global__ void __launch_bounds__(32 * WARPS)
   const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int u = blockIdx.x * WARPS + wl;
   if (u >= n) return;  // uniform per warp
-  double *K = ks + (size_t)u * ICF_IMP_STAGE;
+  const int *P = pos + 16 * (size_t)u;
   const int4 c = ci[u];
-  if (c.x < 0) {
-    for (int i = lane; i < ICF_IMP_STAGE; i += 32) K[i] = 0;
+  if (c.x < 0) {  // no response: zero records, zero forces
+    for (int e = lane; e < 16 * ICF_IMP_REC; e += 32) {
+      const int q = P[e / ICF_IMP_REC];
+      if (q >= 0) rec[ICF_IMP_REC * (size_t)q + e % ICF_IMP_REC] = 0.0;
+    }
+    if (lane < 12) frc[12 * (size_t)u + lane] = 0.0;
     return;
   }
   const double4 cl = cd[u];
@@ -131,24 +158,28 @@ __global__ void __launch_bounds__(32 * WARPS)
   if (c.x == 1) {  // vertex: d2 = |p - x_b|^2
     const int vb = c.z;
     if (lane < 3) sfd[wl][lane] = 2 * (x[lane] - x[3 * vb + lane]);
-    for (int e = lane; e < 144; e += 32) {
-      const int I = e / 12, J = e % 12, bI = I / 3, bJ = J / 3;
+    for (int e = lane; e < 78; e += 32) {
+      int I, J;
+      upper_ij(e, I, J);
+      const int bI = I / 3, bJ = J / 3;
       double v = 0;
       if (I % 3 == J % 3 && (bI == 0 || bI == vb) && (bJ == 0 || bJ == vb)) v = (bI == bJ) ? 2.0 : -2.0;
-      K[e] = kpen * v / 2;
+      v = kpen * v / 2;
+      put(P, rec, I, J, v);
+      if (I != J) put(P, rec, J, I, v);
     }
   } else if (c.x == 2) {  // edge (ia nearer, ib)
     const int ia = c.y, ib = c.z;
     LineSetup &L = sL[wl];
     if (lane == 0) {
-      const double *P = x, *Q1 = x + 3 * ia, *Q2 = x + 3 * ib;
+      const double *Pp = x, *Q1 = x + 3 * ia, *Q2 = x + 3 * ib;
       double sp = 0, f2 = 0;
       for (int k = 0; k < 3; k++) {
         L.spd[k] = Q1[k] - Q2[k];
-        L.spd[3 + k] = P[k] - 2 * Q1[k] + Q2[k];
-        L.spd[6 + k] = Q1[k] - P[k];
-        sp += (Q1[k] - P[k]) * (Q2[k] - Q1[k]);
-        const double a = Q1[k] - P[k], b = Q2[k] - Q1[k];
+        L.spd[3 + k] = Pp[k] - 2 * Q1[k] + Q2[k];
+        L.spd[6 + k] = Q1[k] - Pp[k];
+        sp += (Q1[k] - Pp[k]) * (Q2[k] - Q1[k]);
+        const double a = Q1[k] - Pp[k], b = Q2[k] - Q1[k];
         f2 += b * b;
         L.f1d[3 + k] = 2 * a;
         L.f1d[k] = -(2 * a);
@@ -167,104 +198,112 @@ __global__ void __launch_bounds__(32 * WARPS)
         sfd[wl][k] = L.f1d[k] + (L.g * L.f2d[k] - L.f2 * L.gd[k]) / L.f2sq;
     }
     __syncwarp();
-    for (int e = lane; e < 144; e += 32) {
-      int I = e / 12, J = e % 12;
-      if (I > J) { const int t = I; I = J; J = t; }
+    for (int e = lane; e < 78; e += 32) {
+      int I, J;
+      upper_ij(e, I, J);
       const int bI = I / 3, bJ = J / 3;
       const int pI = bI == 0 ? 0 : (bI == ia ? 1 : (bI == ib ? 2 : -1));
       const int pJ = bJ == 0 ? 0 : (bJ == ia ? 1 : (bJ == ib ? 2 : -1));
       double v = 0;
       if (pI >= 0 && pJ >= 0) v = line_entry(L, 3 * pI + I % 3, 3 * pJ + J % 3);
-      K[e] = kpen * v / 2;
+      v = kpen * v / 2;
+      put(P, rec, I, J, v);
+      if (I != J) put(P, rec, J, I, v);
     }
   } else {  // interior
     PlaneSetup &S = sP[wl];
-    if (lane == 0) {
-      double e0[3], e1[3], w[3];
-      for (int k = 0; k < 3; k++) {
-        S.V[0][k] = x[3 + k];
-        S.V[1][k] = x[6 + k];
-        S.V[2][k] = x[9 + k];
-        e0[k] = -x[3 + k] + x[6 + k];
-        e1[k] = -x[3 + k] + x[9 + k];
-        w[k] = -x[k] + x[3 + k];
-      }
-      S.a = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
-      S.b = e1[1] * e0[1] + e1[2] * e0[2] + e0[0] * e1[0];
-      S.c = e1[1] * e1[1] + e1[2] * e1[2] + e1[0] * e1[0];
-      S.d = w[0] * e0[0] + w[1] * e0[1] + w[2] * e0[2];
-      S.e = e1[1] * w[1] + e1[2] * w[2] + w[0] * e1[0];
-      S.det = S.a * S.c - S.b * S.b;
-      S.idet = 1.0 / S.det;
-      S.idet2 = S.idet * S.idet;
-      S.idet3 = S.idet2 * S.idet;
-      S.s = (S.b * S.e - S.c * S.d) * S.idet;
-      S.t = (S.b * S.d - S.a * S.e) * S.idet;
-      S.u = 1 - (S.s + S.t);
-      S.sN = -(S.c * S.d) + S.b * S.e;
-      S.tN = S.b * S.d - S.a * S.e;
-      for (int k = 0; k < 3; k++) S.q[k] = -x[k] + x[6 + k] * S.s + x[9 + k] * S.t + x[3 + k] * S.u;
-      for (int i = 0; i < 12; i++) {
-        const int bi = i / 3, k = i % 3;
-        S.ag[i] = 2.0 * sgE0(bi) * e0[k];
-        S.bg[i] = sgE0(bi) * e1[k] + sgE1(bi) * e0[k];
-        S.cg[i] = 2.0 * sgE1(bi) * e1[k];
-        S.dg[i] = sgE0(bi) * w[k] + sgW(bi) * e0[k];
-        S.eg[i] = sgE1(bi) * w[k] + sgW(bi) * e1[k];
-      }
+    // the scalars of point_plane_distance, on every lane (no round trip)
+    double e0[3], e1[3], w[3];
+    for (int k = 0; k < 3; k++) {
+      e0[k] = -x[3 + k] + x[6 + k];
+      e1[k] = -x[3 + k] + x[9 + k];
+      w[k] = -x[k] + x[3 + k];
     }
-    __syncwarp();
+    const double a = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
+    const double b = e1[1] * e0[1] + e1[2] * e0[2] + e0[0] * e1[0];
+    const double c2 = e1[1] * e1[1] + e1[2] * e1[2] + e1[0] * e1[0];
+    const double d = w[0] * e0[0] + w[1] * e0[1] + w[2] * e0[2];
+    const double e = e1[1] * w[1] + e1[2] * w[2] + w[0] * e1[0];
+    const double det = a * c2 - b * b;
+    const double idet = 1.0 / det, idet2 = idet * idet, idet3 = idet2 * idet;
+    const double ss = (b * e - c2 * d) * idet, tt = (b * d - a * e) * idet, uu = 1 - (ss + tt);
+    if (lane == 0) {
+      S.a = a; S.b = b; S.c = c2; S.d = d; S.e = e;
+      S.det = det; S.idet = idet; S.idet2 = idet2; S.idet3 = idet3;
+      S.s = ss; S.t = tt; S.u = uu;
+      S.sN = -(c2 * d) + b * e;
+      S.tN = b * d - a * e;
+    }
+    if (lane < 9) S.V[lane / 3][lane % 3] = x[3 + lane];
+    if (lane < 3) S.q[lane] = -x[lane] + x[6 + lane] * ss + x[9 + lane] * tt + x[3 + lane] * uu;
     if (lane < 12) {
-      const int i = lane;
-      const double a = S.a, b = S.b, c2 = S.c, d = S.d, e = S.e;
-      const double det1 = c2 * S.ag[i] + a * S.cg[i] - 2 * b * S.bg[i];
-      const double s1 = ((c2 * d - b * e) * det1) * S.idet2 + ((e * S.bg[i] + b * S.eg[i]) - (d * S.cg[i] + c2 * S.dg[i])) * S.idet;
-      const double t1 = ((a * e - b * d) * det1) * S.idet2 + ((d * S.bg[i] + b * S.dg[i]) - (a * S.eg[i] + e * S.ag[i])) * S.idet;
+      const int i = lane, bi = i / 3, k = i % 3;
+      const double ag = 2.0 * sgE0(bi) * e0[k];
+      const double bg = sgE0(bi) * e1[k] + sgE1(bi) * e0[k];
+      const double cg = 2.0 * sgE1(bi) * e1[k];
+      const double dg = sgE0(bi) * w[k] + sgW(bi) * e0[k];
+      const double eg = sgE1(bi) * w[k] + sgW(bi) * e1[k];
+      S.ag[i] = ag; S.bg[i] = bg; S.cg[i] = cg; S.dg[i] = dg; S.eg[i] = eg;
+      const double det1 = c2 * ag + a * cg - 2 * b * bg;
+      const double s1 = ((c2 * d - b * e) * det1) * idet2 + ((e * bg + b * eg) - (d * cg + c2 * dg)) * idet;
+      const double t1 = ((a * e - b * d) * det1) * idet2 + ((d * bg + b * dg) - (a * eg + e * ag)) * idet;
       S.det1[i] = det1;
       S.s1[i] = s1;
       S.t1[i] = t1;
       S.u1[i] = -(s1 + t1);
-      for (int k = 0; k < 3; k++) {
-        double v = S.V[1][k] * s1 + S.V[2][k] * t1 + S.V[0][k] * (-(s1 + t1));
-        if (i == k) v -= 1;
-        if (i == 3 + k) v += S.u;
-        if (i == 6 + k) v += S.s;
-        if (i == 9 + k) v += S.t;
-        S.J[k][i] = v;
+      for (int kk = 0; kk < 3; kk++) {
+        double v = x[6 + kk] * s1 + x[9 + kk] * t1 + x[3 + kk] * (-(s1 + t1));
+        if (i == kk) v -= 1;
+        if (i == 3 + kk) v += uu;
+        if (i == 6 + kk) v += ss;
+        if (i == 9 + kk) v += tt;
+        S.J[kk][i] = v;
       }
     }
     __syncwarp();
     if (lane < 3) sfd[wl][lane] = 2 * (S.q[0] * S.J[0][lane] + S.q[1] * S.J[1][lane] + S.q[2] * S.J[2][lane]);
-    for (int e = lane; e < 144; e += 32) {
-      int I = e / 12, J = e % 12;
-      if (I > J) { const int t = I; I = J; J = t; }
-      K[e] = kpen * plane_entry(S, I, J) / 2;
+    for (int en = lane; en < 78; en += 32) {
+      int I, J;
+      upper_ij(en, I, J);
+      const double v = kpen * plane_entry(S, I, J) / 2;
+      put(P, rec, I, J, v);
+      if (I != J) put(P, rec, J, I, v);
     }
   }
   __syncwarp();
+  // vertex forces (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp, w = (1-s-t, s, t)
+  // (collision_response.h:89-109): into the force record, and as the rhs of
+  // the vertex's diagonal code
   if (lane < 12) {
     const double s = cl.x, t = cl.y;
-    const double w[3] = {1 - (s + t), s, t};
+    const double wv[3] = {1 - (s + t), s, t};
     const int comp = lane % 3, blk = lane / 3;
     const double F = hk * sfd[wl][comp];
-    K[144 + lane] = blk == 0 ? -F : w[blk - 1] * F;
+    const double f = blk == 0 ? -F : wv[blk - 1] * F;
+    frc[12 * (size_t)u + lane] = f;
+    const int q = P[5 * blk];
+    if (q >= 0) rec[ICF_IMP_REC * (size_t)q + 9 + comp] = f;
+  } else if (lane < 28) {  // off-diagonal codes carry no rhs
+    const int pr = lane - 12;
+    const int q = P[pr];
+    if ((pr >> 2) != (pr & 3) && q >= 0)
+      for (int k = 0; k < 3; k++) rec[ICF_IMP_REC * (size_t)q + 9 + k] = 0.0;
   }
 }
 
 }  // namespace
 
 int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d, cudaStream_t stream) {
-  k_imp_deriv<<<icf_blocks(ctx->n_imp, WARPS), 32 * WARPS, 0, stream>>>(
-      ctx->n_imp, ctx->d_imp, ctx->d_xc, cls_i, cls_d, ctx->prm.penaltyK, ctx->d_ks);
-  ICF_CUDA(ctx, cudaGetLastError());
-  return ICF_OK;
+  return icf_launch_imp_deriv_bufs(ctx, ctx->d_xc, cls_i, cls_d, ctx->d_ks, stream);
 }
 
-// Derivative kernel with caller-chosen buffers (allocation-free entry point).
+// Derivative kernel with caller-chosen buffers (the allocation-free entry
+// point passes its own staging).
 int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, const int4 *cls_i, const double4 *cls_d,
                               double *ks, cudaStream_t stream) {
-  k_imp_deriv<<<icf_blocks(ctx->n_imp, WARPS), 32 * WARPS, 0, stream>>>(ctx->n_imp, ctx->d_imp, xc, cls_i,
-                                                                       cls_d, ctx->prm.penaltyK, ks);
+  k_imp_deriv<<<icf_blocks(ctx->n_imp, WARPS), 32 * WARPS, 0, stream>>>(
+      ctx->n_imp, ctx->d_imp, xc, cls_i, cls_d, ctx->prm.penaltyK, ctx->d_imp_pos, ks,
+      icf_imp_forces(ks, ctx->n_imp));
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }

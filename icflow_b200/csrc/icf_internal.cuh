@@ -38,7 +38,17 @@
 #define ICF_MAX_TET_UNITS (1 << 26)
 #define ICF_MAX_CZ_UNITS (1 << 24)
 #define ICF_CZ_STAGE 48   // doubles per CZ in the staging buffer
-#define ICF_IMP_STAGE 160 // doubles per impact in the staging buffer
+#define ICF_IMP_STAGE 160 // doubles per impact in the staging buffer (allocation)
+// The staging buffer of n impacts holds, from the start, one record of
+// ICF_IMP_REC doubles per impact contribution code, at the code's position in
+// the slot-sorted list d_cr (the 3x3 block of the code's vertex pair, then the
+// rhs of the vertex on diagonal codes, else zeros; at most 10 codes per
+// impact), and from ICF_IMP_FORCE_AT * n the 12 vertex forces of every impact.
+#define ICF_IMP_REC 12
+#define ICF_IMP_FORCE_AT 120
+__host__ __device__ inline double *icf_imp_forces(double *ks, long long n_imp) {
+  return ks + (long long)ICF_IMP_FORCE_AT * n_imp;
+}
 
 // node -> (unit << 2 | vertex) incidence list in CSR form
 struct icf_node_inc {
@@ -299,6 +309,10 @@ struct icf_ctx {
   int *d_cr_slot = nullptr, *d_cr_off = nullptr;
   uint32_t *d_cr = nullptr;
   int cr_cap = 0;
+  // position in d_cr of the code (impact u, vertices a, b) at 16 u + 4 a + b,
+  // or -1 (no code: an anchored vertex, or the pair taken as (b, a))
+  int *d_imp_pos = nullptr;
+  long long imp_pos_cap = 0;
 
   // narrow phase
   int n_pairs = 0, pairs_cap = 0;

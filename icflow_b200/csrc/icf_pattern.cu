@@ -307,6 +307,16 @@ __global__ void k_cand_imp_rc(int ni, const int4 *__restrict__ imp, const int *_
     }
 }
 
+// pos[16 u + 4 a + b] = position of impact code (u, a, b) in the slot-sorted
+// list, for the valid codes (those before the invalid-slot run)
+__global__ void k_imp_pos(int n, const int *__restrict__ n_valid, const uint32_t *__restrict__ code,
+                          int *__restrict__ pos) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n || q >= *n_valid) return;
+  const uint32_t c = code[q];
+  pos[16 * (size_t)((c >> 4) & 0x3FFFFFFu) + (c & 15u)] = q;
+}
+
 // node incidence lists: (node, unit << 2 | vertex)
 __global__ void k_node_inc_tet(int ne, const int4 *__restrict__ elem, int *__restrict__ node,
                                int *__restrict__ code) {
@@ -885,6 +895,16 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
     ICF_CUDA(ctx, cudaFreeAsync(cnt, s));
     ICF_CUDA(ctx, cudaFreeAsync(d_nr, s));
     ctx->n_crs = nvalid;
+    // where each code's record goes (k_imp_deriv writes, k_imp_add reads)
+    if (n > ctx->imp_pos_cap || !ctx->d_imp_pos) {
+      cudaFree(ctx->d_imp_pos);
+      ctx->d_imp_pos = nullptr;
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_imp_pos, sizeof(int) * 2 * (size_t)n));
+      ctx->imp_pos_cap = 2LL * n;
+    }
+    ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_imp_pos, 0xFF, sizeof(int) * (size_t)n, s));
+    k_imp_pos<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_cr_off + nvalid, ctx->d_cr, ctx->d_imp_pos);
+    ICF_CUDA(ctx, cudaGetLastError());
     // how many of them the off-diagonal gather writes
     ctx->n_crs_off = 0;
     if (nvalid > 0) {

@@ -49,6 +49,7 @@ class OracleModel:
         self.iterations = []
         self.contact = contact
         self.trace = []  # per Newton iteration: the impact list
+        self.trace_x = []  # ... and the tentative positions it was found at
         # per step: CZs newly damaged and failed (the counters _checkDamage reads)
         self.damage_counts = []
         imps = np.zeros((0, 4), np.int32)
@@ -94,6 +95,7 @@ class OracleModel:
                 else:
                     imps = np.zeros((0, 4), np.int32)
                 self.trace.append(imps.copy())
+                self.trace_x.append(xt.copy())
                 N, rows, cols = O.build_structure(c.alt, c.elems, c.czs, imps)
                 ep = O.pcsr(c.elems, 4, c.alt, rows, cols, N)
                 cp = O.pcsr(c.czs, 6, c.alt, rows, cols, N)

@@ -98,11 +98,18 @@ def test_contact_steps_converge():
 
 
 def test_contact_steps_match_oracle():
-    """20 steps of a polycrystal pressed between closing platens, contact on:
-    every Newton iteration's impact list (device broad phase, narrow phase and
-    closest face) equals the CPU twin's (host candidate pairs, oracle narrow
-    phase and closest face), the iteration counts are equal, and the
-    displacements and CZ damage state match.  The reference would discard a
+    """20 steps of a polycrystal pressed between closing platens, contact on
+    (platen contact and contact across the grain boundaries): every Newton
+    iteration's impacts (device broad phase, narrow phase and closest face)
+    against the CPU twin's (host pair rule, oracle narrow phase and closest
+    face), equal iteration counts, and matching displacements and CZ damage
+    state.  The two runs' solves differ by rounding (device MINRES, host
+    SuperLU), and a penetrating split-node copy often lies on an edge shared
+    by two faces, so the closest face is a tie that rounding decides: the
+    twin alone, its solve perturbed by 1e-13, changes such faces too.  So per
+    iteration the impacting nodes must be equal, and a face may differ only
+    where both faces are at the same distance from the node (to 1e-12 of the
+    element size).  The reference would discard a
     step and shrink the time step when more than 1 % of the CZs newly damage
     or fail in it, or when Newton does not converge (_checkDamage,
     _adjustTimeStep, ImplicitModel3.cs:198-212, 259-287); the run stays below
@@ -127,8 +134,19 @@ def test_contact_steps_match_oracle():
         assert (dmg - damaged_prev) / nc <= p.maxDamagePerStep and fail / nc <= p.maxFailPerStep, (step, dmg, fail)
         damaged_prev = dmg
     assert len(g.trace) == len(o.trace)
-    for i, (a, b) in enumerate(zip(g.trace, o.trace)):
-        assert np.array_equal(a, b), f"impact lists differ at iteration {i}"
+    from oracle.oracle import Oracle
+
+    O = Oracle()
+    h_el = float(np.linalg.norm(c.x0[c.elems[0, 1]] - c.x0[c.elems[0, 0]]))
+    ties = 0
+    for i, (a, b, x) in enumerate(zip(g.trace, o.trace, o.trace_x)):
+        assert a.shape == b.shape and np.array_equal(a[:, 0], b[:, 0]), f"impacting nodes differ at iteration {i}"
+        for r in np.nonzero((a != b).any(axis=1))[0]:
+            p_ = x[a[r, 0]]
+            da = O.dtn(x[a[r, 1:]].ravel(), p_)
+            db = O.dtn(x[b[r, 1:]].ravel(), p_)
+            assert abs(np.sqrt(da) - np.sqrt(db)) <= 1e-12 * h_el, (i, a[r].tolist(), b[r].tolist(), da, db)
+            ties += 1
     assert sum(len(t) for t in o.trace) > 0, "no contact: the case does not test the contact path"
     u, v, a, cz = g.state()
     assert _rel(u, o.u) <= 1e-8, _rel(u, o.u)
@@ -137,5 +155,6 @@ def test_contact_steps_match_oracle():
         assert _rel(cz["pmax"], o.pmax) <= 1e-8 and _rel(cz["tmax"], o.tmax) <= 1e-8
     assert np.array_equal(cz["failed"], o.failed)
     print(f"contact parity: 20 steps, {sum(o.iterations)} iterations, "
-          f"{sum(len(t) for t in o.trace)} impacts over the iterations, u {_rel(u, o.u):.1e}")
+          f"{sum(len(t) for t in o.trace)} impacts over the iterations ({ties} closest-face ties decided "
+          f"differently), u {_rel(u, o.u):.1e}")
     g.close()

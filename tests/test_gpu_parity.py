@@ -465,12 +465,13 @@ def test_device_broad_phase_matches_host_pairs(O):
         # for group ids that do not fit them (a negative one), the per-cell scan
         from icflow_b200 import _lib
         cross = M.candidate_pairs(coll, coll.x0 + un, same_mesh=False)
-        assert 0 < len(cross) < len(host)
+        assert len(cross) < len(host)  # none when the platens stand clear (gap > 0)
         for shift in (0, -1):
             grp = np.ascontiguousarray(coll.selem_mesh, np.int32) + shift
             _lib.check(gf.ctx, gf.lib.icf_set_surface_groups(gf.ctx, len(grp), _lib.iptr(grp)))
             n2 = C.c_int()
             _lib.check(gf.ctx, gf.lib.icf_broad_phase(gf.ctx, 0.0, C.byref(n2)))
+            gf.nPairs = n2.value
             assert n2.value == len(cross) and np.array_equal(gf.GetPairs(), cross), shift
         gf.close()
 
