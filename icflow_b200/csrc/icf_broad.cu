@@ -169,7 +169,7 @@ __device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, cons
 // candidates are the entries from the end of its (cell, group) run to the end
 // of its cell, found by binary search.
 __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const int *__restrict__ elem,
-                        const double *__restrict__ lohi, const double *__restrict__ red, int nb,
+                        const double *__restrict__ lohi, const int4 *__restrict__ clo, int nb,
                         const int *__restrict__ group, int gbits,
                         const int4 *__restrict__ selem, const double4 *__restrict__ xc, const int *__restrict__ off,
                         int *__restrict__ cnt, unsigned long long *__restrict__ out, long long cap, int pb) {
@@ -191,10 +191,10 @@ __global__ void k_pairs(int m, const unsigned long long *__restrict__ key, const
   for (int j = j0; j < j1 && (gbits >= 0 || key[j] == here); j++) {
     const int b0 = elem[j];
     const int a = a0 < b0 ? a0 : b0, b = a0 < b0 ? b0 : a0;
-    const double *la = lohi + 6 * (size_t)a, *lb = lohi + 6 * (size_t)b;
-    if (cell_of(fmax(la[0], lb[0]), red[1], red[0]) != cx || cell_of(fmax(la[1], lb[1]), red[2], red[0]) != cy ||
-        cell_of(fmax(la[2], lb[2]), red[3], red[0]) != cz)
-      continue;
+    // the cell index is monotone in the coordinate, so the cell of the
+    // intersection's low corner is the larger of the two low cells
+    const int4 ca = clo[a], cb = clo[b];
+    if (max(ca.x, cb.x) != cx || max(ca.y, cb.y) != cy || max(ca.z, cb.z) != cz) continue;
     if (keep_pair(a, b, lohi, group, selem, xc)) {
       // beyond the capacity nothing is written; the host sees the total
       // and repeats with a larger buffer
@@ -381,7 +381,7 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
   cub::DeviceRadixSort::SortPairs(nullptr, tb, W.ek0, W.ek1, W.ee0, W.ee1, m, 0, end_bit, s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->d_tmp, tb, W.ek0, W.ek1, W.ee0, W.ee1, m, 0, end_bit, s));
-  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, W.red, nb, d_group, gbits, ctx->d_selem, ctx->d_xc,
+  k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, W.clo, nb, d_group, gbits, ctx->d_selem, ctx->d_xc,
                                               nullptr, W.pc, nullptr, 0, 0);
   ICF_CUDA(ctx, cudaMemsetAsync(W.pc + m, 0, sizeof(int), s));
   tb = 0;
@@ -406,7 +406,7 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     }
     // pad with all-ones keys: they sort after every pair and form one run
     ICF_CUDA(ctx, cudaMemsetAsync(W.p0, 0xFF, sizeof(unsigned long long) * (size_t)P, s));
-    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, W.red, nb, d_group, gbits, ctx->d_selem, ctx->d_xc,
+    k_pairs<<<icf_blocks(m, 128), 128, 0, s>>>(m, W.ek1, W.ee1, W.lohi, W.clo, nb, d_group, gbits, ctx->d_selem, ctx->d_xc,
                                                 W.po, nullptr, W.p0, P, pb);
     tb = 0;
     // the padding is all ones in every bit, so sorting the low 2 pb bits

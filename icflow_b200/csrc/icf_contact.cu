@@ -84,20 +84,20 @@ __global__ void k_narrow(int np, const int *__restrict__ pairs,
 // element is inside the first; bit 4+k: vertex k of the first inside the second.
 __global__ void k_expand(int np, const int *__restrict__ pairs,
                          const int4 *__restrict__ selem, const int *__restrict__ masks,
-                         const int *__restrict__ off,
+                         const int *__restrict__ off, int eb,
                          unsigned long long *__restrict__ keys) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= np) return;
   const int m = masks[i];
   if (!m) return;
-  const int ea = pairs[2 * i], eb = pairs[2 * i + 1];
-  const int4 A = selem[ea], B = selem[eb];
+  const int ea = pairs[2 * i], eb_ = pairs[2 * i + 1];
+  const int4 A = selem[ea], B = selem[eb_];
   const int na[4] = {A.x, A.y, A.z, A.w}, nb[4] = {B.x, B.y, B.z, B.w};
   int w = off[i];
   for (int k = 0; k < 4; k++)
-    if (m & (1 << k)) keys[w++] = ((unsigned long long)(unsigned)nb[k] << 32) | (unsigned)ea;
+    if (m & (1 << k)) keys[w++] = ((unsigned long long)(unsigned)nb[k] << eb) | (unsigned)ea;
   for (int k = 0; k < 4; k++)
-    if (m & (16 << k)) keys[w++] = ((unsigned long long)(unsigned)na[k] << 32) | (unsigned)eb;
+    if (m & (16 << k)) keys[w++] = ((unsigned long long)(unsigned)na[k] << eb) | (unsigned)eb_;
 }
 
 __device__ double clamp01(double n) { return n <= 0 ? 0 : n >= 1 ? 1 : n; }
@@ -150,14 +150,14 @@ __device__ double dtn(const double f[9], const double p[3]) {
   return r;
 }
 
-__global__ void k_closest(int n, const int *__restrict__ n_dev, const unsigned long long *__restrict__ keys,
+__global__ void k_closest(int n, const int *__restrict__ n_dev, int eb, const unsigned long long *__restrict__ keys,
                           const int *__restrict__ adj_off, const int *__restrict__ adj,
                           const int *__restrict__ faces, const double4 *__restrict__ xc,
                           int4 *__restrict__ imp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || i >= *n_dev) return;
   const unsigned long long key = keys[i];
-  const int node = (int)(key >> 32), el = (int)(key & 0xffffffffULL);
+  const int node = (int)(key >> eb), el = (int)(key & ((1ull << eb) - 1));
   const double4 pp = xc[node];
   const double p[3] = {pp.x, pp.y, pp.z};
   int best = -1;
@@ -461,17 +461,21 @@ int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts) {
       ctx->imp_cap = 2 * total;
       ctx->imp_gen++;
     }
+    // keys node << eb | element, over the bits the ids need
+    int eb = 1, vb = 1;
+    while ((1LL << eb) < (long long)ctx->n_surf) eb++;
+    while ((1LL << vb) < (long long)ctx->n_nodes) vb++;
     k_expand<<<icf_blocks(n_pairs, 128), 128, 0, s>>>(n_pairs, ctx->d_pairs, ctx->d_selem, ctx->d_masks, W.noff,
-                                                     W.nk0);
+                                                     eb, W.nk0);
     tb = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb, W.nk0, W.nk1, total, 0, 64, s);
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, W.nk0, W.nk1, total, 0, eb + vb, s);
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, W.nk0, W.nk1, total, 0, 64, s));
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, W.nk0, W.nk1, total, 0, eb + vb, s));
     tb = 0;
     cub::DeviceSelect::Unique(nullptr, tb, W.nk1, W.nk0, W.d_small, total, s);
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
     ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, W.nk1, W.nk0, W.d_small, total, s));
-    k_closest<<<icf_blocks(total, 128), 128, 0, s>>>(total, W.d_small, W.nk0, ctx->d_adj_off, ctx->d_adj,
+    k_closest<<<icf_blocks(total, 128), 128, 0, s>>>(total, W.d_small, eb, W.nk0, ctx->d_adj_off, ctx->d_adj,
                                                     ctx->d_faces, ctx->d_xc, ctx->d_imp);
     ICF_CUDA(ctx, cudaGetLastError());
     ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 1, 0, sizeof(int), s));

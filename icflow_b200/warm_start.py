@@ -230,7 +230,24 @@ class LearnedWarmStart:
         return du + g * corr
 
     def __call__(self, model, h, u, v, a):
+        if self.select_gains:
+            return self.judged_guess(model, h, u, v, a)
         return self.guess(model, h, u, v, a)
+
+    # per step, the network's correction is judged before it is used: the
+    # first-iterate residual of the guess at each candidate gain (one assembly
+    # each, no solve) picks the gain; 0 is the extrapolation alone
+    select_gains: tuple = ()
+    chosen: list = None
+
+    def judged_guess(self, model, h, u, v, a):
+        gains = self.select_gains
+        guesses = [self.guess(model, h, u, v, a, gain=g) for g in gains]
+        rs = model.guess_residuals(guesses)
+        k = int(np.argmin(rs))
+        if self.chosen is not None:
+            self.chosen.append(gains[k])
+        return guesses[k]
 
     def calibrate(self, model, steps: int, gains=(0.0, 0.05, 0.2, 0.5, 1.0)) -> dict:
         """Runs `steps` steps of `model` (plain guess) and, before each, the
