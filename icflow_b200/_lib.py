@@ -136,6 +136,7 @@ SIGNATURES = {
     "icf_mlp_set_params": (I, [P, P, P]),
     "icf_mlp_get_params": (I, [P, P, P]),
     "icf_mlp_forward": (I, [P, I, P, P]),
+    "icf_mlp_forward_trace": (I, [P, I, P, P, P, P, P, P]),
     "icf_mlp_grad": (I, [P, I, P, P, P, C.POINTER(C.c_float)]),
     "icf_mlp_train": (I, [P, I, P, P, I, I, C.c_float, C.c_ulonglong, C.POINTER(C.c_float)]),
     "icf_mlp_grad_dy": (I, [P, I, P, P, P]),

@@ -545,6 +545,30 @@ int icf_mlp_forward(icf_mlp *m, int n, const float *x, float *y) {
   return ICF_OK;
 }
 
+int icf_mlp_forward_trace(icf_mlp *m, int n, const float *x, float *z1, float *h1, float *z2, float *h2, float *y) {
+  if (!m || n <= 0 || !x || !z1 || !h1 || !z2 || !h2 || !y) return ICF_ERR_ARG;
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  if (ensure_cap(m, n)) return ICF_ERR_CUDA;
+  cudaStream_t s = m->stream;
+  MLP_CUDA(m, cudaMemcpyAsync(m->d_x, x, sizeof(float) * NI * (size_t)n, cudaMemcpyHostToDevice, s));
+  const int tiles = (n + 15) / 16;
+  // the training forward writes the activations (no target: dy untouched)
+  k_mlp_fwd_train<<<(tiles + 7) / 8, 256, 0, s>>>(n, m->d_x, nullptr, m->d_wb, m->d_master, m->d_norm, m->d_z1,
+                                                  m->d_h1, m->d_z2, m->d_h2, m->d_dy, m->d_loss + 1);
+  int blocks = (tiles + 7) / 8;
+  if (blocks > 1184) blocks = 1184;
+  k_mlp_infer<<<blocks, 256, 0, s>>>(n, m->d_x, m->d_wb, m->d_master, m->d_norm, m->d_out);
+  MLP_CUDA(m, cudaGetLastError());
+  const size_t hb = sizeof(float) * NH * (size_t)n;
+  MLP_CUDA(m, cudaMemcpyAsync(z1, m->d_z1, hb, cudaMemcpyDeviceToHost, s));
+  MLP_CUDA(m, cudaMemcpyAsync(h1, m->d_h1, hb, cudaMemcpyDeviceToHost, s));
+  MLP_CUDA(m, cudaMemcpyAsync(z2, m->d_z2, hb, cudaMemcpyDeviceToHost, s));
+  MLP_CUDA(m, cudaMemcpyAsync(h2, m->d_h2, hb, cudaMemcpyDeviceToHost, s));
+  MLP_CUDA(m, cudaMemcpyAsync(y, m->d_out, sizeof(float) * NO * (size_t)n, cudaMemcpyDeviceToHost, s));
+  MLP_CUDA(m, cudaStreamSynchronize(s));
+  return ICF_OK;
+}
+
 int icf_mlp_grad(icf_mlp *m, int n, const float *x, const float *y, float *grad, float *loss) {
   if (!m || n <= 0 || !x || !y || !grad) return ICF_ERR_ARG;
   MLP_CUDA(m, cudaSetDevice(m->device));

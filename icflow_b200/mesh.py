@@ -390,21 +390,27 @@ def polycrystal(n: int = 32, grains: int = 128, edge: float = 1e-3, seed: int = 
 
 
 def ice_impact(n: int = 40, grains: int = 64, seed: int = 0, size=(0.2, 0.2, 0.1), gap: float = 1e-4,
-               speed: float = 2.5):
+               speed: float = 2.5, shift=(0.37, 0.21)):
     """Two ice blocks colliding: each size[0] x size[1] x size[2] m, n x n x
     n/2 hexahedra (3 n^3 tets; n = 40 gives 192,000 tets per block), `grains`
     Voronoi grains with CZs on every grain boundary; block B sits `gap` m above
-    block A, and they approach at +-speed m/s along z (5 m/s relative by
-    default: the 0.1 mm gap closes in 4 steps of 5 us).  No node is anchored.
+    block A, shifted in x and y by `shift` times the hexahedron edge, and they
+    approach at +-speed m/s along z (5 m/s relative by default: the 0.1 mm gap
+    closes in 4 steps of 5 us).  Without the shift both blocks share one x-y
+    grid, every node of A's top face meets a vertical edge of B's bottom layer,
+    and the point-in-tet test (strict inequalities) contains it in no tet.  No
+    node is anchored.
     Returns the collection and the initial velocity of every node [N, 3] (the
     reference has no such input, ImplicitModel3 starts at rest; v0 is
     ImplicitModel3's extension for this workload)."""
     nz = max(1, n // 2)
     meshes = []
     for k, (z0, name) in enumerate(((0.0, "blockA"), (size[2] + gap, "blockB"))):
-        m = box_mesh((n, n, nz), size, (0.0, 0.0, z0), name=name)
-        g = voronoi_grains(m.x0, m.elems, grains, seed * 1000 + k, lo=(0.0, 0.0, z0),
-                           hi=(size[0], size[1], z0 + size[2]))
+        ox = k * shift[0] * size[0] / n
+        oy = k * shift[1] * size[1] / n
+        m = box_mesh((n, n, nz), size, (ox, oy, z0), name=name)
+        g = voronoi_grains(m.x0, m.elems, grains, seed * 1000 + k, lo=(ox, oy, z0),
+                           hi=(ox + size[0], oy + size[1], z0 + size[2]))
         meshes.append(insert_czs(m, g))
     coll = Collection(meshes).prepare()
     v0 = np.zeros_like(coll.x0)

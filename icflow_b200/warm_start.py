@@ -72,6 +72,17 @@ class MLP:
         self._check(self.lib.icf_mlp_forward(self.h, len(x), x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p)))
         return y
 
+    def forward_trace(self, x: np.ndarray) -> dict:
+        """z1, h1, z2, h2 [n, 64] and y [n, 3] of the forward (layer-by-layer checks)."""
+        x = np.ascontiguousarray(x, np.float32)
+        n = len(x)
+        out = {k: np.zeros((n, 64), np.float32) for k in ("z1", "h1", "z2", "h2")}
+        out["y"] = np.zeros((n, 3), np.float32)
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        self._check(self.lib.icf_mlp_forward_trace(self.h, n, ptr(x), ptr(out["z1"]), ptr(out["h1"]), ptr(out["z2"]),
+                                                   ptr(out["h2"]), ptr(out["y"])))
+        return out
+
     def grad(self, x: np.ndarray, y: np.ndarray):
         x = np.ascontiguousarray(x, np.float32).reshape(-1, NI)
         y = np.ascontiguousarray(y, np.float32).reshape(-1, NO)

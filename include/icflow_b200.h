@@ -351,6 +351,11 @@ int icf_mlp_set_params(icf_mlp *m, const float *params, const float *norm);
 int icf_mlp_get_params(icf_mlp *m, float *params, float *norm);
 /* y[n*3] = network(x[n*15]) */
 int icf_mlp_forward(icf_mlp *m, int n, const float *x, float *y);
+/* the forward's intermediate values for n nodes (host buffers): z1, z2 the
+ * float32 pre-activations [n][64], h1, h2 = bf16(GELU(z)) as floats [n][64],
+ * y the output [n][3] of icf_mlp_forward; for checking the kernels layer by
+ * layer (no reference counterpart) */
+int icf_mlp_forward_trace(icf_mlp *m, int n, const float *x, float *z1, float *h1, float *z2, float *h2, float *y);
 /* gradient of the mean squared error over n nodes and 3 outputs */
 int icf_mlp_grad(icf_mlp *m, int n, const float *x, const float *y, float *grad, float *loss);
 /* gradient for a loss the caller defines: dy[n*3] = dL/d(output), so that

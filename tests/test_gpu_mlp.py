@@ -7,7 +7,7 @@ import pytest
 
 from icflow_b200.implicit_model import ImplicitModel3
 from icflow_b200.warm_start import MLP, LearnedWarmStart, init_params
-from oracle.mlp_oracle import NI, NO, forward, loss_and_grad
+from oracle.mlp_oracle import NI, NO, check_trace, forward, loss_and_grad
 from tests.test_gpu_newton import _prms, fast_cantilever
 
 pytestmark = pytest.mark.gpu
@@ -23,13 +23,33 @@ def _setup(seed=0, n=3000):
 
 
 def test_forward_matches_cpu():
+    """Layer by layer (oracle.mlp_oracle.check_trace): every float32
+    pre-activation within the float32 summation bound of the float64 value
+    from the kernel's own previous layer, every bf16 activation the correct
+    rounding of GELU of the kernel's pre-activation (or, within float32
+    error of a rounding boundary, its neighbour).  End to end: within 1e-4 of
+    the restatement (max-norm relative) on every node where the two made the
+    same bf16 roundings; elsewhere a rounding boundary moves one activation
+    by one bf16 unit, within 2e-3."""
     p, norm, x = _setup(0, 1037)  # not a multiple of 16
     net = MLP()
     net.set_params(p, norm)
     y = net.forward(x)
-    ref = forward(p, norm, x)["y"]
-    err = np.abs(y - ref).max() / np.abs(ref).max()
-    assert err <= 2e-3, err
+    tr = net.forward_trace(x)
+    assert np.array_equal(tr["y"], y)
+    rep = check_trace(p, norm, x, tr)
+    assert rep["mismatched"] == 0 and max(rep["z1"], rep["z2"], rep["z3"]) <= 1.0, rep
+    c = forward(p, norm, x)
+    ref = c["y"]
+    same = (tr["h1"] == c["h1"]).all(axis=1) & (tr["h2"] == c["h2"]).all(axis=1)
+    scale = np.abs(ref).max()
+    err_same = np.abs(y - ref)[same].max() / scale
+    err_all = np.abs(y - ref).max() / scale
+    print(f"MLP forward: layer bound ratios {rep}; nodes with equal roundings {same.sum()}/{len(x)}, "
+          f"error there {err_same:.1e}, over all nodes {err_all:.1e}")
+    assert same.sum() >= len(x) // 2  # measured: 874 of 1037 (the rest hold a near-tie activation)
+    assert err_same <= 1e-4, err_same
+    assert err_all <= 2e-3, err_all
     net.close()
 
 
@@ -40,10 +60,10 @@ def test_gradient_matches_cpu():
     net.set_params(p, norm)
     g, loss = net.grad(x, t)
     lref, gref = loss_and_grad(p, norm, x, t)
-    assert abs(loss - lref) <= 1e-3 * lref
+    assert abs(loss - lref) <= 1e-5 * lref, (loss, lref)
     err = np.abs(g - gref).max() / np.abs(gref).max()
     print(f"MLP gradient vs CPU restatement: {err:.2e} (max-norm relative)")
-    assert err <= 1e-2, err
+    assert err <= 1e-5, err
     # identical on a second run (fixed-order reductions)
     g2, _ = net.grad(x, t)
     assert np.array_equal(g, g2)

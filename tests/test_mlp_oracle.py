@@ -33,3 +33,26 @@ def test_bf16_rounding():
     assert r[3] == np.float32(-3.140625) and r[4] == 0.0
     # bf16 keeps 8 significant bits
     assert np.all(np.abs(r - x) <= np.abs(x) * 2 ** -8 + 1e-38)
+
+
+def test_trace_check_accepts_the_restatement_and_catches_planted_errors():
+    """check_trace on the restatement's own float32 trace passes; a hidden
+    activation moved by one bf16 unit, or a pre-activation moved well beyond
+    float32 summation error, fails it (the mistakes are planted in the
+    restatement's trace, on the CPU)."""
+    from oracle.mlp_oracle import check_trace, forward
+
+    rng = np.random.default_rng(4)
+    p = _params(4).astype(np.float32)
+    norm = np.concatenate([rng.normal(size=NI), rng.uniform(0.5, 2, NI), np.ones(NO)]).astype(np.float32)
+    x = (rng.normal(size=(300, NI)) / norm[NI:2 * NI] + norm[:NI]).astype(np.float32)
+    c = forward(p, norm, x)
+    tr = {k: c[k] for k in ("z1", "h1", "z2", "h2", "y")}
+    rep = check_trace(p, norm, x, tr)
+    assert rep["mismatched"] == 0 and max(rep["z1"], rep["z2"], rep["z3"]) <= 1.0, rep
+    h1 = tr["h1"].copy()
+    h1.view(np.uint32)[7, 11] += 0x10000
+    assert check_trace(p, norm, x, dict(tr, h1=h1))["mismatched"] == 1
+    z2 = tr["z2"].copy()
+    z2[3, 4] += 1e-2 * (abs(z2[3, 4]) + 1)
+    assert check_trace(p, norm, x, dict(tr, z2=z2))["z2"] > 1.0
