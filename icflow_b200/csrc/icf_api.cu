@@ -219,7 +219,8 @@ static void free_all(icf_ctx *c) {
                   c->sell_off_cz.meta, c->sell_off_cz.unit, c->sell_off_cz.codes, c->sell_diag_cz.meta,
                   c->sell_diag_cz.unit, c->sell_diag_cz.codes, c->sell_off.unit_s, c->sell_diag.unit_s,
                   c->sell_off_cz.unit_s, c->sell_diag_cz.unit_s, c->d_czhist,
-                  c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup, c->d_imp_built, c->d_imp_pos};
+                  c->d_tetpos, c->d_stage_off, c->d_stage_diag, c->d_sgroup, c->d_imp_built, c->d_imp_pos,
+                  c->d_snode, c->d_sinc_off, c->d_sinc};
   for (void *p : ptrs) cudaFree(p);
 }
 
@@ -445,6 +446,8 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->d_stage_off = ctx->d_stage_diag = nullptr;
   ctx->stage_off_cap = ctx->stage_diag_cap = 0;
   ctx->d_sgroup = nullptr;
+  ctx->d_snode = ctx->d_sinc_off = ctx->d_sinc = nullptr;
+  ctx->n_snode = 0;
   ctx->pairs_from_broad = false;
   ctx->per_cz_prm = false;
   ctx->have_structure = false;
@@ -517,6 +520,39 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
     if (adj_offsets[n_surface] > 0)
       ICF_CUDA(ctx, cudaMemcpy(ctx->d_adj, adj_faces, sizeof(int) * (size_t)adj_offsets[n_surface], cudaMemcpyHostToDevice));
     ICF_CUDA(ctx, cudaMemcpy(ctx->d_faces, faces, sizeof(int) * 3 * (size_t)n_faces, cudaMemcpyHostToDevice));
+    // surface nodes and the surface elements holding each (counting sort by
+    // node: ascending nodes, ascending elements per node)
+    std::vector<int> cnt(n + 1, 0);
+    for (long long i = 0; i < 4LL * n_surface; i++) cnt[surface_elems[i] + 1]++;
+    std::vector<int> idx(n, -1), snode, soff(1, 0);
+    for (int v = 0; v < n_nodes; v++)
+      if (cnt[v + 1]) {
+        idx[v] = (int)snode.size();
+        snode.push_back(v);
+        soff.push_back(soff.back() + cnt[v + 1]);
+      }
+    std::vector<int> cur(soff.begin(), soff.end() - 1), sinc(4 * (size_t)n_surface);
+    for (int e = 0; e < n_surface; e++)
+      for (int k = 0; k < 4; k++) {
+        const int j = idx[surface_elems[4 * (size_t)e + k]];
+        // an element listing a node twice is held once
+        if (cur[j] > soff[j] && sinc[cur[j] - 1] == e) continue;
+        sinc[cur[j]++] = e;
+      }
+    // compact the per-node lists (repeated nodes left gaps at their ends)
+    std::vector<int> off2(1, 0), inc2;
+    inc2.reserve(sinc.size());
+    for (size_t j = 0; j < snode.size(); j++) {
+      for (int q = soff[j]; q < cur[j]; q++) inc2.push_back(sinc[q]);
+      off2.push_back((int)inc2.size());
+    }
+    ctx->n_snode = (int)snode.size();
+    ICF_TRY(dalloc(ctx, &ctx->d_snode, snode.size()));
+    ICF_TRY(dalloc(ctx, &ctx->d_sinc_off, off2.size()));
+    ICF_TRY(dalloc(ctx, &ctx->d_sinc, inc2.size()));
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_snode, snode.data(), sizeof(int) * snode.size(), cudaMemcpyHostToDevice));
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_sinc_off, off2.data(), sizeof(int) * off2.size(), cudaMemcpyHostToDevice));
+    ICF_CUDA(ctx, cudaMemcpy(ctx->d_sinc, inc2.data(), sizeof(int) * inc2.size(), cudaMemcpyHostToDevice));
   }
   ctx->have_static = true;
   ctx->version++;
@@ -591,6 +627,23 @@ int icf_broad_phase(icf_ctx *ctx, double pad, int *n_pairs) {
   ICF_CUDA(ctx, cudaSetDevice(ctx->device));
   ICF_TRY(icf_broad_phase_impl(ctx, pad, ctx->d_sgroup, n_pairs));
   ctx->pairs_from_broad = true;
+  return ICF_OK;
+}
+
+int icf_detect_contacts(icf_ctx *ctx, double pad, int *n_impacts) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_static || !ctx->have_nodes) return icf_fail(ctx, ICF_ERR_STATE, "static data and node state first");
+  if (!n_impacts || !(pad >= 0) || !std::isfinite(pad)) return icf_fail(ctx, ICF_ERR_ARG, "pad >= 0 and n_impacts required");
+  ICF_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (ctx->prm.CollisionScheme == 0) {
+    ctx->n_imp = 0;
+    *n_impacts = 0;
+    ctx->have_structure = false;
+    ctx->imp_cmp_valid = false;
+    return ICF_OK;
+  }
+  ICF_TRY(icf_detect_contacts_impl(ctx, pad, ctx->d_sgroup, n_impacts));
+  ctx->have_structure = false;
   return ICF_OK;
 }
 

@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstdint>
 
+#include "icf_collide.cuh"
 #include "icf_internal.cuh"
 
 namespace {
@@ -133,36 +134,7 @@ __device__ __forceinline__ int upper_key(const unsigned long long *key, int lo, 
   return lo;
 }
 
-// A vertex of one element inside the other's box (closed).
-__device__ __forceinline__ bool vertex_in_box(const int n[4], const double4 *xc, const double *lh) {
-#pragma unroll
-  for (int v = 0; v < 4; v++) {
-    const double4 p = xc[n[v]];
-    if (p.x >= lh[0] && p.x <= lh[3] && p.y >= lh[1] && p.y <= lh[4] && p.z >= lh[2] && p.z <= lh[5])
-      return true;
-  }
-  return false;
-}
-
-// A candidate pair: boxes overlap, no node in common (the narrow phase skips
-// such pairs, kNarrowPhase_new, narrowphase.h:67-70), a vertex of one inside
-// the other's box (an impact needs a vertex inside the other tet, so this
-// drops no pair that can give one), and different groups when groups are set.
-__device__ __forceinline__ bool keep_pair(int a, int b, const double *lohi, const int *group,
-                                          const int4 *selem, const double4 *xc) {
-  if (group && group[a] == group[b]) return false;
-  for (int k = 0; k < 3; k++)
-    if (!(lohi[6 * (size_t)a + k] <= lohi[6 * (size_t)b + 3 + k] && lohi[6 * (size_t)b + k] <= lohi[6 * (size_t)a + 3 + k]))
-      return false;
-  const int4 p = selem[a], q = selem[b];
-  const int pa[4] = {p.x, p.y, p.z, p.w}, qb[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      if (pa[i] == qb[j]) return false;
-  return vertex_in_box(pa, xc, lohi + 6 * (size_t)b) || vertex_in_box(qb, xc, lohi + 6 * (size_t)a);
-}
+// vertex_in_box and keep_pair (the pair rule): icf_collide.cuh
 
 // entry i pairs with the later entries of its cell; count, then write.  With
 // group keys (gbits >= 0) the later entries of its own group are skipped: the
@@ -286,6 +258,100 @@ __global__ void k_red7_final(int nb, int n, const double *__restrict__ part, dou
   }
 }
 
+// ---- contact detection without the pair list ------------------------------------
+// A pair (a, b) gives the impact (p, b) when p is a node of a, the narrow
+// phase finds p strictly inside b, and (a, b) satisfies the pair rule.  So
+// the impact list follows from one query per surface node p: the surface
+// elements b whose boxes hold p (the grid cell of p lists them all, a box
+// being entered in every cell it reaches), p not a node of b, p inside b
+// (tet_contains with b's inverse, the same bits as in k_narrow), and some
+// surface element a holding p with keep_pair(a, b).  Every (p, b) is found
+// once (p lies in one cell).  tet_contains needs the barycentric coordinates
+// above 1e-10, so p is then strictly inside b's box.
+
+// per surface element: the inverse of its edge matrix and its first vertex
+__global__ void k_tet_inv(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
+                          double *__restrict__ inv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 id = selem[i];
+  const int nn[4] = {id.x, id.y, id.z, id.w};
+  double x[12];
+  for (int k = 0; k < 4; k++) {
+    const double4 p = xc[nn[k]];
+    x[3 * k] = p.x; x[3 * k + 1] = p.y; x[3 * k + 2] = p.z;
+  }
+  double b[9];
+  tet_inverse(x, b);
+  double *o = inv + 12 * (size_t)i;
+  for (int k = 0; k < 9; k++) o[k] = b[k];
+  o[9] = x[0]; o[10] = x[1]; o[11] = x[2];
+}
+
+__device__ __forceinline__ long long cell_lin(int x, int y, int z, int ny, int nz) {
+  return ((long long)x * ny + y) * nz + z;
+}
+
+// count (off == nullptr) or place every (cell, element) entry of the dense grid
+__global__ void k_grid_put(int n, const int4 *__restrict__ clo, int ny, int nz, int *__restrict__ cnt,
+                           const int *__restrict__ off, int *__restrict__ ent, long long cap) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 c = clo[i];
+  const int sx = c.w & 1023, sy = (c.w >> 10) & 1023, sz = (c.w >> 20) & 1023;
+  for (int dx = 0; dx <= sx; dx++)
+    for (int dy = 0; dy <= sy; dy++)
+      for (int dz = 0; dz <= sz; dz++) {
+        const long long l = cell_lin(c.x + dx, c.y + dy, c.z + dz, ny, nz);
+        const int k = atomicAdd(cnt + l, 1);
+        if (off) {
+          const long long pos = (long long)off[l] + k;
+          if (pos < cap) ent[pos] = i;
+        }
+      }
+}
+
+// one thread per surface node: keys node << eb | element of its impacts
+__global__ void __launch_bounds__(128) k_detect(int ns, const int *__restrict__ snode, const int *__restrict__ sinc_off,
+                                                const int *__restrict__ sinc, const double4 *__restrict__ xc,
+                                                const double *__restrict__ red, int nx, int ny, int nz,
+                                                const int *__restrict__ goff, const int *__restrict__ gent,
+                                                long long ent_cap, const double *__restrict__ lohi,
+                                                const double *__restrict__ inv, const int4 *__restrict__ selem,
+                                                const int *__restrict__ group, int eb,
+                                                unsigned long long *__restrict__ out, long long cap,
+                                                int *__restrict__ count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  const int p = snode[k];
+  const double4 P = xc[p];
+  const double cell = red[0];
+  const int cx = cell_of(P.x, red[1], cell), cy = cell_of(P.y, red[2], cell), cz = cell_of(P.z, red[3], cell);
+  if (cx < 0 || cy < 0 || cz < 0 || cx >= nx || cy >= ny || cz >= nz) return;
+  const long long l = cell_lin(cx, cy, cz, ny, nz);
+  const long long e0 = goff[l], e1 = min((long long)goff[l + 1], ent_cap);
+  for (long long e = e0; e < e1; e++) {
+    const int b = gent[e];
+    const double *lh = lohi + 6 * (size_t)b;
+    if (!(P.x >= lh[0] && P.x <= lh[3] && P.y >= lh[1] && P.y <= lh[4] && P.z >= lh[2] && P.z <= lh[5])) continue;
+    const int4 B = selem[b];
+    if (B.x == p || B.y == p || B.z == p || B.w == p) continue;
+    const double *q = inv + 12 * (size_t)b;
+    double bi[9];
+#pragma unroll
+    for (int t = 0; t < 9; t++) bi[t] = q[t];
+    if (!tet_contains(bi, P.x - q[9], P.y - q[10], P.z - q[11])) continue;
+    bool any = false;
+    for (int j = sinc_off[k]; j < sinc_off[k + 1] && !any; j++) {
+      const int a = sinc[j];
+      any = keep_pair(a < b ? a : b, a < b ? b : a, lohi, group, selem, xc);
+    }
+    if (!any) continue;
+    const int w = atomicAdd(count, 1);
+    if (w < cap) out[w] = ((unsigned long long)(unsigned)p << eb) | (unsigned)b;
+  }
+}
+
 }  // namespace
 
 template <typename T>
@@ -299,7 +365,7 @@ static int grow(icf_ctx *ctx, T **p, long long n) {
 void icf_free_contact_ws(icf_ctx *ctx) {
   icf_contact_ws &W = ctx->cws;
   void *d[] = {W.lohi, W.ext, W.tmpv, W.red, W.bcnt, W.boff, W.clo, W.ek0, W.ek1, W.ee0, W.ee1, W.pc, W.po,
-               W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small};
+               W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small, W.tinv, W.gcnt, W.goff, W.gcur, W.gent};
   for (void *q : d) cudaFree(q);
   cudaFreeHost(W.h_small);
   cudaFreeHost(W.h_red);
@@ -432,4 +498,128 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
     W.pair_cap = c;
   }
   return icf_fail(ctx, ICF_ERR_SIZE, "broad phase: pair buffer growth did not converge");
+}
+
+// Contact detection without the pair list.  Three synchronisations: the grid
+// (cell size and corners, which set the grid's dimensions), the entry and hit
+// counts (to grow the buffers and repeat when they overflow), and the impact
+// list's count in icf_finish_impacts.  The grid is dense: if the boxes' hull
+// holds more than 8 cells per surface element at the mean box extent, the
+// cell grows until it holds at most that many.
+int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_impacts) {
+  cudaStream_t s = ctx->stream;
+  const int n = ctx->n_surf;
+  icf_contact_ws &W = ctx->cws;
+  *n_impacts = 0;
+  ctx->imp_cmp_valid = false;
+  if (n < 2 || ctx->n_snode == 0) {
+    ctx->n_imp = 0;
+    return ICF_OK;
+  }
+  ICF_TRY_RC(ensure_small(ctx));
+  const int nbk = (int)std::min<long long>((n + 255) / 256, 2LL * ctx->n_sm);
+  if (n > W.b_cap) {
+    ICF_TRY_RC(grow(ctx, &W.lohi, 6LL * n));
+    ICF_TRY_RC(grow(ctx, &W.ext, n));
+    ICF_TRY_RC(grow(ctx, &W.bcnt, n + 1LL));
+    ICF_TRY_RC(grow(ctx, &W.boff, n + 1LL));
+    ICF_TRY_RC(grow(ctx, &W.clo, n));
+    W.b_cap = n;
+  }
+  if (n > W.tinv_cap) {
+    ICF_TRY_RC(grow(ctx, &W.tinv, 12LL * n));
+    W.tinv_cap = n;
+  }
+  if (!W.tmpv) ICF_TRY_RC(grow(ctx, &W.tmpv, 8LL * (2 * ctx->n_sm + 1)));
+  if (!W.red) ICF_TRY_RC(grow(ctx, &W.red, 8));
+  k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext);
+  k_red7<<<nbk, 256, 0, s>>>(n, W.lohi, W.ext, W.tmpv);
+  k_red7_final<<<1, 256, 0, s>>>(nbk, n, W.tmpv, W.red);
+  k_tet_inv<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.tinv);
+  ICF_CUDA(ctx, cudaMemcpyAsync(W.h_red, W.red, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaStreamSynchronize(s));
+  double *h_red = W.h_red;
+  if (!(h_red[0] > 0) || !std::isfinite(h_red[0])) return icf_fail(ctx, ICF_ERR_NUMERIC, "contact detection: degenerate boxes");
+  double cell = h_red[0];
+  long long dims[3], C = 0;
+  for (int attempt = 0; attempt < 64; attempt++) {
+    C = 1;
+    for (int k = 0; k < 3; k++) {
+      const double span = (h_red[4 + k] - h_red[1 + k]) / cell;
+      dims[k] = std::isfinite(span) ? (long long)span + 2 : (1LL << 40);
+      C = (dims[k] > (1LL << 40) / std::max(C, 1LL)) ? (1LL << 40) : C * dims[k];
+    }
+    if (C <= 8LL * n + 4096) break;
+    cell *= 1.25;
+  }
+  if (C > 8LL * n + 4096 || dims[0] > INT32_MAX || dims[1] > INT32_MAX || dims[2] > INT32_MAX)
+    return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: grid too large");
+  if (cell != h_red[0]) {
+    h_red[0] = cell;
+    ICF_CUDA(ctx, cudaMemcpyAsync(W.red, h_red, sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  const int nx = (int)dims[0], ny = (int)dims[1], nz = (int)dims[2];
+  if (C + 1 > W.cell_cap) {
+    ICF_TRY_RC(grow(ctx, &W.gcnt, C + 1));
+    ICF_TRY_RC(grow(ctx, &W.goff, C + 1));
+    ICF_TRY_RC(grow(ctx, &W.gcur, C + 1));
+    W.cell_cap = C + 1;
+  }
+  if (W.dent_cap == 0) {
+    ICF_TRY_RC(grow(ctx, &W.gent, 8LL * n + 1024));
+    W.dent_cap = 8LL * n + 1024;
+  }
+  if (W.nkey_cap == 0) {
+    const long long c = std::max<long long>(n / 4, 1024);
+    ICF_TRY_RC(grow(ctx, &W.nk0, c));
+    ICF_TRY_RC(grow(ctx, &W.nk1, c));
+    W.nkey_cap = c;
+  }
+  k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
+  ICF_CUDA(ctx, cudaMemsetAsync(W.gcnt, 0, sizeof(int) * (size_t)(C + 1), s));
+  k_grid_put<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.clo, ny, nz, W.gcnt, nullptr, nullptr, 0);
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, W.gcnt, W.goff, (int)(C + 1), s);
+  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.gcnt, W.goff, (int)(C + 1), s));
+  int eb = 1, vb = 1;
+  while ((1LL << eb) < (long long)n) eb++;
+  while ((1LL << vb) < (long long)ctx->n_nodes) vb++;
+  int hits = 0;
+  for (int attempt = 0; attempt < 3; attempt++) {
+    ICF_CUDA(ctx, cudaMemsetAsync(W.gcur, 0, sizeof(int) * (size_t)(C + 1), s));
+    ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, sizeof(int), s));
+    k_grid_put<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.clo, ny, nz, W.gcur, W.goff, W.gent, W.dent_cap);
+    k_detect<<<icf_blocks(ctx->n_snode, 128), 128, 0, s>>>(
+        ctx->n_snode, ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, ctx->d_xc, W.red, nx, ny, nz, W.goff, W.gent,
+        W.dent_cap, W.lohi, W.tinv, ctx->d_selem, d_group, eb, W.nk0, W.nkey_cap, W.d_small + 5);
+    ICF_CUDA(ctx, cudaGetLastError());
+    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 5, W.d_small + 5, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 6, W.goff + C, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaStreamSynchronize(s));
+    hits = W.h_small[5];
+    const long long m = W.h_small[6];
+    bool again = false;
+    if (m > W.dent_cap) {
+      ICF_TRY_RC(grow(ctx, &W.gent, m + m / 4 + 1024));
+      W.dent_cap = m + m / 4 + 1024;
+      again = true;
+    }
+    if (hits > W.nkey_cap) {
+      const long long c = hits + hits / 4 + 1024;
+      ICF_TRY_RC(grow(ctx, &W.nk0, c));
+      ICF_TRY_RC(grow(ctx, &W.nk1, c));
+      W.nkey_cap = c;
+      again = true;
+    }
+    if (!again) break;
+    if (attempt == 2) return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: buffer growth did not converge");
+  }
+  if (hits > 0) {
+    tb = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, W.nk0, W.nk1, hits, 0, eb + vb, s);
+    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, W.nk0, W.nk1, hits, 0, eb + vb, s));
+  }
+  return icf_finish_impacts(ctx, W.nk1, hits, W.d_small + 5, eb, n_impacts);
 }

@@ -17,36 +17,12 @@
 //                 the derivatives follow in icf_contact_deriv.cu
 #include <cub/cub.cuh>
 
+#include "icf_collide.cuh"
 #include "icf_internal.cuh"
 
 namespace {
 
-// ---- narrow phase ---------------------------------------------------------------
-__device__ void tet_inverse(const double *x, double b[9]) {
-  const double a11 = x[3] - x[0], a12 = x[6] - x[0], a13 = x[9] - x[0];
-  const double a21 = x[4] - x[1], a22 = x[7] - x[1], a23 = x[10] - x[1];
-  const double a31 = x[5] - x[2], a32 = x[8] - x[2], a33 = x[11] - x[2];
-  const double det = a31 * (-a13 * a22 + a12 * a23) + a32 * (a13 * a21 - a11 * a23) +
-                     a33 * (-a12 * a21 + a11 * a22);
-  b[0] = (-a23 * a32 + a22 * a33) / det;
-  b[1] = (a13 * a32 - a12 * a33) / det;
-  b[2] = (-a13 * a22 + a12 * a23) / det;
-  b[3] = (a23 * a31 - a21 * a33) / det;
-  b[4] = (-a13 * a31 + a11 * a33) / det;
-  b[5] = (a13 * a21 - a11 * a23) / det;
-  b[6] = (-a22 * a31 + a21 * a32) / det;
-  b[7] = (a12 * a31 - a11 * a32) / det;
-  b[8] = (-a12 * a21 + a11 * a22) / det;
-}
-
-__device__ bool tet_contains(const double b[9], double x, double y, double z) {
-  const double eps = 1E-10;
-  const double y1 = x * b[0] + y * b[1] + z * b[2];
-  const double y2 = x * b[3] + y * b[4] + z * b[5];
-  const double y3 = x * b[6] + y * b[7] + z * b[8];
-  return (y1 > eps && y2 > eps && y3 > eps && (y1 + y2 + y3) < (1 - eps));
-}
-
+// ---- narrow phase (tet_inverse, tet_contains: icf_collide.cuh) ----------------
 __global__ void k_narrow(int np, const int *__restrict__ pairs,
                          const int4 *__restrict__ selem,
                          const double4 *__restrict__ xc, int *__restrict__ masks,
@@ -446,8 +422,9 @@ int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts) {
   ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 4, W.noff + n_pairs, sizeof(int), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaStreamSynchronize(s));
   const int total = W.h_small[4];
-  const bool cmp = ctx->n_imp_built >= 0 && ctx->imp_gen == ctx->imp_gen_built;
-  int nu = 0;
+  int eb = 1, vb = 1;
+  while ((1LL << eb) < (long long)ctx->n_surf) eb++;
+  while ((1LL << vb) < (long long)ctx->n_nodes) vb++;
   if (total > 0) {
     if (total > W.nkey_cap) {
       const long long c = total + total / 4 + 64;
@@ -455,16 +432,7 @@ int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts) {
       ICF_TRY_RC(grow_buf(ctx, &W.nk1, c));
       W.nkey_cap = c;
     }
-    // the impact list holds at most `total` entries
-    if (total > ctx->imp_cap) {
-      ICF_TRY_RC(grow_buf(ctx, &ctx->d_imp, 2LL * total));
-      ctx->imp_cap = 2 * total;
-      ctx->imp_gen++;
-    }
     // keys node << eb | element, over the bits the ids need
-    int eb = 1, vb = 1;
-    while ((1LL << eb) < (long long)ctx->n_surf) eb++;
-    while ((1LL << vb) < (long long)ctx->n_nodes) vb++;
     k_expand<<<icf_blocks(n_pairs, 128), 128, 0, s>>>(n_pairs, ctx->d_pairs, ctx->d_selem, ctx->d_masks, W.noff,
                                                      eb, W.nk0);
     tb = 0;
@@ -475,14 +443,35 @@ int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts) {
     cub::DeviceSelect::Unique(nullptr, tb, W.nk1, W.nk0, W.d_small, total, s);
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
     ICF_CUDA(ctx, cub::DeviceSelect::Unique(ctx->d_tmp, tb, W.nk1, W.nk0, W.d_small, total, s));
-    k_closest<<<icf_blocks(total, 128), 128, 0, s>>>(total, W.d_small, eb, W.nk0, ctx->d_adj_off, ctx->d_adj,
+  }
+  return icf_finish_impacts(ctx, W.nk0, total, W.d_small, eb, n_impacts);
+}
+
+// The impacts of sorted, unique keys (node << eb | element; at most `total`,
+// their count in d_n on the device): closest face of each, the comparison
+// with the list the current structure was built from, one synchronisation.
+int icf_finish_impacts(icf_ctx *ctx, const unsigned long long *keys, int total, const int *d_n, int eb,
+                       int *n_impacts) {
+  cudaStream_t s = ctx->stream;
+  icf_contact_ws &W = ctx->cws;
+  const bool cmp = ctx->n_imp_built >= 0 && ctx->imp_gen == ctx->imp_gen_built;
+  int nu = 0;
+  if (total > 0) {
+    // the impact list holds at most `total` entries
+    if (total > ctx->imp_cap) {
+      ICF_TRY_RC(grow_buf(ctx, &ctx->d_imp, 2LL * total));
+      ctx->imp_cap = 2 * total;
+      ctx->imp_gen++;
+    }
+    k_closest<<<icf_blocks(total, 128), 128, 0, s>>>(total, d_n, eb, keys, ctx->d_adj_off, ctx->d_adj,
                                                     ctx->d_faces, ctx->d_xc, ctx->d_imp);
     ICF_CUDA(ctx, cudaGetLastError());
     ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 1, 0, sizeof(int), s));
     if (cmp && ctx->imp_gen == ctx->imp_gen_built)
-      k_imp_same<<<icf_blocks(total, 256), 256, 0, s>>>(total, W.d_small, ctx->n_imp_built, ctx->d_imp,
+      k_imp_same<<<icf_blocks(total, 256), 256, 0, s>>>(total, d_n, ctx->n_imp_built, ctx->d_imp,
                                                        ctx->d_imp_built, W.d_small + 1);
-    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small, W.d_small, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small, d_n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 1, W.d_small + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     ICF_CUDA(ctx, cudaStreamSynchronize(s));
     nu = W.h_small[0];
     ctx->imp_cmp_valid = cmp && ctx->imp_gen == ctx->imp_gen_built;

@@ -141,6 +141,13 @@ struct icf_contact_ws {
   long long ncnt_cap = 0;
   unsigned long long *nk0 = nullptr, *nk1 = nullptr;
   long long nkey_cap = 0;
+  // direct contact detection: per surface element the tet inverse and first
+  // vertex (12 doubles, capacity b_cap); a dense grid of cells (counts,
+  // offsets, cursors; capacity cell_cap) and its element entries (capacity
+  // dent_cap)
+  double *tinv = nullptr;
+  int *gcnt = nullptr, *goff = nullptr, *gcur = nullptr, *gent = nullptr;
+  long long cell_cap = 0, dent_cap = 0, tinv_cap = 0;
   // small device results and their pinned host copy: [0] unique count,
   // [1] impact list differs from the built one, [2] pairs before de-duplication
   int *d_small = nullptr, *h_small = nullptr;
@@ -157,6 +164,7 @@ struct icf_solver {
   long long x_cap = 0, r_cap = 0, z_cap = 0, p_cap = 0, q_cap = 0, d_cap = 0, w_cap = 0, w2_cap = 0;
   double *part = nullptr, *sc = nullptr;
   double *h_sc = nullptr;  // pinned
+  int n_indefinite = 0;    // diagonal blocks of the last solve preconditioned by |S|^-1
 };
 
 // Parameters the kernels read, passed by value (they live in the kernel
@@ -318,6 +326,11 @@ struct icf_ctx {
   int n_pairs = 0, pairs_cap = 0;
   int *d_pairs = nullptr, *d_masks = nullptr;
   int *d_sgroup = nullptr;  // group (mesh) of every surface element, or null
+  // surface nodes (the nodes of the surface elements, ascending) and, per
+  // surface node, the surface elements holding it (ascending): the direct
+  // contact detection's queries and its pair-rule check
+  int *d_snode = nullptr, *d_sinc_off = nullptr, *d_sinc = nullptr;
+  int n_snode = 0;
   int sgroup_bits = -1;     // bits of the largest group id; -1: none set or some negative
   bool pairs_from_broad = false;
 
@@ -459,6 +472,12 @@ int icf_build_merged_pattern(icf_ctx *ctx);
 int icf_launch_assembly(icf_ctx *ctx, double h);
 int icf_launch_node_force(icf_ctx *ctx);
 int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts);
+int icf_finish_impacts(icf_ctx *ctx, const unsigned long long *keys, int total, const int *d_n, int eb,
+                       int *n_impacts);
+// broad phase, narrow phase and closest face in one, without the pair list
+// (icf_broad.cu): the impact list icf_run_narrow_phase gives on the pairs of
+// icf_broad_phase_impl with the same pad and groups
+int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_impacts);
 int icf_launch_pcsr(icf_ctx *ctx, int kind, int *d_out);
 int icf_launch_pack_nodes(icf_ctx *ctx, const double *d_un, const double *d_vn,
                           const double *d_an);

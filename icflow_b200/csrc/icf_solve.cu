@@ -6,7 +6,9 @@
 // Here the system stays where it was assembled and is solved by
 // the minimal residual method (MINRES: the matrix is symmetric but, with
 // softening cohesive zones, may be indefinite, as PARDISO's mtype -2 allows)
-// with a block-Jacobi (3x3) preconditioner:
+// with a block-Jacobi (3x3) preconditioner, positive definite as MINRES needs
+// (a row whose diagonal block is indefinite uses |S|^-1 of the block's
+// symmetric part):
 //   - A x uses the stored upper blocks directly and their transposes through
 //     a per-structure index of the lower blocks (row = column of the upper
 //     block), four lanes per row and a fixed shuffle tree, so every product
@@ -55,7 +57,62 @@ __global__ void k_lower_rows(int N, int n, const unsigned long long *__restrict_
     if (key[i] != ~0ull) lcols[i] = (int)(key[i] & 0xffffffffull);
 }
 
-// inverse of each diagonal block (the first block of its row)
+// |S|^-1 for a symmetric 3x3 block S = V diag(l) V^T: V diag(1 / |l|) V^T,
+// the eigenvalues by cyclic Jacobi rotations (Golub & Van Loan, Matrix
+// Computations, section 8.5), |l| floored at 1e-14 of the largest.  Returns
+// false when S is zero or not finite.
+__device__ bool abs_inverse_sym3(const double S[9], double *o) {
+  double a[3][3], v[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      a[i][j] = S[3 * i + j];
+      v[i][j] = i == j ? 1.0 : 0.0;
+    }
+  for (int sweep = 0; sweep < 10; sweep++) {
+    const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
+    const double dia = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
+    if (!(off > 1e-300) || off <= 1e-18 * dia) break;
+    for (int p = 0; p < 2; p++)
+      for (int q = p + 1; q < 3; q++) {
+        if (a[p][q] == 0.0) continue;
+        const double th = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+        const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+        // A <- J^T A J, V <- V J with J the rotation in the (p, q) plane
+        for (int k = 0; k < 3; k++) {
+          const double akp = a[k][p], akq = a[k][q];
+          a[k][p] = c * akp - sn * akq;
+          a[k][q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < 3; k++) {
+          const double apk = a[p][k], aqk = a[q][k];
+          a[p][k] = c * apk - sn * aqk;
+          a[q][k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < 3; k++) {
+          const double vkp = v[k][p], vkq = v[k][q];
+          v[k][p] = c * vkp - sn * vkq;
+          v[k][q] = sn * vkp + c * vkq;
+        }
+      }
+  }
+  double l[3], lmax = 0;
+  for (int i = 0; i < 3; i++) {
+    l[i] = fabs(a[i][i]);
+    lmax = fmax(lmax, l[i]);
+  }
+  if (!(lmax > 0) || !isfinite(lmax)) return false;
+  for (int i = 0; i < 3; i++) l[i] = 1.0 / fmax(l[i], 1e-14 * lmax);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) o[3 * i + j] = v[i][0] * l[0] * v[j][0] + v[i][1] * l[1] * v[j][1] + v[i][2] * l[2] * v[j][2];
+  return true;
+}
+
+// The preconditioner of each row: the inverse of its diagonal block (the
+// first block of its row) when the block is positive definite; otherwise
+// (softening cohesive zones can make it indefinite) |S|^-1 of its symmetric
+// part S, which keeps the preconditioner positive definite as MINRES needs.
+// bad: bit 0 a zero or non-finite block; count[0]: blocks replaced by |S|^-1.
 __global__ void k_dinv(int N, const int *__restrict__ rows, const double *__restrict__ vals,
                        double *__restrict__ dinv, int *__restrict__ bad) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -64,9 +121,17 @@ __global__ void k_dinv(int N, const int *__restrict__ rows, const double *__rest
   const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
   const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
   double *o = dinv + 9 * (size_t)r;
-  if (!(fabs(det) > 0) || !isfinite(det)) {
-    atomicOr(bad, 1);
-    for (int k = 0; k < 9; k++) o[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  const double m2 = a[0] * a[4] - 0.25 * (a[1] + a[3]) * (a[1] + a[3]);
+  if (!(a[0] > 0 && m2 > 0 && det > 0) || !isfinite(det)) {
+    double S[9];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) S[3 * i + j] = 0.5 * (a[3 * i + j] + a[3 * j + i]);
+    if (!abs_inverse_sym3(S, o)) {
+      atomicOr(bad, 1);
+      for (int k = 0; k < 9; k++) o[k] = (k % 4 == 0) ? 1.0 : 0.0;
+    } else {
+      atomicAdd(bad + 1, 1);
+    }
     return;
   }
   const double id = 1.0 / det;
@@ -357,11 +422,11 @@ int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, doubl
   ICF_TRY_RC(grow(ctx, &S.w2, &S.w2_cap, n3));
   ICF_TRY_RC(grow(ctx, &S.dinv, &S.d_cap, 9LL * N));
   if (!S.part) ICF_CUDA(ctx, cudaMalloc(&S.part, sizeof(double) * 2 * RED_BLOCKS));
-  if (!S.sc) ICF_CUDA(ctx, cudaMalloc(&S.sc, sizeof(double) * NSC + sizeof(int)));
+  if (!S.sc) ICF_CUDA(ctx, cudaMalloc(&S.sc, sizeof(double) * NSC + 2 * sizeof(int)));
   if (!S.h_sc) ICF_CUDA(ctx, cudaMallocHost(&S.h_sc, sizeof(double) * NSC));
   double *x = S.x, *r1 = S.r, *r2 = S.z, *y = S.p, *v = S.q;
   int *bad = reinterpret_cast<int *>(S.sc + NSC);
-  ICF_CUDA(ctx, cudaMemsetAsync(bad, 0, sizeof(int), s));
+  ICF_CUDA(ctx, cudaMemsetAsync(bad, 0, 2 * sizeof(int), s));
   k_dinv<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_rows, ctx->d_vals, S.dinv, bad);
   k_mr_start<<<icf_blocks(N, 256), 256, 0, s>>>(N, ctx->d_rhs, S.dinv, x, r1, r2, y, S.w, S.w2);
   k_dot<<<RED_BLOCKS, 256, 0, s>>>((int)n3, r1, y, S.part);
@@ -375,7 +440,7 @@ int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, doubl
     ICF_CUDA(ctx, cudaStreamSynchronize(s));
     const double phibar = S.h_sc[8], beta1 = S.h_sc[9];
     if (S.h_sc[13] != 0)
-      return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: the block-Jacobi preconditioner is not positive definite");
+      return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: breakdown (preconditioned residual norm negative or not finite)");
     rel = beta1 > 0 ? phibar / beta1 : 0.0;
     if (!std::isfinite(rel)) return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: non-finite residual");
     if (rel <= rel_tol || beta1 == 0 || it >= max_iter) break;
@@ -391,9 +456,10 @@ int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, doubl
     }
     ICF_CUDA(ctx, cudaGetLastError());
   }
-  int hbad = 0;
-  ICF_CUDA(ctx, cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost));
-  if (hbad) return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: singular diagonal block");
+  int hbad[2] = {0, 0};
+  ICF_CUDA(ctx, cudaMemcpy(hbad, bad, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+  if (hbad[0]) return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: zero or non-finite diagonal block");
+  S.n_indefinite = hbad[1];
   if (iters) *iters = it;
   if (relres) *relres = rel;
   if (rel > rel_tol && it >= max_iter)

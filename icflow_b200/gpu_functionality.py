@@ -130,21 +130,39 @@ class GPU_Functionality:
                                                        iptr(failed)))
 
     # -- broad phase on the device (replaces the host BVH, BVHT.cs:29-77) --
+    def _set_groups(self, same_mesh: bool):
+        if getattr(self, "_groups_same_mesh", None) != same_mesh:
+            grp = None if same_mesh else np.ascontiguousarray(self.mc.selem_mesh, np.int32)
+            check(self.ctx, self.lib.icf_set_surface_groups(self.ctx, len(self.mc.selem_mesh),
+                                                            iptr(grp) if grp is not None else None))
+            self._groups_same_mesh = same_mesh
+
     def BroadPhase(self, pad: float = 0.0, same_mesh: bool = True) -> int:
         """Candidate surface-element pairs with overlapping boxes at the
         current positions that share no node, as the reference's BVH lists
         them (BVHT.cs:29-77: every surface element of every mesh, so pairs of
         one mesh too); same_mesh=False keeps only pairs of different meshes.
         The pairs stay on the device for NarrowPhaseCollisionDetection(None)."""
-        if getattr(self, "_groups_same_mesh", None) != same_mesh:
-            grp = None if same_mesh else np.ascontiguousarray(self.mc.selem_mesh, np.int32)
-            check(self.ctx, self.lib.icf_set_surface_groups(self.ctx, len(self.mc.selem_mesh),
-                                                            iptr(grp) if grp is not None else None))
-            self._groups_same_mesh = same_mesh
+        self._set_groups(same_mesh)
         n = C.c_int()
         check(self.ctx, self.lib.icf_broad_phase(self.ctx, float(pad), C.byref(n)))
         self.nPairs = n.value
         return n.value
+
+    def DetectContacts(self, pad: float = 0.0, same_mesh: bool = True) -> np.ndarray:
+        """The impacts BroadPhase(pad, same_mesh) followed by
+        NarrowPhaseCollisionDetection(None) gives, found without the pair
+        list (one query per surface node in a grid of the surface elements).
+        Returns the impact list (node, face vertices) as
+        NarrowPhaseCollisionDetection does."""
+        self._set_groups(same_mesh)
+        n = C.c_int()
+        check(self.ctx, self.lib.icf_detect_contacts(self.ctx, float(pad), C.byref(n)))
+        self.nImpacts = self.cf.nCollisions = n.value
+        self.c_itet = np.zeros((n.value, 4), np.int32)
+        if n.value:
+            check(self.ctx, self.lib.icf_get_impacts(self.ctx, n.value, iptr(self.c_itet)))
+        return self.c_itet
 
     def GetPairs(self) -> np.ndarray:
         out = np.zeros((max(self.nPairs, 1), 2), np.int32)

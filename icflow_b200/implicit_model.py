@@ -19,10 +19,12 @@ Per step (ImplicitModel3.Step, :369-435):
 
 The time step is fixed: _adjustTimeStep's time-scale factor (:259-287) and the
 damage-explosion frame discard are not reproduced.  The node state, the
-contact pairs, the matrix and the Newton increment stay on the device; the
-host reads v once per step (for the guess).  broad_phase="host" swaps the
-device broad phase for the host grid generator (the tentative positions then
-cross to the host every iteration).
+contact detection, the matrix and the Newton increment stay on the device;
+the host reads v once per step (for the guess).  Contact detection is one
+device call without a pair list by default (broad_phase="device"); "pairs"
+runs the device broad phase and the narrow phase on its pair list, and
+"host" the host grid generator (the tentative positions then cross to the
+host every iteration).  All three give the same impacts.
 """
 from __future__ import annotations
 
@@ -89,8 +91,8 @@ class ImplicitModel3:
             raise ValueError("convergence is 'increment' or 'residual'")
         self.convergence = convergence
         self.res_tol = res_tol
-        if broad_phase not in ("device", "host"):
-            raise ValueError("broad_phase is 'device' or 'host'")
+        if broad_phase not in ("device", "pairs", "host"):
+            raise ValueError("broad_phase is 'device', 'pairs' or 'host'")
         self.broad_phase = broad_phase
         self.coll = coll
         self.prms = prms
@@ -177,9 +179,13 @@ class ImplicitModel3:
 
     def _contact(self):
         """Broad and narrow phase at the tentative positions: on the device
-        (pairs never leave it), or with the host grid generator."""
+        in one call without a pair list ("device"), on the device through the
+        pair list ("pairs", which never leaves the device), or with the host
+        grid generator ("host").  All three give the same impacts."""
         gf = self.gf
         if self.broad_phase == "device":
+            gf.DetectContacts()
+        elif self.broad_phase == "pairs":
             gf.BroadPhase()
             gf.NarrowPhaseCollisionDetection(None)
         else:

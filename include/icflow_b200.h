@@ -157,14 +157,25 @@ int icf_narrow_phase(icf_ctx *ctx, int n_pairs, const int *pairs,
                      int *n_impacts);
 /* Broad phase on the device (replaces the host k-DOP BVH, BVHT.cs:29-77,
  * BVHN.cs:39-194, whose element-pair list NarrowPhaseCollisionDetection
- * receives): surface-element pairs a < b of different groups whose
- * axis-aligned boxes at the current positions, widened by pad, overlap.
- * Groups (e.g. the mesh of each surface element) come from
- * icf_set_surface_groups; without them every pair qualifies.  The pairs stay
- * on the device: icf_narrow_phase(ctx, -1, NULL, &n) uses them; icf_get_pairs
- * copies them out (pairs[n*2], ascending). */
+ * receives): surface-element pairs a < b whose axis-aligned boxes at the
+ * current positions, widened by pad, overlap, that share no node and where a
+ * vertex of one lies in the other's box; with groups (e.g. the mesh of each
+ * surface element, icf_set_surface_groups) only pairs of different groups.
+ * Like the reference's tree, which holds every surface element of every
+ * mesh, pairs of one mesh qualify by default.  The pairs stay on the device:
+ * icf_narrow_phase(ctx, -1, NULL, &n) uses them; icf_get_pairs copies them
+ * out (pairs[n*2], ascending). */
 int icf_set_surface_groups(icf_ctx *ctx, int n_surface, const int *group);
 int icf_broad_phase(icf_ctx *ctx, double pad, int *n_pairs);
+/* Broad phase, narrow phase and closest face in one call, without the pair
+ * list (no reference counterpart; it stands for BVH self-collision +
+ * kNarrowPhase_new + the set expansion + kFindClosestFace,
+ * GPU_Functionality.cs:539-616): the impact list is the one
+ * icf_broad_phase(ctx, pad) followed by icf_narrow_phase(ctx, -1, NULL, ...)
+ * gives, found by one query per surface node in a grid of the surface
+ * elements.  The pair list and the narrow-phase masks are left as they were.
+ * Requires CollisionScheme != 0 (with 0 the list is empty). */
+int icf_detect_contacts(icf_ctx *ctx, double pad, int *n_impacts);
 int icf_get_pairs(icf_ctx *ctx, int capacity, int *pairs);
 /* impacts[n*4] = (node, face vertex 0, 1, 2), the c_itet rows of :611. */
 int icf_get_impacts(icf_ctx *ctx, int capacity, int *impacts);
@@ -317,11 +328,13 @@ int icf_add_dx(icf_ctx *ctx, const double *dx, double *norm);
  * (LinearSystem.cs:48-64, MKL PARDISO on the host, after the D2H of
  * :481-485).  Solves A dx = rhs for the matrix and rhs of the last assembly
  * (A symmetric, stored as its upper blocks, possibly indefinite as PARDISO's
- * mtype -2 allows) by MINRES with a 3x3 block-Jacobi preconditioner, until the
- * preconditioned residual is at most rel_tol times its initial value.
- * dx[N*3] (nullable) receives the solution, which also stays on the device
- * for icf_apply_dx.  ICF_ERR_NUMERIC if it does not converge in max_iter
- * iterations or the block-Jacobi preconditioner is not positive definite. */
+ * mtype -2 allows) by MINRES with a 3x3 block-Jacobi preconditioner (a row
+ * whose diagonal block is not positive definite is preconditioned by |S|^-1 of
+ * the block's symmetric part S), until the preconditioned residual is at most
+ * rel_tol times its initial value.  dx[N*3] (nullable) receives the solution,
+ * which also stays on the device for icf_apply_dx.  ICF_ERR_NUMERIC if it does
+ * not converge in max_iter iterations, a diagonal block is zero or not finite,
+ * or the recurrence breaks down. */
 int icf_solve(icf_ctx *ctx, double rel_tol, int max_iter, double *dx, int *iters, double *relres);
 /* Sum of squares of the rhs of the last assembly (the Newton residual norm,
  * squared).  No counterpart in the reference, whose convergence test is on

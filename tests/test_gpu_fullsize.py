@@ -7,8 +7,8 @@ autotuner picks (as bench.py does), and compare with the CPU oracle:
 
   cfg1  polycrystal compression, 196,608 tets, 34,819 CZs, ~22,700 impacts
         (platens and grain boundaries): the device broad phase's pair set
-        equals the host rule's; masks, impacts, csr_rows/cols and every slot
-        map bit-exact; blocks
+        equals the host rule's; masks, impacts (also from the detection
+        without a pair list), csr_rows/cols and every slot map bit-exact; blocks
         within 1e-12 per block row; rhs within 1e-12; CZ flags equal;
         tentative state and averages within 1e-12.
   cfg2  the same at 1,572,864 tets in FP64 (same bar), then in FP32-mixed with
@@ -116,6 +116,8 @@ def test_cfg1_bench_workload_parity():
     assert len(imps) > 1000 and np.array_equal(gf.c_itet, imps)
     rep = compare(g, o)
     assert g["counts"].nImpacts == len(imps) and g["counts"].nLawExact == 0
+    # contact detection without the pair list: the same impacts
+    assert np.array_equal(gf.DetectContacts(), imps)
     gf.close()
     print("cfg1 parity:", {k: f"{v:.1e}" for k, v in rep.items()})
 
@@ -131,6 +133,7 @@ def test_cfg2_bench_workload_fp64_parity_and_mixed_error():
     assert np.array_equal(gf.NarrowPhaseMasks(len(pairs)), masks)
     assert np.array_equal(gf.c_itet, imps)
     rep = compare(g, o)
+    assert np.array_equal(gf.DetectContacts(), imps)
     print("cfg2 FP64 parity:", {k: f"{v:.1e}" for k, v in rep.items()})
     gf.SetPrecision(1)
     g32 = _gpu(gf, coll, state, pairs, tune=True)

@@ -476,6 +476,52 @@ def test_device_broad_phase_matches_host_pairs(O):
         gf.close()
 
 
+def test_detect_contacts_matches_the_pair_pipeline(O):
+    """icf_detect_contacts (one query per surface node in a grid of the
+    surface elements, no pair list) gives the impact list of the device broad
+    phase + narrow phase + closest face, entry for entry: platen contact at
+    several gaps, rotated meshes, a widened box (pad), groups (also with a
+    negative group id), and two ice blocks driven into each other."""
+    from icflow_b200 import _lib
+
+    cases = [("poly", 1, -0.3, None, 0.0), ("poly", 2, -0.05, _rot([1, 1, 0], 35), 0.0),
+             ("poly", 3, 0.2, None, 0.0), ("poly", 4, -0.25, _rot([1, 0, 2], 60), 2e-3), ("ice", 5, 0, None, 0.0)]
+    for kind, seed, gap, R, pad in cases:
+        if kind == "poly":
+            coll = M.polycrystal(n=7, grains=5, seed=seed, platens=True, gap=gap)
+            if R is not None:
+                coll = _rotate(coll, R)
+            un, vn, an = random_state(coll, seed, du=3e-6)
+        else:
+            coll, _ = M.ice_impact(n=6, grains=6, seed=seed, size=(0.02, 0.02, 0.01))
+            un, vn, an = random_state(coll, seed, du=1e-6)
+            na = coll.meshes[0].n_nodes
+            un[:na, 2] += 2e-4  # block A driven 0.1 mm into block B
+        gf = _gf(coll, config_prms(penaltyK=1e8))
+        gf.TransferNodesToGPU(un, vn, an)
+        for same_mesh in (True, False):
+            gf.BroadPhase(pad=pad, same_mesh=same_mesh)
+            ref = gf.NarrowPhaseCollisionDetection(None).copy()
+            det = gf.DetectContacts(pad=pad, same_mesh=same_mesh).copy()
+            assert np.array_equal(det, ref), (kind, seed, same_mesh, len(det), len(ref))
+            if same_mesh:
+                n_same = len(ref)
+        assert n_same > 0 or gap > 0, (kind, seed)
+        # a negative group id
+        grp = np.ascontiguousarray(coll.selem_mesh, np.int32) - 1
+        _lib.check(gf.ctx, gf.lib.icf_set_surface_groups(gf.ctx, len(grp), _lib.iptr(grp)))
+        n2 = C.c_int()
+        _lib.check(gf.ctx, gf.lib.icf_broad_phase(gf.ctx, pad, C.byref(n2)))
+        ref = gf.NarrowPhaseCollisionDetection(None).copy()
+        _lib.check(gf.ctx, gf.lib.icf_detect_contacts(gf.ctx, pad, C.byref(n2)))
+        det = np.zeros((n2.value, 4), np.int32)
+        if n2.value:
+            _lib.check(gf.ctx, gf.lib.icf_get_impacts(gf.ctx, n2.value, _lib.iptr(det)))
+        assert np.array_equal(det, ref), (kind, seed, "negative groups")
+        print(f"{kind} seed {seed}: {n_same} impacts (all meshes), equal to the pair pipeline")
+        gf.close()
+
+
 def _rotate(coll, R, mesh=None):
     """A copy of the collection with the nodes of one mesh (all meshes when
     None) rotated by R about that part's centroid."""
@@ -545,6 +591,7 @@ def test_broad_phase_covers_the_reference_kdop_pairs(O):
         imp_ref = O.impacts(kd, masks, coll.selem, coll.adj_off, coll.adj, coll.faces, xt)
         assert len(imp_ref) > 0, seed
         assert np.array_equal(imp_dev, imp_ref), (seed, len(imp_dev), len(imp_ref))
+        assert np.array_equal(gf.DetectContacts(), imp_ref), seed
         print(f"seed {seed}: device pairs {n_dev}, k-DOP pairs {len(kd)} ({len(cross)} across meshes, "
               f"{len(can)} that can give an impact), impacts {len(imp_ref)}")
         gf.close()
