@@ -129,6 +129,7 @@ SIGNATURES = {
     "icf_set_surface_groups": (I, [P, I, P]),
     "icf_broad_phase": (I, [P, D, C.POINTER(C.c_int)]),
     "icf_detect_contacts": (I, [P, D, C.POINTER(C.c_int)]),
+    "icf_count_damaged": (I, [P, C.POINTER(C.c_int)]),
     "icf_get_pairs": (I, [P, I, P]),
     "icf_mlp_create": (I, [I, C.POINTER(P)]),
     "icf_mlp_destroy": (I, [P]),

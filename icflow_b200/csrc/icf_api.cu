@@ -630,6 +630,19 @@ int icf_broad_phase(icf_ctx *ctx, double pad, int *n_pairs) {
   return ICF_OK;
 }
 
+int icf_count_damaged(icf_ctx *ctx, int *n_damaged) {
+  ICF_CHECK_CTX(ctx);
+  if (!ctx->have_prm || !ctx->have_static) return icf_fail(ctx, ICF_ERR_STATE, "constants and static data first");
+  if (!n_damaged) return icf_fail(ctx, ICF_ERR_ARG, "n_damaged required");
+  ICF_CUDA(ctx, cudaSetDevice(ctx->device));
+  icf_contact_ws &W = ctx->cws;
+  if (!W.d_small) ICF_CUDA(ctx, cudaMalloc(&W.d_small, 8 * sizeof(int)));
+  ICF_TRY(icf_launch_count_damaged(ctx, W.d_small + 7));
+  ICF_CUDA(ctx, cudaMemcpyAsync(n_damaged, W.d_small + 7, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  ICF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ICF_OK;
+}
+
 int icf_detect_contacts(icf_ctx *ctx, double pad, int *n_impacts) {
   ICF_CHECK_CTX(ctx);
   if (!ctx->have_static || !ctx->have_nodes) return icf_fail(ctx, ICF_ERR_STATE, "static data and node state first");

@@ -604,7 +604,30 @@ __global__ void k_commit_cz(int nc, const double *__restrict__ tent,
   }
 }
 
+// Non-failed committed CZs damaged at the level of _acceptFrame
+// (ImplicitModel3.cs:304-317, CZ.damagedAtLevel, CZ.cs:13-16): pmax of the
+// first Gauss point above deln lambda_n or tmax above delt lambda_t (per-CZ
+// lengths with per-CZ strengths).
+__global__ void k_count_damaged(int nc, const double *__restrict__ czs, const int *__restrict__ fail,
+                                const double4 *__restrict__ czprm, double lambda_n, double lambda_t, double deln,
+                                double delt, int *__restrict__ count) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc || fail[c]) return;
+  const double dn = czprm ? czprm[c].z : deln, dt = czprm ? czprm[c].w : delt;
+  if (czs[8 * (size_t)c] > dn * lambda_n || czs[8 * (size_t)c + 3] > dt * lambda_t) atomicAdd(count, 1);
+}
+
 }  // namespace
+
+int icf_launch_count_damaged(icf_ctx *ctx, int *d_count) {
+  ICF_CUDA(ctx, cudaMemsetAsync(d_count, 0, sizeof(int), ctx->stream));
+  if (ctx->n_cz == 0) return ICF_OK;
+  k_count_damaged<<<icf_blocks(ctx->n_cz, 256), 256, 0, ctx->stream>>>(
+      ctx->n_cz, ctx->d_czs, ctx->d_czfail, ctx->per_cz_prm ? ctx->d_czprm : nullptr, ctx->prm.lambda_n,
+      ctx->prm.lambda_t, ctx->prm.deln, ctx->prm.delt, d_count);
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
 
 namespace {
 // Contribution layout (ICF_LAYOUT_CONTRIB): besides the compact rhs records

@@ -472,6 +472,7 @@ int icf_build_merged_pattern(icf_ctx *ctx);
 int icf_launch_assembly(icf_ctx *ctx, double h);
 int icf_launch_node_force(icf_ctx *ctx);
 int icf_run_narrow_phase(icf_ctx *ctx, int n_pairs, int *n_impacts);
+int icf_launch_count_damaged(icf_ctx *ctx, int *d_count);
 int icf_finish_impacts(icf_ctx *ctx, const unsigned long long *keys, int total, const int *d_n, int eb,
                        int *n_impacts);
 // broad phase, narrow phase and closest face in one, without the pair list

@@ -271,6 +271,13 @@ class GPU_Functionality:
                                                             dptr(avg), dptr(F)))
         return dict(pmax=pmax[:nc], tmax=tmax[:nc], failed=failed[:nc], avg=avg[:nc], nodeF=F)
 
+    def CountDamagedCZs(self) -> int:
+        """Non-failed committed CZs damaged at the level _acceptFrame counts
+        (ImplicitModel3.cs:304-317): the accepted frame's nCZDamaged."""
+        n = C.c_int()
+        check(self.ctx, self.lib.icf_count_damaged(self.ctx, C.byref(n)))
+        return n.value
+
     def GetCZTentative(self):
         nc = self.cf.nCZ
         tent = np.zeros((max(nc, 1), 2))

@@ -167,6 +167,13 @@ int icf_narrow_phase(icf_ctx *ctx, int n_pairs, const int *pairs,
  * out (pairs[n*2], ascending). */
 int icf_set_surface_groups(icf_ctx *ctx, int n_surface, const int *group);
 int icf_broad_phase(icf_ctx *ctx, double pad, int *n_pairs);
+/* Non-failed CZs of the committed state damaged at the level _acceptFrame
+ * counts (ImplicitModel3.cs:304-317 with CZ.damagedAtLevel, CZ.cs:13-16):
+ * pmax of the first Gauss point above deln * lambda_n or tmax above
+ * delt * lambda_t (per-CZ deln, delt with per-CZ strengths).  The accepted
+ * frame's nCZDamaged, against which _checkDamage measures a step's new
+ * damage. */
+int icf_count_damaged(icf_ctx *ctx, int *n_damaged);
 /* Broad phase, narrow phase and closest face in one call, without the pair
  * list (no reference counterpart; it stands for BVH self-collision +
  * kNarrowPhase_new + the set expansion + kFindClosestFace,

@@ -95,20 +95,23 @@ def test_learned_warm_start_reduces_newton_iterations():
     p.maxIterations = 20
     ws = LearnedWarmStart(seed=0)
     for rate in (0.015, 0.02, 0.03):
-        g = ImplicitModel3(fast_cantilever(rate), p, convergence="residual", res_tol=1e-8)
+        g = ImplicitModel3(fast_cantilever(rate), p, convergence="residual", res_tol=1e-8,
+                           step_control=False)
         g.recorder = ws
         for _ in range(40):
             assert g.Step().converged
         g.close()
     loss = ws.fit_residual(epochs=40, lr=3e-4)
-    cal = ImplicitModel3(fast_cantilever(0.022), p, convergence="residual", res_tol=1e-8)
+    cal = ImplicitModel3(fast_cantilever(0.022), p, convergence="residual", res_tol=1e-8,
+                           step_control=False)
     for _ in range(3):
         cal.Step()
     by_gain = ws.calibrate(cal, 12)
     cal.close()
     its = {}
     for name, warm in (("plain", None), ("learned", ws)):
-        m = ImplicitModel3(fast_cantilever(0.025), p, convergence="residual", res_tol=1e-8)
+        m = ImplicitModel3(fast_cantilever(0.025), p, convergence="residual", res_tol=1e-8,
+                           step_control=False)
         for _ in range(40):
             s = m.Step(warm_start=warm)
             assert s.converged
