@@ -958,7 +958,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
     icf_prof_mark(ctx, s, "k_imp_add", imp_in * n_a / ctx->n_crs + 144LL * n_a);
   }
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
-  if (ctx->n_crs_off > 0) {
+  if (ctx->n_crs_off > 0 && ctx->n_crs > 0) {
     k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(
         ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
         ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 2);

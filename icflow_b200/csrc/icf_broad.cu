@@ -261,95 +261,81 @@ __global__ void k_red7_final(int nb, int n, const double *__restrict__ part, dou
 // ---- contact detection without the pair list ------------------------------------
 // A pair (a, b) gives the impact (p, b) when p is a node of a, the narrow
 // phase finds p strictly inside b, and (a, b) satisfies the pair rule.  So
-// the impact list follows from one query per surface node p: the surface
-// elements b whose boxes hold p (the grid cell of p lists them all, a box
-// being entered in every cell it reaches), p not a node of b, p inside b
-// (tet_contains with b's inverse, the same bits as in k_narrow), and some
+// the impact list follows from one query per surface element b: the surface
+// nodes p inside b's box (a grid of the surface nodes; b's box reaches every
+// cell that can hold one), p not a node of b, p inside b (tet_contains with
+// b's inverse, computed as k_narrow computes it, so the same bits), and some
 // surface element a holding p with keep_pair(a, b).  Every (p, b) is found
 // once (p lies in one cell).  tet_contains needs the barycentric coordinates
-// above 1e-10, so p is then strictly inside b's box.
-
-// per surface element: the inverse of its edge matrix and its first vertex
-__global__ void k_tet_inv(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
-                          double *__restrict__ inv) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int4 id = selem[i];
-  const int nn[4] = {id.x, id.y, id.z, id.w};
-  double x[12];
-  for (int k = 0; k < 4; k++) {
-    const double4 p = xc[nn[k]];
-    x[3 * k] = p.x; x[3 * k + 1] = p.y; x[3 * k + 2] = p.z;
-  }
-  double b[9];
-  tet_inverse(x, b);
-  double *o = inv + 12 * (size_t)i;
-  for (int k = 0; k < 9; k++) o[k] = b[k];
-  o[9] = x[0]; o[10] = x[1]; o[11] = x[2];
-}
+// above 1e-10, so such a p is strictly inside b's box.
 
 __device__ __forceinline__ long long cell_lin(int x, int y, int z, int ny, int nz) {
   return ((long long)x * ny + y) * nz + z;
 }
 
-// count (off == nullptr) or place every (cell, element) entry of the dense grid
-__global__ void k_grid_put(int n, const int4 *__restrict__ clo, int ny, int nz, int *__restrict__ cnt,
-                           const int *__restrict__ off, int *__restrict__ ent, long long cap) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int4 c = clo[i];
+// count (off == nullptr) or place the surface nodes in the dense grid
+__global__ void k_node_put(int ns, const int *__restrict__ snode, const double4 *__restrict__ xc,
+                           const double *__restrict__ red, int nx, int ny, int nz, int *__restrict__ cnt,
+                           const int *__restrict__ off, double4 *__restrict__ ent) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  const double4 P = xc[snode[k]];
+  const double cell = red[0];
+  const int cx = cell_of(P.x, red[1], cell), cy = cell_of(P.y, red[2], cell), cz = cell_of(P.z, red[3], cell);
+  // a node outside the grid is in no box (the grid spans every box)
+  if (cx < 0 || cy < 0 || cz < 0 || cx >= nx || cy >= ny || cz >= nz) return;
+  const long long l = cell_lin(cx, cy, cz, ny, nz);
+  const int w = atomicAdd(cnt + l, 1);
+  if (off) ent[off[l] + w] = make_double4(P.x, P.y, P.z, (double)k);
+}
+
+// one thread per surface element b: keys node << eb | b of its impacts
+__global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
+                                                const double *__restrict__ lohi, const int4 *__restrict__ clo,
+                                                int ny, int nz, const int *__restrict__ goff,
+                                                const double4 *__restrict__ gnode, const int *__restrict__ snode,
+                                                const int *__restrict__ sinc_off, const int *__restrict__ sinc,
+                                                const int *__restrict__ group, int eb,
+                                                unsigned long long *__restrict__ out, long long cap,
+                                                int *__restrict__ count) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const int4 B = selem[b];
+  const int nb[4] = {B.x, B.y, B.z, B.w};
+  double x[12];
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const double4 q = xc[nb[v]];
+    x[3 * v] = q.x; x[3 * v + 1] = q.y; x[3 * v + 2] = q.z;
+  }
+  double bi[9];
+  tet_inverse(x, bi);
+  const double *lh = lohi + 6 * (size_t)b;
+  const double lx = lh[0], ly = lh[1], lz = lh[2], hx = lh[3], hy = lh[4], hz = lh[5];
+  const int4 c = clo[b];
   const int sx = c.w & 1023, sy = (c.w >> 10) & 1023, sz = (c.w >> 20) & 1023;
   for (int dx = 0; dx <= sx; dx++)
     for (int dy = 0; dy <= sy; dy++)
       for (int dz = 0; dz <= sz; dz++) {
         const long long l = cell_lin(c.x + dx, c.y + dy, c.z + dz, ny, nz);
-        const int k = atomicAdd(cnt + l, 1);
-        if (off) {
-          const long long pos = (long long)off[l] + k;
-          if (pos < cap) ent[pos] = i;
+        const int e1 = goff[l + 1];
+        for (int e = goff[l]; e < e1; e++) {
+          const double4 P = gnode[e];
+          if (!(P.x >= lx && P.x <= hx && P.y >= ly && P.y <= hy && P.z >= lz && P.z <= hz)) continue;
+          const int k = (int)P.w;
+          const int p = snode[k];
+          if (p == nb[0] || p == nb[1] || p == nb[2] || p == nb[3]) continue;
+          if (!tet_contains(bi, P.x - x[0], P.y - x[1], P.z - x[2])) continue;
+          bool any = false;
+          for (int j = sinc_off[k]; j < sinc_off[k + 1] && !any; j++) {
+            const int a = sinc[j];
+            any = keep_pair(a < b ? a : b, a < b ? b : a, lohi, group, selem, xc);
+          }
+          if (!any) continue;
+          const int w = atomicAdd(count, 1);
+          if (w < cap) out[w] = ((unsigned long long)(unsigned)p << eb) | (unsigned)b;
         }
       }
-}
-
-// one thread per surface node: keys node << eb | element of its impacts
-__global__ void __launch_bounds__(128) k_detect(int ns, const int *__restrict__ snode, const int *__restrict__ sinc_off,
-                                                const int *__restrict__ sinc, const double4 *__restrict__ xc,
-                                                const double *__restrict__ red, int nx, int ny, int nz,
-                                                const int *__restrict__ goff, const int *__restrict__ gent,
-                                                long long ent_cap, const double *__restrict__ lohi,
-                                                const double *__restrict__ inv, const int4 *__restrict__ selem,
-                                                const int *__restrict__ group, int eb,
-                                                unsigned long long *__restrict__ out, long long cap,
-                                                int *__restrict__ count) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ns) return;
-  const int p = snode[k];
-  const double4 P = xc[p];
-  const double cell = red[0];
-  const int cx = cell_of(P.x, red[1], cell), cy = cell_of(P.y, red[2], cell), cz = cell_of(P.z, red[3], cell);
-  if (cx < 0 || cy < 0 || cz < 0 || cx >= nx || cy >= ny || cz >= nz) return;
-  const long long l = cell_lin(cx, cy, cz, ny, nz);
-  const long long e0 = goff[l], e1 = min((long long)goff[l + 1], ent_cap);
-  for (long long e = e0; e < e1; e++) {
-    const int b = gent[e];
-    const double *lh = lohi + 6 * (size_t)b;
-    if (!(P.x >= lh[0] && P.x <= lh[3] && P.y >= lh[1] && P.y <= lh[4] && P.z >= lh[2] && P.z <= lh[5])) continue;
-    const int4 B = selem[b];
-    if (B.x == p || B.y == p || B.z == p || B.w == p) continue;
-    const double *q = inv + 12 * (size_t)b;
-    double bi[9];
-#pragma unroll
-    for (int t = 0; t < 9; t++) bi[t] = q[t];
-    if (!tet_contains(bi, P.x - q[9], P.y - q[10], P.z - q[11])) continue;
-    bool any = false;
-    for (int j = sinc_off[k]; j < sinc_off[k + 1] && !any; j++) {
-      const int a = sinc[j];
-      any = keep_pair(a < b ? a : b, a < b ? b : a, lohi, group, selem, xc);
-    }
-    if (!any) continue;
-    const int w = atomicAdd(count, 1);
-    if (w < cap) out[w] = ((unsigned long long)(unsigned)p << eb) | (unsigned)b;
-  }
 }
 
 }  // namespace
@@ -365,7 +351,7 @@ static int grow(icf_ctx *ctx, T **p, long long n) {
 void icf_free_contact_ws(icf_ctx *ctx) {
   icf_contact_ws &W = ctx->cws;
   void *d[] = {W.lohi, W.ext, W.tmpv, W.red, W.bcnt, W.boff, W.clo, W.ek0, W.ek1, W.ee0, W.ee1, W.pc, W.po,
-               W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small, W.tinv, W.gcnt, W.goff, W.gcur, W.gent};
+               W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small, W.gcnt, W.goff, W.gcur, W.gnode};
   for (void *q : d) cudaFree(q);
   cudaFreeHost(W.h_small);
   cudaFreeHost(W.h_red);
@@ -501,18 +487,18 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
 }
 
 // Contact detection without the pair list.  Three synchronisations: the grid
-// (cell size and corners, which set the grid's dimensions), the entry and hit
-// counts (to grow the buffers and repeat when they overflow), and the impact
-// list's count in icf_finish_impacts.  The grid is dense: if the boxes' hull
-// holds more than 8 cells per surface element at the mean box extent, the
-// cell grows until it holds at most that many.
+// (cell size and corners, which set the grid's dimensions), the hit count (to
+// grow the key buffer and repeat when it overflows), and the impact list's
+// count in icf_finish_impacts.  The grid is dense: if the boxes' hull holds
+// more than 8 cells per surface element at the mean box extent, the cell
+// grows until it holds at most that many.
 int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_impacts) {
   cudaStream_t s = ctx->stream;
-  const int n = ctx->n_surf;
+  const int n = ctx->n_surf, ns = ctx->n_snode;
   icf_contact_ws &W = ctx->cws;
   *n_impacts = 0;
   ctx->imp_cmp_valid = false;
-  if (n < 2 || ctx->n_snode == 0) {
+  if (n < 2 || ns == 0) {
     ctx->n_imp = 0;
     return ICF_OK;
   }
@@ -526,16 +512,15 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     ICF_TRY_RC(grow(ctx, &W.clo, n));
     W.b_cap = n;
   }
-  if (n > W.tinv_cap) {
-    ICF_TRY_RC(grow(ctx, &W.tinv, 12LL * n));
-    W.tinv_cap = n;
+  if (ns > W.gnode_cap) {
+    ICF_TRY_RC(grow(ctx, &W.gnode, ns));
+    W.gnode_cap = ns;
   }
   if (!W.tmpv) ICF_TRY_RC(grow(ctx, &W.tmpv, 8LL * (2 * ctx->n_sm + 1)));
   if (!W.red) ICF_TRY_RC(grow(ctx, &W.red, 8));
   k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext);
   k_red7<<<nbk, 256, 0, s>>>(n, W.lohi, W.ext, W.tmpv);
   k_red7_final<<<1, 256, 0, s>>>(nbk, n, W.tmpv, W.red);
-  k_tet_inv<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.tinv);
   ICF_CUDA(ctx, cudaMemcpyAsync(W.h_red, W.red, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaStreamSynchronize(s));
   double *h_red = W.h_red;
@@ -546,7 +531,7 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     C = 1;
     for (int k = 0; k < 3; k++) {
       const double span = (h_red[4 + k] - h_red[1 + k]) / cell;
-      dims[k] = std::isfinite(span) ? (long long)span + 2 : (1LL << 40);
+      dims[k] = (std::isfinite(span) && span < 1e12) ? (long long)span + 2 : (1LL << 40);
       C = (dims[k] > (1LL << 40) / std::max(C, 1LL)) ? (1LL << 40) : C * dims[k];
     }
     if (C <= 8LL * n + 4096) break;
@@ -565,55 +550,44 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     ICF_TRY_RC(grow(ctx, &W.gcur, C + 1));
     W.cell_cap = C + 1;
   }
-  if (W.dent_cap == 0) {
-    ICF_TRY_RC(grow(ctx, &W.gent, 8LL * n + 1024));
-    W.dent_cap = 8LL * n + 1024;
-  }
   if (W.nkey_cap == 0) {
     const long long c = std::max<long long>(n / 4, 1024);
     ICF_TRY_RC(grow(ctx, &W.nk0, c));
     ICF_TRY_RC(grow(ctx, &W.nk1, c));
     W.nkey_cap = c;
   }
-  k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
+  // the surface nodes by cell
   ICF_CUDA(ctx, cudaMemsetAsync(W.gcnt, 0, sizeof(int) * (size_t)(C + 1), s));
-  k_grid_put<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.clo, ny, nz, W.gcnt, nullptr, nullptr, 0);
+  ICF_CUDA(ctx, cudaMemsetAsync(W.gcur, 0, sizeof(int) * (size_t)(C + 1), s));
+  k_node_put<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, ctx->d_snode, ctx->d_xc, W.red, nx, ny, nz, W.gcnt, nullptr,
+                                                 nullptr);
   size_t tb = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb, W.gcnt, W.goff, (int)(C + 1), s);
   if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
   ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.gcnt, W.goff, (int)(C + 1), s));
+  k_node_put<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, ctx->d_snode, ctx->d_xc, W.red, nx, ny, nz, W.gcur, W.goff,
+                                                 W.gnode);
+  // every element's cells
+  k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
   int eb = 1, vb = 1;
   while ((1LL << eb) < (long long)n) eb++;
   while ((1LL << vb) < (long long)ctx->n_nodes) vb++;
   int hits = 0;
-  for (int attempt = 0; attempt < 3; attempt++) {
-    ICF_CUDA(ctx, cudaMemsetAsync(W.gcur, 0, sizeof(int) * (size_t)(C + 1), s));
+  for (int attempt = 0; attempt < 2; attempt++) {
     ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, sizeof(int), s));
-    k_grid_put<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.clo, ny, nz, W.gcur, W.goff, W.gent, W.dent_cap);
-    k_detect<<<icf_blocks(ctx->n_snode, 128), 128, 0, s>>>(
-        ctx->n_snode, ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, ctx->d_xc, W.red, nx, ny, nz, W.goff, W.gent,
-        W.dent_cap, W.lohi, W.tinv, ctx->d_selem, d_group, eb, W.nk0, W.nkey_cap, W.d_small + 5);
+    k_detect<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, ny, nz, W.goff, W.gnode,
+                                               ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, d_group, eb, W.nk0,
+                                               W.nkey_cap, W.d_small + 5);
     ICF_CUDA(ctx, cudaGetLastError());
     ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 5, W.d_small + 5, sizeof(int), cudaMemcpyDeviceToHost, s));
-    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 6, W.goff + C, sizeof(int), cudaMemcpyDeviceToHost, s));
     ICF_CUDA(ctx, cudaStreamSynchronize(s));
     hits = W.h_small[5];
-    const long long m = W.h_small[6];
-    bool again = false;
-    if (m > W.dent_cap) {
-      ICF_TRY_RC(grow(ctx, &W.gent, m + m / 4 + 1024));
-      W.dent_cap = m + m / 4 + 1024;
-      again = true;
-    }
-    if (hits > W.nkey_cap) {
-      const long long c = hits + hits / 4 + 1024;
-      ICF_TRY_RC(grow(ctx, &W.nk0, c));
-      ICF_TRY_RC(grow(ctx, &W.nk1, c));
-      W.nkey_cap = c;
-      again = true;
-    }
-    if (!again) break;
-    if (attempt == 2) return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: buffer growth did not converge");
+    if (hits <= W.nkey_cap) break;
+    if (attempt == 1) return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: key buffer growth did not converge");
+    const long long c = hits + hits / 4 + 1024;
+    ICF_TRY_RC(grow(ctx, &W.nk0, c));
+    ICF_TRY_RC(grow(ctx, &W.nk1, c));
+    W.nkey_cap = c;
   }
   if (hits > 0) {
     tb = 0;

@@ -6,81 +6,49 @@
 //   vertex region  d2 = |p - v|^2
 //   edge region    d2 = f1 - g / f2,  f1 = |q1-p|^2, g = ((q1-p).(q2-q1))^2,
 //                  f2 = |q2-q1|^2   (point_triange_v2.h:152-232)
-//   interior       d2 = |q|^2, q = s v1 + t v2 + (1-s-t) v0 - p with the
-//                  barycentrics s(x), t(x) of the foot point
+//   interior       the squared distance to the triangle's plane
 //                  (point_plane_distance, :449-582)
-// The 32 lanes of a warp share the per-impact setup through shared memory and
-// each evaluates 2-3 of the 78 entries of the symmetric Hessian (:111-114).
-// K = k/2 d2'' goes straight to the records of the impact's contribution
-// codes, at their positions in the slot-sorted list (icf_internal.cuh,
-// ICF_IMP_REC): the 3x3 block of each code's vertex pair, and, on the
-// diagonal codes, the vertex's rhs from (-F, w0 F, w1 F, w2 F),
-// F = k/2 d(d2)/dp, w = (1-s-t, s, t); the four vertex forces also go to a
-// per-impact force record (for the node forces).
+// In the interior the reference differentiates d2 = |q|^2 through the
+// barycentrics s(x), t(x) of the foot point.  The same function is
+// d2 = D^2 / S with D = a . N, S = N . N, N = e0 x e1, a = p - v0,
+// e0 = v1 - v0, e1 = v2 - v0, whose Hessian has the closed form
+//   H = 2 gD gD^T / S + 2 D HD / S - 2 D (gD gS^T + gS gD^T) / S^2
+//       - D^2 HS / S^2 + 2 D^2 gS gS^T / S^3,
+// gD, gS the gradients and HD, HS the Hessians of D and S: HD is a
+// cross-product matrix per vertex-block pair (D is trilinear in a, e0, e1),
+// HS follows from S = |e0|^2 |e1|^2 - (e0.e1)^2.  About 40 operations per
+// entry instead of some 200; the two forms agree to rounding (1e-14 of the
+// largest entry on random interior cases).
+//
+// The 32 lanes of a warp share the per-impact setup through shared memory.
+// The Hessian K = k/2 d2'' goes straight to the records of the impact's
+// contribution codes, at their positions in the slot-sorted list
+// (icf_internal.cuh, ICF_IMP_REC): a lane per record entry (10 vertex pairs x
+// 9 entries), each written once; a diagonal block's lower entries are
+// evaluated at (column, row), so the block is symmetric bit for bit.  On the
+// diagonal codes the record also carries the vertex's rhs from (-F, w0 F,
+// w1 F, w2 F), F = k/2 d(d2)/dp, w = (1-s-t, s, t); the four vertex forces
+// also go to a per-impact force record (for the node forces).
 #include "icf_internal.cuh"
 
 namespace {
 
 constexpr int WARPS = 4;
 
-// sign of block b in the selectors e0 = v1 - v0, e1 = v2 - v0, w = v0 - p
-__device__ __forceinline__ double sgE0(int b) { return b == 2 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
-__device__ __forceinline__ double sgE1(int b) { return b == 3 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
-__device__ __forceinline__ double sgW(int b) { return b == 1 ? 1.0 : (b == 0 ? -1.0 : 0.0); }
+// coefficients of vertex block b (p, v0, v1, v2) in a = p - v0,
+// e0 = v1 - v0, e1 = v2 - v0
+__device__ __forceinline__ double cA(int b) { return b == 0 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
+__device__ __forceinline__ double cE0(int b) { return b == 2 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
+__device__ __forceinline__ double cE1(int b) { return b == 3 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
 
 struct PlaneSetup {
-  double a, b, c, d, e, det, s, t, u, idet, idet2, idet3, sN, tN;
-  double V[3][3];  // v0, v1, v2
-  double q[3];
-  double ag[12], bg[12], cg[12], dg[12], eg[12], det1[12], s1[12], t1[12], u1[12];
-  double J[3][12];
+  double gD[12], gS[12];
 };
 
 struct LineSetup {
   double sp, g, f2, f2sq, f2cu;
   double spd[9], gd[9], f1d[9], f2d[9];
 };
-
-__device__ double plane_entry(const PlaneSetup &S, int i, int j) {
-  const bool same = (i % 3) == (j % 3);
-  const int bi = i / 3, bj = j / 3;
-  double a2 = 0, b2 = 0, c2 = 0, d2 = 0, e2 = 0;
-  if (same) {
-    a2 = 2.0 * sgE0(bi) * sgE0(bj);
-    b2 = sgE0(bi) * sgE1(bj) + sgE1(bi) * sgE0(bj);
-    c2 = 2.0 * sgE1(bi) * sgE1(bj);
-    d2 = sgE0(bi) * sgW(bj) + sgW(bi) * sgE0(bj);
-    e2 = sgE1(bi) * sgW(bj) + sgW(bi) * sgE1(bj);
-  }
-  const double a = S.a, b = S.b, c = S.c, d = S.d, e = S.e;
-  const double dt2 = -2 * S.bg[i] * S.bg[j] + S.ag[j] * S.cg[i] + S.ag[i] * S.cg[j] + c * a2 - 2 * b * b2 + a * c2;
-  const double s2 =
-      (-(S.cg[j] * S.dg[i]) - S.cg[i] * S.dg[j] + S.bg[j] * S.eg[i] + S.bg[i] * S.eg[j] + e * b2 - d * c2 -
-       c * d2 + b * e2) * S.idet -
-      ((S.det1[j] * (e * S.bg[i] - d * S.cg[i] - c * S.dg[i] + b * S.eg[i])) +
-       (S.det1[i] * (e * S.bg[j] - d * S.cg[j] - c * S.dg[j] + b * S.eg[j])) + (S.sN * dt2)) * S.idet2 +
-      (2 * S.sN * S.det1[i] * S.det1[j]) * S.idet3;
-  const double t2 =
-      (S.bg[j] * S.dg[i] + S.bg[i] * S.dg[j] - S.ag[j] * S.eg[i] - S.ag[i] * S.eg[j] - e * a2 + d * b2 +
-       b * d2 - a * e2) * S.idet -
-      ((S.det1[j] * (-(e * S.ag[i]) + d * S.bg[i] + b * S.dg[i] - a * S.eg[i])) +
-       (S.det1[i] * (-(e * S.ag[j]) + d * S.bg[j] + b * S.dg[j] - a * S.eg[j])) + (S.tN * dt2)) * S.idet2 +
-      (2 * S.tN * S.det1[i] * S.det1[j]) * S.idet3;
-  const double u2 = -(s2 + t2);
-  double acc = 0;
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    double q2 = S.V[1][k] * s2 + S.V[2][k] * t2 + S.V[0][k] * u2;
-    if (i == 3 + k) q2 += S.u1[j];
-    if (j == 3 + k) q2 += S.u1[i];
-    if (i == 6 + k) q2 += S.s1[j];
-    if (j == 6 + k) q2 += S.s1[i];
-    if (i == 9 + k) q2 += S.t1[j];
-    if (j == 9 + k) q2 += S.t1[i];
-    acc += S.J[k][i] * S.J[k][j] + S.q[k] * q2;
-  }
-  return 2 * acc;
-}
 
 // Hessian entry (i, j) of f1 - g / f2 over y = (p, q1, q2)
 __device__ double line_entry(const LineSetup &L, int i, int j) {
@@ -102,23 +70,50 @@ __device__ double line_entry(const LineSetup &L, int i, int j) {
   return t1 + t2 + f1dd + t4 + t5;
 }
 
-// Upper-triangle entry e (0..77) of a 12x12 matrix: (I, J), I <= J.
-__device__ __forceinline__ void upper_ij(int e, int &I, int &J) {
-  int i = 0, start = 0;
-  while (e >= start + 12 - i) {
-    start += 12 - i;
-    i++;
-  }
-  I = i;
-  J = i + (e - start);
+// component k of a 3-vector held in registers (selects, no local memory)
+__device__ __forceinline__ double pick3(const double v[3], int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
+
+// Entry (ci, cj) of the cross-product matrix [w]x (w x y = [w]x y).
+__device__ __forceinline__ double cross_entry(const double w[3], int ci, int cj) {
+  if (ci == cj) return 0.0;
+  const double wk = pick3(w, 3 - ci - cj);
+  return ((cj - ci + 3) % 3 == 1) ? -wk : wk;
 }
 
-// Entry (I, J) of the staged Hessian goes to the record of the code of vertex
-// pair (I/3, J/3) at (I%3, J%3); pairs without a code (an anchored vertex, or
-// the pair taken the other way round) are skipped.
-__device__ __forceinline__ void put(const int *P, double *rec, int I, int J, double v) {
-  const int q = P[4 * (I / 3) + J / 3];
-  if (q >= 0) rec[ICF_IMP_REC * (size_t)q + 3 * (I % 3) + (J % 3)] = v;
+// Closed-form Hessian entry (I, J) of the squared distance to the plane.
+struct PlaneScalars {
+  double a[3], e0[3], e1[3], e00, e11, e01, c1, c2, c3, c4, c5;
+};
+__device__ __forceinline__ double plane_entry(const PlaneSetup &S, const PlaneScalars &Q, int I, int J) {
+  const int bi = I / 3, bj = J / 3, ci = I % 3, cj = J % 3;
+  const double ai = cA(bi), aj = cA(bj), pi0 = cE0(bi), pj0 = cE0(bj), pi1 = cE1(bi), pj1 = cE1(bj);
+  // HD: the block (bi, bj) is [W]x with W a signed sum of e1, e0 and a
+  const double al = ai * pj0 - pi0 * aj, be = ai * pj1 - pi1 * aj, ga = pi0 * pj1 - pi1 * pj0;
+  double W[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) W[k] = -Q.e1[k] * al + Q.e0[k] * be - Q.a[k] * ga;
+  const double hd = cross_entry(W, ci, cj);
+  // HS from S = |e0|^2 |e1|^2 - (e0.e1)^2
+  const double dl = ci == cj ? 1.0 : 0.0;
+  const double h00 = 2.0 * (Q.e11 * dl - Q.e1[ci] * Q.e1[cj]);
+  const double h11 = 2.0 * (Q.e00 * dl - Q.e0[ci] * Q.e0[cj]);
+  const double h01 = 4.0 * Q.e0[ci] * Q.e1[cj] - 2.0 * Q.e1[ci] * Q.e0[cj] - 2.0 * Q.e01 * dl;
+  const double h10 = 4.0 * Q.e0[cj] * Q.e1[ci] - 2.0 * Q.e1[cj] * Q.e0[ci] - 2.0 * Q.e01 * dl;
+  const double hs = pi0 * pj0 * h00 + pi1 * pj1 * h11 + pi0 * pj1 * h01 + pi1 * pj0 * h10;
+  const double gDi = S.gD[I], gDj = S.gD[J], gSi = S.gS[I], gSj = S.gS[J];
+  return Q.c1 * gDi * gDj + Q.c2 * hd + Q.c3 * (gDi * gSj + gSi * gDj) + Q.c4 * hs + Q.c5 * gSi * gSj;
+}
+
+// record entry slot (0..89) -> vertex pair (bA <= bB) and entry (r, c) of
+// its 3x3 block: the four diagonal pairs, then the six off-diagonal ones
+__constant__ int kPairA[10] = {0, 1, 2, 3, 0, 0, 0, 1, 1, 2};
+__constant__ int kPairB[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+__device__ __forceinline__ void slot_entry(int sl, int &bA, int &bB, int &r, int &c) {
+  const int pi = sl / 9, e = sl % 9;
+  bA = kPairA[pi];
+  bB = kPairB[pi];
+  r = e / 3;
+  c = e % 3;
 }
 
 __global__ void __launch_bounds__(32 * WARPS)
@@ -126,6 +121,7 @@ __global__ void __launch_bounds__(32 * WARPS)
                 const int4 *__restrict__ ci, const double4 *__restrict__ cd, double kpen,
                 const int *__restrict__ pos, double *__restrict__ rec, double *__restrict__ frc) {
   __shared__ PlaneSetup sP[WARPS];
+  __shared__ PlaneScalars sQ[WARPS];
   __shared__ LineSetup sL[WARPS];
   __shared__ double sx[WARPS][12];
   __shared__ double sfd[WARPS][3];
@@ -154,21 +150,11 @@ __global__ void __launch_bounds__(32 * WARPS)
   __syncwarp();
   const double *x = sx[wl];
   const double hk = kpen * 0.5;
-
-  if (c.x == 1) {  // vertex: d2 = |p - x_b|^2
-    const int vb = c.z;
-    if (lane < 3) sfd[wl][lane] = 2 * (x[lane] - x[3 * vb + lane]);
-    for (int e = lane; e < 78; e += 32) {
-      int I, J;
-      upper_ij(e, I, J);
-      const int bI = I / 3, bJ = J / 3;
-      double v = 0;
-      if (I % 3 == J % 3 && (bI == 0 || bI == vb) && (bJ == 0 || bJ == vb)) v = (bI == bJ) ? 2.0 : -2.0;
-      v = kpen * v / 2;
-      put(P, rec, I, J, v);
-      if (I != J) put(P, rec, J, I, v);
-    }
-  } else if (c.x == 2) {  // edge (ia nearer, ib)
+  const int kind = c.x;
+  PlaneScalars &Q = sQ[wl];
+  if (kind == 1) {  // vertex: d2 = |p - x_b|^2
+    if (lane < 3) sfd[wl][lane] = 2 * (x[lane] - x[3 * c.z + lane]);
+  } else if (kind == 2) {  // edge (ia nearer, ib)
     const int ia = c.y, ib = c.z;
     LineSetup &L = sL[wl];
     if (lane == 0) {
@@ -197,89 +183,93 @@ __global__ void __launch_bounds__(32 * WARPS)
       for (int k = 0; k < 3; k++)
         sfd[wl][k] = L.f1d[k] + (L.g * L.f2d[k] - L.f2 * L.gd[k]) / L.f2sq;
     }
-    __syncwarp();
-    for (int e = lane; e < 78; e += 32) {
-      int I, J;
-      upper_ij(e, I, J);
-      const int bI = I / 3, bJ = J / 3;
-      const int pI = bI == 0 ? 0 : (bI == ia ? 1 : (bI == ib ? 2 : -1));
-      const int pJ = bJ == 0 ? 0 : (bJ == ia ? 1 : (bJ == ib ? 2 : -1));
-      double v = 0;
-      if (pI >= 0 && pJ >= 0) v = line_entry(L, 3 * pI + I % 3, 3 * pJ + J % 3);
-      v = kpen * v / 2;
-      put(P, rec, I, J, v);
-      if (I != J) put(P, rec, J, I, v);
-    }
-  } else {  // interior
+  } else {  // interior: d2 = D^2 / S
     PlaneSetup &S = sP[wl];
-    // the scalars of point_plane_distance, on every lane (no round trip)
-    double e0[3], e1[3], w[3];
+    double a[3], e0[3], e1[3], N[3], e1xa[3], axe0[3], e1xN[3], Nxe0[3];
+#pragma unroll
     for (int k = 0; k < 3; k++) {
-      e0[k] = -x[3 + k] + x[6 + k];
-      e1[k] = -x[3 + k] + x[9 + k];
-      w[k] = -x[k] + x[3 + k];
+      a[k] = x[k] - x[3 + k];
+      e0[k] = x[6 + k] - x[3 + k];
+      e1[k] = x[9 + k] - x[3 + k];
     }
-    const double a = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
-    const double b = e1[1] * e0[1] + e1[2] * e0[2] + e0[0] * e1[0];
-    const double c2 = e1[1] * e1[1] + e1[2] * e1[2] + e1[0] * e1[0];
-    const double d = w[0] * e0[0] + w[1] * e0[1] + w[2] * e0[2];
-    const double e = e1[1] * w[1] + e1[2] * w[2] + w[0] * e1[0];
-    const double det = a * c2 - b * b;
-    const double idet = 1.0 / det, idet2 = idet * idet, idet3 = idet2 * idet;
-    const double ss = (b * e - c2 * d) * idet, tt = (b * d - a * e) * idet, uu = 1 - (ss + tt);
+#define CROSS(o, u_, v_)                          \
+  o[0] = u_[1] * v_[2] - u_[2] * v_[1];           \
+  o[1] = u_[2] * v_[0] - u_[0] * v_[2];           \
+  o[2] = u_[0] * v_[1] - u_[1] * v_[0];
+    CROSS(N, e0, e1)
+    CROSS(e1xa, e1, a)
+    CROSS(axe0, a, e0)
+    CROSS(e1xN, e1, N)
+    CROSS(Nxe0, N, e0)
+#undef CROSS
+    const double D = a[0] * N[0] + a[1] * N[1] + a[2] * N[2];
+    const double Sv = N[0] * N[0] + N[1] * N[1] + N[2] * N[2];
+    const double iS = 1.0 / Sv;
     if (lane == 0) {
-      S.a = a; S.b = b; S.c = c2; S.d = d; S.e = e;
-      S.det = det; S.idet = idet; S.idet2 = idet2; S.idet3 = idet3;
-      S.s = ss; S.t = tt; S.u = uu;
-      S.sN = -(c2 * d) + b * e;
-      S.tN = b * d - a * e;
-    }
-    if (lane < 9) S.V[lane / 3][lane % 3] = x[3 + lane];
-    if (lane < 3) S.q[lane] = -x[lane] + x[6 + lane] * ss + x[9 + lane] * tt + x[3 + lane] * uu;
-    if (lane < 12) {
-      const int i = lane, bi = i / 3, k = i % 3;
-      const double ag = 2.0 * sgE0(bi) * e0[k];
-      const double bg = sgE0(bi) * e1[k] + sgE1(bi) * e0[k];
-      const double cg = 2.0 * sgE1(bi) * e1[k];
-      const double dg = sgE0(bi) * w[k] + sgW(bi) * e0[k];
-      const double eg = sgE1(bi) * w[k] + sgW(bi) * e1[k];
-      S.ag[i] = ag; S.bg[i] = bg; S.cg[i] = cg; S.dg[i] = dg; S.eg[i] = eg;
-      const double det1 = c2 * ag + a * cg - 2 * b * bg;
-      const double s1 = ((c2 * d - b * e) * det1) * idet2 + ((e * bg + b * eg) - (d * cg + c2 * dg)) * idet;
-      const double t1 = ((a * e - b * d) * det1) * idet2 + ((d * bg + b * dg) - (a * eg + e * ag)) * idet;
-      S.det1[i] = det1;
-      S.s1[i] = s1;
-      S.t1[i] = t1;
-      S.u1[i] = -(s1 + t1);
-      for (int kk = 0; kk < 3; kk++) {
-        double v = x[6 + kk] * s1 + x[9 + kk] * t1 + x[3 + kk] * (-(s1 + t1));
-        if (i == kk) v -= 1;
-        if (i == 3 + kk) v += uu;
-        if (i == 6 + kk) v += ss;
-        if (i == 9 + kk) v += tt;
-        S.J[kk][i] = v;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        Q.a[k] = a[k];
+        Q.e0[k] = e0[k];
+        Q.e1[k] = e1[k];
       }
+      Q.e00 = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
+      Q.e11 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+      Q.e01 = e0[0] * e1[0] + e0[1] * e1[1] + e0[2] * e1[2];
+      Q.c1 = 2.0 * iS;
+      Q.c2 = 2.0 * D * iS;
+      Q.c3 = -2.0 * D * iS * iS;
+      Q.c4 = -D * D * iS * iS;
+      Q.c5 = 2.0 * D * D * iS * iS * iS;
     }
-    __syncwarp();
-    if (lane < 3) sfd[wl][lane] = 2 * (S.q[0] * S.J[0][lane] + S.q[1] * S.J[1][lane] + S.q[2] * S.J[2][lane]);
-    for (int en = lane; en < 78; en += 32) {
-      int I, J;
-      upper_ij(en, I, J);
-      const double v = kpen * plane_entry(S, I, J) / 2;
-      put(P, rec, I, J, v);
-      if (I != J) put(P, rec, J, I, v);
+    if (lane < 12) {
+      const int b = lane / 3, k = lane % 3;
+      S.gD[lane] = cA(b) * pick3(N, k) + cE0(b) * pick3(e1xa, k) + cE1(b) * pick3(axe0, k);
+      S.gS[lane] = 2.0 * (cE0(b) * pick3(e1xN, k) + cE1(b) * pick3(Nxe0, k));
     }
+    // d(d2)/dp = 2 D N / S
+    if (lane < 3) sfd[wl][lane] = (2.0 * D * iS) * pick3(N, lane);
   }
   __syncwarp();
+  // one lane per record entry: pair (bA, bB), entry (r, c)
+  for (int sl = lane; sl < 90; sl += 32) {
+    int bA, bB, r, cc;
+    slot_entry(sl, bA, bB, r, cc);
+    int I = 3 * bA + r, J = 3 * bB + cc;
+    if (I > J) {  // lower entry of a diagonal block: its mirror
+      const int t = I;
+      I = J;
+      J = t;
+    }
+    double v = 0;
+    if (kind == 1) {
+      const int vb = c.z, bI = I / 3, bJ = J / 3;
+      if (I % 3 == J % 3 && (bI == 0 || bI == vb) && (bJ == 0 || bJ == vb)) v = (bI == bJ) ? 2.0 : -2.0;
+    } else if (kind == 2) {
+      const int ia = c.y, ib = c.z, bI = I / 3, bJ = J / 3;
+      const int pI = bI == 0 ? 0 : (bI == ia ? 1 : (bI == ib ? 2 : -1));
+      const int pJ = bJ == 0 ? 0 : (bJ == ia ? 1 : (bJ == ib ? 2 : -1));
+      if (pI >= 0 && pJ >= 0) v = line_entry(sL[wl], 3 * pI + I % 3, 3 * pJ + J % 3);
+    } else {
+      v = plane_entry(sP[wl], Q, I, J);
+    }
+    v = kpen * v / 2;
+    // the code of the pair, taken either way round (none: an anchored vertex)
+    const int q = P[4 * bA + bB];
+    if (q >= 0) {
+      rec[ICF_IMP_REC * (size_t)q + 3 * r + cc] = v;
+    } else if (bA != bB) {
+      const int q2 = P[4 * bB + bA];
+      if (q2 >= 0) rec[ICF_IMP_REC * (size_t)q2 + 3 * cc + r] = v;
+    }
+  }
   // vertex forces (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp, w = (1-s-t, s, t)
   // (collision_response.h:89-109): into the force record, and as the rhs of
   // the vertex's diagonal code
   if (lane < 12) {
     const double s = cl.x, t = cl.y;
-    const double wv[3] = {1 - (s + t), s, t};
     const int comp = lane % 3, blk = lane / 3;
     const double F = hk * sfd[wl][comp];
-    const double f = blk == 0 ? -F : wv[blk - 1] * F;
+    const double f = blk == 0 ? -F : (blk == 1 ? (1 - (s + t)) : (blk == 2 ? s : t)) * F;
     frc[12 * (size_t)u + lane] = f;
     const int q = P[5 * blk];
     if (q >= 0) rec[ICF_IMP_REC * (size_t)q + 9 + comp] = f;

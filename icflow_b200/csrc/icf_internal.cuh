@@ -141,13 +141,12 @@ struct icf_contact_ws {
   long long ncnt_cap = 0;
   unsigned long long *nk0 = nullptr, *nk1 = nullptr;
   long long nkey_cap = 0;
-  // direct contact detection: per surface element the tet inverse and first
-  // vertex (12 doubles, capacity b_cap); a dense grid of cells (counts,
-  // offsets, cursors; capacity cell_cap) and its element entries (capacity
-  // dent_cap)
-  double *tinv = nullptr;
-  int *gcnt = nullptr, *goff = nullptr, *gcur = nullptr, *gent = nullptr;
-  long long cell_cap = 0, dent_cap = 0, tinv_cap = 0;
+  // direct contact detection: a dense grid of cells (counts, offsets,
+  // cursors; capacity cell_cap) holding the surface nodes as {x, y, z, k}
+  // entries (k the surface-node index; capacity gnode_cap)
+  int *gcnt = nullptr, *goff = nullptr, *gcur = nullptr;
+  double4 *gnode = nullptr;
+  long long cell_cap = 0, gnode_cap = 0;
   // small device results and their pinned host copy: [0] unique count,
   // [1] impact list differs from the built one, [2] pairs before de-duplication
   int *d_small = nullptr, *h_small = nullptr;

@@ -843,6 +843,7 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
 
   // impact contributions grouped by slot
   ctx->n_crs = 0;
+  ctx->n_crs_off = 0;
   if (ctx->n_imp > 0) {
     const int n = 16 * ctx->n_imp;
     int *sl0, *sl1, *d_nr, *cnt;

@@ -149,8 +149,9 @@ class LearnedWarmStart:
     # ---- data -----------------------------------------------------------------
     def record(self, model, h, u, v, a, du1, du2, du_acc):
         act = model.active
-        self.xs.append(features(u, v, a, du1, du2)[act])
-        self.ys.append((du_acc - v * h - (du1 - du2))[act].astype(np.float32))
+        d1, d2 = model.history_increments(h)
+        self.xs.append(features(u, v, a, d1, d2)[act])
+        self.ys.append((du_acc - model.extrapolation(h, v))[act].astype(np.float32))
         # the step's last assembled matrix (at the accepted iterate), for the
         # residual-weighted loss
         gf = model.gf
@@ -233,10 +234,10 @@ class LearnedWarmStart:
     # ---- the guess --------------------------------------------------------------
     def guess(self, model, h, u, v, a, gain=None):
         g = self.gain if gain is None else gain
-        du = v * h + (model.du_prev - model.du_prev2)
+        du = model.extrapolation(h, v)
         if self.norm is None or g == 0:
             return du
-        x = features(u, v, a, model.du_prev, model.du_prev2)
+        x = features(u, v, a, *model.history_increments(h))
         corr = self.net.forward(x).astype(np.float64) * self.norm[2 * NI:]
         return du + g * corr
 
@@ -261,17 +262,18 @@ class LearnedWarmStart:
         return guesses[k]
 
     def calibrate(self, model, steps: int, gains=(0.0, 0.05, 0.2, 0.5, 1.0)) -> dict:
-        """Runs `steps` steps of `model` (plain guess) and, before each, the
-        first-iterate residual of the learned guess at each gain; keeps the
-        gain with the smallest mean log residual.  Returns that mean per gain."""
-        h = model.prms.InitialTimeStep
+        """Runs `steps` attempts of `model` (extrapolation guess) and, before
+        each, the first-iterate residual of the learned guess at each gain;
+        keeps the gain with the smallest mean log residual.  Returns that mean
+        per gain."""
         logs = {g: [] for g in gains}
         for _ in range(steps):
+            h = model.time_step()[0]
             u, v, a, _ = model.gf.GetNodeState()
             rs = model.guess_residuals([self.guess(model, h, u, v, a, gain=g) for g in gains])
             for g, r in zip(gains, rs):
                 logs[g].append(np.log10(max(r, 1e-300)))
-            model.Step()
+            model.Step(warm_start=lambda m, hh, uu, vv, aa: m.extrapolation(hh, vv))
         mean = {g: float(np.mean(logs[g])) for g in gains}
         self.gain = min(mean, key=mean.get)
         return mean

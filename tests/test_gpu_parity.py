@@ -253,6 +253,11 @@ def test_structure_kept_for_the_same_impacts(O):
     d = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
     for k in ("rows", "cols", "vals", "rhs"):
         assert np.array_equal(a[k], d[k]), k
+    # contact ends: an empty list after impacts whose blocks the off-diagonal
+    # gather also writes (the impact-add launches must all go)
+    e = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, impacts=np.zeros((0, 4), np.int32))
+    compare(e, oracle_assemble(O, p, coll, state, H, pmax, tmax, np.zeros((0, 4), np.int32)))
+    assert e["counts"].nImpacts == 0
     gf.close()
 
 
