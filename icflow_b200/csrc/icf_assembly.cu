@@ -404,27 +404,26 @@ __global__ void k_zero_dyn(int nd, const int *__restrict__ pos, double *__restri
 // block's codes (k_imp_deriv writes them at the codes' positions in the
 // slot-sorted list, so a block's records are contiguous) are summed in code
 // order and added to the block, and to the rhs row for a diagonal block.
-__global__ void k_imp_add(int n_slots, const int *__restrict__ slot, const int *__restrict__ off,
-                          const int *__restrict__ cols, const double *__restrict__ rec,
+__global__ void k_imp_add(int count, const int *__restrict__ ord, int first, const int *__restrict__ slot,
+                          const int *__restrict__ off, const int *__restrict__ cols, const double *__restrict__ rec,
                           double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite,
-                          const unsigned long long *__restrict__ mkey, const int *__restrict__ src,
-                          int identity, int which) {
-  // which: 0 every touched block; 1 those the off-diagonal gather does not
-  // write (diagonal or contact-only); 2 those it does (static, off-diagonal).
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+                          const unsigned long long *__restrict__ mkey) {
+  // touched slot ord[first + t] (or first + t without an order)
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   bool bad = false;
-  if (w < n_slots) {
+  if (t < count) {
+    const int w = ord ? ord[first + t] : first + t;
     const int s = slot[w];
-    if (which == 0 || icf_off_static(mkey, src, identity, s) == (which == 2)) {
+    {
       const int q0 = off[w], q1 = off[w + 1];
       double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int q = q0; q < q1; q++) {
         const double2 *R = reinterpret_cast<const double2 *>(rec + ICF_IMP_REC * (size_t)q);
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-          const double2 t = __ldg(R + k);
-          v[2 * k] += t.x;
-          v[2 * k + 1] += t.y;
+          const double2 r2 = __ldg(R + k);
+          v[2 * k] += r2.x;
+          v[2 * k + 1] += r2.y;
         }
       }
       double *o = vals + 9 * (size_t)s;
@@ -944,7 +943,6 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   // impact terms: the blocks that the off-diagonal gather does not write
   // (diagonal blocks, written on main, and contact-only blocks, zeroed on
   // aux1) as soon as the impacts are staged; the others after the join
-  const int ident = ctx->src_identity ? 1 : 0;
   // algorithmic bytes: the impact staging once, 172 B per touched block and
   // 4 B per code, split between the two launches by their blocks
   const long long n_codes = 10LL * ctx->n_imp;  // at most; records of 12 doubles
@@ -952,16 +950,16 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   const int n_a = ctx->n_crs - ctx->n_crs_off;
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
   if (n_a > 0) {
-    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(
-        ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
-        ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 1);
+    k_imp_add<<<icf_blocks(n_a, 128), 128, 0, s>>>(n_a, ctx->d_cr_ord, 0, ctx->d_cr_slot, ctx->d_cr_off,
+                                                  ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
+                                                  ctx->d_counts + 4, ctx->d_mkeys);
     icf_prof_mark(ctx, s, "k_imp_add", imp_in * n_a / ctx->n_crs + 144LL * n_a);
   }
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   if (ctx->n_crs_off > 0 && ctx->n_crs > 0) {
-    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(
-        ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
-        ctx->d_counts + 4, ctx->d_mkeys, ctx->d_src, ident, 2);
+    k_imp_add<<<icf_blocks(ctx->n_crs_off, 128), 128, 0, s>>>(
+        ctx->n_crs_off, ctx->d_cr_ord, n_a, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols, ctx->d_ks, ctx->d_vals,
+        ctx->d_rhs, ctx->d_counts + 4, ctx->d_mkeys);
     icf_prof_mark(ctx, s, "k_imp_add_off", imp_in * ctx->n_crs_off / ctx->n_crs + 144LL * ctx->n_crs_off);
   }
 
@@ -1207,9 +1205,9 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
                                           B.rhs, s));
   }
   if (ctx->n_crs > 0)
-    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols,
-                                                        B.ks, B.vals, B.rhs, ctx->d_counts + 4, ctx->d_mkeys,
-                                                        ctx->d_src, ctx->src_identity ? 1 : 0, 0);
+    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, nullptr, 0, ctx->d_cr_slot, ctx->d_cr_off,
+                                                        ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4,
+                                                        ctx->d_mkeys);
 
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));

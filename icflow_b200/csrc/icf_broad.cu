@@ -289,7 +289,9 @@ __global__ void k_node_put(int ns, const int *__restrict__ snode, const double4 
   if (off) ent[off[l] + w] = make_double4(P.x, P.y, P.z, (double)k);
 }
 
-// one thread per surface element b: keys node << eb | b of its impacts
+// eight threads per surface element b, each taking every eighth cell its box
+// reaches: keys k << eb | b of its impacts (k the surface-node index) and a
+// count per surface node
 __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
                                                 const double *__restrict__ lohi, const int4 *__restrict__ clo,
                                                 int ny, int nz, const int *__restrict__ goff,
@@ -297,8 +299,9 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
                                                 const int *__restrict__ sinc_off, const int *__restrict__ sinc,
                                                 const int *__restrict__ group, int eb,
                                                 unsigned long long *__restrict__ out, long long cap,
-                                                int *__restrict__ count) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+                                                int *__restrict__ count, int *__restrict__ kcnt) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = (int)(t >> 3), g = (int)(t & 7);
   if (b >= n) return;
   const int4 B = selem[b];
   const int nb[4] = {B.x, B.y, B.z, B.w};
@@ -314,28 +317,57 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
   const double lx = lh[0], ly = lh[1], lz = lh[2], hx = lh[3], hy = lh[4], hz = lh[5];
   const int4 c = clo[b];
   const int sx = c.w & 1023, sy = (c.w >> 10) & 1023, sz = (c.w >> 20) & 1023;
-  for (int dx = 0; dx <= sx; dx++)
-    for (int dy = 0; dy <= sy; dy++)
-      for (int dz = 0; dz <= sz; dz++) {
-        const long long l = cell_lin(c.x + dx, c.y + dy, c.z + dz, ny, nz);
-        const int e1 = goff[l + 1];
-        for (int e = goff[l]; e < e1; e++) {
-          const double4 P = gnode[e];
-          if (!(P.x >= lx && P.x <= hx && P.y >= ly && P.y <= hy && P.z >= lz && P.z <= hz)) continue;
-          const int k = (int)P.w;
-          const int p = snode[k];
-          if (p == nb[0] || p == nb[1] || p == nb[2] || p == nb[3]) continue;
-          if (!tet_contains(bi, P.x - x[0], P.y - x[1], P.z - x[2])) continue;
-          bool any = false;
-          for (int j = sinc_off[k]; j < sinc_off[k + 1] && !any; j++) {
-            const int a = sinc[j];
-            any = keep_pair(a < b ? a : b, a < b ? b : a, lohi, group, selem, xc);
-          }
-          if (!any) continue;
-          const int w = atomicAdd(count, 1);
-          if (w < cap) out[w] = ((unsigned long long)(unsigned)p << eb) | (unsigned)b;
-        }
+  const int ncell = (sx + 1) * (sy + 1) * (sz + 1);
+  for (int j = g; j < ncell; j += 8) {
+    const int dz = j % (sz + 1), dy = (j / (sz + 1)) % (sy + 1), dx = j / ((sz + 1) * (sy + 1));
+    const long long l = cell_lin(c.x + dx, c.y + dy, c.z + dz, ny, nz);
+    const int e1 = goff[l + 1];
+    for (int e = goff[l]; e < e1; e++) {
+      const double4 P = gnode[e];
+      if (!(P.x >= lx && P.x <= hx && P.y >= ly && P.y <= hy && P.z >= lz && P.z <= hz)) continue;
+      const int k = (int)P.w;
+      const int p = snode[k];
+      if (p == nb[0] || p == nb[1] || p == nb[2] || p == nb[3]) continue;
+      if (!tet_contains(bi, P.x - x[0], P.y - x[1], P.z - x[2])) continue;
+      bool any = false;
+      for (int q = sinc_off[k]; q < sinc_off[k + 1] && !any; q++) {
+        const int a = sinc[q];
+        any = keep_pair(a < b ? a : b, a < b ? b : a, lohi, group, selem, xc);
       }
+      if (!any) continue;
+      const int w = atomicAdd(count, 1);
+      atomicAdd(kcnt + k, 1);
+      if (w < cap) out[w] = ((unsigned long long)(unsigned)k << eb) | (unsigned)b;
+    }
+  }
+}
+
+// the hits grouped by surface node (ascending, so by node id): key
+// node << eb | b at koff[k] + the node's running count
+__global__ void k_place(int hits, const unsigned long long *__restrict__ in, int eb, const int *__restrict__ koff,
+                        int *__restrict__ kcur, const int *__restrict__ snode, unsigned long long *__restrict__ out) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= hits) return;
+  const unsigned long long key = in[h];
+  const int k = (int)(key >> eb);
+  const unsigned long long b = key & ((1ull << eb) - 1);
+  out[koff[k] + atomicAdd(kcur + k, 1)] = ((unsigned long long)(unsigned)snode[k] << eb) | b;
+}
+
+// each surface node's few hits in ascending element order (insertion sort)
+__global__ void k_sort_seg(int ns, const int *__restrict__ koff, unsigned long long *__restrict__ keys) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  const int a = koff[k], e = koff[k + 1];
+  for (int i = a + 1; i < e; i++) {
+    const unsigned long long v = keys[i];
+    int j = i - 1;
+    while (j >= a && keys[j] > v) {
+      keys[j + 1] = keys[j];
+      j--;
+    }
+    keys[j + 1] = v;
+  }
 }
 
 }  // namespace
@@ -351,7 +383,8 @@ static int grow(icf_ctx *ctx, T **p, long long n) {
 void icf_free_contact_ws(icf_ctx *ctx) {
   icf_contact_ws &W = ctx->cws;
   void *d[] = {W.lohi, W.ext, W.tmpv, W.red, W.bcnt, W.boff, W.clo, W.ek0, W.ek1, W.ee0, W.ee1, W.pc, W.po,
-               W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small, W.gcnt, W.goff, W.gcur, W.gnode};
+               W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small, W.gcnt, W.goff, W.gcur, W.gnode,
+               W.kcnt, W.koff, W.kcur};
   for (void *q : d) cudaFree(q);
   cudaFreeHost(W.h_small);
   cudaFreeHost(W.h_red);
@@ -569,15 +602,21 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
                                                  W.gnode);
   // every element's cells
   k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
-  int eb = 1, vb = 1;
+  int eb = 1;
   while ((1LL << eb) < (long long)n) eb++;
-  while ((1LL << vb) < (long long)ctx->n_nodes) vb++;
+  if (ns + 1LL > W.kcap) {
+    ICF_TRY_RC(grow(ctx, &W.kcnt, ns + 1LL));
+    ICF_TRY_RC(grow(ctx, &W.koff, ns + 1LL));
+    ICF_TRY_RC(grow(ctx, &W.kcur, ns + 1LL));
+    W.kcap = ns + 1LL;
+  }
   int hits = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
     ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, sizeof(int), s));
-    k_detect<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, ny, nz, W.goff, W.gnode,
-                                               ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, d_group, eb, W.nk0,
-                                               W.nkey_cap, W.d_small + 5);
+    ICF_CUDA(ctx, cudaMemsetAsync(W.kcnt, 0, sizeof(int) * (ns + 1LL), s));
+    k_detect<<<icf_blocks(8LL * n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, ny, nz, W.goff,
+                                                     W.gnode, ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, d_group, eb,
+                                                     W.nk0, W.nkey_cap, W.d_small + 5, W.kcnt);
     ICF_CUDA(ctx, cudaGetLastError());
     ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 5, W.d_small + 5, sizeof(int), cudaMemcpyDeviceToHost, s));
     ICF_CUDA(ctx, cudaStreamSynchronize(s));
@@ -590,10 +629,16 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     W.nkey_cap = c;
   }
   if (hits > 0) {
+    // grouped by surface node (a counting sort), each node's hits sorted:
+    // the keys node << eb | element ascending
     tb = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb, W.nk0, W.nk1, hits, 0, eb + vb, s);
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, W.kcnt, W.koff, ns + 1, s);
     if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(ctx->d_tmp, tb, W.nk0, W.nk1, hits, 0, eb + vb, s));
+    ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.kcnt, W.koff, ns + 1, s));
+    ICF_CUDA(ctx, cudaMemsetAsync(W.kcur, 0, sizeof(int) * (ns + 1LL), s));
+    k_place<<<icf_blocks(hits, 256), 256, 0, s>>>(hits, W.nk0, eb, W.koff, W.kcur, ctx->d_snode, W.nk1);
+    k_sort_seg<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, W.koff, W.nk1);
+    ICF_CUDA(ctx, cudaGetLastError());
   }
   return icf_finish_impacts(ctx, W.nk1, hits, W.d_small + 5, eb, n_impacts);
 }

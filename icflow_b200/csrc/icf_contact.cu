@@ -126,36 +126,60 @@ __device__ double dtn(const double f[9], const double p[3]) {
   return r;
 }
 
+// Eight threads per (node, element) key, each taking every eighth adjacent
+// face; the group keeps the smallest distance, the first face in list order
+// on ties (kFindClosestFace's strict minimum over the list in order).
 __global__ void k_closest(int n, const int *__restrict__ n_dev, int eb, const unsigned long long *__restrict__ keys,
                           const int *__restrict__ adj_off, const int *__restrict__ adj,
                           const int *__restrict__ faces, const double4 *__restrict__ xc,
                           int4 *__restrict__ imp) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || i >= *n_dev) return;
-  const unsigned long long key = keys[i];
-  const int node = (int)(key >> eb), el = (int)(key & ((1ull << eb) - 1));
-  const double4 pp = xc[node];
-  const double p[3] = {pp.x, pp.y, pp.z};
-  int best = -1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(t >> 3), g = (int)(t & 7);
+  const bool valid = i < n && i < *n_dev;
+  int node = 0, best = 0x7fffffff;
   double bestd = 0;
-  for (int q = adj_off[el]; q < adj_off[el + 1]; q++) {
-    const int fc = adj[q];
-    double fx[9];
-    for (int v = 0; v < 3; v++) {
-      const double4 c = xc[faces[3 * fc + v]];
-      fx[3 * v] = c.x; fx[3 * v + 1] = c.y; fx[3 * v + 2] = c.z;
-    }
-    const double dd = dtn(fx, p);
-    if (q == adj_off[el] || dd < bestd) {
-      best = fc;
-      bestd = dd;
+  bool have = false;
+  if (valid) {
+    const unsigned long long key = keys[i];
+    node = (int)(key >> eb);
+    const int el = (int)(key & ((1ull << eb) - 1));
+    const double4 pp = xc[node];
+    const double p[3] = {pp.x, pp.y, pp.z};
+    for (int q = adj_off[el] + g; q < adj_off[el + 1]; q += 8) {
+      const int fc = adj[q];
+      double fx[9];
+      for (int v = 0; v < 3; v++) {
+        const double4 c = xc[faces[3 * fc + v]];
+        fx[3 * v] = c.x; fx[3 * v + 1] = c.y; fx[3 * v + 2] = c.z;
+      }
+      const double dd = dtn(fx, p);
+      if (!have || dd < bestd) {
+        best = q;
+        bestd = dd;
+        have = true;
+      }
     }
   }
-  if (best < 0) {
+  // (distance, list position) minimum over the group; lanes without a face
+  // (or past the keys) take part with the largest position
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    const double od = __shfl_xor_sync(0xffffffffu, bestd, o);
+    const int oq = __shfl_xor_sync(0xffffffffu, best, o);
+    const bool oh = __shfl_xor_sync(0xffffffffu, (int)have, o) != 0;
+    if (oh && (!have || od < bestd || (od == bestd && oq < best))) {
+      bestd = od;
+      best = oq;
+      have = true;
+    }
+  }
+  if (!valid || g != 0) return;
+  if (!have) {
     imp[i] = make_int4(node, -1, -1, -1);
     return;
   }
-  imp[i] = make_int4(node, faces[3 * best], faces[3 * best + 1], faces[3 * best + 2]);
+  const int fc = adj[best];
+  imp[i] = make_int4(node, faces[3 * fc], faces[3 * fc + 1], faces[3 * fc + 2]);
 }
 
 // ---- point-triangle classification -------------------------------------------------
@@ -463,8 +487,8 @@ int icf_finish_impacts(icf_ctx *ctx, const unsigned long long *keys, int total, 
       ctx->imp_cap = 2 * total;
       ctx->imp_gen++;
     }
-    k_closest<<<icf_blocks(total, 128), 128, 0, s>>>(total, d_n, eb, keys, ctx->d_adj_off, ctx->d_adj,
-                                                    ctx->d_faces, ctx->d_xc, ctx->d_imp);
+    k_closest<<<icf_blocks(8LL * total, 128), 128, 0, s>>>(total, d_n, eb, keys, ctx->d_adj_off, ctx->d_adj,
+                                                          ctx->d_faces, ctx->d_xc, ctx->d_imp);
     ICF_CUDA(ctx, cudaGetLastError());
     ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 1, 0, sizeof(int), s));
     if (cmp && ctx->imp_gen == ctx->imp_gen_built)

@@ -125,11 +125,13 @@ __global__ void __launch_bounds__(32 * WARPS)
   __shared__ LineSetup sL[WARPS];
   __shared__ double sx[WARPS][12];
   __shared__ double sfd[WARPS][3];
+  __shared__ int sPos[WARPS][16];
   const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int u = blockIdx.x * WARPS + wl;
   if (u >= n) return;  // uniform per warp
   const int *P = pos + 16 * (size_t)u;
   const int4 c = ci[u];
+  if (lane < 16) sPos[wl][lane] = P[lane];
   if (c.x < 0) {  // no response: zero records, zero forces
     for (int e = lane; e < 16 * ICF_IMP_REC; e += 32) {
       const int q = P[e / ICF_IMP_REC];
@@ -230,38 +232,51 @@ __global__ void __launch_bounds__(32 * WARPS)
     if (lane < 3) sfd[wl][lane] = (2.0 * D * iS) * pick3(N, lane);
   }
   __syncwarp();
-  // one lane per record entry: pair (bA, bB), entry (r, c)
-  for (int sl = lane; sl < 90; sl += 32) {
-    int bA, bB, r, cc;
-    slot_entry(sl, bA, bB, r, cc);
-    int I = 3 * bA + r, J = 3 * bB + cc;
-    if (I > J) {  // lower entry of a diagonal block: its mirror
-      const int t = I;
-      I = J;
-      J = t;
-    }
-    double v = 0;
-    if (kind == 1) {
-      const int vb = c.z, bI = I / 3, bJ = J / 3;
-      if (I % 3 == J % 3 && (bI == 0 || bI == vb) && (bJ == 0 || bJ == vb)) v = (bI == bJ) ? 2.0 : -2.0;
-    } else if (kind == 2) {
-      const int ia = c.y, ib = c.z, bI = I / 3, bJ = J / 3;
-      const int pI = bI == 0 ? 0 : (bI == ia ? 1 : (bI == ib ? 2 : -1));
-      const int pJ = bJ == 0 ? 0 : (bJ == ia ? 1 : (bJ == ib ? 2 : -1));
-      if (pI >= 0 && pJ >= 0) v = line_entry(sL[wl], 3 * pI + I % 3, 3 * pJ + J % 3);
-    } else {
-      v = plane_entry(sP[wl], Q, I, J);
-    }
-    v = kpen * v / 2;
-    // the code of the pair, taken either way round (none: an anchored vertex)
-    const int q = P[4 * bA + bB];
-    if (q >= 0) {
-      rec[ICF_IMP_REC * (size_t)q + 3 * r + cc] = v;
-    } else if (bA != bB) {
-      const int q2 = P[4 * bB + bA];
-      if (q2 >= 0) rec[ICF_IMP_REC * (size_t)q2 + 3 * cc + r] = v;
+  // one lane per record entry: pair (bA, bB), entry (r, c); the three
+  // entries of a lane are computed first and stored after, so that their
+  // shared-memory reads overlap
+  double val[3];
+  long long dst[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int sl = lane + 32 * k;
+    val[k] = 0.0;
+    dst[k] = -1;
+    if (sl < 90) {
+      int bA, bB, r, cc;
+      slot_entry(sl, bA, bB, r, cc);
+      int I = 3 * bA + r, J = 3 * bB + cc;
+      if (I > J) {  // lower entry of a diagonal block: its mirror
+        const int t = I;
+        I = J;
+        J = t;
+      }
+      double v = 0;
+      if (kind == 1) {
+        const int vb = c.z, bI = I / 3, bJ = J / 3;
+        if (I % 3 == J % 3 && (bI == 0 || bI == vb) && (bJ == 0 || bJ == vb)) v = (bI == bJ) ? 2.0 : -2.0;
+      } else if (kind == 2) {
+        const int ia = c.y, ib = c.z, bI = I / 3, bJ = J / 3;
+        const int pI = bI == 0 ? 0 : (bI == ia ? 1 : (bI == ib ? 2 : -1));
+        const int pJ = bJ == 0 ? 0 : (bJ == ia ? 1 : (bJ == ib ? 2 : -1));
+        if (pI >= 0 && pJ >= 0) v = line_entry(sL[wl], 3 * pI + I % 3, 3 * pJ + J % 3);
+      } else {
+        v = plane_entry(sP[wl], Q, I, J);
+      }
+      val[k] = kpen * v / 2;
+      // the code of the pair, taken either way round (none: an anchored vertex)
+      const int q = sPos[wl][4 * bA + bB];
+      if (q >= 0) {
+        dst[k] = ICF_IMP_REC * (long long)q + 3 * r + cc;
+      } else if (bA != bB) {
+        const int q2 = sPos[wl][4 * bB + bA];
+        if (q2 >= 0) dst[k] = ICF_IMP_REC * (long long)q2 + 3 * cc + r;
+      }
     }
   }
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+    if (dst[k] >= 0) rec[dst[k]] = val[k];
   // vertex forces (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp, w = (1-s-t, s, t)
   // (collision_response.h:89-109): into the force record, and as the rhs of
   // the vertex's diagonal code

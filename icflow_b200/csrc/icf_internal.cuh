@@ -14,7 +14,8 @@
 //             cs[nc*48] double                    per CZ: 6 symmetric 3x3
 //                                                 blocks Kt[i][j] (i<=j, 6 each)
 //                                                 then rt[3][3], pad
-//             ks[ni*160] double                   per impact: 144 LHS + 12 rhs
+//             ks[ni*132] double                   per impact: the records of its
+//                                                 codes (<= 10 x 12) + 12 forces
 //   pattern   static keys (row<<32|col) sorted, rc_off[nnz_s+1], rc[] codes
 //             merged pattern rows/cols + src (static index of merged slot)
 //
@@ -38,7 +39,7 @@
 #define ICF_MAX_TET_UNITS (1 << 26)
 #define ICF_MAX_CZ_UNITS (1 << 24)
 #define ICF_CZ_STAGE 48   // doubles per CZ in the staging buffer
-#define ICF_IMP_STAGE 160 // doubles per impact in the staging buffer (allocation)
+#define ICF_IMP_STAGE 132 // doubles per impact in the staging buffer (allocation)
 // The staging buffer of n impacts holds, from the start, one record of
 // ICF_IMP_REC doubles per impact contribution code, at the code's position in
 // the slot-sorted list d_cr (the 3x3 block of the code's vertex pair, then the
@@ -46,6 +47,8 @@
 // impact), and from ICF_IMP_FORCE_AT * n the 12 vertex forces of every impact.
 #define ICF_IMP_REC 12
 #define ICF_IMP_FORCE_AT 120
+static_assert(ICF_IMP_FORCE_AT >= 10 * ICF_IMP_REC && ICF_IMP_STAGE >= ICF_IMP_FORCE_AT + 12,
+              "impact staging: 10 code records, then 12 vertex forces");
 __host__ __device__ inline double *icf_imp_forces(double *ks, long long n_imp) {
   return ks + (long long)ICF_IMP_FORCE_AT * n_imp;
 }
@@ -147,6 +150,9 @@ struct icf_contact_ws {
   int *gcnt = nullptr, *goff = nullptr, *gcur = nullptr;
   double4 *gnode = nullptr;
   long long cell_cap = 0, gnode_cap = 0;
+  // per surface node: hit counts, offsets, cursors (capacity kcap)
+  int *kcnt = nullptr, *koff = nullptr, *kcur = nullptr;
+  long long kcap = 0;
   // small device results and their pinned host copy: [0] unique count,
   // [1] impact list differs from the built one, [2] pairs before de-duplication
   int *d_small = nullptr, *h_small = nullptr;
@@ -316,6 +322,10 @@ struct icf_ctx {
   int *d_cr_slot = nullptr, *d_cr_off = nullptr;
   uint32_t *d_cr = nullptr;
   int cr_cap = 0;
+  // the touched slots' indices, those the off-diagonal gather does not write
+  // (diagonal and contact-only blocks, n_crs - n_crs_off) first, then the
+  // static off-diagonal ones: each k_imp_add launch covers its own range
+  int *d_cr_ord = nullptr;
   // position in d_cr of the code (impact u, vertices a, b) at 16 u + 4 a + b,
   // or -1 (no code: an anchored vertex, or the pair taken as (b, a))
   int *d_imp_pos = nullptr;

@@ -11,7 +11,7 @@
 // cudaFree or allocating library routine.
 //
 // The array's size is fixed at ICF_NOALLOC_BYTES (8 MiB).  A model whose
-// temporaries do not fit (80 B per node, 256 B per tet, 384 B per CZ, 1328 B
+// temporaries do not fit (80 B per node, 256 B per tet, 384 B per CZ, 1104 B
 // per impact, each section rounded up to 256 B) is rejected with
 // ICF_ERR_SIZE and a message giving both numbers.
 //

@@ -20,6 +20,8 @@
 // reference's _XtoDU, ImplicitModel3.cs:247-256).
 #include <cub/cub.cuh>
 
+#include <cstdio>
+
 #include <cmath>
 #include <string>
 
@@ -463,7 +465,11 @@ int icf_solve_impl(icf_ctx *ctx, double rel_tol, int max_iter, int *iters, doubl
   if (iters) *iters = it;
   if (relres) *relres = rel;
   if (rel > rel_tol && it >= max_iter)
+  {
+    char buf[64];
+    snprintf(buf, sizeof(buf), "%.3e", rel);
     return icf_fail(ctx, ICF_ERR_NUMERIC, "linear solve: no convergence in " + std::to_string(max_iter) +
-                                              " iterations (relative residual " + std::to_string(rel) + ")");
+                                              " iterations (relative residual " + buf + ")");
+  }
   return ICF_OK;
 }

@@ -3,24 +3,30 @@
 icFlow starts every Newton loop from du = v h (ImplicitModel3.cs:149-156).
 LearnedWarmStart replaces that guess for the active nodes with
 
-    du = v h + (du_{n-1} - du_{n-2}) + gain * out_scale * net(x),
-    x = (u, v, a, du_{n-1}, du_{n-2})
+    du = v h + (d1 - d2) + gain * out_scale * net(x),
+    x = (u, v, a, d1, d2)
 
-where net is the per-node MLP of the library (icf_mlp: 15 -> 64 -> 64 -> 3,
-GELU, BF16 weights, FP32 accumulation, trained on the GPU by the library's own
-forward and backward kernels).  Training data are the method's own
-trajectories: every accepted step contributes, per active node, the inputs
-seen at the start of the step and the correction the Newton loop found
-beyond the second-order extrapolation, du_accepted - v h - (du_{n-1} -
-du_{n-2}).  (With the reference's accept, v h = du_{n-1}, so the first two
-terms extrapolate the increments linearly.)  The network is trained per node
-on displacements, but what the Newton loop pays for is the force residual of
-the guess, and per-node prediction errors that are not spatially coherent
-cost far more force than they save displacement; `gain` is therefore
-calibrated on a separate trajectory by the first-iterate residual
-(calibrate) and may come out 0, leaving the extrapolation alone.  The plain
-guess v h stays the fallback and the judge: both run to the same residual
-tolerance.
+where d1, d2 are the increments of the two previous accepted steps, each
+scaled to the current step (du_k h / h_k; step control changes h), and net is
+the per-node MLP of the library (icf_mlp: 15 -> 64 -> 64 -> 3, GELU, BF16
+weights, FP32 accumulation, trained on the GPU by the library's own forward
+and backward kernels).  Training data are the method's own trajectories:
+every accepted step contributes, per active node, the inputs seen at the
+start of the step and the correction the Newton loop found beyond the
+extrapolation, du_accepted - v h - (d1 - d2).  (With the reference's accept,
+v h = du_{n-1} at a constant step, so the first two terms extrapolate the
+increments linearly.)
+
+The network is trained per node on displacements, but what the Newton loop
+pays for is the force residual of the guess: per-node errors that are not
+spatially coherent cost far more force than they save displacement, and
+where the extrapolation is already close (free flight, slow loading) any
+correction only adds error.  So the correction is judged before it is used:
+`calibrate` picks one gain from a separate trajectory, and with
+`select_gains` set each step picks the gain whose guess has the smallest
+residual (one assembly per candidate, gain 0 being the extrapolation alone).
+The plain guess v h stays the fallback and the judge: every arm runs to the
+same residual tolerance.
 """
 from __future__ import annotations
 
