@@ -211,7 +211,8 @@ static void free_all(icf_ctx *c) {
                   c->d_x0, c->d_xc, c->d_va, c->d_u, c->d_v, c->d_a, c->d_du, c->d_un, c->d_h3,
                   c->d_czs, c->d_czfail, c->d_cztent, c->d_czflags, c->d_czavg, c->d_czprm,
                   c->d_es, c->d_cs, c->d_ks, c->d_skeys, c->d_rc_off, c->d_rc, c->d_rows, c->d_cols,
-                  c->d_src, c->d_mkeys, c->d_imp, c->d_cr_slot, c->d_cr_off, c->d_cr, c->d_cr_ord, c->d_pairs,
+                  c->d_src, c->d_mkeys, c->d_imp, c->d_cr_slot, c->d_cr_off, c->d_cr, c->d_cr_range, c->d_cr_pslot,
+                  c->d_cr_row, c->d_pairs,
                   c->d_masks, c->d_imp_ci, c->d_imp_cd, c->d_rc_mid, c->d_diag, c->d_offd,
                   c->d_s2m, c->d_dynpos, c->d_gdesc_diag, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
                   c->imp_inc.off, c->imp_inc.inc, c->d_tmp, c->sell_off.meta, c->sell_off.unit,
@@ -425,7 +426,8 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->d_s2m = ctx->d_dynpos = nullptr; ctx->s2m_cap = ctx->dynpos_cap = ctx->n_dyn = 0;
   ctx->d_gdesc_diag = ctx->d_gdesc_off = nullptr; ctx->gdesc_cap = 0; ctx->d_skeys = nullptr; ctx->d_rc_off = nullptr; ctx->d_rc = nullptr;
   ctx->d_rows = ctx->d_cols = ctx->d_src = nullptr; ctx->rows_cap = ctx->cols_cap = 0; ctx->d_mkeys = nullptr;
-  ctx->d_imp = nullptr; ctx->imp_cap = 0; ctx->n_imp = 0; ctx->d_cr_slot = ctx->d_cr_off = ctx->d_cr_ord = nullptr;
+  ctx->d_imp = nullptr; ctx->imp_cap = 0; ctx->n_imp = 0; ctx->d_cr_slot = ctx->d_cr_off = nullptr;
+  ctx->d_cr_range = nullptr; ctx->d_cr_pslot = ctx->d_cr_row = nullptr;
   ctx->d_cr = nullptr; ctx->cr_cap = 0; ctx->n_crs = 0; ctx->d_pairs = ctx->d_masks = nullptr;
   ctx->pairs_cap = 0; ctx->n_pairs = 0; ctx->d_vals = ctx->d_rhs = ctx->d_nodeF = nullptr; ctx->vals_cap = 0;
   ctx->tet_inc = icf_node_inc(); ctx->imp_inc = icf_node_inc(); ctx->d_tmp = nullptr; ctx->tmp_bytes = 0;

@@ -403,43 +403,40 @@ __global__ void k_zero_dyn(int nd, const int *__restrict__ pos, double *__restri
 // Impact contributions, one thread per block they touch: the records of the
 // block's codes (k_imp_deriv writes them at the codes' positions in the
 // slot-sorted list, so a block's records are contiguous) are summed in code
-// order and added to the block, and to the rhs row for a diagonal block.
-__global__ void k_imp_add(int count, const int *__restrict__ ord, int first, const int *__restrict__ slot,
-                          const int *__restrict__ off, const int *__restrict__ cols, const double *__restrict__ rec,
-                          double *__restrict__ vals, double *__restrict__ rhs, int *__restrict__ nonfinite,
-                          const unsigned long long *__restrict__ mkey) {
-  // touched slot ord[first + t] (or first + t without an order)
+// order and added to the block, and to the rhs row for a diagonal block.  The
+// touched blocks come in k_imp_add's order (icf_pattern.cu k_split_off): the
+// launch over [first, first + count) reads its metadata contiguously.
+__global__ void k_imp_add(int count, int first, const int2 *__restrict__ range, const int *__restrict__ pslot,
+                          const int *__restrict__ row, const double *__restrict__ rec, double *__restrict__ vals,
+                          double *__restrict__ rhs, int *__restrict__ nonfinite) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   bool bad = false;
   if (t < count) {
-    const int w = ord ? ord[first + t] : first + t;
-    const int s = slot[w];
-    {
-      const int q0 = off[w], q1 = off[w + 1];
-      double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int q = q0; q < q1; q++) {
-        const double2 *R = reinterpret_cast<const double2 *>(rec + ICF_IMP_REC * (size_t)q);
+    const int w = first + t;
+    const int2 qr = range[w];
+    const int s = pslot[w], rw = row[w];
+    double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int q = qr.x; q < qr.y; q++) {
+      const double2 *R = reinterpret_cast<const double2 *>(rec + ICF_IMP_REC * (size_t)q);
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
-          const double2 r2 = __ldg(R + k);
-          v[2 * k] += r2.x;
-          v[2 * k + 1] += r2.y;
-        }
+      for (int k = 0; k < 6; k++) {
+        const double2 r2 = __ldg(R + k);
+        v[2 * k] += r2.x;
+        v[2 * k + 1] += r2.y;
       }
-      double *o = vals + 9 * (size_t)s;
+    }
+    double *o = vals + 9 * (size_t)s;
 #pragma unroll
-      for (int k = 0; k < 9; k++) {
-        o[k] += v[k];
-        bad |= !isfinite(v[k]);
-      }
-      const unsigned long long key = mkey[s];
-      if ((key >> 32) == (key & 0xffffffffull)) {
-        double *r = rhs + 3 * (size_t)cols[s];
+    for (int k = 0; k < 9; k++) {
+      o[k] += v[k];
+      bad |= !isfinite(v[k]);
+    }
+    if (rw >= 0) {
+      double *r = rhs + 3 * (size_t)rw;
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-          r[k] += v[9 + k];
-          bad |= !isfinite(v[9 + k]);
-        }
+      for (int k = 0; k < 3; k++) {
+        r[k] += v[9 + k];
+        bad |= !isfinite(v[9 + k]);
       }
     }
   }
@@ -950,16 +947,15 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   const int n_a = ctx->n_crs - ctx->n_crs_off;
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
   if (n_a > 0) {
-    k_imp_add<<<icf_blocks(n_a, 128), 128, 0, s>>>(n_a, ctx->d_cr_ord, 0, ctx->d_cr_slot, ctx->d_cr_off,
-                                                  ctx->d_cols, ctx->d_ks, ctx->d_vals, ctx->d_rhs,
-                                                  ctx->d_counts + 4, ctx->d_mkeys);
+    k_imp_add<<<icf_blocks(n_a, 128), 128, 0, s>>>(n_a, 0, ctx->d_cr_range, ctx->d_cr_pslot, ctx->d_cr_row,
+                                                  ctx->d_ks, ctx->d_vals, ctx->d_rhs, ctx->d_counts + 4);
     icf_prof_mark(ctx, s, "k_imp_add", imp_in * n_a / ctx->n_crs + 144LL * n_a);
   }
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   if (ctx->n_crs_off > 0 && ctx->n_crs > 0) {
-    k_imp_add<<<icf_blocks(ctx->n_crs_off, 128), 128, 0, s>>>(
-        ctx->n_crs_off, ctx->d_cr_ord, n_a, ctx->d_cr_slot, ctx->d_cr_off, ctx->d_cols, ctx->d_ks, ctx->d_vals,
-        ctx->d_rhs, ctx->d_counts + 4, ctx->d_mkeys);
+    k_imp_add<<<icf_blocks(ctx->n_crs_off, 128), 128, 0, s>>>(ctx->n_crs_off, n_a, ctx->d_cr_range,
+                                                              ctx->d_cr_pslot, ctx->d_cr_row, ctx->d_ks,
+                                                              ctx->d_vals, ctx->d_rhs, ctx->d_counts + 4);
     icf_prof_mark(ctx, s, "k_imp_add_off", imp_in * ctx->n_crs_off / ctx->n_crs + 144LL * ctx->n_crs_off);
   }
 
@@ -1205,9 +1201,8 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
                                           B.rhs, s));
   }
   if (ctx->n_crs > 0)
-    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, nullptr, 0, ctx->d_cr_slot, ctx->d_cr_off,
-                                                        ctx->d_cols, B.ks, B.vals, B.rhs, ctx->d_counts + 4,
-                                                        ctx->d_mkeys);
+    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, 0, ctx->d_cr_range, ctx->d_cr_pslot,
+                                                        ctx->d_cr_row, B.ks, B.vals, B.rhs, ctx->d_counts + 4);
 
   ICF_CUDA(ctx, cudaGetLastError());
   ICF_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));

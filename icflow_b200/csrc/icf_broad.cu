@@ -289,6 +289,43 @@ __global__ void k_node_put(int ns, const int *__restrict__ snode, const double4 
   if (off) ent[off[l] + w] = make_double4(P.x, P.y, P.z, (double)k);
 }
 
+// per surface element: the inverse of its edge matrix (as k_narrow computes
+// it) and its first vertex, 12 doubles
+__global__ void k_tet_inv(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
+                          double *__restrict__ inv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 id = selem[i];
+  const int nn[4] = {id.x, id.y, id.z, id.w};
+  double x[12];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const double4 p = xc[nn[k]];
+    x[3 * k] = p.x; x[3 * k + 1] = p.y; x[3 * k + 2] = p.z;
+  }
+  double b[9];
+  tet_inverse(x, b);
+  double2 *o = reinterpret_cast<double2 *>(inv + 12 * (size_t)i);
+  o[0] = make_double2(b[0], b[1]);
+  o[1] = make_double2(b[2], b[3]);
+  o[2] = make_double2(b[4], b[5]);
+  o[3] = make_double2(b[6], b[7]);
+  o[4] = make_double2(b[8], x[0]);
+  o[5] = make_double2(x[1], x[2]);
+}
+
+// some surface element holding surface node k forms a candidate pair with b
+// (only on a hit)
+__device__ __forceinline__ bool pair_exists(int k, int b, const int *__restrict__ sinc_off, const int *__restrict__ sinc,
+                                         const double *__restrict__ lohi, const int *__restrict__ group,
+                                         const int4 *__restrict__ selem, const double4 *__restrict__ xc) {
+  for (int q = sinc_off[k]; q < sinc_off[k + 1]; q++) {
+    const int a = sinc[q];
+    if (keep_pair(a < b ? a : b, a < b ? b : a, lohi, group, selem, xc)) return true;
+  }
+  return false;
+}
+
 // eight threads per surface element b, each taking every eighth cell its box
 // reaches: keys k << eb | b of its impacts (k the surface-node index) and a
 // count per surface node
@@ -299,20 +336,21 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
                                                 const int *__restrict__ sinc_off, const int *__restrict__ sinc,
                                                 const int *__restrict__ group, int eb,
                                                 unsigned long long *__restrict__ out, long long cap,
-                                                int *__restrict__ count, int *__restrict__ kcnt) {
+                                                int *__restrict__ count, int *__restrict__ kcnt,
+                                                const double *__restrict__ inv) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int b = (int)(t >> 3), g = (int)(t & 7);
   if (b >= n) return;
   const int4 B = selem[b];
   const int nb[4] = {B.x, B.y, B.z, B.w};
-  double x[12];
-#pragma unroll
-  for (int v = 0; v < 4; v++) {
-    const double4 q = xc[nb[v]];
-    x[3 * v] = q.x; x[3 * v + 1] = q.y; x[3 * v + 2] = q.z;
+  double bi[9], x0[3];
+  {
+    const double2 *r = reinterpret_cast<const double2 *>(inv + 12 * (size_t)b);
+    const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5];
+    bi[0] = r0.x; bi[1] = r0.y; bi[2] = r1.x; bi[3] = r1.y; bi[4] = r2.x; bi[5] = r2.y;
+    bi[6] = r3.x; bi[7] = r3.y; bi[8] = r4.x;
+    x0[0] = r4.y; x0[1] = r5.x; x0[2] = r5.y;
   }
-  double bi[9];
-  tet_inverse(x, bi);
   const double *lh = lohi + 6 * (size_t)b;
   const double lx = lh[0], ly = lh[1], lz = lh[2], hx = lh[3], hy = lh[4], hz = lh[5];
   const int4 c = clo[b];
@@ -328,13 +366,8 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
       const int k = (int)P.w;
       const int p = snode[k];
       if (p == nb[0] || p == nb[1] || p == nb[2] || p == nb[3]) continue;
-      if (!tet_contains(bi, P.x - x[0], P.y - x[1], P.z - x[2])) continue;
-      bool any = false;
-      for (int q = sinc_off[k]; q < sinc_off[k + 1] && !any; q++) {
-        const int a = sinc[q];
-        any = keep_pair(a < b ? a : b, a < b ? b : a, lohi, group, selem, xc);
-      }
-      if (!any) continue;
+      if (!tet_contains(bi, P.x - x0[0], P.y - x0[1], P.z - x0[2])) continue;
+      if (!pair_exists(k, b, sinc_off, sinc, lohi, group, selem, xc)) continue;
       const int w = atomicAdd(count, 1);
       atomicAdd(kcnt + k, 1);
       if (w < cap) out[w] = ((unsigned long long)(unsigned)k << eb) | (unsigned)b;
@@ -384,7 +417,7 @@ void icf_free_contact_ws(icf_ctx *ctx) {
   icf_contact_ws &W = ctx->cws;
   void *d[] = {W.lohi, W.ext, W.tmpv, W.red, W.bcnt, W.boff, W.clo, W.ek0, W.ek1, W.ee0, W.ee1, W.pc, W.po,
                W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small, W.gcnt, W.goff, W.gcur, W.gnode,
-               W.kcnt, W.koff, W.kcur};
+               W.kcnt, W.koff, W.kcur, W.tinv};
   for (void *q : d) cudaFree(q);
   cudaFreeHost(W.h_small);
   cudaFreeHost(W.h_red);
@@ -549,11 +582,16 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     ICF_TRY_RC(grow(ctx, &W.gnode, ns));
     W.gnode_cap = ns;
   }
+  if (n > W.tinv_cap) {
+    ICF_TRY_RC(grow(ctx, &W.tinv, 12LL * n));
+    W.tinv_cap = n;
+  }
   if (!W.tmpv) ICF_TRY_RC(grow(ctx, &W.tmpv, 8LL * (2 * ctx->n_sm + 1)));
   if (!W.red) ICF_TRY_RC(grow(ctx, &W.red, 8));
   k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext);
   k_red7<<<nbk, 256, 0, s>>>(n, W.lohi, W.ext, W.tmpv);
   k_red7_final<<<1, 256, 0, s>>>(nbk, n, W.tmpv, W.red);
+  k_tet_inv<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.tinv);
   ICF_CUDA(ctx, cudaMemcpyAsync(W.h_red, W.red, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaStreamSynchronize(s));
   double *h_red = W.h_red;
@@ -616,7 +654,7 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     ICF_CUDA(ctx, cudaMemsetAsync(W.kcnt, 0, sizeof(int) * (ns + 1LL), s));
     k_detect<<<icf_blocks(8LL * n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, ny, nz, W.goff,
                                                      W.gnode, ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, d_group, eb,
-                                                     W.nk0, W.nkey_cap, W.d_small + 5, W.kcnt);
+                                                     W.nk0, W.nkey_cap, W.d_small + 5, W.kcnt, W.tinv);
     ICF_CUDA(ctx, cudaGetLastError());
     ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 5, W.d_small + 5, sizeof(int), cudaMemcpyDeviceToHost, s));
     ICF_CUDA(ctx, cudaStreamSynchronize(s));

@@ -41,8 +41,15 @@ __device__ __forceinline__ double cA(int b) { return b == 0 ? 1.0 : (b == 1 ? -1
 __device__ __forceinline__ double cE0(int b) { return b == 2 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
 __device__ __forceinline__ double cE1(int b) { return b == 3 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
 
+// Interior region, per impact: the gradients of D and S, the rank-two part's
+// factors u = c1 gD + c3 gS, w = c3 gD + c5 gS (so that c1 gD gD^T + c3 (gD gS^T
+// + gS gD^T) + c5 gS gS^T = u gD^T + w gS^T), the Hessian blocks of S over
+// (e0, e0), (e1, e1), (e0, e1), and per vertex-block pair (bi, bj) the vector W
+// with HD's block = [W]x.
 struct PlaneSetup {
-  double gD[12], gS[12];
+  double gD[12], gS[12], u[12], w[12];
+  double h00[9], h11[9], h01[9];
+  double W[16][3];
 };
 
 struct LineSetup {
@@ -80,28 +87,15 @@ __device__ __forceinline__ double cross_entry(const double w[3], int ci, int cj)
   return ((cj - ci + 3) % 3 == 1) ? -wk : wk;
 }
 
-// Closed-form Hessian entry (I, J) of the squared distance to the plane.
-struct PlaneScalars {
-  double a[3], e0[3], e1[3], e00, e11, e01, c1, c2, c3, c4, c5;
-};
-__device__ __forceinline__ double plane_entry(const PlaneSetup &S, const PlaneScalars &Q, int I, int J) {
+// Closed-form Hessian entry (I, J) of the squared distance to the plane:
+// u_I gD_J + w_I gS_J + c2 HD_IJ + c4 HS_IJ.
+__device__ __forceinline__ double plane_entry(const PlaneSetup &S, double c2, double c4, int I, int J) {
   const int bi = I / 3, bj = J / 3, ci = I % 3, cj = J % 3;
-  const double ai = cA(bi), aj = cA(bj), pi0 = cE0(bi), pj0 = cE0(bj), pi1 = cE1(bi), pj1 = cE1(bj);
-  // HD: the block (bi, bj) is [W]x with W a signed sum of e1, e0 and a
-  const double al = ai * pj0 - pi0 * aj, be = ai * pj1 - pi1 * aj, ga = pi0 * pj1 - pi1 * pj0;
-  double W[3];
-#pragma unroll
-  for (int k = 0; k < 3; k++) W[k] = -Q.e1[k] * al + Q.e0[k] * be - Q.a[k] * ga;
-  const double hd = cross_entry(W, ci, cj);
-  // HS from S = |e0|^2 |e1|^2 - (e0.e1)^2
-  const double dl = ci == cj ? 1.0 : 0.0;
-  const double h00 = 2.0 * (Q.e11 * dl - Q.e1[ci] * Q.e1[cj]);
-  const double h11 = 2.0 * (Q.e00 * dl - Q.e0[ci] * Q.e0[cj]);
-  const double h01 = 4.0 * Q.e0[ci] * Q.e1[cj] - 2.0 * Q.e1[ci] * Q.e0[cj] - 2.0 * Q.e01 * dl;
-  const double h10 = 4.0 * Q.e0[cj] * Q.e1[ci] - 2.0 * Q.e1[cj] * Q.e0[ci] - 2.0 * Q.e01 * dl;
-  const double hs = pi0 * pj0 * h00 + pi1 * pj1 * h11 + pi0 * pj1 * h01 + pi1 * pj0 * h10;
-  const double gDi = S.gD[I], gDj = S.gD[J], gSi = S.gS[I], gSj = S.gS[J];
-  return Q.c1 * gDi * gDj + Q.c2 * hd + Q.c3 * (gDi * gSj + gSi * gDj) + Q.c4 * hs + Q.c5 * gSi * gSj;
+  const double pi0 = cE0(bi), pj0 = cE0(bj), pi1 = cE1(bi), pj1 = cE1(bj);
+  const double hd = cross_entry(S.W[4 * bi + bj], ci, cj);
+  const double hs = pi0 * pj0 * S.h00[3 * ci + cj] + pi1 * pj1 * S.h11[3 * ci + cj] +
+                    pi0 * pj1 * S.h01[3 * ci + cj] + pi1 * pj0 * S.h01[3 * cj + ci];
+  return S.u[I] * S.gD[J] + S.w[I] * S.gS[J] + c2 * hd + c4 * hs;
 }
 
 // record entry slot (0..89) -> vertex pair (bA <= bB) and entry (r, c) of
@@ -121,7 +115,6 @@ __global__ void __launch_bounds__(32 * WARPS)
                 const int4 *__restrict__ ci, const double4 *__restrict__ cd, double kpen,
                 const int *__restrict__ pos, double *__restrict__ rec, double *__restrict__ frc) {
   __shared__ PlaneSetup sP[WARPS];
-  __shared__ PlaneScalars sQ[WARPS];
   __shared__ LineSetup sL[WARPS];
   __shared__ double sx[WARPS][12];
   __shared__ double sfd[WARPS][3];
@@ -153,7 +146,7 @@ __global__ void __launch_bounds__(32 * WARPS)
   const double *x = sx[wl];
   const double hk = kpen * 0.5;
   const int kind = c.x;
-  PlaneScalars &Q = sQ[wl];
+  double c2 = 0, c4 = 0;  // interior: the scalars of HD and HS
   if (kind == 1) {  // vertex: d2 = |p - x_b|^2
     if (lane < 3) sfd[wl][lane] = 2 * (x[lane] - x[3 * c.z + lane]);
   } else if (kind == 2) {  // edge (ia nearer, ib)
@@ -207,29 +200,39 @@ __global__ void __launch_bounds__(32 * WARPS)
     const double D = a[0] * N[0] + a[1] * N[1] + a[2] * N[2];
     const double Sv = N[0] * N[0] + N[1] * N[1] + N[2] * N[2];
     const double iS = 1.0 / Sv;
-    if (lane == 0) {
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        Q.a[k] = a[k];
-        Q.e0[k] = e0[k];
-        Q.e1[k] = e1[k];
-      }
-      Q.e00 = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
-      Q.e11 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
-      Q.e01 = e0[0] * e1[0] + e0[1] * e1[1] + e0[2] * e1[2];
-      Q.c1 = 2.0 * iS;
-      Q.c2 = 2.0 * D * iS;
-      Q.c3 = -2.0 * D * iS * iS;
-      Q.c4 = -D * D * iS * iS;
-      Q.c5 = 2.0 * D * D * iS * iS * iS;
-    }
+    const double c1 = 2.0 * iS, c3 = -2.0 * D * iS * iS, c5 = 2.0 * D * D * iS * iS * iS;
+    c2 = 2.0 * D * iS;
+    c4 = -D * D * iS * iS;
     if (lane < 12) {
       const int b = lane / 3, k = lane % 3;
-      S.gD[lane] = cA(b) * pick3(N, k) + cE0(b) * pick3(e1xa, k) + cE1(b) * pick3(axe0, k);
-      S.gS[lane] = 2.0 * (cE0(b) * pick3(e1xN, k) + cE1(b) * pick3(Nxe0, k));
+      const double gd = cA(b) * pick3(N, k) + cE0(b) * pick3(e1xa, k) + cE1(b) * pick3(axe0, k);
+      const double gs = 2.0 * (cE0(b) * pick3(e1xN, k) + cE1(b) * pick3(Nxe0, k));
+      S.gD[lane] = gd;
+      S.gS[lane] = gs;
+      S.u[lane] = c1 * gd + c3 * gs;
+      S.w[lane] = c3 * gd + c5 * gs;
+    } else if (lane < 21) {  // HS blocks, S = |e0|^2 |e1|^2 - (e0.e1)^2
+      const int r = (lane - 12) / 3, q = (lane - 12) % 3;
+      const double dl = r == q ? 1.0 : 0.0;
+      const double e00 = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
+      const double e11 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+      const double e01 = e0[0] * e1[0] + e0[1] * e1[1] + e0[2] * e1[2];
+      const double e0r = pick3(e0, r), e0q = pick3(e0, q), e1r = pick3(e1, r), e1q = pick3(e1, q);
+      S.h00[3 * r + q] = 2.0 * (e11 * dl - e1r * e1q);
+      S.h11[3 * r + q] = 2.0 * (e00 * dl - e0r * e0q);
+      S.h01[3 * r + q] = 4.0 * e0r * e1q - 2.0 * e1r * e0q - 2.0 * e01 * dl;
+    }
+    // W per vertex-block pair: D is trilinear in (a, e0, e1), so HD's block
+    // (bi, bj) is [W]x, W = -e1 (ai pj0 - pi0 aj) + e0 (ai pj1 - pi1 aj)
+    // - a (pi0 pj1 - pi1 pj0)
+    for (int l = lane; l < 48; l += 32) {
+      const int pr = l / 3, k = l % 3, bi = pr / 4, bj = pr % 4;
+      const double ai = cA(bi), aj = cA(bj), pi0 = cE0(bi), pj0 = cE0(bj), pi1 = cE1(bi), pj1 = cE1(bj);
+      const double al = ai * pj0 - pi0 * aj, be = ai * pj1 - pi1 * aj, ga = pi0 * pj1 - pi1 * pj0;
+      S.W[pr][k] = -pick3(e1, k) * al + pick3(e0, k) * be - pick3(a, k) * ga;
     }
     // d(d2)/dp = 2 D N / S
-    if (lane < 3) sfd[wl][lane] = (2.0 * D * iS) * pick3(N, lane);
+    if (lane < 3) sfd[wl][lane] = c2 * pick3(N, lane);
   }
   __syncwarp();
   // one lane per record entry: pair (bA, bB), entry (r, c); the three
@@ -261,7 +264,7 @@ __global__ void __launch_bounds__(32 * WARPS)
         const int pJ = bJ == 0 ? 0 : (bJ == ia ? 1 : (bJ == ib ? 2 : -1));
         if (pI >= 0 && pJ >= 0) v = line_entry(sL[wl], 3 * pI + I % 3, 3 * pJ + J % 3);
       } else {
-        v = plane_entry(sP[wl], Q, I, J);
+        v = plane_entry(sP[wl], c2, c4, I, J);
       }
       val[k] = kpen * v / 2;
       // the code of the pair, taken either way round (none: an anchored vertex)

@@ -153,6 +153,9 @@ struct icf_contact_ws {
   // per surface node: hit counts, offsets, cursors (capacity kcap)
   int *kcnt = nullptr, *koff = nullptr, *kcur = nullptr;
   long long kcap = 0;
+  // per surface element: edge-matrix inverse and first vertex (12 doubles)
+  double *tinv = nullptr;
+  long long tinv_cap = 0;
   // small device results and their pinned host copy: [0] unique count,
   // [1] impact list differs from the built one, [2] pairs before de-duplication
   int *d_small = nullptr, *h_small = nullptr;
@@ -322,10 +325,13 @@ struct icf_ctx {
   int *d_cr_slot = nullptr, *d_cr_off = nullptr;
   uint32_t *d_cr = nullptr;
   int cr_cap = 0;
-  // the touched slots' indices, those the off-diagonal gather does not write
-  // (diagonal and contact-only blocks, n_crs - n_crs_off) first, then the
-  // static off-diagonal ones: each k_imp_add launch covers its own range
-  int *d_cr_ord = nullptr;
+  // the touched slots in k_imp_add's order: those the off-diagonal gather
+  // does not write (diagonal and contact-only blocks, n_crs - n_crs_off)
+  // first, then the static off-diagonal ones, so that each k_imp_add launch
+  // covers its own contiguous range: per slot its records' range in d_cr,
+  // the slot and, for a diagonal block, its rhs row (else -1)
+  int2 *d_cr_range = nullptr;
+  int *d_cr_pslot = nullptr, *d_cr_row = nullptr;
   // position in d_cr of the code (impact u, vertices a, b) at 16 u + 4 a + b,
   // or -1 (no code: an anchored vertex, or the pair taken as (b, a))
   int *d_imp_pos = nullptr;

@@ -284,17 +284,23 @@ __global__ void k_count_off_static(int n, const int *__restrict__ slot, const un
   if ((threadIdx.x & 31) == 0 && m) atomicAdd(out, __popc(m));
 }
 
-// the touched slots split: diagonal and contact-only blocks at [0, n_a), the
-// static off-diagonal ones at [n_a, n) (order within each part free: every
-// slot is its own block)
-__global__ void k_split_off(int n, int n_a, const int *__restrict__ slot, const unsigned long long *__restrict__ mkey,
-                            const int *__restrict__ src, int identity, int *__restrict__ cur,
-                            int *__restrict__ ord) {
+// the touched slots in k_imp_add's order: diagonal and contact-only blocks at
+// [0, n_a), the static off-diagonal ones at [n_a, n) (order within each part
+// free: every slot is its own block); per slot its record range, slot and rhs
+// row (diagonal blocks) or -1
+__global__ void k_split_off(int n, int n_a, const int *__restrict__ slot, const int *__restrict__ off,
+                            const unsigned long long *__restrict__ mkey, const int *__restrict__ src, int identity,
+                            int *__restrict__ cur, int2 *__restrict__ range, int *__restrict__ pslot,
+                            int *__restrict__ row) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n) return;
-  const bool f = icf_off_static(mkey, src, identity, slot[g]);
+  const int sl = slot[g];
+  const bool f = icf_off_static(mkey, src, identity, sl);
   const int p = f ? n_a + atomicAdd(cur + 1, 1) : atomicAdd(cur, 1);
-  ord[p] = g;
+  range[p] = make_int2(off[g], off[g + 1]);
+  pslot[p] = sl;
+  const unsigned long long k = mkey[sl];
+  row[p] = (k >> 32) == (k & 0xffffffffull) ? (int)(k & 0xffffffffull) : -1;
 }
 
 __global__ void k_cand_imp_rc(int ni, const int4 *__restrict__ imp, const int *__restrict__ alt,
@@ -870,14 +876,20 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
       cudaFree(ctx->d_cr);
       cudaFree(ctx->d_cr_slot);
       cudaFree(ctx->d_cr_off);
-      cudaFree(ctx->d_cr_ord);
+      cudaFree(ctx->d_cr_range);
+      cudaFree(ctx->d_cr_pslot);
+      cudaFree(ctx->d_cr_row);
       ctx->d_cr = nullptr;
-      ctx->d_cr_slot = ctx->d_cr_off = ctx->d_cr_ord = nullptr;
+      ctx->d_cr_slot = ctx->d_cr_off = nullptr;
+      ctx->d_cr_range = nullptr;
+      ctx->d_cr_pslot = ctx->d_cr_row = nullptr;
       const long long cap = 2LL * n + 2;
       ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr, sizeof(uint32_t) * (size_t)cap));
       ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr_slot, sizeof(int) * (size_t)cap));
       ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr_off, sizeof(int) * (size_t)cap));
-      ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr_ord, sizeof(int) * (size_t)cap));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr_range, sizeof(int2) * (size_t)cap));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr_pslot, sizeof(int) * (size_t)cap));
+      ICF_CUDA(ctx, cudaMalloc(&ctx->d_cr_row, sizeof(int) * (size_t)cap));
       ctx->cr_cap = (int)cap;
     }
     k_cand_imp_rc<<<icf_blocks(ctx->n_imp, 128), 128, 0, s>>>(ctx->n_imp, ctx->d_imp, ctx->d_alt,
@@ -936,8 +948,9 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
       ICF_CUDA(ctx, cudaMallocAsync(&d_cur, 2 * sizeof(int), s));
       ICF_CUDA(ctx, cudaMemsetAsync(d_cur, 0, 2 * sizeof(int), s));
       k_split_off<<<icf_blocks(nvalid, 256), 256, 0, s>>>(nvalid, nvalid - ctx->n_crs_off, ctx->d_cr_slot,
-                                                           ctx->d_mkeys, ctx->d_src, ctx->src_identity ? 1 : 0,
-                                                           d_cur, ctx->d_cr_ord);
+                                                           ctx->d_cr_off, ctx->d_mkeys, ctx->d_src,
+                                                           ctx->src_identity ? 1 : 0, d_cur, ctx->d_cr_range,
+                                                           ctx->d_cr_pslot, ctx->d_cr_row);
       ICF_CUDA(ctx, cudaGetLastError());
       ICF_CUDA(ctx, cudaFreeAsync(d_cur, s));
     }

@@ -253,6 +253,18 @@ def test_structure_kept_for_the_same_impacts(O):
     d = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, pairs=pairs)
     for k in ("rows", "cols", "vals", "rhs"):
         assert np.array_equal(a[k], d[k]), k
+    # the list grows past the impact buffer (which is then reallocated) and
+    # returns to a list a structure was built from: the structure (and the
+    # captured graph, which holds the buffer's address) must be rebuilt
+    imps = gf.c_itet.copy()
+    small = imps[: max(1, len(imps) // 8)]
+    f = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, impacts=small)
+    big = np.concatenate([imps] * 32)  # repeats are allowed; beyond the buffer's capacity
+    gpu_assemble(gf, coll, state, H, pmax, tmax, failed, impacts=big)
+    f2 = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, impacts=small)
+    for k in ("rows", "cols", "vals", "rhs"):
+        assert np.array_equal(f[k], f2[k]), k
+    compare(f2, oracle_assemble(O, p, coll, state, H, pmax, tmax, small))
     # contact ends: an empty list after impacts whose blocks the off-diagonal
     # gather also writes (the impact-add launches must all go)
     e = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, impacts=np.zeros((0, 4), np.int32))
