@@ -343,14 +343,6 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
   if (b >= n) return;
   const int4 B = selem[b];
   const int nb[4] = {B.x, B.y, B.z, B.w};
-  double bi[9], x0[3];
-  {
-    const double2 *r = reinterpret_cast<const double2 *>(inv + 12 * (size_t)b);
-    const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5];
-    bi[0] = r0.x; bi[1] = r0.y; bi[2] = r1.x; bi[3] = r1.y; bi[4] = r2.x; bi[5] = r2.y;
-    bi[6] = r3.x; bi[7] = r3.y; bi[8] = r4.x;
-    x0[0] = r4.y; x0[1] = r5.x; x0[2] = r5.y;
-  }
   const double *lh = lohi + 6 * (size_t)b;
   const double lx = lh[0], ly = lh[1], lz = lh[2], hx = lh[3], hy = lh[4], hz = lh[5];
   const int4 c = clo[b];
@@ -366,6 +358,15 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
       const int k = (int)P.w;
       const int p = snode[k];
       if (p == nb[0] || p == nb[1] || p == nb[2] || p == nb[3]) continue;
+      // b's inverse and first vertex, read when a node lies in its box
+      double bi[9], x0[3];
+      {
+        const double2 *r = reinterpret_cast<const double2 *>(inv + 12 * (size_t)b);
+        const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5];
+        bi[0] = r0.x; bi[1] = r0.y; bi[2] = r1.x; bi[3] = r1.y; bi[4] = r2.x; bi[5] = r2.y;
+        bi[6] = r3.x; bi[7] = r3.y; bi[8] = r4.x;
+        x0[0] = r4.y; x0[1] = r5.x; x0[2] = r5.y;
+      }
       if (!tet_contains(bi, P.x - x0[0], P.y - x0[1], P.z - x0[2])) continue;
       if (!pair_exists(k, b, sinc_off, sinc, lohi, group, selem, xc)) continue;
       const int w = atomicAdd(count, 1);

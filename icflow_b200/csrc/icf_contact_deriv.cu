@@ -1,4 +1,4 @@
-// icf_contact_deriv.cu -- penalty response of the impacts, one warp per impact.
+// icf_contact_deriv.cu -- penalty response of the impacts, two impacts per warp.
 //
 // kCollisionResponseForce (collision_response.h:38-127) needs the gradient
 // and Hessian of the squared point-triangle distance d2(x), x = (p, v0, v1,
@@ -20,7 +20,7 @@
 // entry instead of some 200; the two forms agree to rounding (1e-14 of the
 // largest entry on random interior cases).
 //
-// The 32 lanes of a warp share the per-impact setup through shared memory.
+// Sixteen lanes share an impact's setup through shared memory.
 // The Hessian K = k/2 d2'' goes straight to the records of the impact's
 // contribution codes, at their positions in the slot-sorted list
 // (icf_internal.cuh, ICF_IMP_REC): a lane per record entry (10 vertex pairs x
@@ -49,7 +49,7 @@ __device__ __forceinline__ double cE1(int b) { return b == 3 ? 1.0 : (b == 1 ? -
 struct PlaneSetup {
   double gD[12], gS[12], u[12], w[12];
   double h00[9], h11[9], h01[9];
-  double W[16][3];
+  double W[48];  // [3 (4 bi + bj) + k]
 };
 
 struct LineSetup {
@@ -80,79 +80,119 @@ __device__ double line_entry(const LineSetup &L, int i, int j) {
 // component k of a 3-vector held in registers (selects, no local memory)
 __device__ __forceinline__ double pick3(const double v[3], int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
 
-// Entry (ci, cj) of the cross-product matrix [w]x (w x y = [w]x y).
-__device__ __forceinline__ double cross_entry(const double w[3], int ci, int cj) {
-  if (ci == cj) return 0.0;
-  const double wk = pick3(w, 3 - ci - cj);
-  return ((cj - ci + 3) % 3 == 1) ? -wk : wk;
-}
 
-// Closed-form Hessian entry (I, J) of the squared distance to the plane:
-// u_I gD_J + w_I gS_J + c2 HD_IJ + c4 HS_IJ.
-__device__ __forceinline__ double plane_entry(const PlaneSetup &S, double c2, double c4, int I, int J) {
-  const int bi = I / 3, bj = J / 3, ci = I % 3, cj = J % 3;
-  const double pi0 = cE0(bi), pj0 = cE0(bj), pi1 = cE1(bi), pj1 = cE1(bj);
-  const double hd = cross_entry(S.W[4 * bi + bj], ci, cj);
-  const double hs = pi0 * pj0 * S.h00[3 * ci + cj] + pi1 * pj1 * S.h11[3 * ci + cj] +
-                    pi0 * pj1 * S.h01[3 * ci + cj] + pi1 * pj0 * S.h01[3 * cj + ci];
+// Record entry slots (0..89): vertex pair (bA <= bB; the four diagonal
+// pairs, then the six off-diagonal ones) and entry (r, c) of its 3x3 block.
+// Everything an entry needs that depends on the slot alone is tabulated at
+// compile time (kSlots):
+//   a: I | J << 4 (the evaluated entry, I <= J: a diagonal block's lower
+//      entries are taken at their mirror) | HD's index in W (3 (4 bi + bj) +
+//      k) << 8 | (HD's sign + 1) << 14
+//   b: 3 ci + cj | (3 cj + ci) << 4 | the coefficients + 1 of HS's four
+//      terms (pi0 pj0, pi1 pj1, pi0 pj1, pi1 pj0) << 8, 10, 12, 14
+//   c: the code index of (bA, bB) | of (bB, bA) << 4 | offset 3 r + c in the
+//      first's record << 8 | 3 c + r in the second's << 12
+//   d: r | c << 2 | bA << 4 | bB << 6
+struct SlotMeta {
+  int a, b, c, d;
+};
+struct SlotTable {
+  SlotMeta s[90];
+};
+constexpr int cst_cE0(int b) { return b == 2 ? 1 : (b == 1 ? -1 : 0); }
+constexpr int cst_cE1(int b) { return b == 3 ? 1 : (b == 1 ? -1 : 0); }
+constexpr SlotTable make_slot_table() {
+  SlotTable t{};
+  const int PA[10] = {0, 1, 2, 3, 0, 0, 0, 1, 1, 2}, PB[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+  for (int sl = 0; sl < 90; sl++) {
+    const int pi = sl / 9, e = sl % 9, bA = PA[pi], bB = PB[pi], r = e / 3, c = e % 3;
+    int I = 3 * bA + r, J = 3 * bB + c;
+    if (I > J) {
+      const int x = I;
+      I = J;
+      J = x;
+    }
+    const int bi = I / 3, bj = J / 3, ci = I % 3, cj = J % 3;
+    int hdk = 0, hds = 0;  // sign 0: HD's entry is zero (ci == cj)
+    if (ci != cj) {
+      hdk = 3 - ci - cj;
+      hds = ((cj - ci + 3) % 3 == 1) ? -1 : 1;
+    }
+    const int q00 = cst_cE0(bi) * cst_cE0(bj), q11 = cst_cE1(bi) * cst_cE1(bj);
+    const int q01 = cst_cE0(bi) * cst_cE1(bj), q10 = cst_cE1(bi) * cst_cE0(bj);
+    t.s[sl].a = I | (J << 4) | ((3 * (4 * bi + bj) + hdk) << 8) | ((hds + 1) << 14);
+    t.s[sl].b = (3 * ci + cj) | ((3 * cj + ci) << 4) | ((q00 + 1) << 8) | ((q11 + 1) << 10) | ((q01 + 1) << 12) |
+                ((q10 + 1) << 14);
+    t.s[sl].c = (4 * bA + bB) | ((4 * bB + bA) << 4) | ((3 * r + c) << 8) | ((3 * c + r) << 12);
+    t.s[sl].d = r | (c << 2) | (bA << 4) | (bB << 6);
+  }
+  return t;
+}
+__device__ const SlotTable kSlots = make_slot_table();
+
+// the interior entry of a slot: u_I gD_J + w_I gS_J + c2 HD_IJ + c4 HS_IJ
+__device__ __forceinline__ double plane_slot(const PlaneSetup &S, double c2, double c4, const SlotMeta &m) {
+  const int I = m.a & 15, J = (m.a >> 4) & 15;
+  const double hd = S.W[(m.a >> 8) & 63] * (double)(((m.a >> 14) & 3) - 1);
+  const int ix = m.b & 15, ixt = (m.b >> 4) & 15;
+  const double hs = (double)(((m.b >> 8) & 3) - 1) * S.h00[ix] + (double)(((m.b >> 10) & 3) - 1) * S.h11[ix] +
+                    (double)(((m.b >> 12) & 3) - 1) * S.h01[ix] + (double)(((m.b >> 14) & 3) - 1) * S.h01[ixt];
   return S.u[I] * S.gD[J] + S.w[I] * S.gS[J] + c2 * hd + c4 * hs;
 }
 
-// record entry slot (0..89) -> vertex pair (bA <= bB) and entry (r, c) of
-// its 3x3 block: the four diagonal pairs, then the six off-diagonal ones
-__constant__ int kPairA[10] = {0, 1, 2, 3, 0, 0, 0, 1, 1, 2};
-__constant__ int kPairB[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
-__device__ __forceinline__ void slot_entry(int sl, int &bA, int &bB, int &r, int &c) {
-  const int pi = sl / 9, e = sl % 9;
-  bA = kPairA[pi];
-  bB = kPairB[pi];
-  r = e / 3;
-  c = e % 3;
-}
+// Sixteen lanes per impact (two impacts per warp): every warp instruction of
+// the per-impact setup serves two impacts, and twice as many impacts' loads
+// are in flight per SM.  Group-local synchronisation only (the two halves of a
+// warp may take different branches).
+constexpr int GL = 32;                // lanes per impact
+constexpr int GPW = 32 / GL;          // impacts per warp
+constexpr int GROUPS = WARPS * GPW;   // impacts per block
 
 __global__ void __launch_bounds__(32 * WARPS)
     k_imp_deriv(int n, const int4 *__restrict__ imp, const double4 *__restrict__ xc,
                 const int4 *__restrict__ ci, const double4 *__restrict__ cd, double kpen,
                 const int *__restrict__ pos, double *__restrict__ rec, double *__restrict__ frc) {
-  __shared__ PlaneSetup sP[WARPS];
-  __shared__ LineSetup sL[WARPS];
-  __shared__ double sx[WARPS][12];
-  __shared__ double sfd[WARPS][3];
-  __shared__ int sPos[WARPS][16];
-  const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int u = blockIdx.x * WARPS + wl;
-  if (u >= n) return;  // uniform per warp
+  __shared__ PlaneSetup sP[GROUPS];
+  __shared__ LineSetup sL[GROUPS];
+  __shared__ double sx[GROUPS][12];
+  __shared__ double sfd[GROUPS][3];
+  __shared__ int sPos[GROUPS][16];
+  const int lane = threadIdx.x & 31;
+  const int gi = threadIdx.x / GL, gl = threadIdx.x % GL;  // group in the block, lane in the group
+  const unsigned gmask = (GL == 32) ? 0xffffffffu : (((1u << GL) - 1u) << (lane & ~(GL - 1)));
+  const int u = blockIdx.x * GROUPS + gi;
+  if (u >= n) return;  // uniform per group
   const int *P = pos + 16 * (size_t)u;
   const int4 c = ci[u];
-  if (lane < 16) sPos[wl][lane] = P[lane];
+  for (int l = gl; l < 16; l += GL) sPos[gi][l] = P[l];
   if (c.x < 0) {  // no response: zero records, zero forces
-    for (int e = lane; e < 16 * ICF_IMP_REC; e += 32) {
+    for (int e = gl; e < 16 * ICF_IMP_REC; e += GL) {
       const int q = P[e / ICF_IMP_REC];
       if (q >= 0) rec[ICF_IMP_REC * (size_t)q + e % ICF_IMP_REC] = 0.0;
     }
-    if (lane < 12) frc[12 * (size_t)u + lane] = 0.0;
+    for (int l = gl; l < 12; l += GL) frc[12 * (size_t)u + l] = 0.0;
     return;
   }
   const double4 cl = cd[u];
   const int4 id = imp[u];
-  if (lane < 4) {
-    const int nd = lane == 0 ? id.x : lane == 1 ? id.y : lane == 2 ? id.z : id.w;
+  if (gl < 4) {
+    const int nd = gl == 0 ? id.x : gl == 1 ? id.y : gl == 2 ? id.z : id.w;
     const double4 p = xc[nd];
-    sx[wl][3 * lane] = p.x;
-    sx[wl][3 * lane + 1] = p.y;
-    sx[wl][3 * lane + 2] = p.z;
+    sx[gi][3 * gl] = p.x;
+    sx[gi][3 * gl + 1] = p.y;
+    sx[gi][3 * gl + 2] = p.z;
   }
-  __syncwarp();
-  const double *x = sx[wl];
+  __syncwarp(gmask);
+  const double *x = sx[gi];
   const double hk = kpen * 0.5;
   const int kind = c.x;
   double c2 = 0, c4 = 0;  // interior: the scalars of HD and HS
   if (kind == 1) {  // vertex: d2 = |p - x_b|^2
-    if (lane < 3) sfd[wl][lane] = 2 * (x[lane] - x[3 * c.z + lane]);
+    if (gl < 3) sfd[gi][gl] = 2 * (x[gl] - x[3 * c.z + gl]);
   } else if (kind == 2) {  // edge (ia nearer, ib)
     const int ia = c.y, ib = c.z;
-    LineSetup &L = sL[wl];
-    if (lane == 0) {
+    LineSetup &L = sL[gi];
+    if (gl == 0) {
       const double *Pp = x, *Q1 = x + 3 * ia, *Q2 = x + 3 * ib;
       double sp = 0, f2 = 0;
       for (int k = 0; k < 3; k++) {
@@ -176,10 +216,10 @@ __global__ void __launch_bounds__(32 * WARPS)
       L.f2cu = L.f2sq * f2;
       for (int i = 0; i < 9; i++) L.gd[i] = 2 * sp * L.spd[i];
       for (int k = 0; k < 3; k++)
-        sfd[wl][k] = L.f1d[k] + (L.g * L.f2d[k] - L.f2 * L.gd[k]) / L.f2sq;
+        sfd[gi][k] = L.f1d[k] + (L.g * L.f2d[k] - L.f2 * L.gd[k]) / L.f2sq;
     }
   } else {  // interior: d2 = D^2 / S
-    PlaneSetup &S = sP[wl];
+    PlaneSetup &S = sP[gi];
     double a[3], e0[3], e1[3], N[3], e1xa[3], axe0[3], e1xN[3], Nxe0[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -203,57 +243,56 @@ __global__ void __launch_bounds__(32 * WARPS)
     const double c1 = 2.0 * iS, c3 = -2.0 * D * iS * iS, c5 = 2.0 * D * D * iS * iS * iS;
     c2 = 2.0 * D * iS;
     c4 = -D * D * iS * iS;
-    if (lane < 12) {
-      const int b = lane / 3, k = lane % 3;
+    for (int l = gl; l < 12; l += GL) {
+      const int b = l / 3, k = l % 3;
       const double gd = cA(b) * pick3(N, k) + cE0(b) * pick3(e1xa, k) + cE1(b) * pick3(axe0, k);
       const double gs = 2.0 * (cE0(b) * pick3(e1xN, k) + cE1(b) * pick3(Nxe0, k));
-      S.gD[lane] = gd;
-      S.gS[lane] = gs;
-      S.u[lane] = c1 * gd + c3 * gs;
-      S.w[lane] = c3 * gd + c5 * gs;
-    } else if (lane < 21) {  // HS blocks, S = |e0|^2 |e1|^2 - (e0.e1)^2
-      const int r = (lane - 12) / 3, q = (lane - 12) % 3;
-      const double dl = r == q ? 1.0 : 0.0;
+      S.gD[l] = gd;
+      S.gS[l] = gs;
+      S.u[l] = c1 * gd + c3 * gs;
+      S.w[l] = c3 * gd + c5 * gs;
+    }
+    // HS blocks, S = |e0|^2 |e1|^2 - (e0.e1)^2
+    {
       const double e00 = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
       const double e11 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
       const double e01 = e0[0] * e1[0] + e0[1] * e1[1] + e0[2] * e1[2];
-      const double e0r = pick3(e0, r), e0q = pick3(e0, q), e1r = pick3(e1, r), e1q = pick3(e1, q);
-      S.h00[3 * r + q] = 2.0 * (e11 * dl - e1r * e1q);
-      S.h11[3 * r + q] = 2.0 * (e00 * dl - e0r * e0q);
-      S.h01[3 * r + q] = 4.0 * e0r * e1q - 2.0 * e1r * e0q - 2.0 * e01 * dl;
+      for (int l = gl; l < 9; l += GL) {
+        const int r = l / 3, q = l % 3;
+        const double dl = r == q ? 1.0 : 0.0;
+        const double e0r = pick3(e0, r), e0q = pick3(e0, q), e1r = pick3(e1, r), e1q = pick3(e1, q);
+        S.h00[l] = 2.0 * (e11 * dl - e1r * e1q);
+        S.h11[l] = 2.0 * (e00 * dl - e0r * e0q);
+        S.h01[l] = 4.0 * e0r * e1q - 2.0 * e1r * e0q - 2.0 * e01 * dl;
+      }
     }
     // W per vertex-block pair: D is trilinear in (a, e0, e1), so HD's block
     // (bi, bj) is [W]x, W = -e1 (ai pj0 - pi0 aj) + e0 (ai pj1 - pi1 aj)
     // - a (pi0 pj1 - pi1 pj0)
-    for (int l = lane; l < 48; l += 32) {
+    for (int l = gl; l < 48; l += GL) {
       const int pr = l / 3, k = l % 3, bi = pr / 4, bj = pr % 4;
       const double ai = cA(bi), aj = cA(bj), pi0 = cE0(bi), pj0 = cE0(bj), pi1 = cE1(bi), pj1 = cE1(bj);
       const double al = ai * pj0 - pi0 * aj, be = ai * pj1 - pi1 * aj, ga = pi0 * pj1 - pi1 * pj0;
-      S.W[pr][k] = -pick3(e1, k) * al + pick3(e0, k) * be - pick3(a, k) * ga;
+      S.W[l] = -pick3(e1, k) * al + pick3(e0, k) * be - pick3(a, k) * ga;
     }
     // d(d2)/dp = 2 D N / S
-    if (lane < 3) sfd[wl][lane] = c2 * pick3(N, lane);
+    if (gl < 3) sfd[gi][gl] = c2 * pick3(N, gl);
   }
-  __syncwarp();
-  // one lane per record entry: pair (bA, bB), entry (r, c); the three
-  // entries of a lane are computed first and stored after, so that their
-  // shared-memory reads overlap
-  double val[3];
-  long long dst[3];
+  __syncwarp(gmask);
+  // one lane per record entry: pair (bA, bB), entry (r, c); a lane's entries
+  // are computed first and stored after, so that their shared-memory reads
+  // overlap
+  constexpr int NS = (90 + GL - 1) / GL;
+  double val[NS];
+  long long dst[NS];
 #pragma unroll
-  for (int k = 0; k < 3; k++) {
-    const int sl = lane + 32 * k;
+  for (int k = 0; k < NS; k++) {
+    const int sl = gl + GL * k;
     val[k] = 0.0;
     dst[k] = -1;
     if (sl < 90) {
-      int bA, bB, r, cc;
-      slot_entry(sl, bA, bB, r, cc);
-      int I = 3 * bA + r, J = 3 * bB + cc;
-      if (I > J) {  // lower entry of a diagonal block: its mirror
-        const int t = I;
-        I = J;
-        J = t;
-      }
+      const SlotMeta m = kSlots.s[sl];
+      const int I = m.a & 15, J = (m.a >> 4) & 15;
       double v = 0;
       if (kind == 1) {
         const int vb = c.z, bI = I / 3, bJ = J / 3;
@@ -262,38 +301,38 @@ __global__ void __launch_bounds__(32 * WARPS)
         const int ia = c.y, ib = c.z, bI = I / 3, bJ = J / 3;
         const int pI = bI == 0 ? 0 : (bI == ia ? 1 : (bI == ib ? 2 : -1));
         const int pJ = bJ == 0 ? 0 : (bJ == ia ? 1 : (bJ == ib ? 2 : -1));
-        if (pI >= 0 && pJ >= 0) v = line_entry(sL[wl], 3 * pI + I % 3, 3 * pJ + J % 3);
+        if (pI >= 0 && pJ >= 0) v = line_entry(sL[gi], 3 * pI + I % 3, 3 * pJ + J % 3);
       } else {
-        v = plane_entry(sP[wl], c2, c4, I, J);
+        v = plane_slot(sP[gi], c2, c4, m);
       }
       val[k] = kpen * v / 2;
       // the code of the pair, taken either way round (none: an anchored vertex)
-      const int q = sPos[wl][4 * bA + bB];
+      const int q = sPos[gi][m.c & 15];
       if (q >= 0) {
-        dst[k] = ICF_IMP_REC * (long long)q + 3 * r + cc;
-      } else if (bA != bB) {
-        const int q2 = sPos[wl][4 * bB + bA];
-        if (q2 >= 0) dst[k] = ICF_IMP_REC * (long long)q2 + 3 * cc + r;
+        dst[k] = ICF_IMP_REC * (long long)q + ((m.c >> 8) & 15);
+      } else if ((m.c & 15) != ((m.c >> 4) & 15)) {
+        const int q2 = sPos[gi][(m.c >> 4) & 15];
+        if (q2 >= 0) dst[k] = ICF_IMP_REC * (long long)q2 + ((m.c >> 12) & 15);
       }
     }
   }
 #pragma unroll
-  for (int k = 0; k < 3; k++)
+  for (int k = 0; k < NS; k++)
     if (dst[k] >= 0) rec[dst[k]] = val[k];
   // vertex forces (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp, w = (1-s-t, s, t)
   // (collision_response.h:89-109): into the force record, and as the rhs of
-  // the vertex's diagonal code
-  if (lane < 12) {
+  // the vertex's diagonal code; off-diagonal codes carry no rhs
+  for (int l = gl; l < 12; l += GL) {
     const double s = cl.x, t = cl.y;
-    const int comp = lane % 3, blk = lane / 3;
-    const double F = hk * sfd[wl][comp];
+    const int comp = l % 3, blk = l / 3;
+    const double F = hk * sfd[gi][comp];
     const double f = blk == 0 ? -F : (blk == 1 ? (1 - (s + t)) : (blk == 2 ? s : t)) * F;
-    frc[12 * (size_t)u + lane] = f;
-    const int q = P[5 * blk];
+    frc[12 * (size_t)u + l] = f;
+    const int q = sPos[gi][5 * blk];
     if (q >= 0) rec[ICF_IMP_REC * (size_t)q + 9 + comp] = f;
-  } else if (lane < 28) {  // off-diagonal codes carry no rhs
-    const int pr = lane - 12;
-    const int q = P[pr];
+  }
+  for (int pr = gl; pr < 16; pr += GL) {
+    const int q = sPos[gi][pr];
     if ((pr >> 2) != (pr & 3) && q >= 0)
       for (int k = 0; k < 3; k++) rec[ICF_IMP_REC * (size_t)q + 9 + k] = 0.0;
   }
@@ -309,7 +348,7 @@ int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d, 
 // point passes its own staging).
 int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, const int4 *cls_i, const double4 *cls_d,
                               double *ks, cudaStream_t stream) {
-  k_imp_deriv<<<icf_blocks(ctx->n_imp, WARPS), 32 * WARPS, 0, stream>>>(
+  k_imp_deriv<<<icf_blocks(ctx->n_imp, GROUPS), 32 * WARPS, 0, stream>>>(
       ctx->n_imp, ctx->d_imp, xc, cls_i, cls_d, ctx->prm.penaltyK, ctx->d_imp_pos, ks,
       icf_imp_forces(ks, ctx->n_imp));
   ICF_CUDA(ctx, cudaGetLastError());
