@@ -49,7 +49,7 @@ __device__ __forceinline__ double cE1(int b) { return b == 3 ? 1.0 : (b == 1 ? -
 struct PlaneSetup {
   double gD[12], gS[12], u[12], w[12];
   double h00[9], h11[9], h01[9];
-  double W[48];  // [3 (4 bi + bj) + k]
+  double W[30];  // [3 pair + k], pairs (bi <= bj) in slot order
 };
 
 struct LineSetup {
@@ -86,13 +86,19 @@ __device__ __forceinline__ double pick3(const double v[3], int k) { return k == 
 // Everything an entry needs that depends on the slot alone is tabulated at
 // compile time (kSlots):
 //   a: I | J << 4 (the evaluated entry, I <= J: a diagonal block's lower
-//      entries are taken at their mirror) | HD's index in W (3 (4 bi + bj) +
-//      k) << 8 | (HD's sign + 1) << 14
+//      entries are taken at their mirror) | HD's index in W (3 pair + k)
+//      << 8 | (HD's sign + 1) << 14
 //   b: 3 ci + cj | (3 cj + ci) << 4 | the coefficients + 1 of HS's four
 //      terms (pi0 pj0, pi1 pj1, pi0 pj1, pi1 pj0) << 8, 10, 12, 14
 //   c: the code index of (bA, bB) | of (bB, bA) << 4 | offset 3 r + c in the
 //      first's record << 8 | 3 c + r in the second's << 12
 //   d: r | c << 2 | bA << 4 | bB << 6
+// the vertex pairs in slot order: (0,0) (1,1) (2,2) (3,3) (0,1) (0,2) (0,3)
+// (1,2) (1,3) (2,3)
+__device__ __forceinline__ int pair_a(int p) { return p < 4 ? p : (p < 7 ? 0 : (p < 9 ? 1 : 2)); }
+__device__ __forceinline__ int pair_b(int p) {
+  return p < 4 ? p : (p == 4 ? 1 : (p == 5 || p == 7) ? 2 : 3);
+}
 struct SlotMeta {
   int a, b, c, d;
 };
@@ -120,7 +126,7 @@ constexpr SlotTable make_slot_table() {
     }
     const int q00 = cst_cE0(bi) * cst_cE0(bj), q11 = cst_cE1(bi) * cst_cE1(bj);
     const int q01 = cst_cE0(bi) * cst_cE1(bj), q10 = cst_cE1(bi) * cst_cE0(bj);
-    t.s[sl].a = I | (J << 4) | ((3 * (4 * bi + bj) + hdk) << 8) | ((hds + 1) << 14);
+    t.s[sl].a = I | (J << 4) | ((3 * pi + hdk) << 8) | ((hds + 1) << 14);
     t.s[sl].b = (3 * ci + cj) | ((3 * cj + ci) << 4) | ((q00 + 1) << 8) | ((q11 + 1) << 10) | ((q01 + 1) << 12) |
                 ((q10 + 1) << 14);
     t.s[sl].c = (4 * bA + bB) | ((4 * bB + bA) << 4) | ((3 * r + c) << 8) | ((3 * c + r) << 12);
@@ -266,11 +272,11 @@ __global__ void __launch_bounds__(32 * WARPS)
         S.h01[l] = 4.0 * e0r * e1q - 2.0 * e1r * e0q - 2.0 * e01 * dl;
       }
     }
-    // W per vertex-block pair: D is trilinear in (a, e0, e1), so HD's block
-    // (bi, bj) is [W]x, W = -e1 (ai pj0 - pi0 aj) + e0 (ai pj1 - pi1 aj)
+    // W per vertex-block pair (bi <= bj, the slots' pairs): D is trilinear in
+    // (a, e0, e1), so HD's block (bi, bj) is [W]x, W = -e1 (ai pj0 - pi0 aj) + e0 (ai pj1 - pi1 aj)
     // - a (pi0 pj1 - pi1 pj0)
-    for (int l = gl; l < 48; l += GL) {
-      const int pr = l / 3, k = l % 3, bi = pr / 4, bj = pr % 4;
+    for (int l = gl; l < 30; l += GL) {
+      const int pr = l / 3, k = l % 3, bi = pair_a(pr), bj = pair_b(pr);
       const double ai = cA(bi), aj = cA(bj), pi0 = cE0(bi), pj0 = cE0(bj), pi1 = cE1(bi), pj1 = cE1(bj);
       const double al = ai * pj0 - pi0 * aj, be = ai * pj1 - pi1 * aj, ga = pi0 * pj1 - pi1 * pj0;
       S.W[l] = -pick3(e1, k) * al + pick3(e0, k) * be - pick3(a, k) * ga;

@@ -276,27 +276,28 @@ __global__ void k_iota(int n, int *__restrict__ a) {
 }
 
 // impact contributions keyed by their merged slot
-__global__ void k_count_off_static(int n, const int *__restrict__ slot, const unsigned long long *__restrict__ mkey,
-                                   const int *__restrict__ src, int identity, int *__restrict__ out) {
+// 1 where the touched slot is a static off-diagonal block (written by the
+// off-diagonal gather), else 0; flag[n] = 0
+__global__ void k_flag_off(int n, const int *__restrict__ slot, const unsigned long long *__restrict__ mkey,
+                           const int *__restrict__ src, int identity, int *__restrict__ flag) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool f = g < n && icf_off_static(mkey, src, identity, slot[g]);
-  const unsigned m = __ballot_sync(0xffffffffu, f);
-  if ((threadIdx.x & 31) == 0 && m) atomicAdd(out, __popc(m));
+  if (g > n) return;
+  flag[g] = g < n && icf_off_static(mkey, src, identity, slot[g]) ? 1 : 0;
 }
 
-// the touched slots in k_imp_add's order: diagonal and contact-only blocks at
-// [0, n_a), the static off-diagonal ones at [n_a, n) (order within each part
-// free: every slot is its own block); per slot its record range, slot and rhs
-// row (diagonal blocks) or -1
+// the touched slots in k_imp_add's order, a stable partition: diagonal and
+// contact-only blocks at [0, n_a), static off-diagonal ones at [n_a, n), each
+// part in slot order (so a warp's records and blocks lie close together); per
+// slot its record range, slot and rhs row (diagonal blocks) or -1.  pref: the
+// exclusive prefix sum of k_flag_off's flags.
 __global__ void k_split_off(int n, int n_a, const int *__restrict__ slot, const int *__restrict__ off,
-                            const unsigned long long *__restrict__ mkey, const int *__restrict__ src, int identity,
-                            int *__restrict__ cur, int2 *__restrict__ range, int *__restrict__ pslot,
-                            int *__restrict__ row) {
+                            const unsigned long long *__restrict__ mkey, const int *__restrict__ pref,
+                            int2 *__restrict__ range, int *__restrict__ pslot, int *__restrict__ row) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n) return;
   const int sl = slot[g];
-  const bool f = icf_off_static(mkey, src, identity, sl);
-  const int p = f ? n_a + atomicAdd(cur + 1, 1) : atomicAdd(cur, 1);
+  const bool f = pref[g + 1] != pref[g];
+  const int p = f ? n_a + pref[g] : g - pref[g];
   range[p] = make_int2(off[g], off[g + 1]);
   pslot[p] = sl;
   const unsigned long long k = mkey[sl];
@@ -933,26 +934,26 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
     ICF_CUDA(ctx, cudaMemsetAsync(ctx->d_imp_pos, 0xFF, sizeof(int) * (size_t)n, s));
     k_imp_pos<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_cr_off + nvalid, ctx->d_cr, ctx->d_imp_pos);
     ICF_CUDA(ctx, cudaGetLastError());
-    // how many of them the off-diagonal gather writes
+    // how many of them the off-diagonal gather writes, and the launch order
     ctx->n_crs_off = 0;
     if (nvalid > 0) {
-      int *d_c;
-      ICF_CUDA(ctx, cudaMallocAsync(&d_c, sizeof(int), s));
-      ICF_CUDA(ctx, cudaMemsetAsync(d_c, 0, sizeof(int), s));
-      k_count_off_static<<<icf_blocks(nvalid, 256), 256, 0, s>>>(nvalid, ctx->d_cr_slot, ctx->d_mkeys, ctx->d_src,
-                                                                  ctx->src_identity ? 1 : 0, d_c);
-      ICF_CUDA(ctx, cudaMemcpyAsync(&ctx->n_crs_off, d_c, sizeof(int), cudaMemcpyDeviceToHost, s));
-      ICF_CUDA(ctx, cudaFreeAsync(d_c, s));
+      int *d_flag, *d_pref;
+      ICF_CUDA(ctx, cudaMallocAsync(&d_flag, sizeof(int) * (nvalid + 1LL), s));
+      ICF_CUDA(ctx, cudaMallocAsync(&d_pref, sizeof(int) * (nvalid + 1LL), s));
+      k_flag_off<<<icf_blocks(nvalid + 1LL, 256), 256, 0, s>>>(nvalid, ctx->d_cr_slot, ctx->d_mkeys, ctx->d_src,
+                                                              ctx->src_identity ? 1 : 0, d_flag);
+      tb = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tb, d_flag, d_pref, nvalid + 1, s);
+      if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
+      ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, d_flag, d_pref, nvalid + 1, s));
+      ICF_CUDA(ctx, cudaMemcpyAsync(&ctx->n_crs_off, d_pref + nvalid, sizeof(int), cudaMemcpyDeviceToHost, s));
       ICF_CUDA(ctx, cudaStreamSynchronize(s));
-      int *d_cur;
-      ICF_CUDA(ctx, cudaMallocAsync(&d_cur, 2 * sizeof(int), s));
-      ICF_CUDA(ctx, cudaMemsetAsync(d_cur, 0, 2 * sizeof(int), s));
       k_split_off<<<icf_blocks(nvalid, 256), 256, 0, s>>>(nvalid, nvalid - ctx->n_crs_off, ctx->d_cr_slot,
-                                                           ctx->d_cr_off, ctx->d_mkeys, ctx->d_src,
-                                                           ctx->src_identity ? 1 : 0, d_cur, ctx->d_cr_range,
+                                                           ctx->d_cr_off, ctx->d_mkeys, d_pref, ctx->d_cr_range,
                                                            ctx->d_cr_pslot, ctx->d_cr_row);
       ICF_CUDA(ctx, cudaGetLastError());
-      ICF_CUDA(ctx, cudaFreeAsync(d_cur, s));
+      ICF_CUDA(ctx, cudaFreeAsync(d_flag, s));
+      ICF_CUDA(ctx, cudaFreeAsync(d_pref, s));
     }
     // impact staging
     if (ctx->n_imp > ctx->ks_cap) {
