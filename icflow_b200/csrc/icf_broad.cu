@@ -30,6 +30,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
+#include <vector>
 
 #include "icf_collide.cuh"
 #include "icf_internal.cuh"
@@ -274,11 +276,60 @@ __device__ __forceinline__ long long cell_lin(int x, int y, int z, int ny, int n
 }
 
 // count (off == nullptr) or place the surface nodes in the dense grid
+// The detection grid's parameters, decided on the device: the cell (the mean
+// box extent, at least a sixteenth of the largest) grows by 1.25 until the
+// boxes' hull holds at most 8 n + 4096 cells.  gp = {nx, ny, nz, C, status}:
+// status 0 ok, 1 degenerate boxes, 2 grid too large, 3 more cells than the
+// buffers hold (cap cells + 1).
+__global__ void k_grid_params(int n, long long cap, double *__restrict__ red, int *__restrict__ gp) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double cell = red[0];
+  if (!(cell > 0) || !isfinite(cell)) {
+    gp[4] = 1;
+    return;
+  }
+  long long dims[3], C = 0;
+  const long long lim = 8LL * n + 4096;
+  for (int attempt = 0; attempt < 64; attempt++) {
+    C = 1;
+    for (int k = 0; k < 3; k++) {
+      const double span = (red[4 + k] - red[1 + k]) / cell;
+      dims[k] = (isfinite(span) && span < 1e12) ? (long long)span + 2 : (1LL << 40);
+      C = (dims[k] > (1LL << 40) / (C > 1 ? C : 1)) ? (1LL << 40) : C * dims[k];
+    }
+    if (C <= lim) break;
+    cell *= 1.25;
+  }
+  red[0] = cell;
+  if (C > lim || dims[0] > INT32_MAX || dims[1] > INT32_MAX || dims[2] > INT32_MAX) {
+    gp[4] = 2;
+    return;
+  }
+  gp[0] = (int)dims[0];
+  gp[1] = (int)dims[1];
+  gp[2] = (int)dims[2];
+  gp[3] = (int)C;
+  gp[4] = (C + 1 > cap) ? 3 : 0;
+}
+
+// zero the first C + 1 counts of the grid's two counters (nothing when the
+// parameters failed)
+__global__ void k_grid_clear(const int *__restrict__ gp, int *__restrict__ a, int *__restrict__ b) {
+  if (gp[4] != 0) return;
+  const long long m = (long long)gp[3] + 1;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+    a[i] = 0;
+    b[i] = 0;
+  }
+}
+
+// count (off == nullptr) or place the surface nodes in the dense grid
 __global__ void k_node_put(int ns, const int *__restrict__ snode, const double4 *__restrict__ xc,
-                           const double *__restrict__ red, int nx, int ny, int nz, int *__restrict__ cnt,
+                           const double *__restrict__ red, const int *__restrict__ gp, int *__restrict__ cnt,
                            const int *__restrict__ off, double4 *__restrict__ ent) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ns) return;
+  if (k >= ns || gp[4] != 0) return;
+  const int nx = gp[0], ny = gp[1], nz = gp[2];
   const double4 P = xc[snode[k]];
   const double cell = red[0];
   const int cx = cell_of(P.x, red[1], cell), cy = cell_of(P.y, red[2], cell), cz = cell_of(P.z, red[3], cell);
@@ -331,7 +382,7 @@ __device__ __forceinline__ bool pair_exists(int k, int b, const int *__restrict_
 // count per surface node
 __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
                                                 const double *__restrict__ lohi, const int4 *__restrict__ clo,
-                                                int ny, int nz, const int *__restrict__ goff,
+                                                const int *__restrict__ gp, const int *__restrict__ goff,
                                                 const double4 *__restrict__ gnode, const int *__restrict__ snode,
                                                 const int *__restrict__ sinc_off, const int *__restrict__ sinc,
                                                 const int *__restrict__ group, int eb,
@@ -340,7 +391,8 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
                                                 const double *__restrict__ inv) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int b = (int)(t >> 3), g = (int)(t & 7);
-  if (b >= n) return;
+  if (b >= n || gp[4] != 0) return;
+  const int ny = gp[1], nz = gp[2];
   const int4 B = selem[b];
   const int nb[4] = {B.x, B.y, B.z, B.w};
   const double *lh = lohi + 6 * (size_t)b;
@@ -378,21 +430,24 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
 
 // the hits grouped by surface node (ascending, so by node id): key
 // node << eb | b at koff[k] + the node's running count
-__global__ void k_place(int hits, const unsigned long long *__restrict__ in, int eb, const int *__restrict__ koff,
-                        int *__restrict__ kcur, const int *__restrict__ snode, unsigned long long *__restrict__ out) {
-  const int h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= hits) return;
+__global__ void k_place(long long cap, const int *__restrict__ count, const unsigned long long *__restrict__ in, int eb,
+                        const int *__restrict__ koff, int *__restrict__ kcur, const int *__restrict__ snode,
+                        unsigned long long *__restrict__ out) {
+  const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= cap || h >= *count) return;
   const unsigned long long key = in[h];
   const int k = (int)(key >> eb);
   const unsigned long long b = key & ((1ull << eb) - 1);
-  out[koff[k] + atomicAdd(kcur + k, 1)] = ((unsigned long long)(unsigned)snode[k] << eb) | b;
+  const long long p = (long long)koff[k] + atomicAdd(kcur + k, 1);
+  if (p < cap) out[p] = ((unsigned long long)(unsigned)snode[k] << eb) | b;
 }
 
 // each surface node's few hits in ascending element order (insertion sort)
-__global__ void k_sort_seg(int ns, const int *__restrict__ koff, unsigned long long *__restrict__ keys) {
+__global__ void k_sort_seg(int ns, long long cap, const int *__restrict__ koff, unsigned long long *__restrict__ keys) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ns) return;
-  const int a = koff[k], e = koff[k + 1];
+  const int a = koff[k];
+  const int e = (int)(koff[k + 1] < cap ? koff[k + 1] : cap);
   for (int i = a + 1; i < e; i++) {
     const unsigned long long v = keys[i];
     int j = i - 1;
@@ -418,10 +473,12 @@ void icf_free_contact_ws(icf_ctx *ctx) {
   icf_contact_ws &W = ctx->cws;
   void *d[] = {W.lohi, W.ext, W.tmpv, W.red, W.bcnt, W.boff, W.clo, W.ek0, W.ek1, W.ee0, W.ee1, W.pc, W.po,
                W.p0, W.p1, W.ncnt, W.noff, W.nk0, W.nk1, W.d_small, W.gcnt, W.goff, W.gcur, W.gnode,
-               W.kcnt, W.koff, W.kcur, W.tinv};
+               W.kcnt, W.koff, W.kcur, W.tinv, W.gp};
   for (void *q : d) cudaFree(q);
   cudaFreeHost(W.h_small);
   cudaFreeHost(W.h_red);
+  cudaFreeHost(W.h_gp);
+  if (W.det_exec) cudaGraphExecDestroy(W.det_exec);
   W = icf_contact_ws();
 }
 
@@ -553,14 +610,134 @@ int icf_broad_phase_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_pa
   return icf_fail(ctx, ICF_ERR_SIZE, "broad phase: pair buffer growth did not converge");
 }
 
-// Contact detection without the pair list.  Three synchronisations: the grid
-// (cell size and corners, which set the grid's dimensions), the hit count (to
-// grow the key buffer and repeat when it overflows), and the impact list's
-// count in icf_finish_impacts.  The grid is dense: if the boxes' hull holds
-// more than 8 cells per surface element at the mean box extent, the cell
-// grows until it holds at most that many.
-int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_impacts) {
+// Contact detection without the pair list, one synchronisation: the grid's
+// parameters are decided on the device (k_grid_params), and the buffers are
+// sized by high-water marks.  When a call finds more cells or more hits than
+// the buffers hold, its result is discarded, the buffers grow to what that
+// call reported, and it runs again.
+// The launches of one detection up to the sorted keys (no synchronisation),
+// with the CUB scratch already sized.
+static int enqueue_detect(icf_ctx *ctx, double pad, const int *d_group, int eb, cudaStream_t s) {
+  const int n = ctx->n_surf, ns = ctx->n_snode;
+  icf_contact_ws &W = ctx->cws;
+  const int nbk = (int)std::min<long long>((n + 255) / 256, 2LL * ctx->n_sm);
+  const long long cap_cells = W.cell_cap;
+  k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext);
+  k_red7<<<nbk, 256, 0, s>>>(n, W.lohi, W.ext, W.tmpv);
+  k_red7_final<<<1, 256, 0, s>>>(nbk, n, W.tmpv, W.red);
+  k_grid_params<<<1, 32, 0, s>>>(n, cap_cells, W.red, W.gp);
+  k_tet_inv<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.tinv);
+  // the surface nodes by cell (over the high-water count of cells: the
+  // counts past this call's C are never read)
+  k_grid_clear<<<2 * ctx->n_sm, 256, 0, s>>>(W.gp, W.gcnt, W.gcur);
+  k_node_put<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, ctx->d_snode, ctx->d_xc, W.red, W.gp, W.gcnt, nullptr, nullptr);
+  size_t tb = ctx->tmp_bytes;
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.gcnt, W.goff, (int)cap_cells, s));
+  k_node_put<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, ctx->d_snode, ctx->d_xc, W.red, W.gp, W.gcur, W.goff, W.gnode);
+  // every element's cells
+  k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
+  ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, sizeof(int), s));
+  ICF_CUDA(ctx, cudaMemsetAsync(W.kcnt, 0, sizeof(int) * (ns + 1LL), s));
+  k_detect<<<icf_blocks(8LL * n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, W.gp, W.goff, W.gnode,
+                                                   ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, d_group, eb, W.nk0,
+                                                   W.nkey_cap, W.d_small + 5, W.kcnt, W.tinv);
+  ICF_CUDA(ctx, cudaGetLastError());
+  // grouped by surface node (a counting sort), each node's hits sorted: the
+  // keys node << eb | element ascending
+  tb = ctx->tmp_bytes;
+  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.kcnt, W.koff, ns + 1, s));
+  ICF_CUDA(ctx, cudaMemsetAsync(W.kcur, 0, sizeof(int) * (ns + 1LL), s));
+  k_place<<<icf_blocks(W.nkey_cap, 256), 256, 0, s>>>(W.nkey_cap, W.d_small + 5, W.nk0, eb, W.koff, W.kcur,
+                                                     ctx->d_snode, W.nk1);
+  k_sort_seg<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, W.nkey_cap, W.koff, W.nk1);
+  // the grid's status and size come back with the impact count
+  ICF_CUDA(ctx, cudaMemcpyAsync(W.h_gp, W.gp, 5 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaGetLastError());
+  return ICF_OK;
+}
+
+// Everything a captured detection depends on: replayed while these hold.
+static void detect_key(const icf_ctx *ctx, double pad, const int *d_group, int eb, std::vector<long long> &k) {
+  const icf_contact_ws &W = ctx->cws;
+  long long pb;
+  std::memcpy(&pb, &pad, sizeof(pb));
+  k = {ctx->n_surf, ctx->n_snode, pb, eb, W.cell_cap, W.nkey_cap, (long long)ctx->tmp_bytes, ctx->n_sm,
+       (long long)(intptr_t)d_group, (long long)(intptr_t)ctx->stream, (long long)(intptr_t)ctx->d_tmp,
+       (long long)(intptr_t)ctx->d_selem, (long long)(intptr_t)ctx->d_xc, (long long)(intptr_t)ctx->d_snode,
+       (long long)(intptr_t)ctx->d_sinc_off, (long long)(intptr_t)ctx->d_sinc, (long long)(intptr_t)W.lohi,
+       (long long)(intptr_t)W.ext, (long long)(intptr_t)W.tmpv, (long long)(intptr_t)W.red,
+       (long long)(intptr_t)W.gp, (long long)(intptr_t)W.h_gp, (long long)(intptr_t)W.tinv,
+       (long long)(intptr_t)W.gcnt, (long long)(intptr_t)W.goff, (long long)(intptr_t)W.gcur,
+       (long long)(intptr_t)W.gnode, (long long)(intptr_t)W.bcnt, (long long)(intptr_t)W.clo,
+       (long long)(intptr_t)W.kcnt, (long long)(intptr_t)W.koff, (long long)(intptr_t)W.kcur,
+       (long long)(intptr_t)W.nk0, (long long)(intptr_t)W.nk1, (long long)(intptr_t)W.d_small};
+}
+
+// One detection: the launches through a CUDA graph captured on first use and
+// replayed while nothing it depends on changed, then the closest faces and
+// the one synchronisation (icf_finish_impacts).
+static int detect_pass(icf_ctx *ctx, double pad, const int *d_group, int *n_impacts, bool *again) {
   cudaStream_t s = ctx->stream;
+  const int n = ctx->n_surf, ns = ctx->n_snode;
+  icf_contact_ws &W = ctx->cws;
+  *again = false;
+  int eb = 1;
+  while ((1LL << eb) < (long long)n) eb++;
+  // the two scans' scratch, sized before any capture
+  size_t tb1 = 0, tb2 = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb1, W.gcnt, W.goff, (int)W.cell_cap, s);
+  cub::DeviceScan::ExclusiveSum(nullptr, tb2, W.kcnt, W.koff, ns + 1, s);
+  if (icf_scratch(ctx, std::max(tb1, tb2))) return ICF_ERR_CUDA;
+  std::vector<long long> key;
+  detect_key(ctx, pad, d_group, eb, key);
+  if (!W.det_exec || key != W.det_key) {
+    if (W.det_exec) {
+      cudaGraphExecDestroy(W.det_exec);
+      W.det_exec = nullptr;
+    }
+    ICF_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_detect(ctx, pad, d_group, eb, s);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(s, &g);
+    if (rc != ICF_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ec != cudaSuccess) return icf_fail(ctx, ICF_ERR_CUDA, std::string("detection capture: ") + cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&W.det_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      W.det_exec = nullptr;
+      return icf_fail(ctx, ICF_ERR_CUDA, std::string("detection graph: ") + cudaGetErrorString(ei));
+    }
+    W.det_key = key;
+  }
+  ICF_CUDA(ctx, cudaGraphLaunch(W.det_exec, s));
+  ICF_TRY_RC(icf_finish_impacts(ctx, W.nk1, (int)W.nkey_cap, W.d_small + 5, eb, n_impacts));
+  const int st = W.h_gp[4];
+  if (st == 1) return icf_fail(ctx, ICF_ERR_NUMERIC, "contact detection: degenerate boxes");
+  if (st == 2) return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: grid too large");
+  if (st == 3) {  // more cells than the buffers hold
+    const long long c = W.h_gp[3] + W.h_gp[3] / 4 + 2;
+    ICF_TRY_RC(grow(ctx, &W.gcnt, c));
+    ICF_TRY_RC(grow(ctx, &W.goff, c));
+    ICF_TRY_RC(grow(ctx, &W.gcur, c));
+    ICF_CUDA(ctx, cudaMemsetAsync(W.gcnt, 0, sizeof(int) * (size_t)c, s));
+    W.cell_cap = c;
+    *again = true;
+  }
+  const long long hits = W.h_small[0];
+  if (hits > W.nkey_cap) {  // more hits than the key buffers hold
+    const long long c = hits + hits / 4 + 1024;
+    ICF_TRY_RC(grow(ctx, &W.nk0, c));
+    ICF_TRY_RC(grow(ctx, &W.nk1, c));
+    W.nkey_cap = c;
+    *again = true;
+  }
+  return ICF_OK;
+}
+
+int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *n_impacts) {
   const int n = ctx->n_surf, ns = ctx->n_snode;
   icf_contact_ws &W = ctx->cws;
   *n_impacts = 0;
@@ -570,7 +747,6 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     return ICF_OK;
   }
   ICF_TRY_RC(ensure_small(ctx));
-  const int nbk = (int)std::min<long long>((n + 255) / 256, 2LL * ctx->n_sm);
   if (n > W.b_cap) {
     ICF_TRY_RC(grow(ctx, &W.lohi, 6LL * n));
     ICF_TRY_RC(grow(ctx, &W.ext, n));
@@ -587,40 +763,24 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     ICF_TRY_RC(grow(ctx, &W.tinv, 12LL * n));
     W.tinv_cap = n;
   }
+  if (ns + 1LL > W.kcap) {
+    ICF_TRY_RC(grow(ctx, &W.kcnt, ns + 1LL));
+    ICF_TRY_RC(grow(ctx, &W.koff, ns + 1LL));
+    ICF_TRY_RC(grow(ctx, &W.kcur, ns + 1LL));
+    W.kcap = ns + 1LL;
+  }
   if (!W.tmpv) ICF_TRY_RC(grow(ctx, &W.tmpv, 8LL * (2 * ctx->n_sm + 1)));
   if (!W.red) ICF_TRY_RC(grow(ctx, &W.red, 8));
-  k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext);
-  k_red7<<<nbk, 256, 0, s>>>(n, W.lohi, W.ext, W.tmpv);
-  k_red7_final<<<1, 256, 0, s>>>(nbk, n, W.tmpv, W.red);
-  k_tet_inv<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.tinv);
-  ICF_CUDA(ctx, cudaMemcpyAsync(W.h_red, W.red, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  ICF_CUDA(ctx, cudaStreamSynchronize(s));
-  double *h_red = W.h_red;
-  if (!(h_red[0] > 0) || !std::isfinite(h_red[0])) return icf_fail(ctx, ICF_ERR_NUMERIC, "contact detection: degenerate boxes");
-  double cell = h_red[0];
-  long long dims[3], C = 0;
-  for (int attempt = 0; attempt < 64; attempt++) {
-    C = 1;
-    for (int k = 0; k < 3; k++) {
-      const double span = (h_red[4 + k] - h_red[1 + k]) / cell;
-      dims[k] = (std::isfinite(span) && span < 1e12) ? (long long)span + 2 : (1LL << 40);
-      C = (dims[k] > (1LL << 40) / std::max(C, 1LL)) ? (1LL << 40) : C * dims[k];
-    }
-    if (C <= 8LL * n + 4096) break;
-    cell *= 1.25;
-  }
-  if (C > 8LL * n + 4096 || dims[0] > INT32_MAX || dims[1] > INT32_MAX || dims[2] > INT32_MAX)
-    return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: grid too large");
-  if (cell != h_red[0]) {
-    h_red[0] = cell;
-    ICF_CUDA(ctx, cudaMemcpyAsync(W.red, h_red, sizeof(double), cudaMemcpyHostToDevice, s));
-  }
-  const int nx = (int)dims[0], ny = (int)dims[1], nz = (int)dims[2];
-  if (C + 1 > W.cell_cap) {
-    ICF_TRY_RC(grow(ctx, &W.gcnt, C + 1));
-    ICF_TRY_RC(grow(ctx, &W.goff, C + 1));
-    ICF_TRY_RC(grow(ctx, &W.gcur, C + 1));
-    W.cell_cap = C + 1;
+  if (!W.gp) ICF_TRY_RC(grow(ctx, &W.gp, 8));
+  if (!W.h_gp) ICF_CUDA(ctx, cudaMallocHost(&W.h_gp, 8 * sizeof(int)));
+  if (W.cell_cap == 0) {  // a first guess: a cell per surface element
+    const long long c = n + 4096LL;
+    ICF_TRY_RC(grow(ctx, &W.gcnt, c));
+    ICF_TRY_RC(grow(ctx, &W.goff, c));
+    ICF_TRY_RC(grow(ctx, &W.gcur, c));
+    // counts past a call's C are scanned but never read; start them at zero
+    ICF_CUDA(ctx, cudaMemsetAsync(W.gcnt, 0, sizeof(int) * (size_t)c, ctx->stream));
+    W.cell_cap = c;
   }
   if (W.nkey_cap == 0) {
     const long long c = std::max<long long>(n / 4, 1024);
@@ -628,56 +788,10 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     ICF_TRY_RC(grow(ctx, &W.nk1, c));
     W.nkey_cap = c;
   }
-  // the surface nodes by cell
-  ICF_CUDA(ctx, cudaMemsetAsync(W.gcnt, 0, sizeof(int) * (size_t)(C + 1), s));
-  ICF_CUDA(ctx, cudaMemsetAsync(W.gcur, 0, sizeof(int) * (size_t)(C + 1), s));
-  k_node_put<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, ctx->d_snode, ctx->d_xc, W.red, nx, ny, nz, W.gcnt, nullptr,
-                                                 nullptr);
-  size_t tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, W.gcnt, W.goff, (int)(C + 1), s);
-  if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-  ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.gcnt, W.goff, (int)(C + 1), s));
-  k_node_put<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, ctx->d_snode, ctx->d_xc, W.red, nx, ny, nz, W.gcur, W.goff,
-                                                 W.gnode);
-  // every element's cells
-  k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
-  int eb = 1;
-  while ((1LL << eb) < (long long)n) eb++;
-  if (ns + 1LL > W.kcap) {
-    ICF_TRY_RC(grow(ctx, &W.kcnt, ns + 1LL));
-    ICF_TRY_RC(grow(ctx, &W.koff, ns + 1LL));
-    ICF_TRY_RC(grow(ctx, &W.kcur, ns + 1LL));
-    W.kcap = ns + 1LL;
+  for (int attempt = 0; attempt < 3; attempt++) {
+    bool again = false;
+    ICF_TRY_RC(detect_pass(ctx, pad, d_group, n_impacts, &again));
+    if (!again) return ICF_OK;
   }
-  int hits = 0;
-  for (int attempt = 0; attempt < 2; attempt++) {
-    ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, sizeof(int), s));
-    ICF_CUDA(ctx, cudaMemsetAsync(W.kcnt, 0, sizeof(int) * (ns + 1LL), s));
-    k_detect<<<icf_blocks(8LL * n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, ny, nz, W.goff,
-                                                     W.gnode, ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, d_group, eb,
-                                                     W.nk0, W.nkey_cap, W.d_small + 5, W.kcnt, W.tinv);
-    ICF_CUDA(ctx, cudaGetLastError());
-    ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 5, W.d_small + 5, sizeof(int), cudaMemcpyDeviceToHost, s));
-    ICF_CUDA(ctx, cudaStreamSynchronize(s));
-    hits = W.h_small[5];
-    if (hits <= W.nkey_cap) break;
-    if (attempt == 1) return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: key buffer growth did not converge");
-    const long long c = hits + hits / 4 + 1024;
-    ICF_TRY_RC(grow(ctx, &W.nk0, c));
-    ICF_TRY_RC(grow(ctx, &W.nk1, c));
-    W.nkey_cap = c;
-  }
-  if (hits > 0) {
-    // grouped by surface node (a counting sort), each node's hits sorted:
-    // the keys node << eb | element ascending
-    tb = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, tb, W.kcnt, W.koff, ns + 1, s);
-    if (icf_scratch(ctx, tb)) return ICF_ERR_CUDA;
-    ICF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_tmp, tb, W.kcnt, W.koff, ns + 1, s));
-    ICF_CUDA(ctx, cudaMemsetAsync(W.kcur, 0, sizeof(int) * (ns + 1LL), s));
-    k_place<<<icf_blocks(hits, 256), 256, 0, s>>>(hits, W.nk0, eb, W.koff, W.kcur, ctx->d_snode, W.nk1);
-    k_sort_seg<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, W.koff, W.nk1);
-    ICF_CUDA(ctx, cudaGetLastError());
-  }
-  return icf_finish_impacts(ctx, W.nk1, hits, W.d_small + 5, eb, n_impacts);
+  return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: buffer growth did not converge");
 }

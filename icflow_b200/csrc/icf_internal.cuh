@@ -156,6 +156,12 @@ struct icf_contact_ws {
   // per surface element: edge-matrix inverse and first vertex (12 doubles)
   double *tinv = nullptr;
   long long tinv_cap = 0;
+  // the detection grid's parameters {nx, ny, nz, C, status} and their pinned
+  // host copy
+  int *gp = nullptr, *h_gp = nullptr;
+  // the detection's captured launches and what they were captured with
+  cudaGraphExec_t det_exec = nullptr;
+  std::vector<long long> det_key;
   // small device results and their pinned host copy: [0] unique count,
   // [1] impact list differs from the built one, [2] pairs before de-duplication
   int *d_small = nullptr, *h_small = nullptr;

@@ -501,19 +501,26 @@ def test_detect_contacts_matches_the_pair_pipeline(O):
     negative group id), and two ice blocks driven into each other."""
     from icflow_b200 import _lib
 
+    # "ice_far": the blocks half a metre apart, so the grid over the boxes' hull
+    # has more cells than the first guess of its buffers (one per surface
+    # element): the first call grows them and runs again
     cases = [("poly", 1, -0.3, None, 0.0), ("poly", 2, -0.05, _rot([1, 1, 0], 35), 0.0),
-             ("poly", 3, 0.2, None, 0.0), ("poly", 4, -0.25, _rot([1, 0, 2], 60), 2e-3), ("ice", 5, 0, None, 0.0)]
+             ("poly", 3, 0.2, None, 0.0), ("poly", 4, -0.25, _rot([1, 0, 2], 60), 2e-3), ("ice", 5, 0, None, 0.0),
+             ("ice_far", 6, 0.5, None, 0.0)]
     for kind, seed, gap, R, pad in cases:
         if kind == "poly":
             coll = M.polycrystal(n=7, grains=5, seed=seed, platens=True, gap=gap)
             if R is not None:
                 coll = _rotate(coll, R)
             un, vn, an = random_state(coll, seed, du=3e-6)
-        else:
+        elif kind == "ice":
             coll, _ = M.ice_impact(n=6, grains=6, seed=seed, size=(0.02, 0.02, 0.01))
             un, vn, an = random_state(coll, seed, du=1e-6)
             na = coll.meshes[0].n_nodes
             un[:na, 2] += 2e-4  # block A driven 0.1 mm into block B
+        else:
+            coll, _ = M.ice_impact(n=6, grains=6, seed=seed, size=(0.02, 0.02, 0.01), gap=gap)
+            un, vn, an = random_state(coll, seed, du=1e-5)
         gf = _gf(coll, config_prms(penaltyK=1e8))
         gf.TransferNodesToGPU(un, vn, an)
         for same_mesh in (True, False):
