@@ -1,4 +1,4 @@
-// icf_contact_deriv.cu -- penalty response of the impacts, two impacts per warp.
+// icf_contact_deriv.cu -- penalty response of the impacts, one thread per impact.
 //
 // kCollisionResponseForce (collision_response.h:38-127) needs the gradient
 // and Hessian of the squared point-triangle distance d2(x), x = (p, v0, v1,
@@ -16,331 +16,344 @@
 //       - D^2 HS / S^2 + 2 D^2 gS gS^T / S^3,
 // gD, gS the gradients and HD, HS the Hessians of D and S: HD is a
 // cross-product matrix per vertex-block pair (D is trilinear in a, e0, e1),
-// HS follows from S = |e0|^2 |e1|^2 - (e0.e1)^2.  About 40 operations per
+// HS follows from S = |e0|^2 |e1|^2 - (e0.e1)^2.  About 10 operations per
 // entry instead of some 200; the two forms agree to rounding (1e-14 of the
 // largest entry on random interior cases).
 //
-// Sixteen lanes share an impact's setup through shared memory.
-// The Hessian K = k/2 d2'' goes straight to the records of the impact's
-// contribution codes, at their positions in the slot-sorted list
-// (icf_internal.cuh, ICF_IMP_REC): a lane per record entry (10 vertex pairs x
-// 9 entries), each written once; a diagonal block's lower entries are
-// evaluated at (column, row), so the block is symmetric bit for bit.  On the
-// diagonal codes the record also carries the vertex's rhs from (-F, w0 F,
-// w1 F, w2 F), F = k/2 d(d2)/dp, w = (1-s-t, s, t); the four vertex forces
-// also go to a per-impact force record (for the node forces).
+// One thread computes an impact's whole response.  The ten vertex pairs
+// (p, v0, v1, v2 taken two at a time, diagonal pairs included) and the
+// entries of their 3x3 blocks are unrolled at compile time, so every
+// coefficient that depends only on the pair (the +-1/0 weights of a, e0, e1
+// in each vertex's gradient, HD's cross-product vector, HS's terms) folds
+// into the instruction stream: no tables, no shared memory, no index
+// arithmetic per entry.  K = k/2 d2'' goes to the record of the pair's
+// contribution code at its position in the slot-sorted list (icf_internal.cuh,
+// ICF_IMP_REC): the block in the code's orientation, then, on a diagonal code,
+// the vertex's rhs from (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp,
+// w = (1-s-t, s, t), else zeros; a record is three 32-byte stores.  A diagonal
+// block's lower entries are its upper ones, so it is symmetric bit for bit.
+// The four vertex forces also go to a per-impact force record (node forces).
 #include "icf_internal.cuh"
+#include "icf_tet.cuh"
 
 namespace {
 
-constexpr int WARPS = 4;
+constexpr int TPB = 128;
 
 // coefficients of vertex block b (p, v0, v1, v2) in a = p - v0,
-// e0 = v1 - v0, e1 = v2 - v0
-__device__ __forceinline__ double cA(int b) { return b == 0 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
-__device__ __forceinline__ double cE0(int b) { return b == 2 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
-__device__ __forceinline__ double cE1(int b) { return b == 3 ? 1.0 : (b == 1 ? -1.0 : 0.0); }
+// e0 = v1 - v0, e1 = v2 - v0 (compile-time after unrolling)
+__host__ __device__ constexpr int cA(int b) { return b == 0 ? 1 : (b == 1 ? -1 : 0); }
+__host__ __device__ constexpr int cE0(int b) { return b == 2 ? 1 : (b == 1 ? -1 : 0); }
+__host__ __device__ constexpr int cE1(int b) { return b == 3 ? 1 : (b == 1 ? -1 : 0); }
 
-// Interior region, per impact: the gradients of D and S, the rank-two part's
-// factors u = c1 gD + c3 gS, w = c3 gD + c5 gS (so that c1 gD gD^T + c3 (gD gS^T
-// + gS gD^T) + c5 gS gS^T = u gD^T + w gS^T), the Hessian blocks of S over
-// (e0, e0), (e1, e1), (e0, e1), and per vertex-block pair (bi, bj) the vector W
-// with HD's block = [W]x.
-struct PlaneSetup {
-  double gD[12], gS[12], u[12], w[12];
-  double h00[9], h11[9], h01[9];
-  double W[30];  // [3 pair + k], pairs (bi <= bj) in slot order
-};
+__device__ __forceinline__ void st4(double *p, double a, double b, double c, double d) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
 
-struct LineSetup {
-  double sp, g, f2, f2sq, f2cu;
-  double spd[9], gd[9], f1d[9], f2d[9];
-};
-
-// Hessian entry (i, j) of f1 - g / f2 over y = (p, q1, q2)
-__device__ double line_entry(const LineSetup &L, int i, int j) {
-  const bool same = (i % 3) == (j % 3);
-  const int bi = i / 3, bj = j / 3;
-  double spdd = 0, f1dd = 0, f2dd = 0;
-  if (same) {
-    if (bi == 1 && bj == 1) spdd = -2.0;
-    else if ((bi == 0 && bj == 2) || (bi == 2 && bj == 0)) spdd = -1.0;
-    else if (bi != bj) spdd = 1.0;
-    if (bi != 2 && bj != 2) f1dd = (bi == bj) ? 2.0 : -2.0;
-    if (bi != 0 && bj != 0) f2dd = (bi == bj) ? 2.0 : -2.0;
+// The record of vertex pair (bA, bB): to the code (bA, bB) if there is one,
+// else the block transposed to the code (bB, bA) (none: an anchored vertex).
+// Records start at 96-byte multiples, so each third is 32-byte aligned.
+__device__ __forceinline__ void put_record(double *__restrict__ rec, int q, int qt, const double B[9], double f0,
+                                           double f1, double f2) {
+  if (q >= 0) {
+    double *o = rec + ICF_IMP_REC * (size_t)q;
+    st4(o, B[0], B[1], B[2], B[3]);
+    st4(o + 4, B[4], B[5], B[6], B[7]);
+    st4(o + 8, B[8], f0, f1, f2);
+  } else if (qt >= 0) {
+    double *o = rec + ICF_IMP_REC * (size_t)qt;
+    st4(o, B[0], B[3], B[6], B[1]);
+    st4(o + 4, B[4], B[7], B[2], B[5]);
+    st4(o + 8, B[8], f0, f1, f2);
   }
-  const double gdd = 2 * (L.spd[i] * L.spd[j] + L.sp * spdd);
-  const double t1 = -2 * L.g * L.f2d[i] * L.f2d[j] / L.f2cu;
-  const double t2 = (L.gd[i] * L.f2d[j] + L.gd[j] * L.f2d[i]) / L.f2sq;
-  const double t4 = L.g * f2dd / L.f2sq;
-  const double t5 = -gdd / L.f2;
-  return t1 + t2 + f1dd + t4 + t5;
 }
 
-// component k of a 3-vector held in registers (selects, no local memory)
-__device__ __forceinline__ double pick3(const double v[3], int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
+// Interior region: everything an entry needs, per impact.
+struct Plane {
+  double a[3], e0[3], e1[3];
+  double gD[12], gS[12];
+  double c1, c2, c3, c4, c5;
+  double e00, e11, e01;
+};
 
-
-// Record entry slots (0..89): vertex pair (bA <= bB; the four diagonal
-// pairs, then the six off-diagonal ones) and entry (r, c) of its 3x3 block.
-// Everything an entry needs that depends on the slot alone is tabulated at
-// compile time (kSlots):
-//   a: I | J << 4 (the evaluated entry, I <= J: a diagonal block's lower
-//      entries are taken at their mirror) | HD's index in W (3 pair + k)
-//      << 8 | (HD's sign + 1) << 14
-//   b: 3 ci + cj | (3 cj + ci) << 4 | the coefficients + 1 of HS's four
-//      terms (pi0 pj0, pi1 pj1, pi0 pj1, pi1 pj0) << 8, 10, 12, 14
-//   c: the code index of (bA, bB) | of (bB, bA) << 4 | offset 3 r + c in the
-//      first's record << 8 | 3 c + r in the second's << 12
-//   d: r | c << 2 | bA << 4 | bB << 6
-// the vertex pairs in slot order: (0,0) (1,1) (2,2) (3,3) (0,1) (0,2) (0,3)
-// (1,2) (1,3) (2,3)
-__device__ __forceinline__ int pair_a(int p) { return p < 4 ? p : (p < 7 ? 0 : (p < 9 ? 1 : 2)); }
-__device__ __forceinline__ int pair_b(int p) {
-  return p < 4 ? p : (p == 4 ? 1 : (p == 5 || p == 7) ? 2 : 3);
+// HS's 3x3 blocks over (e0, e0), (e1, e1), (e0, e1) at (r, q)
+__device__ __forceinline__ double hs00(const Plane &P, int r, int q) {
+  return 2.0 * ((r == q ? P.e11 : 0.0) - P.e1[r] * P.e1[q]);
 }
-struct SlotMeta {
-  int a, b, c, d;
-};
-struct SlotTable {
-  SlotMeta s[90];
-};
-constexpr int cst_cE0(int b) { return b == 2 ? 1 : (b == 1 ? -1 : 0); }
-constexpr int cst_cE1(int b) { return b == 3 ? 1 : (b == 1 ? -1 : 0); }
-constexpr SlotTable make_slot_table() {
-  SlotTable t{};
-  const int PA[10] = {0, 1, 2, 3, 0, 0, 0, 1, 1, 2}, PB[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
-  for (int sl = 0; sl < 90; sl++) {
-    const int pi = sl / 9, e = sl % 9, bA = PA[pi], bB = PB[pi], r = e / 3, c = e % 3;
-    int I = 3 * bA + r, J = 3 * bB + c;
-    if (I > J) {
-      const int x = I;
-      I = J;
-      J = x;
+__device__ __forceinline__ double hs11(const Plane &P, int r, int q) {
+  return 2.0 * ((r == q ? P.e00 : 0.0) - P.e0[r] * P.e0[q]);
+}
+__device__ __forceinline__ double hs01(const Plane &P, int r, int q) {
+  return 4.0 * P.e0[r] * P.e1[q] - 2.0 * P.e1[r] * P.e0[q] - (r == q ? 2.0 * P.e01 : 0.0);
+}
+
+// block (bi, bj) of the interior Hessian (bi <= bj), row-major
+template <int bi, int bj>
+__device__ __forceinline__ void block(const Plane &P, double B[9]) {
+  // HD's block is [W]x, W = -e1 al + e0 be - a ga (D trilinear in a, e0, e1)
+  constexpr int al = cA(bi) * cE0(bj) - cE0(bi) * cA(bj);
+  constexpr int be = cA(bi) * cE1(bj) - cE1(bi) * cA(bj);
+  constexpr int ga = cE0(bi) * cE1(bj) - cE1(bi) * cE0(bj);
+  constexpr int q00 = cE0(bi) * cE0(bj), q11 = cE1(bi) * cE1(bj);
+  constexpr int q01 = cE0(bi) * cE1(bj), q10 = cE1(bi) * cE0(bj);
+  double W[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) W[k] = -P.e1[k] * (double)al + P.e0[k] * (double)be - P.a[k] * (double)ga;
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const int I = 3 * bi + r;
+    const double u = P.c1 * P.gD[I] + P.c3 * P.gS[I];
+    const double w = P.c3 * P.gD[I] + P.c5 * P.gS[I];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if (bi == bj && c < r) {
+        B[3 * r + c] = B[3 * c + r];
+        continue;
+      }
+      const int J = 3 * bj + c;
+      double hd = 0.0;
+      if (r != c) {
+        const int k = 3 - r - c;
+        hd = ((c - r + 3) % 3 == 1) ? -W[k] : W[k];
+      }
+      double hs = 0.0;
+      if (q00) hs += (double)q00 * hs00(P, r, c);
+      if (q11) hs += (double)q11 * hs11(P, r, c);
+      if (q01) hs += (double)q01 * hs01(P, r, c);
+      if (q10) hs += (double)q10 * hs01(P, c, r);
+      B[3 * r + c] = u * P.gD[J] + w * P.gS[J] + P.c2 * hd + P.c4 * hs;
     }
-    const int bi = I / 3, bj = J / 3, ci = I % 3, cj = J % 3;
-    int hdk = 0, hds = 0;  // sign 0: HD's entry is zero (ci == cj)
-    if (ci != cj) {
-      hdk = 3 - ci - cj;
-      hds = ((cj - ci + 3) % 3 == 1) ? -1 : 1;
-    }
-    const int q00 = cst_cE0(bi) * cst_cE0(bj), q11 = cst_cE1(bi) * cst_cE1(bj);
-    const int q01 = cst_cE0(bi) * cst_cE1(bj), q10 = cst_cE1(bi) * cst_cE0(bj);
-    t.s[sl].a = I | (J << 4) | ((3 * pi + hdk) << 8) | ((hds + 1) << 14);
-    t.s[sl].b = (3 * ci + cj) | ((3 * cj + ci) << 4) | ((q00 + 1) << 8) | ((q11 + 1) << 10) | ((q01 + 1) << 12) |
-                ((q10 + 1) << 14);
-    t.s[sl].c = (4 * bA + bB) | ((4 * bB + bA) << 4) | ((3 * r + c) << 8) | ((3 * c + r) << 12);
-    t.s[sl].d = r | (c << 2) | (bA << 4) | (bB << 6);
   }
-  return t;
-}
-__device__ const SlotTable kSlots = make_slot_table();
-
-// the interior entry of a slot: u_I gD_J + w_I gS_J + c2 HD_IJ + c4 HS_IJ
-__device__ __forceinline__ double plane_slot(const PlaneSetup &S, double c2, double c4, const SlotMeta &m) {
-  const int I = m.a & 15, J = (m.a >> 4) & 15;
-  const double hd = S.W[(m.a >> 8) & 63] * (double)(((m.a >> 14) & 3) - 1);
-  const int ix = m.b & 15, ixt = (m.b >> 4) & 15;
-  const double hs = (double)(((m.b >> 8) & 3) - 1) * S.h00[ix] + (double)(((m.b >> 10) & 3) - 1) * S.h11[ix] +
-                    (double)(((m.b >> 12) & 3) - 1) * S.h01[ix] + (double)(((m.b >> 14) & 3) - 1) * S.h01[ixt];
-  return S.u[I] * S.gD[J] + S.w[I] * S.gS[J] + c2 * hd + c4 * hs;
 }
 
-// Sixteen lanes per impact (two impacts per warp): every warp instruction of
-// the per-impact setup serves two impacts, and twice as many impacts' loads
-// are in flight per SM.  Group-local synchronisation only (the two halves of a
-// warp may take different branches).
-constexpr int GL = 32;                // lanes per impact
-constexpr int GPW = 32 / GL;          // impacts per warp
-constexpr int GROUPS = WARPS * GPW;   // impacts per block
+// Edge region: d2 = f1 - g / f2 over y = (p, q1, q2), spread over the four
+// vertex blocks (q1 = block ia, q2 = block ib, the fourth block zero).
+struct Line {
+  double spd[12], f2d[12], gd[12];
+  double sp, g, if2, if2sq, if2cu;
+  int m[4];  // block -> 0 (p), 1 (q1), 2 (q2), -1 (none)
+};
 
-__global__ void __launch_bounds__(32 * WARPS)
+template <int bi, int bj>
+__device__ __forceinline__ void block(const Line &L, double B[9]) {
+  const int pI = L.m[bi], pJ = L.m[bj];
+  if (pI < 0 || pJ < 0) {
+#pragma unroll
+    for (int e = 0; e < 9; e++) B[e] = 0.0;
+    return;
+  }
+  // second derivatives of sp, f1, f2 between the blocks (times the identity)
+  const double spdd = (pI == 1 && pJ == 1) ? -2.0 : ((pI + pJ == 2 && pI != pJ) ? -1.0 : (pI != pJ ? 1.0 : 0.0));
+  const double f1dd = (pI != 2 && pJ != 2) ? (pI == pJ ? 2.0 : -2.0) : 0.0;
+  const double f2dd = (pI != 0 && pJ != 0) ? (pI == pJ ? 2.0 : -2.0) : 0.0;
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const int I = 3 * bi + r;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if (bi == bj && c < r) {
+        B[3 * r + c] = B[3 * c + r];
+        continue;
+      }
+      const int J = 3 * bj + c;
+      const double dl = r == c ? 1.0 : 0.0;
+      const double gdd = 2 * (L.spd[I] * L.spd[J] + L.sp * spdd * dl);
+      const double t1 = -2 * L.g * L.f2d[I] * L.f2d[J] * L.if2cu;
+      const double t2 = (L.gd[I] * L.f2d[J] + L.gd[J] * L.f2d[I]) * L.if2sq;
+      const double t4 = L.g * f2dd * dl * L.if2sq;
+      const double t5 = -gdd * L.if2;
+      B[3 * r + c] = t1 + t2 + f1dd * dl + t4 + t5;
+    }
+  }
+}
+
+// Vertex region, d2 = |p - x_vb|^2: 2 I on (p, p) and (vb, vb), -2 I on (p, vb).
+struct Vertex {
+  int vb;
+};
+template <int bi, int bj>
+__device__ __forceinline__ void block(const Vertex &V, double B[9]) {
+  const bool on = (bi == 0 || bi == V.vb) && (bj == 0 || bj == V.vb);
+  const double d = on ? (bi == bj ? 2.0 : -2.0) : 0.0;
+#pragma unroll
+  for (int e = 0; e < 9; e++) B[e] = (e % 4 == 0) ? d : 0.0;
+}
+
+template <int bi, int bj, class Region>
+__device__ __forceinline__ void emit_pair(const Region &R, double hk, const int pos[16], const double frc[12],
+                                          double *__restrict__ rec) {
+  double B[9];
+  block<bi, bj>(R, B);
+#pragma unroll
+  for (int e = 0; e < 9; e++) B[e] *= hk;  // K = k/2 d2''
+  if (bi == bj) put_record(rec, pos[5 * bi], -1, B, frc[3 * bi], frc[3 * bi + 1], frc[3 * bi + 2]);
+  else put_record(rec, pos[4 * bi + bj], pos[4 * bj + bi], B, 0.0, 0.0, 0.0);
+}
+
+// The impact's vertex forces (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp,
+// w = (1-s-t, s, t) (collision_response.h:89-109), to its force record, then
+// the ten records.
+template <class Region>
+__device__ __forceinline__ void respond(const Region &R, const double fd[3], double hk, double s, double t,
+                                        const int pos[16], double *__restrict__ fo, double *__restrict__ rec) {
+  double frc[12];
+  const double w0 = 1 - (s + t);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const double F = hk * fd[k];
+    frc[k] = -F;
+    frc[3 + k] = w0 * F;
+    frc[6 + k] = s * F;
+    frc[9 + k] = t * F;
+  }
+#pragma unroll
+  for (int k = 0; k < 12; k += 4) st4(fo + k, frc[k], frc[k + 1], frc[k + 2], frc[k + 3]);
+  emit_pair<0, 0>(R, hk, pos, frc, rec);
+  emit_pair<1, 1>(R, hk, pos, frc, rec);
+  emit_pair<2, 2>(R, hk, pos, frc, rec);
+  emit_pair<3, 3>(R, hk, pos, frc, rec);
+  emit_pair<0, 1>(R, hk, pos, frc, rec);
+  emit_pair<0, 2>(R, hk, pos, frc, rec);
+  emit_pair<0, 3>(R, hk, pos, frc, rec);
+  emit_pair<1, 2>(R, hk, pos, frc, rec);
+  emit_pair<1, 3>(R, hk, pos, frc, rec);
+  emit_pair<2, 3>(R, hk, pos, frc, rec);
+}
+
+__global__ void __launch_bounds__(TPB)
     k_imp_deriv(int n, const int4 *__restrict__ imp, const double4 *__restrict__ xc,
                 const int4 *__restrict__ ci, const double4 *__restrict__ cd, double kpen,
-                const int *__restrict__ pos, double *__restrict__ rec, double *__restrict__ frc) {
-  __shared__ PlaneSetup sP[GROUPS];
-  __shared__ LineSetup sL[GROUPS];
-  __shared__ double sx[GROUPS][12];
-  __shared__ double sfd[GROUPS][3];
-  __shared__ int sPos[GROUPS][16];
-  const int lane = threadIdx.x & 31;
-  const int gi = threadIdx.x / GL, gl = threadIdx.x % GL;  // group in the block, lane in the group
-  const unsigned gmask = (GL == 32) ? 0xffffffffu : (((1u << GL) - 1u) << (lane & ~(GL - 1)));
-  const int u = blockIdx.x * GROUPS + gi;
-  if (u >= n) return;  // uniform per group
-  const int *P = pos + 16 * (size_t)u;
-  const int4 c = ci[u];
-  for (int l = gl; l < 16; l += GL) sPos[gi][l] = P[l];
-  if (c.x < 0) {  // no response: zero records, zero forces
-    for (int e = gl; e < 16 * ICF_IMP_REC; e += GL) {
-      const int q = P[e / ICF_IMP_REC];
-      if (q >= 0) rec[ICF_IMP_REC * (size_t)q + e % ICF_IMP_REC] = 0.0;
+                const int *__restrict__ pos16, double *__restrict__ rec, double *__restrict__ frc_out) {
+  const int u = blockIdx.x * TPB + threadIdx.x;
+  if (u >= n) return;
+  int pos[16];
+  {
+    const int4 *P4 = reinterpret_cast<const int4 *>(pos16 + 16 * (size_t)u);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int4 v = __ldg(P4 + k);
+      pos[4 * k] = v.x;
+      pos[4 * k + 1] = v.y;
+      pos[4 * k + 2] = v.z;
+      pos[4 * k + 3] = v.w;
     }
-    for (int l = gl; l < 12; l += GL) frc[12 * (size_t)u + l] = 0.0;
+  }
+  const int4 c = __ldg(ci + u);
+  double *fo = frc_out + 12 * (size_t)u;
+  if (c.x < 0) {  // no response: zero records, zero forces
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      if (pos[k] >= 0) {
+        double *o = rec + ICF_IMP_REC * (size_t)pos[k];
+        st4(o, 0.0, 0.0, 0.0, 0.0);
+        st4(o + 4, 0.0, 0.0, 0.0, 0.0);
+        st4(o + 8, 0.0, 0.0, 0.0, 0.0);
+      }
+#pragma unroll
+    for (int k = 0; k < 12; k += 4) st4(fo + k, 0.0, 0.0, 0.0, 0.0);
     return;
   }
   const double4 cl = cd[u];
-  const int4 id = imp[u];
-  if (gl < 4) {
-    const int nd = gl == 0 ? id.x : gl == 1 ? id.y : gl == 2 ? id.z : id.w;
-    const double4 p = xc[nd];
-    sx[gi][3 * gl] = p.x;
-    sx[gi][3 * gl + 1] = p.y;
-    sx[gi][3 * gl + 2] = p.z;
+  const int4 id = __ldg(imp + u);
+  double x[12];
+  {
+    const int nd[4] = {id.x, id.y, id.z, id.w};
+#pragma unroll
+    for (int b = 0; b < 4; b++) ld_node(xc, nd[b], x + 3 * b);
   }
-  __syncwarp(gmask);
-  const double *x = sx[gi];
   const double hk = kpen * 0.5;
   const int kind = c.x;
-  double c2 = 0, c4 = 0;  // interior: the scalars of HD and HS
+  double fd[3];  // d(d2)/dp
   if (kind == 1) {  // vertex: d2 = |p - x_b|^2
-    if (gl < 3) sfd[gi][gl] = 2 * (x[gl] - x[3 * c.z + gl]);
-  } else if (kind == 2) {  // edge (ia nearer, ib)
-    const int ia = c.y, ib = c.z;
-    LineSetup &L = sL[gi];
-    if (gl == 0) {
-      const double *Pp = x, *Q1 = x + 3 * ia, *Q2 = x + 3 * ib;
-      double sp = 0, f2 = 0;
-      for (int k = 0; k < 3; k++) {
-        L.spd[k] = Q1[k] - Q2[k];
-        L.spd[3 + k] = Pp[k] - 2 * Q1[k] + Q2[k];
-        L.spd[6 + k] = Q1[k] - Pp[k];
-        sp += (Q1[k] - Pp[k]) * (Q2[k] - Q1[k]);
-        const double a = Q1[k] - Pp[k], b = Q2[k] - Q1[k];
-        f2 += b * b;
-        L.f1d[3 + k] = 2 * a;
-        L.f1d[k] = -(2 * a);
-        L.f1d[6 + k] = 0;
-        L.f2d[6 + k] = 2 * b;
-        L.f2d[3 + k] = -(2 * b);
-        L.f2d[k] = 0;
-      }
-      L.sp = sp;
-      L.g = sp * sp;
-      L.f2 = f2;
-      L.f2sq = f2 * f2;
-      L.f2cu = L.f2sq * f2;
-      for (int i = 0; i < 9; i++) L.gd[i] = 2 * sp * L.spd[i];
-      for (int k = 0; k < 3; k++)
-        sfd[gi][k] = L.f1d[k] + (L.g * L.f2d[k] - L.f2 * L.gd[k]) / L.f2sq;
-    }
-  } else {  // interior: d2 = D^2 / S
-    PlaneSetup &S = sP[gi];
-    double a[3], e0[3], e1[3], N[3], e1xa[3], axe0[3], e1xN[3], Nxe0[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      a[k] = x[k] - x[3 + k];
-      e0[k] = x[6 + k] - x[3 + k];
-      e1[k] = x[9 + k] - x[3 + k];
+      const double xb = c.z == 1 ? x[3 + k] : (c.z == 2 ? x[6 + k] : x[9 + k]);
+      fd[k] = 2 * (x[k] - xb);
     }
-#define CROSS(o, u_, v_)                          \
-  o[0] = u_[1] * v_[2] - u_[2] * v_[1];           \
-  o[1] = u_[2] * v_[0] - u_[0] * v_[2];           \
+    respond(Vertex{c.z}, fd, hk, cl.x, cl.y, pos, fo, rec);
+  } else if (kind == 2) {  // edge (ia nearer, ib)
+    const int ia = c.y, ib = c.z;
+    Line L;
+    double Q1[3], Q2[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      Q1[k] = ia == 1 ? x[3 + k] : (ia == 2 ? x[6 + k] : x[9 + k]);
+      Q2[k] = ib == 1 ? x[3 + k] : (ib == 2 ? x[6 + k] : x[9 + k]);
+    }
+    double sp = 0, f2 = 0, spd_p[3], spd_1[3], spd_2[3], f2d_1[3], f2d_2[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double a = Q1[k] - x[k], b = Q2[k] - Q1[k];
+      spd_p[k] = Q1[k] - Q2[k];
+      spd_1[k] = x[k] - 2 * Q1[k] + Q2[k];
+      spd_2[k] = Q1[k] - x[k];
+      sp += a * b;
+      f2 += b * b;
+      f2d_1[k] = -(2 * b);
+      f2d_2[k] = 2 * b;
+    }
+    L.sp = sp;
+    L.g = sp * sp;
+    L.if2 = 1.0 / f2;
+    L.if2sq = L.if2 * L.if2;
+    L.if2cu = L.if2sq * L.if2;
+    L.m[0] = 0;
+#pragma unroll
+    for (int b = 1; b < 4; b++) L.m[b] = b == ia ? 1 : (b == ib ? 2 : -1);
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const int mb = L.m[b];
+        L.spd[3 * b + k] = mb == 0 ? spd_p[k] : (mb == 1 ? spd_1[k] : (mb == 2 ? spd_2[k] : 0.0));
+        L.f2d[3 * b + k] = mb == 1 ? f2d_1[k] : (mb == 2 ? f2d_2[k] : 0.0);
+        L.gd[3 * b + k] = 2 * sp * L.spd[3 * b + k];
+      }
+    // f1 - g / f2 differentiated in p: f1' = -2 (q1 - p), f2' = 0
+#pragma unroll
+    for (int k = 0; k < 3; k++) fd[k] = -(2 * (Q1[k] - x[k])) - L.gd[k] * L.if2;
+    respond(L, fd, hk, cl.x, cl.y, pos, fo, rec);
+  } else {  // interior: d2 = D^2 / S
+    Plane P;
+    double N[3], e1xa[3], axe0[3], e1xN[3], Nxe0[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      P.a[k] = x[k] - x[3 + k];
+      P.e0[k] = x[6 + k] - x[3 + k];
+      P.e1[k] = x[9 + k] - x[3 + k];
+    }
+#define CROSS(o, u_, v_)                \
+  o[0] = u_[1] * v_[2] - u_[2] * v_[1]; \
+  o[1] = u_[2] * v_[0] - u_[0] * v_[2]; \
   o[2] = u_[0] * v_[1] - u_[1] * v_[0];
-    CROSS(N, e0, e1)
-    CROSS(e1xa, e1, a)
-    CROSS(axe0, a, e0)
-    CROSS(e1xN, e1, N)
-    CROSS(Nxe0, N, e0)
+    CROSS(N, P.e0, P.e1)
+    CROSS(e1xa, P.e1, P.a)
+    CROSS(axe0, P.a, P.e0)
+    CROSS(e1xN, P.e1, N)
+    CROSS(Nxe0, N, P.e0)
 #undef CROSS
-    const double D = a[0] * N[0] + a[1] * N[1] + a[2] * N[2];
+    const double D = P.a[0] * N[0] + P.a[1] * N[1] + P.a[2] * N[2];
     const double Sv = N[0] * N[0] + N[1] * N[1] + N[2] * N[2];
     const double iS = 1.0 / Sv;
-    const double c1 = 2.0 * iS, c3 = -2.0 * D * iS * iS, c5 = 2.0 * D * D * iS * iS * iS;
-    c2 = 2.0 * D * iS;
-    c4 = -D * D * iS * iS;
-    for (int l = gl; l < 12; l += GL) {
-      const int b = l / 3, k = l % 3;
-      const double gd = cA(b) * pick3(N, k) + cE0(b) * pick3(e1xa, k) + cE1(b) * pick3(axe0, k);
-      const double gs = 2.0 * (cE0(b) * pick3(e1xN, k) + cE1(b) * pick3(Nxe0, k));
-      S.gD[l] = gd;
-      S.gS[l] = gs;
-      S.u[l] = c1 * gd + c3 * gs;
-      S.w[l] = c3 * gd + c5 * gs;
-    }
-    // HS blocks, S = |e0|^2 |e1|^2 - (e0.e1)^2
-    {
-      const double e00 = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
-      const double e11 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
-      const double e01 = e0[0] * e1[0] + e0[1] * e1[1] + e0[2] * e1[2];
-      for (int l = gl; l < 9; l += GL) {
-        const int r = l / 3, q = l % 3;
-        const double dl = r == q ? 1.0 : 0.0;
-        const double e0r = pick3(e0, r), e0q = pick3(e0, q), e1r = pick3(e1, r), e1q = pick3(e1, q);
-        S.h00[l] = 2.0 * (e11 * dl - e1r * e1q);
-        S.h11[l] = 2.0 * (e00 * dl - e0r * e0q);
-        S.h01[l] = 4.0 * e0r * e1q - 2.0 * e1r * e0q - 2.0 * e01 * dl;
+    P.c1 = 2.0 * iS;
+    P.c3 = -2.0 * D * iS * iS;
+    P.c5 = 2.0 * D * D * iS * iS * iS;
+    P.c2 = 2.0 * D * iS;
+    P.c4 = -D * D * iS * iS;
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        P.gD[3 * b + k] = (double)cA(b) * N[k] + (double)cE0(b) * e1xa[k] + (double)cE1(b) * axe0[k];
+        P.gS[3 * b + k] = 2.0 * ((double)cE0(b) * e1xN[k] + (double)cE1(b) * Nxe0[k]);
       }
-    }
-    // W per vertex-block pair (bi <= bj, the slots' pairs): D is trilinear in
-    // (a, e0, e1), so HD's block (bi, bj) is [W]x, W = -e1 (ai pj0 - pi0 aj) + e0 (ai pj1 - pi1 aj)
-    // - a (pi0 pj1 - pi1 pj0)
-    for (int l = gl; l < 30; l += GL) {
-      const int pr = l / 3, k = l % 3, bi = pair_a(pr), bj = pair_b(pr);
-      const double ai = cA(bi), aj = cA(bj), pi0 = cE0(bi), pj0 = cE0(bj), pi1 = cE1(bi), pj1 = cE1(bj);
-      const double al = ai * pj0 - pi0 * aj, be = ai * pj1 - pi1 * aj, ga = pi0 * pj1 - pi1 * pj0;
-      S.W[l] = -pick3(e1, k) * al + pick3(e0, k) * be - pick3(a, k) * ga;
-    }
+    P.e00 = P.e0[0] * P.e0[0] + P.e0[1] * P.e0[1] + P.e0[2] * P.e0[2];
+    P.e11 = P.e1[0] * P.e1[0] + P.e1[1] * P.e1[1] + P.e1[2] * P.e1[2];
+    P.e01 = P.e0[0] * P.e1[0] + P.e0[1] * P.e1[1] + P.e0[2] * P.e1[2];
     // d(d2)/dp = 2 D N / S
-    if (gl < 3) sfd[gi][gl] = c2 * pick3(N, gl);
-  }
-  __syncwarp(gmask);
-  // one lane per record entry: pair (bA, bB), entry (r, c); a lane's entries
-  // are computed first and stored after, so that their shared-memory reads
-  // overlap
-  constexpr int NS = (90 + GL - 1) / GL;
-  double val[NS];
-  long long dst[NS];
 #pragma unroll
-  for (int k = 0; k < NS; k++) {
-    const int sl = gl + GL * k;
-    val[k] = 0.0;
-    dst[k] = -1;
-    if (sl < 90) {
-      const SlotMeta m = kSlots.s[sl];
-      const int I = m.a & 15, J = (m.a >> 4) & 15;
-      double v = 0;
-      if (kind == 1) {
-        const int vb = c.z, bI = I / 3, bJ = J / 3;
-        if (I % 3 == J % 3 && (bI == 0 || bI == vb) && (bJ == 0 || bJ == vb)) v = (bI == bJ) ? 2.0 : -2.0;
-      } else if (kind == 2) {
-        const int ia = c.y, ib = c.z, bI = I / 3, bJ = J / 3;
-        const int pI = bI == 0 ? 0 : (bI == ia ? 1 : (bI == ib ? 2 : -1));
-        const int pJ = bJ == 0 ? 0 : (bJ == ia ? 1 : (bJ == ib ? 2 : -1));
-        if (pI >= 0 && pJ >= 0) v = line_entry(sL[gi], 3 * pI + I % 3, 3 * pJ + J % 3);
-      } else {
-        v = plane_slot(sP[gi], c2, c4, m);
-      }
-      val[k] = kpen * v / 2;
-      // the code of the pair, taken either way round (none: an anchored vertex)
-      const int q = sPos[gi][m.c & 15];
-      if (q >= 0) {
-        dst[k] = ICF_IMP_REC * (long long)q + ((m.c >> 8) & 15);
-      } else if ((m.c & 15) != ((m.c >> 4) & 15)) {
-        const int q2 = sPos[gi][(m.c >> 4) & 15];
-        if (q2 >= 0) dst[k] = ICF_IMP_REC * (long long)q2 + ((m.c >> 12) & 15);
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < NS; k++)
-    if (dst[k] >= 0) rec[dst[k]] = val[k];
-  // vertex forces (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp, w = (1-s-t, s, t)
-  // (collision_response.h:89-109): into the force record, and as the rhs of
-  // the vertex's diagonal code; off-diagonal codes carry no rhs
-  for (int l = gl; l < 12; l += GL) {
-    const double s = cl.x, t = cl.y;
-    const int comp = l % 3, blk = l / 3;
-    const double F = hk * sfd[gi][comp];
-    const double f = blk == 0 ? -F : (blk == 1 ? (1 - (s + t)) : (blk == 2 ? s : t)) * F;
-    frc[12 * (size_t)u + l] = f;
-    const int q = sPos[gi][5 * blk];
-    if (q >= 0) rec[ICF_IMP_REC * (size_t)q + 9 + comp] = f;
-  }
-  for (int pr = gl; pr < 16; pr += GL) {
-    const int q = sPos[gi][pr];
-    if ((pr >> 2) != (pr & 3) && q >= 0)
-      for (int k = 0; k < 3; k++) rec[ICF_IMP_REC * (size_t)q + 9 + k] = 0.0;
+    for (int k = 0; k < 3; k++) fd[k] = P.c2 * N[k];
+    respond(P, fd, hk, cl.x, cl.y, pos, fo, rec);
   }
 }
 
@@ -354,9 +367,9 @@ int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d, 
 // point passes its own staging).
 int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, const int4 *cls_i, const double4 *cls_d,
                               double *ks, cudaStream_t stream) {
-  k_imp_deriv<<<icf_blocks(ctx->n_imp, GROUPS), 32 * WARPS, 0, stream>>>(
-      ctx->n_imp, ctx->d_imp, xc, cls_i, cls_d, ctx->prm.penaltyK, ctx->d_imp_pos, ks,
-      icf_imp_forces(ks, ctx->n_imp));
+  k_imp_deriv<<<icf_blocks(ctx->n_imp, TPB), TPB, 0, stream>>>(ctx->n_imp, ctx->d_imp, xc, cls_i, cls_d,
+                                                                ctx->prm.penaltyK, ctx->d_imp_pos, ks,
+                                                                icf_imp_forces(ks, ctx->n_imp));
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
