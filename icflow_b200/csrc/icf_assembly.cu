@@ -393,19 +393,58 @@ __global__ void __launch_bounds__(3 * CZ_PER_BLOCK, MINB)
   (void)flag;
 }
 
-// Blocks that only contact pairs create start at zero.
-__global__ void k_zero_dyn(int nd, const int *__restrict__ pos, double *__restrict__ vals) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 9 * nd) return;
-  vals[9 * (size_t)pos[i / 9] + (i % 9)] = 0.0;
+// A 72 B block or a 24 B rhs row (8 B aligned) in 16 B pieces: the split
+// follows the address.
+__device__ __forceinline__ void ld_blk9(const double *o, double b[9]) {
+  if ((reinterpret_cast<uintptr_t>(o) & 8) == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const double2 v = reinterpret_cast<const double2 *>(o)[k];
+      b[2 * k] = v.x;
+      b[2 * k + 1] = v.y;
+    }
+    b[8] = o[8];
+  } else {
+    b[0] = o[0];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const double2 v = reinterpret_cast<const double2 *>(o + 1)[k];
+      b[1 + 2 * k] = v.x;
+      b[2 + 2 * k] = v.y;
+    }
+  }
+}
+__device__ __forceinline__ void st_blk9(double *o, const double b[9]) {
+  if ((reinterpret_cast<uintptr_t>(o) & 8) == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) reinterpret_cast<double2 *>(o)[k] = make_double2(b[2 * k], b[2 * k + 1]);
+    o[8] = b[8];
+  } else {
+    o[0] = b[0];
+#pragma unroll
+    for (int k = 0; k < 4; k++) reinterpret_cast<double2 *>(o + 1)[k] = make_double2(b[1 + 2 * k], b[2 + 2 * k]);
+  }
+}
+__device__ __forceinline__ void add_row3(double *o, const double v[3]) {
+  if ((reinterpret_cast<uintptr_t>(o) & 8) == 0) {
+    const double2 a = reinterpret_cast<const double2 *>(o)[0];
+    reinterpret_cast<double2 *>(o)[0] = make_double2(a.x + v[0], a.y + v[1]);
+    o[2] += v[2];
+  } else {
+    o[0] += v[0];
+    const double2 a = reinterpret_cast<const double2 *>(o + 1)[0];
+    reinterpret_cast<double2 *>(o + 1)[0] = make_double2(a.x + v[1], a.y + v[2]);
+  }
 }
 
 // Impact contributions, one thread per block they touch: the records of the
 // block's codes (k_imp_deriv writes them at the codes' positions in the
-// slot-sorted list, so a block's records are contiguous) are summed in code
-// order and added to the block, and to the rhs row for a diagonal block.  The
-// touched blocks come in k_imp_add's order (icf_pattern.cu k_split_off): the
-// launch over [first, first + count) reads its metadata contiguously.
+// slot-sorted list, so a block's records are contiguous; 96 B each, read as
+// three 32 B loads) are summed in code order and added to the block, and to
+// the rhs row for a diagonal block (row >= 0).  A block that only contact
+// pairs create (row == -2) is written, not added to: nothing else writes it.
+// The touched blocks come in k_imp_add's order (icf_pattern.cu k_split_off):
+// the launch over [first, first + count) reads its metadata contiguously.
 __global__ void k_imp_add(int count, int first, const int2 *__restrict__ range, const int *__restrict__ pslot,
                           const int *__restrict__ row, const double *__restrict__ rec, double *__restrict__ vals,
                           double *__restrict__ rhs, int *__restrict__ nonfinite) {
@@ -417,27 +456,37 @@ __global__ void k_imp_add(int count, int first, const int2 *__restrict__ range, 
     const int s = pslot[w], rw = row[w];
     double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int q = qr.x; q < qr.y; q++) {
-      const double2 *R = reinterpret_cast<const double2 *>(rec + ICF_IMP_REC * (size_t)q);
+      const double4 *R = reinterpret_cast<const double4 *>(rec + ICF_IMP_REC * (size_t)q);
+      double4 r[3];
 #pragma unroll
-      for (int k = 0; k < 6; k++) {
-        const double2 r2 = __ldg(R + k);
-        v[2 * k] += r2.x;
-        v[2 * k + 1] += r2.y;
-      }
-    }
-    double *o = vals + 9 * (size_t)s;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      o[k] += v[k];
-      bad |= !isfinite(v[k]);
-    }
-    if (rw >= 0) {
-      double *r = rhs + 3 * (size_t)rw;
+      for (int k = 0; k < 3; k++)
+        asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+            : "=d"(r[k].x), "=d"(r[k].y), "=d"(r[k].z), "=d"(r[k].w)
+            : "l"(R + k));
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        r[k] += v[9 + k];
-        bad |= !isfinite(v[9 + k]);
+        v[4 * k] += r[k].x;
+        v[4 * k + 1] += r[k].y;
+        v[4 * k + 2] += r[k].z;
+        v[4 * k + 3] += r[k].w;
       }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) bad |= !isfinite(v[k]);
+    double *o = vals + 9 * (size_t)s;
+    if (rw == -2) {
+      st_blk9(o, v);
+    } else {
+      double b[9];
+      ld_blk9(o, b);
+#pragma unroll
+      for (int k = 0; k < 9; k++) b[k] += v[k];
+      st_blk9(o, b);
+    }
+    if (rw >= 0) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) bad |= !isfinite(v[9 + k]);
+      add_row3(rhs + 3 * (size_t)rw, v + 9);
     }
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(nonfinite, 1);
@@ -823,10 +872,7 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   ICF_CUDA(ctx, cudaStreamWaitEvent(sa, e_fork, 0));
   ICF_CUDA(ctx, cudaStreamWaitEvent(sb, e_fork, 0));
 
-  // aux1: contact-only blocks start at zero; impact units
-  if (ctx->n_dyn > 0)
-    k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, sb>>>(ctx->n_dyn, ctx->d_dynpos, ctx->d_vals);
-  if (ctx->n_dyn > 0) icf_prof_mark(ctx, sb, "k_zero_dyn", 76LL * ctx->n_dyn);
+  // aux1: impact units
   if (ctx->n_imp > 0) {
     const int rc = icf_launch_imp_unit(ctx, sb);
     if (rc) return rc;
@@ -1185,8 +1231,6 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
   const double nb = ctx->prm.NewmarkBeta, ng = ctx->prm.NewmarkGamma;
   const double sc = 1.0 + ctx->prm.dampingStiffness * ng / (h * nb);
   const double mc = (1.0 / (h * h) + ctx->prm.dampingMass * ng / h) / nb * (ctx->prm.rho / 20.0);
-  if (ctx->n_dyn > 0)
-    k_zero_dyn<<<icf_blocks(9LL * ctx->n_dyn, 256), 256, 0, s>>>(ctx->n_dyn, ctx->d_dynpos, B.vals);
   if (fused) {
     ICF_TRY_RC(icf_launch_tile_fused(ctx, B.xc, B.va, B.cs, sc, mc, B.vals, B.rhs, s));
   } else if (icf_tiles_active(ctx)) {

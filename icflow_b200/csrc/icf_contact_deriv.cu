@@ -38,7 +38,13 @@
 
 namespace {
 
-constexpr int TPB = 128;
+#ifndef IMP_TPB
+#define IMP_TPB 128
+#endif
+#ifndef IMP_MINB
+#define IMP_MINB 1
+#endif
+constexpr int TPB = IMP_TPB;
 
 // coefficients of vertex block b (p, v0, v1, v2) in a = p - v0,
 // e0 = v1 - v0, e1 = v2 - v0 (compile-time after unrolling)
@@ -220,7 +226,7 @@ __device__ __forceinline__ void respond(const Region &R, const double fd[3], dou
   emit_pair<2, 3>(R, hk, pos, frc, rec);
 }
 
-__global__ void __launch_bounds__(TPB)
+__global__ void __launch_bounds__(TPB, IMP_MINB)
     k_imp_deriv(int n, const int4 *__restrict__ imp, const double4 *__restrict__ xc,
                 const int4 *__restrict__ ci, const double4 *__restrict__ cd, double kpen,
                 const int *__restrict__ pos16, double *__restrict__ rec, double *__restrict__ frc_out) {

@@ -288,8 +288,9 @@ __global__ void k_flag_off(int n, const int *__restrict__ slot, const unsigned l
 // the touched slots in k_imp_add's order, a stable partition: diagonal and
 // contact-only blocks at [0, n_a), static off-diagonal ones at [n_a, n), each
 // part in slot order (so a warp's records and blocks lie close together); per
-// slot its record range, slot and rhs row (diagonal blocks) or -1.  pref: the
-// exclusive prefix sum of k_flag_off's flags.
+// slot its record range, slot and rhs row (diagonal blocks), -1 (static
+// off-diagonal blocks) or -2 (contact-only blocks, which k_imp_add writes
+// rather than adds to).  pref: the exclusive prefix sum of k_flag_off's flags.
 __global__ void k_split_off(int n, int n_a, const int *__restrict__ slot, const int *__restrict__ off,
                             const unsigned long long *__restrict__ mkey, const int *__restrict__ pref,
                             int2 *__restrict__ range, int *__restrict__ pslot, int *__restrict__ row) {
@@ -301,7 +302,7 @@ __global__ void k_split_off(int n, int n_a, const int *__restrict__ slot, const 
   range[p] = make_int2(off[g], off[g + 1]);
   pslot[p] = sl;
   const unsigned long long k = mkey[sl];
-  row[p] = (k >> 32) == (k & 0xffffffffull) ? (int)(k & 0xffffffffull) : -1;
+  row[p] = (k >> 32) == (k & 0xffffffffull) ? (int)(k & 0xffffffffull) : (f ? -1 : -2);
 }
 
 __global__ void k_cand_imp_rc(int ni, const int4 *__restrict__ imp, const int *__restrict__ alt,
