@@ -324,6 +324,7 @@ __global__ void k_grid_clear(const int *__restrict__ gp, int *__restrict__ a, in
 }
 
 // count (off == nullptr) or place the surface nodes in the dense grid
+#define ICF_DET_IDBITS 26
 __global__ void k_node_put(int ns, const int *__restrict__ snode, const double4 *__restrict__ xc,
                            const double *__restrict__ red, const int *__restrict__ gp, int *__restrict__ cnt,
                            const int *__restrict__ off, double4 *__restrict__ ent) {
@@ -337,13 +338,16 @@ __global__ void k_node_put(int ns, const int *__restrict__ snode, const double4 
   if (cx < 0 || cy < 0 || cz < 0 || cx >= nx || cy >= ny || cz >= nz) return;
   const long long l = cell_lin(cx, cy, cz, ny, nz);
   const int w = atomicAdd(cnt + l, 1);
-  if (off) ent[off[l] + w] = make_double4(P.x, P.y, P.z, (double)k);
+  // the fourth component carries the surface-node index and the node id,
+  // k 2^26 + p (an integer below 2^52, exact in a double)
+  if (off) ent[off[l] + w] = make_double4(P.x, P.y, P.z, (double)(((long long)k << ICF_DET_IDBITS) | snode[k]));
 }
 
-// per surface element: the inverse of its edge matrix (as k_narrow computes
-// it) and its first vertex, 12 doubles
-__global__ void k_tet_inv(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
-                          double *__restrict__ inv) {
+// per surface element, for the detection: its box (as k_boxes) and largest
+// extent, and the inverse of its edge matrix (as k_narrow computes it) with
+// its first vertex, 12 doubles; one read of its four nodes serves both
+__global__ void k_boxes_inv(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc, double pad,
+                            double *__restrict__ lohi, double *__restrict__ ext, double *__restrict__ inv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int4 id = selem[i];
@@ -354,6 +358,18 @@ __global__ void k_tet_inv(int n, const int4 *__restrict__ selem, const double4 *
     const double4 p = xc[nn[k]];
     x[3 * k] = p.x; x[3 * k + 1] = p.y; x[3 * k + 2] = p.z;
   }
+  double lo[3], hi[3], e = 0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    lo[k] = fmin(fmin(fmin(x[k], x[3 + k]), x[6 + k]), x[9 + k]) - pad;
+    hi[k] = fmax(fmax(fmax(x[k], x[3 + k]), x[6 + k]), x[9 + k]) + pad;
+    e = fmax(e, hi[k] - lo[k]);
+  }
+  double2 *l = reinterpret_cast<double2 *>(lohi + 6 * (size_t)i);
+  l[0] = make_double2(lo[0], lo[1]);
+  l[1] = make_double2(lo[2], hi[0]);
+  l[2] = make_double2(hi[1], hi[2]);
+  ext[i] = e;
   double b[9];
   tet_inverse(x, b);
   double2 *o = reinterpret_cast<double2 *>(inv + 12 * (size_t)i);
@@ -377,13 +393,17 @@ __device__ __forceinline__ bool pair_exists(int k, int b, const int *__restrict_
   return false;
 }
 
-// eight threads per surface element b, each taking every eighth cell its box
-// reaches: keys k << eb | b of its impacts (k the surface-node index) and a
-// count per surface node
-__global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
+// eight threads per surface element b: the entries of the cells its box
+// reaches are dealt out by their index modulo 8, so the threads share the
+// work evenly however it falls into cells; keys k << eb | b of its impacts
+// (k the surface-node index) and a count per surface node
+#ifndef DET_MINB
+#define DET_MINB 8
+#endif
+__global__ void __launch_bounds__(128, DET_MINB) k_detect(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
                                                 const double *__restrict__ lohi, const int4 *__restrict__ clo,
                                                 const int *__restrict__ gp, const int *__restrict__ goff,
-                                                const double4 *__restrict__ gnode, const int *__restrict__ snode,
+                                                const double4 *__restrict__ gnode,
                                                 const int *__restrict__ sinc_off, const int *__restrict__ sinc,
                                                 const int *__restrict__ group, int eb,
                                                 unsigned long long *__restrict__ out, long long cap,
@@ -394,22 +414,43 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
   if (b >= n || gp[4] != 0) return;
   const int ny = gp[1], nz = gp[2];
   const int4 B = selem[b];
-  const int nb[4] = {B.x, B.y, B.z, B.w};
   const double *lh = lohi + 6 * (size_t)b;
   const double lx = lh[0], ly = lh[1], lz = lh[2], hx = lh[3], hy = lh[4], hz = lh[5];
   const int4 c = clo[b];
   const int sx = c.w & 1023, sy = (c.w >> 10) & 1023, sz = (c.w >> 20) & 1023;
-  const int ncell = (sx + 1) * (sy + 1) * (sz + 1);
-  for (int j = g; j < ncell; j += 8) {
-    const int dz = j % (sz + 1), dy = (j / (sz + 1)) % (sy + 1), dx = j / ((sz + 1) * (sy + 1));
-    const long long l = cell_lin(c.x + dx, c.y + dy, c.z + dz, ny, nz);
-    const int e1 = goff[l + 1];
-    for (int e = goff[l]; e < e1; e++) {
+  // the (x, y) columns of the box's cells: a run of cells along z is
+  // contiguous in the grid, so a column's entries are one range; the next
+  // column's range is read while this one's entries are tested
+  const int ncol = (sx + 1) * (sy + 1);
+  long long l = cell_lin(c.x, c.y, c.z, ny, nz);
+  int e0 = goff[l], e1 = goff[l + sz + 1];
+#ifdef DET_PREFETCH_INV
+  // b's inverse and first vertex (the eight threads read the same line)
+  double bi[9], x0[3];
+  {
+    const double2 *r = reinterpret_cast<const double2 *>(inv + 12 * (size_t)b);
+    const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5];
+    bi[0] = r0.x; bi[1] = r0.y; bi[2] = r1.x; bi[3] = r1.y; bi[4] = r2.x; bi[5] = r2.y;
+    bi[6] = r3.x; bi[7] = r3.y; bi[8] = r4.x;
+    x0[0] = r4.y; x0[1] = r5.x; x0[2] = r5.y;
+  }
+#endif
+  for (int j = 0; j < ncol; j++) {
+    int f0 = 0, f1 = 0;
+    if (j + 1 < ncol) {
+      const int dx = (j + 1) / (sy + 1), dy = (j + 1) % (sy + 1);
+      l = cell_lin(c.x + dx, c.y + dy, c.z, ny, nz);
+      f0 = goff[l];
+      f1 = goff[l + sz + 1];
+    }
+    // thread g takes the entries whose index is g modulo 8
+    for (int e = e0 + ((g - e0) & 7); e < e1; e += 8) {
       const double4 P = gnode[e];
       if (!(P.x >= lx && P.x <= hx && P.y >= ly && P.y <= hy && P.z >= lz && P.z <= hz)) continue;
-      const int k = (int)P.w;
-      const int p = snode[k];
-      if (p == nb[0] || p == nb[1] || p == nb[2] || p == nb[3]) continue;
+      const long long kp = (long long)P.w;
+      const int p = (int)(kp & ((1LL << ICF_DET_IDBITS) - 1));
+      if (p == B.x || p == B.y || p == B.z || p == B.w) continue;
+#ifndef DET_PREFETCH_INV
       // b's inverse and first vertex, read when a node lies in its box
       double bi[9], x0[3];
       {
@@ -419,12 +460,16 @@ __global__ void __launch_bounds__(128) k_detect(int n, const int4 *__restrict__ 
         bi[6] = r3.x; bi[7] = r3.y; bi[8] = r4.x;
         x0[0] = r4.y; x0[1] = r5.x; x0[2] = r5.y;
       }
+#endif
       if (!tet_contains(bi, P.x - x0[0], P.y - x0[1], P.z - x0[2])) continue;
+      const int k = (int)(kp >> ICF_DET_IDBITS);
       if (!pair_exists(k, b, sinc_off, sinc, lohi, group, selem, xc)) continue;
       const int w = atomicAdd(count, 1);
       atomicAdd(kcnt + k, 1);
       if (w < cap) out[w] = ((unsigned long long)(unsigned)k << eb) | (unsigned)b;
     }
+    e0 = f0;
+    e1 = f1;
   }
 }
 
@@ -622,11 +667,10 @@ static int enqueue_detect(icf_ctx *ctx, double pad, const int *d_group, int eb, 
   icf_contact_ws &W = ctx->cws;
   const int nbk = (int)std::min<long long>((n + 255) / 256, 2LL * ctx->n_sm);
   const long long cap_cells = W.cell_cap;
-  k_boxes<<<icf_blocks(n, 256), 256, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext);
+  k_boxes_inv<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, pad, W.lohi, W.ext, W.tinv);
   k_red7<<<nbk, 256, 0, s>>>(n, W.lohi, W.ext, W.tmpv);
   k_red7_final<<<1, 256, 0, s>>>(nbk, n, W.tmpv, W.red);
   k_grid_params<<<1, 32, 0, s>>>(n, cap_cells, W.red, W.gp);
-  k_tet_inv<<<icf_blocks(n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.tinv);
   // the surface nodes by cell (over the high-water count of cells: the
   // counts past this call's C are never read)
   k_grid_clear<<<2 * ctx->n_sm, 256, 0, s>>>(W.gp, W.gcnt, W.gcur);
@@ -639,7 +683,7 @@ static int enqueue_detect(icf_ctx *ctx, double pad, const int *d_group, int eb, 
   ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, sizeof(int), s));
   ICF_CUDA(ctx, cudaMemsetAsync(W.kcnt, 0, sizeof(int) * (ns + 1LL), s));
   k_detect<<<icf_blocks(8LL * n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, W.gp, W.goff, W.gnode,
-                                                   ctx->d_snode, ctx->d_sinc_off, ctx->d_sinc, d_group, eb, W.nk0,
+                                                   ctx->d_sinc_off, ctx->d_sinc, d_group, eb, W.nk0,
                                                    W.nkey_cap, W.d_small + 5, W.kcnt, W.tinv);
   ICF_CUDA(ctx, cudaGetLastError());
   // grouped by surface node (a counting sort), each node's hits sorted: the
@@ -746,6 +790,8 @@ int icf_detect_contacts_impl(icf_ctx *ctx, double pad, const int *d_group, int *
     ctx->n_imp = 0;
     return ICF_OK;
   }
+  if (ctx->n_nodes >= (1 << ICF_DET_IDBITS) || ns >= (1 << ICF_DET_IDBITS))
+    return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: more than 2^26 nodes");
   ICF_TRY_RC(ensure_small(ctx));
   if (n > W.b_cap) {
     ICF_TRY_RC(grow(ctx, &W.lohi, 6LL * n));

@@ -149,16 +149,20 @@ class GPU_Functionality:
         self.nPairs = n.value
         return n.value
 
-    def DetectContacts(self, pad: float = 0.0, same_mesh: bool = True) -> np.ndarray:
+    def DetectContacts(self, pad: float = 0.0, same_mesh: bool = True, copy_back: bool = True):
         """The impacts BroadPhase(pad, same_mesh) followed by
         NarrowPhaseCollisionDetection(None) gives, found without the pair
         list (one query per surface node in a grid of the surface elements).
         Returns the impact list (node, face vertices) as
-        NarrowPhaseCollisionDetection does."""
+        NarrowPhaseCollisionDetection does.  With copy_back=False the list
+        stays on the device, where CreateStructure and the assembly read it,
+        and only its length is returned."""
         self._set_groups(same_mesh)
         n = C.c_int()
         check(self.ctx, self.lib.icf_detect_contacts(self.ctx, float(pad), C.byref(n)))
         self.nImpacts = self.cf.nCollisions = n.value
+        if not copy_back:
+            return n.value
         self.c_itet = np.zeros((n.value, 4), np.int32)
         if n.value:
             check(self.ctx, self.lib.icf_get_impacts(self.ctx, n.value, iptr(self.c_itet)))
