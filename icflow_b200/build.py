@@ -22,7 +22,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           "--expt-relaxed-constexpr"]
 # Files whose integer outputs depend on floating-point comparisons are built
 # without fused multiply-add so that every operation rounds on its own.
-NO_FMA = {"icf_contact.cu", "icf_broad.cu"}
+NO_FMA = {"icf_contact.cu", "icf_broad.cu", "icf_contact_deriv.cu"}
 SOURCES = ["icf_api.cu", "icf_assembly.cu", "icf_pattern.cu", "icf_contact.cu", "icf_contact_deriv.cu",
            "icf_noalloc.cu", "icf_gather.cu", "icf_tune.cu", "icf_solve.cu", "icf_broad.cu", "icf_mlp.cu",
            "icf_tile.cu"]

@@ -213,7 +213,7 @@ static void free_all(icf_ctx *c) {
                   c->d_es, c->d_cs, c->d_ks, c->d_skeys, c->d_rc_off, c->d_rc, c->d_rows, c->d_cols,
                   c->d_src, c->d_mkeys, c->d_imp, c->d_cr_slot, c->d_cr_off, c->d_cr, c->d_cr_range, c->d_cr_pslot,
                   c->d_cr_row, c->d_pairs,
-                  c->d_masks, c->d_imp_ci, c->d_imp_cd, c->d_rc_mid, c->d_diag, c->d_offd,
+                  c->d_masks, c->d_rc_mid, c->d_diag, c->d_offd,
                   c->d_s2m, c->d_dynpos, c->d_gdesc_diag, c->d_vals, c->d_rhs, c->d_nodeF, c->tet_inc.off, c->tet_inc.inc,
                   c->imp_inc.off, c->imp_inc.inc, c->d_tmp, c->sell_off.meta, c->sell_off.unit,
                   c->sell_off.codes, c->sell_diag.meta, c->sell_diag.unit, c->sell_diag.codes,
@@ -421,7 +421,7 @@ int icf_transfer_static(icf_ctx *ctx, int n_nodes, const double *x0, const int *
   ctx->d_u = ctx->d_v = ctx->d_a = ctx->d_du = ctx->d_un = ctx->d_h3 = nullptr;
   ctx->d_czs = nullptr; ctx->d_czfail = nullptr; ctx->d_cztent = nullptr; ctx->d_czflags = nullptr;
   ctx->d_czavg = nullptr; ctx->d_czprm = nullptr; ctx->d_es = nullptr; ctx->d_cs = nullptr;
-  ctx->d_ks = nullptr; ctx->ks_cap = 0; ctx->d_imp_ci = nullptr; ctx->d_imp_cd = nullptr;
+  ctx->d_ks = nullptr; ctx->ks_cap = 0;
   ctx->d_rc_mid = ctx->d_diag = ctx->d_offd = nullptr; ctx->n_offd = 0;
   ctx->d_s2m = ctx->d_dynpos = nullptr; ctx->s2m_cap = ctx->dynpos_cap = ctx->n_dyn = 0;
   ctx->d_gdesc_diag = ctx->d_gdesc_off = nullptr; ctx->gdesc_cap = 0; ctx->d_skeys = nullptr; ctx->d_rc_off = nullptr; ctx->d_rc = nullptr;

@@ -1225,7 +1225,7 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
     ICF_TRY_RC(icf_launch_cz(ctx, ctx->tune_cz, B.xc, B.cs, s));
   }
   if (ctx->n_imp > 0) {
-    const int rc = icf_launch_imp_unit_bufs(ctx, B.xc, B.ci, B.cd, B.ks, s);
+    const int rc = icf_launch_imp_unit_bufs(ctx, B.xc, B.ks, s);
     if (rc) return rc;
   }
   const double nb = ctx->prm.NewmarkBeta, ng = ctx->prm.NewmarkGamma;

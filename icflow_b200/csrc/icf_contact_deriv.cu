@@ -1,8 +1,10 @@
 // icf_contact_deriv.cu -- penalty response of the impacts, one thread per impact.
 //
-// kCollisionResponseForce (collision_response.h:38-127) needs the gradient
-// and Hessian of the squared point-triangle distance d2(x), x = (p, v0, v1,
-// v2), in the Voronoi region found by k_imp_classify (icf_contact.cu):
+// kCollisionResponseForce (collision_response.h:38-127): whether the impact
+// responds (a vertex off the anchors, distance above DistanceEpsilon, :47-51
+// and :91), then the gradient and Hessian of the squared point-triangle
+// distance d2(x), x = (p, v0, v1, v2), in its Voronoi region (pt_classify,
+// icf_ptri.cuh):
 //   vertex region  d2 = |p - v|^2
 //   edge region    d2 = f1 - g / f2,  f1 = |q1-p|^2, g = ((q1-p).(q2-q1))^2,
 //                  f2 = |q2-q1|^2   (point_triange_v2.h:152-232)
@@ -34,7 +36,11 @@
 // block's lower entries are its upper ones, so it is symmetric bit for bit.
 // The four vertex forces also go to a per-impact force record (node forces).
 #include "icf_internal.cuh"
+#include "icf_ptri.cuh"
 #include "icf_tet.cuh"
+
+// This file is compiled with -fmad=false (pt_classify's region decision must
+// round every operation on its own); the Hessian arithmetic is unfused too.
 
 namespace {
 
@@ -227,9 +233,9 @@ __device__ __forceinline__ void respond(const Region &R, const double fd[3], dou
 }
 
 __global__ void __launch_bounds__(TPB, IMP_MINB)
-    k_imp_deriv(int n, const int4 *__restrict__ imp, const double4 *__restrict__ xc,
-                const int4 *__restrict__ ci, const double4 *__restrict__ cd, double kpen,
-                const int *__restrict__ pos16, double *__restrict__ rec, double *__restrict__ frc_out) {
+    k_imp_deriv(int n, const int4 *__restrict__ imp, const int *__restrict__ alt, const double4 *__restrict__ xc,
+                double eps2, double kpen, const int *__restrict__ pos16, double *__restrict__ rec,
+                double *__restrict__ frc_out, int *__restrict__ counts) {
   const int u = blockIdx.x * TPB + threadIdx.x;
   if (u >= n) return;
   int pos[16];
@@ -244,9 +250,28 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
       pos[4 * k + 3] = v.w;
     }
   }
-  const int4 c = __ldg(ci + u);
+  const int4 id = __ldg(imp + u);
+  const int nd[4] = {id.x, id.y, id.z, id.w};
+  bool any_active = false, valid = true;
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    valid &= nd[b] >= 0;
+    any_active |= (nd[b] >= 0 && __ldg(alt + nd[b]) >= 0);
+  }
+  double x[12];
+  pt_cls cl;
+  cl.kind = -1;
+  if (valid && any_active) {
+#pragma unroll
+    for (int b = 0; b < 4; b++) ld_node(xc, nd[b], x + 3 * b);
+    cl = pt_classify(x);
+    if (!(cl.dsq > eps2)) cl.kind = -1;  // within DistanceEpsilon: no response
+  }
+  // the impacts that respond, one atomic per warp
+  const unsigned act = __ballot_sync(__activemask(), cl.kind >= 0);
+  if ((threadIdx.x & 31) == __ffs(__activemask()) - 1 && act) atomicAdd(counts + 3, __popc(act));
   double *fo = frc_out + 12 * (size_t)u;
-  if (c.x < 0) {  // no response: zero records, zero forces
+  if (cl.kind < 0) {  // no response: zero records, zero forces
 #pragma unroll
     for (int k = 0; k < 16; k++)
       if (pos[k] >= 0) {
@@ -259,14 +284,8 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
     for (int k = 0; k < 12; k += 4) st4(fo + k, 0.0, 0.0, 0.0, 0.0);
     return;
   }
-  const double4 cl = cd[u];
-  const int4 id = __ldg(imp + u);
-  double x[12];
-  {
-    const int nd[4] = {id.x, id.y, id.z, id.w};
-#pragma unroll
-    for (int b = 0; b < 4; b++) ld_node(xc, nd[b], x + 3 * b);
-  }
+  const int4 c = make_int4(cl.kind, cl.ia, cl.ib, 0);
+  const double2 st = make_double2(cl.s, cl.t);
   const double hk = kpen * 0.5;
   const int kind = c.x;
   double fd[3];  // d(d2)/dp
@@ -276,7 +295,7 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
       const double xb = c.z == 1 ? x[3 + k] : (c.z == 2 ? x[6 + k] : x[9 + k]);
       fd[k] = 2 * (x[k] - xb);
     }
-    respond(Vertex{c.z}, fd, hk, cl.x, cl.y, pos, fo, rec);
+    respond(Vertex{c.z}, fd, hk, st.x, st.y, pos, fo, rec);
   } else if (kind == 2) {  // edge (ia nearer, ib)
     const int ia = c.y, ib = c.z;
     Line L;
@@ -318,7 +337,7 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
     // f1 - g / f2 differentiated in p: f1' = -2 (q1 - p), f2' = 0
 #pragma unroll
     for (int k = 0; k < 3; k++) fd[k] = -(2 * (Q1[k] - x[k])) - L.gd[k] * L.if2;
-    respond(L, fd, hk, cl.x, cl.y, pos, fo, rec);
+    respond(L, fd, hk, st.x, st.y, pos, fo, rec);
   } else {  // interior: d2 = D^2 / S
     Plane P;
     double N[3], e1xa[3], axe0[3], e1xN[3], Nxe0[3];
@@ -359,23 +378,23 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
     // d(d2)/dp = 2 D N / S
 #pragma unroll
     for (int k = 0; k < 3; k++) fd[k] = P.c2 * N[k];
-    respond(P, fd, hk, cl.x, cl.y, pos, fo, rec);
+    respond(P, fd, hk, st.x, st.y, pos, fo, rec);
   }
 }
 
 }  // namespace
 
-int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d, cudaStream_t stream) {
-  return icf_launch_imp_deriv_bufs(ctx, ctx->d_xc, cls_i, cls_d, ctx->d_ks, stream);
+int icf_launch_imp_deriv(icf_ctx *ctx, cudaStream_t stream) {
+  return icf_launch_imp_deriv_bufs(ctx, ctx->d_xc, ctx->d_ks, stream);
 }
 
 // Derivative kernel with caller-chosen buffers (the allocation-free entry
 // point passes its own staging).
-int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, const int4 *cls_i, const double4 *cls_d,
-                              double *ks, cudaStream_t stream) {
-  k_imp_deriv<<<icf_blocks(ctx->n_imp, TPB), TPB, 0, stream>>>(ctx->n_imp, ctx->d_imp, xc, cls_i, cls_d,
+int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, double *ks, cudaStream_t stream) {
+  const double eps2 = ctx->prm.DistanceEpsilon * ctx->prm.DistanceEpsilon;
+  k_imp_deriv<<<icf_blocks(ctx->n_imp, TPB), TPB, 0, stream>>>(ctx->n_imp, ctx->d_imp, ctx->d_alt, xc, eps2,
                                                                 ctx->prm.penaltyK, ctx->d_imp_pos, ks,
-                                                                icf_imp_forces(ks, ctx->n_imp));
+                                                                icf_imp_forces(ks, ctx->n_imp), ctx->d_counts);
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }

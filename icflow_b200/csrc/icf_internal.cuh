@@ -325,8 +325,6 @@ struct icf_ctx {
   icf_contact_ws cws;
   // per-impact classification {kind, ia, ib, 0} and {s, t, dsq, 0}; same
   // capacity as the impact staging d_ks (ks_cap)
-  int4 *d_imp_ci = nullptr;
-  double4 *d_imp_cd = nullptr;
   int n_crs = 0;                  // slots touched by impacts
   int *d_cr_slot = nullptr, *d_cr_off = nullptr;
   uint32_t *d_cr = nullptr;
@@ -508,7 +506,7 @@ int icf_launch_add_dx(icf_ctx *ctx, const double *d_dx);
 int icf_launch_accept(icf_ctx *ctx, double h);
 int icf_launch_commit_cz(icf_ctx *ctx);
 int icf_launch_imp_unit(icf_ctx *ctx, cudaStream_t stream);
-int icf_launch_imp_deriv(icf_ctx *ctx, const int4 *cls_i, const double4 *cls_d, cudaStream_t stream);
+int icf_launch_imp_deriv(icf_ctx *ctx, cudaStream_t stream);
 int icf_get_node_inc(icf_ctx *ctx, icf_node_inc *tets, icf_node_inc *imps);
 
 // Buffers of one assembly when the caller, not the context, provides them
@@ -519,13 +517,9 @@ struct icf_asm_bufs {
   double2 *va;                 // 3*n_nodes
   double4 *es;                 // 8*n_elem
   double *cs;                  // ICF_CZ_STAGE*n_cz
-  int4 *ci;                    // n_imp
-  double4 *cd;                 // n_imp
   double *ks;                  // ICF_IMP_STAGE*n_imp
   double *vals, *rhs;          // outputs, nnz*9 and N*3
 };
 int icf_enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, cudaStream_t s);
-int icf_launch_imp_unit_bufs(icf_ctx *ctx, const double4 *xc, int4 *ci, double4 *cd, double *ks,
-                             cudaStream_t stream);
-int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, const int4 *cls_i, const double4 *cls_d,
-                              double *ks, cudaStream_t stream);
+int icf_launch_imp_unit_bufs(icf_ctx *ctx, const double4 *xc, double *ks, cudaStream_t stream);
+int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, double *ks, cudaStream_t stream);

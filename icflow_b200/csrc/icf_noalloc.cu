@@ -11,7 +11,7 @@
 // cudaFree or allocating library routine.
 //
 // The array's size is fixed at ICF_NOALLOC_BYTES (8 MiB).  A model whose
-// temporaries do not fit (80 B per node, 256 B per tet, 384 B per CZ, 1104 B
+// temporaries do not fit (80 B per node, 256 B per tet, 384 B per CZ, 1056 B
 // per impact, each section rounded up to 256 B) is rejected with
 // ICF_ERR_SIZE and a message giving both numbers.
 //
@@ -63,10 +63,8 @@ extern "C" int icf_assemble_noalloc(icf_ctx *ctx, double h, const double *d_un, 
   const size_t b_xc = round256(sizeof(double4) * n), b_va = round256(sizeof(double2) * 3 * n);
   const size_t b_es = round256(sizeof(double4) * 8 * (size_t)ctx->n_elem);
   const size_t b_cs = round256(sizeof(double) * ICF_CZ_STAGE * (size_t)ctx->n_cz);
-  const size_t b_ci = round256(sizeof(int4) * (size_t)ctx->n_imp);
-  const size_t b_cd = round256(sizeof(double4) * (size_t)ctx->n_imp);
   const size_t b_ks = round256(sizeof(double) * ICF_IMP_STAGE * (size_t)ctx->n_imp);
-  const size_t need = b_xc + b_va + b_es + b_cs + b_ci + b_cd + b_ks;
+  const size_t need = b_xc + b_va + b_es + b_cs + b_ks;
   if (need > ICF_NOALLOC_BYTES)
     return icf_fail(ctx, ICF_ERR_SIZE,
                     "model needs " + std::to_string(need) + " bytes of scratch; the allocation-free "
@@ -99,10 +97,6 @@ extern "C" int icf_assemble_noalloc(icf_ctx *ctx, double h, const double *d_un, 
   p += b_es;
   B.cs = reinterpret_cast<double *>(p);
   p += b_cs;
-  B.ci = reinterpret_cast<int4 *>(p);
-  p += b_ci;
-  B.cd = reinterpret_cast<double4 *>(p);
-  p += b_cd;
   B.ks = reinterpret_cast<double *>(p);
   B.vals = d_vals;
   B.rhs = d_rhs;

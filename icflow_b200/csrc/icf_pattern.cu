@@ -959,15 +959,9 @@ int icf_build_merged_pattern(icf_ctx *ctx) {
     // impact staging
     if (ctx->n_imp > ctx->ks_cap) {
       cudaFree(ctx->d_ks);
-      cudaFree(ctx->d_imp_ci);
-      cudaFree(ctx->d_imp_cd);
       ctx->d_ks = nullptr;
-      ctx->d_imp_ci = nullptr;
-      ctx->d_imp_cd = nullptr;
       const size_t cap = 2 * (size_t)ctx->n_imp;
       ICF_CUDA(ctx, cudaMalloc(&ctx->d_ks, sizeof(double) * ICF_IMP_STAGE * cap));
-      ICF_CUDA(ctx, cudaMalloc(&ctx->d_imp_ci, sizeof(int4) * cap));
-      ICF_CUDA(ctx, cudaMalloc(&ctx->d_imp_cd, sizeof(double4) * cap));
       ctx->ks_cap = (int)cap;
     }
   }

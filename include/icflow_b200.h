@@ -275,7 +275,7 @@ int icf_set_variant(icf_ctx *ctx, int kind, int variant);
  * caller's device arrays d_vals (nnz*9) and d_rhs (N*3), with every temporary
  * held in one 8 MiB static device array that each GPU loading the library keeps
  * until exit.  It calls no cudaMalloc or cudaFree.  Models whose temporaries
- * exceed 8 MiB (80 B/node + 256 B/tet + 384 B/CZ + 1104 B/impact) get
+ * exceed 8 MiB (80 B/node + 256 B/tet + 384 B/CZ + 1056 B/impact) get
  * ICF_ERR_SIZE.  The context must hold constants, static data and a structure
  * from earlier calls.  The first call on a device looks up the array's device
  * address (make it before any stream capture).  All calls share the array:

@@ -287,7 +287,7 @@ def test_profile_assembly_kernels(O):
     names = [k["name"] for k in ks]
     assert {"k_tet_unit", "k_cz_gp", "k_gather_off", "k_gather_diag"} <= set(names)
     if len(gf.c_itet):
-        assert {"k_imp_classify", "k_imp_deriv", "k_imp_add"} <= set(names)
+        assert {"k_imp_deriv", "k_imp_add"} <= set(names)
     assert all(k["ms"] > 0 and k["bytes"] > 0 for k in ks)
     vals, rhs = gf.TransferLinearSystemToHost()
     assert np.array_equal(vals.ravel(), a["vals"].ravel()) and np.array_equal(rhs.ravel(), a["rhs"].ravel())
