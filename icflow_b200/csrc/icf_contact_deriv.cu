@@ -267,9 +267,11 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
     cl = pt_classify(x);
     if (!(cl.dsq > eps2)) cl.kind = -1;  // within DistanceEpsilon: no response
   }
-  // the impacts that respond, one atomic per warp
-  const unsigned act = __ballot_sync(__activemask(), cl.kind >= 0);
-  if ((threadIdx.x & 31) == __ffs(__activemask()) - 1 && act) atomicAdd(counts + 3, __popc(act));
+  // the impacts that respond, one atomic per group of converged lanes (the
+  // same mask for the vote and the choice of the lane that adds)
+  const unsigned am = __activemask();
+  const unsigned act = __ballot_sync(am, cl.kind >= 0);
+  if ((int)(threadIdx.x & 31) == __ffs(am) - 1 && act) atomicAdd(counts + 3, __popc(act));
   double *fo = frc_out + 12 * (size_t)u;
   if (cl.kind < 0) {  // no response: zero records, zero forces
 #pragma unroll
