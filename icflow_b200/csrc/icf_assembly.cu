@@ -440,11 +440,21 @@ __device__ __forceinline__ void add_row3(double *o, const double v[3]) {
 // Impact contributions, one thread per block they touch: the records of the
 // block's codes (k_imp_deriv writes them at the codes' positions in the
 // slot-sorted list, so a block's records are contiguous; 96 B each, read as
-// three 32 B loads) are summed in code order and added to the block, and to
+// three 32 B loads; FP32-mixed: the FP32 block and the rhs in the first 64 B,
+// two loads) are summed in FP64, in code order, and added to the block, and to
 // the rhs row for a diagonal block (row >= 0).  A block that only contact
 // pairs create (row == -2) is written, not added to: nothing else writes it.
 // The touched blocks come in k_imp_add's order (icf_pattern.cu k_split_off):
 // the launch over [first, first + count) reads its metadata contiguously.
+__device__ __forceinline__ double4 ld_nc4(const double4 *p) {
+  double4 r;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ double lo32(double w) { return (double)__int_as_float(__double2loint(w)); }
+__device__ __forceinline__ double hi32(double w) { return (double)__int_as_float(__double2hiint(w)); }
+
+template <bool MIXED>
 __global__ void k_imp_add(int count, int first, const int2 *__restrict__ range, const int *__restrict__ pslot,
                           const int *__restrict__ row, const double *__restrict__ rec, double *__restrict__ vals,
                           double *__restrict__ rhs, int *__restrict__ nonfinite) {
@@ -457,18 +467,22 @@ __global__ void k_imp_add(int count, int first, const int2 *__restrict__ range, 
     double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int q = qr.x; q < qr.y; q++) {
       const double4 *R = reinterpret_cast<const double4 *>(rec + ICF_IMP_REC * (size_t)q);
-      double4 r[3];
+      if (MIXED) {  // the block in FP32, two values per word, then the rhs
+        const double4 a = ld_nc4(R), b = ld_nc4(R + 1);
+        v[0] += lo32(a.x); v[1] += hi32(a.x); v[2] += lo32(a.y); v[3] += hi32(a.y);
+        v[4] += lo32(a.z); v[5] += hi32(a.z); v[6] += lo32(a.w); v[7] += hi32(a.w);
+        v[8] += lo32(b.x); v[9] += b.y; v[10] += b.z; v[11] += b.w;
+      } else {
+        double4 r[3];
 #pragma unroll
-      for (int k = 0; k < 3; k++)
-        asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
-            : "=d"(r[k].x), "=d"(r[k].y), "=d"(r[k].z), "=d"(r[k].w)
-            : "l"(R + k));
+        for (int k = 0; k < 3; k++) r[k] = ld_nc4(R + k);
 #pragma unroll
-      for (int k = 0; k < 3; k++) {
-        v[4 * k] += r[k].x;
-        v[4 * k + 1] += r[k].y;
-        v[4 * k + 2] += r[k].z;
-        v[4 * k + 3] += r[k].w;
+        for (int k = 0; k < 3; k++) {
+          v[4 * k] += r[k].x;
+          v[4 * k + 1] += r[k].y;
+          v[4 * k + 2] += r[k].z;
+          v[4 * k + 3] += r[k].w;
+        }
       }
     }
 #pragma unroll
@@ -492,6 +506,13 @@ __global__ void k_imp_add(int count, int first, const int2 *__restrict__ range, 
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(nonfinite, 1);
 }
 
+
+// the impact add of the context's record format
+using imp_add_fn = void (*)(int, int, const int2 *, const int *, const int *, const double *, double *, double *,
+                            int *);
+static imp_add_fn imp_add_for(const icf_ctx *ctx) {
+  return ctx->precision == ICF_FP32_MIXED ? k_imp_add<true> : k_imp_add<false>;
+}
 
 // Node forces (the F field of the node array, GPU_Functionality.cs:519-527):
 // per node the sum of the rhs of every tet vertex on it plus impact forces.
@@ -993,13 +1014,13 @@ static int enqueue_assembly(icf_ctx *ctx, double h) {
   const int n_a = ctx->n_crs - ctx->n_crs_off;
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_b, 0));
   if (n_a > 0) {
-    k_imp_add<<<icf_blocks(n_a, 128), 128, 0, s>>>(n_a, 0, ctx->d_cr_range, ctx->d_cr_pslot, ctx->d_cr_row,
+    imp_add_for(ctx)<<<icf_blocks(n_a, 128), 128, 0, s>>>(n_a, 0, ctx->d_cr_range, ctx->d_cr_pslot, ctx->d_cr_row,
                                                   ctx->d_ks, ctx->d_vals, ctx->d_rhs, ctx->d_counts + 4);
     icf_prof_mark(ctx, s, "k_imp_add", imp_in * n_a / ctx->n_crs + 144LL * n_a);
   }
   ICF_CUDA(ctx, cudaStreamWaitEvent(s, e_a, 0));
   if (ctx->n_crs_off > 0 && ctx->n_crs > 0) {
-    k_imp_add<<<icf_blocks(ctx->n_crs_off, 128), 128, 0, s>>>(ctx->n_crs_off, n_a, ctx->d_cr_range,
+    imp_add_for(ctx)<<<icf_blocks(ctx->n_crs_off, 128), 128, 0, s>>>(ctx->n_crs_off, n_a, ctx->d_cr_range,
                                                               ctx->d_cr_pslot, ctx->d_cr_row, ctx->d_ks,
                                                               ctx->d_vals, ctx->d_rhs, ctx->d_counts + 4);
     icf_prof_mark(ctx, s, "k_imp_add_off", imp_in * ctx->n_crs_off / ctx->n_crs + 144LL * ctx->n_crs_off);
@@ -1245,7 +1266,7 @@ static int enqueue_assembly_bufs(icf_ctx *ctx, double h, const icf_asm_bufs &B, 
                                           B.rhs, s));
   }
   if (ctx->n_crs > 0)
-    k_imp_add<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, 0, ctx->d_cr_range, ctx->d_cr_pslot,
+    imp_add_for(ctx)<<<icf_blocks(ctx->n_crs, 128), 128, 0, s>>>(ctx->n_crs, 0, ctx->d_cr_range, ctx->d_cr_pslot,
                                                         ctx->d_cr_row, B.ks, B.vals, B.rhs, ctx->d_counts + 4);
 
   ICF_CUDA(ctx, cudaGetLastError());

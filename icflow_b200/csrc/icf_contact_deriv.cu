@@ -32,7 +32,8 @@
 // contribution code at its position in the slot-sorted list (icf_internal.cuh,
 // ICF_IMP_REC): the block in the code's orientation, then, on a diagonal code,
 // the vertex's rhs from (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp,
-// w = (1-s-t, s, t), else zeros; a record is three 32-byte stores.  A diagonal
+// w = (1-s-t, s, t), else zeros; a record is three 32-byte stores (FP32-mixed:
+// the block in FP32, then the rhs, two 32-byte stores).  A diagonal
 // block's lower entries are its upper ones, so it is symmetric bit for bit.
 // The four vertex forces also go to a per-impact force record (node forces).
 #include "icf_internal.cuh"
@@ -62,21 +63,33 @@ __device__ __forceinline__ void st4(double *p, double a, double b, double c, dou
   asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
 }
 
+// Two FP32 values in one 64-bit word: a in the low half, b in the high half.
+__device__ __forceinline__ double pack2(double a, double b) {
+  return __hiloint2double(__float_as_int((float)b), __float_as_int((float)a));
+}
+
 // The record of vertex pair (bA, bB): to the code (bA, bB) if there is one,
 // else the block transposed to the code (bB, bA) (none: an anchored vertex).
 // Records start at 96-byte multiples, so each third is 32-byte aligned.
+// FP64: the block, then the rhs, in three 32-byte stores.  FP32-mixed: the
+// block rounded to FP32 (two values per 64-bit word), then the rhs in FP64,
+// in the first two 32-byte sectors of the record's slot.
+template <bool MIXED>
 __device__ __forceinline__ void put_record(double *__restrict__ rec, int q, int qt, const double B[9], double f0,
                                            double f1, double f2) {
-  if (q >= 0) {
-    double *o = rec + ICF_IMP_REC * (size_t)q;
-    st4(o, B[0], B[1], B[2], B[3]);
-    st4(o + 4, B[4], B[5], B[6], B[7]);
-    st4(o + 8, B[8], f0, f1, f2);
-  } else if (qt >= 0) {
-    double *o = rec + ICF_IMP_REC * (size_t)qt;
-    st4(o, B[0], B[3], B[6], B[1]);
-    st4(o + 4, B[4], B[7], B[2], B[5]);
-    st4(o + 8, B[8], f0, f1, f2);
+  const bool fw = q >= 0;
+  if (!fw && qt < 0) return;
+  double *o = rec + ICF_IMP_REC * (size_t)(fw ? q : qt);
+  // the entries in the code's orientation
+  const double b0 = B[0], b1 = fw ? B[1] : B[3], b2 = fw ? B[2] : B[6], b3 = fw ? B[3] : B[1], b4 = B[4];
+  const double b5 = fw ? B[5] : B[7], b6 = fw ? B[6] : B[2], b7 = fw ? B[7] : B[5], b8 = B[8];
+  if (MIXED) {
+    st4(o, pack2(b0, b1), pack2(b2, b3), pack2(b4, b5), pack2(b6, b7));
+    st4(o + 4, pack2(b8, 0.0), f0, f1, f2);
+  } else {
+    st4(o, b0, b1, b2, b3);
+    st4(o + 4, b4, b5, b6, b7);
+    st4(o + 8, b8, f0, f1, f2);
   }
 }
 
@@ -191,21 +204,21 @@ __device__ __forceinline__ void block(const Vertex &V, double B[9]) {
   for (int e = 0; e < 9; e++) B[e] = (e % 4 == 0) ? d : 0.0;
 }
 
-template <int bi, int bj, class Region>
+template <int bi, int bj, bool MIXED, class Region>
 __device__ __forceinline__ void emit_pair(const Region &R, double hk, const int pos[16], const double frc[12],
                                           double *__restrict__ rec) {
   double B[9];
   block<bi, bj>(R, B);
 #pragma unroll
   for (int e = 0; e < 9; e++) B[e] *= hk;  // K = k/2 d2''
-  if (bi == bj) put_record(rec, pos[5 * bi], -1, B, frc[3 * bi], frc[3 * bi + 1], frc[3 * bi + 2]);
-  else put_record(rec, pos[4 * bi + bj], pos[4 * bj + bi], B, 0.0, 0.0, 0.0);
+  if (bi == bj) put_record<MIXED>(rec, pos[5 * bi], -1, B, frc[3 * bi], frc[3 * bi + 1], frc[3 * bi + 2]);
+  else put_record<MIXED>(rec, pos[4 * bi + bj], pos[4 * bj + bi], B, 0.0, 0.0, 0.0);
 }
 
 // The impact's vertex forces (-F, w0 F, w1 F, w2 F), F = k/2 d(d2)/dp,
 // w = (1-s-t, s, t) (collision_response.h:89-109), to its force record, then
 // the ten records.
-template <class Region>
+template <bool MIXED, class Region>
 __device__ __forceinline__ void respond(const Region &R, const double fd[3], double hk, double s, double t,
                                         const int pos[16], double *__restrict__ fo, double *__restrict__ rec) {
   double frc[12];
@@ -220,18 +233,19 @@ __device__ __forceinline__ void respond(const Region &R, const double fd[3], dou
   }
 #pragma unroll
   for (int k = 0; k < 12; k += 4) st4(fo + k, frc[k], frc[k + 1], frc[k + 2], frc[k + 3]);
-  emit_pair<0, 0>(R, hk, pos, frc, rec);
-  emit_pair<1, 1>(R, hk, pos, frc, rec);
-  emit_pair<2, 2>(R, hk, pos, frc, rec);
-  emit_pair<3, 3>(R, hk, pos, frc, rec);
-  emit_pair<0, 1>(R, hk, pos, frc, rec);
-  emit_pair<0, 2>(R, hk, pos, frc, rec);
-  emit_pair<0, 3>(R, hk, pos, frc, rec);
-  emit_pair<1, 2>(R, hk, pos, frc, rec);
-  emit_pair<1, 3>(R, hk, pos, frc, rec);
-  emit_pair<2, 3>(R, hk, pos, frc, rec);
+  emit_pair<0, 0, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<1, 1, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<2, 2, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<3, 3, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<0, 1, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<0, 2, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<0, 3, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<1, 2, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<1, 3, MIXED>(R, hk, pos, frc, rec);
+  emit_pair<2, 3, MIXED>(R, hk, pos, frc, rec);
 }
 
+template <bool MIXED>
 __global__ void __launch_bounds__(TPB, IMP_MINB)
     k_imp_deriv(int n, const int4 *__restrict__ imp, const int *__restrict__ alt, const double4 *__restrict__ xc,
                 double eps2, double kpen, const int *__restrict__ pos16, double *__restrict__ rec,
@@ -280,7 +294,7 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
         double *o = rec + ICF_IMP_REC * (size_t)pos[k];
         st4(o, 0.0, 0.0, 0.0, 0.0);
         st4(o + 4, 0.0, 0.0, 0.0, 0.0);
-        st4(o + 8, 0.0, 0.0, 0.0, 0.0);
+        if (!MIXED) st4(o + 8, 0.0, 0.0, 0.0, 0.0);
       }
 #pragma unroll
     for (int k = 0; k < 12; k += 4) st4(fo + k, 0.0, 0.0, 0.0, 0.0);
@@ -297,7 +311,7 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
       const double xb = c.z == 1 ? x[3 + k] : (c.z == 2 ? x[6 + k] : x[9 + k]);
       fd[k] = 2 * (x[k] - xb);
     }
-    respond(Vertex{c.z}, fd, hk, st.x, st.y, pos, fo, rec);
+    respond<MIXED>(Vertex{c.z}, fd, hk, st.x, st.y, pos, fo, rec);
   } else if (kind == 2) {  // edge (ia nearer, ib)
     const int ia = c.y, ib = c.z;
     Line L;
@@ -339,7 +353,7 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
     // f1 - g / f2 differentiated in p: f1' = -2 (q1 - p), f2' = 0
 #pragma unroll
     for (int k = 0; k < 3; k++) fd[k] = -(2 * (Q1[k] - x[k])) - L.gd[k] * L.if2;
-    respond(L, fd, hk, st.x, st.y, pos, fo, rec);
+    respond<MIXED>(L, fd, hk, st.x, st.y, pos, fo, rec);
   } else {  // interior: d2 = D^2 / S
     Plane P;
     double N[3], e1xa[3], axe0[3], e1xN[3], Nxe0[3];
@@ -380,7 +394,7 @@ __global__ void __launch_bounds__(TPB, IMP_MINB)
     // d(d2)/dp = 2 D N / S
 #pragma unroll
     for (int k = 0; k < 3; k++) fd[k] = P.c2 * N[k];
-    respond(P, fd, hk, st.x, st.y, pos, fo, rec);
+    respond<MIXED>(P, fd, hk, st.x, st.y, pos, fo, rec);
   }
 }
 
@@ -394,7 +408,8 @@ int icf_launch_imp_deriv(icf_ctx *ctx, cudaStream_t stream) {
 // point passes its own staging).
 int icf_launch_imp_deriv_bufs(icf_ctx *ctx, const double4 *xc, double *ks, cudaStream_t stream) {
   const double eps2 = ctx->prm.DistanceEpsilon * ctx->prm.DistanceEpsilon;
-  k_imp_deriv<<<icf_blocks(ctx->n_imp, TPB), TPB, 0, stream>>>(ctx->n_imp, ctx->d_imp, ctx->d_alt, xc, eps2,
+  auto kern = ctx->precision == ICF_FP32_MIXED ? k_imp_deriv<true> : k_imp_deriv<false>;
+  kern<<<icf_blocks(ctx->n_imp, TPB), TPB, 0, stream>>>(ctx->n_imp, ctx->d_imp, ctx->d_alt, xc, eps2,
                                                                 ctx->prm.penaltyK, ctx->d_imp_pos, ks,
                                                                 icf_imp_forces(ks, ctx->n_imp), ctx->d_counts);
   ICF_CUDA(ctx, cudaGetLastError());
