@@ -100,6 +100,36 @@ def test_contact_parity(O):
     gf.close()
 
 
+def test_contact_regions_parity(O):
+    """Every Voronoi region of the point-triangle distance (interior, the three
+    edges, the three vertices: point_triange_v2.h:589-841) through the impact
+    derivative kernel: 400 impacts of random nodes against random faces of
+    the cantilever, injected with SetImpacts, some with anchored vertices (the
+    root face).  The oracle's own region of each impact is tallied to show
+    the coverage; the assembled matrix and rhs match it to 1e-12."""
+    coll = M.cantilever()
+    prms = config_prms(penaltyK=1e8)
+    p = orc_prms_from(O, prms)
+    pmax, tmax, failed = _zeros_cz(coll)
+    state = random_state(coll, 11, du=2e-6)
+    rng = np.random.default_rng(5)
+    faces = coll.faces[rng.integers(0, len(coll.faces), 400)]
+    nodes = rng.integers(0, len(coll.x0), 400)
+    keep = ~np.any(faces == nodes[:, None], axis=1)
+    imps = np.concatenate([nodes[keep, None], faces[keep]], 1).astype(np.int32)
+    # at least one vertex of each impact off the anchors (the others respond nothing)
+    imps = imps[~np.all(coll.anchored[imps], axis=1)]
+    xt = coll.x0 + state[0]
+    branches = [O.pt(xt[i].ravel())[5] for i in imps]
+    assert len(set(branches)) >= 7, sorted(set(branches))
+    gf = _gf(coll, prms)
+    g = gpu_assemble(gf, coll, state, H, pmax, tmax, failed, impacts=imps)
+    o = oracle_assemble(O, p, coll, state, H, pmax, tmax, imps)
+    rep = compare(g, o)
+    print("contact regions:", {b: branches.count(b) for b in sorted(set(branches))}, rep)
+    gf.close()
+
+
 def test_deterministic(O):
     coll = M.polycrystal(n=6, grains=5, seed=2, platens=True, gap=-0.3)
     prms = config_prms(penaltyK=1e8)
