@@ -395,20 +395,17 @@ __device__ __forceinline__ bool pair_exists(int k, int b, const int *__restrict_
 
 // eight threads per surface element b: the entries of the cells its box
 // reaches are dealt out by their index modulo 8, so the threads share the
-// work evenly however it falls into cells; keys k << eb | b of its impacts
-// (k the surface-node index) and a count per surface node
+// work evenly however it falls into cells; keys k << eb | b of the surface
+// nodes k strictly inside b (candidates for k_pair_check)
 #ifndef DET_MINB
 #define DET_MINB 8
 #endif
 __global__ void __launch_bounds__(128, DET_MINB) k_detect(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
                                                 const double *__restrict__ lohi, const int4 *__restrict__ clo,
                                                 const int *__restrict__ gp, const int *__restrict__ goff,
-                                                const double4 *__restrict__ gnode,
-                                                const int *__restrict__ sinc_off, const int *__restrict__ sinc,
-                                                const int *__restrict__ group, int eb,
+                                                const double4 *__restrict__ gnode, int eb,
                                                 unsigned long long *__restrict__ out, long long cap,
-                                                int *__restrict__ count, int *__restrict__ kcnt,
-                                                const double *__restrict__ inv) {
+                                                int *__restrict__ count, const double *__restrict__ inv) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int b = (int)(t >> 3), g = (int)(t & 7);
   if (b >= n || gp[4] != 0) return;
@@ -462,14 +459,35 @@ __global__ void __launch_bounds__(128, DET_MINB) k_detect(int n, const int4 *__r
       }
 #endif
       if (!tet_contains(bi, P.x - x0[0], P.y - x0[1], P.z - x0[2])) continue;
+      // a candidate: the pair rule is checked by k_pair_check, one thread
+      // per candidate, so that its chain of loads stalls no other entry
       const int k = (int)(kp >> ICF_DET_IDBITS);
-      if (!pair_exists(k, b, sinc_off, sinc, lohi, group, selem, xc)) continue;
       const int w = atomicAdd(count, 1);
-      atomicAdd(kcnt + k, 1);
       if (w < cap) out[w] = ((unsigned long long)(unsigned)k << eb) | (unsigned)b;
     }
     e0 = f0;
     e1 = f1;
+  }
+}
+
+// the candidates k << eb | b that satisfy the pair rule (some surface element
+// holding node k forms a candidate pair with b) are counted per surface node
+// and in total; the others become ~0
+__global__ void k_pair_check(long long cap, const int *__restrict__ count, unsigned long long *__restrict__ keys, int eb,
+                             const int *__restrict__ sinc_off, const int *__restrict__ sinc,
+                             const double *__restrict__ lohi, const int *__restrict__ group,
+                             const int4 *__restrict__ selem, const double4 *__restrict__ xc, int *__restrict__ kcnt,
+                             int *__restrict__ valid) {
+  const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= cap || h >= *count) return;
+  const unsigned long long key = keys[h];
+  const int k = (int)(key >> eb);
+  const int b = (int)(key & ((1ull << eb) - 1));
+  if (pair_exists(k, b, sinc_off, sinc, lohi, group, selem, xc)) {
+    atomicAdd(kcnt + k, 1);
+    atomicAdd(valid, 1);
+  } else {
+    keys[h] = ~0ull;
   }
 }
 
@@ -481,6 +499,7 @@ __global__ void k_place(long long cap, const int *__restrict__ count, const unsi
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= cap || h >= *count) return;
   const unsigned long long key = in[h];
+  if (key == ~0ull) return;  // failed the pair rule
   const int k = (int)(key >> eb);
   const unsigned long long b = key & ((1ull << eb) - 1);
   const long long p = (long long)koff[k] + atomicAdd(kcur + k, 1);
@@ -680,11 +699,13 @@ static int enqueue_detect(icf_ctx *ctx, double pad, const int *d_group, int eb, 
   k_node_put<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, ctx->d_snode, ctx->d_xc, W.red, W.gp, W.gcur, W.goff, W.gnode);
   // every element's cells
   k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
-  ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, sizeof(int), s));
+  ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, 2 * sizeof(int), s));
   ICF_CUDA(ctx, cudaMemsetAsync(W.kcnt, 0, sizeof(int) * (ns + 1LL), s));
   k_detect<<<icf_blocks(8LL * n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, W.gp, W.goff, W.gnode,
-                                                   ctx->d_sinc_off, ctx->d_sinc, d_group, eb, W.nk0,
-                                                   W.nkey_cap, W.d_small + 5, W.kcnt, W.tinv);
+                                                   eb, W.nk0, W.nkey_cap, W.d_small + 5, W.tinv);
+  k_pair_check<<<icf_blocks(W.nkey_cap, 256), 256, 0, s>>>(W.nkey_cap, W.d_small + 5, W.nk0, eb, ctx->d_sinc_off,
+                                                          ctx->d_sinc, W.lohi, d_group, ctx->d_selem, ctx->d_xc,
+                                                          W.kcnt, W.d_small + 6);
   ICF_CUDA(ctx, cudaGetLastError());
   // grouped by surface node (a counting sort), each node's hits sorted: the
   // keys node << eb | element ascending
@@ -694,8 +715,10 @@ static int enqueue_detect(icf_ctx *ctx, double pad, const int *d_group, int eb, 
   k_place<<<icf_blocks(W.nkey_cap, 256), 256, 0, s>>>(W.nkey_cap, W.d_small + 5, W.nk0, eb, W.koff, W.kcur,
                                                      ctx->d_snode, W.nk1);
   k_sort_seg<<<icf_blocks(ns, 256), 256, 0, s>>>(ns, W.nkey_cap, W.koff, W.nk1);
-  // the grid's status and size come back with the impact count
+  // the grid's status and size and the candidate count come back with the
+  // impact count
   ICF_CUDA(ctx, cudaMemcpyAsync(W.h_gp, W.gp, 5 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ICF_CUDA(ctx, cudaMemcpyAsync(W.h_small + 2, W.d_small + 5, sizeof(int), cudaMemcpyDeviceToHost, s));
   ICF_CUDA(ctx, cudaGetLastError());
   return ICF_OK;
 }
@@ -757,7 +780,7 @@ static int detect_pass(icf_ctx *ctx, double pad, const int *d_group, int *n_impa
     W.det_key = key;
   }
   ICF_CUDA(ctx, cudaGraphLaunch(W.det_exec, s));
-  ICF_TRY_RC(icf_finish_impacts(ctx, W.nk1, (int)W.nkey_cap, W.d_small + 5, eb, n_impacts));
+  ICF_TRY_RC(icf_finish_impacts(ctx, W.nk1, (int)W.nkey_cap, W.d_small + 6, eb, n_impacts));
   const int st = W.h_gp[4];
   if (st == 1) return icf_fail(ctx, ICF_ERR_NUMERIC, "contact detection: degenerate boxes");
   if (st == 2) return icf_fail(ctx, ICF_ERR_SIZE, "contact detection: grid too large");
@@ -770,8 +793,8 @@ static int detect_pass(icf_ctx *ctx, double pad, const int *d_group, int *n_impa
     W.cell_cap = c;
     *again = true;
   }
-  const long long hits = W.h_small[0];
-  if (hits > W.nkey_cap) {  // more hits than the key buffers hold
+  const long long hits = W.h_small[2];  // candidates, before the pair rule
+  if (hits > W.nkey_cap) {  // more candidates than the key buffers hold
     const long long c = hits + hits / 4 + 1024;
     ICF_TRY_RC(grow(ctx, &W.nk0, c));
     ICF_TRY_RC(grow(ctx, &W.nk1, c));
