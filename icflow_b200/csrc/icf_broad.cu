@@ -393,12 +393,16 @@ __device__ __forceinline__ bool pair_exists(int k, int b, const int *__restrict_
   return false;
 }
 
-// eight threads per surface element b: the entries of the cells its box
-// reaches are dealt out by their index modulo 8, so the threads share the
-// work evenly however it falls into cells; keys k << eb | b of the surface
-// nodes k strictly inside b (candidates for k_pair_check)
+// DET_TPE threads per surface element b (four: 2, 8, 16 and 32 measured
+// slower over cfg1 and cfg2): the entries of the cells its box reaches are
+// dealt out by their index modulo DET_TPE, so the threads share the work
+// evenly however it falls into cells; keys k << eb | b of the surface nodes k
+// strictly inside b (candidates for k_pair_check)
 #ifndef DET_MINB
 #define DET_MINB 8
+#endif
+#ifndef DET_TPE
+#define DET_TPE 4  // threads per surface element (a power of two)
 #endif
 __global__ void __launch_bounds__(128, DET_MINB) k_detect(int n, const int4 *__restrict__ selem, const double4 *__restrict__ xc,
                                                 const double *__restrict__ lohi, const int4 *__restrict__ clo,
@@ -407,7 +411,7 @@ __global__ void __launch_bounds__(128, DET_MINB) k_detect(int n, const int4 *__r
                                                 unsigned long long *__restrict__ out, long long cap,
                                                 int *__restrict__ count, const double *__restrict__ inv) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = (int)(t >> 3), g = (int)(t & 7);
+  const int b = (int)(t / DET_TPE), g = (int)(t % DET_TPE);
   if (b >= n || gp[4] != 0) return;
   const int ny = gp[1], nz = gp[2];
   const int4 B = selem[b];
@@ -421,17 +425,6 @@ __global__ void __launch_bounds__(128, DET_MINB) k_detect(int n, const int4 *__r
   const int ncol = (sx + 1) * (sy + 1);
   long long l = cell_lin(c.x, c.y, c.z, ny, nz);
   int e0 = goff[l], e1 = goff[l + sz + 1];
-#ifdef DET_PREFETCH_INV
-  // b's inverse and first vertex (the eight threads read the same line)
-  double bi[9], x0[3];
-  {
-    const double2 *r = reinterpret_cast<const double2 *>(inv + 12 * (size_t)b);
-    const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5];
-    bi[0] = r0.x; bi[1] = r0.y; bi[2] = r1.x; bi[3] = r1.y; bi[4] = r2.x; bi[5] = r2.y;
-    bi[6] = r3.x; bi[7] = r3.y; bi[8] = r4.x;
-    x0[0] = r4.y; x0[1] = r5.x; x0[2] = r5.y;
-  }
-#endif
   for (int j = 0; j < ncol; j++) {
     int f0 = 0, f1 = 0;
     if (j + 1 < ncol) {
@@ -440,14 +433,13 @@ __global__ void __launch_bounds__(128, DET_MINB) k_detect(int n, const int4 *__r
       f0 = goff[l];
       f1 = goff[l + sz + 1];
     }
-    // thread g takes the entries whose index is g modulo 8
-    for (int e = e0 + ((g - e0) & 7); e < e1; e += 8) {
+    // thread g takes the entries whose index is g modulo DET_TPE
+    for (int e = e0 + ((g - e0) & (DET_TPE - 1)); e < e1; e += DET_TPE) {
       const double4 P = gnode[e];
       if (!(P.x >= lx && P.x <= hx && P.y >= ly && P.y <= hy && P.z >= lz && P.z <= hz)) continue;
       const long long kp = (long long)P.w;
       const int p = (int)(kp & ((1LL << ICF_DET_IDBITS) - 1));
       if (p == B.x || p == B.y || p == B.z || p == B.w) continue;
-#ifndef DET_PREFETCH_INV
       // b's inverse and first vertex, read when a node lies in its box
       double bi[9], x0[3];
       {
@@ -457,7 +449,6 @@ __global__ void __launch_bounds__(128, DET_MINB) k_detect(int n, const int4 *__r
         bi[6] = r3.x; bi[7] = r3.y; bi[8] = r4.x;
         x0[0] = r4.y; x0[1] = r5.x; x0[2] = r5.y;
       }
-#endif
       if (!tet_contains(bi, P.x - x0[0], P.y - x0[1], P.z - x0[2])) continue;
       // a candidate: the pair rule is checked by k_pair_check, one thread
       // per candidate, so that its chain of loads stalls no other entry
@@ -701,7 +692,7 @@ static int enqueue_detect(icf_ctx *ctx, double pad, const int *d_group, int eb, 
   k_cells<<<icf_blocks(n, 256), 256, 0, s>>>(n, W.lohi, W.red, W.bcnt, W.clo);
   ICF_CUDA(ctx, cudaMemsetAsync(W.d_small + 5, 0, 2 * sizeof(int), s));
   ICF_CUDA(ctx, cudaMemsetAsync(W.kcnt, 0, sizeof(int) * (ns + 1LL), s));
-  k_detect<<<icf_blocks(8LL * n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, W.gp, W.goff, W.gnode,
+  k_detect<<<icf_blocks((long long)DET_TPE * n, 128), 128, 0, s>>>(n, ctx->d_selem, ctx->d_xc, W.lohi, W.clo, W.gp, W.goff, W.gnode,
                                                    eb, W.nk0, W.nkey_cap, W.d_small + 5, W.tinv);
   k_pair_check<<<icf_blocks(W.nkey_cap, 256), 256, 0, s>>>(W.nkey_cap, W.d_small + 5, W.nk0, eb, ctx->d_sinc_off,
                                                           ctx->d_sinc, W.lohi, d_group, ctx->d_selem, ctx->d_xc,
