@@ -207,6 +207,8 @@ class _Reader:
             return _Nulls(self.take("<i"))
         if rt == ARRAY_PRIMITIVE:
             oid, n, t = self.take("<i"), self.take("<i"), self.take("<B")
+            if n < 0:
+                raise NrbfError(f"bad array length {n}")
             if t in _PRIM and t != P_CHAR:
                 fmt = _PRIM[t][1]
                 size = struct.calcsize("<" + fmt)
@@ -241,6 +243,8 @@ class _Reader:
                 info = (self.string(), self.take("<i"))
             total = 1
             for n in lens:
+                if n < 0:
+                    raise NrbfError(f"bad array length {n}")
                 total *= n
             arr = self.elements(total, t, info)
             self.objs[oid] = arr
@@ -250,6 +254,8 @@ class _Reader:
         raise NrbfError(f"unsupported record type {rt}")
 
     def elements(self, n, t, info):
+        if n < 0 or n > len(self.b):  # every element takes at least one byte
+            raise NrbfError(f"bad array length {n}")
         out = []
         while len(out) < n:
             if t == BT_PRIMITIVE:
@@ -257,11 +263,11 @@ class _Reader:
                 continue
             v = self.value()
             if isinstance(v, _Nulls):
+                if v.n < 0 or len(out) + v.n > n:
+                    raise NrbfError("null run past the end of an array")
                 out.extend([None] * v.n)
             else:
                 out.append(v)
-        if len(out) != n:
-            raise NrbfError("null run past the end of an array")
         return out
 
     def resolve(self, v, seen):

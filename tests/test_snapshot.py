@@ -174,3 +174,15 @@ def test_nrbf_fragment_records():
     assert items[0]["faces"].type_name.startswith("System.Collections.Generic.List`1[[System.Int32, mscorlib")
     assert blob.count(bytes([nrbf.CLASS_WITH_ID])) >= 1
     assert S._fragments_from(root) == frags
+
+
+def test_nrbf_rejects_bad_lengths():
+    """Negative lengths and null runs past an array's end raise instead of
+    allocating."""
+    head = bytes([0]) + struct.pack("<4i", 1, -1, 1, 0)
+    bad_prim = head + bytes([15]) + struct.pack("<2i", 1, -5) + bytes([8]) + bytes([11])
+    bad_run = head + bytes([16]) + struct.pack("<2i", 1, 2) + bytes([14]) + struct.pack("<i", 1 << 30) + bytes([11])
+    huge = head + bytes([16]) + struct.pack("<2i", 1, 1 << 30) + bytes([11])
+    for b in (bad_prim, bad_run, huge):
+        with pytest.raises(nrbf.NrbfError):
+            nrbf.read(b)
