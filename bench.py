@@ -577,6 +577,38 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
+def run_learned(args):
+    """The second metric, Newton iterations per attempt with the learned warm
+    start against the plain guess: the same 200 us of the ice-block impact
+    (two blocks of 1,536 tets, 8 grains each, 5 m/s, dt 5 us, the reference's
+    step control, Newton to 1e-8 of the zero-increment residual) under v h,
+    the extrapolation, and the extrapolation plus the network trained on the
+    device on four other impacts.  One JSON line on rank 0."""
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    import torch
+
+    from icflow_b200.warm_start import three_arms
+
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    r = three_arms()
+    wall = time.perf_counter() - t0
+    plain, ext, net = r["plain"], r["extrapolation"], r["network"]
+    line = {"metric": "iters/step learned vs plain", "value": net[0] / net[1], "unit": "Newton iterations per attempt",
+            "higher_is_better": False, "n_gpus": 1, "data": "synthetic (seeded)",
+            "config": {"workload": "ice-block impact, 2 x 1,536 tets, 8 grains each, 5 m/s relative, dt 5 us, "
+                                   "200 us simulated, residual tolerance 1e-8, reference step control"},
+            "arms": {k: {"iterations": v[0], "attempts": v[1], "accepted": v[2], "per_attempt": v[0] / v[1]}
+                     for k, v in (("plain", plain), ("extrapolation", ext), ("network", net))},
+            "fewer_than_plain": 1 - net[0] / plain[0], "extrapolation_fewer_than_plain": 1 - ext[0] / plain[0],
+            "network_fewer_than_extrapolation": 1 - net[0] / ext[0],
+            "network_used": r["network_used"], "attempts_judged": r["attempts_judged"],
+            "training_loss": r["training_loss"], "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -594,8 +626,13 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="fp64, or FP32 Hessian arithmetic with FP64 rotation, law, rhs and accumulation "
                          "(default: fp64 for cfg1/cfg2, mixed for cfg3); the line also carries the other")
+    ap.add_argument("--learned", action="store_true",
+                    help="measure the second metric instead: Newton iterations per attempt, learned warm start "
+                         "against the plain guess, on the ice-block impact")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.learned:
+        run_learned(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -5,10 +5,7 @@ tolerance."""
 import numpy as np
 import pytest
 
-from icflow_b200 import mesh as M
-from icflow_b200.implicit_model import ImplicitModel3
-from icflow_b200.model_prms import config_prms
-from icflow_b200.warm_start import MLP, LearnedWarmStart, init_params
+from icflow_b200.warm_start import MLP, init_params, three_arms
 from oracle.mlp_oracle import NI, NO, check_trace, forward, loss_and_grad
 
 pytestmark = pytest.mark.gpu
@@ -84,34 +81,6 @@ def test_training_fits_a_smooth_map():
     net.close()
 
 
-def _ice(speed, seed, n=8):
-    """Two ice blocks (cfg4's geometry at n = 8: 1,536 tets per block, 8
-    grains) approaching at 2 x speed, penalty contact, dt 5 us, Newton to a
-    residual of 1e-8 of the zero-increment residual, with the reference's
-    step control."""
-    c, v0 = M.ice_impact(n=n, grains=8, seed=seed, speed=speed)
-    sig = np.concatenate([M.lognormal_strengths(len(m.czs), seed=seed * 10 + i, granule_pairs=m.cz_grains)
-                          for i, m in enumerate(c.meshes)])
-    p = config_prms(penaltyK=1e8)
-    p.InitialTimeStep = 5e-6
-    p.CollisionScheme = 1
-    p.minIterations = 1
-    p.maxIterations = 12
-    return ImplicitModel3(c, p, strengths=sig, contact=True, v0=v0, convergence="residual", res_tol=1e-8,
-                          rel_tol=1e-10)
-
-
-def _run(warm, speed=2.5, seed=1, recorder=None, t_end=40 * 5e-6):
-    g = _ice(speed, seed)
-    g.recorder = recorder
-    while g.t < t_end * (1 - 1e-9):
-        g.Step(warm_start=warm)
-    its = sum(s.iterations for s in g.history)
-    attempts, accepted = len(g.history), sum(s.accepted for s in g.history)
-    g.close()
-    return its, attempts, accepted
-
-
 def test_learned_warm_start_on_ice_impact():
     """Three arms over the same 200 us of an ice-block impact (contact onset,
     damage, step control discarding and halving steps), each to the same
@@ -122,22 +91,13 @@ def test_learned_warm_start_on_ice_impact():
     impacts (speeds 1.5-3 m/s, other grain seeds).  Asserted: the network arm
     needs fewer Newton iterations than the extrapolation alone, which needs
     fewer than v h; measured 671 / 694 / 754 over about 480 attempts."""
-    extrap = lambda m, h, u, v, a: m.extrapolation(h, v)
-    plain = _run(None)
-    ext = _run(extrap)
-    ws = LearnedWarmStart(seed=0)
-    for speed, seed in ((2.0, 2), (3.0, 3), (2.5, 4), (1.5, 5)):
-        _run(extrap, speed, seed, recorder=ws)
-    loss = ws.fit(epochs=80, batch=4096, lr=2e-3)
-    ws.select_gains = (0.0, 0.5, 1.0)
-    ws.chosen = []
-    net = _run(ws)
-    used = sum(g > 0 for g in ws.chosen)
+    r = three_arms()
+    plain, ext, net, used = r["plain"], r["extrapolation"], r["network"], r["network_used"]
+    loss = r["training_loss"]
     print(f"ice impact, Newton iterations over 200 us: v h {plain[0]} ({plain[1]} attempts), extrapolation "
           f"{ext[0]} ({100 * (1 - ext[0] / plain[0]):.1f} % fewer), extrapolation + network {net[0]} "
           f"({100 * (1 - net[0] / plain[0]):.1f} % fewer than v h, {100 * (1 - net[0] / ext[0]):.1f} % fewer than "
-          f"the extrapolation); network correction used on {used} of {len(ws.chosen)} attempts; training loss "
+          f"the extrapolation); network correction used on {used} of {r['attempts_judged']} attempts; training loss "
           f"{loss:.3f} of the correction's variance")
     assert net[0] < ext[0] < plain[0], (plain, ext, net)
     assert used > 0
-    ws.close()
