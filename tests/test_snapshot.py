@@ -186,3 +186,17 @@ def test_nrbf_rejects_bad_lengths():
     for b in (bad_prim, bad_run, huge):
         with pytest.raises(nrbf.NrbfError):
             nrbf.read(b)
+
+
+@pytest.mark.parametrize("n", [1, 3, 4, 5, 300, 513])
+def test_translation_lists_of_every_null_run(n):
+    """TranslationCollection round trips whatever its capacity leaves empty:
+    no nulls, one (ObjectNull), a short run (ObjectNullMultiple256) and a long
+    one (ObjectNullMultiple)."""
+    trans = [S.Translation(0.001 * i, -0.002 * i, 0.5, 1e-3 * i) for i in range(n)]
+    blob = S._translations_blob(trans)
+    root, end = nrbf.read(blob)
+    assert end == len(blob)
+    assert S._translations_from(root) == trans
+    cap = max(4, 1 << (n - 1).bit_length())
+    assert len(root.member("_items")) == cap
